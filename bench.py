@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Bond-force evaluations per second of the pdMTEL hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the pre-cracked plate, 400x400x4 nodes on a cubic lattice (spacing
+0.5 mm, horizon 3.015 spacings, E = 72 GPa, rho = 2440 kg/m^3, 2x2x2 Gauss
+points with MLS), a central 40 mm slit along x through the thickness, +-0.05
+m/s on the top and bottom node layers, dt = 5e-9 s, from rest.  Synthetic
+input (a generated lattice); one step is one RK4 step (4 stages, each one
+Gauss-point force evaluation per unbroken family entry and point).
+
+ours: the FP32-compensated form is the headline `value`; the FP64 drop-in is
+timed beside it (`fp64`) and the relative displacement/velocity error of the
+FP32 form against it after W+K steps is reported.  `e2e` is the same metric
+through the C ABI with host buffers (pd_rk4_steps_host, one step per call:
+state uploaded from pinned memory and downloaded every step).
+
+reference: the reference CPU solver (oracle/_ref, built from the reference
+sources) on a 40x40x4 sub-plate of the same workload, one process per host
+core, each step one RK4 step of every process.
+
+Multi-GPU: replicas (one full plate per rank, no data-path collective);
+weak scaling; time = max over ranks of the device-timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bond-force evals/s on 1 B200: FP32-comp vs FP64 at ≤1e-6 rel err; adjoint s/step"
+UNIT = "bond-force evals/s"
+PLATE = dict(dims=(400, 400, 4), spacing=5e-4, slit_half_length=0.02, vel=0.05, dt=5e-9)
+SUBPLATE = dict(dims=(40, 40, 4), spacing=5e-4, slit_half_length=0.004, vel=0.05, dt=5e-9)
+FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9  # FP32 lanes x FMA x max SM clock
+FLOP_PER_EVAL = 22
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_plate(workdir, cfg):
+    import pdmtel_b200 as P
+    from pdmtel_b200 import decks as D
+    deck = D.config_plate(dims=cfg["dims"], spacing=cfg["spacing"], slit_half_length=cfg["slit_half_length"],
+                          vel=cfg["vel"], dt=cfg["dt"], steps=100000)
+    deck.write(workdir)
+    t0 = time.time()
+    dm = P.pdDataManager(workdir)
+    P.pdSolve.InitialProblem(dm)
+    ctx = dm.context()
+    ctx.set_energy(False)
+    return dm, ctx, time.time() - t0
+
+
+def cpu_baseline_reference(workers, steps, tmp):
+    """Times the reference solver on the 40x40x4 sub-plate with `workers`
+    concurrent processes; returns (evals/s aggregate, details)."""
+    from pdmtel_b200 import decks as D
+    harness = os.path.join(ROOT, "oracle", "_ref", "pdref_harness")
+    if not os.path.exists(harness):
+        return None
+    cfg = SUBPLATE
+    procs = []
+    for w in range(workers):
+        wd = os.path.join(tmp, f"ref{w}")
+        D.config_plate(dims=cfg["dims"], spacing=cfg["spacing"], slit_half_length=cfg["slit_half_length"],
+                       vel=cfg["vel"], dt=cfg["dt"], steps=100000).write(wd)
+        procs.append(subprocess.Popen([harness, "time", wd, str(steps)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True))
+    outs = [json.loads(p.communicate()[0]) for p in procs]
+    return outs
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    workers = max(1, min(os.cpu_count() or 1, 32))
+    tmp = tempfile.mkdtemp(prefix="pdref_")
+    outs = cpu_baseline_reference(workers, args.warmup + args.steps, tmp)
+    if outs is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pdref_harness is not built "
+                          "(run make -C oracle where the reference sources exist)"}))
+        return 0
+    ev = sum(o["evals_per_step"] for o in outs)
+    t_steps = max(sum(o["step_s"][args.warmup:]) for o in outs)
+    value = ev * args.steps / t_steps
+    ms = 1e3 * t_steps / args.steps
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "plate 400x400x4 (sample: 40x40x4 sub-plate per process)",
+                       "sample_nodes": outs[0]["nodes"], "processes": workers},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "reference",
+                             "sample": f"{workers} processes x 40x40x4 sub-plate, {args.steps} timed RK4 steps each"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import pdmtel_b200 as P
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    tmp = tempfile.mkdtemp(prefix=f"pdbench{rank}_")
+    cfg = PLATE
+    dm, ctx, setup_s = setup_plate(tmp, cfg)
+    dt = cfg["dt"]
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    evals_stage = ctx.evals_per_stage()
+    evals_step = 4 * evals_stage
+    n = ctx.n
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(prec, sampler=None):
+        ctx.set_precision(prec)
+        ctx.reset_state()
+        ctx.rk4_steps(dt, 0.0, args.warmup)
+        ctx.sync()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.start()
+        e0.record(stream)
+        ctx.rk4_steps(dt, args.warmup * dt, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        U, V = ctx.get_state()
+        return ms, U, V, clocks
+
+    sampler = ClockSampler(dev)
+    ms32, U32, V32, clocks = timed(P.PREC_FP32C, sampler)
+    ms64, U64, V64, _ = timed(P.PREC_FP64)
+    err_u = float(np.linalg.norm(U32 - U64) / max(np.linalg.norm(U64), 1e-300))
+    err_v = float(np.linalg.norm(V32 - V64) / max(np.linalg.norm(V64), 1e-300))
+
+    # per-kernel device times of one step, FP32 form (events on the context stream)
+    ctx.set_precision(P.PREC_FP32C)
+    prof = np.zeros(4)
+    reps = 3
+    t = (args.warmup + args.steps) * dt
+    for _ in range(reps):
+        t += dt
+        prof += ctx.profile_step(dt, t)
+    prof /= reps
+    ctx.set_precision(P.PREC_FP64)
+    prof64 = ctx.profile_step(dt, t + dt)
+
+    # end to end through the C ABI with host buffers
+    ctx.set_precision(P.PREC_FP32C)
+    ctx.reset_state()
+    hU = torch.zeros(3 * n, dtype=torch.float64).pin_memory()
+    hV = torch.zeros(3 * n, dtype=torch.float64).pin_memory()
+    import ctypes as C
+    pU = C.cast(hU.data_ptr(), C.POINTER(C.c_double))
+    pV = C.cast(hV.data_ptr(), C.POINTER(C.c_double))
+    L = P.lib()
+    for k in range(args.warmup):
+        L.pd_rk4_steps_host(ctx.h, dt, k * dt, 1, pU, pV, pU, pV)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        rc = L.pd_rk4_steps_host(ctx.h, dt, (args.warmup + k) * dt, 1, pU, pV, pU, pV)
+        if rc != 0:
+            raise P.PdError(rc, "pd_rk4_steps_host")
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+
+    I = dm.info()
+    hbm_peak, peak_kind = load_peaks()
+    force_ms = prof[0] / 4.0  # one launch per stage
+    gather_ms = prof[1] / 4.0
+    npt = I.num_gauss
+    ncb = I.num_contrib
+    gather_bytes = ncb * npt * 4 + ncb * 4 + n * 8 * 4 + n * npt * 12 + n * npt * 4 + (n + 1) * 8
+    force_flops = FLOP_PER_EVAL * evals_stage
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("force_f32c_bytes_per_launch")
+    value = ws * evals_step * args.steps / (ms32 / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "plate 400x400x4, 2x2x2 Gauss+MLS, 40 mm slit, +-0.05 m/s, dt 5e-9",
+                   "nodes": n, "bond_halves": I.num_halves, "broken_halves": I.num_broken,
+                   "evals_per_step": evals_step, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (MLS coefficients and family lists are GBs per step)",
+                   "form": "FP32 forces + Kahan family sums, FP64 state"},
+        "fp64": {"value": ws * evals_step * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                 "speedup_fp32c_over_fp64": ms64 / ms32},
+        "rel_err_vs_fp64": {"U": err_u, "V": err_v, "after_steps": args.warmup + args.steps},
+        "e2e": {"value": ws * evals_step * args.steps / (ms_e2e / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 2 * 3 * n * 8, "d2h_bytes_per_step": 2 * 3 * n * 8},
+        "gpu_launches": 13 * args.steps,
+        "roofline": {"bound": "fp32", "kernel": "k_force_f32c", "achieved": force_flops / (force_ms / 1e3) / 1e12,
+                     "peak": FP32_PEAK_NOMINAL / 1e12, "unit": "TFLOP/s",
+                     "frac": force_flops / (force_ms / 1e3) / FP32_PEAK_NOMINAL, "traffic": traffic,
+                     "peak_kind": "nominal FP32 (148 SMs x 128 lanes x FMA x 1965 MHz); no measured FP32 peak",
+                     "launch_ms": force_ms, "flop_per_launch": force_flops},
+        "roofline_gather": {"bound": "hbm", "kernel": "k_gather_f32c",
+                            "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                            "frac": gather_bytes / (gather_ms / 1e3) / 1e9 / hbm_peak,
+                            "peak_kind": peak_kind, "launch_ms": gather_ms, "bytes_per_launch": gather_bytes},
+        "kernel_ms_per_step": {"fp32c": {"force": prof[0], "gather": prof[1], "epilogue": prof[2], "other": prof[3]},
+                               "fp64": {"force": prof64[0], "gather": prof64[1], "epilogue": prof64[2],
+                                        "other": prof64[3]}},
+        "clocks": clocks, "setup_s": setup_s,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        outs = cpu_baseline_reference(1, 2, tmp)
+        if outs:
+            o = outs[0]
+            line["cpu_baseline"] = {"value": o["evals_per_step"] / o["step_s"][-1], "unit": UNIT, "cores": 1,
+                                    "kind": "reference",
+                                    "sample": "40x40x4 sub-plate of the workload, reference solver, 2nd RK4 step"}
+        else:
+            line["cpu_baseline"] = None
+    if rank == 0:
+        print(json.dumps(line))
+    shutil.rmtree(tmp, ignore_errors=True)
+    del ctx
+    dm.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

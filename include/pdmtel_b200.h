@@ -1,0 +1,197 @@
+/*
+ * pdmtel_b200.h — C ABI of the B200 pdMTEL hot path (libpdmtel_b200.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status:
+ * PD_OK (0) or a negative PD_ERR_* code; pd_last_error() gives a message.
+ * Host arrays are caller-owned and copied; device memory is owned by the
+ * context.  One CUDA stream per context (given in pd_problem.stream, or
+ * created).  A context is not thread-safe; distinct contexts may be used from
+ * distinct threads.
+ *
+ * Vectors of node quantities use the reference's row order (3*i + a, the
+ * "_rowOfNode" layout of pdDataManager.cpp:1089-1091).  Gauss-point
+ * displacements are [node][point][3] (the pdNode Gaussian point list order,
+ * pdDataManager2.cpp:72-104).
+ */
+#ifndef PDMTEL_B200_H
+#define PDMTEL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PD_ABI_VERSION 1
+
+enum pd_status {
+    PD_OK = 0,
+    PD_ERR_ARG = -1,       /* bad argument or call order */
+    PD_ERR_OOM = -2,       /* device or host allocation failed */
+    PD_ERR_CUDA = -3,      /* CUDA runtime error */
+    PD_ERR_TIMEOUT = -4,   /* a bounded device wait gave up */
+    PD_ERR_SINGULAR = -5,  /* singular MLS moment matrix (pdMatrix.cpp:297,335) */
+    PD_ERR_CAPACITY = -6,  /* caller buffer too small */
+    PD_ERR_NOCONV = -7,    /* iterative solve did not reach the tolerance */
+    PD_ERR_NODEV = -8      /* no CUDA device */
+};
+
+/* boundary-condition types, pdDataManager.h:231 / pdBdryCondition.h:25 */
+enum pd_bc_type { PD_BC_DISPL = 1, PD_BC_VELOC = 2, PD_BC_DISPLGRAD = 3, PD_BC_TRACTION = 4 };
+/* volume integration scheme, pdDataManager.cpp:571-730 */
+enum pd_integration { PD_INTG_CCI = 0, PD_INTG_FGI = 1 };
+/* arithmetic of the force / gather / matvec kernels */
+enum pd_precision {
+    PD_PREC_FP64 = 0,  /* the drop-in: bit-faithful to the reference CPU path */
+    PD_PREC_FP32C = 1  /* FP32 forces, compensated sums, FP64 state */
+};
+
+/* bond-based (PMB) material, pdMaterialBond.cpp:8-11; spring = 18K/(pi d^4)
+ * as pdDataManager.cpp:1314 computes it */
+typedef struct pd_material {
+    double spring;
+    double density;
+    double ecrit;
+    double grav[3];
+} pd_material;
+
+/* pdBdryCondition (pdBdryCondition.h:25-67): value[3] for DISPL, VELOC and
+ * TRACTION, value[9] (row-major gradient) for DISPLGRAD; load_type 1 = ramp */
+typedef struct pd_bc {
+    int32_t type;
+    int32_t dir[3];
+    double value[9];
+    double end_time;
+    double load_type;
+} pd_bc;
+
+typedef struct pd_problem {
+    int64_t num_nodes;
+    const double* coords;        /* [N][3] (pdDataManager.cpp:846-907) */
+    const int32_t* mat_id;       /* [N] material index (0-based) */
+    const int32_t* bc_id;        /* [N] bc index or -1; NULL = none */
+    int32_t num_materials;
+    const pd_material* materials;
+    int32_t num_bcs;
+    const pd_bc* bcs;
+    double grid_spacing;         /* _gridSpacing */
+    double horizon;              /* _horizon */
+    int32_t integration;         /* pd_integration */
+    int32_t cci_modified;        /* _cciMdf */
+    int32_t intg_point;          /* 1-D Gauss order n (FGI); n^3 points */
+    const double* abscissae;     /* [n], pdDataManager3.cpp:1706-1799 */
+    const double* weights;       /* [n] */
+    double damping;              /* _dampCoeff */
+    int32_t num_slits;           /* slit rectangles x1lo x1hi x2lo x2hi x3lo x3hi */
+    const double* slits;
+    const double* spring_factor; /* [N] per-node micromodulus factor, or NULL */
+    void* stream;                /* cudaStream_t to run on, or NULL */
+} pd_problem;
+
+typedef struct pd_ctx pd_ctx;
+
+int pd_abi_version(void);
+const char* pd_last_error(void);
+/* number of CUDA devices visible (0 on a machine without a GPU) */
+int pd_device_count(int* count);
+
+/* Allocates the device arrays of one problem (pdDataManager state of
+ * pdDataManager.h:169-234).  Replaces the data set up by InitNode and
+ * InitMaterial (pdDataManager.cpp:813-1098,1297-1338). */
+int pd_ctx_create(const pd_problem* problem, pd_ctx** out);
+int pd_ctx_destroy(pd_ctx* ctx);
+/* the CUDA stream of the context (cudaStream_t) */
+int pd_ctx_stream(pd_ctx* ctx, void** stream);
+int pd_sync(pd_ctx* ctx);
+
+/* Cell-binned, Morton-ordered family search on the device.  Replaces
+ * pdDataManager::InitBond (pdDataManager2.cpp:12-70) with its cube-distance
+ * test (pdDataManager3.cpp:637-685,1573-1704); the family list of every
+ * node is in ascending id order, as the reference's is.  Slit rectangles
+ * mark crossing bonds broken.  Outputs the number of family entries
+ * (2 x bonds) and _minBondLength. */
+int pd_bond_search(pd_ctx* ctx, int64_t* num_halves, int64_t* num_broken, double* min_bond_length);
+/* Copies the family CSR out (row_ptr [N+1], col [H], broken [H] or NULL). */
+int pd_get_family(pd_ctx* ctx, int64_t* row_ptr, int32_t* col, uint8_t* broken);
+/* Installs a family CSR built elsewhere (same layout); broken may be NULL. */
+int pd_set_family(pd_ctx* ctx, const int64_t* row_ptr, const int32_t* col, const uint8_t* broken);
+
+/* Boundary-effect factors (pdNode::SetBdryEffFactor, from
+ * pdDataManager::InitBdryEffectFactor pdDataManager.cpp:1340-1473). */
+int pd_set_bdry_eff(pd_ctx* ctx, const double* bdry_eff);
+/* MLS contributors and coefficients from InitIntegrationPoint
+ * (pdDataManager2.cpp:118-256): cb_ptr [N+1], cb_idx, coeff laid out per
+ * node as [point][contributor]. */
+int pd_set_mls(pd_ctx* ctx, const int64_t* cb_ptr, const int32_t* cb_idx, const double* coeff);
+
+/* Arithmetic of the subsequent force/gather/step calls (pd_precision). */
+int pd_set_precision(pd_ctx* ctx, int precision);
+/* Whether the elastic-energy diagnostic (pdDataManager2.cpp:1340-1342,
+ * pdDataManager.cpp:2096-2115) is accumulated; on by default. */
+int pd_set_energy(pd_ctx* ctx, int on);
+
+/* Nodal state U and V ([3N] each; either may be NULL).  Setting the state
+ * also sets the velocity buffer to V (InitDynamicSolve). */
+int pd_set_state(pd_ctx* ctx, const double* U, const double* V);
+int pd_get_state(pd_ctx* ctx, double* U, double* V);
+int pd_get_vbuf(pd_ctx* ctx, double* vbuf);
+int pd_set_gauss_displ(pd_ctx* ctx, const double* ug);
+int pd_get_gauss_displ(pd_ctx* ctx, double* ug);
+/* per-node elastic energy density of the current step */
+int pd_get_energy_density(pd_ctx* ctx, double* eed);
+
+/* pdDataManager::InitDynamicSolve (pdDataManager2.cpp:410-439). */
+int pd_init_dynamic(pd_ctx* ctx);
+/* pdDataManager::CalcIntgPointDisplRK4 (pdDataManager.cpp:2402-2495): the
+ * Gauss-point displacements from trial nodal displacements us [3N] (host);
+ * us == NULL uses the nodal state U. */
+int pd_gather(pd_ctx* ctx, double time, const double* us);
+/* pdDataManager::CalcBondBasedMotionRK4 (pdDataManager.cpp:1767-1992): adds
+ * the bond forces of trial displacements us [3N] to the velocity buffer,
+ * applies the boundary conditions (UpdateNodeStatusWithBC :2497-2602) and
+ * writes k = vbuf*dt into k_out [3N] (may be NULL). */
+int pd_force_stage(pd_ctx* ctx, double dt, double time, const double* us, double* k_out);
+/* pdDataManager::RK4 (pdDataManager.cpp:1994-2134), preceded by
+ * InitDynamicSolve; ke/ee (may be NULL) receive the kinetic and elastic
+ * energies of the step (pdSolve.cpp:85-91). */
+int pd_rk4_step(pd_ctx* ctx, double dt, double time, double* ke, double* ee);
+/* nsteps consecutive RK4 steps on the device, the time advancing as
+ * pdSolve.cpp:59-61 advances it (t += dt before each step, from t0).  The
+ * steps are captured once into a CUDA graph and replayed. */
+int pd_rk4_steps(pd_ctx* ctx, double dt, double t0, int nsteps);
+/* The same through host buffers: U,V in [3N] are uploaded, nsteps run and
+ * the new state written to U_out,V_out. */
+int pd_rk4_steps_host(pd_ctx* ctx, double dt, double t0, int nsteps, const double* U_in, const double* V_in,
+                      double* U_out, double* V_out);
+/* number of Gauss-point force evaluations of one RK4 stage (unbroken
+ * family entries x points per node, CCI: one per entry) */
+int pd_evals_per_stage(pd_ctx* ctx, int64_t* evals);
+/* Back to the state InitNode and SetGaussianPoint leave (pdDataManager.cpp:
+ * 1062-1087, pdDataManager2.cpp:93-96): displacements, velocities, the
+ * velocity buffer and every Gauss-point displacement zero. */
+int pd_reset_state(pd_ctx* ctx);
+/* One RK4 step like pd_rk4_step, with CUDA events on the context's stream
+ * around every kernel; ms[0..3] receive the summed device time of the force,
+ * gather, stage-epilogue and remaining kernels of the step. */
+int pd_profile_step(pd_ctx* ctx, double dt, double time, double* ms);
+
+/* Linearised stiffness operator of pdSolve::AssembleEquation (pdSolve.cpp:
+ * 195-527) applied matrix-free: free rows sum c V_j xi xi^T / r^3 (x_i - x_j)
+ * over the unbroken family with prescribed columns masked, prescribed rows
+ * return x.  time selects VELOC values (val*time, pdSolve.cpp:245-262). */
+int pd_static_matvec(pd_ctx* ctx, double time, const double* x, double* y);
+/* right-hand side: prescribed values, moved prescribed columns and the
+ * traction load (value*factor/grid_spacing on TRACTION nodes). */
+int pd_static_rhs(pd_ctx* ctx, double time, double* b);
+/* Matrix-free CG on the static system (the dense Gauss-Jordan of
+ * pdSolve::Gauss pdSolve.cpp:545-673 is replaced).  PD_PREC_FP64: plain FP64
+ * CG; PD_PREC_FP32C: FP32 matvec inner CG inside FP64 iterative refinement
+ * (FP64 residuals and dot products).  x [3N] is the initial guess in and the
+ * solution out.  iters/relres may be NULL. */
+int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int maxit, double* x, int* iters,
+                    double* relres);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,722 @@
+// pdDataManager / pdSolve of the drop-in (see pdDataManager.h).
+#include "pdDataManager.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+#include <thread>
+
+#include "pd_deck.h"
+
+namespace pdh {
+
+namespace {
+const double kPI = std::acos(-1.0);  // pdIntgManager.h:25
+
+enum { DISPL = 1, VELOC, DISPLGRAD, TRACTION };
+
+int host_threads() {
+    unsigned n = std::thread::hardware_concurrency();
+    if (const char* e = std::getenv("PDMTEL_HOST_THREADS")) n = (unsigned)std::max(1, std::atoi(e));
+    return (int)std::max(1u, std::min(n, 64u));
+}
+}  // namespace
+
+pdDataManager::pdDataManager() {}
+
+pdDataManager::~pdDataManager() {
+    if (_ctx) pd_ctx_destroy(_ctx);
+}
+
+int pdDataManager::Error(int code, const std::string& msg) {
+    _err = msg;
+    if (!_outFilePath.empty()) {
+        std::ofstream o(_outFilePath.c_str(), std::ios::app);
+        o << msg << "\n";
+    }
+    return code;
+}
+
+int pdDataManager::Cuda(int rc, const char* what) {
+    if (rc == PD_OK) return rc;
+    return Error(rc, std::string(what) + ": " + pd_last_error());
+}
+
+int pdDataManager::SetWkDir(const std::string& dir) {
+    _workDir = dir;
+    if (!_workDir.empty() && _workDir.back() != '/') _workDir += '/';
+    _inFilePath = _workDir + "pds_input.txt";
+    _outFilePath = _workDir + "pds_output.dat";
+    std::ifstream in(_inFilePath.c_str());
+    if (!in) return Error(PD_ERR_ARG, "SetWkDir: input file not exits! " + _inFilePath);
+    std::ofstream out(_outFilePath.c_str(), std::ios::out);
+    return PD_OK;
+}
+
+// pdDataManager::ReadInputFile, pdDataManager.cpp:4-758
+int pdDataManager::ReadInputFile() {
+    DeckReader D;
+    if (!D.Load(_inFilePath)) return Error(PD_ERR_ARG, "ReadInputFile: cannot open " + _inFilePath);
+    std::ofstream log(_outFilePath.c_str(), std::ios::app);
+    auto req = [&](const std::string& k) -> int {
+        if (!D.Find(k)) return Error(PD_ERR_ARG, "FindKeyword: required keyword " + k + " not found!");
+        return PD_OK;
+    };
+    int rc;
+    auto rd = [&](const std::string& k, int pos, auto& v) -> int {
+        int e = D.Read(k, pos, v);
+        if (e == 1) return Error(PD_ERR_ARG, "ReadKeyword: keyword not found, keyword = " + k);
+        if (e == 2) return Error(PD_ERR_ARG, "ReadKeyword: value missing at desired position, keyword = " + k);
+        return PD_OK;
+    };
+#define PDH_TRY(x)                          \
+    do {                                    \
+        if ((rc = (x)) != PD_OK) return rc; \
+    } while (0)
+    _title = "Peridynamic test problem";
+    if (D.Find("problem_title")) PDH_TRY(rd("problem_title", 1, _title));
+    for (int a = 0; a < 3; ++a) _center[a] = 0.0;
+    if (D.Find("grid_center"))
+        for (int a = 0; a < 3; ++a) PDH_TRY(rd("grid_center", a + 1, _center[a]));
+    PDH_TRY(req("grid_dimension"));
+    for (int a = 0; a < 3; ++a) PDH_TRY(rd("grid_dimension", a + 1, _dims[a]));
+    PDH_TRY(req("grid_spacing"));
+    PDH_TRY(rd("grid_spacing", 1, _gridSpacing));
+    if (D.Find("horizon")) PDH_TRY(rd("horizon", 1, _horizon));
+    else _horizon = 3.015 * _gridSpacing;
+    PDH_TRY(req("total_time"));
+    PDH_TRY(rd("total_time", 1, _totalTime));
+    PDH_TRY(req("total_step"));
+    PDH_TRY(rd("total_step", 1, _totalStep));
+    PDH_TRY(req("step_dump_frequency"));
+    PDH_TRY(rd("step_dump_frequency", 1, _stepDumpFrequency));
+    _safeFactor = 0.8;
+    if (D.Find("safety_factor")) PDH_TRY(rd("safety_factor", 1, _safeFactor));
+    _fixedTimeStepOn = false;
+    if (D.Find("fixed_time_step")) {
+        _fixedTimeStepOn = true;
+        PDH_TRY(rd("fixed_time_step", 1, _fixedTimeStep));
+    }
+    if (D.Find("grid_file")) return Error(PD_ERR_ARG, "ReadInputFile: external grid files are not supported");
+    // materials
+    PDH_TRY(req("number_of_materials"));
+    int nm = 0;
+    PDH_TRY(rd("number_of_materials", 1, nm));
+    if (nm <= 0) return Error(PD_ERR_ARG, "ReadInputFile: number_of_materials must be positive");
+    _mats.assign(nm, Material());
+    for (int i = 0; i < nm; ++i) {
+        const std::string k = keyword_append("material_", i + 1);
+        Material& m = _mats[i];
+        PDH_TRY(rd(k, 1, m.type));
+        if (m.type == 1) {
+            PDH_TRY(rd(k, 2, m.ymod));
+            PDH_TRY(rd(k, 3, m.sigmay));
+            PDH_TRY(rd(k, 4, m.ecrit));
+            PDH_TRY(rd(k, 5, m.density));
+            m.nu = 0.25;  // pdMaterialBond.cpp:10
+        } else if (m.type == 2) {
+            PDH_TRY(rd(k, 2, m.ymod));
+            PDH_TRY(rd(k, 3, m.sigmay));
+            PDH_TRY(rd(k, 4, m.nu));
+            PDH_TRY(rd(k, 5, m.ecrit));
+            PDH_TRY(rd(k, 6, m.density));
+        } else {
+            return Error(PD_ERR_ARG, "ReadInputFile: unknown material type in " + k);
+        }
+        const std::string gk = keyword_append("gravity_", i + 1);
+        if (D.Find(gk))
+            for (int a = 0; a < 3; ++a) PDH_TRY(rd(gk, a + 1, m.grav[a]));
+    }
+    // boundary conditions
+    PDH_TRY(req("number_of_boundary_conditions"));
+    int nb = 0;
+    PDH_TRY(rd("number_of_boundary_conditions", 1, nb));
+    _bcs.assign(std::max(nb, 0), BdryCondition());
+    for (int i = 0; i < nb; ++i) {
+        const std::string k = keyword_append("boundary_condition_", i + 1);
+        BdryCondition& b = _bcs[i];
+        PDH_TRY(rd(k, 1, b.type));
+        if (b.type < DISPL || b.type > TRACTION) return Error(PD_ERR_ARG, "ReadInputFile: unknown bc type in " + k);
+        for (int a = 0; a < 3; ++a) PDH_TRY(rd(k, a + 2, b.dir[a]));
+        const int nv = b.type == DISPLGRAD ? 9 : 3;
+        b.value.assign(nv, 0.0);
+        for (int a = 0; a < nv; ++a) PDH_TRY(rd(k, a + 5, b.value[a]));
+        PDH_TRY(rd(k, nv + 5, b.end_time));
+        PDH_TRY(rd(k, nv + 6, b.load_type));
+    }
+    // spaces
+    auto read_space = [&](const std::string& k, bool has_ref, int nref, Space& s) -> int {
+        int r;
+        if ((r = rd(k, 1, s.geo)) != PD_OK) return r;
+        int pos = 2;
+        if (has_ref) {
+            int id = 0;
+            if ((r = rd(k, pos++, id)) != PD_OK) return r;
+            s.ref = id - 1;
+            if (s.ref < 0 || s.ref >= nref) return Error(PD_ERR_ARG, "ReadInputFile: id out of range in " + k);
+        }
+        if (s.geo == 1) {
+            for (int a = 0; a < 3; ++a) {
+                if ((r = rd(k, pos++, s.lo[a])) != PD_OK) return r;
+                if ((r = rd(k, pos++, s.hi[a])) != PD_OK) return r;
+            }
+        } else if (s.geo == 2) {
+            if ((r = rd(k, pos++, s.rad)) != PD_OK) return r;
+            if ((r = rd(k, pos++, s.c1)) != PD_OK) return r;
+            if ((r = rd(k, pos++, s.c2)) != PD_OK) return r;
+            if ((r = rd(k, pos++, s.lo[2])) != PD_OK) return r;
+            if ((r = rd(k, pos++, s.hi[2])) != PD_OK) return r;
+        } else {
+            return Error(PD_ERR_ARG, "ReadInputFile: unknown space geometry in " + k);
+        }
+        return PD_OK;
+    };
+    PDH_TRY(req("number_of_material_spaces"));
+    int nms = 0;
+    PDH_TRY(rd("number_of_material_spaces", 1, nms));
+    _matSpaces.assign(std::max(nms, 0), Space());
+    for (int i = 0; i < nms; ++i)
+        PDH_TRY(read_space(keyword_append("material_space_", i + 1), true, nm, _matSpaces[i]));
+    _delSpaces.clear();
+    if (D.Find("number_of_deletion_spaces")) {
+        int nd = 0;
+        PDH_TRY(rd("number_of_deletion_spaces", 1, nd));
+        _delSpaces.assign(std::max(nd, 0), Space());
+        for (int i = 0; i < nd; ++i)
+            PDH_TRY(read_space(keyword_append("deletion_space_", i + 1), false, 0, _delSpaces[i]));
+    }
+    PDH_TRY(req("number_of_boundary_spaces"));
+    int nbs = 0;
+    PDH_TRY(rd("number_of_boundary_spaces", 1, nbs));
+    _bdrySpaces.assign(std::max(nbs, 0), Space());
+    for (int i = 0; i < nbs; ++i)
+        PDH_TRY(read_space(keyword_append("boundary_space_", i + 1), true, nb, _bdrySpaces[i]));
+    // slits (keyword format of pdSlit.h:6-10)
+    _slits.clear();
+    if (D.Find("number_of_slits")) {
+        int ns = 0;
+        PDH_TRY(rd("number_of_slits", 1, ns));
+        for (int i = 0; i < ns; ++i) {
+            const std::string k = keyword_append("slit_", i + 1);
+            int type = 0;
+            PDH_TRY(rd(k, 1, type));
+            if (type != 1) return Error(PD_ERR_ARG, "ReadInputFile: only rectangular slits (type 1) exist");
+            for (int a = 0; a < 6; ++a) {
+                double v = 0;
+                PDH_TRY(rd(k, a + 2, v));
+                _slits.push_back(v);
+            }
+        }
+    }
+    // control flags
+    PDH_TRY(req("damping_coeff"));
+    PDH_TRY(rd("damping_coeff", 1, _dampCoeff));
+    PDH_TRY(req("bdryEff_on"));
+    PDH_TRY(rd("bdryEff_on", 1, _bdryEffOn));
+    _tolerance = 1.0e-4 * _gridSpacing;
+    PDH_TRY(req("cci_on"));
+    PDH_TRY(rd("cci_on", 1, _cciOn));
+    if (_cciOn) {
+        _fgiOn = _mlsOn = false;
+        _intgPoint = 0;
+        PDH_TRY(rd("cci_on", 2, _cciMdf));
+    } else {
+        PDH_TRY(req("fgi_on"));
+        PDH_TRY(rd("fgi_on", 1, _fgiOn));
+        _cciMdf = false;
+        if (!_fgiOn) return Error(PD_ERR_ARG, "ReadInputFile: adaptive integration (ai_on) is not supported");
+        _intgPoint = 3;
+        if (D.Find("intg_point")) PDH_TRY(rd("intg_point", 1, _intgPoint));
+        _mlsOn = _intgPoint != 1;
+        _rw = 3.0 * _gridSpacing;
+        if (D.Find("support_domain_size")) PDH_TRY(rd("support_domain_size", 1, _rw));
+        if (_intgPoint < 1 || _intgPoint > 8 || _intgPoint == 7)
+            return Error(PD_ERR_ARG, "ReadInputFile: intg_point must be 1-6 or 8");
+    }
+#undef PDH_TRY
+    const int n1 = _cciOn ? 1 : _intgPoint;
+    _npt = n1 * n1 * n1;
+    gauss_rule(n1, _abscis, _weights);
+    log << "ReadInputFile: Problem title = " << _title << "\n"
+        << "ReadInputFile: Grid dimension = " << _dims[0] << " * " << _dims[1] << " * " << _dims[2] << "\n"
+        << "ReadInputFile: Global grid spacing = " << _gridSpacing << "\n"
+        << "ReadInputFile: Global grid horizon = " << _horizon << "\n";
+    _stage = true;
+    return PD_OK;
+}
+
+// pdDataManager::InitNode, pdDataManager.cpp:813-1098
+int pdDataManager::InitNode() {
+    if (!_stage) return Error(PD_ERR_ARG, "InitNode: ReadInputFile first");
+    const double tol = _tolerance;
+    _x.clear();
+    for (int n = 1; n != _dims[2] + 1; ++n)
+        for (int m = 1; m != _dims[1] + 1; ++m)
+            for (int l = 1; l != _dims[0] + 1; ++l) {
+                const double x1 = (l - (_dims[0] + 1) * 0.5) * _gridSpacing + _center[0];
+                const double x2 = (m - (_dims[1] + 1) * 0.5) * _gridSpacing + _center[1];
+                const double x3 = (n - (_dims[2] + 1) * 0.5) * _gridSpacing + _center[2];
+                bool del = false;
+                for (const Space& s : _delSpaces) del = del || s.Contains(x1, x2, x3, tol);
+                if (!del) {
+                    _x.push_back(x1);
+                    _x.push_back(x2);
+                    _x.push_back(x3);
+                }
+            }
+    _numNodes = (int64_t)(_x.size() / 3);
+    if (_numNodes > INT32_MAX) return Error(PD_ERR_ARG, "InitNode: too many nodes");
+    _mat.assign(_numNodes, -1);
+    _bc.assign(_numNodes, -1);
+    for (int64_t i = 0; i < _numNodes; ++i) {
+        const double* p = &_x[3 * i];
+        // every material space overwrites: a node outside the last space
+        // has no material (pdDataManager.cpp:937-955,960-970)
+        for (const Space& s : _matSpaces) _mat[i] = s.Contains(p[0], p[1], p[2], tol) ? s.ref : -1;
+        if (_mat[i] < 0) {
+            std::ostringstream o;
+            o << "InitNode: node " << i << " not in any material space!";
+            return Error(PD_ERR_ARG, o.str());
+        }
+        for (const Space& s : _bdrySpaces)
+            if (s.Contains(p[0], p[1], p[2], tol)) _bc[i] = s.ref;
+    }
+    _bdryEff.assign(_numNodes, 1.0);
+    _nodesDone = true;
+    std::ofstream log(_outFilePath.c_str(), std::ios::app);
+    log << "\nInitNode: total node number = " << _numNodes << "\n";
+    return PD_OK;
+}
+
+int pdDataManager::EnsureContext() {
+    if (_ctx) return PD_OK;
+    if (!_nodesDone) return Error(PD_ERR_ARG, "EnsureContext: InitNode first");
+    std::vector<pd_material> mats(_mats.size());
+    for (size_t k = 0; k < _mats.size(); ++k) {
+        const Material& m = _mats[k];
+        // spring constant as InitMaterial sets it (pdDataManager.cpp:1310-1322)
+        mats[k].spring = m.type == 1 ? 18 * m.BulkModulus() / (kPI * std::pow(_horizon, 4.0)) : 0.0;
+        mats[k].density = m.density;
+        mats[k].ecrit = m.ecrit;
+        for (int a = 0; a < 3; ++a) mats[k].grav[a] = m.grav[a];
+    }
+    std::vector<pd_bc> bcs(_bcs.size());
+    for (size_t k = 0; k < _bcs.size(); ++k) {
+        std::memset(&bcs[k], 0, sizeof(pd_bc));
+        bcs[k].type = _bcs[k].type;
+        for (int a = 0; a < 3; ++a) bcs[k].dir[a] = _bcs[k].dir[a];
+        for (size_t a = 0; a < _bcs[k].value.size() && a < 9; ++a) bcs[k].value[a] = _bcs[k].value[a];
+        bcs[k].end_time = _bcs[k].end_time;
+        bcs[k].load_type = _bcs[k].load_type;
+    }
+    pd_problem P;
+    std::memset(&P, 0, sizeof P);
+    P.num_nodes = _numNodes;
+    P.coords = _x.data();
+    P.mat_id = _mat.data();
+    P.bc_id = _bc.data();
+    P.num_materials = (int32_t)mats.size();
+    P.materials = mats.data();
+    P.num_bcs = (int32_t)bcs.size();
+    P.bcs = bcs.empty() ? nullptr : bcs.data();
+    P.grid_spacing = _gridSpacing;
+    P.horizon = _horizon;
+    P.integration = _cciOn ? PD_INTG_CCI : PD_INTG_FGI;
+    P.cci_modified = _cciMdf ? 1 : 0;
+    P.intg_point = _cciOn ? 1 : _intgPoint;
+    P.abscissae = _abscis.data();
+    P.weights = _weights.data();
+    P.damping = _dampCoeff;
+    P.num_slits = (int32_t)(_slits.size() / 6);
+    P.slits = _slits.empty() ? nullptr : _slits.data();
+    P.spring_factor = _springFactor.empty() ? nullptr : _springFactor.data();
+    int rc = pd_ctx_create(&P, &_ctx);
+    if (rc != PD_OK) return Cuda(rc, "pd_ctx_create");
+    pd_set_precision(_ctx, _precision);
+    pd_set_energy(_ctx, _energy ? 1 : 0);
+    _uploaded = false;
+    return PD_OK;
+}
+
+// pdDataManager::InitBond, pdDataManager2.cpp:12-70, on the device
+int pdDataManager::InitBond() {
+    int rc = EnsureContext();
+    if (rc != PD_OK) return rc;
+    int64_t nh = 0, nb = 0;
+    double mb = 0;
+    if ((rc = pd_bond_search(_ctx, &nh, &nb, &mb)) != PD_OK) return Cuda(rc, "pd_bond_search");
+    _famPtr.assign(_numNodes + 1, 0);
+    _famCol.assign(std::max<int64_t>(nh, 0), 0);
+    _famBroken.assign(std::max<int64_t>(nh, 0), 0);
+    if ((rc = pd_get_family(_ctx, _famPtr.data(), _famCol.data(), _famBroken.data())) != PD_OK)
+        return Cuda(rc, "pd_get_family");
+    _numHalves = nh;
+    _numBroken = nb;
+    _minBondLength = mb;
+    _bondsDone = true;
+    _familyOnDevice = true;
+    std::ofstream log(_outFilePath.c_str(), std::ios::app);
+    log << "\nInitBond: total bonds number = " << nh / 2 << "\n";
+    return PD_OK;
+}
+
+int pdDataManager::SetFamily(const std::vector<int64_t>& row_ptr, const std::vector<int32_t>& col,
+                             const std::vector<uint8_t>& broken, double min_bond) {
+    if ((int64_t)row_ptr.size() != _numNodes + 1) return Error(PD_ERR_ARG, "SetFamily: row_ptr size");
+    _famPtr = row_ptr;
+    _famCol = col;
+    _famBroken = broken.empty() ? std::vector<uint8_t>(col.size(), 0) : broken;
+    _numHalves = (int64_t)col.size();
+    _numBroken = 0;
+    for (uint8_t b : _famBroken) _numBroken += b ? 1 : 0;
+    _minBondLength = min_bond;
+    _bondsDone = true;
+    _uploaded = false;
+    _familyOnDevice = false;
+    if (_ctx) {
+        int rc = pd_set_family(_ctx, _famPtr.data(), _famCol.data(), _famBroken.data());
+        if (rc != PD_OK) return Cuda(rc, "pd_set_family");
+        _familyOnDevice = true;
+    }
+    return PD_OK;
+}
+
+// pdDataManager::InitMaterial, pdDataManager.cpp:1297-1338
+int pdDataManager::InitMaterial() {
+    for (Material& m : _mats) m.spring = m.type == 1 ? 18 * m.BulkModulus() / (kPI * std::pow(_horizon, 4.0)) : 0.0;
+    _minMaterialDensity = 1.0e10;
+    _maxBulkSoundSpeed = 0.0;
+    for (const Material& m : _mats) {
+        _minMaterialDensity = std::min(_minMaterialDensity, m.density);
+        _maxBulkSoundSpeed = std::max(_maxBulkSoundSpeed, m.BulkSoundSpeed());
+    }
+    _matDone = true;
+    return PD_OK;
+}
+
+// pdDataManager::InitBdryEffectFactor, pdDataManager.cpp:1340-1473, with
+// CalcBdryEffFactor / CalcBdryEffFactorTypeOne (pdDataManager2.cpp:1353-1485)
+int pdDataManager::InitBdryEffectFactor() {
+    if (!_bdryEffOn) return PD_OK;
+    if (!_bondsDone || !_matDone) return Error(PD_ERR_ARG, "InitBdryEffectFactor: bonds and materials first");
+    const double dx = _gridSpacing, delta = _horizon, tol = _tolerance;
+    // full-sphere family count on a virtual lattice around the origin
+    const int vd = 2 * (int(delta / dx) + 1);
+    const double origin[3] = {0.0, 0.0, 0.0};
+    int full = 0;
+    for (int n = 1; n != vd + 1; ++n)
+        for (int m = 1; m != vd + 1; ++m)
+            for (int l = 1; l != vd + 1; ++l) {
+                const double q[3] = {(l - vd * 0.5) * dx, (m - vd * 0.5) * dx, (n - vd * 0.5) * dx};
+                double mn, mx;
+                cube_distance(origin, q, dx, &mn, &mx);
+                if (mn < delta + tol) ++full;
+            }
+    _numMaxFamily = full;
+    const double lo[3] = {-_dims[0] * 0.5 * dx + _center[0], -_dims[1] * 0.5 * dx + _center[1],
+                          -_dims[2] * 0.5 * dx + _center[2]};
+    const double hi[3] = {_dims[0] * 0.5 * dx + _center[0], _dims[1] * 0.5 * dx + _center[1],
+                          _dims[2] * 0.5 * dx + _center[2]};
+    const double ns = (int(delta / dx)) * dx;
+    const double vol = std::pow(dx, 3.0);
+    auto type_one = [&](const Material& m, double h) {
+        const double fullE = 3.0 * m.ymod;
+        const double part = fullE - 0.5 * m.spring * kPI *
+                                        (std::pow(delta, 4) / 4.0 - h * std::pow(delta, 3) / 3.0 + std::pow(h, 4) / 12.0);
+        return fullE / part;
+    };
+    const bool cci_orig = _cciOn && !_cciMdf;
+    for (int64_t i = 0; i < _numNodes; ++i) {
+        const double a = _x[3 * i], b = _x[3 * i + 1], c = _x[3 * i + 2];
+        const Material& m = _mats[_mat[i]];
+        const int64_t nf = _famPtr[i + 1] - _famPtr[i];
+        const bool in1 = b >= lo[1] + ns && b <= hi[1] - ns && c >= lo[2] + ns && c <= hi[2] - ns;
+        const bool in2 = a >= lo[0] + ns && a <= hi[0] - ns && c >= lo[2] + ns && c <= hi[2] - ns;
+        const bool in3 = a >= lo[0] + ns && a <= hi[0] - ns && b >= lo[1] + ns && b <= hi[1] - ns;
+        double f;
+        if (nf == full) f = 1.0;
+        else if (a >= hi[0] - ns && a <= hi[0] && in1) f = type_one(m, hi[0] - a);
+        else if (a >= lo[0] && a <= lo[0] + ns && in1) f = type_one(m, a - lo[0]);
+        else if (b >= hi[1] - ns && b <= hi[1] && in2) f = type_one(m, hi[1] - b);
+        else if (b >= lo[1] && b <= lo[1] + ns && in2) f = type_one(m, b - lo[1]);
+        else if (c >= hi[2] - ns && c <= hi[2] && in3) f = type_one(m, hi[2] - c);
+        else if (c >= lo[2] && c <= lo[2] + ns && in3) f = type_one(m, c - lo[2]);
+        else {
+            // energy ratio under a 1e-4 uniform dilatation
+            const double e11 = 1.0e-4;
+            const double eps[9] = {e11, 0.0, 0.0, 0.0, e11, 0.0, 0.0, 0.0, e11};
+            double sum = 0.0;
+            for (int64_t p = _famPtr[i]; p < _famPtr[i + 1]; ++p) {
+                if (_famBroken[p]) continue;
+                const double* Y = &_x[3 * (int64_t)_famCol[p]];
+                const double x1 = Y[0] - a, x2 = Y[1] - b, x3 = Y[2] - c;
+                const double e1 = eps[0] * x1 + eps[1] * x2 + eps[2] * x3;
+                const double e2 = eps[3] * x1 + eps[4] * x2 + eps[5] * x3;
+                const double e3 = eps[6] * x1 + eps[7] * x2 + eps[8] * x3;
+                const double r = std::sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+                const double p1 = x1 + e1, p2 = x2 + e2, p3 = x3 + e3;
+                const double pl = std::sqrt(p1 * p1 + p2 * p2 + p3 * p3);
+                const double u = pl - r, s = u / r;
+                const double el = (u <= 0 || (u > 0 && s <= m.ecrit)) ? 0.5 * (m.spring / r) * u * u : 0.0;
+                const double beta = beta_factor(r, delta, dx, cci_orig);
+                const double elj = el * beta * vol;
+                sum += 0.5 * elj;
+            }
+            const double pinf = 3.0 * m.ymod * e11 * e11;
+            f = pinf / sum;
+        }
+        _bdryEff[i] = f;
+    }
+    if (_ctx) {
+        int rc = pd_set_bdry_eff(_ctx, _bdryEff.data());
+        if (rc != PD_OK) return Cuda(rc, "pd_set_bdry_eff");
+    }
+    return PD_OK;
+}
+
+// pdDataManager::InitGridBoundary, pdDataManager.cpp:1100-1295: the model
+// bounds are only used by output planes, which this build does not write.
+int pdDataManager::InitGridBoundary() { return PD_OK; }
+
+// pdDataManager::InitIntegrationPoint, pdDataManager2.cpp:106-309
+int pdDataManager::InitIntegrationPoint() {
+    if (!_mlsOn) return PD_OK;
+    if (!_bondsDone) return Error(PD_ERR_ARG, "InitIntegrationPoint: bonds first");
+    mls_contributors(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _rw, _cbPtr, _cbIdx);
+    int64_t bad = -1;
+    int rc = mls_coefficients(_numNodes, _x.data(), _abscis.data(), _intgPoint, _gridSpacing, _cbPtr, _cbIdx, _rw,
+                              _coeff, host_threads(), &bad);
+    if (rc != PD_OK) {
+        std::ostringstream o;
+        o << "pdMatrix::Gauss: Singular Matrix (MLS moment matrix of node " << bad << ")";
+        return Error(rc, o.str());
+    }
+    if (_ctx) {
+        rc = pd_set_mls(_ctx, _cbPtr.data(), _cbIdx.data(), _coeff.data());
+        if (rc != PD_OK) return Cuda(rc, "pd_set_mls");
+    }
+    return PD_OK;
+}
+
+int pdDataManager::UploadSetup() {
+    int rc = EnsureContext();
+    if (rc != PD_OK) return rc;
+    if (_uploaded) return PD_OK;
+    if (!_bondsDone) return Error(PD_ERR_ARG, "no family: InitBond first");
+    if (!_familyOnDevice) {
+        // the family was installed on the host (SetFamily) before the context existed
+        rc = pd_set_family(_ctx, _famPtr.data(), _famCol.data(), _famBroken.data());
+        if (rc != PD_OK) return Cuda(rc, "pd_set_family");
+        _familyOnDevice = true;
+    }
+    if ((rc = pd_set_bdry_eff(_ctx, _bdryEff.data())) != PD_OK) return Cuda(rc, "pd_set_bdry_eff");
+    if (_mlsOn) {
+        if (_cbPtr.empty()) return Error(PD_ERR_ARG, "no MLS data: InitIntegrationPoint first");
+        if ((rc = pd_set_mls(_ctx, _cbPtr.data(), _cbIdx.data(), _coeff.data())) != PD_OK) return Cuda(rc, "pd_set_mls");
+    }
+    _uploaded = true;
+    return PD_OK;
+}
+
+int pdDataManager::SetPrecision(int p) {
+    _precision = p;
+    if (_ctx) return Cuda(pd_set_precision(_ctx, p), "pd_set_precision");
+    return PD_OK;
+}
+
+int pdDataManager::SetEnergy(bool on) {
+    _energy = on;
+    if (_ctx) return Cuda(pd_set_energy(_ctx, on ? 1 : 0), "pd_set_energy");
+    return PD_OK;
+}
+
+// pdDataManager::CalcStableTimeStep, pdDataManager2.cpp:6-10
+double pdDataManager::CalcStableTimeStep() const {
+    return _fixedTimeStepOn ? _fixedTimeStep : _safeFactor * _minBondLength / _maxBulkSoundSpeed;
+}
+
+int pdDataManager::InitDynamicSolve() {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    _kineticEnergyStep = _elasticEnergyStep = 0.0;
+    return Cuda(pd_init_dynamic(_ctx), "pd_init_dynamic");
+}
+
+int pdDataManager::RK4(double dt, double time) {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    return Cuda(pd_rk4_step(_ctx, dt, time, &_kineticEnergyStep, &_elasticEnergyStep), "pd_rk4_step");
+}
+
+int pdDataManager::RK4Steps(double dt, double t0, int nsteps) {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    return Cuda(pd_rk4_steps(_ctx, dt, t0, nsteps), "pd_rk4_steps");
+}
+
+int pdDataManager::CalcBondBasedMotionRK4(double dt, double time, const std::vector<double>& us,
+                                          std::vector<double>& k) {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    if ((int64_t)us.size() != 3 * _numNodes) return Error(PD_ERR_ARG, "CalcBondBasedMotionRK4: size");
+    k.assign(3 * _numNodes, 0.0);
+    return Cuda(pd_force_stage(_ctx, dt, time, us.data(), k.data()), "pd_force_stage");
+}
+
+int pdDataManager::CalcIntgPointDisplRK4(double time, const std::vector<double>& us) {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    if ((int64_t)us.size() != 3 * _numNodes) return Error(PD_ERR_ARG, "CalcIntgPointDisplRK4: size");
+    return Cuda(pd_gather(_ctx, time, us.data()), "pd_gather");
+}
+
+int pdDataManager::StaticSolve(double time, int precision, double rtol, int maxit, std::vector<double>& u,
+                               int* iters, double* relres) {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    if ((int64_t)u.size() != 3 * _numNodes) u.assign(3 * _numNodes, 0.0);
+    return Cuda(pd_static_solve(_ctx, time, precision, rtol, maxit, u.data(), iters, relres), "pd_static_solve");
+}
+
+int pdDataManager::GetDispl(std::vector<double>& U) {
+    U.assign(3 * _numNodes, 0.0);
+    if (!_ctx) return PD_OK;
+    return Cuda(pd_get_state(_ctx, U.data(), nullptr), "pd_get_state");
+}
+
+int pdDataManager::GetVeloc(std::vector<double>& V) {
+    V.assign(3 * _numNodes, 0.0);
+    if (!_ctx) return PD_OK;
+    return Cuda(pd_get_state(_ctx, nullptr, V.data()), "pd_get_state");
+}
+
+int pdDataManager::SetState(const std::vector<double>& U, const std::vector<double>& V) {
+    int rc = UploadSetup();
+    if (rc != PD_OK) return rc;
+    return Cuda(pd_set_state(_ctx, U.empty() ? nullptr : U.data(), V.empty() ? nullptr : V.data()), "pd_set_state");
+}
+
+// ------------------------------------------------------------------ pdSolve
+
+int pdSolve::InitialProblem(pdDataManager& dat) {
+    int rc;
+    if ((rc = dat.ReadInputFile()) != PD_OK) return rc;
+    if ((rc = dat.InitNode()) != PD_OK) return rc;
+    if ((rc = dat.InitBond()) != PD_OK) return rc;
+    if ((rc = dat.InitMaterial()) != PD_OK) return rc;
+    if ((rc = dat.InitBdryEffectFactor()) != PD_OK) return rc;
+    if ((rc = dat.InitGridBoundary()) != PD_OK) return rc;
+    if ((rc = dat.InitIntegrationPoint()) != PD_OK) return rc;
+    return PD_OK;
+}
+
+// one node record as pdNode::Print writes it (pdNode.cpp:418-433)
+static void print_node(std::ostream& os, int64_t i, const pdDataManager& dat, const std::vector<double>& U,
+                       const std::vector<double>& V) {
+    const auto& x = dat.Coords();
+    os << i << "\t" << x[3 * i] << "\t" << x[3 * i + 1] << "\t" << x[3 * i + 2] << "\t" << U[3 * i] << "\t"
+       << U[3 * i + 1] << "\t" << U[3 * i + 2] << "\t" << V[3 * i] << "\t" << V[3 * i + 1] << "\t" << V[3 * i + 2]
+       << "\t" << dat.MatIds()[i] << "\t" << dat.BcIds()[i] << "\t" << dat.BdryEff()[i] << "\t" << 0;
+}
+
+int pdSolve::WriteTecplot(pdDataManager& dat, int step, double time) {
+    std::vector<double> U, V;
+    int rc;
+    if ((rc = dat.GetDispl(U)) != PD_OK || (rc = dat.GetVeloc(V)) != PD_OK) return rc;
+    std::ofstream out((dat.GetWkDir() + keyword_append("pds_tecplot_", step) + ".dat").c_str());
+    out << "Tecplot formatting output mode\n";
+    out.setf(std::ios::scientific);
+    out.precision(5);
+    out << "VARIABLES = \n ID X1 X2 X3 U1 U2 U3 V1 V2 V3 MatID BCID bdryEff DmgFrac \n"
+        << "ZONE I=" << dat.GetGridDimension(0) << ", J=" << dat.GetGridDimension(1)
+        << ", K=" << dat.GetGridDimension(2) << ", F=POINT\n\n";
+    for (int64_t i = 0; i < dat.GetNumNode(); ++i) {
+        print_node(out, i, dat, U, V);
+        out << "\n";
+    }
+    (void)time;
+    return PD_OK;
+}
+
+// pdSolve::SolveDynamic, pdSolve.cpp:24-130
+int pdSolve::SolveDynamic(pdDataManager& dat, bool write_files) {
+    const int totalStep = dat.GetTotalStep();
+    int lastStep = totalStep;
+    const int dump = std::max(1, dat.GetStepDumpFrequency());
+    const double totalTime = dat.GetTotalTime();
+    const double stable = dat.CalcStableTimeStep();
+    double t = 0.0, cur = stable;
+    std::ofstream log, steps;
+    if (write_files) {
+        log.open((dat.GetWkDir() + "pds_output.dat").c_str(), std::ios::app);
+        log.setf(std::ios::scientific);
+        log.precision(5);
+        log << "\n** Dynamic solution: starting from cycle 1 **\n";
+        steps.open((dat.GetWkDir() + "pds_steps.dat").c_str());
+        steps << "Data at given node for each time step output mode\n\n";
+        steps << "Step Time ID X1 X2 X3 U1 U2 U3 V1 V2 V3 MatID BCID bdryEff DmgFrac \n";
+        steps.setf(std::ios::scientific);
+        steps.precision(5);
+    }
+    int rc = dat.SetEnergy(write_files);
+    if (rc != PD_OK) return rc;
+    // probe node at (dx/2, dx/2, dx/2), pdSolve.cpp:764-771
+    int64_t probe = -1;
+    const double h = 0.5 * dat.GetGridSpacing();
+    for (int64_t i = 0; i < dat.GetNumNode(); ++i)
+        if (dat.Coords()[3 * i] == h && dat.Coords()[3 * i + 1] == h && dat.Coords()[3 * i + 2] == h) probe = i;
+    for (int iter = 1; iter != totalStep + 1; ++iter) {
+        t += cur;
+        if (!(t <= totalTime)) break;
+        if (write_files) {
+            if ((rc = dat.InitDynamicSolve()) != PD_OK) return rc;
+            if ((rc = dat.RK4(cur, t)) != PD_OK) return rc;
+            log << iter << ": dt= " << cur << " t= " << t << " KE= " << dat.GetKinetTotal()
+                << " EE= " << dat.GetElastStep() << "\n";
+            if (iter == 1 || iter == lastStep || iter % dump == 0)
+                if ((rc = WriteTecplot(dat, iter, t)) != PD_OK) return rc;
+            if (probe >= 0) {
+                std::vector<double> U, V;
+                dat.GetDispl(U);
+                dat.GetVeloc(V);
+                steps << iter << "\t" << t << "\t";
+                print_node(steps, probe, dat, U, V);
+                steps << "\n";
+            }
+        } else {
+            if ((rc = dat.RK4Steps(cur, t - cur, 1)) != PD_OK) return rc;
+        }
+        if (t + stable > totalTime && t != totalTime) {
+            lastStep = iter + 1;
+            cur = totalTime - t;
+        }
+    }
+    if (!write_files && dat.Context()) pd_sync(dat.Context());
+    return PD_OK;
+}
+
+// Static solve: the operator of pdSolve::AssembleEquation solved matrix-free
+// (CG) at time = the stable time step of the first cycle (pdSolve.cpp:156-158).
+int pdSolve::SolveStatic(pdDataManager& dat, int precision, double rtol, bool write_files) {
+    std::vector<double> u(3 * (size_t)dat.GetNumNode(), 0.0);
+    const double t = dat.CalcStableTimeStep();
+    int iters = 0;
+    double rel = 0.0;
+    int rc = dat.StaticSolve(t, precision, rtol, 200000, u, &iters, &rel);
+    if (rc != PD_OK) return rc;
+    std::vector<double> V(u.size(), 0.0);
+    if ((rc = dat.SetState(u, V)) != PD_OK) return rc;
+    if (write_files) {
+        std::ofstream log((dat.GetWkDir() + "pds_output.dat").c_str(), std::ios::app);
+        log << "** Static solution: CG iterations = " << iters << ", relative residual = " << rel << " **\n";
+        return WriteTecplot(dat, 1, t);
+    }
+    return PD_OK;
+}
+
+}  // namespace pdh

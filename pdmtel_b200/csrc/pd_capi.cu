@@ -1,0 +1,985 @@
+// The C ABI of libpdmtel_b200 (include/pdmtel_b200.h): context life cycle,
+// uploads in the reference's row layout, the RK4 driver and the static CG.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pd_internal.cuh"
+
+namespace pd {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+int fail(int code, const char* msg) {
+    g_last_error = msg ? msg : "";
+    return code;
+}
+
+int fail_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%s:%d %s: %s", file, line, what, cudaGetErrorString(e));
+    g_last_error = buf;
+    return e == cudaErrorMemoryAllocation ? PD_ERR_OOM : PD_ERR_CUDA;
+}
+
+}  // namespace pd
+
+using pd::fail;
+
+struct pd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    pd::Dev d{};
+    int64_t n = 0, H = 0, Ha = 0;
+    int npt = 1;
+    int precision = PD_PREC_FP64;
+    int nslit = 0;
+    std::vector<double> coords;  // [N][3] host copy
+    std::vector<double> slits;
+    double* dslits = nullptr;   // [nslit][6] on the device
+    bool have_family = false, have_mls = false;
+    // owned device buffers
+    std::vector<void*> owned;
+    int64_t *frow = nullptr, *arow = nullptr, *cbptr = nullptr;
+    int32_t *fcol = nullptr, *acol = nullptr, *cbidx = nullptr;
+    uint8_t* fbroken = nullptr;
+    double *coeff = nullptr, *scratch = nullptr, *dotpart = nullptr, *scal = nullptr;
+    float *coeff32 = nullptr, *csum = nullptr;
+    double* hstage = nullptr;  // pinned host staging, 3N doubles x 2
+    double* hscalar = nullptr; // pinned host scalars
+    // CUDA graph of one RK4 step
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+    int graph_prec = -1, graph_energy = -1;
+    uint64_t generation = 0, graph_generation = ~0ull;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(pd_ctx* c, T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return pd::fail_cuda(e, "cudaMalloc", __FILE__, __LINE__);
+    c->owned.push_back(q);
+    *p = (T*)q;
+    return PD_OK;
+}
+
+void dfree(pd_ctx* c, void* p) {
+    if (!p) return;
+    auto it = std::find(c->owned.begin(), c->owned.end(), p);
+    if (it != c->owned.end()) c->owned.erase(it);
+    cudaFree(p);
+}
+
+#define PD_TRY(expr)                       \
+    do {                                   \
+        int _rc = (expr);                  \
+        if (_rc != PD_OK) return _rc;      \
+    } while (0)
+
+int upload(pd_ctx* c, void* dst, const void* src, size_t bytes) {
+    PD_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+// [N][3] host -> [3][N] device (through the scratch buffer)
+int upload_vec3(pd_ctx* c, double* dst_soa, const double* src_aos) {
+    if (c->n == 0) return PD_OK;
+    const size_t bytes = sizeof(double) * 3 * c->n;
+    std::memcpy(c->hstage, src_aos, bytes);
+    PD_CUDA_TRY(cudaMemcpyAsync(c->scratch, c->hstage, bytes, cudaMemcpyHostToDevice, c->stream));
+    pd::launch_to_soa(c->scratch, dst_soa, c->n, 3, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int download_vec3(pd_ctx* c, double* dst_aos, const double* src_soa) {
+    if (c->n == 0) return PD_OK;
+    const size_t bytes = sizeof(double) * 3 * c->n;
+    pd::launch_to_aos(src_soa, c->scratch, c->n, 3, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    PD_CUDA_TRY(cudaMemcpyAsync(c->hstage, c->scratch, bytes, cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    std::memcpy(dst_aos, c->hstage, bytes);
+    return PD_OK;
+}
+
+int set_time(pd_ctx* c, double t) {
+    *c->hscalar = t;
+    PD_CUDA_TRY(cudaMemcpyAsync(c->d.tdev, c->hscalar, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffull;
+        v = (v | v << 16) & 0x1f0000ff0000ffull;
+        v = (v | v << 8) & 0x100f00f00f00f00full;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+        v = (v | v << 2) & 0x1249249249249249ull;
+        return v;
+    };
+    return spread(x) | spread(y) << 1 | spread(z) << 2;
+}
+
+bool ready_dynamic(pd_ctx* c) {
+    if (!c->have_family) return false;
+    if (!c->d.cci && c->d.mls && !c->have_mls) return false;
+    return true;
+}
+
+// the four stages of pdDataManager::RK4 and the closing gather
+void enqueue_step_body(pd_ctx* c, double dt) {
+    cudaStream_t s = c->stream;
+    const pd::Dev& d = c->d;
+    const int64_t n3 = 3 * c->n;
+    const bool f32 = c->precision == PD_PREC_FP32C;
+    auto force = [&](double dts) {
+        if (f32) pd::launch_force_f32c(d, dts, s);
+        else pd::launch_force_f64(d, dts, s);
+    };
+    auto gather = [&](const double* us) {
+        if (f32) pd::launch_gather_f32c(d, us, s);
+        else pd::launch_gather_f64(d, us, s);
+    };
+    const double dtHalf = 0.5 * dt;
+    // InitDynamicSolve: vbuf = V, energy density 0; u1 = us = U
+    cudaMemcpyAsync(d.vbuf, d.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.u1, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.us, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    if (d.energy) cudaMemsetAsync(d.eed, 0, sizeof(double) * c->n, s);
+    force(dtHalf);
+    pd::launch_epilogue(d, 1, dtHalf, dt, s);
+    gather(d.us);
+    force(dtHalf);
+    pd::launch_epilogue(d, 2, dtHalf, dt, s);
+    gather(d.us);
+    force(dt);
+    pd::launch_epilogue(d, 3, dt, dt, s);
+    gather(d.us);
+    force(dt);
+    pd::launch_epilogue(d, 4, dt, dt, s);
+    if (d.energy) pd::launch_energy_reduce(d, s);
+    gather(d.U);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pd_abi_version(void) { return PD_ABI_VERSION; }
+
+const char* pd_last_error(void) { return pd::g_last_error.c_str(); }
+
+int pd_device_count(int* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) n = 0;
+    if (count) *count = n;
+    return PD_OK;
+}
+
+int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
+    if (!P || !out) return fail(PD_ERR_ARG, "pd_ctx_create: null argument");
+    *out = nullptr;
+    if (P->num_nodes < 0 || (P->num_nodes > 0 && (!P->coords || !P->mat_id)))
+        return fail(PD_ERR_ARG, "pd_ctx_create: bad node arrays");
+    if (P->num_nodes > INT32_MAX) return fail(PD_ERR_ARG, "pd_ctx_create: more than 2^31-1 nodes");
+    if (P->num_materials <= 0 || !P->materials) return fail(PD_ERR_ARG, "pd_ctx_create: no materials");
+    if (P->num_bcs < 0 || (P->num_bcs > 0 && !P->bcs)) return fail(PD_ERR_ARG, "pd_ctx_create: bad bc table");
+    if (!(P->grid_spacing > 0.0) || !(P->horizon > 0.0)) return fail(PD_ERR_ARG, "pd_ctx_create: bad spacing/horizon");
+    if (P->integration != PD_INTG_CCI && P->integration != PD_INTG_FGI)
+        return fail(PD_ERR_ARG, "pd_ctx_create: unknown integration scheme");
+    int n1 = P->integration == PD_INTG_FGI ? P->intg_point : 1;
+    if (n1 < 1 || n1 > 8) return fail(PD_ERR_ARG, "pd_ctx_create: intg_point must be 1..8");
+    if (P->integration == PD_INTG_FGI && (!P->abscissae || !P->weights))
+        return fail(PD_ERR_ARG, "pd_ctx_create: Gauss abscissae/weights required");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PD_ERR_NODEV, "no CUDA device");
+    const int64_t N = P->num_nodes;
+    for (int64_t i = 0; i < N; ++i) {
+        if (P->mat_id[i] < 0 || P->mat_id[i] >= P->num_materials) return fail(PD_ERR_ARG, "mat_id out of range");
+        if (P->bc_id && (P->bc_id[i] < -1 || P->bc_id[i] >= P->num_bcs)) return fail(PD_ERR_ARG, "bc_id out of range");
+    }
+    pd_ctx* c = new pd_ctx();
+    auto bail = [&](int rc) {
+        pd_ctx_destroy(c);
+        return rc;
+    };
+    cudaGetDevice(&c->device);
+    if (P->stream) {
+        c->stream = (cudaStream_t)P->stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return bail(pd::fail_cuda(e, "cudaStreamCreate", __FILE__, __LINE__));
+        c->own_stream = true;
+    }
+    c->n = N;
+    c->npt = n1 * n1 * n1;
+    c->coords.assign(P->coords, P->coords + 3 * N);
+    c->nslit = P->num_slits > 0 ? P->num_slits : 0;
+    if (c->nslit) c->slits.assign(P->slits, P->slits + 6 * c->nslit);
+    pd::Dev& d = c->d;
+    d.n = N;
+    d.npt = c->npt;
+    d.cci = P->integration == PD_INTG_CCI;
+    d.cci_mdf = P->cci_modified ? 1 : 0;
+    d.mls = (!d.cci && n1 > 1) ? 1 : 0;
+    d.energy = 1;
+    d.dx = P->grid_spacing;
+    d.delta = P->horizon;
+    d.damping = P->damping;
+    d.vol = std::pow(d.dx, 3.0);           // node volume, pdDataManager.cpp:1081
+    d.vol_cci = d.dx * d.dx * d.dx;        // pdDataManager2.cpp:1328
+    const size_t n3 = (size_t)(3 * N);
+    if (cudaMallocHost(&c->hstage, sizeof(double) * std::max<size_t>(n3, 1) * 2) != cudaSuccess)
+        return bail(fail(PD_ERR_OOM, "pinned staging"));
+    if (cudaMallocHost(&c->hscalar, sizeof(double) * 16) != cudaSuccess) return bail(fail(PD_ERR_OOM, "pinned scalar"));
+    double* x = nullptr;
+    int32_t *mat = nullptr, *bc = nullptr;
+    pd::MatDev* mats = nullptr;
+    pd::BcDev* bcs = nullptr;
+    pd::GaussConst* gc = nullptr;
+    double* bdry = nullptr;
+    int rc = PD_OK;
+    if ((rc = dalloc(c, &c->scratch, n3 * 2)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &x, n3)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &mat, N)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &bc, N)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &mats, P->num_materials)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &bcs, std::max(P->num_bcs, 1))) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &gc, c->npt)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &bdry, N)) != PD_OK) return bail(rc);
+    double *U, *V, *vbuf, *u1, *us, *k1, *k2, *k32, *ug, *eed, *red, *tdev;
+    float* ugrel;
+    if ((rc = dalloc(c, &U, n3)) || (rc = dalloc(c, &V, n3)) || (rc = dalloc(c, &vbuf, n3)) ||
+        (rc = dalloc(c, &u1, n3)) || (rc = dalloc(c, &us, n3)) || (rc = dalloc(c, &k1, n3)) ||
+        (rc = dalloc(c, &k2, n3)) || (rc = dalloc(c, &k32, n3)) || (rc = dalloc(c, &ug, n3 * c->npt)) ||
+        (rc = dalloc(c, &ugrel, n3 * c->npt)) || (rc = dalloc(c, &eed, N)) ||
+        (rc = dalloc(c, &red, 2 * N + 4 + 2 * 160)) || (rc = dalloc(c, &tdev, 1)) ||
+        (rc = dalloc(c, &c->dotpart, pd::kDotBlocks + 8)) || (rc = dalloc(c, &c->scal, pd::CG_NSLOT)))
+        return bail(rc);
+    if (c->nslit) {
+        double* sl = nullptr;
+        if ((rc = dalloc(c, &sl, 6 * c->nslit)) != PD_OK) return bail(rc);
+        if ((rc = upload(c, sl, c->slits.data(), sizeof(double) * 6 * c->nslit)) != PD_OK) return bail(rc);
+        c->dslits = sl;
+    }
+    // materials, boundary conditions, Gauss constants
+    std::vector<pd::MatDev> hm(P->num_materials);
+    for (int k = 0; k < P->num_materials; ++k) {
+        hm[k].spring = P->materials[k].spring;
+        hm[k].density = P->materials[k].density;
+        hm[k].ecrit = P->materials[k].ecrit;
+        for (int a = 0; a < 3; ++a) hm[k].grav[a] = P->materials[k].grav[a];
+    }
+    std::vector<pd::BcDev> hb(std::max(P->num_bcs, 1));
+    for (int k = 0; k < P->num_bcs; ++k) {
+        hb[k].type = P->bcs[k].type;
+        for (int a = 0; a < 3; ++a) hb[k].dir[a] = P->bcs[k].dir[a];
+        for (int a = 0; a < 9; ++a) hb[k].val[a] = P->bcs[k].value[a];
+        hb[k].end_time = P->bcs[k].end_time;
+        hb[k].load_type = P->bcs[k].load_type;
+    }
+    std::vector<pd::GaussConst> hg(c->npt);
+    {
+        const double vol8 = std::pow(d.dx, 3.0) / 8.0;  // pow(_gridSpacing, 3)/8.0, pdDataManager.cpp:1953
+        std::vector<double> a(n1, 0.0), w(n1, 2.0);
+        if (!d.cci) {
+            for (int k = 0; k < n1; ++k) { a[k] = P->abscissae[k]; w[k] = P->weights[k]; }
+        }
+        for (int i = 0; i < n1; ++i)
+            for (int j = 0; j < n1; ++j)
+                for (int k = 0; k < n1; ++k) {
+                    pd::GaussConst& G = hg[(i * n1 + j) * n1 + k];
+                    G.hg[0] = 0.5 * d.dx * a[i];
+                    G.hg[1] = 0.5 * d.dx * a[j];
+                    G.hg[2] = 0.5 * d.dx * a[k];
+                    const double w1 = w[i], w2 = w[j], w3 = w[k];
+                    const double effw = std::pow(w1 * w2 * w3, 1.0 / 3.0);
+                    G.W = vol8 * w1 * w2 * w3;
+                    G.dxe = effw * d.dx / 2.0;
+                    G.pw3 = std::pow(0.5 * effw, 3);
+                    for (int q = 0; q < 3; ++q) G.hgf[q] = (float)G.hg[q];
+                    G.Wf = (float)G.W;
+                    G.A = (float)(d.delta + 0.5 * G.dxe);
+                    G.B = (float)(1.0 / G.dxe);
+                }
+    }
+    std::vector<double> xs(n3);
+    for (int64_t i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) xs[a * N + i] = P->coords[3 * i + a];
+    std::vector<int32_t> bcv(N, -1);
+    if (P->bc_id) std::copy(P->bc_id, P->bc_id + N, bcv.begin());
+    std::vector<double> ones(N, 1.0);
+    if ((rc = upload(c, x, xs.data(), sizeof(double) * n3)) || (rc = upload(c, mat, P->mat_id, sizeof(int32_t) * N)) ||
+        (rc = upload(c, bc, bcv.data(), sizeof(int32_t) * N)) ||
+        (rc = upload(c, mats, hm.data(), sizeof(pd::MatDev) * hm.size())) ||
+        (rc = upload(c, bcs, hb.data(), sizeof(pd::BcDev) * hb.size())) ||
+        (rc = upload(c, gc, hg.data(), sizeof(pd::GaussConst) * hg.size())) ||
+        (rc = upload(c, bdry, ones.data(), sizeof(double) * N)))
+        return bail(rc);
+    if (P->spring_factor) {
+        double* sf = nullptr;
+        if ((rc = dalloc(c, &sf, N)) != PD_OK || (rc = upload(c, sf, P->spring_factor, sizeof(double) * N)) != PD_OK)
+            return bail(rc);
+        d.sfac = sf;
+    }
+    d.x = x;
+    d.mat = mat;
+    d.bc = bc;
+    d.mats = mats;
+    d.nmat = P->num_materials;
+    d.bcs = bcs;
+    d.nbc = P->num_bcs;
+    d.bdry = bdry;
+    d.gc = gc;
+    d.U = U;
+    d.V = V;
+    d.vbuf = vbuf;
+    d.u1 = u1;
+    d.us = us;
+    d.k1 = k1;
+    d.k2 = k2;
+    d.k32 = k32;
+    d.ug = ug;
+    d.ugrel = ugrel;
+    d.eed = eed;
+    d.red = red;
+    d.tdev = tdev;
+    cudaMemsetAsync(U, 0, sizeof(double) * n3, c->stream);
+    cudaMemsetAsync(V, 0, sizeof(double) * n3, c->stream);
+    cudaMemsetAsync(vbuf, 0, sizeof(double) * n3, c->stream);
+    cudaMemsetAsync(u1, 0, sizeof(double) * n3, c->stream);
+    cudaMemsetAsync(us, 0, sizeof(double) * n3, c->stream);
+    cudaMemsetAsync(ug, 0, sizeof(double) * n3 * c->npt, c->stream);
+    cudaMemsetAsync(ugrel, 0, sizeof(float) * n3 * c->npt, c->stream);
+    cudaMemsetAsync(eed, 0, sizeof(double) * N, c->stream);
+    cudaMemsetAsync(tdev, 0, sizeof(double), c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return bail(pd::fail_cuda(e, "init", __FILE__, __LINE__));
+    *out = c;
+    return PD_OK;
+}
+
+int pd_ctx_destroy(pd_ctx* c) {
+    if (!c) return PD_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    for (void* p : c->owned)
+        if (p) cudaFree(p);
+    if (c->hstage) cudaFreeHost(c->hstage);
+    if (c->hscalar) cudaFreeHost(c->hscalar);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PD_OK;
+}
+
+int pd_ctx_stream(pd_ctx* c, void** s) {
+    if (!c || !s) return fail(PD_ERR_ARG, "pd_ctx_stream: null argument");
+    *s = (void*)c->stream;
+    return PD_OK;
+}
+
+int pd_sync(pd_ctx* c) {
+    if (!c) return fail(PD_ERR_ARG, "pd_sync: null context");
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr, int64_t* arow, int32_t* acol,
+                           int64_t H, int64_t Ha) {
+    dfree(c, c->frow); dfree(c, c->fcol); dfree(c, c->fbroken); dfree(c, c->arow); dfree(c, c->acol);
+    c->frow = frow; c->fcol = fcol; c->fbroken = fbr; c->arow = arow; c->acol = acol;
+    for (void* p : {(void*)frow, (void*)fcol, (void*)fbr, (void*)arow, (void*)acol}) c->owned.push_back(p);
+    c->d.frow = frow; c->d.fcol = fcol; c->d.fbroken = fbr; c->d.arow = arow; c->d.acol = acol;
+    c->H = H;
+    c->Ha = Ha;
+    c->have_family = true;
+    c->generation++;
+}
+
+int pd_bond_search(pd_ctx* c, int64_t* num_halves, int64_t* num_broken, double* min_bond_length) {
+    if (!c) return fail(PD_ERR_ARG, "pd_bond_search: null context");
+    const int64_t N = c->n;
+    pd::SearchGrid g{};
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a) { lo[a] = INFINITY; hi[a] = -INFINITY; }
+    for (int64_t i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], c->coords[3 * i + a]);
+            hi[a] = std::max(hi[a], c->coords[3 * i + a]);
+        }
+    if (N == 0)
+        for (int a = 0; a < 3; ++a) lo[a] = hi[a] = 0.0;
+    g.h = c->d.delta + c->d.dx;  // >= horizon + tolerance + half cell diagonal
+    int64_t ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = lo[a];
+        g.nc[a] = (int64_t)std::floor((hi[a] - lo[a]) / g.h) + 1;
+        ncell *= g.nc[a];
+    }
+    // Morton rank of every cell
+    std::vector<std::pair<uint64_t, int64_t>> keys(ncell);
+    for (int64_t z = 0; z < g.nc[2]; ++z)
+        for (int64_t y = 0; y < g.nc[1]; ++y)
+            for (int64_t xx = 0; xx < g.nc[0]; ++xx) {
+                int64_t lin = (z * g.nc[1] + y) * g.nc[0] + xx;
+                keys[lin] = {morton3(xx, y, z), lin};
+            }
+    std::sort(keys.begin(), keys.end());
+    std::vector<int32_t> rank(ncell);
+    for (int64_t r = 0; r < ncell; ++r) rank[keys[r].second] = (int32_t)r;
+    int32_t* drank = nullptr;
+    PD_TRY(dalloc(c, &drank, ncell));
+    int rc = upload(c, drank, rank.data(), sizeof(int32_t) * ncell);
+    if (rc != PD_OK) { dfree(c, drank); return rc; }
+    double* sl = c->dslits;
+    int64_t *frow, *arow;
+    int32_t *fcol, *acol;
+    uint8_t* fbr;
+    int64_t nh = 0, nb = 0;
+    double mb = 0.0;
+    rc = pd::bond_search(c->d, g, drank, ncell, c->nslit, sl, &frow, &fcol, &fbr, &arow, &acol, &nh, &nb, &mb,
+                         c->stream);
+    dfree(c, drank);
+    if (rc != PD_OK) return rc;
+    install_family(c, frow, fcol, fbr, arow, acol, nh, nh - nb);
+    if (num_halves) *num_halves = nh;
+    if (num_broken) *num_broken = nb;
+    if (min_bond_length) *min_bond_length = mb;
+    return PD_OK;
+}
+
+int pd_get_family(pd_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* broken) {
+    if (!c || !c->have_family) return fail(PD_ERR_ARG, "pd_get_family: no family");
+    if (row_ptr) PD_CUDA_TRY(cudaMemcpyAsync(row_ptr, c->frow, sizeof(int64_t) * (c->n + 1), cudaMemcpyDeviceToHost, c->stream));
+    if (col) PD_CUDA_TRY(cudaMemcpyAsync(col, c->fcol, sizeof(int32_t) * c->H, cudaMemcpyDeviceToHost, c->stream));
+    if (broken) PD_CUDA_TRY(cudaMemcpyAsync(broken, c->fbroken, c->H, cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_set_family(pd_ctx* c, const int64_t* row_ptr, const int32_t* col, const uint8_t* broken) {
+    if (!c || !row_ptr || (!col && row_ptr[c->n] > 0)) return fail(PD_ERR_ARG, "pd_set_family: null argument");
+    const int64_t N = c->n, H = row_ptr[N];
+    if (row_ptr[0] != 0 || H < 0) return fail(PD_ERR_ARG, "pd_set_family: bad row_ptr");
+    for (int64_t i = 0; i < N; ++i)
+        if (row_ptr[i + 1] < row_ptr[i]) return fail(PD_ERR_ARG, "pd_set_family: row_ptr not monotone");
+    for (int64_t p = 0; p < H; ++p)
+        if (col[p] < 0 || col[p] >= N) return fail(PD_ERR_ARG, "pd_set_family: column out of range");
+    std::vector<int64_t> ar(N + 1, 0);
+    std::vector<int32_t> ac;
+    std::vector<uint8_t> br(std::max<int64_t>(H, 1), 0);
+    if (broken) std::copy(broken, broken + H, br.begin());
+    ac.reserve(H);
+    for (int64_t i = 0; i < N; ++i) {
+        for (int64_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p)
+            if (!br[p]) ac.push_back(col[p]);
+        ar[i + 1] = (int64_t)ac.size();
+    }
+    int64_t *frow, *arow;
+    int32_t *fcol, *acol;
+    uint8_t* fbr;
+    PD_TRY(dalloc(c, &frow, N + 1));
+    PD_TRY(dalloc(c, &fcol, H));
+    PD_TRY(dalloc(c, &fbr, H));
+    PD_TRY(dalloc(c, &arow, N + 1));
+    PD_TRY(dalloc(c, &acol, ac.size()));
+    for (void* p : {(void*)frow, (void*)fcol, (void*)fbr, (void*)arow, (void*)acol}) {
+        auto it = std::find(c->owned.begin(), c->owned.end(), p);
+        c->owned.erase(it);
+    }
+    PD_TRY(upload(c, frow, row_ptr, sizeof(int64_t) * (N + 1)));
+    if (H) PD_TRY(upload(c, fcol, col, sizeof(int32_t) * H));
+    if (H) PD_TRY(upload(c, fbr, br.data(), H));
+    PD_TRY(upload(c, arow, ar.data(), sizeof(int64_t) * (N + 1)));
+    if (!ac.empty()) PD_TRY(upload(c, acol, ac.data(), sizeof(int32_t) * ac.size()));
+    install_family(c, frow, fcol, fbr, arow, acol, H, (int64_t)ac.size());
+    return PD_OK;
+}
+
+int pd_set_bdry_eff(pd_ctx* c, const double* bE) {
+    if (!c || !bE) return fail(PD_ERR_ARG, "pd_set_bdry_eff: null argument");
+    return upload(c, (void*)c->d.bdry, bE, sizeof(double) * c->n);
+}
+
+int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const double* coeff) {
+    if (!c || !cb_ptr || !cb_idx || !coeff) return fail(PD_ERR_ARG, "pd_set_mls: null argument");
+    if (!c->d.mls) return fail(PD_ERR_ARG, "pd_set_mls: MLS is off for this integration scheme");
+    const int64_t N = c->n, T = cb_ptr[N];
+    const int npt = c->npt;
+    if (cb_ptr[0] != 0) return fail(PD_ERR_ARG, "pd_set_mls: bad cb_ptr");
+    for (int64_t i = 0; i < N; ++i)
+        if (cb_ptr[i + 1] < cb_ptr[i]) return fail(PD_ERR_ARG, "pd_set_mls: cb_ptr not monotone");
+    for (int64_t k = 0; k < T; ++k)
+        if (cb_idx[k] < 0 || cb_idx[k] >= N) return fail(PD_ERR_ARG, "pd_set_mls: contributor out of range");
+    // re-layout [node][point][contributor] -> [node][contributor][point]
+    std::vector<double> co((size_t)T * npt);
+    std::vector<float> co32((size_t)T * npt), cs((size_t)N * npt);
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t b = cb_ptr[i], nc = cb_ptr[i + 1] - b;
+        for (int g = 0; g < npt; ++g) {
+            double s = 0.0;
+            for (int64_t k = 0; k < nc; ++k) {
+                const double v = coeff[b * npt + (int64_t)g * nc + k];
+                co[(b + k) * npt + g] = v;
+                co32[(b + k) * npt + g] = (float)v;
+                s += v;
+            }
+            cs[i * npt + g] = (float)(s - 1.0);
+        }
+    }
+    dfree(c, c->cbptr); dfree(c, c->cbidx); dfree(c, c->coeff); dfree(c, c->coeff32); dfree(c, c->csum);
+    c->cbptr = nullptr; c->cbidx = nullptr; c->coeff = nullptr; c->coeff32 = nullptr; c->csum = nullptr;
+    PD_TRY(dalloc(c, &c->cbptr, N + 1));
+    PD_TRY(dalloc(c, &c->cbidx, T));
+    PD_TRY(dalloc(c, &c->coeff, (size_t)T * npt));
+    PD_TRY(dalloc(c, &c->coeff32, (size_t)T * npt));
+    PD_TRY(dalloc(c, &c->csum, (size_t)N * npt));
+    PD_TRY(upload(c, c->cbptr, cb_ptr, sizeof(int64_t) * (N + 1)));
+    if (T) PD_TRY(upload(c, c->cbidx, cb_idx, sizeof(int32_t) * T));
+    if (T) PD_TRY(upload(c, c->coeff, co.data(), sizeof(double) * co.size()));
+    if (T) PD_TRY(upload(c, c->coeff32, co32.data(), sizeof(float) * co32.size()));
+    PD_TRY(upload(c, c->csum, cs.data(), sizeof(float) * cs.size()));
+    c->d.cbptr = c->cbptr;
+    c->d.cbidx = c->cbidx;
+    c->d.coeff = c->coeff;
+    c->d.coeff32 = c->coeff32;
+    c->d.csum = c->csum;
+    c->have_mls = true;
+    c->generation++;
+    return PD_OK;
+}
+
+int pd_set_precision(pd_ctx* c, int p) {
+    if (!c || (p != PD_PREC_FP64 && p != PD_PREC_FP32C)) return fail(PD_ERR_ARG, "pd_set_precision: bad argument");
+    c->precision = p;
+    return PD_OK;
+}
+
+int pd_set_energy(pd_ctx* c, int on) {
+    if (!c) return fail(PD_ERR_ARG, "pd_set_energy: null context");
+    c->d.energy = on ? 1 : 0;
+    return PD_OK;
+}
+
+int pd_set_state(pd_ctx* c, const double* U, const double* V) {
+    if (!c) return fail(PD_ERR_ARG, "pd_set_state: null context");
+    const size_t b3 = sizeof(double) * 3 * c->n;
+    if (U) {
+        PD_TRY(upload_vec3(c, c->d.U, U));
+        PD_CUDA_TRY(cudaMemcpyAsync(c->d.u1, c->d.U, b3, cudaMemcpyDeviceToDevice, c->stream));
+        PD_CUDA_TRY(cudaMemcpyAsync(c->d.us, c->d.U, b3, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    if (V) {
+        PD_TRY(upload_vec3(c, c->d.V, V));
+        PD_CUDA_TRY(cudaMemcpyAsync(c->d.vbuf, c->d.V, b3, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_get_state(pd_ctx* c, double* U, double* V) {
+    if (!c) return fail(PD_ERR_ARG, "pd_get_state: null context");
+    if (U) PD_TRY(download_vec3(c, U, c->d.U));
+    if (V) PD_TRY(download_vec3(c, V, c->d.V));
+    return PD_OK;
+}
+
+int pd_get_vbuf(pd_ctx* c, double* vb) {
+    if (!c || !vb) return fail(PD_ERR_ARG, "pd_get_vbuf: null argument");
+    return download_vec3(c, vb, c->d.vbuf);
+}
+
+int pd_set_gauss_displ(pd_ctx* c, const double* ug) {
+    if (!c || !ug) return fail(PD_ERR_ARG, "pd_set_gauss_displ: null argument");
+    const int64_t M = c->n * c->npt;
+    double* tmp = nullptr;
+    PD_TRY(dalloc(c, &tmp, 3 * M));
+    int rc = upload(c, tmp, ug, sizeof(double) * 3 * M);
+    if (rc == PD_OK) {
+        // [node][point][3] -> [point*3 + a][node]
+        std::vector<double> h(3 * M);
+        for (int64_t i = 0; i < c->n; ++i)
+            for (int g = 0; g < c->npt; ++g)
+                for (int a = 0; a < 3; ++a) h[(int64_t)(3 * g + a) * c->n + i] = ug[(i * c->npt + g) * 3 + a];
+        rc = upload(c, c->d.ug, h.data(), sizeof(double) * 3 * M);
+    }
+    dfree(c, tmp);
+    return rc;
+}
+
+int pd_get_gauss_displ(pd_ctx* c, double* ug) {
+    if (!c || !ug) return fail(PD_ERR_ARG, "pd_get_gauss_displ: null argument");
+    const int64_t M = c->n * c->npt;
+    std::vector<double> h(3 * M);
+    PD_CUDA_TRY(cudaMemcpyAsync(h.data(), c->d.ug, sizeof(double) * 3 * M, cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < c->n; ++i)
+        for (int g = 0; g < c->npt; ++g)
+            for (int a = 0; a < 3; ++a) ug[(i * c->npt + g) * 3 + a] = h[(int64_t)(3 * g + a) * c->n + i];
+    return PD_OK;
+}
+
+int pd_get_energy_density(pd_ctx* c, double* eed) {
+    if (!c || !eed) return fail(PD_ERR_ARG, "pd_get_energy_density: null argument");
+    PD_CUDA_TRY(cudaMemcpyAsync(eed, c->d.eed, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_init_dynamic(pd_ctx* c) {
+    if (!c) return fail(PD_ERR_ARG, "pd_init_dynamic: null context");
+    const size_t b3 = sizeof(double) * 3 * c->n;
+    PD_CUDA_TRY(cudaMemcpyAsync(c->d.vbuf, c->d.V, b3, cudaMemcpyDeviceToDevice, c->stream));
+    PD_CUDA_TRY(cudaMemsetAsync(c->d.eed, 0, sizeof(double) * c->n, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_gather(pd_ctx* c, double time, const double* us) {
+    if (!c) return fail(PD_ERR_ARG, "pd_gather: null context");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_gather: family/MLS data not set");
+    PD_TRY(set_time(c, time));
+    const double* src = c->d.U;
+    if (us) {
+        PD_TRY(upload_vec3(c, c->d.us, us));
+        src = c->d.us;
+    }
+    if (c->precision == PD_PREC_FP32C) pd::launch_gather_f32c(c->d, src, c->stream);
+    else pd::launch_gather_f64(c->d, src, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_force_stage(pd_ctx* c, double dt, double time, const double* us, double* k_out) {
+    if (!c || !us) return fail(PD_ERR_ARG, "pd_force_stage: null argument");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_force_stage: family/MLS data not set");
+    PD_TRY(set_time(c, time));
+    PD_TRY(upload_vec3(c, c->d.us, us));
+    if (c->precision == PD_PREC_FP32C) pd::launch_force_f32c(c->d, dt, c->stream);
+    else pd::launch_force_f64(c->d, dt, c->stream);
+    pd::launch_epilogue(c->d, 0, dt, dt, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    if (k_out) PD_TRY(download_vec3(c, k_out, c->d.k1));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_rk4_step(pd_ctx* c, double dt, double time, double* ke, double* ee) {
+    if (!c) return fail(PD_ERR_ARG, "pd_rk4_step: null context");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_rk4_step: family/MLS data not set");
+    PD_TRY(set_time(c, time));
+    enqueue_step_body(c, dt);
+    PD_CUDA_TRY(cudaGetLastError());
+    if (c->d.energy && (ke || ee)) {
+        PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, c->d.red + 2 * c->n, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    }
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (ke) *ke = c->d.energy ? c->hscalar[0] : 0.0;
+    if (ee) *ee = c->d.energy ? c->hscalar[1] : 0.0;
+    return PD_OK;
+}
+
+int pd_rk4_steps(pd_ctx* c, double dt, double t0, int nsteps) {
+    if (!c || nsteps < 0) return fail(PD_ERR_ARG, "pd_rk4_steps: bad argument");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_rk4_steps: family/MLS data not set");
+    if (nsteps == 0) return PD_OK;
+    PD_TRY(set_time(c, t0));
+    if (!c->step_graph || c->graph_dt != dt || c->graph_prec != c->precision || c->graph_energy != c->d.energy ||
+        c->graph_generation != c->generation) {
+        if (c->step_graph) {
+            cudaGraphExecDestroy(c->step_graph);
+            c->step_graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        PD_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        pd::launch_advance_time(c->d.tdev, dt, c->stream);
+        enqueue_step_body(c, dt);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (e != cudaSuccess) return pd::fail_cuda(e, "capture", __FILE__, __LINE__);
+        e = cudaGraphInstantiate(&c->step_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return pd::fail_cuda(e, "instantiate", __FILE__, __LINE__);
+        c->graph_dt = dt;
+        c->graph_prec = c->precision;
+        c->graph_energy = c->d.energy;
+        c->graph_generation = c->generation;
+    }
+    for (int k = 0; k < nsteps; ++k) PD_CUDA_TRY(cudaGraphLaunch(c->step_graph, c->stream));
+    PD_CUDA_TRY(cudaGetLastError());
+    return PD_OK;
+}
+
+int pd_rk4_steps_host(pd_ctx* c, double dt, double t0, int nsteps, const double* U_in, const double* V_in,
+                      double* U_out, double* V_out) {
+    if (!c) return fail(PD_ERR_ARG, "pd_rk4_steps_host: null context");
+    const size_t b3 = sizeof(double) * 3 * c->n;
+    if (U_in) {
+        PD_CUDA_TRY(cudaMemcpyAsync(c->scratch, U_in, b3, cudaMemcpyHostToDevice, c->stream));
+        pd::launch_to_soa(c->scratch, c->d.U, c->n, 3, c->stream);
+    }
+    if (V_in) {
+        PD_CUDA_TRY(cudaMemcpyAsync(c->scratch + 3 * c->n, V_in, b3, cudaMemcpyHostToDevice, c->stream));
+        pd::launch_to_soa(c->scratch + 3 * c->n, c->d.V, c->n, 3, c->stream);
+    }
+    PD_TRY(pd_rk4_steps(c, dt, t0, nsteps));
+    if (U_out) {
+        pd::launch_to_aos(c->d.U, c->scratch, c->n, 3, c->stream);
+        PD_CUDA_TRY(cudaMemcpyAsync(U_out, c->scratch, b3, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (V_out) {
+        pd::launch_to_aos(c->d.V, c->scratch + 3 * c->n, c->n, 3, c->stream);
+        PD_CUDA_TRY(cudaMemcpyAsync(V_out, c->scratch + 3 * c->n, b3, cudaMemcpyDeviceToHost, c->stream));
+    }
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
+int pd_reset_state(pd_ctx* c) {
+    if (!c) return fail(PD_ERR_ARG, "pd_reset_state: null context");
+    const size_t b3 = sizeof(double) * 3 * c->n;
+    cudaStream_t s = c->stream;
+    for (double* p : {c->d.U, c->d.V, c->d.vbuf, c->d.u1, c->d.us}) PD_CUDA_TRY(cudaMemsetAsync(p, 0, b3, s));
+    PD_CUDA_TRY(cudaMemsetAsync(c->d.ug, 0, b3 * c->npt, s));
+    PD_CUDA_TRY(cudaMemsetAsync(c->d.ugrel, 0, sizeof(float) * 3 * c->n * c->npt, s));
+    PD_CUDA_TRY(cudaMemsetAsync(c->d.eed, 0, sizeof(double) * c->n, s));
+    PD_CUDA_TRY(cudaStreamSynchronize(s));
+    return PD_OK;
+}
+
+int pd_profile_step(pd_ctx* c, double dt, double time, double* ms) {
+    if (!c || !ms) return fail(PD_ERR_ARG, "pd_profile_step: null argument");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_profile_step: family/MLS data not set");
+    PD_TRY(set_time(c, time));
+    cudaStream_t s = c->stream;
+    const pd::Dev& d = c->d;
+    const bool f32 = c->precision == PD_PREC_FP32C;
+    const int64_t n3 = 3 * c->n;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> cls;
+    auto mark = [&](int k) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        ev.push_back(e);
+        cls.push_back(k);
+    };
+    auto force = [&](double dts) {
+        mark(-1);
+        if (f32) pd::launch_force_f32c(d, dts, s);
+        else pd::launch_force_f64(d, dts, s);
+        mark(0);
+    };
+    auto gather = [&](const double* us) {
+        mark(-1);
+        if (f32) pd::launch_gather_f32c(d, us, s);
+        else pd::launch_gather_f64(d, us, s);
+        mark(1);
+    };
+    auto epi = [&](int st, double dts) {
+        mark(-1);
+        pd::launch_epilogue(d, st, dts, dt, s);
+        mark(2);
+    };
+    const double h = 0.5 * dt;
+    mark(-1);
+    cudaMemcpyAsync(d.vbuf, d.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.u1, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.us, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    if (d.energy) cudaMemsetAsync(d.eed, 0, sizeof(double) * c->n, s);
+    mark(3);
+    force(h); epi(1, h);
+    gather(d.us); force(h); epi(2, h);
+    gather(d.us); force(dt); epi(3, dt);
+    gather(d.us); force(dt); epi(4, dt);
+    mark(-1);
+    if (d.energy) pd::launch_energy_reduce(d, s);
+    mark(3);
+    gather(d.U);
+    cudaError_t e = cudaStreamSynchronize(s);
+    for (int k = 0; k < 4; ++k) ms[k] = 0.0;
+    for (size_t k = 1; k < ev.size(); ++k) {
+        if (cls[k] < 0) continue;
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[k - 1], ev[k]);
+        ms[cls[k]] += t;
+    }
+    for (cudaEvent_t x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) return pd::fail_cuda(e, "profile step", __FILE__, __LINE__);
+    return PD_OK;
+}
+
+int pd_evals_per_stage(pd_ctx* c, int64_t* ev) {
+    if (!c || !ev) return fail(PD_ERR_ARG, "pd_evals_per_stage: null argument");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_evals_per_stage: no family");
+    *ev = c->d.cci ? c->Ha : c->Ha * c->npt;
+    return PD_OK;
+}
+
+// ----------------------------------------------------------------- static
+
+int pd_static_matvec(pd_ctx* c, double time, const double* x, double* y) {
+    if (!c || !x || !y) return fail(PD_ERR_ARG, "pd_static_matvec: null argument");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_static_matvec: no family");
+    PD_TRY(upload_vec3(c, c->d.us, x));
+    pd::launch_static_apply_f64(c->d, time, c->d.us, c->d.k1, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    return download_vec3(c, y, c->d.k1);
+}
+
+int pd_static_rhs(pd_ctx* c, double time, double* b) {
+    if (!c || !b) return fail(PD_ERR_ARG, "pd_static_rhs: null argument");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_static_rhs: no family");
+    pd::launch_static_rhs(c->d, time, c->d.k1, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    return download_vec3(c, b, c->d.k1);
+}
+
+}  // extern "C"
+
+namespace {
+
+// plain CG on A x = b, FP64 or FP32 vectors; scalars live on the device and
+// the residual is read back every `check` iterations
+template <typename T>
+int cg_device(pd_ctx* c, double time, const T* b, T* x, T* r, T* p, T* q, double rtol, int maxit, int* iters,
+              double* relres, bool zero_guess) {
+    const int64_t n3 = 3 * c->n;
+    cudaStream_t s = c->stream;
+    double* scal = c->scal;
+    auto apply = [&](const T* in, T* out) {
+        if constexpr (sizeof(T) == 8) pd::launch_static_apply_f64(c->d, time, (const double*)in, (double*)out, s);
+        else pd::launch_static_apply_f32(c->d, time, (const float*)in, (float*)out, s);
+    };
+    auto dot = [&](const T* a, const T* bb, double* out) {
+        if constexpr (sizeof(T) == 8) pd::launch_dot_f64((const double*)a, (const double*)bb, n3, c->dotpart, out, s);
+        else pd::launch_dot_f32((const float*)a, (const float*)bb, n3, c->dotpart, out, s);
+    };
+    dot(b, b, scal + pd::CG_BB);
+    if (zero_guess) {
+        PD_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * n3, s));
+        PD_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(T) * n3, cudaMemcpyDeviceToDevice, s));
+    } else {
+        apply(x, q);
+        if constexpr (sizeof(T) == 8) pd::launch_sub_f64((const double*)b, (const double*)q, (double*)r, n3, s);
+        else return fail(PD_ERR_ARG, "FP32 CG needs a zero initial guess");
+    }
+    PD_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(T) * n3, cudaMemcpyDeviceToDevice, s));
+    dot(r, r, scal + pd::CG_RR);
+    PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    PD_CUDA_TRY(cudaStreamSynchronize(s));
+    const double bb = c->hscalar[pd::CG_BB] > 0.0 ? c->hscalar[pd::CG_BB] : 1.0;
+    double rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+    int it = 0;
+    const int check = 10;
+    while (rel > rtol && it < maxit) {
+        for (int k = 0; k < check && it < maxit; ++k, ++it) {
+            apply(p, q);
+            dot(p, q, scal + pd::CG_PQ);
+            if constexpr (sizeof(T) == 8) {
+                pd::launch_cg_update_x_f64((double*)x, (double*)r, (const double*)p, (const double*)q, n3, scal, s);
+                dot(r, r, scal + pd::CG_RRN);
+                pd::launch_cg_update_p_f64((const double*)r, (double*)p, n3, scal, s);
+            } else {
+                pd::launch_cg_update_x_f32((float*)x, (float*)r, (const float*)p, (const float*)q, n3, scal, s);
+                dot(r, r, scal + pd::CG_RRN);
+                pd::launch_cg_update_p_f32((const float*)r, (float*)p, n3, scal, s);
+            }
+            pd::launch_cg_swap(scal, s);
+        }
+        PD_CUDA_TRY(cudaGetLastError());
+        PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+        PD_CUDA_TRY(cudaStreamSynchronize(s));
+        rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+        if (!std::isfinite(rel)) break;
+    }
+    if (iters) *iters = it;
+    if (relres) *relres = rel;
+    return (rel <= rtol) ? PD_OK : PD_ERR_NOCONV;
+}
+
+}  // namespace
+
+extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rtol, int maxit, double* x, int* iters,
+                    double* relres) {
+    if (!c || !x) return fail(PD_ERR_ARG, "pd_static_solve: null argument");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_static_solve: no family");
+    const int64_t n3 = 3 * c->n;
+    cudaStream_t s = c->stream;
+    double *b = nullptr, *xd = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    PD_TRY(dalloc(c, &b, n3));
+    PD_TRY(dalloc(c, &xd, n3));
+    PD_TRY(dalloc(c, &r, n3));
+    PD_TRY(dalloc(c, &p, n3));
+    PD_TRY(dalloc(c, &q, n3));
+    auto cleanup = [&]() { dfree(c, b); dfree(c, xd); dfree(c, r); dfree(c, p); dfree(c, q); };
+    int rc = upload_vec3(c, xd, x);
+    if (rc != PD_OK) { cleanup(); return rc; }
+    pd::launch_static_rhs(c->d, time, b, s);
+    int it_total = 0;
+    double rel = 0.0;
+    if (precision == PD_PREC_FP64) {
+        rc = cg_device<double>(c, time, b, xd, r, p, q, rtol, maxit, &it_total, &rel, false);
+    } else {
+        // iterative refinement: FP64 residual, FP32 inner CG on the scaled residual
+        float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *b32 = nullptr;
+        rc = dalloc(c, &d32, n3);
+        if (rc == PD_OK) rc = dalloc(c, &r32, n3);
+        if (rc == PD_OK) rc = dalloc(c, &p32, n3);
+        if (rc == PD_OK) rc = dalloc(c, &q32, n3);
+        if (rc == PD_OK) rc = dalloc(c, &b32, n3);
+        double bb = 0.0;
+        if (rc == PD_OK) {
+            pd::launch_dot_f64(b, b, n3, c->dotpart, c->scal + pd::CG_BB, s);
+            cudaMemcpyAsync(c->hscalar + 4, c->scal + pd::CG_BB, sizeof(double), cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
+            bb = std::sqrt(c->hscalar[4]);
+            if (!(bb > 0.0)) bb = 1.0;
+        }
+        int outer = 0;
+        while (rc == PD_OK) {
+            pd::launch_static_apply_f64(c->d, time, xd, q, s);
+            pd::launch_sub_f64(b, q, r, n3, s);
+            pd::launch_dot_f64(r, r, n3, c->dotpart, c->scal + pd::CG_RRN, s);
+            cudaMemcpyAsync(c->hscalar + 4, c->scal + pd::CG_RRN, sizeof(double), cudaMemcpyDeviceToHost, s);
+            if (cudaStreamSynchronize(s) != cudaSuccess) { rc = fail(PD_ERR_CUDA, "refinement residual"); break; }
+            const double rn = std::sqrt(c->hscalar[4]);
+            rel = rn / bb;
+            if (rel <= rtol || it_total >= maxit || outer > 60 || !std::isfinite(rel)) break;
+            ++outer;
+            // inner solve on r / |r| in FP32 to a relative 1e-4
+            pd::launch_f64_to_f32(r, b32, 1.0 / rn, n3, s);
+            int inner = 0;
+            double irel = 0.0;
+            int irc = cg_device<float>(c, time, b32, d32, r32, p32, q32, 1e-4, maxit - it_total, &inner, &irel, true);
+            it_total += inner;
+            if (irc != PD_OK && irc != PD_ERR_NOCONV) { rc = irc; break; }
+            pd::launch_add_f32_to_f64(xd, d32, rn, n3, s);
+        }
+        dfree(c, d32); dfree(c, r32); dfree(c, p32); dfree(c, q32); dfree(c, b32);
+        if (rc == PD_OK && rel > rtol) rc = PD_ERR_NOCONV;
+    }
+    int rc2 = download_vec3(c, x, xd);
+    cleanup();
+    if (iters) *iters = it_total;
+    if (relres) *relres = rel;
+    if (rc == PD_ERR_NOCONV) return fail(PD_ERR_NOCONV, "static solve did not reach the tolerance");
+    return rc != PD_OK ? rc : rc2;
+}

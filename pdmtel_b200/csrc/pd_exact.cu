@@ -1,0 +1,728 @@
+// FP64 kernels of the drop-in path.
+//
+// This translation unit is compiled with -fmad=false: every multiply and add
+// is rounded on its own, in the order the reference's C++ evaluates it, and
+// double division and square root are IEEE round-to-nearest.  One thread owns
+// one node and sums its family in ascending id order, which is the order of
+// the reference's loops, so the force, gather and state vectors are bit-for-
+// bit those of the reference CPU path (pdDataManager.cpp:1767-2134).
+#include <cfloat>
+#include <cstdio>
+#include <vector>
+
+#include "pd_internal.cuh"
+
+namespace pd {
+
+namespace {
+
+constexpr double kMega = DBL_MAX;  // pdIntgManager.h:26
+constexpr double kTiny = DBL_MIN;  // pdIntgManager.h:27
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+
+// pdBdryCondition*::GetTimeFactor (pdBdryConditionDispl.cpp:15, ...Veloc.cpp:15,
+// ...DisplGrad.cpp:16, ...Tract.cpp:15)
+__device__ __forceinline__ double time_factor(const BcDev& b, double t) {
+    if (b.type == PD_BC_VELOC) return (t <= b.end_time) ? 1.0 : 0.0;
+    if (b.load_type == 1.0) return (t <= b.end_time) ? t / b.end_time : 1.0;
+    return 1.0;
+}
+
+// pdDataManager::CalcBetaFactor, pdDataManager3.cpp:1801-1829
+__device__ __forceinline__ double beta_factor(double dist, double delta, double dx, bool cci_original) {
+    double inner = delta - 0.5 * dx;
+    double outer = delta + 0.5 * dx;
+    if (cci_original) outer = delta;
+    if (dist <= inner) return 1.0;
+    if (dist > inner && dist <= outer) return (delta + 0.5 * dx - dist) / dx;
+    return 0.0;
+}
+
+// ------------------------------------------------------------------ force
+
+// One thread per node.  FGI: the Gauss-point summation branch of
+// CalcBondBasedMotionRK4 (pdDataManager.cpp:1917-1962) with the per-point
+// CalcBondForceCCI (pdDataManager2.cpp:1293-1351).  CCI: the one-point
+// branch (pdDataManager.cpp:1818-1866).
+template <bool CCI, bool ENERGY, bool SFAC>
+__global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
+    extern __shared__ GaussConst sg[];
+    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const MatDev Mi = d.mats[d.mat[i]];
+    const double rho = Mi.density;
+    const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
+    const bool bci = d.bc[i] >= 0;
+    const double* src = bci ? d.U : d.us;
+    const double ui0 = src[i], ui1 = src[N + i], ui2 = src[2 * N + i];
+    const double xi0 = d.x[i], xi1 = d.x[N + i], xi2 = d.x[2 * N + i];
+    const double bEi = d.bdry[i];
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
+    double eacc = ENERGY ? d.eed[i] : 0.0;
+    const bool cci_orig = d.cci && !d.cci_mdf;
+    const int64_t pe = d.arow[i + 1];
+    for (int64_t p = d.arow[i]; p < pe; ++p) {
+        const int64_t j = d.acol[p];
+        const MatDev& Mj = d.mats[d.mat[j]];
+        const double ecrit = dmin(Mi.ecrit, Mj.ecrit);
+        double c = dmin(Mi.spring, Mj.spring);
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const double bE = 0.5 * (bEi + d.bdry[j]);
+        const double xj0 = d.x[j], xj1 = d.x[N + j], xj2 = d.x[2 * N + j];
+        double F0 = 0.0, F1 = 0.0, F2 = 0.0;
+        if (CCI) {
+            const double* sj = (d.bc[j] >= 0) ? d.U : d.us;
+            const double xv0 = xj0 - xi0, xv1 = xj1 - xi1, xv2 = xj2 - xi2;
+            const double ev0 = sj[j] - ui0, ev1 = sj[N + j] - ui1, ev2 = sj[2 * N + j] - ui2;
+            const double r = sqrt(xv0 * xv0 + xv1 * xv1 + xv2 * xv2);
+            const double y0 = xv0 + ev0, y1 = xv1 + ev1, y2 = xv2 + ev2;
+            const double pl = sqrt(y0 * y0 + y1 * y1 + y2 * y2);
+            const double dxe = 2.0 * d.dx / 2.0;
+            const double beta = beta_factor(r, d.delta, dxe, cci_orig);
+            const double u = pl - r;
+            const double s = u / r;
+            if (u <= 0.0 || (u > 0.0 && s <= ecrit)) {
+                const double t = bE * d.vol_cci * beta * c * s;
+                F0 = t * y0 / pl;
+                F1 = t * y1 / pl;
+                F2 = t * y2 / pl;
+                if (ENERGY) eacc += bE * 0.5 * (0.5 * beta * (c / r) * u * u) * 1.0;
+            } else if (ENERGY) {
+                eacc += 0.0;
+            }
+        } else {
+            for (int g = 0; g < d.npt; ++g) {
+                const GaussConst& G = sg[g];
+                const double xv0 = (G.hg[0] + xj0) - xi0;
+                const double xv1 = (G.hg[1] + xj1) - xi1;
+                const double xv2 = (G.hg[2] + xj2) - xi2;
+                const double* ugp = d.ug + (int64_t)(3 * g) * N + j;
+                const double ev0 = ugp[0] - ui0, ev1 = ugp[N] - ui1, ev2 = ugp[2 * N] - ui2;
+                const double r = sqrt(xv0 * xv0 + xv1 * xv1 + xv2 * xv2);
+                const double y0 = xv0 + ev0, y1 = xv1 + ev1, y2 = xv2 + ev2;
+                const double pl = sqrt(y0 * y0 + y1 * y1 + y2 * y2);
+                const double beta = beta_factor(r, d.delta, G.dxe, false);
+                const double u = pl - r;
+                const double s = u / r;
+                double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+                if (u <= 0.0 || (u > 0.0 && s <= ecrit)) {
+                    const double t = bE * beta * c * s;
+                    f0 = t * y0 / pl;
+                    f1 = t * y1 / pl;
+                    f2 = t * y2 / pl;
+                    if (ENERGY) eacc += bE * 0.5 * (0.5 * beta * (c / r) * u * u) * G.pw3;
+                } else if (ENERGY) {
+                    eacc += 0.0;
+                }
+                F0 += G.W * f0;
+                F1 += G.W * f1;
+                F2 += G.W * f2;
+            }
+        }
+        v0 += (F0 + b0) * dts / rho;
+        v1 += (F1 + b1) * dts / rho;
+        v2 += (F2 + b2) * dts / rho;
+    }
+    d.vbuf[i] = v0;
+    d.vbuf[N + i] = v1;
+    d.vbuf[2 * N + i] = v2;
+    if (ENERGY) d.eed[i] = eacc;
+}
+
+// ----------------------------------------------------------------- gather
+
+// One thread per (node, Gauss point): CalcIntgPointDisplRK4 (pdDataManager.cpp:
+// 2402-2495) with UpdateIntgPointStatusWithBC (:2604-2703).  Nodes with a
+// boundary condition keep the displacement of their unflagged directions
+// (VELOC and TRACTION nodes keep all three), exactly as the reference's
+// Gaussian points do.
+__global__ void k_gather_f64(Dev d, const double* __restrict__ us) {
+    const int64_t N = d.n;
+    const double t = *d.tdev;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= N * d.npt) return;
+    const int64_t i = tid / d.npt;
+    const int g = (int)(tid - i * d.npt);
+    double* ug = d.ug + (int64_t)(3 * g) * N + i;
+    const int b = d.bc[i];
+    if (b >= 0) {
+        const BcDev& B = d.bcs[b];
+        const double fac = time_factor(B, t);
+        const GaussConst& G = d.gc[g];
+        const double q0 = G.hg[0] + d.x[i], q1 = G.hg[1] + d.x[N + i], q2 = G.hg[2] + d.x[2 * N + i];
+        for (int a = 0; a < 3; ++a) {
+            if (B.dir[a] != 1) continue;
+            if (B.type == PD_BC_DISPL) ug[a * N] = B.val[a] * fac;
+            else if (B.type == PD_BC_DISPLGRAD)
+                ug[a * N] = (B.val[3 * a] * q0 + B.val[3 * a + 1] * q1 + B.val[3 * a + 2] * q2) * fac;
+        }
+        return;
+    }
+    if (d.mls) {
+        const int64_t c0 = d.cbptr[i], nc = d.cbptr[i + 1] - c0;
+        const double* cf = d.coeff + c0 * d.npt + g;
+        const int32_t* cb = d.cbidx + c0;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int64_t k = 0; k < nc; ++k) {
+            const int64_t m = cb[k];
+            const double c = cf[k * d.npt];
+            a0 += us[m] * c;
+            a1 += us[N + m] * c;
+            a2 += us[2 * N + m] * c;
+        }
+        ug[0] = a0;
+        ug[N] = a1;
+        ug[2 * N] = a2;
+    } else {
+        ug[0] = us[i];
+        ug[N] = us[N + i];
+        ug[2 * N] = us[2 * N + i];
+    }
+}
+
+// --------------------------------------------------------------- epilogue
+
+// Per node, after the force kernel of stage `stage` (1..4): the traction load
+// (project rule), UpdateNodeStatusWithBC (pdDataManager.cpp:2497-2602),
+// k = vbuf*dt_s (:1977-1990) and the RK4 bookkeeping of pdDataManager::RK4
+// (:2027-2092): next trial displacement, k3 += k2, and at stage 4 the
+// combination, the damping and the new velocity.
+__global__ void k_epilogue(Dev d, int stage, double dts, double dt) {
+    const int64_t N = d.n;
+    const double t = *d.tdev;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double rho = d.mats[d.mat[i]].density;
+    double v[3] = {d.vbuf[i], d.vbuf[N + i], d.vbuf[2 * N + i]};
+    double U[3] = {d.U[i], d.U[N + i], d.U[2 * N + i]};
+    const int b = d.bc[i];
+    if (b >= 0) {
+        const BcDev& B = d.bcs[b];
+        const double fac = time_factor(B, t);
+        const double X[3] = {d.x[i], d.x[N + i], d.x[2 * N + i]};
+        for (int a = 0; a < 3; ++a) {
+            if (B.dir[a] != 1) continue;
+            if (B.type == PD_BC_TRACTION) {
+                const double tb = B.val[a] * fac / d.dx;
+                v[a] += tb * dts / rho;
+            } else if (B.type == PD_BC_DISPL) {
+                U[a] = B.val[a] * fac;
+                v[a] = 0.0;
+            } else if (B.type == PD_BC_VELOC) {
+                v[a] = B.val[a] * fac;
+            } else if (B.type == PD_BC_DISPLGRAD) {
+                U[a] = (B.val[3 * a] * X[0] + B.val[3 * a + 1] * X[1] + B.val[3 * a + 2] * X[2]) * fac;
+                v[a] = 0.0;
+            }
+        }
+    }
+    const double dt6 = 1.0 / 6.0;
+    double ke = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        const int64_t r = a * N + i;
+        const double k = v[a] * dts;
+        if (stage == 0) {  // single stage call: k is returned in k1
+            d.k1[r] = k;
+        } else if (stage == 1) {
+            d.k1[r] = k;
+            d.us[r] = d.u1[r] + 0.5 * k;
+        } else if (stage == 2) {
+            d.k2[r] = k;
+            d.us[r] = d.u1[r] + 0.5 * k;
+        } else if (stage == 3) {
+            d.us[r] = d.u1[r] + k;
+            d.k32[r] = k + d.k2[r];
+        } else {
+            const double Vold = d.V[r];
+            const double inc = dt6 * (d.k1[r] + k + 2.0 * d.k32[r]);
+            if (b >= 0) U[a] = U[a] + inc;
+            else U[a] = U[a] + inc - dt * d.damping * Vold * dt / rho;
+            v[a] += -d.damping * Vold * dt / rho;
+            d.V[r] = v[a];
+            d.u1[r] = U[a];
+            d.us[r] = U[a];
+        }
+        d.vbuf[r] = v[a];
+        d.U[r] = U[a];
+    }
+    if (stage == 4 && d.energy) {
+        const double velsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        ke = 0.5 * rho * velsq * d.vol;
+        d.red[i] = ke;
+        d.red[N + i] = d.vol * d.eed[i];
+    }
+}
+
+// Deterministic two-level sum of red[0..N) and red[N..2N) into red[2N], red[2N+1].
+__global__ void k_energy_partial(const double* __restrict__ red, int64_t N, double* __restrict__ part) {
+    __shared__ double s0[256], s1[256];
+    double a = 0.0, c = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        a += red[i];
+        c += red[N + i];
+    }
+    s0[threadIdx.x] = a;
+    s1[threadIdx.x] = c;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s0[threadIdx.x] += s0[threadIdx.x + w];
+            s1[threadIdx.x] += s1[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = s0[0];
+        part[2 * blockIdx.x + 1] = s1[0];
+    }
+}
+
+__global__ void k_energy_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int k = 0; k < nb; ++k) {
+            a += part[2 * k];
+            c += part[2 * k + 1];
+        }
+        out[0] = a;
+        out[1] = c;
+    }
+}
+
+__global__ void k_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int64_t n, int comps) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n * comps) return;
+    const int64_t i = t / comps;
+    const int c = (int)(t - i * comps);
+    soa[c * n + i] = aos[t];
+}
+
+__global__ void k_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int64_t n, int comps) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n * comps) return;
+    const int64_t i = t / comps;
+    const int c = (int)(t - i * comps);
+    aos[t] = soa[c * n + i];
+}
+
+__global__ void k_fill(double* p, double v, int64_t n) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+
+inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+void launch_force_f64(const Dev& d, double dts, cudaStream_t s) {
+    if (d.n == 0) return;
+    const int bs = 128;
+    size_t sh = (size_t)d.npt * sizeof(GaussConst);
+    unsigned nb = blocks_for(d.n, bs);
+    const bool sf = d.sfac != nullptr;
+#define PD_FORCE(C, E, S) k_force_f64<C, E, S><<<nb, bs, sh, s>>>(d, dts)
+    if (d.cci) {
+        if (d.energy) { if (sf) PD_FORCE(true, true, true); else PD_FORCE(true, true, false); }
+        else { if (sf) PD_FORCE(true, false, true); else PD_FORCE(true, false, false); }
+    } else {
+        if (d.energy) { if (sf) PD_FORCE(false, true, true); else PD_FORCE(false, true, false); }
+        else { if (sf) PD_FORCE(false, false, true); else PD_FORCE(false, false, false); }
+    }
+#undef PD_FORCE
+}
+
+void launch_gather_f64(const Dev& d, const double* us, cudaStream_t s) {
+    if (d.cci || d.n == 0) return;
+    const int bs = 256;
+    k_gather_f64<<<blocks_for(d.n * d.npt, bs), bs, 0, s>>>(d, us);
+}
+
+void launch_epilogue(const Dev& d, int stage, double dts, double dt, cudaStream_t s) {
+    if (d.n == 0) return;
+    const int bs = 256;
+    k_epilogue<<<blocks_for(d.n, bs), bs, 0, s>>>(d, stage, dts, dt);
+}
+
+// t += dt on the device, as pdSolve.cpp:61 advances currentTime
+__global__ void k_advance_time(double* t, double dt) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *t = *t + dt;
+}
+
+void launch_advance_time(double* t, double dt, cudaStream_t s) { k_advance_time<<<1, 32, 0, s>>>(t, dt); }
+
+void launch_energy_reduce(const Dev& d, cudaStream_t s) {
+    const int nb = 148;
+    double* part = d.red + 2 * d.n + 2;
+    k_energy_partial<<<nb, 256, 0, s>>>(d.red, d.n, part);
+    k_energy_final<<<1, 32, 0, s>>>(part, nb, d.red + 2 * d.n);
+}
+
+void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s) {
+    if (n == 0) return;
+    k_to_soa<<<blocks_for(n * comps, 256), 256, 0, s>>>(aos, soa, n, comps);
+}
+
+void launch_to_aos(const double* soa, double* aos, int64_t n, int comps, cudaStream_t s) {
+    if (n == 0) return;
+    k_to_aos<<<blocks_for(n * comps, 256), 256, 0, s>>>(soa, aos, n, comps);
+}
+
+void launch_fill(double* p, double v, int64_t n, cudaStream_t s) {
+    if (n == 0) return;
+    k_fill<<<blocks_for(n, 256), 256, 0, s>>>(p, v, n);
+}
+
+// ============================================================ bond search
+
+namespace {
+
+__device__ __forceinline__ double shortest_between(double v, double lo, double hi, double tol) {
+    if (v < lo - tol) return fabs(v - lo);
+    if (v > hi + tol) return fabs(v - hi);
+    return 0.0;
+}
+
+__device__ __forceinline__ double longest_between(double v, double lo, double hi, double tol) {
+    if (v < lo - tol) return fabs(v - hi);
+    if (v > hi + tol) return fabs(v - lo);
+    if (v > 0.5 * (hi + lo)) return fabs(v - lo);
+    return fabs(v - hi);
+}
+
+// pdDataManager::CalcDistanceToFace, pdDataManager3.cpp:1573-1661
+__device__ void dist_to_face(int nrm, double xf, const double* pi, const double* pj, double dx, double* dmn,
+                             double* dmx) {
+    const double tol = 1e-4 * dx;
+    const int n1 = nrm == 1, n2 = nrm == 2, n3 = nrm == 3;
+    const double xi1 = pi[0], xi2 = pi[1], xi3 = pi[2];
+    const double xj1 = pj[0], xj2 = pj[1], xj3 = pj[2];
+    if (fabs((xi1 - xj1) * n1 + (xi2 - xj2) * n2 + (xi3 - xj3) * n3) < tol) {
+        *dmn = kMega;
+        *dmx = kTiny;
+        return;
+    }
+    const double x1lo = xj1 - 0.5 * dx, x1hi = xj1 + 0.5 * dx;
+    const double x2lo = xj2 - 0.5 * dx, x2hi = xj2 + 0.5 * dx;
+    const double x3lo = xj3 - 0.5 * dx, x3hi = xj3 + 0.5 * dx;
+    const double x_i = xi1 * n1 + xi2 * n2 + xi3 * n3;
+    const double x_j = xj1 * n1 + xj2 * n2 + xj3 * n3;
+    const double fac = (xf - x_i) / (x_j - x_i);
+    const double x1int = xi1 + fac * (xj1 - xi1);
+    const double x2int = xi2 + fac * (xj2 - xi2);
+    const double x3int = xi3 + fac * (xj3 - xi3);
+    if (x1int > x1lo - tol && x1int < x1hi + tol && x2int > x2lo - tol && x2int < x2hi + tol && x3int > x3lo - tol &&
+        x3int < x3hi + tol) {
+        const double f1 = (1 - n1) * xi1 + n1 * xf;
+        const double f2 = (1 - n2) * xi2 + n2 * xf;
+        const double f3 = (1 - n3) * xi3 + n3 * xf;
+        const double s1 = (1 - n1) * shortest_between(f1, x1lo, x1hi, tol);
+        const double s2 = (1 - n2) * shortest_between(f2, x2lo, x2hi, tol);
+        const double s3 = (1 - n3) * shortest_between(f3, x3lo, x3hi, tol);
+        const double l1 = (1 - n1) * longest_between(f1, x1lo, x1hi, tol);
+        const double l2 = (1 - n2) * longest_between(f2, x2lo, x2hi, tol);
+        const double l3 = (1 - n3) * longest_between(f3, x3lo, x3hi, tol);
+        const double ffs = sqrt(s1 * s1 + s2 * s2 + s3 * s3);
+        const double ffl = sqrt(l1 * l1 + l2 * l2 + l3 * l3);
+        const double itf = sqrt((f1 - xi1) * (f1 - xi1) + (f2 - xi2) * (f2 - xi2) + (f3 - xi3) * (f3 - xi3));
+        *dmn = sqrt(ffs * ffs + itf * itf);
+        *dmx = sqrt(ffl * ffl + itf * itf);
+        return;
+    }
+    *dmn = kMega;
+    *dmx = kTiny;
+}
+
+// InitBond's membership test for the pair (a < b): the rough distance
+// reject of pdDataManager2.cpp:34-38, then CalcDistanceToCube's minimum
+// (pdDataManager3.cpp:637-685) against horizon + tolerance.
+__device__ bool pair_bonded(const double* pa, const double* pb, double dx, double delta, double tol, double* dist) {
+    const double d1 = pb[0] - pa[0], d2 = pb[1] - pa[1], d3 = pb[2] - pa[2];
+    *dist = sqrt(d1 * d1 + d2 * d2 + d3 * d3);
+    if (delta < *dist - 1.5 * dx) return false;
+    double mn = kMega, a, b;
+    for (int ax = 0; ax < 3; ++ax) {
+        dist_to_face(ax + 1, pb[ax] - 0.5 * dx, pa, pb, dx, &a, &b);
+        mn = dmin(mn, a);
+        dist_to_face(ax + 1, pb[ax] + 0.5 * dx, pa, pb, dx, &a, &b);
+        mn = dmin(mn, a);
+    }
+    return mn < delta + tol;
+}
+
+// Project rule for pdSlit (pdSlit.h:6-10 fixes only the keyword): the segment
+// from the lower-id to the higher-id node crosses the rectangle.
+__device__ bool slit_crosses(const double* s, const double* a, const double* b) {
+    int nrm = 0;
+    double ext = s[1] - s[0];
+    for (int k = 1; k < 3; ++k)
+        if (s[2 * k + 1] - s[2 * k] < ext) {
+            ext = s[2 * k + 1] - s[2 * k];
+            nrm = k;
+        }
+    const double c = 0.5 * (s[2 * nrm] + s[2 * nrm + 1]);
+    const double da = a[nrm] - c, db = b[nrm] - c;
+    if (!((da < 0.0 && db > 0.0) || (da > 0.0 && db < 0.0))) return false;
+    const double t = (c - a[nrm]) / (b[nrm] - a[nrm]);
+    for (int k = 0; k < 3; ++k) {
+        if (k == nrm) continue;
+        const double p = a[k] + t * (b[k] - a[k]);
+        if (p < s[2 * k] || p > s[2 * k + 1]) return false;
+    }
+    return true;
+}
+
+struct SearchArgs {
+    const double* x;  // [3][N]
+    int64_t n;
+    double dx, delta, tol;
+    SearchGrid g;
+    const int32_t* cell_rank;  // linear cell -> Morton rank
+    const int64_t* cstart;     // [ncell+1] by rank
+    const int32_t* sorted;     // nodes ordered by Morton rank of their cell
+    int nslit;
+    const double* slits;
+};
+
+__device__ __forceinline__ void load_x(const SearchArgs& A, int64_t i, double* p) {
+    p[0] = A.x[i];
+    p[1] = A.x[A.n + i];
+    p[2] = A.x[2 * A.n + i];
+}
+
+__device__ __forceinline__ int64_t cell_coord(const SearchArgs& A, double v, int a) {
+    int64_t c = (int64_t)floor((v - A.g.lo[a]) / A.g.h);
+    if (c < 0) c = 0;
+    if (c >= A.g.nc[a]) c = A.g.nc[a] - 1;
+    return c;
+}
+
+__global__ void k_cell_count(SearchArgs A, int32_t* node_rank, int64_t* cnt) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    double p[3];
+    load_x(A, i, p);
+    const int64_t cx = cell_coord(A, p[0], 0), cy = cell_coord(A, p[1], 1), cz = cell_coord(A, p[2], 2);
+    const int32_t r = A.cell_rank[(cz * A.g.nc[1] + cy) * A.g.nc[0] + cx];
+    node_rank[i] = r;
+    atomicAdd((unsigned long long*)&cnt[r], 1ull);
+}
+
+__global__ void k_cell_scatter(SearchArgs A, const int32_t* node_rank, const int64_t* cstart, int64_t* fillc,
+                               int32_t* sorted) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const int32_t r = node_rank[i];
+    const int64_t pos = (int64_t)atomicAdd((unsigned long long*)&fillc[r], 1ull);
+    sorted[cstart[r] + pos] = (int32_t)i;
+}
+
+// One warp per node (taken in Morton order of the cells so that neighbouring
+// warps scan overlapping cells).  PASS 0 counts family and unbroken entries
+// and the minimum bond length; PASS 1 collects the family into shared
+// memory, orders it by id and writes both CSRs.
+template <int PASS>
+__global__ void k_search(SearchArgs A, int64_t* cnt_full, int64_t* cnt_act, unsigned long long* min_bits,
+                         unsigned long long* max_cnt, const int64_t* frow, int32_t* fcol, uint8_t* fbroken,
+                         const int64_t* arow, int32_t* acol, int cap) {
+    extern __shared__ int32_t sbuf[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (w >= A.n) return;
+    int32_t* buf = sbuf + (size_t)wib * cap;
+    uint8_t* brk = (uint8_t*)(sbuf + (size_t)(blockDim.x >> 5) * cap) + (size_t)wib * cap;
+    const int64_t i = A.sorted[w];
+    double pi[3];
+    load_x(A, i, pi);
+    const int64_t cx = cell_coord(A, pi[0], 0), cy = cell_coord(A, pi[1], 1), cz = cell_coord(A, pi[2], 2);
+    int64_t nfull = 0, nact = 0;
+    double mb = A.delta;
+    for (int64_t dz = -1; dz <= 1; ++dz) {
+        const int64_t qz = cz + dz;
+        if (qz < 0 || qz >= A.g.nc[2]) continue;
+        for (int64_t dy = -1; dy <= 1; ++dy) {
+            const int64_t qy = cy + dy;
+            if (qy < 0 || qy >= A.g.nc[1]) continue;
+            for (int64_t dxc = -1; dxc <= 1; ++dxc) {
+                const int64_t qx = cx + dxc;
+                if (qx < 0 || qx >= A.g.nc[0]) continue;
+                const int32_t r = A.cell_rank[(qz * A.g.nc[1] + qy) * A.g.nc[0] + qx];
+                const int64_t s0 = A.cstart[r], s1 = A.cstart[r + 1];
+                for (int64_t s = s0; s < s1; s += 32) {
+                    bool hit = false, br = false;
+                    int64_t j = -1;
+                    if (s + lane < s1) {
+                        j = A.sorted[s + lane];
+                        if (j != i) {
+                            double pj[3], dist;
+                            load_x(A, j, pj);
+                            const double* pa = (i < j) ? pi : pj;
+                            const double* pb = (i < j) ? pj : pi;
+                            hit = pair_bonded(pa, pb, A.dx, A.delta, A.tol, &dist);
+                            if (hit) {
+                                if (i < j) mb = dmin(mb, dist);
+                                for (int k = 0; k < A.nslit; ++k) br = br || slit_crosses(A.slits + 6 * k, pa, pb);
+                            }
+                        }
+                    }
+                    const unsigned hm = __ballot_sync(0xffffffffu, hit);
+                    const unsigned bm = __ballot_sync(0xffffffffu, hit && !br);
+                    if (PASS == 1 && hit) {
+                        const int slot = (int)nfull + __popc(hm & ((1u << lane) - 1u));
+                        if (slot < cap) {
+                            buf[slot] = (int32_t)j;
+                            brk[slot] = br ? 1 : 0;
+                        }
+                    }
+                    nfull += __popc(hm);
+                    nact += __popc(bm);
+                }
+            }
+        }
+    }
+    if (PASS == 0) {
+        for (int o = 16; o > 0; o >>= 1) mb = dmin(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        if (lane == 0) {
+            cnt_full[i] = nfull;
+            cnt_act[i] = nact;
+            atomicMin(min_bits, (unsigned long long)__double_as_longlong(mb));
+            atomicMax(max_cnt, (unsigned long long)nfull);
+        }
+        return;
+    }
+    __syncwarp();
+    const int nf = (int)(nfull < cap ? nfull : cap);
+    const int64_t fo = frow[i], ao = arow[i];
+    for (int e = lane; e < nf; e += 32) {
+        const int32_t v = buf[e];
+        int rk = 0, ra = 0;
+        for (int k = 0; k < nf; ++k) {
+            const int32_t o = buf[k];
+            if (o < v) {
+                ++rk;
+                ra += brk[k] ? 0 : 1;
+            }
+        }
+        fcol[fo + rk] = v;
+        fbroken[fo + rk] = brk[e];
+        if (!brk[e]) acol[ao + ra] = v;
+    }
+}
+
+}  // namespace
+
+int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int64_t ncell, int nslit,
+                const double* slits_dev, int64_t** frow_o, int32_t** fcol_o, uint8_t** fbroken_o, int64_t** arow_o,
+                int32_t** acol_o, int64_t* nh, int64_t* nb, double* min_bond, cudaStream_t s) {
+    const int64_t N = d.n;
+    SearchArgs A;
+    A.x = d.x;
+    A.n = N;
+    A.dx = d.dx;
+    A.delta = d.delta;
+    A.tol = 1.0e-4 * d.dx;
+    A.g = g;
+    A.cell_rank = cell_rank;
+    A.nslit = nslit;
+    A.slits = slits_dev;
+    int32_t *node_rank = nullptr, *sorted = nullptr;
+    int64_t *ccnt = nullptr, *cstart = nullptr, *fillc = nullptr, *cf = nullptr, *ca = nullptr;
+    int64_t *frow = nullptr, *arow = nullptr;
+    unsigned long long* scal = nullptr;
+    int32_t *fcol = nullptr, *acol = nullptr;
+    uint8_t* fbr = nullptr;
+    int rc = PD_OK;
+    auto cleanup = [&]() {
+        cudaFree(node_rank); cudaFree(sorted); cudaFree(ccnt); cudaFree(cstart); cudaFree(fillc);
+        cudaFree(cf); cudaFree(ca); cudaFree(scal);
+    };
+#define PD_S_TRY(expr)                                                        \
+    do {                                                                      \
+        cudaError_t _e = (expr);                                              \
+        if (_e != cudaSuccess) {                                              \
+            rc = fail_cuda(_e, #expr, __FILE__, __LINE__);                    \
+            cleanup(); cudaFree(frow); cudaFree(arow); cudaFree(fcol);        \
+            cudaFree(acol); cudaFree(fbr);                                    \
+            return rc;                                                        \
+        }                                                                     \
+    } while (0)
+    PD_S_TRY(cudaMalloc(&node_rank, sizeof(int32_t) * (N + 1)));
+    PD_S_TRY(cudaMalloc(&sorted, sizeof(int32_t) * (N + 1)));
+    PD_S_TRY(cudaMalloc(&ccnt, sizeof(int64_t) * (ncell + 1)));
+    PD_S_TRY(cudaMalloc(&cstart, sizeof(int64_t) * (ncell + 1)));
+    PD_S_TRY(cudaMalloc(&fillc, sizeof(int64_t) * (ncell + 1)));
+    PD_S_TRY(cudaMalloc(&cf, sizeof(int64_t) * (N + 1)));
+    PD_S_TRY(cudaMalloc(&ca, sizeof(int64_t) * (N + 1)));
+    PD_S_TRY(cudaMalloc(&frow, sizeof(int64_t) * (N + 1)));
+    PD_S_TRY(cudaMalloc(&arow, sizeof(int64_t) * (N + 1)));
+    PD_S_TRY(cudaMalloc(&scal, sizeof(unsigned long long) * 2));
+    PD_S_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int64_t) * (ncell + 1), s));
+    PD_S_TRY(cudaMemsetAsync(fillc, 0, sizeof(int64_t) * (ncell + 1), s));
+    unsigned long long init[2] = {(unsigned long long)__builtin_bit_cast(unsigned long long, d.delta), 0ull};
+    PD_S_TRY(cudaMemcpyAsync(scal, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int bs = 256;
+    if (N > 0) {
+        k_cell_count<<<blocks_for(N, bs), bs, 0, s>>>(A, node_rank, ccnt);
+        PD_S_TRY(cudaGetLastError());
+    }
+    if (exclusive_scan_i64(ccnt, cstart, ncell, s) != PD_OK) { cleanup(); return fail(PD_ERR_CUDA, "scan failed"); }
+    if (N > 0) {
+        k_cell_scatter<<<blocks_for(N, bs), bs, 0, s>>>(A, node_rank, cstart, fillc, sorted);
+        PD_S_TRY(cudaGetLastError());
+    }
+    A.cstart = cstart;
+    A.sorted = sorted;
+    const int wpb = 4;  // warps per block
+    if (N > 0) {
+        k_search<0><<<blocks_for(N * 32, 32 * wpb), 32 * wpb, 0, s>>>(A, cf, ca, scal, scal + 1, nullptr, nullptr,
+                                                                      nullptr, nullptr, nullptr, 0);
+        PD_S_TRY(cudaGetLastError());
+    }
+    unsigned long long hs[2];
+    PD_S_TRY(cudaMemcpyAsync(hs, scal, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    PD_S_TRY(cudaStreamSynchronize(s));
+    if (exclusive_scan_i64(cf, frow, N, s) != PD_OK || exclusive_scan_i64(ca, arow, N, s) != PD_OK) {
+        cleanup();
+        return fail(PD_ERR_CUDA, "scan failed");
+    }
+    int64_t tot[2] = {0, 0};
+    PD_S_TRY(cudaMemcpyAsync(&tot[0], frow + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    PD_S_TRY(cudaMemcpyAsync(&tot[1], arow + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    PD_S_TRY(cudaStreamSynchronize(s));
+    PD_S_TRY(cudaMalloc(&fcol, sizeof(int32_t) * (tot[0] + 1)));
+    PD_S_TRY(cudaMalloc(&fbr, sizeof(uint8_t) * (tot[0] + 1)));
+    PD_S_TRY(cudaMalloc(&acol, sizeof(int32_t) * (tot[1] + 1)));
+    const int cap = (int)hs[1] + 1;
+    size_t sh = (size_t)wpb * cap * (sizeof(int32_t) + sizeof(uint8_t));
+    if (sh > 200 * 1024) {
+        cleanup();
+        cudaFree(frow); cudaFree(arow); cudaFree(fcol); cudaFree(acol); cudaFree(fbr);
+        return fail(PD_ERR_CAPACITY, "family larger than the search kernel's shared buffer");
+    }
+    if (sh > 48 * 1024)
+        PD_S_TRY(cudaFuncSetAttribute(k_search<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    if (N > 0) {
+        k_search<1><<<blocks_for(N * 32, 32 * wpb), 32 * wpb, sh, s>>>(A, nullptr, nullptr, nullptr, nullptr, frow,
+                                                                       fcol, fbr, arow, acol, cap);
+        PD_S_TRY(cudaGetLastError());
+    }
+    PD_S_TRY(cudaStreamSynchronize(s));
+#undef PD_S_TRY
+    cleanup();
+    *frow_o = frow;
+    *fcol_o = fcol;
+    *fbroken_o = fbr;
+    *arow_o = arow;
+    *acol_o = acol;
+    *nh = tot[0];
+    *nb = tot[0] - tot[1];
+    *min_bond = __builtin_bit_cast(double, hs[0]);
+    return PD_OK;
+}
+
+}  // namespace pd

@@ -1,0 +1,534 @@
+// FP32-compensated force and gather kernels, the static operator, scans and
+// reductions.
+//
+// FP32 form.  The stretch of a bond is tiny (1e-6..1e-3) next to its length,
+// so (|xi+eta| - |xi|) / |xi| loses every digit in FP32.  These kernels never
+// form that difference: with d = |xi+eta|^2 - |xi|^2 = eta.(2 xi + eta),
+//     s = d / (r (p + r)),   f = c beta s (xi+eta) / p,
+// all terms of which are accurate to FP32 rounding relative to the strain
+// itself.  eta is likewise assembled from differences taken in FP64 and only
+// then rounded: eta = (float)(us_j - u_i) + ugrel_j,g with ugrel = ug - us_j,
+// the Gauss-point displacement relative to its own node, which the gather
+// produces directly.  Per-bond forces are summed in FP32 and the family sum of
+// each node is Kahan-compensated; the state update stays FP64.
+#include <cstdio>
+
+#include "pd_internal.cuh"
+
+namespace pd {
+
+namespace {
+
+inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+__device__ __forceinline__ double time_factor(const BcDev& b, double t) {
+    if (b.type == PD_BC_VELOC) return (t <= b.end_time) ? 1.0 : 0.0;
+    if (b.load_type == 1.0) return (t <= b.end_time) ? t / b.end_time : 1.0;
+    return 1.0;
+}
+
+// ------------------------------------------------------------ FP32 force
+
+template <bool CCI, bool SFAC>
+__global__ void __launch_bounds__(128) k_force_f32c(Dev d, double dts) {
+    __shared__ float sh[kMaxPoints][6];  // hg[3], W, A, B
+    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) {
+        const GaussConst& G = d.gc[g];
+        sh[g][0] = G.hgf[0];
+        sh[g][1] = G.hgf[1];
+        sh[g][2] = G.hgf[2];
+        sh[g][3] = G.Wf;
+        sh[g][4] = G.A;
+        sh[g][5] = G.B;
+    }
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const MatDev Mi = d.mats[d.mat[i]];
+    const double rho = Mi.density;
+    const bool bci = d.bc[i] >= 0;
+    const double* src = bci ? d.U : d.us;
+    const double ui0 = src[i], ui1 = src[N + i], ui2 = src[2 * N + i];
+    const double xi0 = d.x[i], xi1 = d.x[N + i], xi2 = d.x[2 * N + i];
+    const double bEi = d.bdry[i];
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;  // Kahan sums
+    const int64_t pb = d.arow[i], pe = d.arow[i + 1];
+    const float delta = (float)d.delta;
+    const float dxf = (float)d.dx;
+    for (int64_t p = pb; p < pe; ++p) {
+        const int64_t j = d.acol[p];
+        const MatDev& Mj = d.mats[d.mat[j]];
+        const float ecrit = (float)((Mj.ecrit < Mi.ecrit) ? Mj.ecrit : Mi.ecrit);
+        double c = (Mj.spring < Mi.spring) ? Mj.spring : Mi.spring;
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const float coef = (float)(0.5 * (bEi + d.bdry[j]) * c);
+        const float dx0 = (float)(d.x[j] - xi0), dx1 = (float)(d.x[N + j] - xi1), dx2 = (float)(d.x[2 * N + j] - xi2);
+        float F0 = 0.f, F1 = 0.f, F2 = 0.f;
+        if (CCI) {
+            const double* sj = (d.bc[j] >= 0) ? d.U : d.us;
+            const float e0 = (float)(sj[j] - ui0), e1 = (float)(sj[N + j] - ui1), e2 = (float)(sj[2 * N + j] - ui2);
+            const float y0 = dx0 + e0, y1 = dx1 + e1, y2 = dx2 + e2;
+            const float r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+            const float dd = e0 * (dx0 + y0) + e1 * (dx1 + y1) + e2 * (dx2 + y2);
+            const float p2 = r2 + dd;
+            const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
+            const float r = r2 * rinv, pl = p2 * pinv;
+            const float s = dd * rinv * __frcp_rn(pl + r);
+            float beta;
+            if (d.cci_mdf) beta = __saturatef((delta + 0.5f * dxf - r) / dxf);
+            else beta = (r > delta) ? 0.f : __saturatef((delta + 0.5f * dxf - r) / dxf);
+            const float fm = (dd > 0.f && s > ecrit) ? 0.f : coef * (float)d.vol_cci * beta * s * pinv;
+            F0 = fm * y0;
+            F1 = fm * y1;
+            F2 = fm * y2;
+        } else {
+            const float du0 = (float)(d.us[j] - ui0), du1 = (float)(d.us[N + j] - ui1), du2 = (float)(d.us[2 * N + j] - ui2);
+            const float* ur = d.ugrel + j;
+#pragma unroll 4
+            for (int g = 0; g < d.npt; ++g) {
+                const float x0 = dx0 + sh[g][0], x1 = dx1 + sh[g][1], x2 = dx2 + sh[g][2];
+                const float e0 = du0 + ur[(3 * g) * N], e1 = du1 + ur[(3 * g + 1) * N], e2 = du2 + ur[(3 * g + 2) * N];
+                const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
+                const float r2 = x0 * x0 + x1 * x1 + x2 * x2;
+                const float dd = e0 * (x0 + y0) + e1 * (x1 + y1) + e2 * (x2 + y2);
+                const float p2 = r2 + dd;
+                const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
+                const float r = r2 * rinv, pl = p2 * pinv;
+                const float s = dd * rinv * __frcp_rn(pl + r);
+                const float beta = __saturatef((sh[g][4] - r) * sh[g][5]);
+                const float fm = (dd > 0.f && s > ecrit) ? 0.f : sh[g][3] * beta * s * pinv;
+                F0 = fmaf(fm, y0, F0);
+                F1 = fmaf(fm, y1, F1);
+                F2 = fmaf(fm, y2, F2);
+            }
+            F0 *= coef;
+            F1 *= coef;
+            F2 *= coef;
+        }
+        // Kahan accumulation of the family sum
+        float yk = F0 - c0, tk = s0 + yk;
+        c0 = (tk - s0) - yk;
+        s0 = tk;
+        yk = F1 - c1; tk = s1 + yk; c1 = (tk - s1) - yk; s1 = tk;
+        yk = F2 - c2; tk = s2 + yk; c2 = (tk - s2) - yk; s2 = tk;
+    }
+    const double nb = (double)(pe - pb);
+    const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
+    d.vbuf[i] += ((double)s0 - (double)c0 + nb * b0) * dts / rho;
+    d.vbuf[N + i] += ((double)s1 - (double)c1 + nb * b1) * dts / rho;
+    d.vbuf[2 * N + i] += ((double)s2 - (double)c2 + nb * b2) * dts / rho;
+}
+
+// ----------------------------------------------------------- FP32 gather
+
+// One thread per (node, point).  Writes ugrel = ug - us(node) in FP32 and, for
+// nodes with a boundary condition, keeps the FP64 ug of the reference rules.
+__global__ void k_gather_f32c(Dev d, const double* __restrict__ us) {
+    const int64_t N = d.n;
+    const double t = *d.tdev;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= N * d.npt) return;
+    const int64_t i = tid / d.npt;
+    const int g = (int)(tid - i * d.npt);
+    const double u0 = us[i], u1 = us[N + i], u2 = us[2 * N + i];
+    float* out = d.ugrel + (int64_t)(3 * g) * N + i;
+    const int b = d.bc[i];
+    if (b >= 0) {
+        double* ug = d.ug + (int64_t)(3 * g) * N + i;
+        const BcDev& B = d.bcs[b];
+        const double fac = time_factor(B, t);
+        const GaussConst& G = d.gc[g];
+        const double q0 = G.hg[0] + d.x[i], q1 = G.hg[1] + d.x[N + i], q2 = G.hg[2] + d.x[2 * N + i];
+        for (int a = 0; a < 3; ++a) {
+            if (B.dir[a] != 1) continue;
+            if (B.type == PD_BC_DISPL) ug[a * N] = B.val[a] * fac;
+            else if (B.type == PD_BC_DISPLGRAD)
+                ug[a * N] = (B.val[3 * a] * q0 + B.val[3 * a + 1] * q1 + B.val[3 * a + 2] * q2) * fac;
+        }
+        out[0] = (float)(ug[0] - u0);
+        out[N] = (float)(ug[N] - u1);
+        out[2 * N] = (float)(ug[2 * N] - u2);
+        return;
+    }
+    if (d.mls) {
+        const int64_t cb0 = d.cbptr[i], nc = d.cbptr[i + 1] - cb0;
+        const float* cf = d.coeff32 + cb0 * d.npt + g;
+        const int32_t* cb = d.cbidx + cb0;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int64_t k = 0; k < nc; ++k) {
+            const int64_t m = cb[k];
+            const double c = (double)cf[k * d.npt];
+            a0 = fma(c, us[m] - u0, a0);
+            a1 = fma(c, us[N + m] - u1, a1);
+            a2 = fma(c, us[2 * N + m] - u2, a2);
+        }
+        const double S = (double)d.csum[i * d.npt + g];
+        out[0] = (float)fma(S, u0, a0);
+        out[N] = (float)fma(S, u1, a1);
+        out[2 * N] = (float)fma(S, u2, a2);
+    } else {
+        out[0] = 0.f;
+        out[N] = 0.f;
+        out[2 * N] = 0.f;
+    }
+}
+
+// -------------------------------------------------------- static operator
+
+__device__ __forceinline__ void prescribed(const Dev& d, int64_t i, double t, bool* pre, double* val) {
+    pre[0] = pre[1] = pre[2] = false;
+    val[0] = val[1] = val[2] = 0.0;
+    const int b = d.bc[i];
+    if (b < 0) return;
+    const BcDev& B = d.bcs[b];
+    if (B.type != PD_BC_DISPL && B.type != PD_BC_VELOC) return;
+    for (int a = 0; a < 3; ++a)
+        if (B.dir[a] == 1) {
+            pre[a] = true;
+            val[a] = (B.type == PD_BC_DISPL) ? B.val[a] : B.val[a] * t;
+        }
+}
+
+// y = K x on free rows (prescribed columns masked), y = x on prescribed rows.
+// One thread per node over its unbroken family; pdSolve.cpp:195-527.
+template <bool SFAC>
+__global__ void k_static_apply_f64(Dev d, double t, const double* __restrict__ x, double* __restrict__ y) {
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bool pi[3];
+    double pv[3];
+    prescribed(d, i, t, pi, pv);
+    const double X0 = d.x[i], X1 = d.x[N + i], X2 = d.x[2 * N + i];
+    const double xi0 = pi[0] ? 0.0 : x[i], xi1 = pi[1] ? 0.0 : x[N + i], xi2 = pi[2] ? 0.0 : x[2 * N + i];
+    const double ci = d.mats[d.mat[i]].spring;
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+        const int64_t j = d.acol[p];
+        bool pj[3];
+        double qv[3];
+        prescribed(d, j, t, pj, qv);
+        const double e0 = d.x[j] - X0, e1 = d.x[N + j] - X1, e2 = d.x[2 * N + j] - X2;
+        const double r2 = e0 * e0 + e1 * e1 + e2 * e2;
+        const double r = sqrt(r2);
+        const double cj = d.mats[d.mat[j]].spring;
+        double c = (cj < ci) ? cj : ci;
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const double w = c * d.vol / (r2 * r);
+        const double d0 = xi0 - (pj[0] ? 0.0 : x[j]);
+        const double d1 = xi1 - (pj[1] ? 0.0 : x[N + j]);
+        const double d2 = xi2 - (pj[2] ? 0.0 : x[2 * N + j]);
+        const double pr = w * (e0 * d0 + e1 * d1 + e2 * d2);
+        a0 += pr * e0;
+        a1 += pr * e1;
+        a2 += pr * e2;
+    }
+    y[i] = pi[0] ? x[i] : a0;
+    y[N + i] = pi[1] ? x[N + i] : a1;
+    y[2 * N + i] = pi[2] ? x[2 * N + i] : a2;
+}
+
+template <bool SFAC>
+__global__ void k_static_apply_f32(Dev d, double t, const float* __restrict__ x, float* __restrict__ y) {
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bool pi[3];
+    double pv[3];
+    prescribed(d, i, t, pi, pv);
+    const double X0 = d.x[i], X1 = d.x[N + i], X2 = d.x[2 * N + i];
+    const float xi0 = pi[0] ? 0.f : x[i], xi1 = pi[1] ? 0.f : x[N + i], xi2 = pi[2] ? 0.f : x[2 * N + i];
+    const double ci = d.mats[d.mat[i]].spring;
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    const float cv = (float)(ci * d.vol);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+        const int64_t j = d.acol[p];
+        bool pj[3];
+        double qv[3];
+        prescribed(d, j, t, pj, qv);
+        const float e0 = (float)(d.x[j] - X0), e1 = (float)(d.x[N + j] - X1), e2 = (float)(d.x[2 * N + j] - X2);
+        const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
+        const float rinv = rsqrtf(r2);
+        float c = cv;
+        const double cj = d.mats[d.mat[j]].spring;
+        if (cj < ci) c = (float)(cj * d.vol);
+        if (SFAC) c = c * (float)(0.5 * (sfi + d.sfac[j]));
+        const float w = c * rinv * rinv * rinv;
+        const float d0 = xi0 - (pj[0] ? 0.f : x[j]);
+        const float d1 = xi1 - (pj[1] ? 0.f : x[N + j]);
+        const float d2 = xi2 - (pj[2] ? 0.f : x[2 * N + j]);
+        const float pr = w * (e0 * d0 + e1 * d1 + e2 * d2);
+        a0 = fmaf(pr, e0, a0);
+        a1 = fmaf(pr, e1, a1);
+        a2 = fmaf(pr, e2, a2);
+    }
+    y[i] = pi[0] ? x[i] : a0;
+    y[N + i] = pi[1] ? x[N + i] : a1;
+    y[2 * N + i] = pi[2] ? x[2 * N + i] : a2;
+}
+
+// b = prescribed values on prescribed rows; on free rows the moved prescribed
+// columns (pdSolve.cpp:296-363 sign pattern) plus the traction load.
+template <bool SFAC>
+__global__ void k_static_rhs(Dev d, double t, double* __restrict__ out) {
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bool pi[3];
+    double pv[3];
+    prescribed(d, i, t, pi, pv);
+    const double X0 = d.x[i], X1 = d.x[N + i], X2 = d.x[2 * N + i];
+    const double ci = d.mats[d.mat[i]].spring;
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    const double m0 = pi[0] ? pv[0] : 0.0, m1 = pi[1] ? pv[1] : 0.0, m2 = pi[2] ? pv[2] : 0.0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+        const int64_t j = d.acol[p];
+        bool pj[3];
+        double qv[3];
+        prescribed(d, j, t, pj, qv);
+        const double e0 = d.x[j] - X0, e1 = d.x[N + j] - X1, e2 = d.x[2 * N + j] - X2;
+        const double r2 = e0 * e0 + e1 * e1 + e2 * e2;
+        const double r = sqrt(r2);
+        const double cj = d.mats[d.mat[j]].spring;
+        double c = (cj < ci) ? cj : ci;
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const double w = c * d.vol / (r2 * r);
+        // -K_ii(prescribed cols) ubar_i + K_ij-part: +c xi xi^T ubar_j
+        const double d0 = (pj[0] ? qv[0] : 0.0) - m0;
+        const double d1 = (pj[1] ? qv[1] : 0.0) - m1;
+        const double d2 = (pj[2] ? qv[2] : 0.0) - m2;
+        const double pr = w * (e0 * d0 + e1 * d1 + e2 * d2);
+        a0 += pr * e0;
+        a1 += pr * e1;
+        a2 += pr * e2;
+    }
+    double acc[3] = {a0, a1, a2};
+    const int b = d.bc[i];
+    for (int a = 0; a < 3; ++a) {
+        if (pi[a]) {
+            out[a * N + i] = pv[a];
+            continue;
+        }
+        double load = acc[a];
+        if (b >= 0) {
+            const BcDev& B = d.bcs[b];
+            if (B.type == PD_BC_TRACTION && B.dir[a] == 1) load += B.val[a] * time_factor(B, t) / d.dx;
+        }
+        out[a * N + i] = load;
+    }
+}
+
+// ------------------------------------------------------------------ scan
+
+constexpr int kScanBlock = 1024;
+
+__global__ void k_scan_block(const int64_t* __restrict__ in, int64_t* __restrict__ out, int64_t n,
+                             int64_t* __restrict__ bsum) {
+    __shared__ int64_t wsum[32];
+    const int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+    int64_t v = (i < n) ? in[i] : 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t s = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    const int64_t incl = x + (w > 0 ? wsum[w - 1] : 0);
+    if (i < n) out[i] = incl - v;  // exclusive
+    if (threadIdx.x == kScanBlock - 1) bsum[blockIdx.x] = incl;
+}
+
+__global__ void k_scan_add(int64_t* out, int64_t n, const int64_t* __restrict__ boff) {
+    const int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+    if (i < n) out[i] += boff[blockIdx.x];
+}
+
+__global__ void k_scan_total(const int64_t* in, int64_t* out, int64_t n) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) out[n] = (n > 0) ? out[n - 1] + in[n - 1] : 0;
+}
+
+}  // namespace
+
+int exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s) {
+    if (n <= 0) {
+        int64_t z = 0;
+        if (cudaMemcpyAsync(out, &z, sizeof(z), cudaMemcpyHostToDevice, s) != cudaSuccess) return PD_ERR_CUDA;
+        return cudaStreamSynchronize(s) == cudaSuccess ? PD_OK : PD_ERR_CUDA;
+    }
+    const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    int64_t *bsum = nullptr, *boff = nullptr;
+    if (cudaMalloc(&bsum, sizeof(int64_t) * (nb + 1)) != cudaSuccess) return PD_ERR_OOM;
+    if (cudaMalloc(&boff, sizeof(int64_t) * (nb + 1)) != cudaSuccess) {
+        cudaFree(bsum);
+        return PD_ERR_OOM;
+    }
+    k_scan_block<<<(unsigned)nb, kScanBlock, 0, s>>>(in, out, n, bsum);
+    int rc = PD_OK;
+    if (nb > 1) {
+        rc = exclusive_scan_i64(bsum, boff, nb, s);
+        if (rc == PD_OK) k_scan_add<<<(unsigned)nb, kScanBlock, 0, s>>>(out, n, boff);
+    }
+    if (rc == PD_OK) k_scan_total<<<1, 32, 0, s>>>(in, out, n);
+    if (rc == PD_OK && cudaGetLastError() != cudaSuccess) rc = PD_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) rc = PD_ERR_CUDA;
+    cudaFree(bsum);
+    cudaFree(boff);
+    return rc;
+}
+
+void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
+    if (d.n == 0) return;
+    const unsigned nb = blocks_for(d.n, 128);
+    if (d.cci) {
+        if (d.sfac) k_force_f32c<true, true><<<nb, 128, 0, s>>>(d, dts);
+        else k_force_f32c<true, false><<<nb, 128, 0, s>>>(d, dts);
+    } else {
+        if (d.sfac) k_force_f32c<false, true><<<nb, 128, 0, s>>>(d, dts);
+        else k_force_f32c<false, false><<<nb, 128, 0, s>>>(d, dts);
+    }
+}
+
+void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
+    if (d.cci || d.n == 0) return;
+    k_gather_f32c<<<blocks_for(d.n * d.npt, 256), 256, 0, s>>>(d, us);
+}
+
+void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y, cudaStream_t s) {
+    if (d.n == 0) return;
+    if (d.sfac) k_static_apply_f64<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+    else k_static_apply_f64<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+}
+
+void launch_static_apply_f32(const Dev& d, double t, const float* x, float* y, cudaStream_t s) {
+    if (d.n == 0) return;
+    if (d.sfac) k_static_apply_f32<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+    else k_static_apply_f32<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+}
+
+void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s) {
+    if (d.n == 0) return;
+    if (d.sfac) k_static_rhs<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, b);
+    else k_static_rhs<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, b);
+}
+
+// -------------------------------------------------------------- CG pieces
+
+namespace {
+
+template <typename T>
+__global__ void k_dot_partial(const T* __restrict__ a, const T* __restrict__ b, int64_t n, double* __restrict__ part) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += (double)a[i] * (double)b[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_dot_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nb; k += 32) acc += part[k];
+    sh[threadIdx.x] = acc;
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < 32; ++k) s += sh[k];
+        *out = s;
+    }
+}
+
+template <typename T>
+__global__ void k_cg_x(T* x, T* r, const T* p, const T* q, int64_t n, const double* scal) {
+    const double alpha = scal[CG_RR] / scal[CG_PQ];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] = (T)((double)x[i] + alpha * (double)p[i]);
+        r[i] = (T)((double)r[i] - alpha * (double)q[i]);
+    }
+}
+
+template <typename T>
+__global__ void k_cg_p(const T* r, T* p, int64_t n, const double* scal) {
+    const double beta = scal[CG_RRN] / scal[CG_RR];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = (T)((double)r[i] + beta * (double)p[i]);
+}
+
+__global__ void k_cg_swap(double* scal) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) scal[CG_RR] = scal[CG_RRN];
+}
+
+__global__ void k_sub(const double* a, const double* b, double* o, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        o[i] = a[i] - b[i];
+}
+
+__global__ void k_to_f32(const double* a, float* o, double scale, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        o[i] = (float)(a[i] * scale);
+}
+
+__global__ void k_add_f32(double* x, const float* dd, double scale, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += scale * (double)dd[i];
+}
+
+constexpr int kStreamBlocks = 148 * 8;
+
+}  // namespace
+
+void launch_dot_f64(const double* a, const double* b, int64_t n, double* part, double* out, cudaStream_t s) {
+    k_dot_partial<double><<<kDotBlocks, 256, 0, s>>>(a, b, n, part);
+    k_dot_final<<<1, 32, 0, s>>>(part, kDotBlocks, out);
+}
+void launch_dot_f32(const float* a, const float* b, int64_t n, double* part, double* out, cudaStream_t s) {
+    k_dot_partial<float><<<kDotBlocks, 256, 0, s>>>(a, b, n, part);
+    k_dot_final<<<1, 32, 0, s>>>(part, kDotBlocks, out);
+}
+void launch_cg_update_x_f64(double* x, double* r, const double* p, const double* q, int64_t n, const double* scal,
+                            cudaStream_t s) {
+    k_cg_x<double><<<kStreamBlocks, 256, 0, s>>>(x, r, p, q, n, scal);
+}
+void launch_cg_update_p_f64(const double* r, double* p, int64_t n, const double* scal, cudaStream_t s) {
+    k_cg_p<double><<<kStreamBlocks, 256, 0, s>>>(r, p, n, scal);
+}
+void launch_cg_update_x_f32(float* x, float* r, const float* p, const float* q, int64_t n, const double* scal,
+                            cudaStream_t s) {
+    k_cg_x<float><<<kStreamBlocks, 256, 0, s>>>(x, r, p, q, n, scal);
+}
+void launch_cg_update_p_f32(const float* r, float* p, int64_t n, const double* scal, cudaStream_t s) {
+    k_cg_p<float><<<kStreamBlocks, 256, 0, s>>>(r, p, n, scal);
+}
+void launch_cg_swap(double* scal, cudaStream_t s) { k_cg_swap<<<1, 32, 0, s>>>(scal); }
+void launch_sub_f64(const double* a, const double* b, double* o, int64_t n, cudaStream_t s) {
+    k_sub<<<kStreamBlocks, 256, 0, s>>>(a, b, o, n);
+}
+void launch_f64_to_f32(const double* a, float* o, double scale, int64_t n, cudaStream_t s) {
+    k_to_f32<<<kStreamBlocks, 256, 0, s>>>(a, o, scale, n);
+}
+void launch_add_f32_to_f64(double* x, const float* dd, double scale, int64_t n, cudaStream_t s) {
+    k_add_f32<<<kStreamBlocks, 256, 0, s>>>(x, dd, scale, n);
+}
+
+}  // namespace pd

@@ -1,0 +1,144 @@
+// Internal declarations shared by the translation units of libpdmtel_b200.
+//
+// Device layout (HBM): every per-node vector is structure-of-arrays [3][N]
+// (component-major) so that a warp of consecutive nodes reads 256 B per
+// component; Gauss-point data are [npt*3][N]; the family is CSR with int64
+// row offsets and int32 columns in ascending id order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pdmtel_b200.h"
+
+namespace pd {
+
+constexpr int kMaxPoints = 512;  // 8x8x8 Gauss rule
+
+struct MatDev {
+    double spring, density, ecrit, grav[3];
+};
+
+struct BcDev {
+    int type;
+    int dir[3];
+    double val[9];
+    double end_time;
+    double load_type;
+};
+
+// Per-Gauss-point constants computed on the host in the reference's order:
+// hg = (0.5*dx)*abscissa, W = ((vol8*w1)*w2)*w3, dxe = (effW*dx)/2,
+// pw3 = pow(0.5*effW, 3) (pdDataManager.cpp:1932-1955, pdDataManager2.cpp:1313-1342).
+struct GaussConst {
+    double hg[3];
+    double W;
+    double dxe;
+    double pw3;
+    float hgf[3];
+    float Wf;
+    float A, B;  // beta = saturate((A - r) * B), FP32 form
+};
+
+// Everything a kernel needs, passed by value.
+struct Dev {
+    int64_t n;
+    int npt;
+    int cci, cci_mdf, mls, energy;
+    double dx, delta, damping, vol, vol_cci;  // vol = pow(dx,3.0), vol_cci = (dx*dx)*dx
+    const double* x;          // [3][N]
+    const int32_t* mat;       // [N]
+    const int32_t* bc;        // [N]
+    const MatDev* mats;
+    int nmat;
+    const BcDev* bcs;
+    int nbc;
+    const double* bdry;       // [N]
+    const double* sfac;       // [N] or nullptr
+    const GaussConst* gc;     // [npt]
+    // family (full) and active (unbroken) CSR
+    const int64_t* frow;
+    const int32_t* fcol;
+    const uint8_t* fbroken;
+    const int64_t* arow;
+    const int32_t* acol;
+    // MLS, coefficient layout [node][contributor][point]
+    const int64_t* cbptr;
+    const int32_t* cbidx;
+    const double* coeff;
+    const float* coeff32;
+    const float* csum;        // [N][npt] partition-of-unity defect sum(c)-1
+    // state [3][N]
+    double* U;
+    double* V;
+    double* vbuf;
+    double* u1;
+    double* us;
+    double* k1;
+    double* k2;
+    double* k32;
+    double* ug;               // [npt*3][N]
+    float* ugrel;             // [npt*3][N] FP32 form: ug - us(node)
+    double* eed;              // [N]
+    double* red;              // reduction scratch
+    double* tdev;             // current time (device scalar; advanced on the device)
+};
+
+// kernel launchers (pd_exact.cu: compiled without FMA contraction)
+void launch_force_f64(const Dev& d, double dts, cudaStream_t s);
+void launch_gather_f64(const Dev& d, const double* us, cudaStream_t s);
+void launch_epilogue(const Dev& d, int stage, double dts, double dt, cudaStream_t s);
+void launch_advance_time(double* t, double dt, cudaStream_t s);
+void launch_energy_reduce(const Dev& d, cudaStream_t s);
+void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s);
+void launch_to_aos(const double* soa, double* aos, int64_t n, int comps, cudaStream_t s);
+void launch_fill(double* p, double v, int64_t n, cudaStream_t s);
+
+// bond search (pd_exact.cu)
+struct SearchGrid {
+    double lo[3];
+    double h;
+    int64_t nc[3];
+};
+int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int64_t ncell, int nslit,
+                const double* slits_dev, int64_t** frow, int32_t** fcol, uint8_t** fbroken, int64_t** arow,
+                int32_t** acol, int64_t* nh, int64_t* nb, double* min_bond, cudaStream_t s);
+
+// FP32 compensated form (pd_fast.cu)
+void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);
+void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s);
+
+// CG helpers (pd_fast.cu): slots of the device scalar array
+enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_NSLOT = 8 };
+void launch_dot_f64(const double* a, const double* b, int64_t n, double* part, double* out, cudaStream_t s);
+void launch_dot_f32(const float* a, const float* b, int64_t n, double* part, double* out, cudaStream_t s);
+void launch_cg_update_x_f64(double* x, double* r, const double* p, const double* q, int64_t n, const double* scal, cudaStream_t s);
+void launch_cg_update_p_f64(const double* r, double* p, int64_t n, const double* scal, cudaStream_t s);
+void launch_cg_update_x_f32(float* x, float* r, const float* p, const float* q, int64_t n, const double* scal, cudaStream_t s);
+void launch_cg_update_p_f32(const float* r, float* p, int64_t n, const double* scal, cudaStream_t s);
+void launch_cg_swap(double* scal, cudaStream_t s);
+void launch_sub_f64(const double* a, const double* b, double* out, int64_t n, cudaStream_t s);
+void launch_f64_to_f32(const double* a, float* out, double scale, int64_t n, cudaStream_t s);
+void launch_add_f32_to_f64(double* x, const float* d, double scale, int64_t n, cudaStream_t s);
+constexpr int kDotBlocks = 296;
+
+// static operator (pd_fast.cu)
+void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
+void launch_static_apply_f32(const Dev& d, double t, const float* x, float* y, cudaStream_t s);
+void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s);
+
+// scans and reductions (pd_fast.cu)
+int exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);  // out has n+1 entries
+
+}  // namespace pd
+
+#define PD_CUDA_TRY(expr)                                                        \
+    do {                                                                         \
+        cudaError_t _e = (expr);                                                 \
+        if (_e != cudaSuccess) return pd::fail_cuda(_e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+namespace pd {
+int fail_cuda(cudaError_t e, const char* what, const char* file, int line);
+int fail(int code, const char* msg);
+}  // namespace pd

@@ -1,0 +1,211 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the
+reference's golden vectors (bit for bit in FP64) and against the oracle."""
+import numpy as np
+import pytest
+
+import pdmtel_b200 as P
+from conftest import deck_dir, kat, load_golden, CASES
+from golden_model import model_from_golden, params
+from pdmtel_b200 import decks as D
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_model(name_or_dir, init=True):
+    dm = P.pdDataManager(deck_dir(name_or_dir) if name_or_dir in CASES else name_or_dir)
+    if init:
+        P.pdSolve.InitialProblem(dm)
+    return dm
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_device_bond_search_is_the_reference_family(name):
+    g = load_golden(name)
+    dm = gpu_model(name)
+    rp, col, br = dm.family()
+    assert np.array_equal(rp, g["fam_ptr"])
+    assert np.array_equal(col, g["fam_col"])
+    assert np.array_equal(br.astype(np.int32), g["broken"])
+    assert dm.info().min_bond_length == g["min_bond"][0]
+    assert np.array_equal(dm.bdry_eff(), g["bdry_eff"])
+    if dm.info().mls:
+        assert np.array_equal(dm.mls()[2], g["coeff"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_force_stage_bit_exact(name):
+    g = load_golden(name)
+    t, dts = g["force_args"]
+    dm = gpu_model(name)
+    ctx = dm.context()
+    ctx.set_state(g["u_test"], g["v_test"])
+    ctx.init_dynamic()
+    ctx.gather(t, g["u_test"])
+    if len(g["ug"]):
+        assert np.array_equal(ctx.get_gauss_displ(), g["ug"])
+    k = ctx.force_stage(dts, t, g["u_test"])
+    assert np.array_equal(k, g["k"])
+    assert np.array_equal(ctx.get_vbuf(), g["vbuf"])
+    U, _ = ctx.get_state()
+    assert np.array_equal(U, g["U_after"])
+    assert np.array_equal(ctx.get_energy_density(), g["eed"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rk4_trajectory_bit_exact(name):
+    g = load_golden(name)
+    dm = gpu_model(name)
+    ctx = dm.context()
+    dt = g["dt"][0]
+    for it, t in enumerate(g["traj_times"], start=1):
+        ke, ee = ctx.rk4_step(dt, t)
+        # energies are sums over nodes: a tree sum on the device
+        assert ke == pytest.approx(g["traj_ke"][it - 1], rel=1e-12, abs=1e-300)
+        assert ee == pytest.approx(g["traj_ee"][it - 1], rel=1e-12, abs=1e-300)
+        if f"traj_U_{it}" in g:
+            U, V = ctx.get_state()
+            assert np.array_equal(U, g[f"traj_U_{it}"])
+            assert np.array_equal(V, g[f"traj_V_{it}"])
+            if len(g[f"traj_ug_{it}"]):
+                assert np.array_equal(ctx.get_gauss_displ(), g[f"traj_ug_{it}"])
+
+
+def test_graph_replay_equals_single_steps():
+    g = load_golden("fgi_slit")
+    dt = g["dt"][0]
+    a = gpu_model("fgi_slit").context()
+    b = gpu_model("fgi_slit").context()
+    t = 0.0
+    for _ in range(5):
+        t += dt
+        a.rk4_step(dt, t)
+    b.rk4_steps(dt, 0.0, 5)
+    b.sync()
+    Ua, Va = a.get_state()
+    Ub, Vb = b.get_state()
+    assert np.array_equal(Ua, Ub) and np.array_equal(Va, Vb)
+
+
+def test_host_buffer_steps_equal_device_steps():
+    g = load_golden("fgi_velo")
+    dt = g["dt"][0]
+    a = gpu_model("fgi_velo").context()
+    a.rk4_steps(dt, 0.0, 3)
+    a.sync()
+    b = gpu_model("fgi_velo").context()
+    n3 = 3 * b.n
+    U0, V0 = np.zeros(n3), np.zeros(n3)
+    U1, V1 = np.zeros(n3), np.zeros(n3)
+    b.rk4_steps_host(dt, 0.0, 3, U0, V0, U1, V1)
+    Ua, Va = a.get_state()
+    assert np.array_equal(Ua, U1) and np.array_equal(Va, V1)
+
+
+def test_sample_like_deck_known_answers():
+    """The reference sample deck's parameters: 1,655,072 bonds and the
+    energies of the first two steps (CCI, displacement-gradient layers)."""
+    K = kat()["sample_like"]
+    dm = gpu_model(deck_dir("sample_like"))
+    assert dm.info().num_halves == 2 * K["bonds"]
+    assert dm.CalcStableTimeStep() == K["dt"]
+    ctx = dm.context()
+    t = 0.0
+    for it in range(2):
+        t += K["dt"]
+        ke, ee = ctx.rk4_step(K["dt"], t)
+        assert ke == pytest.approx(K["ke"][it], rel=1e-12)
+        assert ee == pytest.approx(K["ee"][it], rel=1e-12)
+    U, V = ctx.get_state()
+    assert np.abs(U).sum() == pytest.approx(K["u2_sum_abs"], rel=1e-12)
+    assert np.abs(V).sum() == pytest.approx(K["v2_sum_abs"], rel=1e-12)
+
+
+def test_bond_counts_of_larger_lattices(tmp_path):
+    for dims, bonds in (((20, 10, 10), 168392), ((64, 64, 8), 3196784)):
+        d = D.config_bar(dims=dims, traction_as_veloc=0.01)
+        d.write(str(tmp_path / f"{dims[0]}"))
+        dm = P.pdDataManager(str(tmp_path / f"{dims[0]}"))
+        dm.InitNode()
+        dm.InitBond()
+        assert dm.info().num_halves == 2 * bonds
+
+
+def test_traction_bar_matches_oracle(tmp_path):
+    """The traction load (a project rule; the reference only parses it) on
+    the full 20x10x10 bar: device and oracle agree bit for bit."""
+    d = D.config_bar(dims=(20, 10, 10), traction=1e6, bdry_eff=1)
+    d.write(str(tmp_path))
+    dm = gpu_model(str(tmp_path))
+    x, mat, bc = dm.nodes()
+    rp, col, br = dm.family()
+    cp, ci, co = dm.mls()
+    I = dm.info()
+    import oracle_lib as O
+    xg, gw = O.gauss_points(x, I.grid_spacing, 2)
+    spring = 18 * (72e9 / (3.0 * (1.0 - 2.0 * 0.25))) / (np.arccos(-1.0) * I.horizon ** 4.0)
+    m = O.Model(n=I.num_nodes, x=x, dx=I.grid_spacing, delta=I.horizon, mls=1, npt=8, xg=xg, gw=gw,
+                fam_ptr=rp, fam_col=col, broken=br, cb_ptr=cp, cb_idx=ci, coeff=co, bdry_eff=dm.bdry_eff(),
+                mat=mat, mat_spring=np.array([spring]), mat_ecrit=np.array([1e20]), mat_density=np.array([2440.0]),
+                mat_ymod=np.array([72e9]), bc=bc, bc_type=[1, 4], bc_dir=[1, 1, 1, 1, 0, 0],
+                bc_val=[0] * 9 + [1e6] + [0] * 8, bc_end=[1.0, 1.0], bc_load=[2.0, 2.0])
+    ctx = dm.context()
+    t = 0.0
+    for _ in range(3):
+        t += 1e-8
+        m.rk4_step(1e-8, t)
+        ctx.rk4_step(1e-8, t)
+    U, V = ctx.get_state()
+    # the oracle's spring constant is formed in numpy here, so allow for one
+    # ulp of difference in it
+    assert np.linalg.norm(U - m.U) <= 1e-12 * np.linalg.norm(m.U)
+    assert np.linalg.norm(V - m.V) <= 1e-12 * np.linalg.norm(m.V)
+    assert np.abs(U).max() > 0
+
+
+@pytest.mark.parametrize("name", ["fgi_velo", "fgi_slit", "fgi3_ramp", "cci_mdf"])
+def test_fp32c_within_1e6_of_fp64(name):
+    g = load_golden(name)
+    dt = g["dt"][0]
+    a = gpu_model(name).context()
+    b = gpu_model(name)
+    b.SetPrecision(P.PREC_FP32C)
+    b = b.context()
+    a.rk4_steps(dt, 0.0, 50)
+    b.rk4_steps(dt, 0.0, 50)
+    Ua, Va = a.get_state()
+    Ub, Vb = b.get_state()
+    eu = np.linalg.norm(Ub - Ua) / np.linalg.norm(Ua)
+    ev = np.linalg.norm(Vb - Va) / np.linalg.norm(Va)
+    assert eu <= 1e-6, eu
+    assert ev <= 1e-5, ev
+
+
+def test_static_operator_matches_oracle(tmp_path):
+    d = D.config_bar(dims=(10, 6, 6), traction=1e6, bdry_eff=0)
+    d.write(str(tmp_path))
+    dm = gpu_model(str(tmp_path))
+    x, mat, bc = dm.nodes()
+    rp, col, br = dm.family()
+    I = dm.info()
+    import oracle_lib as O
+    spring = 18 * (72e9 / 1.5) / (np.arccos(-1.0) * I.horizon ** 4.0)
+    m = O.Model(n=I.num_nodes, x=x, dx=I.grid_spacing, delta=I.horizon, mls=0, npt=1, fam_ptr=rp, fam_col=col,
+                broken=br, mat=mat, mat_spring=np.array([spring]), mat_ecrit=np.array([1e20]),
+                mat_density=np.array([2440.0]), mat_ymod=np.array([72e9]), bc=bc, bc_type=[1, 4],
+                bc_dir=[1, 1, 1, 1, 0, 0], bc_val=[0] * 9 + [1e6] + [0] * 8, bc_end=[1.0, 1.0], bc_load=[2.0, 2.0])
+    ctx = dm.context()
+    rng = np.random.default_rng(3)
+    xv = rng.standard_normal(3 * I.num_nodes) * 1e-7
+    y_gpu = ctx.static_matvec(1e-8, xv)
+    y_or = m.static_apply(1e-8, xv)
+    assert np.linalg.norm(y_gpu - y_or) <= 1e-12 * np.linalg.norm(y_or)
+    b_gpu = ctx.static_rhs(1e-8)
+    b_or = m.static_rhs(1e-8)
+    assert np.linalg.norm(b_gpu - b_or) <= 1e-12 * np.linalg.norm(b_or)
+    u64, it64, r64 = ctx.static_solve(1e-8, P.PREC_FP64, 1e-10)
+    assert r64 <= 1e-10
+    res = np.linalg.norm(m.static_apply(1e-8, u64) - b_or) / np.linalg.norm(b_or)
+    assert res <= 2e-10
+    u32, it32, r32 = ctx.static_solve(1e-8, P.PREC_FP32C, 1e-10)
+    assert r32 <= 1e-10
+    assert np.linalg.norm(u32 - u64) <= 1e-8 * np.linalg.norm(u64)
