@@ -31,6 +31,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
 
 CUDA_UNITS = {
     "pd_exact.cu": ["-fmad=false"],
+    "pd_f32c.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "pd_fast.cu": [],
     "pd_capi.cu": [],
 }

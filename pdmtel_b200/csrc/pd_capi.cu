@@ -44,6 +44,8 @@ struct pd_ctx {
     std::vector<double> coords;  // [N][3] host copy
     std::vector<double> slits;
     double* dslits = nullptr;   // [nslit][6] on the device
+    std::vector<pd::GaussConst> gch;            // Gauss constants (host copy)
+    std::vector<double> bdry_host, sfac_host;   // per-node factors (host copies)
     bool have_family = false, have_mls = false;
     // owned device buffers
     std::vector<void*> owned;
@@ -120,6 +122,69 @@ int set_time(pd_ctx* c, double t) {
     PD_CUDA_TRY(cudaMemcpyAsync(c->d.tdev, c->hscalar, sizeof(double), cudaMemcpyHostToDevice, c->stream));
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return PD_OK;
+}
+
+// Static per-node block of the FP32 form: coordinates split hi/lo, boundary
+// factor, spring factor.
+int upload_static_f32(pd_ctx* c) {
+    const int64_t N = c->n;
+    std::vector<float> h((size_t)N * 8);
+    for (int64_t i = 0; i < N; ++i) {
+        float* o = &h[8 * i];
+        for (int a = 0; a < 3; ++a) {
+            const double x = c->coords[3 * i + a];
+            o[a] = (float)x;
+            o[3 + a] = (float)(x - (double)o[a]);
+        }
+        o[6] = (float)c->bdry_host[i];
+        o[7] = c->sfac_host.empty() ? 1.0f : (float)c->sfac_host[i];
+    }
+    return upload(c, (void*)c->d.sblk, h.data(), sizeof(float) * h.size());
+}
+
+// Work order of the node-parallel kernels: nodes grouped into 8x4x4 tiles of
+// lattice positions (x fastest inside a tile), tiles in x, y, z order, so
+// that a 128-thread block covers one compact tile.
+std::vector<int32_t> tiled_order(const std::vector<double>& x, int64_t N, double dx) {
+    std::vector<int32_t> ord(N);
+    if (N == 0) return ord;
+    double lo[3] = {x[0], x[1], x[2]};
+    for (int64_t i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], x[3 * i + a]);
+    std::vector<std::pair<uint64_t, int32_t>> key(N);
+    for (int64_t i = 0; i < N; ++i) {
+        int64_t l[3];
+        for (int a = 0; a < 3; ++a) l[a] = (int64_t)std::llround((x[3 * i + a] - lo[a]) / dx);
+        const uint64_t tx = l[0] >> 3, ty = l[1] >> 2, tz = l[2] >> 2;
+        const uint64_t tile = (tz << 42) | (ty << 21) | tx;
+        const uint64_t local = ((uint64_t)(l[2] & 3) << 5) | ((uint64_t)(l[1] & 3) << 3) | (uint64_t)(l[0] & 7);
+        key[i] = {(tile << 7) | local, (int32_t)i};
+    }
+    std::sort(key.begin(), key.end());
+    for (int64_t k = 0; k < N; ++k) ord[k] = key[k].second;
+    return ord;
+}
+
+// Packed lattice positions x | y << 11 | z << 22 when every node lies within
+// 1e-6 spacings of the cubic lattice through the lowest corner (the lattices
+// InitNode generates, pdDataManager.cpp:846-907); false otherwise.
+bool lattice_positions(const std::vector<double>& x, int64_t N, double dx, std::vector<int32_t>& out) {
+    if (N == 0) return false;
+    double lo[3] = {x[0], x[1], x[2]};
+    for (int64_t i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], x[3 * i + a]);
+    const int64_t lim[3] = {2048, 2048, 1024};
+    out.assign(N, 0);
+    for (int64_t i = 0; i < N; ++i) {
+        int64_t l[3];
+        for (int a = 0; a < 3; ++a) {
+            l[a] = (int64_t)std::llround((x[3 * i + a] - lo[a]) / dx);
+            if (l[a] < 0 || l[a] >= lim[a]) return false;
+            if (std::fabs(x[3 * i + a] - (lo[a] + (double)l[a] * dx)) > 1e-6 * dx) return false;
+        }
+        out[i] = (int32_t)(l[0] | (l[1] << 11) | (l[2] << 22));
+    }
+    return true;
 }
 
 uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
@@ -264,11 +329,14 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     if ((rc = dalloc(c, &gc, c->npt)) != PD_OK) return bail(rc);
     if ((rc = dalloc(c, &bdry, N)) != PD_OK) return bail(rc);
     double *U, *V, *vbuf, *u1, *us, *k1, *k2, *k32, *ug, *eed, *red, *tdev;
-    float* ugrel;
+    float *nblk, *sblk;
+    int32_t* order;
+    d.bs = ((3 * c->npt + 6) + 3) / 4 * 4;
     if ((rc = dalloc(c, &U, n3)) || (rc = dalloc(c, &V, n3)) || (rc = dalloc(c, &vbuf, n3)) ||
         (rc = dalloc(c, &u1, n3)) || (rc = dalloc(c, &us, n3)) || (rc = dalloc(c, &k1, n3)) ||
         (rc = dalloc(c, &k2, n3)) || (rc = dalloc(c, &k32, n3)) || (rc = dalloc(c, &ug, n3 * c->npt)) ||
-        (rc = dalloc(c, &ugrel, n3 * c->npt)) || (rc = dalloc(c, &eed, N)) ||
+        (rc = dalloc(c, &nblk, (size_t)N * d.bs)) || (rc = dalloc(c, &sblk, (size_t)N * 8)) ||
+        (rc = dalloc(c, &order, N)) || (rc = dalloc(c, &eed, N)) ||
         (rc = dalloc(c, &red, 2 * N + 4 + 2 * 160)) || (rc = dalloc(c, &tdev, 1)) ||
         (rc = dalloc(c, &c->dotpart, pd::kDotBlocks + 8)) || (rc = dalloc(c, &c->scal, pd::CG_NSLOT)))
         return bail(rc);
@@ -337,6 +405,32 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
         if ((rc = dalloc(c, &sf, N)) != PD_OK || (rc = upload(c, sf, P->spring_factor, sizeof(double) * N)) != PD_OK)
             return bail(rc);
         d.sfac = sf;
+        c->sfac_host.assign(P->spring_factor, P->spring_factor + N);
+    }
+    // FP32-form constants: one material -> kernel constants; a failure test
+    // only when some critical stretch is within reach
+    d.multimat = P->num_materials > 1;
+    d.c0 = (float)P->materials[0].spring;
+    d.e0 = (float)P->materials[0].ecrit;
+    d.hasfail = 0;
+    for (int k = 0; k < P->num_materials; ++k) d.hasfail |= !(P->materials[k].ecrit >= 1e10);
+    c->gch = hg;
+    d.gc_host = c->gch.data();
+    c->bdry_host.assign(N, 1.0);
+    d.nblk = nblk;
+    d.sblk = sblk;
+    d.order = order;
+    if ((rc = upload_static_f32(c)) != PD_OK) return bail(rc);
+    {
+        std::vector<int32_t> ord = tiled_order(c->coords, N, d.dx);
+        if ((rc = upload(c, order, ord.data(), sizeof(int32_t) * N)) != PD_OK) return bail(rc);
+        std::vector<int32_t> lat;
+        if (lattice_positions(c->coords, N, d.dx, lat)) {
+            int32_t* dl = nullptr;
+            if ((rc = dalloc(c, &dl, N)) != PD_OK || (rc = upload(c, dl, lat.data(), sizeof(int32_t) * N)) != PD_OK)
+                return bail(rc);
+            d.lat = dl;
+        }
     }
     d.x = x;
     d.mat = mat;
@@ -356,7 +450,6 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     d.k2 = k2;
     d.k32 = k32;
     d.ug = ug;
-    d.ugrel = ugrel;
     d.eed = eed;
     d.red = red;
     d.tdev = tdev;
@@ -366,7 +459,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     cudaMemsetAsync(u1, 0, sizeof(double) * n3, c->stream);
     cudaMemsetAsync(us, 0, sizeof(double) * n3, c->stream);
     cudaMemsetAsync(ug, 0, sizeof(double) * n3 * c->npt, c->stream);
-    cudaMemsetAsync(ugrel, 0, sizeof(float) * n3 * c->npt, c->stream);
+    cudaMemsetAsync(nblk, 0, sizeof(float) * N * d.bs, c->stream);
     cudaMemsetAsync(eed, 0, sizeof(double) * N, c->stream);
     cudaMemsetAsync(tdev, 0, sizeof(double), c->stream);
     cudaError_t e = cudaStreamSynchronize(c->stream);
@@ -514,7 +607,12 @@ int pd_set_family(pd_ctx* c, const int64_t* row_ptr, const int32_t* col, const u
 
 int pd_set_bdry_eff(pd_ctx* c, const double* bE) {
     if (!c || !bE) return fail(PD_ERR_ARG, "pd_set_bdry_eff: null argument");
-    return upload(c, (void*)c->d.bdry, bE, sizeof(double) * c->n);
+    PD_TRY(upload(c, (void*)c->d.bdry, bE, sizeof(double) * c->n));
+    c->bdry_host.assign(bE, bE + c->n);
+    c->d.bdry_on = 0;
+    for (int64_t i = 0; i < c->n; ++i) c->d.bdry_on |= (bE[i] != 1.0);
+    c->generation++;
+    return upload_static_f32(c);
 }
 
 int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const double* coeff) {
@@ -758,7 +856,7 @@ int pd_reset_state(pd_ctx* c) {
     cudaStream_t s = c->stream;
     for (double* p : {c->d.U, c->d.V, c->d.vbuf, c->d.u1, c->d.us}) PD_CUDA_TRY(cudaMemsetAsync(p, 0, b3, s));
     PD_CUDA_TRY(cudaMemsetAsync(c->d.ug, 0, b3 * c->npt, s));
-    PD_CUDA_TRY(cudaMemsetAsync(c->d.ugrel, 0, sizeof(float) * 3 * c->n * c->npt, s));
+    PD_CUDA_TRY(cudaMemsetAsync(c->d.nblk, 0, sizeof(float) * c->n * c->d.bs, s));
     PD_CUDA_TRY(cudaMemsetAsync(c->d.eed, 0, sizeof(double) * c->n, s));
     PD_CUDA_TRY(cudaStreamSynchronize(s));
     return PD_OK;

@@ -51,8 +51,9 @@ __global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
     for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
     __syncthreads();
     const int64_t N = d.n;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= N) return;
+    const int64_t i = d.order[tid];
     const MatDev Mi = d.mats[d.mat[i]];
     const double rho = Mi.density;
     const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
@@ -146,8 +147,8 @@ __global__ void k_gather_f64(Dev d, const double* __restrict__ us) {
     const double t = *d.tdev;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (tid >= N * d.npt) return;
-    const int64_t i = tid / d.npt;
-    const int g = (int)(tid - i * d.npt);
+    const int64_t i = d.order[tid / d.npt];
+    const int g = (int)(tid % d.npt);
     double* ug = d.ug + (int64_t)(3 * g) * N + i;
     const int b = d.bc[i];
     if (b >= 0) {

@@ -1,0 +1,494 @@
+// FP32-compensated form of the bond force and the MLS gather.
+//
+// Compiled with -ftz=true -prec-div=false -prec-sqrt=false: reciprocals and
+// reciprocal square roots are single MUFU operations.
+//
+// Numerics.  The stretch of a bond is tiny (1e-6..1e-3) next to its length,
+// so (|xi+eta| - |xi|) / |xi| loses every digit in FP32.  The kernel never
+// forms that difference: with d = |xi+eta|^2 - |xi|^2 = eta.(2 xi + eta),
+//     s = d / (r (p + r)),   f = c beta s (xi+eta) / p,
+// every term is accurate to FP32 rounding relative to the strain itself.
+// eta is assembled from differences that are exact or nearly so:
+//     eta = (us_j - u_i) + (ug_j,g - us_j)
+// where the second term is produced by the gather directly, and the first is
+// (hi_j - hi_i) + (lo_j - lo_i) from FP32 hi/lo splits of the FP64 values
+// (hi = fl32(u), lo = fl32(u - hi)); hi_j - hi_i is exact whenever the two
+// are within a factor of two (Sterbenz), which is the case for neighbours
+// unless both are tiny.  Coordinates are split the same way.  Per-bond forces
+// are summed in FP32 over the Gauss points, the family sum of each node is
+// Kahan-compensated, and the state update stays FP64.
+#include <climits>
+
+#include "pd_internal.cuh"
+
+namespace pd {
+
+namespace {
+
+inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+__device__ __forceinline__ double time_factor(const BcDev& b, double t) {
+    if (b.type == PD_BC_VELOC) return (t <= b.end_time) ? 1.0 : 0.0;
+    if (b.load_type == 1.0) return (t <= b.end_time) ? t / b.end_time : 1.0;
+    return 1.0;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+struct PointF {
+    float hx, hy, hz, W, A, B;  // offset of the point from its node, weight*vol/8, beta = sat((A - r) B)
+};
+
+template <int NPT>
+struct PointPack {
+    PointF p[NPT > 0 ? NPT : 1];
+};
+
+// Four Gauss points q..q+3 of cell j on one bond (without the pair
+// coefficient), given xi_ij (dx), us_j - u_i (du) and the Gauss-point
+// displacements of j relative to us_j (u4: x[4], y[4], z[4]).
+template <bool HASFAIL>
+__device__ __forceinline__ void bond4(const PointPack<8>& G, int q, const float* u4, const float* dx,
+                                      const float* du, float ecrit, float* F) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const PointF& P = G.p[q + k];
+        const float x0 = dx[0] + P.hx, x1 = dx[1] + P.hy, x2 = dx[2] + P.hz;
+        const float e0 = du[0] + u4[k], e1 = du[1] + u4[4 + k], e2 = du[2] + u4[8 + k];
+        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
+        const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
+        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
+        const float p2 = r2 + dd;
+        const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
+        const float r = r2 * rinv;
+        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
+        const float beta = __saturatef((P.A - r) * P.B);
+        float fm = P.W * beta * s * pinv;
+        if (HASFAIL && dd > 0.f && s > ecrit) fm = 0.f;
+        F[0] = fmaf(fm, y0, F[0]);
+        F[1] = fmaf(fm, y1, F[1]);
+        F[2] = fmaf(fm, y2, F[2]);
+    }
+}
+
+struct Own {
+    float uh[3], ul[3];  // displacement of the node, FP32 hi/lo
+    float ph[3], pl[3];  // position hi/lo (off the lattice path)
+    int lat;             // packed lattice position
+    float be, sf, c, e;
+    int mat;
+    float s[3], k[3];    // Kahan sum of the family force
+};
+
+__device__ __forceinline__ void kahan_add(Own& o, float F0, float F1, float F2) {
+    float y = F0 - o.k[0], t = o.s[0] + y;
+    o.k[0] = (t - o.s[0]) - y;
+    o.s[0] = t;
+    y = F1 - o.k[1]; t = o.s[1] + y; o.k[1] = (t - o.s[1]) - y; o.s[1] = t;
+    y = F2 - o.k[2]; t = o.s[2] + y; o.k[2] = (t - o.s[2]) - y; o.s[2] = t;
+}
+
+template <bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
+__device__ __forceinline__ void load_own(const Dev& d, int64_t i, Own& o) {
+    const int64_t N = d.n;
+    const double* src = d.bc[i] >= 0 ? d.U : d.us;
+    for (int a = 0; a < 3; ++a) {
+        const double u = src[a * N + i];
+        o.uh[a] = (float)u;
+        o.ul[a] = (float)(u - (double)o.uh[a]);
+        o.s[a] = o.k[a] = 0.f;
+    }
+    const float* sb = d.sblk + 8 * i;
+    if (LAT) {
+        o.lat = d.lat[i];
+    } else {
+        for (int a = 0; a < 3; ++a) {
+            o.ph[a] = sb[a];
+            o.pl[a] = sb[3 + a];
+        }
+    }
+    o.be = BDRY ? sb[6] : 1.f;
+    o.sf = SFAC ? sb[7] : 1.f;
+    o.mat = MULTIMAT ? d.mat[i] : 0;
+    o.c = MULTIMAT ? (float)d.mats[o.mat].spring : d.c0;
+    o.e = MULTIMAT ? (float)d.mats[o.mat].ecrit : d.e0;
+}
+
+__device__ __forceinline__ void store_own(const Dev& d, int64_t i, const Own& o, int64_t nbonds, double dts) {
+    const int64_t N = d.n;
+    const MatDev& M = d.mats[o.mat];
+    const double rho = M.density;
+    for (int a = 0; a < 3; ++a)
+        d.vbuf[a * N + i] += ((double)o.s[a] - (double)o.k[a] + (double)nbonds * (M.grav[a] * rho)) * dts / rho;
+}
+
+// FGI with 2x2x2 Gauss points, two nodes per thread.  The work order pairs
+// x-adjacent nodes; the thread walks the merge of their two ascending family
+// lists and loads every neighbour's block once for both bonds, which cuts
+// the L1 traffic per evaluation (the bound of this kernel) by the overlap of
+// the two families.  pdDataManager.cpp:1917-1962 in FP32 form.
+template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
+__global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> G, double dts) {
+    const int64_t N = d.n;
+    const int64_t t2 = 2 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+    if (t2 >= N) return;
+    const int64_t ia = d.order[t2];
+    const int64_t ib = (t2 + 1 < N) ? d.order[t2 + 1] : -1;
+    Own A, B;
+    load_own<LAT, BDRY, SFAC, MULTIMAT>(d, ia, A);
+    if (ib >= 0) load_own<LAT, BDRY, SFAC, MULTIMAT>(d, ib, B);
+    int64_t pa = d.arow[ia], ea = d.arow[ia + 1];
+    int64_t pb = 0, eb = 0;
+    if (ib >= 0) {
+        pb = d.arow[ib];
+        eb = d.arow[ib + 1];
+    }
+    const int64_t nba = ea - pa, nbb = eb - pb;
+    const float h = (float)d.dx;
+    for (;;) {
+        const int ja = pa < ea ? d.acol[pa] : INT_MAX;
+        const int jb = pb < eb ? d.acol[pb] : INT_MAX;
+        const int j = min(ja, jb);
+        if (j == INT_MAX) break;
+        const float* bj = d.nblk + (int64_t)j * 32;
+        const float4 us0 = ld4(bj + 24), us1 = ld4(bj + 28);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
+        float pj[6];
+        int lj = 0;
+        if (LAT) {
+            lj = d.lat[j];
+        } else {
+            const float4 s0 = ld4(d.sblk + 8 * (int64_t)j), s1 = ld4(d.sblk + 8 * (int64_t)j + 4);
+            pj[0] = s0.x; pj[1] = s0.y; pj[2] = s0.z; pj[3] = s0.w; pj[4] = s1.x; pj[5] = s1.y;
+        }
+        float bej = 1.f, sfj = 1.f;
+        if (BDRY || SFAC) {
+            const float2 v = __ldg(reinterpret_cast<const float2*>(d.sblk + 8 * (int64_t)j + 6));
+            bej = v.x;
+            sfj = v.y;
+        }
+        float cj = 0.f, ej = 0.f;
+        if (MULTIMAT) {
+            const int mj = d.mat[j];
+            cj = (float)d.mats[mj].spring;
+            ej = (float)d.mats[mj].ecrit;
+        }
+        const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
+        const bool has[2] = {ja == j, jb == j};
+        // per-bond terms of both sides
+        float dx[2][3], du[2][3], coef[2], ecrit[2];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const Own& O = side == 0 ? A : B;
+            if (LAT) {
+                dx[side][0] = (float)((lj & 2047) - (O.lat & 2047)) * h;
+                dx[side][1] = (float)(((lj >> 11) & 2047) - ((O.lat >> 11) & 2047)) * h;
+                dx[side][2] = (float)((lj >> 22) - (O.lat >> 22)) * h;  // packed values are non-negative
+            } else {
+                for (int a = 0; a < 3; ++a) dx[side][a] = (pj[a] - O.ph[a]) + (pj[3 + a] - O.pl[a]);
+            }
+            for (int a = 0; a < 3; ++a) du[side][a] = (ujh[a] - O.uh[a]) + (ujl[a] - O.ul[a]);
+            float c = O.c;
+            ecrit[side] = O.e;
+            if (MULTIMAT) {
+                c = fminf(c, cj);
+                ecrit[side] = fminf(ecrit[side], ej);
+            }
+            if (BDRY) c *= 0.5f * (O.be + bej);
+            if (SFAC) c *= 0.5f * (O.sf + sfj);
+            coef[side] = c;
+        }
+        float F[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        // the eight Gauss points of cell j in two halves of four, each half
+        // applied to both bonds
+#pragma unroll
+        for (int q = 0; q < 8; q += 4) {
+            const float4 vx = ld4(bj + q), vy = ld4(bj + 8 + q), vz = ld4(bj + 16 + q);
+            const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
+#pragma unroll
+            for (int side = 0; side < 2; ++side)
+                if (has[side])
+                    bond4<HASFAIL>(G, q, u4, dx[side], du[side], ecrit[side], F[side]);
+        }
+        if (has[0]) {
+            kahan_add(A, F[0][0] * coef[0], F[0][1] * coef[0], F[0][2] * coef[0]);
+            ++pa;
+        }
+        if (has[1]) {
+            kahan_add(B, F[1][0] * coef[1], F[1][1] * coef[1], F[1][2] * coef[1]);
+            ++pb;
+        }
+    }
+    store_own(d, ia, A, nba, dts);
+    if (ib >= 0) store_own(d, ib, B, nbb, dts);
+}
+
+// The same for any number of Gauss points (constants from shared memory).
+template <bool SFAC>
+__global__ void __launch_bounds__(128) k_force_f32c_any(Dev d, double dts) {
+    __shared__ PointF sp[kMaxPoints];
+    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) {
+        const GaussConst& Q = d.gc[g];
+        sp[g] = PointF{Q.hgf[0], Q.hgf[1], Q.hgf[2], Q.Wf, Q.A, Q.B};
+    }
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= N) return;
+    const int64_t i = d.order[tid];
+    const int npt = d.npt, bs = d.bs;
+    const double* src = d.bc[i] >= 0 ? d.U : d.us;
+    const double u0 = src[i], u1 = src[N + i], u2 = src[2 * N + i];
+    const float uh0 = (float)u0, uh1 = (float)u1, uh2 = (float)u2;
+    const float ul0 = (float)(u0 - (double)uh0), ul1 = (float)(u1 - (double)uh1), ul2 = (float)(u2 - (double)uh2);
+    const float* si = d.sblk + 8 * i;
+    const int mi = d.mat[i];
+    const MatDev& Mi = d.mats[mi];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, k0 = 0.f, k1 = 0.f, k2 = 0.f;
+    const int64_t pb = d.arow[i], pe = d.arow[i + 1];
+    for (int64_t p = pb; p < pe; ++p) {
+        const int64_t j = d.acol[p];
+        const float* bj = d.nblk + j * bs;
+        const float* sj = d.sblk + 8 * j;
+        const float dx0 = (sj[0] - si[0]) + (sj[3] - si[3]);
+        const float dx1 = (sj[1] - si[1]) + (sj[4] - si[4]);
+        const float dx2 = (sj[2] - si[2]) + (sj[5] - si[5]);
+        const float* uj = bj + 3 * npt;
+        const float du0 = (uj[0] - uh0) + (uj[3] - ul0);
+        const float du1 = (uj[1] - uh1) + (uj[4] - ul1);
+        const float du2 = (uj[2] - uh2) + (uj[5] - ul2);
+        const MatDev& Mj = d.mats[d.mat[j]];
+        const float ecrit = (float)fmin(Mi.ecrit, Mj.ecrit);
+        float coef = 0.5f * (si[6] + sj[6]) * (float)fmin(Mi.spring, Mj.spring);
+        if (SFAC) coef *= 0.5f * (si[7] + sj[7]);
+        float F0 = 0.f, F1 = 0.f, F2 = 0.f;
+        for (int g = 0; g < npt; ++g) {
+            const PointF& P = sp[g];
+            const float x0 = dx0 + P.hx, x1 = dx1 + P.hy, x2 = dx2 + P.hz;
+            const float e0 = du0 + bj[g], e1 = du1 + bj[npt + g], e2 = du2 + bj[2 * npt + g];
+            const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
+            const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
+            const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
+            const float p2 = r2 + dd;
+            const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
+            const float r = r2 * rinv;
+            const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
+            const float beta = __saturatef((P.A - r) * P.B);
+            float fm = P.W * beta * s * pinv;
+            if (dd > 0.f && s > ecrit) fm = 0.f;
+            F0 = fmaf(fm, y0, F0);
+            F1 = fmaf(fm, y1, F1);
+            F2 = fmaf(fm, y2, F2);
+        }
+        F0 *= coef; F1 *= coef; F2 *= coef;
+        float y = F0 - k0, t = s0 + y; k0 = (t - s0) - y; s0 = t;
+        y = F1 - k1; t = s1 + y; k1 = (t - s1) - y; s1 = t;
+        y = F2 - k2; t = s2 + y; k2 = (t - s2) - y; s2 = t;
+    }
+    const double rho = Mi.density, nb = (double)(pe - pb);
+    d.vbuf[i] += ((double)s0 - (double)k0 + nb * (Mi.grav[0] * rho)) * dts / rho;
+    d.vbuf[N + i] += ((double)s1 - (double)k1 + nb * (Mi.grav[1] * rho)) * dts / rho;
+    d.vbuf[2 * N + i] += ((double)s2 - (double)k2 + nb * (Mi.grav[2] * rho)) * dts / rho;
+}
+
+// CCI in FP32 form: one point at node j, pdDataManager.cpp:1818-1866.  The
+// effective displacement of every node (U for nodes with a boundary
+// condition, us otherwise) is packed as hi/lo by k_pack_cci.
+template <bool SFAC>
+__global__ void __launch_bounds__(128) k_force_f32c_cci(Dev d, double dts) {
+    const int64_t N = d.n;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= N) return;
+    const int64_t i = d.order[tid];
+    const float* si = d.sblk + 8 * i;
+    const float* ui = d.nblk + i * d.bs;
+    const MatDev& Mi = d.mats[d.mat[i]];
+    const float dl = (float)d.delta, h = (float)d.dx;
+    const float outer = d.cci_mdf ? dl + 0.5f * h : dl;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, k0 = 0.f, k1 = 0.f, k2 = 0.f;
+    const int64_t pb = d.arow[i], pe = d.arow[i + 1];
+    for (int64_t p = pb; p < pe; ++p) {
+        const int64_t j = d.acol[p];
+        const float* sj = d.sblk + 8 * j;
+        const float* uj = d.nblk + j * d.bs;
+        const float x0 = (sj[0] - si[0]) + (sj[3] - si[3]);
+        const float x1 = (sj[1] - si[1]) + (sj[4] - si[4]);
+        const float x2 = (sj[2] - si[2]) + (sj[5] - si[5]);
+        const float e0 = (uj[0] - ui[0]) + (uj[3] - ui[3]);
+        const float e1 = (uj[1] - ui[1]) + (uj[4] - ui[4]);
+        const float e2 = (uj[2] - ui[2]) + (uj[5] - ui[5]);
+        const MatDev& Mj = d.mats[d.mat[j]];
+        const float ecrit = (float)fmin(Mi.ecrit, Mj.ecrit);
+        float coef = 0.5f * (si[6] + sj[6]) * (float)fmin(Mi.spring, Mj.spring) * (float)d.vol_cci;
+        if (SFAC) coef *= 0.5f * (si[7] + sj[7]);
+        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
+        const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
+        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
+        const float p2 = r2 + dd;
+        const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
+        const float r = r2 * rinv;
+        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
+        const float beta = (r > outer) ? 0.f : __saturatef((dl + 0.5f * h - r) / h);
+        float fm = coef * beta * s * pinv;
+        if (dd > 0.f && s > ecrit) fm = 0.f;
+        const float F0 = fm * y0, F1 = fm * y1, F2 = fm * y2;
+        float y = F0 - k0, t = s0 + y; k0 = (t - s0) - y; s0 = t;
+        y = F1 - k1; t = s1 + y; k1 = (t - s1) - y; s1 = t;
+        y = F2 - k2; t = s2 + y; k2 = (t - s2) - y; s2 = t;
+    }
+    const double rho = Mi.density, nb = (double)(pe - pb);
+    d.vbuf[i] += ((double)s0 - (double)k0 + nb * (Mi.grav[0] * rho)) * dts / rho;
+    d.vbuf[N + i] += ((double)s1 - (double)k1 + nb * (Mi.grav[1] * rho)) * dts / rho;
+    d.vbuf[2 * N + i] += ((double)s2 - (double)k2 + nb * (Mi.grav[2] * rho)) * dts / rho;
+}
+
+__global__ void k_pack_cci(Dev d) {
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double* src = d.bc[i] >= 0 ? d.U : d.us;
+    float* o = d.nblk + i * d.bs;
+    for (int a = 0; a < 3; ++a) {
+        const double u = src[a * N + i];
+        const float hi = (float)u;
+        o[a] = hi;
+        o[3 + a] = (float)(u - (double)hi);
+    }
+}
+
+// ----------------------------------------------------------------- gather
+
+// One thread per (node, group of up to four Gauss points): the Gauss-point
+// displacement relative to the node, sum_k c_k (us_k - us_i) + (sum_k c_k - 1)
+// us_i, accumulated in FP64 from FP32 coefficients (the MLS coefficients
+// satisfy the partition of unity only to the accuracy the reference's
+// ill-conditioned moment matrices allow, hence the second term).  Nodes with a
+// boundary condition keep the reference's rules on the FP64 Gauss-point
+// displacement (pdDataManager.cpp:2604-2703) and store its difference.
+__global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __restrict__ us) {
+    const int64_t N = d.n;
+    const int npt = d.npt, ngrp = (npt + 3) / 4;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= N * ngrp) return;
+    const int64_t i = d.order[tid / ngrp];
+    const int grp = (int)(tid % ngrp);
+    const int g0 = 4 * grp, ng = min(4, npt - g0);
+    const double t = *d.tdev;
+    const double u0 = us[i], u1 = us[N + i], u2 = us[2 * N + i];
+    float* o = d.nblk + i * d.bs;
+    if (grp == 0) {
+        const float h0 = (float)u0, h1 = (float)u1, h2 = (float)u2;
+        o[3 * npt + 0] = h0;
+        o[3 * npt + 1] = h1;
+        o[3 * npt + 2] = h2;
+        o[3 * npt + 3] = (float)(u0 - (double)h0);
+        o[3 * npt + 4] = (float)(u1 - (double)h1);
+        o[3 * npt + 5] = (float)(u2 - (double)h2);
+    }
+    const int b = d.bc[i];
+    if (b >= 0) {
+        const BcDev& B = d.bcs[b];
+        const double fac = time_factor(B, t);
+        for (int q = 0; q < ng; ++q) {
+            const int g = g0 + q;
+            double* ug = d.ug + (int64_t)(3 * g) * N + i;
+            const GaussConst& G = d.gc[g];
+            const double q0 = G.hg[0] + d.x[i], q1 = G.hg[1] + d.x[N + i], q2 = G.hg[2] + d.x[2 * N + i];
+            for (int a = 0; a < 3; ++a) {
+                if (B.dir[a] != 1) continue;
+                if (B.type == PD_BC_DISPL) ug[a * N] = B.val[a] * fac;
+                else if (B.type == PD_BC_DISPLGRAD)
+                    ug[a * N] = (B.val[3 * a] * q0 + B.val[3 * a + 1] * q1 + B.val[3 * a + 2] * q2) * fac;
+            }
+            o[g] = (float)(ug[0] - u0);
+            o[npt + g] = (float)(ug[N] - u1);
+            o[2 * npt + g] = (float)(ug[2 * N] - u2);
+        }
+        return;
+    }
+    if (!d.mls) {
+        for (int q = 0; q < ng; ++q) o[g0 + q] = o[npt + g0 + q] = o[2 * npt + g0 + q] = 0.f;
+        return;
+    }
+    double a[4][3] = {};
+    const int64_t c0 = d.cbptr[i], nc = d.cbptr[i + 1] - c0;
+    const int32_t* cb = d.cbidx + c0;
+    const float* cf = d.coeff32 + c0 * npt + g0;
+    const bool vec = (ng == 4) && ((npt & 3) == 0);
+    for (int64_t k = 0; k < nc; ++k) {
+        const int64_t m = cb[k];
+        const double d0 = us[m] - u0, d1 = us[N + m] - u1, d2 = us[2 * N + m] - u2;
+        float c[4];
+        if (vec) {
+            const float4 v = ld4(cf + k * npt);
+            c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+        } else {
+            for (int q = 0; q < 4; ++q) c[q] = q < ng ? cf[k * npt + q] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            a[q][0] = fma((double)c[q], d0, a[q][0]);
+            a[q][1] = fma((double)c[q], d1, a[q][1]);
+            a[q][2] = fma((double)c[q], d2, a[q][2]);
+        }
+    }
+    for (int q = 0; q < ng; ++q) {
+        const double S = (double)d.csum[i * npt + g0 + q];
+        o[g0 + q] = (float)fma(S, u0, a[q][0]);
+        o[npt + g0 + q] = (float)fma(S, u1, a[q][1]);
+        o[2 * npt + g0 + q] = (float)fma(S, u2, a[q][2]);
+    }
+}
+
+template <int NPT>
+PointPack<NPT> pack_points(const Dev& d, const GaussConst* host_gc) {
+    PointPack<NPT> P;
+    for (int g = 0; g < NPT; ++g)
+        P.p[g] = PointF{host_gc[g].hgf[0], host_gc[g].hgf[1], host_gc[g].hgf[2], host_gc[g].Wf, host_gc[g].A,
+                        host_gc[g].B};
+    return P;
+}
+
+}  // namespace
+
+void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
+    if (d.n == 0) return;
+    const unsigned nb = blocks_for(d.n, 128);
+    if (d.cci) {
+        k_pack_cci<<<blocks_for(d.n, 256), 256, 0, s>>>(d);
+        if (d.sfac) k_force_f32c_cci<true><<<nb, 128, 0, s>>>(d, dts);
+        else k_force_f32c_cci<false><<<nb, 128, 0, s>>>(d, dts);
+        return;
+    }
+    if (d.npt == 8 && d.gc_host) {
+        const PointPack<8> P = pack_points<8>(d, d.gc_host);
+        const unsigned np = blocks_for((d.n + 1) / 2, 128);
+        const bool lat = d.lat != nullptr, bd = d.bdry_on != 0, sf = d.sfac != nullptr;
+#define PD_F32(HF, LT, BD, SF, MM) k_force_f32c_pair<HF, LT, BD, SF, MM><<<np, 128, 0, s>>>(d, P, dts)
+        if (d.hasfail || d.multimat) {
+            PD_F32(true, false, true, true, true);
+        } else if (lat) {
+            if (bd) { if (sf) PD_F32(false, true, true, true, false); else PD_F32(false, true, true, false, false); }
+            else { if (sf) PD_F32(false, true, false, true, false); else PD_F32(false, true, false, false, false); }
+        } else {
+            if (bd) { if (sf) PD_F32(false, false, true, true, false); else PD_F32(false, false, true, false, false); }
+            else { if (sf) PD_F32(false, false, false, true, false); else PD_F32(false, false, false, false, false); }
+        }
+#undef PD_F32
+        return;
+    }
+    if (d.sfac) k_force_f32c_any<true><<<nb, 128, 0, s>>>(d, dts);
+    else k_force_f32c_any<false><<<nb, 128, 0, s>>>(d, dts);
+}
+
+void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
+    if (d.cci || d.n == 0) return;
+    const int ngrp = (d.npt + 3) / 4;
+    k_gather_f32c<<<blocks_for(d.n * ngrp, 256), 256, 0, s>>>(d, us);
+}
+
+void launch_pack_cci_f32c(const Dev& d, cudaStream_t s) {
+    if (!d.cci || d.n == 0) return;
+    k_pack_cci<<<blocks_for(d.n, 256), 256, 0, s>>>(d);
+}
+
+}  // namespace pd

@@ -1,16 +1,5 @@
-// FP32-compensated force and gather kernels, the static operator, scans and
-// reductions.
-//
-// FP32 form.  The stretch of a bond is tiny (1e-6..1e-3) next to its length,
-// so (|xi+eta| - |xi|) / |xi| loses every digit in FP32.  These kernels never
-// form that difference: with d = |xi+eta|^2 - |xi|^2 = eta.(2 xi + eta),
-//     s = d / (r (p + r)),   f = c beta s (xi+eta) / p,
-// all terms of which are accurate to FP32 rounding relative to the strain
-// itself.  eta is likewise assembled from differences taken in FP64 and only
-// then rounded: eta = (float)(us_j - u_i) + ugrel_j,g with ugrel = ug - us_j,
-// the Gauss-point displacement relative to its own node, which the gather
-// produces directly.  Per-bond forces are summed in FP32 and the family sum of
-// each node is Kahan-compensated; the state update stays FP64.
+// The static operator (FP64 and FP32 matvec, right-hand side), the CG pieces,
+// scans and reductions.
 #include <cstdio>
 
 #include "pd_internal.cuh"
@@ -25,154 +14,6 @@ __device__ __forceinline__ double time_factor(const BcDev& b, double t) {
     if (b.type == PD_BC_VELOC) return (t <= b.end_time) ? 1.0 : 0.0;
     if (b.load_type == 1.0) return (t <= b.end_time) ? t / b.end_time : 1.0;
     return 1.0;
-}
-
-// ------------------------------------------------------------ FP32 force
-
-template <bool CCI, bool SFAC>
-__global__ void __launch_bounds__(128) k_force_f32c(Dev d, double dts) {
-    __shared__ float sh[kMaxPoints][6];  // hg[3], W, A, B
-    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) {
-        const GaussConst& G = d.gc[g];
-        sh[g][0] = G.hgf[0];
-        sh[g][1] = G.hgf[1];
-        sh[g][2] = G.hgf[2];
-        sh[g][3] = G.Wf;
-        sh[g][4] = G.A;
-        sh[g][5] = G.B;
-    }
-    __syncthreads();
-    const int64_t N = d.n;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const MatDev Mi = d.mats[d.mat[i]];
-    const double rho = Mi.density;
-    const bool bci = d.bc[i] >= 0;
-    const double* src = bci ? d.U : d.us;
-    const double ui0 = src[i], ui1 = src[N + i], ui2 = src[2 * N + i];
-    const double xi0 = d.x[i], xi1 = d.x[N + i], xi2 = d.x[2 * N + i];
-    const double bEi = d.bdry[i];
-    const double sfi = SFAC ? d.sfac[i] : 0.0;
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;  // Kahan sums
-    const int64_t pb = d.arow[i], pe = d.arow[i + 1];
-    const float delta = (float)d.delta;
-    const float dxf = (float)d.dx;
-    for (int64_t p = pb; p < pe; ++p) {
-        const int64_t j = d.acol[p];
-        const MatDev& Mj = d.mats[d.mat[j]];
-        const float ecrit = (float)((Mj.ecrit < Mi.ecrit) ? Mj.ecrit : Mi.ecrit);
-        double c = (Mj.spring < Mi.spring) ? Mj.spring : Mi.spring;
-        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
-        const float coef = (float)(0.5 * (bEi + d.bdry[j]) * c);
-        const float dx0 = (float)(d.x[j] - xi0), dx1 = (float)(d.x[N + j] - xi1), dx2 = (float)(d.x[2 * N + j] - xi2);
-        float F0 = 0.f, F1 = 0.f, F2 = 0.f;
-        if (CCI) {
-            const double* sj = (d.bc[j] >= 0) ? d.U : d.us;
-            const float e0 = (float)(sj[j] - ui0), e1 = (float)(sj[N + j] - ui1), e2 = (float)(sj[2 * N + j] - ui2);
-            const float y0 = dx0 + e0, y1 = dx1 + e1, y2 = dx2 + e2;
-            const float r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
-            const float dd = e0 * (dx0 + y0) + e1 * (dx1 + y1) + e2 * (dx2 + y2);
-            const float p2 = r2 + dd;
-            const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
-            const float r = r2 * rinv, pl = p2 * pinv;
-            const float s = dd * rinv * __frcp_rn(pl + r);
-            float beta;
-            if (d.cci_mdf) beta = __saturatef((delta + 0.5f * dxf - r) / dxf);
-            else beta = (r > delta) ? 0.f : __saturatef((delta + 0.5f * dxf - r) / dxf);
-            const float fm = (dd > 0.f && s > ecrit) ? 0.f : coef * (float)d.vol_cci * beta * s * pinv;
-            F0 = fm * y0;
-            F1 = fm * y1;
-            F2 = fm * y2;
-        } else {
-            const float du0 = (float)(d.us[j] - ui0), du1 = (float)(d.us[N + j] - ui1), du2 = (float)(d.us[2 * N + j] - ui2);
-            const float* ur = d.ugrel + j;
-#pragma unroll 4
-            for (int g = 0; g < d.npt; ++g) {
-                const float x0 = dx0 + sh[g][0], x1 = dx1 + sh[g][1], x2 = dx2 + sh[g][2];
-                const float e0 = du0 + ur[(3 * g) * N], e1 = du1 + ur[(3 * g + 1) * N], e2 = du2 + ur[(3 * g + 2) * N];
-                const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
-                const float r2 = x0 * x0 + x1 * x1 + x2 * x2;
-                const float dd = e0 * (x0 + y0) + e1 * (x1 + y1) + e2 * (x2 + y2);
-                const float p2 = r2 + dd;
-                const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
-                const float r = r2 * rinv, pl = p2 * pinv;
-                const float s = dd * rinv * __frcp_rn(pl + r);
-                const float beta = __saturatef((sh[g][4] - r) * sh[g][5]);
-                const float fm = (dd > 0.f && s > ecrit) ? 0.f : sh[g][3] * beta * s * pinv;
-                F0 = fmaf(fm, y0, F0);
-                F1 = fmaf(fm, y1, F1);
-                F2 = fmaf(fm, y2, F2);
-            }
-            F0 *= coef;
-            F1 *= coef;
-            F2 *= coef;
-        }
-        // Kahan accumulation of the family sum
-        float yk = F0 - c0, tk = s0 + yk;
-        c0 = (tk - s0) - yk;
-        s0 = tk;
-        yk = F1 - c1; tk = s1 + yk; c1 = (tk - s1) - yk; s1 = tk;
-        yk = F2 - c2; tk = s2 + yk; c2 = (tk - s2) - yk; s2 = tk;
-    }
-    const double nb = (double)(pe - pb);
-    const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
-    d.vbuf[i] += ((double)s0 - (double)c0 + nb * b0) * dts / rho;
-    d.vbuf[N + i] += ((double)s1 - (double)c1 + nb * b1) * dts / rho;
-    d.vbuf[2 * N + i] += ((double)s2 - (double)c2 + nb * b2) * dts / rho;
-}
-
-// ----------------------------------------------------------- FP32 gather
-
-// One thread per (node, point).  Writes ugrel = ug - us(node) in FP32 and, for
-// nodes with a boundary condition, keeps the FP64 ug of the reference rules.
-__global__ void k_gather_f32c(Dev d, const double* __restrict__ us) {
-    const int64_t N = d.n;
-    const double t = *d.tdev;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (tid >= N * d.npt) return;
-    const int64_t i = tid / d.npt;
-    const int g = (int)(tid - i * d.npt);
-    const double u0 = us[i], u1 = us[N + i], u2 = us[2 * N + i];
-    float* out = d.ugrel + (int64_t)(3 * g) * N + i;
-    const int b = d.bc[i];
-    if (b >= 0) {
-        double* ug = d.ug + (int64_t)(3 * g) * N + i;
-        const BcDev& B = d.bcs[b];
-        const double fac = time_factor(B, t);
-        const GaussConst& G = d.gc[g];
-        const double q0 = G.hg[0] + d.x[i], q1 = G.hg[1] + d.x[N + i], q2 = G.hg[2] + d.x[2 * N + i];
-        for (int a = 0; a < 3; ++a) {
-            if (B.dir[a] != 1) continue;
-            if (B.type == PD_BC_DISPL) ug[a * N] = B.val[a] * fac;
-            else if (B.type == PD_BC_DISPLGRAD)
-                ug[a * N] = (B.val[3 * a] * q0 + B.val[3 * a + 1] * q1 + B.val[3 * a + 2] * q2) * fac;
-        }
-        out[0] = (float)(ug[0] - u0);
-        out[N] = (float)(ug[N] - u1);
-        out[2 * N] = (float)(ug[2 * N] - u2);
-        return;
-    }
-    if (d.mls) {
-        const int64_t cb0 = d.cbptr[i], nc = d.cbptr[i + 1] - cb0;
-        const float* cf = d.coeff32 + cb0 * d.npt + g;
-        const int32_t* cb = d.cbidx + cb0;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int64_t k = 0; k < nc; ++k) {
-            const int64_t m = cb[k];
-            const double c = (double)cf[k * d.npt];
-            a0 = fma(c, us[m] - u0, a0);
-            a1 = fma(c, us[N + m] - u1, a1);
-            a2 = fma(c, us[2 * N + m] - u2, a2);
-        }
-        const double S = (double)d.csum[i * d.npt + g];
-        out[0] = (float)fma(S, u0, a0);
-        out[N] = (float)fma(S, u1, a1);
-        out[2 * N] = (float)fma(S, u2, a2);
-    } else {
-        out[0] = 0.f;
-        out[N] = 0.f;
-        out[2 * N] = 0.f;
-    }
 }
 
 // -------------------------------------------------------- static operator
@@ -390,23 +231,6 @@ int exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t 
     cudaFree(bsum);
     cudaFree(boff);
     return rc;
-}
-
-void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
-    if (d.n == 0) return;
-    const unsigned nb = blocks_for(d.n, 128);
-    if (d.cci) {
-        if (d.sfac) k_force_f32c<true, true><<<nb, 128, 0, s>>>(d, dts);
-        else k_force_f32c<true, false><<<nb, 128, 0, s>>>(d, dts);
-    } else {
-        if (d.sfac) k_force_f32c<false, true><<<nb, 128, 0, s>>>(d, dts);
-        else k_force_f32c<false, false><<<nb, 128, 0, s>>>(d, dts);
-    }
-}
-
-void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
-    if (d.cci || d.n == 0) return;
-    k_gather_f32c<<<blocks_for(d.n * d.npt, 256), 256, 0, s>>>(d, us);
 }
 
 void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y, cudaStream_t s) {

@@ -56,6 +56,7 @@ struct Dev {
     const double* bdry;       // [N]
     const double* sfac;       // [N] or nullptr
     const GaussConst* gc;     // [npt]
+    const GaussConst* gc_host;  // host copy of gc (kernel-parameter constants)
     // family (full) and active (unbroken) CSR
     const int64_t* frow;
     const int32_t* fcol;
@@ -78,10 +79,27 @@ struct Dev {
     double* k2;
     double* k32;
     double* ug;               // [npt*3][N]
-    float* ugrel;             // [npt*3][N] FP32 form: ug - us(node)
     double* eed;              // [N]
     double* red;              // reduction scratch
     double* tdev;             // current time (device scalar; advanced on the device)
+    // work order: node-parallel kernels take node order[tid], so that a block
+    // covers a compact 3-D tile of the lattice (its neighbours then share L1)
+    const int32_t* order;
+    // FP32 form, per node (array-of-structures, 16-byte aligned):
+    //  nblk [N][bs]: Gauss-point displacement relative to the node, component-
+    //        major ([x:npt][y:npt][z:npt]), then the node's trial displacement
+    //        split into FP32 hi and lo parts (hi[3], lo[3]); rewritten by every
+    //        gather (or, for CCI, by the pack kernel)
+    //  sblk [N][8]:  coordinates split hi[3], lo[3], boundary factor, spring factor
+    float* nblk;
+    int bs;
+    const float* sblk;
+    int multimat, hasfail;
+    int bdry_on;              // some boundary factor differs from 1
+    // lattice positions packed x | y << 11 | z << 22 (x, y < 2048, z < 1024)
+    // when every node sits on one cubic lattice of spacing dx; else nullptr
+    const int32_t* lat;
+    float c0, e0;             // spring and critical stretch when there is one material
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -107,6 +125,7 @@ int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int
 // FP32 compensated form (pd_fast.cu)
 void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s);
+void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
 
 // CG helpers (pd_fast.cu): slots of the device scalar array
 enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_NSLOT = 8 };
