@@ -175,6 +175,43 @@ int pd_reset_state(pd_ctx* ctx);
  * gather, stage-epilogue and remaining kernels of the step. */
 int pd_profile_step(pd_ctx* ctx, double dt, double time, double* ms);
 
+/* ---- Bond search for callers that cannot allocate device memory ----
+ *
+ * No counterpart in the reference.  pd_bond_search needs a context, and a
+ * context calls cudaMalloc.  Some hosts cannot: an application that hands
+ * all device memory to its own pool at start-up and forbids allocations
+ * afterwards, or a plugin whose memory is owned by the host program, or a
+ * loop that must not block on cudaMalloc's implicit synchronisation.  This
+ * entry point performs the same search (same membership test, same
+ * ascending-id family order, same slit marks) into buffers the caller
+ * provides, and allocates nothing: its working memory is one fixed array of
+ * PD_NOALLOC_SCRATCH_BYTES in device memory, part of the library image, which
+ * every GPU that loads the library holds until the process exits.
+ *
+ * Limits: at most PD_NOALLOC_MAX_NODES nodes, PD_NOALLOC_MAX_CELLS search
+ * cells (bounding box / (horizon + spacing), rounded up, per axis, multiplied)
+ * and PD_NOALLOC_MAX_SLITS slits; larger problems return PD_ERR_CAPACITY.
+ *
+ * coords: device, [n][3].  row_ptr: device, [n+1], always written.  col and
+ * broken (broken may be NULL): device, [capacity]; when the family is larger
+ * than capacity the call returns PD_ERR_CAPACITY after writing row_ptr and
+ * *num_halves, so the caller can size col and call again.  slits: host,
+ * [num_slits][6].  stream: a cudaStream_t or NULL; the call synchronises it.
+ *
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the one array and it keeps the
+ * last call's contents (the call clears what must start at zero): calls that
+ * overlap on the GPU, from several threads or streams, race and must be
+ * serialised by the caller. */
+#define PD_NOALLOC_MAX_NODES 65536
+#define PD_NOALLOC_MAX_CELLS 65536
+#define PD_NOALLOC_MAX_SLITS 16
+#define PD_NOALLOC_SCRATCH_BYTES 2622360
+int pd_bond_search_noalloc(const double* coords, int64_t num_nodes, double grid_spacing, double horizon,
+                           int32_t num_slits, const double* slits, int64_t* row_ptr, int32_t* col, uint8_t* broken,
+                           int64_t capacity, void* stream, int64_t* num_halves, double* min_bond_length);
+
 /* Linearised stiffness operator of pdSolve::AssembleEquation (pdSolve.cpp:
  * 195-527) applied matrix-free: free rows sum c V_j xi xi^T / r^3 (x_i - x_j)
  * over the unbroken family with prescribed columns masked, prescribed rows

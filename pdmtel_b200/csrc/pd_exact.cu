@@ -7,7 +7,9 @@
 // the reference's loops, so the force, gather and state vectors are bit-for-
 // bit those of the reference CPU path (pdDataManager.cpp:1767-2134).
 #include <cfloat>
+#include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "pd_internal.cuh"
@@ -726,4 +728,295 @@ int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int
     return PD_OK;
 }
 
+// ======================================= bond search without allocation
+
+// pd_bond_search_noalloc works entirely in this fixed device array, carved
+// into the regions below.  Every GPU that loads the library holds it until
+// the process exits; all calls share it.
+namespace na {
+constexpr int64_t kNodes = PD_NOALLOC_MAX_NODES;
+constexpr int64_t kCells = PD_NOALLOC_MAX_CELLS;
+constexpr int kSlits = PD_NOALLOC_MAX_SLITS;
+constexpr size_t kOffSorted = sizeof(int32_t) * kNodes;                 // node_cell [kNodes] at 0
+constexpr size_t kOffCnt = kOffSorted + sizeof(int32_t) * kNodes;       // sorted [kNodes]
+constexpr size_t kOffCellCnt = kOffCnt + sizeof(int64_t) * kNodes;      // cnt [kNodes]
+constexpr size_t kOffCstart = kOffCellCnt + sizeof(int64_t) * (kCells + 1);
+constexpr size_t kOffFill = kOffCstart + sizeof(int64_t) * (kCells + 1);
+constexpr size_t kOffSlits = kOffFill + sizeof(int64_t) * (kCells + 1);
+constexpr size_t kOffScal = kOffSlits + sizeof(double) * 6 * kSlits;   // bbox[6], min bits, max count
+constexpr size_t kBytes = kOffScal + 16 * sizeof(double);
+static_assert(kBytes == PD_NOALLOC_SCRATCH_BYTES, "scratch size stated in pdmtel_b200.h");
+}  // namespace na
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[na::kBytes];
+
+namespace {
+
+struct NaArgs {
+    const double* x;  // [n][3], caller's device buffer
+    int64_t n;
+    double dx, delta, tol;
+    SearchGrid g;
+    unsigned char* s;  // device address of g_noalloc_scratch
+    int nslit;
+};
+
+__device__ __forceinline__ int32_t* na_node_cell(unsigned char* s) { return (int32_t*)s; }
+__device__ __forceinline__ int32_t* na_sorted(unsigned char* s) { return (int32_t*)(s + na::kOffSorted); }
+__device__ __forceinline__ int64_t* na_cnt(unsigned char* s) { return (int64_t*)(s + na::kOffCnt); }
+__device__ __forceinline__ int64_t* na_cell_cnt(unsigned char* s) { return (int64_t*)(s + na::kOffCellCnt); }
+__device__ __forceinline__ int64_t* na_cstart(unsigned char* s) { return (int64_t*)(s + na::kOffCstart); }
+__device__ __forceinline__ int64_t* na_fill(unsigned char* s) { return (int64_t*)(s + na::kOffFill); }
+__device__ __forceinline__ double* na_slits(unsigned char* s) { return (double*)(s + na::kOffSlits); }
+__device__ __forceinline__ double* na_scal(unsigned char* s) { return (double*)(s + na::kOffScal); }
+
+// bounding box of the nodes into scal[0..5]; one block
+__global__ void k_na_bbox(const double* __restrict__ x, int64_t n, unsigned char* s) {
+    __shared__ double red[6][32];
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = dmin(lo[a], x[3 * i + a]);
+            hi[a] = -dmin(-hi[a], -x[3 * i + a]);
+        }
+    for (int o = 16; o > 0; o >>= 1)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = dmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = -dmin(-hi[a], -__shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) {
+            red[a][w] = lo[a];
+            red[3 + a][w] = hi[a];
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double* sc = na_scal(s);
+        for (int a = 0; a < 3; ++a) {
+            double l = red[a][0], h = red[3 + a][0];
+            for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+                l = dmin(l, red[a][k]);
+                h = -dmin(-h, -red[3 + a][k]);
+            }
+            sc[a] = l;
+            sc[3 + a] = h;
+        }
+        ((unsigned long long*)sc)[6] = (unsigned long long)__double_as_longlong(0.0);
+        ((unsigned long long*)sc)[7] = 0ull;
+    }
+}
+
+__device__ __forceinline__ int64_t na_cell_of(const NaArgs& A, const double* p, int64_t* c) {
+    for (int a = 0; a < 3; ++a) {
+        int64_t v = (int64_t)floor((p[a] - A.g.lo[a]) / A.g.h);
+        c[a] = v < 0 ? 0 : (v >= A.g.nc[a] ? A.g.nc[a] - 1 : v);
+    }
+    return (c[2] * A.g.nc[1] + c[1]) * A.g.nc[0] + c[0];
+}
+
+__global__ void k_na_cell_count(NaArgs A) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    int64_t c[3];
+    const int64_t cell = na_cell_of(A, A.x + 3 * i, c);
+    na_node_cell(A.s)[i] = (int32_t)cell;
+    atomicAdd((unsigned long long*)&na_cell_cnt(A.s)[cell], 1ull);
+}
+
+// exclusive scan of in[0..n) into out[0..n], out[n] = total; one block of
+// 1024 threads, each thread owning a contiguous run
+__global__ void k_na_scan(const int64_t* __restrict__ in, int64_t* __restrict__ out, int64_t n) {
+    __shared__ int64_t part[1024];
+    const int64_t per = (n + 1023) / 1024;
+    const int64_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+    int64_t sum = 0;
+    for (int64_t k = b; k < e; ++k) sum += in[k];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int64_t v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int64_t run = part[threadIdx.x] - sum;
+    for (int64_t k = b; k < e; ++k) {
+        const int64_t v = in[k];
+        out[k] = run;
+        run += v;
+    }
+    if (threadIdx.x == 1023) out[n] = part[1023];
+}
+
+__global__ void k_na_scatter(NaArgs A) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const int32_t cell = na_node_cell(A.s)[i];
+    const int64_t pos = (int64_t)atomicAdd((unsigned long long*)&na_fill(A.s)[cell], 1ull);
+    na_sorted(A.s)[na_cstart(A.s)[cell] + pos] = (int32_t)i;
+}
+
+// One warp per node, the membership test of InitBond (pdDataManager2.cpp:
+// 12-70).  PASS 0 counts; PASS 1 sorts the family by id in shared memory and
+// writes it with the slit marks.
+template <int PASS>
+__global__ void k_na_search(NaArgs A, int64_t* row_ptr, int32_t* col, uint8_t* broken, int cap) {
+    extern __shared__ int32_t sb[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (i >= A.n) return;
+    int32_t* buf = sb + (size_t)wib * cap;
+    uint8_t* brk = (uint8_t*)(sb + (size_t)(blockDim.x >> 5) * cap) + (size_t)wib * cap;
+    const double* sl = na_slits(A.s);
+    double pi[3] = {A.x[3 * i], A.x[3 * i + 1], A.x[3 * i + 2]};
+    int64_t c[3];
+    na_cell_of(A, pi, c);
+    int64_t nf = 0;
+    double mb = A.delta;
+    for (int64_t dz = -1; dz <= 1; ++dz)
+        for (int64_t dy = -1; dy <= 1; ++dy)
+            for (int64_t dxc = -1; dxc <= 1; ++dxc) {
+                const int64_t qx = c[0] + dxc, qy = c[1] + dy, qz = c[2] + dz;
+                if (qx < 0 || qy < 0 || qz < 0 || qx >= A.g.nc[0] || qy >= A.g.nc[1] || qz >= A.g.nc[2]) continue;
+                const int64_t q = (qz * A.g.nc[1] + qy) * A.g.nc[0] + qx;
+                const int64_t s0 = na_cstart(A.s)[q], s1 = na_cstart(A.s)[q + 1];
+                for (int64_t s = s0; s < s1; s += 32) {
+                    bool hit = false, br = false;
+                    int64_t j = -1;
+                    if (s + lane < s1) {
+                        j = na_sorted(A.s)[s + lane];
+                        if (j != i) {
+                            const double pj[3] = {A.x[3 * j], A.x[3 * j + 1], A.x[3 * j + 2]};
+                            const double* pa = (i < j) ? pi : pj;
+                            const double* pb = (i < j) ? pj : pi;
+                            double dist;
+                            hit = pair_bonded(pa, pb, A.dx, A.delta, A.tol, &dist);
+                            if (hit) {
+                                if (i < j) mb = dmin(mb, dist);
+                                for (int k = 0; k < A.nslit; ++k) br = br || slit_crosses(sl + 6 * k, pa, pb);
+                            }
+                        }
+                    }
+                    const unsigned hm = __ballot_sync(0xffffffffu, hit);
+                    if (PASS == 1 && hit) {
+                        const int slot = (int)nf + __popc(hm & ((1u << lane) - 1u));
+                        if (slot < cap) {
+                            buf[slot] = (int32_t)j;
+                            brk[slot] = br ? 1 : 0;
+                        }
+                    }
+                    nf += __popc(hm);
+                }
+            }
+    if (PASS == 0) {
+        for (int o = 16; o > 0; o >>= 1) mb = dmin(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        if (lane == 0) {
+            na_cnt(A.s)[i] = nf;
+            unsigned long long* sc = (unsigned long long*)na_scal(A.s);
+            atomicMin(&sc[6], (unsigned long long)__double_as_longlong(mb));
+            atomicMax(&sc[7], (unsigned long long)nf);
+        }
+        return;
+    }
+    __syncwarp();
+    const int n = (int)(nf < cap ? nf : cap);
+    const int64_t o = row_ptr[i];
+    for (int e = lane; e < n; e += 32) {
+        const int32_t v = buf[e];
+        int rk = 0;
+        for (int k = 0; k < n; ++k) rk += buf[k] < v ? 1 : 0;
+        col[o + rk] = v;
+        if (broken) broken[o + rk] = brk[e];
+    }
+}
+
+std::mutex g_na_mu;
+void* g_na_addr[64] = {};
+
+}  // namespace
+
 }  // namespace pd
+
+extern "C" int pd_bond_search_noalloc(const double* coords, int64_t n, double grid_spacing, double horizon,
+                                      int32_t num_slits, const double* slits, int64_t* row_ptr, int32_t* col,
+                                      uint8_t* broken, int64_t capacity, void* stream, int64_t* num_halves,
+                                      double* min_bond_length) {
+    using namespace pd;
+    if (n < 0 || n > na::kNodes) return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: more nodes than PD_NOALLOC_MAX_NODES");
+    if (num_slits < 0 || num_slits > na::kSlits || (num_slits > 0 && !slits))
+        return fail(PD_ERR_ARG, "pd_bond_search_noalloc: bad slit list");
+    if (!row_ptr || (n > 0 && !coords) || capacity < 0 || (capacity > 0 && !col) || !(grid_spacing > 0.0) ||
+        !(horizon > 0.0))
+        return fail(PD_ERR_ARG, "pd_bond_search_noalloc: bad argument");
+    int dev = 0;
+    PD_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(PD_ERR_ARG, "pd_bond_search_noalloc: device index above 63");
+    unsigned char* s = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_na_mu);
+        if (!g_na_addr[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+            g_na_addr[dev] = p;
+        }
+        s = (unsigned char*)g_na_addr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    double bb[6] = {0, 0, 0, 0, 0, 0};
+    if (n > 0) {
+        k_na_bbox<<<1, 1024, 0, st>>>(coords, n, s);
+        PD_CUDA_TRY(cudaGetLastError());
+        PD_CUDA_TRY(cudaMemcpyAsync(bb, s + na::kOffScal, sizeof bb, cudaMemcpyDeviceToHost, st));
+        PD_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    NaArgs A;
+    A.x = coords;
+    A.n = n;
+    A.dx = grid_spacing;
+    A.delta = horizon;
+    A.tol = 1.0e-4 * grid_spacing;
+    A.s = s;
+    A.nslit = num_slits;
+    A.g.h = horizon + grid_spacing;
+    int64_t ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        A.g.lo[a] = bb[a];
+        A.g.nc[a] = (int64_t)std::floor((bb[3 + a] - bb[a]) / A.g.h) + 1;
+        ncell *= A.g.nc[a];
+    }
+    if (ncell > na::kCells) return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: more cells than PD_NOALLOC_MAX_CELLS");
+    // the regions read before they are written start at zero
+    PD_CUDA_TRY(cudaMemsetAsync(s + na::kOffCellCnt, 0, sizeof(int64_t) * (ncell + 1), st));
+    PD_CUDA_TRY(cudaMemsetAsync(s + na::kOffFill, 0, sizeof(int64_t) * (ncell + 1), st));
+    if (num_slits > 0)
+        PD_CUDA_TRY(cudaMemcpyAsync(s + na::kOffSlits, slits, sizeof(double) * 6 * num_slits, cudaMemcpyHostToDevice, st));
+    unsigned long long sc[2] = {(unsigned long long)__builtin_bit_cast(unsigned long long, horizon), 0ull};
+    PD_CUDA_TRY(cudaMemcpyAsync(s + na::kOffScal + 6 * sizeof(double), sc, sizeof sc, cudaMemcpyHostToDevice, st));
+    const int bs = 256, wpb = 4;
+    const unsigned nb = (unsigned)((n + bs - 1) / bs), nw = (unsigned)((n * 32 + 32 * wpb - 1) / (32 * wpb));
+    if (n > 0) k_na_cell_count<<<nb, bs, 0, st>>>(A);
+    k_na_scan<<<1, 1024, 0, st>>>((const int64_t*)(s + na::kOffCellCnt), (int64_t*)(s + na::kOffCstart), ncell);
+    if (n > 0) {
+        k_na_scatter<<<nb, bs, 0, st>>>(A);
+        k_na_search<0><<<nw, 32 * wpb, 0, st>>>(A, nullptr, nullptr, nullptr, 0);
+    }
+    k_na_scan<<<1, 1024, 0, st>>>((const int64_t*)(s + na::kOffCnt), row_ptr, n);
+    PD_CUDA_TRY(cudaGetLastError());
+    int64_t total = 0;
+    unsigned long long back[2] = {0, 0};
+    PD_CUDA_TRY(cudaMemcpyAsync(&total, row_ptr + n, sizeof total, cudaMemcpyDeviceToHost, st));
+    PD_CUDA_TRY(cudaMemcpyAsync(back, s + na::kOffScal + 6 * sizeof(double), sizeof back, cudaMemcpyDeviceToHost, st));
+    PD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (num_halves) *num_halves = total;
+    if (min_bond_length) *min_bond_length = n > 0 ? __builtin_bit_cast(double, back[0]) : horizon;
+    if (total > capacity) return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: col capacity below the family size");
+    const int cap = (int)back[1] + 1;
+    const size_t sh = (size_t)wpb * cap * (sizeof(int32_t) + sizeof(uint8_t));
+    if (sh > 48 * 1024) return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: family larger than the shared buffer");
+    if (n > 0) k_na_search<1><<<nw, 32 * wpb, sh, st>>>(A, row_ptr, col, broken, cap);
+    PD_CUDA_TRY(cudaGetLastError());
+    PD_CUDA_TRY(cudaStreamSynchronize(st));
+    return PD_OK;
+}
