@@ -171,7 +171,31 @@ __global__ void k_gather_f64(Dev d, const double* __restrict__ us) {
         const double* cf = d.coeff + c0 * d.npt + g;
         const int32_t* cb = d.cbidx + c0;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int64_t k = 0; k < nc; ++k) {
+        int64_t k = 0;
+        // loads of four contributors are issued together; the sums still run
+        // in contributor order
+        for (; k + 4 <= nc; k += 4) {
+            int64_t m[4];
+            double c[4], v[4][3];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                m[u] = cb[k + u];
+                c[u] = cf[(k + u) * d.npt];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u][0] = us[m[u]];
+                v[u][1] = us[N + m[u]];
+                v[u][2] = us[2 * N + m[u]];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a0 += v[u][0] * c[u];
+                a1 += v[u][1] * c[u];
+                a2 += v[u][2] * c[u];
+            }
+        }
+        for (; k < nc; ++k) {
             const int64_t m = cb[k];
             const double c = cf[k * d.npt];
             a0 += us[m] * c;

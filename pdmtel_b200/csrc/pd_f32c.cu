@@ -414,7 +414,38 @@ __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __rest
     const int32_t* cb = d.cbidx + c0;
     const float* cf = d.coeff32 + c0 * npt + g0;
     const bool vec = (ng == 4) && ((npt & 3) == 0);
-    for (int64_t k = 0; k < nc; ++k) {
+    int64_t k = 0;
+    if (vec) {
+        // four contributors per iteration: their index and displacement loads
+        // are independent, which hides the index -> displacement latency
+        for (; k + 4 <= nc; k += 4) {
+            int m[4];
+            float4 cv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                m[u] = __ldg(cb + k + u);
+                cv[u] = ld4(cf + (k + u) * npt);
+            }
+            double dd[4][3];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                dd[u][0] = __ldg(us + m[u]) - u0;
+                dd[u][1] = __ldg(us + N + m[u]) - u1;
+                dd[u][2] = __ldg(us + 2 * N + m[u]) - u2;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float c[4] = {cv[u].x, cv[u].y, cv[u].z, cv[u].w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    a[q][0] = fma((double)c[q], dd[u][0], a[q][0]);
+                    a[q][1] = fma((double)c[q], dd[u][1], a[q][1]);
+                    a[q][2] = fma((double)c[q], dd[u][2], a[q][2]);
+                }
+            }
+        }
+    }
+    for (; k < nc; ++k) {
         const int64_t m = cb[k];
         const double d0 = us[m] - u0, d1 = us[N + m] - u1, d2 = us[2 * N + m] - u2;
         float c[4];
