@@ -43,7 +43,12 @@ enum pd_integration { PD_INTG_CCI = 0, PD_INTG_FGI = 1 };
 /* arithmetic of the force / gather / matvec kernels */
 enum pd_precision {
     PD_PREC_FP64 = 0,  /* the drop-in: bit-faithful to the reference CPU path */
-    PD_PREC_FP32C = 1  /* FP32 forces, compensated sums, FP64 state */
+    PD_PREC_FP32C = 1, /* FP32 forces, compensated sums, FP64 state */
+    PD_PREC_FP64A = 2  /* FP64 with the bond extension p - r formed as
+                          (2 xi.eta + eta.eta) / (p + r): the same function
+                          without the cancellation of p - r at small strain
+                          (rounding ~eps instead of ~eps/strain); not
+                          bit-faithful to the reference */
 };
 
 /* bond-based (PMB) material, pdMaterialBond.cpp:8-11; spring = 18K/(pi d^4)
@@ -227,6 +232,36 @@ int pd_static_rhs(pd_ctx* ctx, double time, double* b);
  * solution out.  iters/relres may be NULL. */
 int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int maxit, double* x, int* iters,
                     double* relres);
+
+/* ---- Tuning options (no counterpart in the reference) ----
+ * PD_OPT_F64_LANES_BELOW: the FP64 Gauss-point force runs eight lanes per
+ *   node (same arithmetic, same order) when the problem has fewer nodes than
+ *   this, one thread per node otherwise.  Default 131072. */
+enum { PD_OPT_F64_LANES_BELOW = 1 };
+int pd_set_option(pd_ctx* ctx, int option, int64_t value);
+int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
+
+/* ---- Differentiation: gradient with respect to a per-node micromodulus ----
+ *
+ * No counterpart in the reference (its spring constant is per material with
+ * the min(c_i, c_j) pair rule, pdDataManager.cpp:1926).  With spring factors
+ * f the pair constant is min(c_i, c_j) * (f_i + f_j) / 2, which is
+ * differentiable in f; f = exp(m) gives a log-micromodulus field m. */
+/* replace the per-node spring factors f [N] (host, positive) */
+int pd_set_spring_factor(pd_ctx* ctx, const double* f);
+/* Forward half of the adjoint pair: nsteps FP64 RK4 steps of the scheme of
+ * pdDataManager::RK4 (pdDataManager.cpp:1994-2134) from the current state at
+ * time t0, storing (U, V, Gauss-point displacements, time) every
+ * checkpoint_every steps in the context.  The state ends at step nsteps.
+ * FGI (Gauss-point) scheme only. */
+int pd_adjoint_forward(pd_ctx* ctx, double dt, double t0, int nsteps, int checkpoint_every);
+/* Backward half: the vector-Jacobian product of the last forward run.
+ * lam_U, lam_V [3N] (host; lam_V may be NULL) are dJ/dU and dJ/dV of the
+ * final state; grad_f [N] (host) receives dJ/df.  Each checkpointed segment
+ * is recomputed with its stage inputs kept, then reversed stage by stage
+ * (force VJP as two gathers, transposed MLS gather); deterministic, no
+ * atomics.  The state is left at the start of the forward run. */
+int pd_adjoint_backward(pd_ctx* ctx, const double* lam_U, const double* lam_V, double* grad_f);
 
 #ifdef __cplusplus
 }

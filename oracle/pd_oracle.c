@@ -585,8 +585,19 @@ void or_gather(or_model* m, double t, const double* us) {
     }
 }
 
-void or_rk4_step(or_model* m, double dt, double t) {
+static void record_stage(const or_model* m, const double* us, double* out) {
     int64_t n3 = 3 * m->n;
+    memcpy(out, m->U, sizeof(double) * (size_t)n3);
+    memcpy(out + n3, us, sizeof(double) * (size_t)n3);
+    memcpy(out + 2 * n3, m->ug, sizeof(double) * (size_t)(n3 * m->npt));
+}
+
+/* One RK4 step.  With tape != NULL, the inputs of the four force stages
+ * (U, trial displacement, Gauss-point displacements: 3n + 3n + 3n*npt
+ * values each) are copied there before each stage. */
+static void rk4_step_taped(or_model* m, double dt, double t, double* tape) {
+    int64_t n3 = 3 * m->n;
+    int64_t per = 2 * n3 + n3 * m->npt;
     /* InitDynamicSolve, pdDataManager2.cpp:410-439 */
     for (int64_t i = 0; i < n3; ++i) m->vbuf[i] = m->V[i];
     for (int64_t i = 0; i < m->n; ++i) m->eed[i] = 0.0;
@@ -594,15 +605,19 @@ void or_rk4_step(or_model* m, double dt, double t) {
     double *u234 = u1 + n3, *k1 = u1 + 2 * n3, *k24 = u1 + 3 * n3, *k3 = u1 + 4 * n3, *k4 = u1 + 5 * n3;
     double dtHalf = 0.5 * dt, dt6 = 1.0 / 6.0;
     memcpy(u1, m->U, sizeof(double) * (size_t)n3);
+    if (tape) record_stage(m, u1, tape + 0 * per);
     or_force_stage(m, dtHalf, t, u1, k1);
     for (int64_t i = 0; i < n3; ++i) u234[i] = u1[i] + 0.5 * k1[i];
     or_gather(m, t, u234);
+    if (tape) record_stage(m, u234, tape + 1 * per);
     or_force_stage(m, dtHalf, t, u234, k24);
     for (int64_t i = 0; i < n3; ++i) u234[i] = u1[i] + 0.5 * k24[i];
     or_gather(m, t, u234);
+    if (tape) record_stage(m, u234, tape + 2 * per);
     or_force_stage(m, dt, t, u234, k3);
     for (int64_t i = 0; i < n3; ++i) { u234[i] = u1[i] + k3[i]; k3[i] += k24[i]; }
     or_gather(m, t, u234);
+    if (tape) record_stage(m, u234, tape + 3 * per);
     or_force_stage(m, dt, t, u234, k4);
     for (int64_t i = 0; i < m->n; ++i) {
         double rho = m->mat_density[m->mat[i]];
@@ -627,6 +642,224 @@ void or_rk4_step(or_model* m, double dt, double t) {
     m->ee = ee;
     or_gather(m, t, m->U);
     free(u1);
+}
+
+void or_rk4_step(or_model* m, double dt, double t) { rk4_step_taped(m, dt, t, NULL); }
+
+/* ------------------------------------------------------------ adjoint -- */
+
+/* Project rule, no counterpart in the reference: reverse accumulation of
+ * dJ/d(spring factor) through rk4_step_taped.  One Gauss point's force is
+ * f = be*beta*c*s*y/p with s = (p-r)/r (bond_force), i.e. k (1/r - 1/p) y
+ * with k = be*beta*c*W, whose Jacobian in y is k [(1/r - 1/p) I + y y^T/p^3];
+ * a point past the critical stretch has f = 0 and no derivative. */
+
+/* the stage's BC overwrite sets U (DISPL, DISPLGRAD) or vbuf (also VELOC) */
+static int fixes_u(const or_model* m, int64_t i, int a) {
+    int b = m->bc[i];
+    if (b < 0 || m->bc_dir[3 * b + a] != 1) return 0;
+    return m->bc_type[b] == OR_DISPL || m->bc_type[b] == OR_DISPLGRAD;
+}
+static int fixes_v(const or_model* m, int64_t i, int a) {
+    int b = m->bc[i];
+    if (b < 0 || m->bc_dir[3 * b + a] != 1) return 0;
+    return m->bc_type[b] != OR_TRACTION;
+}
+/* a Gauss-point entry of a BC node that the gather prescribes */
+static int gather_sets(const or_model* m, int64_t i, int a) { return fixes_u(m, i, a); }
+
+/* VJP of the bond forces of one stage.  lam [n][3]: adjoint of each node's
+ * summed force.  Adds to bown (the node's own displacement as read), bug
+ * (Gauss-point displacements) and gradf. */
+static void force_vjp(const or_model* m, const double* Us, const double* us, const double* ug, const double* lam,
+                      double* bown, double* bug, double* gradf) {
+    double vol8 = pow(m->dx, 3) / 8.0;
+    for (int64_t i = 0; i < m->n; ++i) {
+        const double* ui = (m->bc[i] >= 0) ? Us + 3 * i : us + 3 * i;
+        const double* xi = m->x + 3 * i;
+        const double* l = lam + 3 * i;
+        for (int64_t p = m->fam_ptr[i]; p < m->fam_ptr[i + 1]; ++p) {
+            if (m->broken && m->broken[p]) continue;
+            int64_t j = m->fam_col[p];
+            int mi = m->mat[i], mj = m->mat[j];
+            double ecrit = dmin2(m->mat_ecrit[mi], m->mat_ecrit[mj]);
+            double cmin = dmin2(m->mat_spring[mi], m->mat_spring[mj]);
+            double c = pair_spring(m, i, j);
+            double be = 0.5 * (m->bdry_eff[i] + m->bdry_eff[j]);
+            double dc = 0.0; /* dJ/dc_ij */
+            for (int g = 0; g < m->npt; ++g) {
+                const double* q = m->xg + (j * m->npt + g) * 3;
+                const double* ugp = ug + (j * m->npt + g) * 3;
+                double w1 = m->gw[3 * g], w2 = m->gw[3 * g + 1], w3 = m->gw[3 * g + 2];
+                double W = vol8 * w1 * w2 * w3;
+                double effw = pow(w1 * w2 * w3, 1.0 / 3.0);
+                double xv[3], ev[3], y[3], qq = 0.0;
+                for (int a = 0; a < 3; ++a) {
+                    xv[a] = q[a] - xi[a];
+                    ev[a] = ugp[a] - ui[a];
+                    y[a] = xv[a] + ev[a];
+                    qq += ev[a] * (2.0 * xv[a] + ev[a]);
+                }
+                double r = sqrt(xv[0] * xv[0] + xv[1] * xv[1] + xv[2] * xv[2]);
+                double pl = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+                double ext = qq / (pl + r); /* p - r without cancellation */
+                if (ext > 0.0 && ext / r > ecrit) continue;
+                double beta = beta_factor(r, m->delta, effw * m->dx / 2.0, 0, 0);
+                double a0 = ext / (r * pl); /* 1/r - 1/p */
+                double yl = y[0] * l[0] + y[1] * l[1] + y[2] * l[2];
+                double kk = be * beta * c * W;
+                for (int a = 0; a < 3; ++a) {
+                    double dy = kk * (a0 * l[a] + y[a] * yl / (pl * pl * pl));
+                    bown[3 * i + a] -= dy;
+                    bug[(j * m->npt + g) * 3 + a] += dy;
+                }
+                dc += be * beta * W * a0 * yl;
+            }
+            if (m->spring_factor) {
+                gradf[i] += 0.5 * cmin * dc;
+                gradf[j] += 0.5 * cmin * dc;
+            }
+        }
+    }
+}
+
+/* transpose of or_gather's node rows: bus[contributor] += coeff * bug */
+static void gather_t(const or_model* m, const double* bug, double* bus) {
+    int npt = m->npt;
+    for (int64_t i = 0; i < m->n; ++i) {
+        if (m->bc[i] >= 0) continue;
+        if (m->mls) {
+            int64_t nc = m->cb_ptr[i + 1] - m->cb_ptr[i];
+            const int32_t* cb = m->cb_idx + m->cb_ptr[i];
+            for (int g = 0; g < npt; ++g) {
+                const double* c = m->coeff + m->cb_ptr[i] * npt + (int64_t)g * nc;
+                const double* b = bug + (i * npt + g) * 3;
+                for (int64_t k = 0; k < nc; ++k)
+                    for (int a = 0; a < 3; ++a) bus[3 * (int64_t)cb[k] + a] += c[k] * b[a];
+            }
+        } else {
+            for (int a = 0; a < 3; ++a) bus[3 * i + a] += bug[i * npt * 3 + a];
+        }
+    }
+}
+
+/* move the BC nodes' carried Gauss-point entries of bug into carry */
+static void carry_bc_entries(const or_model* m, const double* bug, double* carry) {
+    for (int64_t i = 0; i < m->n; ++i) {
+        if (m->bc[i] < 0) continue;
+        for (int g = 0; g < m->npt; ++g)
+            for (int a = 0; a < 3; ++a)
+                if (!gather_sets(m, i, a)) carry[(i * m->npt + g) * 3 + a] += bug[(i * m->npt + g) * 3 + a];
+    }
+}
+
+/* reverse of one step; bU, bV, bug: adjoints of the step's output state in,
+ * of its input state out */
+static void rk4_step_reverse(const or_model* m, double dt, const double* tape, double* bU, double* bV, double* bug,
+                             double* w) {
+    int64_t n = m->n, n3 = 3 * n, ng = n3 * m->npt, per = 2 * n3 + ng;
+    double *bk[5], *bvb, *bu1, *bUs, *bown, *bus, *lam, *bugs, *carry;
+    bk[0] = NULL;
+    for (int s = 1; s <= 4; ++s) bk[s] = w + (s - 1) * n3;
+    bvb = w + 4 * n3; bu1 = w + 5 * n3; bUs = w + 6 * n3; bown = w + 7 * n3; bus = w + 8 * n3; lam = w + 9 * n3;
+    bugs = w + 10 * n3; carry = bugs + ng;
+    memset(w, 0, sizeof(double) * (size_t)(10 * n3 + 2 * ng));
+    /* final gather: ug_end = G(U_new) on free nodes, carried on BC nodes */
+    gather_t(m, bug, bU);
+    carry_bc_entries(m, bug, carry);
+    /* combination and damping */
+    for (int64_t i = 0; i < n; ++i) {
+        double rho = m->mat_density[m->mat[i]];
+        for (int a = 0; a < 3; ++a) {
+            int64_t r = 3 * i + a;
+            double g = bU[r];
+            bk[1][r] = g / 6.0;
+            bk[4][r] = g / 6.0;
+            bk[3][r] = g / 3.0; /* k3 (after k3 += k24) enters twice */
+            bk[2][r] = g / 3.0;
+            bUs[r] = g;
+            double v = -m->damping * dt / rho * bV[r];
+            if (m->bc[i] < 0) v += -dt * m->damping * dt / rho * g;
+            bvb[r] = bV[r];
+            bV[r] = v;
+        }
+    }
+    for (int s = 4; s >= 1; --s) {
+        double dts = s >= 3 ? dt : 0.5 * dt;
+        const double* T = tape + (s - 1) * per;
+        for (int64_t r = 0; r < n3; ++r) bvb[r] += dts * bk[s][r];
+        for (int64_t i = 0; i < n; ++i)
+            for (int a = 0; a < 3; ++a) {
+                if (fixes_v(m, i, a)) bvb[3 * i + a] = 0.0;
+                if (fixes_u(m, i, a)) bUs[3 * i + a] = 0.0;
+            }
+        for (int64_t i = 0; i < n; ++i) {
+            double rho = m->mat_density[m->mat[i]];
+            for (int a = 0; a < 3; ++a) lam[3 * i + a] = bvb[3 * i + a] * dts / rho;
+        }
+        memset(bown, 0, sizeof(double) * (size_t)n3);
+        memset(bugs, 0, sizeof(double) * (size_t)ng);
+        force_vjp(m, T, T + n3, T + 2 * n3, lam, bown, bugs, w + 10 * n3 + 2 * ng);
+        memset(bus, 0, sizeof(double) * (size_t)n3);
+        for (int64_t i = 0; i < n; ++i)
+            for (int a = 0; a < 3; ++a) {
+                if (m->bc[i] >= 0) bUs[3 * i + a] += bown[3 * i + a];
+                else bus[3 * i + a] = bown[3 * i + a];
+            }
+        carry_bc_entries(m, bugs, carry);
+        if (s >= 2) {
+            gather_t(m, bugs, bus);
+            double alpha = s == 4 ? 1.0 : 0.5;
+            for (int64_t r = 0; r < n3; ++r) {
+                bu1[r] += bus[r];
+                bk[s - 1][r] += alpha * bus[r];
+            }
+        } else {
+            for (int64_t r = 0; r < n3; ++r) bu1[r] += bus[r];
+            /* ug at stage 1 is the step's input: free nodes' rows */
+            for (int64_t i = 0; i < n; ++i) {
+                double* o = bug + i * m->npt * 3;
+                const double* src = (m->bc[i] >= 0) ? carry + i * m->npt * 3 : bugs + i * m->npt * 3;
+                for (int e = 0; e < m->npt * 3; ++e) o[e] = src[e];
+            }
+        }
+    }
+    for (int64_t r = 0; r < n3; ++r) {
+        bU[r] = bUs[r] + bu1[r];
+        bV[r] += bvb[r];
+    }
+}
+
+int or_adjoint_grad(or_model* m, double dt, double t0, int nsteps, const double* lamU, const double* lamV,
+                    double* gradf) {
+    int64_t n = m->n, n3 = 3 * n, ng = n3 * m->npt, per = 2 * n3 + ng;
+    double* tape = (double*)malloc(sizeof(double) * (size_t)(4 * per) * (size_t)nsteps);
+    double* w = (double*)malloc(sizeof(double) * (size_t)(10 * n3 + 2 * ng + n));
+    double* st = (double*)malloc(sizeof(double) * (size_t)(2 * n3 + ng));
+    if (!tape || !w || !st) {
+        free(tape); free(w); free(st);
+        return -1;
+    }
+    double t = t0;
+    for (int k = 0; k < nsteps; ++k) {
+        t += dt;
+        rk4_step_taped(m, dt, t, tape + (int64_t)k * 4 * per);
+    }
+    double *bU = st, *bV = st + n3, *bug = st + 2 * n3;
+    for (int64_t r = 0; r < n3; ++r) {
+        bU[r] = lamU[r];
+        bV[r] = lamV ? lamV[r] : 0.0;
+    }
+    memset(bug, 0, sizeof(double) * (size_t)ng);
+    double* gacc = w + 10 * n3 + 2 * ng;
+    memset(gacc, 0, sizeof(double) * (size_t)n);
+    for (int k = nsteps - 1; k >= 0; --k) {
+        /* rk4_step_reverse clears w except the gradient that follows it */
+        rk4_step_reverse(m, dt, tape + (int64_t)k * 4 * per, bU, bV, bug, w);
+    }
+    for (int64_t i = 0; i < n; ++i) gradf[i] = gacc[i];
+    free(tape); free(w); free(st);
+    return 0;
 }
 
 /* ------------------------------------------------- boundary effect ----- */

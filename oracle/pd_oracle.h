@@ -117,6 +117,15 @@ void or_static_rhs(const or_model* m, double t, double* b);
 /* plain FP64 CG on the static system; returns iterations or -1. */
 int or_static_cg(const or_model* m, double t, const double* b, double* x, double rtol, int maxit, double* relres);
 
+/* Project rule (no counterpart in the reference): runs nsteps of
+ * or_rk4_step from the model's state at t0 (t += dt before each step),
+ * keeping every stage's inputs, then accumulates in reverse the gradient
+ * gradf [n] of J with respect to spring_factor, for lamU/lamV [n][3] = dJ/dU,
+ * dJ/dV of the final state (lamV may be NULL).  The model is left at the
+ * final state.  Returns 0, or -1 when memory runs out. */
+int or_adjoint_grad(or_model* m, double dt, double t0, int nsteps, const double* lamU, const double* lamV,
+                    double* gradf);
+
 #ifdef __cplusplus
 }
 #endif

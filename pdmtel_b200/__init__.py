@@ -20,14 +20,15 @@ from typing import Optional
 
 import numpy as np
 
-__all__ = ["PdError", "lib", "pdDataManager", "pdSolve", "DeviceContext", "PREC_FP64", "PREC_FP32C",
+__all__ = ["PdError", "lib", "pdDataManager", "pdSolve", "DeviceContext", "PREC_FP64", "PREC_FP32C", "PREC_FP64A",
            "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpdmtel_b200.so")
 
 PD_OK = 0
-PREC_FP64, PREC_FP32C = 0, 1
+PREC_FP64, PREC_FP32C, PREC_FP64A = 0, 1, 2
+OPT_F64_LANES_BELOW = 1
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}
@@ -105,6 +106,11 @@ _SIGS = {
     "pd_static_matvec": [_vp, C.c_double, _d, _d],
     "pd_static_rhs": [_vp, C.c_double, _d],
     "pd_static_solve": [_vp, C.c_double, C.c_int, C.c_double, C.c_int, _d, C.POINTER(C.c_int), _d],
+    "pd_set_spring_factor": [_vp, _d],
+    "pd_set_option": [_vp, C.c_int, C.c_int64],
+    "pd_get_option": [_vp, C.c_int, _i64],
+    "pd_adjoint_forward": [_vp, C.c_double, C.c_double, C.c_int, C.c_int],
+    "pd_adjoint_backward": [_vp, _d, _d, _d],
     "pdh_open": [C.c_char_p, C.POINTER(_vp)],
     "pdh_close": [_vp],
     "pdh_get_info": [_vp, C.POINTER(pdh_info)],
@@ -383,6 +389,32 @@ class DeviceContext:
         _check(lib().pd_static_solve(self.h, float(t), int(precision), float(rtol), int(maxit), _p(x, _d),
                                      C.byref(it), C.byref(rr)), "pd_static_solve")
         return x, it.value, rr.value
+
+
+    def set_option(self, option, value):
+        _check(lib().pd_set_option(self.h, int(option), int(value)), "pd_set_option")
+
+    def get_option(self, option):
+        v = C.c_int64(0)
+        _check(lib().pd_get_option(self.h, int(option), C.byref(v)), "pd_get_option")
+        return v.value
+
+    def set_spring_factor(self, f):
+        fa = _f64(f, self.n)
+        _check(lib().pd_set_spring_factor(self.h, _p(fa, _d)), "pd_set_spring_factor")
+
+    def adjoint_forward(self, dt, t0, nsteps, checkpoint_every=50):
+        _check(lib().pd_adjoint_forward(self.h, float(dt), float(t0), int(nsteps), int(checkpoint_every)),
+               "pd_adjoint_forward")
+
+    def adjoint_backward(self, lam_U, lam_V=None):
+        """dJ/df for the adjoints lam_U, lam_V ([N, 3]) of the final state of
+        the last adjoint_forward; the state returns to that run's start."""
+        lu = _f64(lam_U, 3 * self.n)
+        lv = None if lam_V is None else _f64(lam_V, 3 * self.n)
+        g = np.zeros(self.n)
+        _check(lib().pd_adjoint_backward(self.h, _p(lu, _d), _p(lv, _d), _p(g, _d)), "pd_adjoint_backward")
+        return g
 
 
 class pdDataManager:

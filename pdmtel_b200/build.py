@@ -34,6 +34,7 @@ CUDA_UNITS = {
     "pd_f32c.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "pd_fast.cu": [],
     "pd_capi.cu": [],
+    "pd_adjoint.cu": [],
 }
 HOST_UNITS = ["host/pd_deck.cpp", "host/pd_setup.cpp", "host/pdDataManager.cpp", "host/pd_host_capi.cpp"]
 

@@ -46,6 +46,19 @@ struct pd_ctx {
     double* dslits = nullptr;   // [nslit][6] on the device
     std::vector<pd::GaussConst> gch;            // Gauss constants (host copy)
     std::vector<double> bdry_host, sfac_host;   // per-node factors (host copies)
+    std::vector<int32_t> bc_host;               // per-node bc index
+    std::vector<int64_t> cbptr_host;            // MLS contributor CSR (host copy)
+    std::vector<int32_t> cbidx_host;
+    // adjoint: checkpoints (U, V, Gauss-point u, time) of the last forward
+    struct Checkpoint {
+        double *U = nullptr, *V = nullptr, *ug = nullptr;
+        double t = 0.0;
+    };
+    std::vector<Checkpoint> ckpt;
+    int adj_steps = 0, adj_every = 0, adj_acc = 0;
+    double adj_dt = 0.0;
+    int64_t *tptr = nullptr;
+    int32_t *tj = nullptr, *tpos = nullptr;
     bool have_family = false, have_mls = false;
     // owned device buffers
     std::vector<void*> owned;
@@ -392,6 +405,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
         for (int a = 0; a < 3; ++a) xs[a * N + i] = P->coords[3 * i + a];
     std::vector<int32_t> bcv(N, -1);
     if (P->bc_id) std::copy(P->bc_id, P->bc_id + N, bcv.begin());
+    c->bc_host = bcv;
     std::vector<double> ones(N, 1.0);
     if ((rc = upload(c, x, xs.data(), sizeof(double) * n3)) || (rc = upload(c, mat, P->mat_id, sizeof(int32_t) * N)) ||
         (rc = upload(c, bc, bcv.data(), sizeof(int32_t) * N)) ||
@@ -410,6 +424,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     // FP32-form constants: one material -> kernel constants; a failure test
     // only when some critical stretch is within reach
     d.multimat = P->num_materials > 1;
+    d.f64_lanes_below = int64_t(1) << 17;
     d.c0 = (float)P->materials[0].spring;
     d.e0 = (float)P->materials[0].ecrit;
     d.hasfail = 0;
@@ -641,6 +656,10 @@ int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const do
             cs[i * npt + g] = (float)(s - 1.0);
         }
     }
+    c->cbptr_host.assign(cb_ptr, cb_ptr + N + 1);
+    c->cbidx_host.assign(cb_idx, cb_idx + T);
+    dfree(c, c->tptr); dfree(c, c->tj); dfree(c, c->tpos);
+    c->tptr = nullptr; c->tj = nullptr; c->tpos = nullptr;
     dfree(c, c->cbptr); dfree(c, c->cbidx); dfree(c, c->coeff); dfree(c, c->coeff32); dfree(c, c->csum);
     c->cbptr = nullptr; c->cbidx = nullptr; c->coeff = nullptr; c->coeff32 = nullptr; c->csum = nullptr;
     PD_TRY(dalloc(c, &c->cbptr, N + 1));
@@ -664,9 +683,32 @@ int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const do
 }
 
 int pd_set_precision(pd_ctx* c, int p) {
-    if (!c || (p != PD_PREC_FP64 && p != PD_PREC_FP32C)) return fail(PD_ERR_ARG, "pd_set_precision: bad argument");
+    if (!c || (p != PD_PREC_FP64 && p != PD_PREC_FP32C && p != PD_PREC_FP64A))
+        return fail(PD_ERR_ARG, "pd_set_precision: bad argument");
     c->precision = p;
+    c->d.acc_stretch = p == PD_PREC_FP64A;
     return PD_OK;
+}
+
+int pd_set_option(pd_ctx* c, int option, int64_t value) {
+    if (!c) return fail(PD_ERR_ARG, "pd_set_option: null context");
+    switch (option) {
+        case PD_OPT_F64_LANES_BELOW:
+            if (value < 0) return fail(PD_ERR_ARG, "pd_set_option: negative value");
+            c->d.f64_lanes_below = value;
+            break;
+        default: return fail(PD_ERR_ARG, "pd_set_option: unknown option");
+    }
+    c->generation++;  // captured graphs hold the old launch choice
+    return PD_OK;
+}
+
+int pd_get_option(pd_ctx* c, int option, int64_t* value) {
+    if (!c || !value) return fail(PD_ERR_ARG, "pd_get_option: null argument");
+    switch (option) {
+        case PD_OPT_F64_LANES_BELOW: *value = c->d.f64_lanes_below; return PD_OK;
+        default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
+    }
 }
 
 int pd_set_energy(pd_ctx* c, int on) {
@@ -1033,7 +1075,7 @@ extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rto
     pd::launch_static_rhs(c->d, time, b, s);
     int it_total = 0;
     double rel = 0.0;
-    if (precision == PD_PREC_FP64) {
+    if (precision == PD_PREC_FP64 || precision == PD_PREC_FP64A) {
         rc = cg_device<double>(c, time, b, xd, r, p, q, rtol, maxit, &it_total, &rel, false);
     } else {
         // iterative refinement: FP64 residual, FP32 inner CG on the scaled residual
@@ -1080,4 +1122,259 @@ extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rto
     if (relres) *relres = rel;
     if (rc == PD_ERR_NOCONV) return fail(PD_ERR_NOCONV, "static solve did not reach the tolerance");
     return rc != PD_OK ? rc : rc2;
+}
+
+// ---------------------------------------------------------------- adjoint
+
+extern "C" int pd_set_spring_factor(pd_ctx* c, const double* f) {
+    if (!c || !f) return fail(PD_ERR_ARG, "pd_set_spring_factor: null argument");
+    for (int64_t i = 0; i < c->n; ++i)
+        if (!(f[i] > 0.0) || !std::isfinite(f[i])) return fail(PD_ERR_ARG, "pd_set_spring_factor: factors must be positive");
+    if (!c->d.sfac) {
+        double* sf = nullptr;
+        PD_TRY(dalloc(c, &sf, c->n));
+        c->d.sfac = sf;
+    }
+    PD_TRY(upload(c, (void*)c->d.sfac, f, sizeof(double) * c->n));
+    c->sfac_host.assign(f, f + c->n);
+    c->generation++;
+    return upload_static_f32(c);
+}
+
+namespace {
+
+// one RK4 step (as enqueue_step_body, FP64) that copies, before every force
+// evaluation, the state the force reads: U, the trial displacement and the
+// Gauss-point displacements (tape[s] = {U, us, ug} of stage s)
+void enqueue_step_tape(pd_ctx* c, double dt, double* tape) {
+    cudaStream_t s = c->stream;
+    const pd::Dev& d = c->d;
+    const int64_t n3 = 3 * c->n, ng = n3 * c->npt;
+    const int64_t per = 2 * n3 + ng;
+    auto copy = [&](int st) {
+        double* t = tape + (int64_t)(st - 1) * per;
+        cudaMemcpyAsync(t, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(t + n3, d.us, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(t + 2 * n3, d.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+    };
+    const double h = 0.5 * dt;
+    pd::launch_advance_time(d.tdev, dt, s);
+    cudaMemcpyAsync(d.vbuf, d.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.u1, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.us, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+    copy(1);
+    pd::launch_force_f64(d, h, s);
+    pd::launch_epilogue(d, 1, h, dt, s);
+    pd::launch_gather_f64(d, d.us, s);
+    copy(2);
+    pd::launch_force_f64(d, h, s);
+    pd::launch_epilogue(d, 2, h, dt, s);
+    pd::launch_gather_f64(d, d.us, s);
+    copy(3);
+    pd::launch_force_f64(d, dt, s);
+    pd::launch_epilogue(d, 3, dt, dt, s);
+    pd::launch_gather_f64(d, d.us, s);
+    copy(4);
+    pd::launch_force_f64(d, dt, s);
+    pd::launch_epilogue(d, 4, dt, dt, s);
+    pd::launch_gather_f64(d, d.U, s);
+}
+
+// transpose of the contributor lists of nodes without a boundary condition
+int build_transpose(pd_ctx* c) {
+    if (c->tptr) return PD_OK;
+    const int64_t N = c->n;
+    std::vector<int64_t> cnt(N + 1, 0);
+    for (int64_t j = 0; j < N; ++j) {
+        if (c->bc_host[j] >= 0) continue;
+        for (int64_t p = c->cbptr_host[j]; p < c->cbptr_host[j + 1]; ++p) cnt[c->cbidx_host[p] + 1]++;
+    }
+    for (int64_t k = 0; k < N; ++k) cnt[k + 1] += cnt[k];
+    std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+    std::vector<int32_t> tj(std::max<int64_t>(cnt[N], 1)), tpos(std::max<int64_t>(cnt[N], 1));
+    for (int64_t j = 0; j < N; ++j) {
+        if (c->bc_host[j] >= 0) continue;
+        for (int64_t p = c->cbptr_host[j]; p < c->cbptr_host[j + 1]; ++p) {
+            const int64_t k = c->cbidx_host[p];
+            tj[fill[k]] = (int32_t)j;
+            tpos[fill[k]] = (int32_t)(p - c->cbptr_host[j]);
+            fill[k]++;
+        }
+    }
+    PD_TRY(dalloc(c, &c->tptr, N + 1));
+    PD_TRY(dalloc(c, &c->tj, tj.size()));
+    PD_TRY(dalloc(c, &c->tpos, tpos.size()));
+    PD_TRY(upload(c, c->tptr, cnt.data(), sizeof(int64_t) * (N + 1)));
+    PD_TRY(upload(c, c->tj, tj.data(), sizeof(int32_t) * tj.size()));
+    PD_TRY(upload(c, c->tpos, tpos.data(), sizeof(int32_t) * tpos.size()));
+    return PD_OK;
+}
+
+void free_checkpoints(pd_ctx* c) {
+    for (auto& k : c->ckpt) {
+        dfree(c, k.U);
+        dfree(c, k.V);
+        dfree(c, k.ug);
+    }
+    c->ckpt.clear();
+}
+
+int save_checkpoint(pd_ctx* c, pd_ctx::Checkpoint& k) {
+    const int64_t n3 = 3 * c->n, ng = n3 * c->npt;
+    if (!k.U) {
+        PD_TRY(dalloc(c, &k.U, n3));
+        PD_TRY(dalloc(c, &k.V, n3));
+        PD_TRY(dalloc(c, &k.ug, ng));
+    }
+    cudaStream_t s = c->stream;
+    PD_CUDA_TRY(cudaMemcpyAsync(k.U, c->d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(k.V, c->d.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(k.ug, c->d.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, c->d.tdev, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PD_CUDA_TRY(cudaStreamSynchronize(s));
+    k.t = c->hscalar[0];
+    return PD_OK;
+}
+
+}  // namespace
+
+// Forward run of nsteps FP64 RK4 steps from the current state, keeping a
+// checkpoint (U, V, Gauss-point u, time) every checkpoint_every steps for
+// pd_adjoint_backward.  PD_PREC_FP64A stays FP64A; any other precision
+// runs as PD_PREC_FP64.
+extern "C" int pd_adjoint_forward(pd_ctx* c, double dt, double t0, int nsteps, int every) {
+    if (!c || nsteps < 1 || every < 1) return fail(PD_ERR_ARG, "pd_adjoint_forward: bad argument");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_adjoint_forward: family/MLS data not set");
+    if (c->d.cci) return fail(PD_ERR_ARG, "pd_adjoint_forward: the adjoint covers the Gauss-point (FGI) scheme");
+    const int prec = c->precision, energy = c->d.energy;
+    if (prec != PD_PREC_FP64A) c->precision = PD_PREC_FP64;
+    c->adj_acc = c->d.acc_stretch = prec == PD_PREC_FP64A;
+    c->d.energy = 0;
+    free_checkpoints(c);
+    const int nck = (nsteps + every - 1) / every;
+    c->ckpt.resize(nck);
+    int rc = set_time(c, t0);
+    int done = 0;
+    for (int k = 0; k < nck && rc == PD_OK; ++k) {
+        rc = save_checkpoint(c, c->ckpt[k]);
+        if (rc != PD_OK) break;
+        const int n = std::min(every, nsteps - done);
+        rc = pd_rk4_steps(c, dt, c->ckpt[k].t, n);
+        done += n;
+    }
+    if (rc == PD_OK) {
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) rc = pd::fail_cuda(e, "adjoint forward", __FILE__, __LINE__);
+    }
+    c->precision = prec;
+    c->d.energy = energy;
+    c->adj_steps = rc == PD_OK ? nsteps : 0;
+    c->adj_every = every;
+    c->adj_dt = dt;
+    return rc;
+}
+
+// Reverse sweep of the last pd_adjoint_forward.  lam_U, lam_V: adjoints of
+// the final U and V ([3N] host, V may be NULL); grad_f [N] receives the
+// gradient with respect to the per-node spring factors.  Leaves the state
+// at the start of the forward run.
+extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double* lam_V, double* grad_f) {
+    if (!c || !lam_U || !grad_f) return fail(PD_ERR_ARG, "pd_adjoint_backward: null argument");
+    if (c->adj_steps < 1) return fail(PD_ERR_ARG, "pd_adjoint_backward: no forward run to reverse");
+    if (!c->d.sfac) return fail(PD_ERR_ARG, "pd_adjoint_backward: set the spring factors first");
+    if (c->d.mls) PD_TRY(build_transpose(c));
+    const int64_t N = c->n, n3 = 3 * N, ng = n3 * c->npt;
+    cudaStream_t s = c->stream;
+    const pd::Dev& d = c->d;
+    const double dt = c->adj_dt;
+    // work buffers
+    std::vector<double*> bufs;
+    auto get = [&](int64_t count) -> double* {
+        double* p = nullptr;
+        if (dalloc(c, &p, count) != PD_OK) return nullptr;
+        bufs.push_back(p);
+        return p;
+    };
+    pd::AdjBuf A;
+    double** fields[] = {&A.lU, &A.lV, &A.lvb, &A.lu1, &A.lk1, &A.lk2, &A.lk3, &A.lk4, &A.lus, &A.lF, &A.lueff};
+    bool ok = true;
+    for (double** f : fields) ok = ok && ((*f = get(n3)) != nullptr);
+    double* lUp = get(n3);
+    double* lVp = get(n3);
+    double* lugSp = get(ng);
+    double* lug = get(ng);
+    double* lugSn = get(ng);
+    double* gradf = get(N);
+    const int every = c->adj_every;
+    const int64_t per = 2 * n3 + ng;
+    double* tape = get((int64_t)every * 4 * per);
+    auto release = [&]() {
+        for (double* p : bufs) dfree(c, p);
+    };
+    if (!ok || !lUp || !lVp || !lugSp || !lug || !lugSn || !gradf || !tape) {
+        release();
+        return fail(PD_ERR_OOM, "pd_adjoint_backward: device memory for the tape");
+    }
+    const int energy = c->d.energy, acc = c->d.acc_stretch;
+    c->d.energy = 0;  // the recomputed steps need no energy density
+    c->d.acc_stretch = c->adj_acc;  // and use the forward run's arithmetic
+    int rc = upload_vec3(c, lUp, lam_U);
+    if (rc == PD_OK && lam_V) rc = upload_vec3(c, lVp, lam_V);
+    if (rc == PD_OK && !lam_V) rc = cudaMemsetAsync(lVp, 0, sizeof(double) * n3, s) == cudaSuccess ? PD_OK : PD_ERR_CUDA;
+    cudaMemsetAsync(lugSp, 0, sizeof(double) * ng, s);
+    cudaMemsetAsync(gradf, 0, sizeof(double) * N, s);
+    const int nck = (int)c->ckpt.size();
+    for (int k = nck - 1; k >= 0 && rc == PD_OK; --k) {
+        const pd_ctx::Checkpoint& K = c->ckpt[k];
+        const int S = std::min(every, c->adj_steps - k * every);
+        // restore the segment's start and recompute it with the stage tape
+        cudaMemcpyAsync(d.U, K.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d.V, K.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d.ug, K.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+        rc = set_time(c, K.t);
+        for (int n = 0; n < S && rc == PD_OK; ++n) enqueue_step_tape(c, dt, tape + (int64_t)n * 4 * per);
+        // reverse the segment's steps
+        for (int n = S - 1; n >= 0 && rc == PD_OK; --n) {
+            const double* tp = tape + (int64_t)n * 4 * per;
+            auto teU = [&](int st) { return tp + (int64_t)(st - 1) * per; };
+            auto teus = [&](int st) { return tp + (int64_t)(st - 1) * per + n3; };
+            auto teug = [&](int st) { return tp + (int64_t)(st - 1) * per + 2 * n3; };
+            pd::launch_gather_T(d, c->tptr, c->tj, c->tpos, lugSp, lUp, s);
+            pd::launch_adj_combine(d, dt, lUp, lVp, A, s);
+            double* lk_of[5] = {nullptr, A.lk1, A.lk2, A.lk3, A.lk4};
+            const double alpha[5] = {0.0, 0.0, 0.5, 0.5, 1.0};
+            for (int st = 4; st >= 2; --st) {
+                const double dts = st >= 3 ? dt : 0.5 * dt;
+                pd::launch_adj_stage_pre(d, dts, lk_of[st], A, s);
+                pd::launch_vjp_own(d, teU(st), teus(st), teug(st), A.lF, A.lueff, gradf, s);
+                pd::launch_vjp_partner(d, teU(st), teus(st), teug(st), A.lF, lug, gradf, s);
+                pd::launch_adj_stage_node(d, A, s);
+                pd::launch_gather_T(d, c->tptr, c->tj, c->tpos, lug, A.lus, s);
+                pd::launch_adj_stage_post(d, alpha[st], lk_of[st - 1], A, s);
+            }
+            pd::launch_adj_stage_pre(d, 0.5 * dt, A.lk1, A, s);
+            pd::launch_vjp_own(d, teU(1), teus(1), teug(1), A.lF, A.lueff, gradf, s);
+            pd::launch_vjp_partner(d, teU(1), teus(1), teug(1), A.lF, lugSn, gradf, s);
+            pd::launch_adj_stage1_end(d, A, s);
+            cudaMemcpyAsync(lUp, A.lU, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(lVp, A.lV, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+            std::swap(lugSp, lugSn);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = pd::fail_cuda(e, "adjoint step", __FILE__, __LINE__);
+        }
+    }
+    if (rc == PD_OK) {
+        // leave the state at the start of the forward run
+        const pd_ctx::Checkpoint& K = c->ckpt[0];
+        cudaMemcpyAsync(d.U, K.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d.V, K.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d.ug, K.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(grad_f, gradf, sizeof(double) * N, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = pd::fail_cuda(e, "adjoint backward", __FILE__, __LINE__);
+    }
+    release();
+    c->d.energy = energy;
+    c->d.acc_stretch = acc;
+    return rc;
 }

@@ -43,11 +43,20 @@ __device__ __forceinline__ double beta_factor(double dist, double delta, double 
 
 // ------------------------------------------------------------------ force
 
+
+// p - r = (p^2 - r^2) / (p + r) with p^2 - r^2 = eta.(2 xi + eta): no
+// cancellation when the strain is small (PD_PREC_FP64A)
+__device__ __forceinline__ double extension(double x0, double x1, double x2, double e0, double e1, double e2,
+                                            double r, double p) {
+    const double q = e0 * (2.0 * x0 + e0) + e1 * (2.0 * x1 + e1) + e2 * (2.0 * x2 + e2);
+    return q / (p + r);
+}
+
 // One thread per node.  FGI: the Gauss-point summation branch of
 // CalcBondBasedMotionRK4 (pdDataManager.cpp:1917-1962) with the per-point
 // CalcBondForceCCI (pdDataManager2.cpp:1293-1351).  CCI: the one-point
 // branch (pdDataManager.cpp:1818-1866).
-template <bool CCI, bool ENERGY, bool SFAC>
+template <bool CCI, bool ENERGY, bool SFAC, bool ACC>
 __global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
     extern __shared__ GaussConst sg[];
     for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
@@ -87,7 +96,7 @@ __global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
             const double pl = sqrt(y0 * y0 + y1 * y1 + y2 * y2);
             const double dxe = 2.0 * d.dx / 2.0;
             const double beta = beta_factor(r, d.delta, dxe, cci_orig);
-            const double u = pl - r;
+            const double u = ACC ? extension(xv0, xv1, xv2, ev0, ev1, ev2, r, pl) : pl - r;
             const double s = u / r;
             if (u <= 0.0 || (u > 0.0 && s <= ecrit)) {
                 const double t = bE * d.vol_cci * beta * c * s;
@@ -110,7 +119,7 @@ __global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
                 const double y0 = xv0 + ev0, y1 = xv1 + ev1, y2 = xv2 + ev2;
                 const double pl = sqrt(y0 * y0 + y1 * y1 + y2 * y2);
                 const double beta = beta_factor(r, d.delta, G.dxe, false);
-                const double u = pl - r;
+                const double u = ACC ? extension(xv0, xv1, xv2, ev0, ev1, ev2, r, pl) : pl - r;
                 const double s = u / r;
                 double f0 = 0.0, f1 = 0.0, f2 = 0.0;
                 if (u <= 0.0 || (u > 0.0 && s <= ecrit)) {
@@ -135,6 +144,95 @@ __global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
     d.vbuf[N + i] = v1;
     d.vbuf[2 * N + i] = v2;
     if (ENERGY) d.eed[i] = eacc;
+}
+
+// FGI with eight lanes per node: lane l evaluates the Gauss points l, l+8,
+// ... of every bond; the bond's force is then summed point by point in the
+// reference's order (F += W_g f_g for g = 0, 1, ...) by passing each lane's
+// product along the group with shuffles, so every lane holds the same F and
+// the velocity update (F + b) dt/rho per bond is the reference's, bit for bit.
+// More threads than k_force_f64 for the same work: the choice for lattices
+// too small to fill the GPU with one thread per node.
+template <bool ENERGY, bool SFAC, bool ACC>
+__global__ void __launch_bounds__(128) k_force_f64_lanes(Dev d, double dts) {
+    extern __shared__ GaussConst sg[];
+    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t slot = t >> 3;
+    const int lane = threadIdx.x & 7;
+    if (slot >= N) return;  // whole groups of 8 leave together
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const int64_t i = d.order[slot];
+    const MatDev Mi = d.mats[d.mat[i]];
+    const double rho = Mi.density;
+    const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
+    const bool bci = d.bc[i] >= 0;
+    const double* src = bci ? d.U : d.us;
+    const double ui0 = src[i], ui1 = src[N + i], ui2 = src[2 * N + i];
+    const double xi0 = d.x[i], xi1 = d.x[N + i], xi2 = d.x[2 * N + i];
+    const double bEi = d.bdry[i];
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
+    double eacc = ENERGY ? d.eed[i] : 0.0;
+    const int npt = d.npt;
+    const int64_t pe = d.arow[i + 1];
+    for (int64_t p = d.arow[i]; p < pe; ++p) {
+        const int64_t j = d.acol[p];
+        const MatDev& Mj = d.mats[d.mat[j]];
+        const double ecrit = dmin(Mi.ecrit, Mj.ecrit);
+        double c = dmin(Mi.spring, Mj.spring);
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const double bE = 0.5 * (bEi + d.bdry[j]);
+        const double xj0 = d.x[j], xj1 = d.x[N + j], xj2 = d.x[2 * N + j];
+        double F0 = 0.0, F1 = 0.0, F2 = 0.0;
+        for (int base = 0; base < npt; base += 8) {
+            const int g = base + lane;
+            double w0 = 0.0, w1 = 0.0, w2 = 0.0, el = 0.0;
+            if (g < npt) {
+                const GaussConst& G = sg[g];
+                const double xv0 = (G.hg[0] + xj0) - xi0;
+                const double xv1 = (G.hg[1] + xj1) - xi1;
+                const double xv2 = (G.hg[2] + xj2) - xi2;
+                const double* ugp = d.ug + (int64_t)(3 * g) * N + j;
+                const double ev0 = ugp[0] - ui0, ev1 = ugp[N] - ui1, ev2 = ugp[2 * N] - ui2;
+                const double r = sqrt(xv0 * xv0 + xv1 * xv1 + xv2 * xv2);
+                const double y0 = xv0 + ev0, y1 = xv1 + ev1, y2 = xv2 + ev2;
+                const double pl = sqrt(y0 * y0 + y1 * y1 + y2 * y2);
+                const double beta = beta_factor(r, d.delta, G.dxe, false);
+                const double u = ACC ? extension(xv0, xv1, xv2, ev0, ev1, ev2, r, pl) : pl - r;
+                const double s = u / r;
+                double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+                if (u <= 0.0 || (u > 0.0 && s <= ecrit)) {
+                    const double tt = bE * beta * c * s;
+                    f0 = tt * y0 / pl;
+                    f1 = tt * y1 / pl;
+                    f2 = tt * y2 / pl;
+                    if (ENERGY) el = bE * 0.5 * (0.5 * beta * (c / r) * u * u) * G.pw3;
+                }
+                w0 = G.W * f0;
+                w1 = G.W * f1;
+                w2 = G.W * f2;
+            }
+            const int cnt = npt - base < 8 ? npt - base : 8;
+            for (int l = 0; l < cnt; ++l) {
+                F0 += __shfl_sync(gmask, w0, l, 8);
+                F1 += __shfl_sync(gmask, w1, l, 8);
+                F2 += __shfl_sync(gmask, w2, l, 8);
+                if (ENERGY) eacc += __shfl_sync(gmask, el, l, 8);
+            }
+        }
+        v0 += (F0 + b0) * dts / rho;
+        v1 += (F1 + b1) * dts / rho;
+        v2 += (F2 + b2) * dts / rho;
+    }
+    if (lane == 0) {
+        d.vbuf[i] = v0;
+        d.vbuf[N + i] = v1;
+        d.vbuf[2 * N + i] = v2;
+        if (ENERGY) d.eed[i] = eacc;
+    }
 }
 
 // ----------------------------------------------------------------- gather
@@ -352,7 +450,23 @@ void launch_force_f64(const Dev& d, double dts, cudaStream_t s) {
     size_t sh = (size_t)d.npt * sizeof(GaussConst);
     unsigned nb = blocks_for(d.n, bs);
     const bool sf = d.sfac != nullptr;
-#define PD_FORCE(C, E, S) k_force_f64<C, E, S><<<nb, bs, sh, s>>>(d, dts)
+    if (!d.cci && d.npt >= 8 && d.n < d.f64_lanes_below) {
+        const unsigned nb8 = blocks_for(8 * d.n, bs);
+#define PD_FORCE_L(E, S)                                                                  \
+    do {                                                                                  \
+        if (d.acc_stretch) k_force_f64_lanes<E, S, true><<<nb8, bs, sh, s>>>(d, dts);    \
+        else k_force_f64_lanes<E, S, false><<<nb8, bs, sh, s>>>(d, dts);                 \
+    } while (0)
+        if (d.energy) { if (sf) PD_FORCE_L(true, true); else PD_FORCE_L(true, false); }
+        else { if (sf) PD_FORCE_L(false, true); else PD_FORCE_L(false, false); }
+#undef PD_FORCE_L
+        return;
+    }
+#define PD_FORCE(C, E, S)                                                     \
+    do {                                                                      \
+        if (d.acc_stretch) k_force_f64<C, E, S, true><<<nb, bs, sh, s>>>(d, dts); \
+        else k_force_f64<C, E, S, false><<<nb, bs, sh, s>>>(d, dts);          \
+    } while (0)
     if (d.cci) {
         if (d.energy) { if (sf) PD_FORCE(true, true, true); else PD_FORCE(true, true, false); }
         else { if (sf) PD_FORCE(true, false, true); else PD_FORCE(true, false, false); }

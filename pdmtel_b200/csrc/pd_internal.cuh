@@ -100,6 +100,8 @@ struct Dev {
     // when every node sits on one cubic lattice of spacing dx; else nullptr
     const int32_t* lat;
     float c0, e0;             // spring and critical stretch when there is one material
+    int acc_stretch;          // FP64 force: extension as (2 xi.eta + eta.eta)/(p + r)
+    int64_t f64_lanes_below;  // FGI FP64 force: eight lanes per node below this many nodes
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -145,6 +147,23 @@ constexpr int kDotBlocks = 296;
 void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
 void launch_static_apply_f32(const Dev& d, double t, const float* x, float* y, cudaStream_t s);
 void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s);
+
+// adjoint (pd_adjoint.cu): per-node adjoint vectors [3][N] of one RK4 step
+struct AdjBuf {
+    double *lU, *lV, *lvb, *lu1, *lk1, *lk2, *lk3, *lk4, *lus, *lF, *lueff;
+};
+void launch_vjp_own(const Dev& d, const double* teU, const double* teus, const double* teug, const double* lamF,
+                    double* lam_u, double* gradf, cudaStream_t s);
+void launch_vjp_partner(const Dev& d, const double* teU, const double* teus, const double* teug, const double* lamF,
+                        double* lam_ug, double* gradf, cudaStream_t s);
+void launch_gather_T(const Dev& d, const int64_t* tptr, const int32_t* tj, const int32_t* tpos, const double* lam_ug,
+                     double* lam_us, cudaStream_t s);
+void launch_adj_combine(const Dev& d, double dt, const double* lUp, const double* lVp, const AdjBuf& A,
+                        cudaStream_t s);
+void launch_adj_stage_pre(const Dev& d, double dts, const double* lk, const AdjBuf& A, cudaStream_t s);
+void launch_adj_stage_node(const Dev& d, const AdjBuf& A, cudaStream_t s);
+void launch_adj_stage_post(const Dev& d, double alpha, double* lk_prev, const AdjBuf& A, cudaStream_t s);
+void launch_adj_stage1_end(const Dev& d, const AdjBuf& A, cudaStream_t s);
 
 // scans and reductions (pd_fast.cu)
 int exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);  // out has n+1 entries

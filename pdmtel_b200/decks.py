@@ -177,6 +177,17 @@ def config_plate(dims=(400, 400, 4), spacing=5e-4, slit_half_length=0.02, vel=0.
                 bdry_eff=0, intg_point=2)
 
 
+def config_identify(dims=(64, 64, 8), spacing=1e-3, vel=0.02, dt=5e-8, steps=1000) -> Deck:
+    """The identification specimen: low-x face fixed (DISPL 0 in xyz), the
+    high-x face pulled at vel along x (VELOC), Gauss-point integration with
+    2x2x2 points and MLS."""
+    bcs = [BC(DISPL, (1, 1, 1), (0.0, 0.0, 0.0), 1.0, 2.0), BC(VELOC, (1, 0, 0), (vel, 0.0, 0.0), 1.0, 2.0)]
+    return Deck(dims=dims, spacing=spacing, horizon=3.015 * spacing, total_time=1.0, total_step=steps,
+                fixed_dt=dt, bcs=bcs,
+                bc_spaces=[Space(1, face_box(dims, spacing, 0, -1)), Space(2, face_box(dims, spacing, 0, +1))],
+                bdry_eff=0, intg_point=2)
+
+
 def config_cube(n=128, spacing=1e-3, traction=1e6) -> Deck:
     """The static cube: bottom face (low z) clamped, top face under a shear
     traction along x."""

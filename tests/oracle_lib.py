@@ -57,6 +57,8 @@ def lib():
         L.or_static_rhs.argtypes = [C.POINTER(OrModel), C.c_double, _d]
         L.or_static_cg.argtypes = [C.POINTER(OrModel), C.c_double, _d, _d, C.c_double, C.c_int, _d]
         L.or_static_cg.restype = C.c_int
+        L.or_adjoint_grad.argtypes = [C.POINTER(OrModel), C.c_double, C.c_double, C.c_int, _d, _d, _d]
+        L.or_adjoint_grad.restype = C.c_int
         _lib = L
     return _lib
 
@@ -209,6 +211,15 @@ class Model:
         b = np.zeros(3 * self.m.n)
         lib().or_static_rhs(self.ref, t, ptr(b, _d))
         return b
+
+    def adjoint_grad(self, dt, t0, nsteps, lam_U, lam_V=None):
+        lu = np.ascontiguousarray(lam_U, dtype=np.float64)
+        lv = None if lam_V is None else np.ascontiguousarray(lam_V, dtype=np.float64)
+        g = np.zeros(self.m.n)
+        rc = lib().or_adjoint_grad(self.ref, dt, t0, int(nsteps), ptr(lu, _d), ptr(lv, _d), ptr(g, _d))
+        if rc != 0:
+            raise MemoryError("or_adjoint_grad")
+        return g
 
     def static_cg(self, t, b, rtol=1e-10, maxit=100000):
         x = np.zeros(3 * self.m.n)
