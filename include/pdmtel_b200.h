@@ -234,12 +234,51 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
                     double* relres);
 
 /* ---- Tuning options (no counterpart in the reference) ----
+ * None of them changes a result; they change launch shapes only.
  * PD_OPT_F64_LANES_BELOW: the FP64 Gauss-point force runs eight lanes per
  *   node (same arithmetic, same order) when the problem has fewer nodes than
- *   this, one thread per node otherwise.  Default 131072. */
-enum { PD_OPT_F64_LANES_BELOW = 1 };
+ *   this, one thread per node otherwise.  Default 131072.
+ * PD_OPT_TILE: the node work order walks lattice tiles of 2^bx x 2^by x 2^bz
+ *   nodes, value = bx | by << 8 | bz << 16 (1 <= bx <= 6, by, bz <= 6).
+ *   Default 8 x 4 x 4.
+ * PD_OPT_PERSIST_BLOCKS_PER_SM: blocks per SM of the persistent launch (0:
+ *   as many as fit).
+ * PD_OPT_PERSIST_FORCE_CHUNK / _GATHER_CHUNK: work items a block takes from
+ *   the queue at a time (multiples of 128; defaults 128 and 256). */
+enum {
+    PD_OPT_F64_LANES_BELOW = 1,
+    PD_OPT_TILE = 2,
+    PD_OPT_PERSIST_BLOCKS_PER_SM = 3,
+    PD_OPT_PERSIST_FORCE_CHUNK = 4,
+    PD_OPT_PERSIST_GATHER_CHUNK = 5
+};
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
+
+/* ---- Batching: persistent stepping and the autotuner (no counterpart in the
+ * reference) ----
+ * A batch of specimens is one context whose family has no bond between
+ * specimens (the host layer places them apart), so every entry point above
+ * steps all specimens at once.  pd_rk4_steps_persistent runs nsteps steps of
+ * the FP32-compensated form in ONE cooperative launch (every block resident;
+ * work taken from per-phase queues; grid barriers between the force and the
+ * gather phases give up after 4 s with PD_ERR_TIMEOUT), captured into a CUDA
+ * graph per (dt, nsteps, launch shape).  Needs PD_PREC_FP32C, 2x2x2 Gauss
+ * points and energy accumulation off; same result bit for bit as
+ * pd_rk4_steps.  Synchronous. */
+int pd_rk4_steps_persistent(pd_ctx* ctx, double dt, double t0, int nsteps);
+typedef struct pd_tune_result {
+    int64_t tile;          /* PD_OPT_TILE value kept */
+    int32_t persistent;    /* 1: the persistent launch was fastest */
+    int32_t blocks_per_sm; /* PD_OPT_PERSIST_BLOCKS_PER_SM kept */
+    int32_t force_chunk, gather_chunk;
+    int32_t trials;
+    double ms_per_step;    /* device time per step of the kept shape */
+} pd_tune_result;
+/* Times candidate launch shapes (node-order tiles; for the persistent launch
+ * blocks per SM and queue chunks) over `steps` steps each from the current
+ * state, keeps the fastest in the context and restores the state. */
+int pd_autotune(pd_ctx* ctx, double dt, int steps, pd_tune_result* out);
 
 /* ---- Differentiation: gradient with respect to a per-node micromodulus ----
  *

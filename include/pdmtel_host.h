@@ -31,6 +31,8 @@ typedef struct pdh_info {
     int32_t total_step, dump_frequency, num_max_family;
     double grid_spacing, horizon, total_time, stable_dt, min_bond_length;
     double ke, ee;            /* energies of the last RK4 step */
+    int32_t num_materials, num_bcs, intg_point, pad;
+    double damping;
 } pdh_info;
 
 /* SetWkDir + ReadInputFile (pdDataManager.cpp:4-758): dir holds pds_input.txt */
@@ -38,6 +40,22 @@ int pdh_open(const char* dir, pdh_model** out);
 int pdh_close(pdh_model* m);
 const char* pdh_last_error(pdh_model* m);
 int pdh_get_info(pdh_model* m, pdh_info* info);
+
+/* Batching (no counterpart in the reference): one model over `count`
+ * specimen models opened with pdh_open (decks read; InitNode and
+ * InitMaterial run here when not yet).  The specimens are placed side by side
+ * on one lattice with gaps wider than the horizon, so pdh_init_bond finds no
+ * bond between them, and pdh_init_integration_point solves each specimen's
+ * MLS in its own coordinates.  Node ids run specimen by specimen
+ * (pdh_batch_offsets, count + 1 entries).  Spring factors set on a specimen
+ * (pdh_set_spring_factor) carry over.  All specimens must share the grid
+ * spacing, horizon, integration scheme and damping, without boundary effect
+ * factors.  out_dir receives the batch's log; the specimen models stay the
+ * caller's.  Then continue as for one model: pdh_init_bond,
+ * pdh_init_integration_point, pdh_context, the solve entry points. */
+int pdh_batch_create(const char* out_dir, pdh_model* const* specimens, int count, pdh_model** out);
+int pdh_batch_offsets(pdh_model* m, int64_t* offsets);
+int pdh_batch_count(pdh_model* m, int* count);
 
 /* the steps of pdSolve::InitialProblem (pdSolve.cpp:10-22) */
 int pdh_init_node(pdh_model* m);
@@ -58,6 +76,10 @@ int pdh_get_nodes(pdh_model* m, double* coords, int32_t* mat, int32_t* bc);
 int pdh_get_family(pdh_model* m, int64_t* row_ptr, int32_t* col, uint8_t* broken);
 int pdh_get_bdry_eff(pdh_model* m, double* bE);
 int pdh_get_mls(pdh_model* m, int64_t* cb_ptr, int32_t* cb_idx, double* coeff);
+/* the tables the device context is built from: materials (spring constant as
+ * InitMaterial sets it, pdDataManager.cpp:1310-1322), boundary conditions,
+ * and the 1-D Gauss rule (intg_point abscissae and weights) */
+int pdh_get_tables(pdh_model* m, pd_material* materials, pd_bc* bcs, double* abscissae, double* weights);
 
 /* the device context of the model (uploads the setup on first use) */
 int pdh_context(pdh_model* m, pd_ctx** ctx);

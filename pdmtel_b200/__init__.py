@@ -28,7 +28,8 @@ LIB_PATH = os.path.join(HERE, "libpdmtel_b200.so")
 
 PD_OK = 0
 PREC_FP64, PREC_FP32C, PREC_FP64A = 0, 1, 2
-OPT_F64_LANES_BELOW = 1
+OPT_F64_LANES_BELOW, OPT_TILE, OPT_PERSIST_BLOCKS_PER_SM = 1, 2, 3
+OPT_PERSIST_FORCE_CHUNK, OPT_PERSIST_GATHER_CHUNK = 4, 5
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}
@@ -71,7 +72,15 @@ class pdh_info(C.Structure):
                 ("bdry_eff_on", C.c_int32), ("dims", C.c_int32 * 3), ("total_step", C.c_int32),
                 ("dump_frequency", C.c_int32), ("num_max_family", C.c_int32), ("grid_spacing", C.c_double),
                 ("horizon", C.c_double), ("total_time", C.c_double), ("stable_dt", C.c_double),
-                ("min_bond_length", C.c_double), ("ke", C.c_double), ("ee", C.c_double)]
+                ("min_bond_length", C.c_double), ("ke", C.c_double), ("ee", C.c_double),
+                ("num_materials", C.c_int32), ("num_bcs", C.c_int32), ("intg_point", C.c_int32),
+                ("pad", C.c_int32), ("damping", C.c_double)]
+
+
+class pd_tune_result(C.Structure):
+    _fields_ = [("tile", C.c_int64), ("persistent", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("force_chunk", C.c_int32), ("gather_chunk", C.c_int32), ("trials", C.c_int32),
+                ("ms_per_step", C.c_double)]
 
 
 # name -> argtypes; every entry point returns int
@@ -131,6 +140,12 @@ _SIGS = {
     "pdh_set_precision": [_vp, C.c_int],
     "pdh_solve_dynamic": [_vp, C.c_int],
     "pdh_solve_static": [_vp, C.c_int, C.c_double, C.POINTER(C.c_int), _d],
+    "pdh_batch_create": [C.c_char_p, C.POINTER(_vp), C.c_int, C.POINTER(_vp)],
+    "pdh_batch_offsets": [_vp, _i64],
+    "pdh_batch_count": [_vp, C.POINTER(C.c_int)],
+    "pdh_get_tables": [_vp, C.POINTER(pd_material), C.POINTER(pd_bc), _d, _d],
+    "pd_rk4_steps_persistent": [_vp, C.c_double, C.c_double, C.c_int],
+    "pd_autotune": [_vp, C.c_double, C.c_int, C.POINTER(pd_tune_result)],
 }
 
 _lib: Optional[C.CDLL] = None
@@ -399,6 +414,14 @@ class DeviceContext:
         _check(lib().pd_get_option(self.h, int(option), C.byref(v)), "pd_get_option")
         return v.value
 
+    def rk4_steps_persistent(self, dt, t0, nsteps):
+        _check(lib().pd_rk4_steps_persistent(self.h, float(dt), float(t0), int(nsteps)), "pd_rk4_steps_persistent")
+
+    def autotune(self, dt, steps=3):
+        R = pd_tune_result()
+        _check(lib().pd_autotune(self.h, float(dt), int(steps), C.byref(R)), "pd_autotune")
+        return {k: getattr(R, k) for k, _ in R._fields_}
+
     def set_spring_factor(self, f):
         fa = _f64(f, self.n)
         _check(lib().pd_set_spring_factor(self.h, _p(fa, _d)), "pd_set_spring_factor")
@@ -426,6 +449,41 @@ class pdDataManager:
         rc = lib().pdh_open(os.fsencode(os.path.abspath(workdir)), C.byref(h))
         self.h = h
         _check(rc, "pdh_open", self.h)
+
+    @classmethod
+    def batch(cls, out_dir: str, specimens):
+        """One model over the specimen models (pdh_batch_create); the
+        specimens must stay open while the batch lives."""
+        os.makedirs(out_dir, exist_ok=True)
+        arr = (_vp * len(specimens))(*[s.h for s in specimens])
+        obj = cls.__new__(cls)
+        obj._specimens = list(specimens)
+        h = _vp()
+        rc = lib().pdh_batch_create(os.fsencode(os.path.abspath(out_dir)), arr, len(specimens), C.byref(h))
+        obj.h = h
+        _check(rc, "pdh_batch_create", obj.h)
+        return obj
+
+    def batch_offsets(self):
+        k = C.c_int(0)
+        self._call("pdh_batch_count", C.byref(k))
+        o = np.zeros(k.value + 1, np.int64)
+        self._call("pdh_batch_offsets", _p(o, _i64))
+        return o
+
+    def tables(self):
+        """(materials, bcs, abscissae, weights) as the device context gets them"""
+        I = self.info()
+        mats = (pd_material * max(I.num_materials, 1))()
+        bcs = (pd_bc * max(I.num_bcs, 1))()
+        n1 = max(I.intg_point, 1)
+        ab, wt = np.zeros(n1), np.zeros(n1)
+        self._call("pdh_get_tables", mats, bcs, _p(ab, _d), _p(wt, _d))
+        ml = [{"spring": m.spring, "density": m.density, "ecrit": m.ecrit, "grav": tuple(m.grav)}
+              for m in list(mats)[:I.num_materials]]
+        bl = [{"type": b.type, "dir": tuple(b.dir), "value": tuple(b.value), "end_time": b.end_time,
+               "load_type": b.load_type} for b in list(bcs)[:I.num_bcs]]
+        return ml, bl, ab, wt
 
     def close(self):
         if self.h:

@@ -8,6 +8,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <array>
 #include <sstream>
 #include <thread>
 
@@ -55,6 +56,16 @@ int pdDataManager::SetWkDir(const std::string& dir) {
     std::ifstream in(_inFilePath.c_str());
     if (!in) return Error(PD_ERR_ARG, "SetWkDir: input file not exits! " + _inFilePath);
     std::ofstream out(_outFilePath.c_str(), std::ios::out);
+    return PD_OK;
+}
+
+int pdDataManager::SetOutputDir(const std::string& dir) {
+    _workDir = dir;
+    if (!_workDir.empty() && _workDir.back() != '/') _workDir += '/';
+    _inFilePath.clear();
+    _outFilePath = _workDir + "pds_output.dat";
+    std::ofstream out(_outFilePath.c_str(), std::ios::out);
+    if (!out) return Error(PD_ERR_ARG, "SetOutputDir: cannot write " + _outFilePath);
     return PD_OK;
 }
 
@@ -293,10 +304,8 @@ int pdDataManager::InitNode() {
     return PD_OK;
 }
 
-int pdDataManager::EnsureContext() {
-    if (_ctx) return PD_OK;
-    if (!_nodesDone) return Error(PD_ERR_ARG, "EnsureContext: InitNode first");
-    std::vector<pd_material> mats(_mats.size());
+void pdDataManager::DeviceTables(std::vector<pd_material>& mats, std::vector<pd_bc>& bcs) const {
+    mats.assign(_mats.size(), pd_material{});
     for (size_t k = 0; k < _mats.size(); ++k) {
         const Material& m = _mats[k];
         // spring constant as InitMaterial sets it (pdDataManager.cpp:1310-1322)
@@ -305,7 +314,7 @@ int pdDataManager::EnsureContext() {
         mats[k].ecrit = m.ecrit;
         for (int a = 0; a < 3; ++a) mats[k].grav[a] = m.grav[a];
     }
-    std::vector<pd_bc> bcs(_bcs.size());
+    bcs.assign(_bcs.size(), pd_bc{});
     for (size_t k = 0; k < _bcs.size(); ++k) {
         std::memset(&bcs[k], 0, sizeof(pd_bc));
         bcs[k].type = _bcs[k].type;
@@ -314,6 +323,14 @@ int pdDataManager::EnsureContext() {
         bcs[k].end_time = _bcs[k].end_time;
         bcs[k].load_type = _bcs[k].load_type;
     }
+}
+
+int pdDataManager::EnsureContext() {
+    if (_ctx) return PD_OK;
+    if (!_nodesDone) return Error(PD_ERR_ARG, "EnsureContext: InitNode first");
+    std::vector<pd_material> mats;
+    std::vector<pd_bc> bcs;
+    DeviceTables(mats, bcs);
     pd_problem P;
     std::memset(&P, 0, sizeof P);
     P.num_nodes = _numNodes;
@@ -487,10 +504,16 @@ int pdDataManager::InitGridBoundary() { return PD_OK; }
 int pdDataManager::InitIntegrationPoint() {
     if (!_mlsOn) return PD_OK;
     if (!_bondsDone) return Error(PD_ERR_ARG, "InitIntegrationPoint: bonds first");
-    mls_contributors(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _rw, _cbPtr, _cbIdx);
     int64_t bad = -1;
-    int rc = mls_coefficients(_numNodes, _x.data(), _abscis.data(), _intgPoint, _gridSpacing, _cbPtr, _cbIdx, _rw,
+    int rc = PD_OK;
+    if (_batch) {
+        rc = BatchMLS(&bad);
+    } else {
+        mls_contributors(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _rw, _cbPtr, _cbIdx);
+        rc = mls_coefficients(_numNodes, _x.data(), _abscis.data(), _intgPoint, _gridSpacing, _cbPtr, _cbIdx, _rw,
                               _coeff, host_threads(), &bad);
+    }
+    if (rc == PD_ERR_ARG) return rc;
     if (rc != PD_OK) {
         std::ostringstream o;
         o << "pdMatrix::Gauss: Singular Matrix (MLS moment matrix of node " << bad << ")";
@@ -715,6 +738,177 @@ int pdSolve::SolveStatic(pdDataManager& dat, int precision, double rtol, bool wr
         std::ofstream log((dat.GetWkDir() + "pds_output.dat").c_str(), std::ios::app);
         log << "** Static solution: CG iterations = " << iters << ", relative residual = " << rel << " **\n";
         return WriteTecplot(dat, 1, t);
+    }
+    return PD_OK;
+}
+
+// ------------------------------------------------------------------ batch
+
+int pdDataManager::InitBatch(const std::vector<pdDataManager*>& sp) {
+    if (sp.empty()) return Error(PD_ERR_ARG, "InitBatch: no specimens");
+    if (_ctx) return Error(PD_ERR_ARG, "InitBatch: this model already has a device context");
+    for (size_t k = 0; k < sp.size(); ++k) {
+        pdDataManager* m = sp[k];
+        if (!m || !m->_stage) return Error(PD_ERR_ARG, "InitBatch: every specimen must have read its deck");
+        int rc = PD_OK;
+        if (!m->_nodesDone && (rc = m->InitNode()) != PD_OK) return Error(rc, "InitBatch: specimen: " + m->_err);
+        if (!m->_matDone && (rc = m->InitMaterial()) != PD_OK) return Error(rc, "InitBatch: specimen: " + m->_err);
+        const pdDataManager& f = *sp[0];
+        if (m->_gridSpacing != f._gridSpacing || m->_horizon != f._horizon || m->_cciOn != f._cciOn ||
+            m->_cciMdf != f._cciMdf || m->_fgiOn != f._fgiOn || m->_mlsOn != f._mlsOn ||
+            m->_intgPoint != f._intgPoint || m->_rw != f._rw || m->_dampCoeff != f._dampCoeff)
+            return Error(PD_ERR_ARG, "InitBatch: specimens differ in spacing, horizon, integration or damping");
+        if (m->_bdryEffOn) return Error(PD_ERR_ARG, "InitBatch: boundary effect factors are not batched");
+        if (!m->_springFactor.empty() && (int64_t)m->_springFactor.size() != m->_numNodes)
+            return Error(PD_ERR_ARG, "InitBatch: spring factor size");
+    }
+    const pdDataManager& f = *sp[0];
+    _gridSpacing = f._gridSpacing;
+    _horizon = f._horizon;
+    _cciOn = f._cciOn;
+    _cciMdf = f._cciMdf;
+    _fgiOn = f._fgiOn;
+    _mlsOn = f._mlsOn;
+    _intgPoint = f._intgPoint;
+    _npt = f._npt;
+    _rw = f._rw;
+    _dampCoeff = f._dampCoeff;
+    _abscis = f._abscis;
+    _weights = f._weights;
+    _tolerance = f._tolerance;
+    _totalStep = f._totalStep;
+    _totalTime = f._totalTime;
+    _fixedTimeStepOn = f._fixedTimeStepOn;
+    _fixedTimeStep = f._fixedTimeStep;
+    _safeFactor = f._safeFactor;
+    _stepDumpFrequency = f._stepDumpFrequency;
+    _bdryEffOn = false;
+    _dims[0] = _dims[1] = _dims[2] = 0;
+    _center[0] = _center[1] = _center[2] = 0.0;
+    {
+        std::ostringstream o;
+        o << "batch of " << sp.size() << " specimens";
+        _title = o.str();
+    }
+    // placement: shelves in the x-y plane, in lattice steps, with a gap
+    // wider than the horizon plus a cell
+    const double h = _gridSpacing;
+    const int64_t gap = (int64_t)std::ceil(_horizon / h) + 3;
+    const size_t K = sp.size();
+    std::vector<std::array<double, 3>> lo(K);
+    std::vector<std::array<int64_t, 3>> ext(K);
+    double area = 0.0;
+    int64_t widest = 0;
+    for (size_t k = 0; k < K; ++k) {
+        const pdDataManager& m = *sp[k];
+        double l[3] = {1e300, 1e300, 1e300}, u[3] = {-1e300, -1e300, -1e300};
+        for (int64_t i = 0; i < m._numNodes; ++i)
+            for (int a = 0; a < 3; ++a) {
+                l[a] = std::min(l[a], m._x[3 * i + a]);
+                u[a] = std::max(u[a], m._x[3 * i + a]);
+            }
+        for (int a = 0; a < 3; ++a) {
+            lo[k][a] = m._numNodes ? l[a] : 0.0;
+            ext[k][a] = m._numNodes ? (int64_t)std::llround((u[a] - l[a]) / h) : 0;
+        }
+        area += (double)(ext[k][0] + gap) * (double)(ext[k][1] + gap);
+        widest = std::max(widest, ext[k][0]);
+    }
+    const int64_t rowmax = std::max<int64_t>(widest, (int64_t)std::ceil(std::sqrt(area)));
+    std::vector<std::array<int64_t, 3>> origin(K);
+    int64_t cx = 0, cy = 0, rowh = 0;
+    for (size_t k = 0; k < K; ++k) {
+        if (cx > 0 && cx + ext[k][0] > rowmax) {
+            cx = 0;
+            cy += rowh + gap;
+            rowh = 0;
+        }
+        origin[k] = {cx, cy, 0};
+        cx += ext[k][0] + gap;
+        rowh = std::max(rowh, ext[k][1]);
+    }
+    // merged node arrays
+    _x.clear();
+    _batchCoords.clear();
+    _mat.clear();
+    _bc.clear();
+    _mats.clear();
+    _bcs.clear();
+    _slits.clear();
+    _springFactor.clear();
+    _batchOffsets.assign(1, 0);
+    bool anyFactor = false;
+    for (const pdDataManager* m : sp) anyFactor = anyFactor || !m->_springFactor.empty();
+    for (size_t k = 0; k < K; ++k) {
+        const pdDataManager& m = *sp[k];
+        const int matBase = (int)_mats.size(), bcBase = (int)_bcs.size();
+        double shift[3];
+        for (int a = 0; a < 3; ++a) shift[a] = (double)origin[k][a] * h;
+        for (int64_t i = 0; i < m._numNodes; ++i) {
+            for (int a = 0; a < 3; ++a) {
+                const double xa = m._x[3 * i + a];
+                _x.push_back(shift[a] + (xa - lo[k][a]));
+                _batchCoords.push_back(xa);
+            }
+            _mat.push_back(m._mat[i] + matBase);
+            _bc.push_back(m._bc[i] >= 0 ? m._bc[i] + bcBase : -1);
+            if (anyFactor) _springFactor.push_back(m._springFactor.empty() ? 1.0 : m._springFactor[i]);
+        }
+        for (const Material& q : m._mats) _mats.push_back(q);
+        for (const BdryCondition& q : m._bcs) _bcs.push_back(q);
+        for (size_t q = 0; q + 6 <= m._slits.size(); q += 6)
+            for (int a = 0; a < 3; ++a)
+                for (int e = 0; e < 2; ++e) _slits.push_back(shift[a] + (m._slits[q + 2 * a + e] - lo[k][a]));
+        _batchOffsets.push_back(_batchOffsets.back() + m._numNodes);
+    }
+    _numNodes = _batchOffsets.back();
+    if (_numNodes > INT32_MAX) return Error(PD_ERR_ARG, "InitBatch: too many nodes");
+    _bdryEff.assign(_numNodes, 1.0);
+    _batch = true;
+    _stage = true;
+    _nodesDone = true;
+    _bondsDone = false;
+    _uploaded = false;
+    int rc = InitMaterial();
+    if (rc != PD_OK) return rc;
+    std::ofstream log(_outFilePath.c_str(), std::ios::app);
+    log << "\nInitBatch: " << K << " specimens, total node number = " << _numNodes << "\n";
+    return PD_OK;
+}
+
+// MLS of every specimen in its own coordinates, merged in node order
+int pdDataManager::BatchMLS(int64_t* bad_node) {
+    const size_t K = _batchOffsets.size() - 1;
+    _cbPtr.assign(1, 0);
+    _cbIdx.clear();
+    _coeff.clear();
+    for (size_t k = 0; k < K; ++k) {
+        const int64_t o = _batchOffsets[k], n = _batchOffsets[k + 1] - o;
+        std::vector<int64_t> fp(n + 1);
+        std::vector<int32_t> fc;
+        fc.reserve(_famPtr[o + n] - _famPtr[o]);
+        for (int64_t i = 0; i <= n; ++i) fp[i] = _famPtr[o + i] - _famPtr[o];
+        for (int64_t p = _famPtr[o]; p < _famPtr[o + n]; ++p) {
+            const int64_t j = _famCol[p] - o;
+            if (j < 0 || j >= n) return Error(PD_ERR_ARG, "InitIntegrationPoint: a bond joins two specimens");
+            fc.push_back((int32_t)j);
+        }
+        std::vector<int64_t> cp;
+        std::vector<int32_t> ci;
+        std::vector<double> co;
+        const double* xs = _batchCoords.data() + 3 * o;
+        mls_contributors(n, xs, fp.data(), fc.data(), _rw, cp, ci);
+        int64_t bad = -1;
+        const int rc = mls_coefficients(n, xs, _abscis.data(), _intgPoint, _gridSpacing, cp, ci, _rw, co,
+                                        host_threads(), &bad);
+        if (rc != PD_OK) {
+            *bad_node = bad >= 0 ? bad + o : -1;
+            return rc;
+        }
+        const int64_t base = _cbPtr.back();
+        for (int64_t i = 1; i <= n; ++i) _cbPtr.push_back(base + cp[i]);
+        for (int32_t v : ci) _cbIdx.push_back((int32_t)(v + o));
+        _coeff.insert(_coeff.end(), co.begin(), co.end());
     }
     return PD_OK;
 }

@@ -55,6 +55,8 @@ public:
 
     // working folder holding pds_input.txt (replaces pdDataManager3.cpp:1503-1541)
     int SetWkDir(const std::string& dir);
+    // output folder only (no deck): the log of a batch model
+    int SetOutputDir(const std::string& dir);
     std::string GetWkDir() const { return _workDir; }
 
     // pdSolve::InitialProblem steps (pdSolve.cpp:10-22)
@@ -65,6 +67,15 @@ public:
     int InitBdryEffectFactor();
     int InitGridBoundary();
     int InitIntegrationPoint();
+    // Batching (no counterpart in the reference): this model becomes one
+    // problem over several specimens, each a model that has read its deck.
+    // The specimens' nodes are placed side by side on one lattice with gaps
+    // wider than the horizon, so InitBond finds no bond between specimens;
+    // InitIntegrationPoint then solves each specimen's MLS in its own
+    // coordinates.  Node ids run specimen by specimen (BatchOffsets).
+    int InitBatch(const std::vector<pdDataManager*>& specimens);
+    bool IsBatch() const { return _batch; }
+    const std::vector<int64_t>& BatchOffsets() const { return _batchOffsets; }
     // installs a family computed elsewhere instead of InitBond (no GPU needed)
     int SetFamily(const std::vector<int64_t>& row_ptr, const std::vector<int32_t>& col,
                   const std::vector<uint8_t>& broken, double min_bond);
@@ -124,6 +135,12 @@ public:
     const std::vector<BdryCondition>& BCs() const { return _bcs; }
     pd_ctx* Context() { return _ctx; }
     int EnsureContext();
+    // the material / BC tables as pd_ctx_create receives them
+    void DeviceTables(std::vector<pd_material>& mats, std::vector<pd_bc>& bcs) const;
+    const std::vector<double>& GaussAbscissae() const { return _abscis; }
+    const std::vector<double>& GaussWeights() const { return _weights; }
+    int GetIntgPoint() const { return _cciOn ? 1 : _intgPoint; }
+    double GetDamping() const { return _dampCoeff; }
     void SetSpringFactor(const std::vector<double>& f) { _springFactor = f; }
 
 private:
@@ -131,6 +148,7 @@ private:
     int Error(int code, const std::string& msg);
     int Cuda(int rc, const char* what);
     int UploadSetup();
+    int BatchMLS(int64_t* bad_node);
 
     std::string _workDir, _inFilePath, _outFilePath, _title, _err;
     std::vector<std::string> _deck;  // lines, trimmed
@@ -167,6 +185,10 @@ private:
     double _minMaterialDensity = 0, _maxBulkSoundSpeed = 0;
     // energies of the last step
     double _kineticEnergyStep = 0, _elasticEnergyStep = 0;
+    // batch of specimens
+    bool _batch = false;
+    std::vector<int64_t> _batchOffsets;  // [specimens + 1]
+    std::vector<double> _batchCoords;    // each specimen's own coordinates
     // device
     pd_ctx* _ctx = nullptr;
     bool _uploaded = false;

@@ -2,6 +2,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "pdDataManager.h"
 #include "pdmtel_host.h"
@@ -30,6 +31,44 @@ int pdh_open(const char* dir, pdh_model** out) {
     if (rc != PD_OK) m->err = m->dat.LastError();
     *out = m;  // kept even on error so that pdh_last_error can report it
     return rc;
+}
+
+int pdh_batch_create(const char* out_dir, pdh_model* const* specimens, int count, pdh_model** out) {
+    if (!out_dir || !specimens || count < 1 || !out) return PD_ERR_ARG;
+    *out = nullptr;
+    pdh_model* m = new (std::nothrow) pdh_model();
+    if (!m) return PD_ERR_OOM;
+    std::vector<pdh::pdDataManager*> sp;
+    for (int k = 0; k < count; ++k) {
+        if (!specimens[k]) {
+            m->err = "pdh_batch_create: null specimen";
+            *out = m;
+            return PD_ERR_ARG;
+        }
+        sp.push_back(&specimens[k]->dat);
+    }
+    int rc = m->dat.SetOutputDir(out_dir);
+    if (rc == PD_OK) rc = m->dat.InitBatch(sp);
+    if (rc != PD_OK) m->err = m->dat.LastError();
+    *out = m;
+    return rc;
+}
+
+int pdh_batch_offsets(pdh_model* m, int64_t* offsets) {
+    if (!m || !offsets) return PD_ERR_ARG;
+    if (!m->dat.IsBatch()) {
+        m->err = "pdh_batch_offsets: not a batch model";
+        return PD_ERR_ARG;
+    }
+    const std::vector<int64_t>& o = m->dat.BatchOffsets();
+    std::memcpy(offsets, o.data(), sizeof(int64_t) * o.size());
+    return PD_OK;
+}
+
+int pdh_batch_count(pdh_model* m, int* count) {
+    if (!m || !count) return PD_ERR_ARG;
+    *count = m->dat.IsBatch() ? (int)m->dat.BatchOffsets().size() - 1 : 0;
+    return PD_OK;
 }
 
 int pdh_close(pdh_model* m) {
@@ -62,6 +101,24 @@ int pdh_get_info(pdh_model* m, pdh_info* I) {
     I->min_bond_length = d.GetMinBondLength();
     I->ke = d.GetKinetTotal();
     I->ee = d.GetElastStep();
+    I->num_materials = (int32_t)d.Materials().size();
+    I->num_bcs = (int32_t)d.BCs().size();
+    I->intg_point = d.GetIntgPoint();
+    I->damping = d.GetDamping();
+    return PD_OK;
+}
+
+int pdh_get_tables(pdh_model* m, pd_material* materials, pd_bc* bcs, double* abscissae, double* weights) {
+    if (!m) return PD_ERR_ARG;
+    std::vector<pd_material> mt;
+    std::vector<pd_bc> bt;
+    m->dat.DeviceTables(mt, bt);
+    if (materials) std::memcpy(materials, mt.data(), sizeof(pd_material) * mt.size());
+    if (bcs) std::memcpy(bcs, bt.data(), sizeof(pd_bc) * bt.size());
+    const std::vector<double>& a = m->dat.GaussAbscissae();
+    const std::vector<double>& w = m->dat.GaussWeights();
+    if (abscissae) std::memcpy(abscissae, a.data(), sizeof(double) * a.size());
+    if (weights) std::memcpy(weights, w.data(), sizeof(double) * w.size());
     return PD_OK;
 }
 

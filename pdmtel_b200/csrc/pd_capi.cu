@@ -56,6 +56,18 @@ struct pd_ctx {
     };
     std::vector<Checkpoint> ckpt;
     int adj_steps = 0, adj_every = 0, adj_acc = 0;
+    // launch shapes (pd_set_option / pd_autotune)
+    int64_t tile = 3 | (2 << 8) | (2 << 16);
+    int persist_per_sm = 0;  // 0: as many as fit
+    unsigned force_chunk = 128, gather_chunk = 256;
+    // persistent stepping: control block and the graph of one launch
+    pd::PersistCtl* pctl = nullptr;
+    int pctl_steps = 0;
+    cudaGraphExec_t persist_graph = nullptr;
+    double persist_dt = 0.0, persist_t0 = 0.0;
+    int persist_steps = 0;
+    uint64_t persist_generation = ~0ull;
+    int tuned_persistent = 0;
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
@@ -158,20 +170,26 @@ int upload_static_f32(pd_ctx* c) {
 // Work order of the node-parallel kernels: nodes grouped into 8x4x4 tiles of
 // lattice positions (x fastest inside a tile), tiles in x, y, z order, so
 // that a 128-thread block covers one compact tile.
-std::vector<int32_t> tiled_order(const std::vector<double>& x, int64_t N, double dx) {
+// Work order: lattice tiles of 2^bx x 2^by x 2^bz nodes, tiles in x-fastest
+// order, nodes x-fastest inside a tile (x-adjacent nodes pair up in the
+// FP32 pair kernel).  Default 8 x 4 x 4.
+std::vector<int32_t> tiled_order(const std::vector<double>& x, int64_t N, double dx, int bx = 3, int by = 2,
+                                 int bz = 2) {
     std::vector<int32_t> ord(N);
     if (N == 0) return ord;
     double lo[3] = {x[0], x[1], x[2]};
     for (int64_t i = 0; i < N; ++i)
         for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], x[3 * i + a]);
     std::vector<std::pair<uint64_t, int32_t>> key(N);
+    const int lb = bx + by + bz;
     for (int64_t i = 0; i < N; ++i) {
         int64_t l[3];
         for (int a = 0; a < 3; ++a) l[a] = (int64_t)std::llround((x[3 * i + a] - lo[a]) / dx);
-        const uint64_t tx = l[0] >> 3, ty = l[1] >> 2, tz = l[2] >> 2;
-        const uint64_t tile = (tz << 42) | (ty << 21) | tx;
-        const uint64_t local = ((uint64_t)(l[2] & 3) << 5) | ((uint64_t)(l[1] & 3) << 3) | (uint64_t)(l[0] & 7);
-        key[i] = {(tile << 7) | local, (int32_t)i};
+        const uint64_t tx = l[0] >> bx, ty = l[1] >> by, tz = l[2] >> bz;
+        const uint64_t tile = (tz << 38) | (ty << 19) | tx;
+        const uint64_t local = ((uint64_t)(l[2] & ((1 << bz) - 1)) << (bx + by)) |
+                               ((uint64_t)(l[1] & ((1 << by) - 1)) << bx) | (uint64_t)(l[0] & ((1 << bx) - 1));
+        key[i] = {(tile << lb) | local, (int32_t)i};
     }
     std::sort(key.begin(), key.end());
     for (int64_t k = 0; k < N; ++k) ord[k] = key[k].second;
@@ -487,6 +505,7 @@ int pd_ctx_destroy(pd_ctx* c) {
     if (!c) return PD_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    if (c->persist_graph) cudaGraphExecDestroy(c->persist_graph);
     for (void* p : c->owned)
         if (p) cudaFree(p);
     if (c->hstage) cudaFreeHost(c->hstage);
@@ -692,10 +711,26 @@ int pd_set_precision(pd_ctx* c, int p) {
 
 int pd_set_option(pd_ctx* c, int option, int64_t value) {
     if (!c) return fail(PD_ERR_ARG, "pd_set_option: null context");
+    if (value < 0) return fail(PD_ERR_ARG, "pd_set_option: negative value");
     switch (option) {
-        case PD_OPT_F64_LANES_BELOW:
-            if (value < 0) return fail(PD_ERR_ARG, "pd_set_option: negative value");
-            c->d.f64_lanes_below = value;
+        case PD_OPT_F64_LANES_BELOW: c->d.f64_lanes_below = value; break;
+        case PD_OPT_TILE: {
+            const int bx = (int)(value & 0xff), by = (int)((value >> 8) & 0xff), bz = (int)((value >> 16) & 0xff);
+            if (bx < 1 || bx > 6 || by > 6 || bz > 6) return fail(PD_ERR_ARG, "pd_set_option: tile exponents");
+            std::vector<int32_t> ord = tiled_order(c->coords, c->n, c->d.dx, bx, by, bz);
+            PD_TRY(upload(c, (void*)c->d.order, ord.data(), sizeof(int32_t) * c->n));
+            PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            c->tile = value;
+            break;
+        }
+        case PD_OPT_PERSIST_BLOCKS_PER_SM:
+            if (value > 32) return fail(PD_ERR_ARG, "pd_set_option: blocks per SM");
+            c->persist_per_sm = (int)value;
+            break;
+        case PD_OPT_PERSIST_FORCE_CHUNK:
+        case PD_OPT_PERSIST_GATHER_CHUNK:
+            if (value < 128 || value > (1 << 20) || value % 128) return fail(PD_ERR_ARG, "pd_set_option: chunk");
+            (option == PD_OPT_PERSIST_FORCE_CHUNK ? c->force_chunk : c->gather_chunk) = (unsigned)value;
             break;
         default: return fail(PD_ERR_ARG, "pd_set_option: unknown option");
     }
@@ -707,6 +742,10 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
     if (!c || !value) return fail(PD_ERR_ARG, "pd_get_option: null argument");
     switch (option) {
         case PD_OPT_F64_LANES_BELOW: *value = c->d.f64_lanes_below; return PD_OK;
+        case PD_OPT_TILE: *value = c->tile; return PD_OK;
+        case PD_OPT_PERSIST_BLOCKS_PER_SM: *value = c->persist_per_sm; return PD_OK;
+        case PD_OPT_PERSIST_FORCE_CHUNK: *value = c->force_chunk; return PD_OK;
+        case PD_OPT_PERSIST_GATHER_CHUNK: *value = c->gather_chunk; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
     }
 }
@@ -1377,4 +1416,230 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
     c->d.energy = energy;
     c->d.acc_stretch = acc;
     return rc;
+}
+
+// ------------------------------------------------------- persistent stepping
+
+namespace {
+
+bool persist_capable(const pd_ctx* c) {
+    return c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.gc_host && !c->d.energy;
+}
+
+int persist_blocks(pd_ctx* c, int* blocks) {
+    int per_sm = 0, sms = 0;
+    if (pd::persist_max_blocks(c->d, &per_sm, &sms) != PD_OK || per_sm < 1)
+        return fail(PD_ERR_CUDA, "persistent launch: no cooperative launch of this kernel fits the device");
+    const int use = c->persist_per_sm > 0 ? std::min(c->persist_per_sm, per_sm) : per_sm;
+    *blocks = use * sms;
+    return PD_OK;
+}
+
+}  // namespace
+
+// nsteps RK4 steps of the FP32-compensated FGI form (2x2x2 points) in one
+// cooperative persistent launch: work-queue phases separated by bounded grid
+// barriers.  The control-block reset and the launch are captured once into a
+// CUDA graph (per dt, step count and launch shape) and replayed.  Same
+// result bit for bit as pd_rk4_steps in PD_PREC_FP32C.  Synchronous: the
+// call waits for the launch and reports a barrier that gave up as
+// PD_ERR_TIMEOUT.
+extern "C" int pd_rk4_steps_persistent(pd_ctx* c, double dt, double t0, int nsteps) {
+    if (!c || nsteps < 0) return fail(PD_ERR_ARG, "pd_rk4_steps_persistent: bad argument");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_rk4_steps_persistent: family/MLS data not set");
+    if (!persist_capable(c))
+        return fail(PD_ERR_ARG,
+                    "pd_rk4_steps_persistent: needs PD_PREC_FP32C, Gauss-point integration with 2x2x2 points and "
+                    "energy accumulation off");
+    if (nsteps == 0) return PD_OK;
+    const size_t bytes = sizeof(pd::PersistCtl) + sizeof(unsigned) * 8 * (size_t)nsteps;
+    if (c->pctl_steps < nsteps) {
+        if (c->persist_graph) {
+            cudaGraphExecDestroy(c->persist_graph);
+            c->persist_graph = nullptr;
+        }
+        dfree(c, c->pctl);
+        c->pctl = nullptr;
+        c->pctl_steps = 0;
+        char* p = nullptr;
+        PD_TRY(dalloc(c, &p, bytes));
+        c->pctl = (pd::PersistCtl*)p;
+        c->pctl_steps = nsteps;
+    }
+    int blocks = 0;
+    PD_TRY(persist_blocks(c, &blocks));
+    PD_TRY(set_time(c, t0));
+    if (!c->persist_graph || c->persist_dt != dt || c->persist_steps != nsteps ||
+        c->persist_generation != c->generation) {
+        if (c->persist_graph) {
+            cudaGraphExecDestroy(c->persist_graph);
+            c->persist_graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        PD_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaMemsetAsync(c->pctl, 0, bytes, c->stream);
+        if (e == cudaSuccess)
+            e = pd::launch_persist_f32c(c->d, dt, nsteps, c->pctl, blocks, c->force_chunk, c->gather_chunk,
+                                        c->stream);
+        cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return pd::fail_cuda(e, "persistent launch capture", __FILE__, __LINE__);
+        }
+        if (e2 != cudaSuccess) return pd::fail_cuda(e2, "persistent launch capture", __FILE__, __LINE__);
+        e = cudaGraphInstantiate(&c->persist_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return pd::fail_cuda(e, "persistent graph instantiate", __FILE__, __LINE__);
+        c->persist_dt = dt;
+        c->persist_steps = nsteps;
+        c->persist_generation = c->generation;
+    }
+    PD_CUDA_TRY(cudaGraphLaunch(c->persist_graph, c->stream));
+    PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, &c->pctl->error, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    int err = 0;
+    std::memcpy(&err, c->hscalar, sizeof(int));
+    if (err) return fail(PD_ERR_TIMEOUT, "pd_rk4_steps_persistent: a grid barrier gave up waiting");
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+
+namespace {
+
+struct Snapshot {
+    double *U = nullptr, *V = nullptr, *ug = nullptr, t = 0.0;
+    float* nblk = nullptr;
+};
+
+int snap_take(pd_ctx* c, Snapshot& S) {
+    const int64_t n3 = 3 * c->n, ng = n3 * c->npt, nb = c->n * (int64_t)c->d.bs;
+    cudaStream_t s = c->stream;
+    if (!S.U) {
+        PD_TRY(dalloc(c, &S.U, n3));
+        PD_TRY(dalloc(c, &S.V, n3));
+        PD_TRY(dalloc(c, &S.ug, ng));
+        PD_TRY(dalloc(c, &S.nblk, nb));
+    }
+    PD_CUDA_TRY(cudaMemcpyAsync(S.U, c->d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(S.V, c->d.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(S.ug, c->d.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(S.nblk, c->d.nblk, sizeof(float) * nb, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, c->d.tdev, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PD_CUDA_TRY(cudaStreamSynchronize(s));
+    S.t = c->hscalar[0];
+    return PD_OK;
+}
+
+int snap_restore(pd_ctx* c, const Snapshot& S) {
+    const int64_t n3 = 3 * c->n, ng = n3 * c->npt, nb = c->n * (int64_t)c->d.bs;
+    cudaStream_t s = c->stream;
+    PD_CUDA_TRY(cudaMemcpyAsync(c->d.U, S.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(c->d.V, S.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(c->d.ug, S.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(c->d.nblk, S.nblk, sizeof(float) * nb, cudaMemcpyDeviceToDevice, s));
+    PD_TRY(set_time(c, S.t));
+    PD_CUDA_TRY(cudaStreamSynchronize(s));
+    return PD_OK;
+}
+
+void snap_free(pd_ctx* c, Snapshot& S) {
+    dfree(c, S.U);
+    dfree(c, S.V);
+    dfree(c, S.ug);
+    dfree(c, S.nblk);
+}
+
+// device time of `steps` steps from the snapshot, after an untimed run of
+// the same length (which captures the graphs)
+int time_steps(pd_ctx* c, const Snapshot& S, double dt, int steps, bool persistent, double* ms) {
+    PD_TRY(snap_restore(c, S));
+    if (persistent) PD_TRY(pd_rk4_steps_persistent(c, dt, S.t, steps));
+    else PD_TRY(pd_rk4_steps(c, dt, S.t, steps));
+    PD_TRY(snap_restore(c, S));
+    cudaEvent_t a, b;
+    PD_CUDA_TRY(cudaEventCreate(&a));
+    PD_CUDA_TRY(cudaEventCreate(&b));
+    cudaEventRecord(a, c->stream);
+    int rc = persistent ? pd_rk4_steps_persistent(c, dt, S.t, steps) : pd_rk4_steps(c, dt, S.t, steps);
+    cudaEventRecord(b, c->stream);
+    cudaError_t e = cudaEventSynchronize(b);
+    float f = 0.f;
+    if (rc == PD_OK && e == cudaSuccess) cudaEventElapsedTime(&f, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc != PD_OK) return rc;
+    if (e != cudaSuccess) return pd::fail_cuda(e, "autotune timing", __FILE__, __LINE__);
+    *ms = f / steps;
+    return PD_OK;
+}
+
+}  // namespace
+
+// Times candidate launch shapes on this context's own problem and keeps the
+// fastest: first the node-order tile with the graph-captured step, then (when
+// the persistent launch applies) its blocks per SM and queue chunk sizes.
+// The state is restored after every trial, so tuning leaves it as it was.
+extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out) {
+    if (!c || !out || steps < 1 || !(dt > 0.0)) return fail(PD_ERR_ARG, "pd_autotune: bad argument");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_autotune: family/MLS data not set");
+    std::memset(out, 0, sizeof *out);
+    Snapshot S;
+    int rc = snap_take(c, S);
+    auto done = [&](int r) {
+        snap_free(c, S);
+        return r;
+    };
+    if (rc != PD_OK) return done(rc);
+    struct Trial {
+        int64_t tile;
+        int persistent, per_sm;
+        unsigned fc, gc;
+        double ms;
+    };
+    Trial best{c->tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 1e300};
+    auto apply = [&](const Trial& T) -> int {
+        if (T.tile != c->tile) PD_TRY(pd_set_option(c, PD_OPT_TILE, T.tile));
+        c->persist_per_sm = T.per_sm;
+        c->force_chunk = T.fc;
+        c->gather_chunk = T.gc;
+        c->generation++;
+        return PD_OK;
+    };
+    auto trial = [&](Trial T) -> int {
+        PD_TRY(apply(T));
+        PD_TRY(time_steps(c, S, dt, steps, T.persistent != 0, &T.ms));
+        out->trials++;
+        if (T.ms < best.ms) best = T;
+        return PD_OK;
+    };
+    // tiles: only meaningful on a lattice
+    std::vector<int64_t> tiles = {c->tile};
+    if (c->d.lat) {
+        const int64_t cand[][3] = {{3, 2, 2}, {3, 3, 1}, {4, 2, 1}, {2, 2, 2}, {4, 1, 1}, {3, 1, 1}, {5, 1, 0}};
+        tiles.clear();
+        for (auto& t3 : cand) tiles.push_back(t3[0] | (t3[1] << 8) | (t3[2] << 16));
+    }
+    for (int64_t tl : tiles)
+        if ((rc = trial({tl, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0})) != PD_OK) return done(rc);
+    if (persist_capable(c)) {
+        int per_sm = 0, sms = 0;
+        if (pd::persist_max_blocks(c->d, &per_sm, &sms) == PD_OK && per_sm >= 1) {
+            const int64_t tl = best.tile;
+            for (int ps = per_sm; ps >= 1 && ps >= per_sm - 2; --ps)
+                for (unsigned fc : {128u, 512u})
+                    for (unsigned gcn : {256u, 1024u})
+                        if ((rc = trial({tl, 1, ps, fc, gcn, 0.0})) != PD_OK) return done(rc);
+        }
+    }
+    if ((rc = apply(best)) != PD_OK) return done(rc);
+    if ((rc = snap_restore(c, S)) != PD_OK) return done(rc);
+    out->tile = best.tile;
+    out->persistent = best.persistent;
+    out->blocks_per_sm = best.per_sm;
+    out->force_chunk = (int32_t)best.fc;
+    out->gather_chunk = (int32_t)best.gc;
+    out->ms_per_step = best.ms;
+    c->tuned_persistent = best.persistent;
+    return done(PD_OK);
 }

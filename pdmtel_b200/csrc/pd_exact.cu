@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "pd_internal.cuh"
+#include "pd_stage.cuh"
 
 namespace pd {
 
@@ -318,69 +319,11 @@ __global__ void k_gather_f64(Dev d, const double* __restrict__ us) {
 // (:2027-2092): next trial displacement, k3 += k2, and at stage 4 the
 // combination, the damping and the new velocity.
 __global__ void k_epilogue(Dev d, int stage, double dts, double dt) {
-    const int64_t N = d.n;
-    const double t = *d.tdev;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const double rho = d.mats[d.mat[i]].density;
-    double v[3] = {d.vbuf[i], d.vbuf[N + i], d.vbuf[2 * N + i]};
-    double U[3] = {d.U[i], d.U[N + i], d.U[2 * N + i]};
-    const int b = d.bc[i];
-    if (b >= 0) {
-        const BcDev& B = d.bcs[b];
-        const double fac = time_factor(B, t);
-        const double X[3] = {d.x[i], d.x[N + i], d.x[2 * N + i]};
-        for (int a = 0; a < 3; ++a) {
-            if (B.dir[a] != 1) continue;
-            if (B.type == PD_BC_TRACTION) {
-                const double tb = B.val[a] * fac / d.dx;
-                v[a] += tb * dts / rho;
-            } else if (B.type == PD_BC_DISPL) {
-                U[a] = B.val[a] * fac;
-                v[a] = 0.0;
-            } else if (B.type == PD_BC_VELOC) {
-                v[a] = B.val[a] * fac;
-            } else if (B.type == PD_BC_DISPLGRAD) {
-                U[a] = (B.val[3 * a] * X[0] + B.val[3 * a + 1] * X[1] + B.val[3 * a + 2] * X[2]) * fac;
-                v[a] = 0.0;
-            }
-        }
-    }
-    const double dt6 = 1.0 / 6.0;
-    double ke = 0.0;
-    for (int a = 0; a < 3; ++a) {
-        const int64_t r = a * N + i;
-        const double k = v[a] * dts;
-        if (stage == 0) {  // single stage call: k is returned in k1
-            d.k1[r] = k;
-        } else if (stage == 1) {
-            d.k1[r] = k;
-            d.us[r] = d.u1[r] + 0.5 * k;
-        } else if (stage == 2) {
-            d.k2[r] = k;
-            d.us[r] = d.u1[r] + 0.5 * k;
-        } else if (stage == 3) {
-            d.us[r] = d.u1[r] + k;
-            d.k32[r] = k + d.k2[r];
-        } else {
-            const double Vold = d.V[r];
-            const double inc = dt6 * (d.k1[r] + k + 2.0 * d.k32[r]);
-            if (b >= 0) U[a] = U[a] + inc;
-            else U[a] = U[a] + inc - dt * d.damping * Vold * dt / rho;
-            v[a] += -d.damping * Vold * dt / rho;
-            d.V[r] = v[a];
-            d.u1[r] = U[a];
-            d.us[r] = U[a];
-        }
-        d.vbuf[r] = v[a];
-        d.U[r] = U[a];
-    }
-    if (stage == 4 && d.energy) {
-        const double velsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-        ke = 0.5 * rho * velsq * d.vol;
-        d.red[i] = ke;
-        d.red[N + i] = d.vol * d.eed[i];
-    }
+    if (i >= d.n) return;
+    const double t = *d.tdev;
+    if (d.energy) stage_epilogue<true>(d, i, stage, dts, dt, t);
+    else stage_epilogue<false>(d, i, stage, dts, dt, t);
 }
 
 // Deterministic two-level sum of red[0..N) and red[N..2N) into red[2N], red[2N+1].

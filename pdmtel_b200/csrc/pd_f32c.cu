@@ -20,6 +20,7 @@
 #include <climits>
 
 #include "pd_internal.cuh"
+#include "pd_stage.cuh"
 
 namespace pd {
 
@@ -34,6 +35,17 @@ __device__ __forceinline__ double time_factor(const BcDev& b, double t) {
 }
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+// data the same launch rewrites (the persistent kernel): through L2, never a
+// possibly stale L1 line; read-only data keep the non-coherent path
+template <bool PERSIST>
+__device__ __forceinline__ float4 ld4m(const float* p) {
+    return PERSIST ? __ldcg(reinterpret_cast<const float4*>(p)) : __ldg(reinterpret_cast<const float4*>(p));
+}
+template <bool PERSIST>
+__device__ __forceinline__ double ldm(const double* p) {
+    return PERSIST ? __ldcg(p) : __ldg(p);
+}
 
 struct PointF {
     float hx, hy, hz, W, A, B;  // offset of the point from its node, weight*vol/8, beta = sat((A - r) B)
@@ -88,12 +100,12 @@ __device__ __forceinline__ void kahan_add(Own& o, float F0, float F1, float F2) 
     y = F2 - o.k[2]; t = o.s[2] + y; o.k[2] = (t - o.s[2]) - y; o.s[2] = t;
 }
 
-template <bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
+template <bool LAT, bool BDRY, bool SFAC, bool MULTIMAT, bool PERSIST = false>
 __device__ __forceinline__ void load_own(const Dev& d, int64_t i, Own& o) {
     const int64_t N = d.n;
     const double* src = d.bc[i] >= 0 ? d.U : d.us;
     for (int a = 0; a < 3; ++a) {
-        const double u = src[a * N + i];
+        const double u = PERSIST ? __ldcg(src + a * N + i) : src[a * N + i];
         o.uh[a] = (float)u;
         o.ul[a] = (float)(u - (double)o.uh[a]);
         o.s[a] = o.k[a] = 0.f;
@@ -114,12 +126,18 @@ __device__ __forceinline__ void load_own(const Dev& d, int64_t i, Own& o) {
     o.e = MULTIMAT ? (float)d.mats[o.mat].ecrit : d.e0;
 }
 
-__device__ __forceinline__ void store_own(const Dev& d, int64_t i, const Own& o, int64_t nbonds, double dts) {
+// vbuf_i = vbase_i + (F_i + n_bonds rho g) dt_s / rho; vbase is vbuf itself,
+// or V at the first stage of a persistent step (InitDynamicSolve's vbuf = V)
+template <bool PERSIST = false>
+__device__ __forceinline__ void store_own(const Dev& d, int64_t i, const Own& o, int64_t nbonds, double dts,
+                                          const double* vbase) {
     const int64_t N = d.n;
     const MatDev& M = d.mats[o.mat];
     const double rho = M.density;
-    for (int a = 0; a < 3; ++a)
-        d.vbuf[a * N + i] += ((double)o.s[a] - (double)o.k[a] + (double)nbonds * (M.grav[a] * rho)) * dts / rho;
+    for (int a = 0; a < 3; ++a) {
+        const double v0 = PERSIST ? __ldcg(vbase + a * N + i) : vbase[a * N + i];
+        d.vbuf[a * N + i] = v0 + ((double)o.s[a] - (double)o.k[a] + (double)nbonds * (M.grav[a] * rho)) * dts / rho;
+    }
 }
 
 // FGI with 2x2x2 Gauss points, two nodes per thread.  The work order pairs
@@ -127,16 +145,31 @@ __device__ __forceinline__ void store_own(const Dev& d, int64_t i, const Own& o,
 // lists and loads every neighbour's block once for both bonds, which cuts
 // the L1 traffic per evaluation (the bound of this kernel) by the overlap of
 // the two families.  pdDataManager.cpp:1917-1962 in FP32 form.
-template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
-__global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> G, double dts) {
+// The pair of work-order slots t2, t2+1.  PERSIST (inside the persistent
+// kernel) adds what the separate launches of a step do around the force: at
+// the first stage u1 = us = U and vbuf starts from V; after the force the
+// stage epilogue of both nodes at time t.
+template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT, bool PERSIST>
+__device__ __forceinline__ void force_pair(const Dev& d, const PointPack<8>& G, double dts, int64_t t2, int pstage,
+                                           double dt, double t) {
     const int64_t N = d.n;
-    const int64_t t2 = 2 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
-    if (t2 >= N) return;
     const int64_t ia = d.order[t2];
     const int64_t ib = (t2 + 1 < N) ? d.order[t2 + 1] : -1;
+    if (PERSIST && pstage == 1) {
+        for (int a = 0; a < 3; ++a) {
+            const double ua = __ldcg(d.U + a * N + ia);
+            d.u1[a * N + ia] = ua;
+            d.us[a * N + ia] = ua;
+            if (ib >= 0) {
+                const double ub = __ldcg(d.U + a * N + ib);
+                d.u1[a * N + ib] = ub;
+                d.us[a * N + ib] = ub;
+            }
+        }
+    }
     Own A, B;
-    load_own<LAT, BDRY, SFAC, MULTIMAT>(d, ia, A);
-    if (ib >= 0) load_own<LAT, BDRY, SFAC, MULTIMAT>(d, ib, B);
+    load_own<LAT, BDRY, SFAC, MULTIMAT, PERSIST>(d, ia, A);
+    if (ib >= 0) load_own<LAT, BDRY, SFAC, MULTIMAT, PERSIST>(d, ib, B);
     int64_t pa = d.arow[ia], ea = d.arow[ia + 1];
     int64_t pb = 0, eb = 0;
     if (ib >= 0) {
@@ -151,7 +184,7 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> 
         const int j = min(ja, jb);
         if (j == INT_MAX) break;
         const float* bj = d.nblk + (int64_t)j * 32;
-        const float4 us0 = ld4(bj + 24), us1 = ld4(bj + 28);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
+        const float4 us0 = ld4m<PERSIST>(bj + 24), us1 = ld4m<PERSIST>(bj + 28);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
         float pj[6];
         int lj = 0;
         if (LAT) {
@@ -202,7 +235,7 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> 
         // applied to both bonds
 #pragma unroll
         for (int q = 0; q < 8; q += 4) {
-            const float4 vx = ld4(bj + q), vy = ld4(bj + 8 + q), vz = ld4(bj + 16 + q);
+            const float4 vx = ld4m<PERSIST>(bj + q), vy = ld4m<PERSIST>(bj + 8 + q), vz = ld4m<PERSIST>(bj + 16 + q);
             const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
 #pragma unroll
             for (int side = 0; side < 2; ++side)
@@ -218,8 +251,20 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> 
             ++pb;
         }
     }
-    store_own(d, ia, A, nba, dts);
-    if (ib >= 0) store_own(d, ib, B, nbb, dts);
+    const double* vbase = (PERSIST && pstage == 1) ? d.V : d.vbuf;
+    store_own<PERSIST>(d, ia, A, nba, dts, vbase);
+    if (ib >= 0) store_own<PERSIST>(d, ib, B, nbb, dts, vbase);
+    if (PERSIST) {
+        stage_epilogue<false>(d, ia, pstage, dts, dt, t);
+        if (ib >= 0) stage_epilogue<false>(d, ib, pstage, dts, dt, t);
+    }
+}
+
+template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
+__global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> G, double dts) {
+    const int64_t t2 = 2 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+    if (t2 >= d.n) return;
+    force_pair<HASFAIL, LAT, BDRY, SFAC, MULTIMAT, false>(d, G, dts, t2, 0, 0.0, 0.0);
 }
 
 // The same for any number of Gauss points (constants from shared memory).
@@ -364,16 +409,14 @@ __global__ void k_pack_cci(Dev d) {
 // ill-conditioned moment matrices allow, hence the second term).  Nodes with a
 // boundary condition keep the reference's rules on the FP64 Gauss-point
 // displacement (pdDataManager.cpp:2604-2703) and store its difference.
-__global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __restrict__ us) {
+template <bool PERSIST>
+__device__ __forceinline__ void gather_group(const Dev& d, const double* us, int64_t tid, double t) {
     const int64_t N = d.n;
     const int npt = d.npt, ngrp = (npt + 3) / 4;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (tid >= N * ngrp) return;
     const int64_t i = d.order[tid / ngrp];
     const int grp = (int)(tid % ngrp);
     const int g0 = 4 * grp, ng = min(4, npt - g0);
-    const double t = *d.tdev;
-    const double u0 = us[i], u1 = us[N + i], u2 = us[2 * N + i];
+    const double u0 = ldm<PERSIST>(us + i), u1 = ldm<PERSIST>(us + N + i), u2 = ldm<PERSIST>(us + 2 * N + i);
     float* o = d.nblk + i * d.bs;
     if (grp == 0) {
         const float h0 = (float)u0, h1 = (float)u1, h2 = (float)u2;
@@ -399,9 +442,12 @@ __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __rest
                 else if (B.type == PD_BC_DISPLGRAD)
                     ug[a * N] = (B.val[3 * a] * q0 + B.val[3 * a + 1] * q1 + B.val[3 * a + 2] * q2) * fac;
             }
-            o[g] = (float)(ug[0] - u0);
-            o[npt + g] = (float)(ug[N] - u1);
-            o[2 * npt + g] = (float)(ug[2 * N] - u2);
+            const double w0 = PERSIST ? __ldcg(ug) : ug[0];
+            const double w1 = PERSIST ? __ldcg(ug + N) : ug[N];
+            const double w2 = PERSIST ? __ldcg(ug + 2 * N) : ug[2 * N];
+            o[g] = (float)(w0 - u0);
+            o[npt + g] = (float)(w1 - u1);
+            o[2 * npt + g] = (float)(w2 - u2);
         }
         return;
     }
@@ -429,9 +475,9 @@ __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __rest
             double dd[4][3];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                dd[u][0] = __ldg(us + m[u]) - u0;
-                dd[u][1] = __ldg(us + N + m[u]) - u1;
-                dd[u][2] = __ldg(us + 2 * N + m[u]) - u2;
+                dd[u][0] = ldm<PERSIST>(us + m[u]) - u0;
+                dd[u][1] = ldm<PERSIST>(us + N + m[u]) - u1;
+                dd[u][2] = ldm<PERSIST>(us + 2 * N + m[u]) - u2;
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -447,7 +493,8 @@ __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __rest
     }
     for (; k < nc; ++k) {
         const int64_t m = cb[k];
-        const double d0 = us[m] - u0, d1 = us[N + m] - u1, d2 = us[2 * N + m] - u2;
+        const double d0 = ldm<PERSIST>(us + m) - u0, d1 = ldm<PERSIST>(us + N + m) - u1,
+                     d2 = ldm<PERSIST>(us + 2 * N + m) - u2;
         float c[4];
         if (vec) {
             const float4 v = ld4(cf + k * npt);
@@ -468,6 +515,105 @@ __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __rest
         o[npt + g0 + q] = (float)fma(S, u1, a[q][1]);
         o[2 * npt + g0 + q] = (float)fma(S, u2, a[q][2]);
     }
+}
+
+__global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __restrict__ us) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= d.n * ((d.npt + 3) / 4)) return;
+    gather_group<false>(d, us, tid, *d.tdev);
+}
+
+// ------------------------------------------------------------ persistent
+
+// Grid barrier for one cooperative launch (all blocks co-resident).  The
+// arrival counter only grows: barrier k of the launch is passed once it
+// reaches (k+1) * gridDim.x.  The wait is bounded: after kBarrierNs without
+// completion the block sets the error word and every block leaves at its next
+// barrier; the host reads the word and reports PD_ERR_TIMEOUT.
+constexpr unsigned long long kBarrierNs = 4000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_barrier(PersistCtl* ctl, unsigned& passed) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        const unsigned target = (passed + 1) * gridDim.x;
+        __threadfence();
+        atomicAdd(&ctl->arrive, 1u);
+        const unsigned long long t0 = global_ns();
+        for (;;) {
+            const unsigned a = *((volatile unsigned*)&ctl->arrive);
+            if (a >= target) break;
+            if (*((volatile int*)&ctl->error) != 0) { ok = 0; break; }
+            if (global_ns() - t0 > kBarrierNs) {
+                atomicExch(&ctl->error, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(100);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    ++passed;
+    return ok != 0;
+}
+
+// One work-queue phase: blocks take chunks of `chunk` items from a counter
+// of their own (one counter per phase of the launch, zeroed before it).
+template <typename F>
+__device__ __forceinline__ void run_queue(unsigned* counter, int64_t nitems, unsigned chunk, F&& work) {
+    __shared__ unsigned long long base_s;
+    for (;;) {
+        if (threadIdx.x == 0) base_s = (unsigned long long)atomicAdd(counter, chunk);
+        __syncthreads();
+        const int64_t base = (int64_t)base_s;
+        __syncthreads();
+        if (base >= nitems) break;
+        const int64_t end = base + chunk < nitems ? base + chunk : nitems;
+        for (int64_t it = base + threadIdx.x; it < end; it += blockDim.x) work(it);
+    }
+}
+
+// nsteps RK4 steps of the FP32-compensated FGI form (2x2x2 points) in one
+// launch.  Per stage two phases separated by grid barriers: (a) the bond
+// forces of node pairs fused with the stage epilogue of both nodes, (b) the
+// MLS gather of the trial displacement (of U after stage 4).  Same arithmetic
+// as the separate launches of one graph-captured step, so the same result bit
+// for bit.  The time advances as k_advance_time advances it.
+template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
+__global__ void __launch_bounds__(128, 4) k_persist_f32c(Dev d, PointPack<8> G, double dt, int nsteps,
+                                                         PersistCtl* ctl, unsigned force_chunk,
+                                                         unsigned gather_chunk) {
+    const int64_t N = d.n;
+    const int64_t npairs = (N + 1) / 2;
+    const int64_t ngather = N * ((d.npt + 3) / 4);
+    unsigned passed = 0;
+    // every block reads the start time before the first barrier; block 0
+    // writes the end time after the last one
+    double t = __ldcg(d.tdev);
+    const double dtHalf = 0.5 * dt;
+    for (int step = 0; step < nsteps; ++step) {
+        t = t + dt;
+        for (int stage = 1; stage <= 4; ++stage) {
+            const double dts = stage <= 2 ? dtHalf : dt;
+            unsigned* q = ctl->next + 8 * (int64_t)step + 2 * (stage - 1);
+            run_queue(q, npairs, force_chunk, [&](int64_t it) {
+                force_pair<HASFAIL, LAT, BDRY, SFAC, MULTIMAT, true>(d, G, dts, 2 * it, stage, dt, t);
+            });
+            if (!grid_barrier(ctl, passed)) return;
+            const double* src = stage < 4 ? d.us : d.U;
+            run_queue(q + 1, ngather, gather_chunk, [&](int64_t it) { gather_group<true>(d, src, it, t); });
+            if (!grid_barrier(ctl, passed)) return;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.tdev = t;
 }
 
 template <int NPT>
@@ -509,6 +655,50 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
     }
     if (d.sfac) k_force_f32c_any<true><<<nb, 128, 0, s>>>(d, dts);
     else k_force_f32c_any<false><<<nb, 128, 0, s>>>(d, dts);
+}
+
+// The persistent kernel's variant for the problem, and how many of its
+// blocks fit on the device at once (a cooperative launch needs all resident).
+namespace {
+using PersistFn = void (*)(Dev, PointPack<8>, double, int, PersistCtl*, unsigned, unsigned);
+PersistFn persist_variant(const Dev& d) {
+    const bool lat = d.lat != nullptr, bd = d.bdry_on != 0, sf = d.sfac != nullptr;
+    if (d.hasfail || d.multimat) return k_persist_f32c<true, false, true, true, true>;
+    if (lat) {
+        if (bd) return sf ? k_persist_f32c<false, true, true, true, false> : k_persist_f32c<false, true, true, false, false>;
+        return sf ? k_persist_f32c<false, true, false, true, false> : k_persist_f32c<false, true, false, false, false>;
+    }
+    if (bd) return sf ? k_persist_f32c<false, false, true, true, false> : k_persist_f32c<false, false, true, false, false>;
+    return sf ? k_persist_f32c<false, false, false, true, false> : k_persist_f32c<false, false, false, false, false>;
+}
+}  // namespace
+
+int persist_max_blocks(const Dev& d, int* per_sm, int* sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PD_ERR_CUDA;
+    if (cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return PD_ERR_CUDA;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop) return PD_ERR_CUDA;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, persist_variant(d), 128, 0) != cudaSuccess)
+        return PD_ERR_CUDA;
+    return PD_OK;
+}
+
+cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl* ctl, int blocks,
+                                unsigned force_chunk, unsigned gather_chunk, cudaStream_t s) {
+    const PointPack<8> P = pack_points<8>(d, d.gc_host);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, persist_variant(d), d, P, dt, nsteps, ctl, force_chunk, gather_chunk);
 }
 
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {

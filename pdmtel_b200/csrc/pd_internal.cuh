@@ -129,6 +129,19 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s);
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
 
+// persistent FP32C stepping (pd_f32c.cu): control block of one launch.
+// next[8*step + 2*(stage-1) + phase] are the work-queue counters; all of it
+// is zeroed before every launch.
+struct PersistCtl {
+    unsigned arrive;
+    int error;
+    unsigned pad[30];
+    unsigned next[1];  // [8 * nsteps]
+};
+int persist_max_blocks(const Dev& d, int* per_sm, int* sms);
+cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl* ctl, int blocks,
+                                unsigned force_chunk, unsigned gather_chunk, cudaStream_t s);
+
 // CG helpers (pd_fast.cu): slots of the device scalar array
 enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_NSLOT = 8 };
 void launch_dot_f64(const double* a, const double* b, int64_t n, double* part, double* out, cudaStream_t s);
