@@ -2,6 +2,7 @@
 """Bond-force evaluations per second of the pdMTEL hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form precision|batch|static]
 
 Workload: the pre-cracked plate, 400x400x4 nodes on a cubic lattice (spacing
 0.5 mm, horizon 3.015 spacings, E = 72 GPa, rho = 2440 kg/m^3, 2x2x2 Gauss
@@ -19,6 +20,21 @@ state uploaded from pinned memory and downloaded every step).
 reference: the reference CPU solver (oracle/_ref, built from the reference
 sources) on a 40x40x4 sub-plate of the same workload, one process per host
 core, each step one RK4 step of every process.
+
+The headline line also carries `adjoint`: seconds per RK4 step of the
+differentiation form (forward with checkpoints + reverse sweep, FP64) on the
+64x64x8 identification specimen (spacing 1 mm, fixed face and 0.02 m/s pulled
+face, log-micromodulus a Gaussian random field, sigma 0.2, correlation 5 mm).
+
+--form batch: the batching form, 256 specimens with node counts log-uniform
+in [1k, 60k] (aspect factors uniform in [1, 4]), lognormal micromodulus
+factors (sigma 0.15, correlation 4 spacings), K RK4 steps of all specimens
+batched (launch shape from the autotuner: one persistent launch or the
+graph of a step) against the same specimens stepped one context at a time.
+
+--form static: the 128^3 cube (bottom clamped, 1 MPa shear traction on top),
+CG to relative residual 1e-10: FP32 matvec inside FP64 iterative refinement
+against plain FP64 CG; time to solution and the difference of the solutions.
 
 Multi-GPU: replicas (one full plate per rank, no data-path collective);
 weak scaling; time = max over ranks of the device-timed region.
@@ -51,6 +67,35 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+def rank_barrier(ws):
+    """all ranks meet (after their device work is done)"""
+    import torch
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    """the max of a per-rank scalar over all ranks (NCCL on the GPU, or
+    whatever backend the process group has)"""
+    if ws == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(ws, work_per_rank, seconds_max):
+    """whole-job rate of `ws` replicas: every rank's work over the slowest
+    rank's time"""
+    return ws * work_per_rank / seconds_max
 
 
 def load_peaks():
@@ -174,6 +219,163 @@ def run_reference_arm(args):
     return 0
 
 
+IDENT = dict(dims=(64, 64, 8), spacing=1e-3, vel=0.02, dt=1e-8, sigma=0.2, corr=5e-3, every=50)
+
+
+def adjoint_leg(tmp, steps):
+    """Seconds per RK4 step of the adjoint pair on the identification
+    specimen: pd_adjoint_forward (checkpoints) + pd_adjoint_backward."""
+    import numpy as np
+    import torch
+    import pdmtel_b200 as P
+    from pdmtel_b200 import adjoint as AD
+    from pdmtel_b200 import decks as D
+    wd = os.path.join(tmp, "ident")
+    c = IDENT
+    D.config_identify(dims=c["dims"], spacing=c["spacing"], vel=c["vel"], dt=c["dt"], steps=steps).write(wd)
+    dm = P.pdDataManager(wd)
+    P.pdSolve.InitialProblem(dm)
+    ctx = dm.context()
+    x, _, _ = dm.nodes()
+    ctx.set_spring_factor(np.exp(AD.gaussian_random_field(x, c["spacing"], c["corr"], c["sigma"], seed=1)))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for name, prec in (("fp64", P.PREC_FP64), ("fp64a", P.PREC_FP64A)):
+        ctx.set_precision(prec)
+        ctx.reset_state()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        ctx.adjoint_forward(c["dt"], 0.0, steps, c["every"])
+        ev[1].record(stream)
+        U, _ = ctx.get_state()
+        g = ctx.adjoint_backward(U)
+        ev[2].record(stream)
+        ev[2].synchronize()
+        fw = ev[0].elapsed_time(ev[1]) / 1e3
+        bw = ev[1].elapsed_time(ev[2]) / 1e3
+        out[name] = {"s_per_step": (fw + bw) / steps, "forward_s_per_step": fw / steps,
+                     "backward_s_per_step": bw / steps, "grad_norm": float(np.linalg.norm(g))}
+    ev_step = 4 * ctx.evals_per_stage()
+    dm.close()
+    res = dict(out["fp64"])
+    res.update({"unit": "s/step", "steps": steps, "checkpoint_every": c["every"], "nodes": int(x.size // 3),
+                "evals_per_step": ev_step, "fp64a": out["fp64a"],
+                "config": "64x64x8 identification specimen, J = 0.5|U|^2, forward + reverse sweep in FP64"})
+    return res
+
+
+def run_batch(args):
+    """--form batch"""
+    import torch
+    import pdmtel_b200 as P
+    from pdmtel_b200 import batch as B
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    tmp = tempfile.mkdtemp(prefix=f"pdbatch{rank}_")
+    t0 = time.time()
+    spec = B.BatchSpec(dims=B.draw_dims(256, 2026 + rank), seed=2026 + rank)
+    bt = B.Batch(tmp, spec, precision=P.PREC_FP32C)
+    setup_s = time.time() - t0
+    stream = torch.cuda.ExternalStream(bt.ctx.stream)
+    ev_step = bt.evals_per_step()
+    tune = bt.tune(steps=2)
+
+    def timed(fn):
+        bt.ctx.reset_state()
+        fn(args.warmup)
+        bt.ctx.reset_state()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    t_b = timed(lambda k: bt.run(k))
+    clocks = sampler.stop()
+    t_other = timed(lambda k: bt.run(k, persistent=not bt.persistent))
+    # one context per specimen, stepped one after the other
+    ctxs = bt.specimen_contexts(P.PREC_FP32C)
+    t_seq = 0.0
+    for c in ctxs:
+        c.rk4_steps(spec.dt, 0.0, args.warmup)
+        c.sync()
+        c.reset_state()
+        s = torch.cuda.ExternalStream(c.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        c.rk4_steps(spec.dt, 0.0, args.steps)
+        e1.record(s)
+        e1.synchronize()
+        t_seq += e0.elapsed_time(e1) / 1e3
+    value = ev_step * args.steps / t_b
+    n = int(bt.offsets[-1])
+    line = {"metric": "bond-force evals/s, 256 specimens in one batch (FP32-comp)", "value": value,
+            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_b / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "256 box specimens, nodes log-uniform [1k, 60k], aspect [1, 4], "
+                                   "lognormal micromodulus (sigma 0.15, corr 4 spacings), fixed + pulled faces",
+                       "nodes": n, "evals_per_step": ev_step, "form": "batched, one context"},
+            "autotune": tune,
+            "launch": "persistent" if bt.persistent else "graph of one step",
+            "other_launch": {"launch": "graph of one step" if bt.persistent else "persistent",
+                             "value": ev_step * args.steps / t_other},
+            "sequential": {"value": ev_step * args.steps / t_seq, "ms_per_step": 1e3 * t_seq / args.steps,
+                           "speedup_batched_over_sequential": t_seq / t_b},
+            "gpu_launches": 1 if bt.persistent else 13 * args.steps,
+            "clocks": clocks, "setup_s": setup_s}
+    print(json.dumps(line))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def run_static(args):
+    """--form static"""
+    import numpy as np
+    import torch
+    import pdmtel_b200 as P
+    from pdmtel_b200 import decks as D
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp(prefix="pdstatic_")
+    D.config_cube(n=128, intg_point=1).write(tmp)
+    t0 = time.time()
+    dm = P.pdDataManager(tmp)
+    dm.InitNode()
+    dm.InitBond()
+    dm.InitMaterial()
+    ctx = dm.context()
+    setup_s = time.time() - t0
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    I = dm.info()
+    res = {}
+    for name, prec in (("fp64", P.PREC_FP64), ("fp32c", P.PREC_FP32C)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        x, it, rr = ctx.static_solve(1.0, precision=prec, rtol=1e-10)
+        e1.record(stream)
+        e1.synchronize()
+        res[name] = {"s": e0.elapsed_time(e1) / 1e3, "iterations": it, "rel_residual": rr, "x": x}
+    err = float(np.linalg.norm(res["fp32c"]["x"] - res["fp64"]["x"]) / np.linalg.norm(res["fp64"]["x"]))
+    for r in res.values():
+        r.pop("x")
+    line = {"metric": "static solve time to relative residual 1e-10, 128^3 cube", "value": res["fp32c"]["s"],
+            "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * res["fp32c"]["s"],
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "cube 128^3, bottom clamped, 1 MPa shear traction on top",
+                       "nodes": I.num_nodes, "bond_halves": I.num_halves},
+            "fp32_ir": res["fp32c"], "fp64_cg": res["fp64"], "speedup_fp32ir_over_fp64": res["fp64"]["s"] / res["fp32c"]["s"],
+            "rel_diff_fp32ir_vs_fp64": err, "setup_s": setup_s}
+    print(json.dumps(line))
+    dm.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -197,16 +399,7 @@ def run_ours(args):
     n = ctx.n
 
     def barrier():
-        torch.cuda.synchronize()
-        if ws > 1:
-            torch.distributed.barrier()
-
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        rank_barrier(ws)
 
     def timed(prec, sampler=None):
         ctx.set_precision(prec)
@@ -223,7 +416,7 @@ def run_ours(args):
         e1.synchronize()
         clocks = sampler.stop() if sampler else None
         barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1))
+        ms = max_over_ranks(e0.elapsed_time(e1), ws)
         U, V = ctx.get_state()
         return ms, U, V, clocks
 
@@ -266,7 +459,7 @@ def run_ours(args):
     e1.record(stream)
     e1.synchronize()
     barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), ws)
 
     I = dm.info()
     hbm_peak, peak_kind = load_peaks()
@@ -281,7 +474,7 @@ def run_ours(args):
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("force_f32c_bytes_per_launch")
-    value = ws * evals_step * args.steps / (ms32 / 1e3)
+    value = replica_throughput(ws, evals_step * args.steps, ms32 / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
@@ -311,6 +504,8 @@ def run_ours(args):
                                         "other": prof64[3]}},
         "clocks": clocks, "setup_s": setup_s,
     }
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(tmp, args.adjoint_steps)
     if rank == 0 and not args.no_cpu_baseline:
         outs = cpu_baseline_reference(1, 2, tmp)
         if outs:
@@ -337,11 +532,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=100)
+    ap.add_argument("--form", default="precision", choices=["precision", "batch", "static"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.form == "batch":
+        return run_batch(args)
+    if args.form == "static":
+        return run_static(args)
     return run_ours(args)
 
 

@@ -188,11 +188,12 @@ def config_identify(dims=(64, 64, 8), spacing=1e-3, vel=0.02, dt=5e-8, steps=100
                 bdry_eff=0, intg_point=2)
 
 
-def config_cube(n=128, spacing=1e-3, traction=1e6) -> Deck:
+def config_cube(n=128, spacing=1e-3, traction=1e6, intg_point=2) -> Deck:
     """The static cube: bottom face (low z) clamped, top face under a shear
-    traction along x."""
+    traction along x.  The static operator uses the family only, so
+    intg_point=1 (no MLS) skips the Gauss-point setup."""
     dims = (n, n, n)
     bcs = [BC(DISPL, (1, 1, 1), (0.0, 0.0, 0.0), 1.0, 2.0), BC(TRACTION, (1, 0, 0), (traction, 0.0, 0.0), 1.0, 2.0)]
     return Deck(dims=dims, spacing=spacing, horizon=3.015 * spacing, total_time=1.0, total_step=1, fixed_dt=1.0,
                 bcs=bcs, bc_spaces=[Space(1, face_box(dims, spacing, 2, -1)), Space(2, face_box(dims, spacing, 2, +1))],
-                bdry_eff=0, intg_point=2)
+                bdry_eff=0, intg_point=intg_point)
