@@ -217,6 +217,10 @@ int pd_bond_search_noalloc(const double* coords, int64_t num_nodes, double grid_
                            int32_t num_slits, const double* slits, int64_t* row_ptr, int32_t* col, uint8_t* broken,
                            int64_t capacity, void* stream, int64_t* num_halves, double* min_bond_length);
 
+/* Prepares the static operator (done by the first static call otherwise):
+ * decides whether it runs as a lattice stencil (PD_OPT_STATIC_STENCIL) and
+ * builds the stencil; *stencil (may be NULL) receives 1 if it does. */
+int pd_static_prepare(pd_ctx* ctx, int* stencil);
 /* Linearised stiffness operator of pdSolve::AssembleEquation (pdSolve.cpp:
  * 195-527) applied matrix-free: free rows sum c V_j xi xi^T / r^3 (x_i - x_j)
  * over the unbroken family with prescribed columns masked, prescribed rows
@@ -226,10 +230,12 @@ int pd_static_matvec(pd_ctx* ctx, double time, const double* x, double* y);
  * traction load (value*factor/grid_spacing on TRACTION nodes). */
 int pd_static_rhs(pd_ctx* ctx, double time, double* b);
 /* Matrix-free CG on the static system (the dense Gauss-Jordan of
- * pdSolve::Gauss pdSolve.cpp:545-673 is replaced).  PD_PREC_FP64: plain FP64
- * CG; PD_PREC_FP32C: FP32 matvec inner CG inside FP64 iterative refinement
- * (FP64 residuals and dot products).  x [3N] is the initial guess in and the
- * solution out.  iters/relres may be NULL. */
+ * pdSolve::Gauss pdSolve.cpp:545-673 is replaced).  PD_PREC_FP64: FP64 CG;
+ * PD_PREC_FP32C: the iterations' matvec in FP32 (FP64 vectors, dot products
+ * and node sums), refined in FP64 by replacing the residual with the true
+ * b - K x whenever it has fallen 100-fold and at convergence ("reliable
+ * updates"); convergence is judged on the FP64 true residual.  x [3N] is the
+ * initial guess in and the solution out.  iters/relres may be NULL. */
 int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int maxit, double* x, int* iters,
                     double* relres);
 
@@ -244,13 +250,21 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  * PD_OPT_PERSIST_BLOCKS_PER_SM: blocks per SM of the persistent launch (0:
  *   as many as fit).
  * PD_OPT_PERSIST_FORCE_CHUNK / _GATHER_CHUNK: work items a block takes from
- *   the queue at a time (multiples of 128; defaults 128 and 256). */
+ *   the queue at a time (multiples of 128; defaults 128 and 256).
+ * PD_OPT_STATIC_STENCIL: 1 (default) lets the static operator run as a
+ *   lattice stencil when the problem is a complete box with one material,
+ *   no broken bond and stencil-shaped families (checked); 0 keeps the
+ *   family-list kernel.
+ * PD_OPT_GATHER_PER_POINT: 1 runs the FP32-form MLS gather with one thread
+ *   per (node, Gauss point), 0 (default) with one per four points. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
     PD_OPT_PERSIST_BLOCKS_PER_SM = 3,
     PD_OPT_PERSIST_FORCE_CHUNK = 4,
-    PD_OPT_PERSIST_GATHER_CHUNK = 5
+    PD_OPT_PERSIST_GATHER_CHUNK = 5,
+    PD_OPT_STATIC_STENCIL = 6,
+    PD_OPT_GATHER_PER_POINT = 7
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -274,10 +288,13 @@ typedef struct pd_tune_result {
     int32_t force_chunk, gather_chunk;
     int32_t trials;
     double ms_per_step;    /* device time per step of the kept shape */
+    int32_t gather_per_point; /* PD_OPT_GATHER_PER_POINT kept */
+    int32_t pad;
 } pd_tune_result;
-/* Times candidate launch shapes (node-order tiles; for the persistent launch
- * blocks per SM and queue chunks) over `steps` steps each from the current
- * state, keeps the fastest in the context and restores the state. */
+/* Times candidate launch shapes (node-order tiles, the FP32 gather variant;
+ * for the persistent launch blocks per SM and queue chunks) over `steps`
+ * steps each from the current state, keeps the fastest in the context and
+ * restores the state. */
 int pd_autotune(pd_ctx* ctx, double dt, int steps, pd_tune_result* out);
 
 /* ---- Differentiation: gradient with respect to a per-node micromodulus ----

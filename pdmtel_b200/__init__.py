@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(HERE, "libpdmtel_b200.so")
 PD_OK = 0
 PREC_FP64, PREC_FP32C, PREC_FP64A = 0, 1, 2
 OPT_F64_LANES_BELOW, OPT_TILE, OPT_PERSIST_BLOCKS_PER_SM = 1, 2, 3
-OPT_PERSIST_FORCE_CHUNK, OPT_PERSIST_GATHER_CHUNK = 4, 5
+OPT_PERSIST_FORCE_CHUNK, OPT_PERSIST_GATHER_CHUNK, OPT_STATIC_STENCIL, OPT_GATHER_PER_POINT = 4, 5, 6, 7
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}
@@ -80,7 +80,7 @@ class pdh_info(C.Structure):
 class pd_tune_result(C.Structure):
     _fields_ = [("tile", C.c_int64), ("persistent", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("force_chunk", C.c_int32), ("gather_chunk", C.c_int32), ("trials", C.c_int32),
-                ("ms_per_step", C.c_double)]
+                ("ms_per_step", C.c_double), ("gather_per_point", C.c_int32), ("pad", C.c_int32)]
 
 
 # name -> argtypes; every entry point returns int
@@ -112,6 +112,7 @@ _SIGS = {
     "pd_evals_per_stage": [_vp, _i64],
     "pd_reset_state": [_vp],
     "pd_profile_step": [_vp, C.c_double, C.c_double, _d],
+    "pd_static_prepare": [_vp, C.POINTER(C.c_int)],
     "pd_static_matvec": [_vp, C.c_double, _d, _d],
     "pd_static_rhs": [_vp, C.c_double, _d],
     "pd_static_solve": [_vp, C.c_double, C.c_int, C.c_double, C.c_int, _d, C.POINTER(C.c_int), _d],
@@ -397,6 +398,11 @@ class DeviceContext:
         b = np.zeros(3 * self.n)
         _check(lib().pd_static_rhs(self.h, float(t), _p(b, _d)), "pd_static_rhs")
         return b
+
+    def static_prepare(self):
+        st = C.c_int(0)
+        _check(lib().pd_static_prepare(self.h, C.byref(st)), "pd_static_prepare")
+        return bool(st.value)
 
     def static_solve(self, t, precision=PREC_FP64, rtol=1e-10, maxit=200000, x0=None):
         x = np.zeros(3 * self.n) if x0 is None else _f64(x0, 3 * self.n).copy()

@@ -1,9 +1,11 @@
 // The C ABI of libpdmtel_b200 (include/pdmtel_b200.h): context life cycle,
 // uploads in the reference's row layout, the RK4 driver and the static CG.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -68,6 +70,17 @@ struct pd_ctx {
     int persist_steps = 0;
     uint64_t persist_generation = ~0ull;
     int tuned_persistent = 0;
+    // static operator: per-material springs, lattice stencil (static_prepare)
+    std::vector<double> mat_spring;
+    int static_stencil_opt = 1;
+    int static_replacements = 0;
+    bool sten_ok = false;
+    uint64_t sten_gen = ~0ull;
+    pd::StencilDev sten{};
+    int4* sten_off = nullptr;
+    double4* sten_geo = nullptr;
+    uint8_t* sten_pmask = nullptr;
+    double* sten_xm = nullptr;
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
@@ -450,6 +463,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     c->gch = hg;
     d.gc_host = c->gch.data();
     c->bdry_host.assign(N, 1.0);
+    for (int k = 0; k < P->num_materials; ++k) c->mat_spring.push_back(P->materials[k].spring);
     d.nblk = nblk;
     d.sblk = sblk;
     d.order = order;
@@ -727,6 +741,14 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 32) return fail(PD_ERR_ARG, "pd_set_option: blocks per SM");
             c->persist_per_sm = (int)value;
             break;
+        case PD_OPT_STATIC_STENCIL:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            c->static_stencil_opt = (int)value;
+            break;
+        case PD_OPT_GATHER_PER_POINT:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            c->d.gather_per_point = (int)value;
+            break;
         case PD_OPT_PERSIST_FORCE_CHUNK:
         case PD_OPT_PERSIST_GATHER_CHUNK:
             if (value < 128 || value > (1 << 20) || value % 128) return fail(PD_ERR_ARG, "pd_set_option: chunk");
@@ -746,6 +768,8 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_PERSIST_BLOCKS_PER_SM: *value = c->persist_per_sm; return PD_OK;
         case PD_OPT_PERSIST_FORCE_CHUNK: *value = c->force_chunk; return PD_OK;
         case PD_OPT_PERSIST_GATHER_CHUNK: *value = c->gather_chunk; return PD_OK;
+        case PD_OPT_STATIC_STENCIL: *value = c->static_stencil_opt; return PD_OK;
+        case PD_OPT_GATHER_PER_POINT: *value = c->d.gather_per_point; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
     }
 }
@@ -1014,11 +1038,134 @@ int pd_evals_per_stage(pd_ctx* c, int64_t* ev) {
 
 // ----------------------------------------------------------------- static
 
+}  // extern "C"
+
+namespace {
+
+// Decides once per setup whether the static operator can run as a stencil:
+// every lattice position of a box holds one node, node id = x + nx (y + ny z),
+// one material, no broken family entry, and every node's family is the union
+// stencil clipped to the box (checked node by node on the downloaded family).
+int static_prepare(pd_ctx* c) {
+    if (c->sten_gen == c->generation) return PD_OK;
+    c->sten_ok = false;
+    c->sten_gen = c->generation;
+    if (!c->static_stencil_opt || c->d.multimat || c->d.nmat != 1 || c->n == 0) return PD_OK;
+    const int64_t N = c->n;
+    std::vector<int32_t> lat;
+    if (!lattice_positions(c->coords, N, c->d.dx, lat)) return PD_OK;
+    int64_t dims[3] = {0, 0, 0};
+    for (int64_t i = 0; i < N; ++i) {
+        dims[0] = std::max<int64_t>(dims[0], (lat[i] & 2047) + 1);
+        dims[1] = std::max<int64_t>(dims[1], ((lat[i] >> 11) & 2047) + 1);
+        dims[2] = std::max<int64_t>(dims[2], (lat[i] >> 22) + 1);
+    }
+    if (dims[0] * dims[1] * dims[2] != N) return PD_OK;
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t l = (lat[i] & 2047) + dims[0] * (((lat[i] >> 11) & 2047) + dims[1] * (lat[i] >> 22));
+        if (l != i) return PD_OK;
+    }
+    if (c->Ha != c->H) return PD_OK;  // broken entries
+    std::vector<int64_t> rp(N + 1);
+    std::vector<int32_t> col(std::max<int64_t>(c->H, 1));
+    PD_CUDA_TRY(cudaMemcpy(rp.data(), c->d.frow, sizeof(int64_t) * (N + 1), cudaMemcpyDeviceToHost));
+    PD_CUDA_TRY(cudaMemcpy(col.data(), c->d.fcol, sizeof(int32_t) * c->H, cudaMemcpyDeviceToHost));
+    const int64_t nx = dims[0], ny = dims[1], nz = dims[2];
+    auto pos = [&](int64_t i, int64_t* q) {
+        q[0] = i % nx;
+        q[1] = (i / nx) % ny;
+        q[2] = i / (nx * ny);
+    };
+    // union of the offsets, keyed (ox, oy, oz) in [-64, 63]^3
+    std::vector<uint8_t> seen(128 * 128 * 128, 0);
+    std::vector<std::array<int, 3>> offs;
+    for (int64_t i = 0; i < N; ++i) {
+        int64_t qi[3], qj[3];
+        pos(i, qi);
+        for (int64_t p = rp[i]; p < rp[i + 1]; ++p) {
+            pos(col[p], qj);
+            int o[3];
+            for (int a = 0; a < 3; ++a) {
+                o[a] = (int)(qj[a] - qi[a]);
+                if (o[a] < -64 || o[a] > 63) return PD_OK;
+            }
+            const int key = ((o[0] + 64) << 14) | ((o[1] + 64) << 7) | (o[2] + 64);
+            if (!seen[key]) {
+                seen[key] = 1;
+                offs.push_back({o[0], o[1], o[2]});
+            }
+        }
+    }
+    if (offs.empty() || offs.size() > (size_t)pd::kMaxStencil) return PD_OK;
+    // every node's family has exactly the offsets that stay in the box
+    for (int64_t i = 0; i < N; ++i) {
+        int64_t qi[3];
+        pos(i, qi);
+        int64_t in = 0;
+        for (const auto& o : offs)
+            if (qi[0] + o[0] >= 0 && qi[0] + o[0] < nx && qi[1] + o[1] >= 0 && qi[1] + o[1] < ny &&
+                qi[2] + o[2] >= 0 && qi[2] + o[2] < nz)
+                ++in;
+        if (in != rp[i + 1] - rp[i]) return PD_OK;
+    }
+    std::sort(offs.begin(), offs.end(), [&](const std::array<int, 3>& a, const std::array<int, 3>& b) {
+        return a[0] + nx * (a[1] + ny * a[2]) < b[0] + nx * (b[1] + ny * b[2]);
+    });
+    const int ns = (int)offs.size();
+    std::vector<int4> off(ns);
+    std::vector<double4> geo(ns);
+    const double h = c->d.dx, cv = c->mat_spring[0] * c->d.vol;
+    int radius = 0;
+    for (int k = 0; k < ns; ++k) {
+        const auto& o = offs[k];
+        off[k] = make_int4(o[0], o[1], o[2], (int)(o[0] + nx * (o[1] + ny * o[2])));
+        const double e0 = o[0] * h, e1 = o[1] * h, e2 = o[2] * h;
+        const double r2 = e0 * e0 + e1 * e1 + e2 * e2, r = std::sqrt(r2);
+        geo[k] = make_double4(e0, e1, e2, cv / (r2 * r));
+        for (int a = 0; a < 3; ++a) radius = std::max(radius, std::abs(o[a]));
+    }
+    if (!c->sten_off) {
+        PD_TRY(dalloc(c, &c->sten_off, pd::kMaxStencil));
+        PD_TRY(dalloc(c, &c->sten_geo, pd::kMaxStencil));
+        PD_TRY(dalloc(c, &c->sten_pmask, N));
+        PD_TRY(dalloc(c, &c->sten_xm, 3 * N));
+    }
+    PD_TRY(upload(c, c->sten_off, off.data(), sizeof(int4) * ns));
+    PD_TRY(upload(c, c->sten_geo, geo.data(), sizeof(double4) * ns));
+    pd::launch_static_pmask(c->d, c->sten_pmask, c->stream);
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->sten = pd::StencilDev{(int)nx, (int)ny, (int)nz, ns, radius, c->sten_off, c->sten_geo, c->sten_pmask,
+                             c->sten_xm};
+    c->sten_ok = true;
+    return PD_OK;
+}
+
+// y = K x: the stencil kernel when static_prepare accepted the problem, the
+// family-list kernel otherwise; f32: FP32 bond terms on FP64 vectors
+void static_apply(pd_ctx* c, double time, bool f32, const double* x, double* y) {
+    if (c->sten_ok) pd::launch_static_stencil(c->d, c->sten, f32, x, y, c->stream);
+    else if (f32) pd::launch_static_apply_f32x(c->d, time, x, y, c->stream);
+    else pd::launch_static_apply_f64(c->d, time, x, y, c->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pd_static_prepare(pd_ctx* c, int* stencil) {
+    if (!c) return fail(PD_ERR_ARG, "pd_static_prepare: null context");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_static_prepare: no family");
+    PD_TRY(static_prepare(c));
+    if (stencil) *stencil = c->sten_ok ? 1 : 0;
+    return PD_OK;
+}
+
 int pd_static_matvec(pd_ctx* c, double time, const double* x, double* y) {
     if (!c || !x || !y) return fail(PD_ERR_ARG, "pd_static_matvec: null argument");
     if (!c->have_family) return fail(PD_ERR_ARG, "pd_static_matvec: no family");
+    PD_TRY(static_prepare(c));
     PD_TRY(upload_vec3(c, c->d.us, x));
-    pd::launch_static_apply_f64(c->d, time, c->d.us, c->d.k1, c->stream);
+    static_apply(c, time, false, c->d.us, c->d.k1);
     PD_CUDA_TRY(cudaGetLastError());
     return download_vec3(c, y, c->d.k1);
 }
@@ -1035,73 +1182,83 @@ int pd_static_rhs(pd_ctx* c, double time, double* b) {
 
 namespace {
 
-// plain CG on A x = b, FP64 or FP32 vectors; scalars live on the device and
-// the residual is read back every `check` iterations
-template <typename T>
-int cg_device(pd_ctx* c, double time, const T* b, T* x, T* r, T* p, T* q, double rtol, int maxit, int* iters,
-              double* relres, bool zero_guess) {
+// CG on K x = b with FP64 vectors and device scalars; the residual is read
+// back every 10 iterations.  f32: the matvec of the iterations has FP32 bond
+// terms, and the residual is replaced by the FP64 true residual b - K x
+// whenever the recurred one has fallen by 1e-2 since the last replacement
+// and when it reaches the tolerance ("reliable updates", van der Vorst & Ye,
+// SIAM J. Sci. Comput. 22 (2000) 1716-1731): the FP64 refinement of the
+// FP32 iterations, without restarting the Krylov space.  Convergence is
+// decided on the true residual.
+int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, double* p, double* q, bool f32,
+              double rtol, int maxit, int* iters, double* relres, int* replacements) {
     const int64_t n3 = 3 * c->n;
     cudaStream_t s = c->stream;
     double* scal = c->scal;
-    auto apply = [&](const T* in, T* out) {
-        if constexpr (sizeof(T) == 8) pd::launch_static_apply_f64(c->d, time, (const double*)in, (double*)out, s);
-        else pd::launch_static_apply_f32(c->d, time, (const float*)in, (float*)out, s);
+    auto dot = [&](const double* a, const double* bb, double* out) {
+        pd::launch_dot_f64(a, bb, n3, c->dotpart, out, s);
     };
-    auto dot = [&](const T* a, const T* bb, double* out) {
-        if constexpr (sizeof(T) == 8) pd::launch_dot_f64((const double*)a, (const double*)bb, n3, c->dotpart, out, s);
-        else pd::launch_dot_f32((const float*)a, (const float*)bb, n3, c->dotpart, out, s);
-    };
-    dot(b, b, scal + pd::CG_BB);
-    if (zero_guess) {
-        PD_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * n3, s));
-        PD_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(T) * n3, cudaMemcpyDeviceToDevice, s));
-    } else {
-        apply(x, q);
-        if constexpr (sizeof(T) == 8) pd::launch_sub_f64((const double*)b, (const double*)q, (double*)r, n3, s);
-        else return fail(PD_ERR_ARG, "FP32 CG needs a zero initial guess");
-    }
-    PD_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(T) * n3, cudaMemcpyDeviceToDevice, s));
-    dot(r, r, scal + pd::CG_RR);
-    PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
-    PD_CUDA_TRY(cudaStreamSynchronize(s));
-    const double bb = c->hscalar[pd::CG_BB] > 0.0 ? c->hscalar[pd::CG_BB] : 1.0;
-    double rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
-    int it = 0;
-    const int check = 10;
-    while (rel > rtol && it < maxit) {
-        for (int k = 0; k < check && it < maxit; ++k, ++it) {
-            apply(p, q);
-            dot(p, q, scal + pd::CG_PQ);
-            if constexpr (sizeof(T) == 8) {
-                pd::launch_cg_update_x_f64((double*)x, (double*)r, (const double*)p, (const double*)q, n3, scal, s);
-                dot(r, r, scal + pd::CG_RRN);
-                pd::launch_cg_update_p_f64((const double*)r, (double*)p, n3, scal, s);
-            } else {
-                pd::launch_cg_update_x_f32((float*)x, (float*)r, (const float*)p, (const float*)q, n3, scal, s);
-                dot(r, r, scal + pd::CG_RRN);
-                pd::launch_cg_update_p_f32((const float*)r, (float*)p, n3, scal, s);
-            }
-            pd::launch_cg_swap(scal, s);
-        }
+    auto read = [&]() -> int {
         PD_CUDA_TRY(cudaGetLastError());
         PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
         PD_CUDA_TRY(cudaStreamSynchronize(s));
+        return PD_OK;
+    };
+    // true residual into r, |r|^2 into scal[CG_RR]
+    auto true_residual = [&]() {
+        static_apply(c, time, false, x, q);
+        pd::launch_sub_f64(b, q, r, n3, s);
+        dot(r, r, scal + pd::CG_RR);
+    };
+    dot(b, b, scal + pd::CG_BB);
+    true_residual();
+    PD_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_TRY(read());
+    const double bb = c->hscalar[pd::CG_BB] > 0.0 ? c->hscalar[pd::CG_BB] : 1.0;
+    double rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+    double since = rel;  // largest recurred residual since the last replacement
+    int it = 0, nrep = 0;
+    const int check = 10;
+    while (rel > rtol && it < maxit) {
+        for (int k = 0; k < check && it < maxit; ++k, ++it) {
+            static_apply(c, time, f32, p, q);
+            dot(p, q, scal + pd::CG_PQ);
+            pd::launch_cg_update_x_f64(x, r, p, q, n3, scal, s);
+            dot(r, r, scal + pd::CG_RRN);
+            pd::launch_cg_update_p_f64(r, p, n3, scal, s);
+            pd::launch_cg_swap(scal, s);
+        }
+        PD_TRY(read());
         rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
         if (!std::isfinite(rel)) break;
+        since = std::max(since, rel);
+        if (f32 && (rel <= rtol || rel < 1e-2 * since)) {
+            // replace: r = b - K x in FP64; p keeps its direction
+            true_residual();
+            PD_TRY(read());
+            rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+            since = rel;
+            ++nrep;
+        }
     }
     if (iters) *iters = it;
     if (relres) *relres = rel;
+    if (replacements) *replacements = nrep;
     return (rel <= rtol) ? PD_OK : PD_ERR_NOCONV;
 }
 
 }  // namespace
 
+// Matrix-free CG on the static system (replaces the dense Gauss-Jordan of
+// pdSolve::Gauss, pdSolve.cpp:545-673).
 extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rtol, int maxit, double* x, int* iters,
-                    double* relres) {
+                               double* relres) {
     if (!c || !x) return fail(PD_ERR_ARG, "pd_static_solve: null argument");
     if (!c->have_family) return fail(PD_ERR_ARG, "pd_static_solve: no family");
+    if (precision != PD_PREC_FP64 && precision != PD_PREC_FP64A && precision != PD_PREC_FP32C)
+        return fail(PD_ERR_ARG, "pd_static_solve: precision");
+    PD_TRY(static_prepare(c));
     const int64_t n3 = 3 * c->n;
-    cudaStream_t s = c->stream;
     double *b = nullptr, *xd = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
     PD_TRY(dalloc(c, &b, n3));
     PD_TRY(dalloc(c, &xd, n3));
@@ -1111,53 +1268,14 @@ extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rto
     auto cleanup = [&]() { dfree(c, b); dfree(c, xd); dfree(c, r); dfree(c, p); dfree(c, q); };
     int rc = upload_vec3(c, xd, x);
     if (rc != PD_OK) { cleanup(); return rc; }
-    pd::launch_static_rhs(c->d, time, b, s);
-    int it_total = 0;
+    pd::launch_static_rhs(c->d, time, b, c->stream);
+    int it = 0, nrep = 0;
     double rel = 0.0;
-    if (precision == PD_PREC_FP64 || precision == PD_PREC_FP64A) {
-        rc = cg_device<double>(c, time, b, xd, r, p, q, rtol, maxit, &it_total, &rel, false);
-    } else {
-        // iterative refinement: FP64 residual, FP32 inner CG on the scaled residual
-        float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *b32 = nullptr;
-        rc = dalloc(c, &d32, n3);
-        if (rc == PD_OK) rc = dalloc(c, &r32, n3);
-        if (rc == PD_OK) rc = dalloc(c, &p32, n3);
-        if (rc == PD_OK) rc = dalloc(c, &q32, n3);
-        if (rc == PD_OK) rc = dalloc(c, &b32, n3);
-        double bb = 0.0;
-        if (rc == PD_OK) {
-            pd::launch_dot_f64(b, b, n3, c->dotpart, c->scal + pd::CG_BB, s);
-            cudaMemcpyAsync(c->hscalar + 4, c->scal + pd::CG_BB, sizeof(double), cudaMemcpyDeviceToHost, s);
-            cudaStreamSynchronize(s);
-            bb = std::sqrt(c->hscalar[4]);
-            if (!(bb > 0.0)) bb = 1.0;
-        }
-        int outer = 0;
-        while (rc == PD_OK) {
-            pd::launch_static_apply_f64(c->d, time, xd, q, s);
-            pd::launch_sub_f64(b, q, r, n3, s);
-            pd::launch_dot_f64(r, r, n3, c->dotpart, c->scal + pd::CG_RRN, s);
-            cudaMemcpyAsync(c->hscalar + 4, c->scal + pd::CG_RRN, sizeof(double), cudaMemcpyDeviceToHost, s);
-            if (cudaStreamSynchronize(s) != cudaSuccess) { rc = fail(PD_ERR_CUDA, "refinement residual"); break; }
-            const double rn = std::sqrt(c->hscalar[4]);
-            rel = rn / bb;
-            if (rel <= rtol || it_total >= maxit || outer > 60 || !std::isfinite(rel)) break;
-            ++outer;
-            // inner solve on r / |r| in FP32 to a relative 1e-4
-            pd::launch_f64_to_f32(r, b32, 1.0 / rn, n3, s);
-            int inner = 0;
-            double irel = 0.0;
-            int irc = cg_device<float>(c, time, b32, d32, r32, p32, q32, 1e-4, maxit - it_total, &inner, &irel, true);
-            it_total += inner;
-            if (irc != PD_OK && irc != PD_ERR_NOCONV) { rc = irc; break; }
-            pd::launch_add_f32_to_f64(xd, d32, rn, n3, s);
-        }
-        dfree(c, d32); dfree(c, r32); dfree(c, p32); dfree(c, q32); dfree(c, b32);
-        if (rc == PD_OK && rel > rtol) rc = PD_ERR_NOCONV;
-    }
+    rc = cg_static(c, time, b, xd, r, p, q, precision == PD_PREC_FP32C, rtol, maxit, &it, &rel, &nrep);
+    c->static_replacements = nrep;
     int rc2 = download_vec3(c, x, xd);
     cleanup();
-    if (iters) *iters = it_total;
+    if (iters) *iters = it;
     if (relres) *relres = rel;
     if (rc == PD_ERR_NOCONV) return fail(PD_ERR_NOCONV, "static solve did not reach the tolerance");
     return rc != PD_OK ? rc : rc2;
@@ -1622,6 +1740,16 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
     }
     for (int64_t tl : tiles)
         if ((rc = trial({tl, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0})) != PD_OK) return done(rc);
+    if (c->precision == PD_PREC_FP32C && c->d.mls) {
+        // the gather variant, on the best tile so far
+        const int gp0 = c->d.gather_per_point;
+        const double before = best.ms;
+        c->d.gather_per_point = !gp0;
+        Trial T{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+        if ((rc = trial(T)) != PD_OK) return done(rc);
+        if (!(best.ms < before)) c->d.gather_per_point = gp0;
+        out->gather_per_point = c->d.gather_per_point;
+    }
     if (persist_capable(c)) {
         int per_sm = 0, sms = 0;
         if (pd::persist_max_blocks(c->d, &per_sm, &sms) == PD_OK && per_sm >= 1) {

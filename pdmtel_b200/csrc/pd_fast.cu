@@ -72,8 +72,11 @@ __global__ void k_static_apply_f64(Dev d, double t, const double* __restrict__ x
     y[2 * N + i] = pi[2] ? x[2 * N + i] : a2;
 }
 
+// The same operator with FP32 arithmetic on FP64 vectors: the per-bond
+// difference x_i - x_j is formed in FP64 and rounded once, the bond term is
+// FP32, the node sum FP64.  The matvec of the mixed-precision CG.
 template <bool SFAC>
-__global__ void k_static_apply_f32(Dev d, double t, const float* __restrict__ x, float* __restrict__ y) {
+__global__ void k_static_apply_f32x(Dev d, double t, const double* __restrict__ x, double* __restrict__ y) {
     const int64_t N = d.n;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -81,35 +84,126 @@ __global__ void k_static_apply_f32(Dev d, double t, const float* __restrict__ x,
     double pv[3];
     prescribed(d, i, t, pi, pv);
     const double X0 = d.x[i], X1 = d.x[N + i], X2 = d.x[2 * N + i];
-    const float xi0 = pi[0] ? 0.f : x[i], xi1 = pi[1] ? 0.f : x[N + i], xi2 = pi[2] ? 0.f : x[2 * N + i];
+    const double xi0 = pi[0] ? 0.0 : x[i], xi1 = pi[1] ? 0.0 : x[N + i], xi2 = pi[2] ? 0.0 : x[2 * N + i];
     const double ci = d.mats[d.mat[i]].spring;
     const double sfi = SFAC ? d.sfac[i] : 0.0;
-    const float cv = (float)(ci * d.vol);
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
         const int64_t j = d.acol[p];
         bool pj[3];
         double qv[3];
         prescribed(d, j, t, pj, qv);
         const float e0 = (float)(d.x[j] - X0), e1 = (float)(d.x[N + j] - X1), e2 = (float)(d.x[2 * N + j] - X2);
-        const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
-        const float rinv = rsqrtf(r2);
-        float c = cv;
         const double cj = d.mats[d.mat[j]].spring;
-        if (cj < ci) c = (float)(cj * d.vol);
-        if (SFAC) c = c * (float)(0.5 * (sfi + d.sfac[j]));
-        const float w = c * rinv * rinv * rinv;
-        const float d0 = xi0 - (pj[0] ? 0.f : x[j]);
-        const float d1 = xi1 - (pj[1] ? 0.f : x[N + j]);
-        const float d2 = xi2 - (pj[2] ? 0.f : x[2 * N + j]);
-        const float pr = w * (e0 * d0 + e1 * d1 + e2 * d2);
-        a0 = fmaf(pr, e0, a0);
-        a1 = fmaf(pr, e1, a1);
-        a2 = fmaf(pr, e2, a2);
+        double c = (cj < ci) ? cj : ci;
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const float rinv = rsqrtf(fmaf(e0, e0, fmaf(e1, e1, e2 * e2)));
+        const float w = (float)(c * d.vol) * rinv * rinv * rinv;
+        const float d0 = (float)(xi0 - (pj[0] ? 0.0 : x[j]));
+        const float d1 = (float)(xi1 - (pj[1] ? 0.0 : x[N + j]));
+        const float d2 = (float)(xi2 - (pj[2] ? 0.0 : x[2 * N + j]));
+        const float pr = w * fmaf(e0, d0, fmaf(e1, d1, e2 * d2));
+        a0 += (double)(pr * e0);
+        a1 += (double)(pr * e1);
+        a2 += (double)(pr * e2);
     }
     y[i] = pi[0] ? x[i] : a0;
     y[N + i] = pi[1] ? x[N + i] : a1;
     y[2 * N + i] = pi[2] ? x[2 * N + i] : a2;
+}
+
+// prescribed directions of every node as bits 0..2 (the static operator's
+// masks do not depend on the time)
+__global__ void k_static_pmask(Dev d, uint8_t* __restrict__ pm) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    bool pr[3];
+    double v[3];
+    prescribed(d, i, 0.0, pr, v);
+    pm[i] = (uint8_t)((pr[0] ? 1 : 0) | (pr[1] ? 2 : 0) | (pr[2] ? 4 : 0));
+}
+
+// The operator on a complete box lattice whose families are the horizon
+// stencil clipped to the box: the neighbour of slot k is i + off[k].w when
+// the shifted lattice position stays in the box; the bond geometry and
+// c V / r^3 come from the stencil table (one material).  No family list and
+// no coordinates are read.  Threads take nodes in lattice order, so for one
+// stencil slot a warp reads 32 consecutive neighbours; nodes at least the
+// stencil radius inside the box skip the box test.  The input arrives
+// masked (prescribed components zeroed, k_static_mask): FP64, or FP32 for
+// the FP32 operator, whose bond terms are FP32 and node sums FP64.
+template <typename T>
+__global__ void k_static_mask(const uint8_t* __restrict__ pmask, int64_t N, const double* __restrict__ x,
+                              T* __restrict__ xm) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const unsigned m = pmask[i];
+    xm[i] = (m & 1) ? (T)0 : (T)x[i];
+    xm[N + i] = (m & 2) ? (T)0 : (T)x[N + i];
+    xm[2 * N + i] = (m & 4) ? (T)0 : (T)x[2 * N + i];
+}
+
+template <typename T, bool SFAC, bool CHECK>
+__device__ __forceinline__ void stencil_sum(const Dev& d, const StencilDev& S, const double4* sgeo, const int4* soff,
+                                            int64_t i, int ix, int iy, int iz, const T* __restrict__ xm, T xi0,
+                                            T xi1, T xi2, double sfi, double& r0, double& r1, double& r2) {
+    const int64_t N = d.n;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int k = 0; k < S.ns; ++k) {
+        const int4 o = soff[k];
+        if (CHECK && ((unsigned)(ix + o.x) >= (unsigned)S.nx || (unsigned)(iy + o.y) >= (unsigned)S.ny ||
+                      (unsigned)(iz + o.z) >= (unsigned)S.nz))
+            continue;
+        const int64_t j = i + o.w;
+        const double4 g = sgeo[k];
+        const T d0 = xi0 - xm[j], d1 = xi1 - xm[N + j], d2 = xi2 - xm[2 * N + j];
+        if (sizeof(T) == 4) {
+            float w = (float)g.w;
+            if (SFAC) w *= (float)(0.5 * (sfi + d.sfac[j]));
+            const float e0 = (float)g.x, e1 = (float)g.y, e2 = (float)g.z;
+            const float pr = w * fmaf(e0, (float)d0, fmaf(e1, (float)d1, e2 * (float)d2));
+            a0 += (double)(pr * e0);
+            a1 += (double)(pr * e1);
+            a2 += (double)(pr * e2);
+        } else {
+            double w = g.w;
+            if (SFAC) w = w * (0.5 * (sfi + d.sfac[j]));
+            const double pr = w * (g.x * (double)d0 + g.y * (double)d1 + g.z * (double)d2);
+            a0 += pr * g.x;
+            a1 += pr * g.y;
+            a2 += pr * g.z;
+        }
+    }
+    r0 = a0;
+    r1 = a1;
+    r2 = a2;
+}
+
+template <typename T, bool SFAC>
+__global__ void __launch_bounds__(256) k_static_stencil(Dev d, StencilDev S, const double* __restrict__ x,
+                                                        const T* __restrict__ xm, double* __restrict__ y) {
+    extern __shared__ double4 sgeo[];
+    int4* soff = reinterpret_cast<int4*>(sgeo + S.ns);
+    for (int k = threadIdx.x; k < S.ns; k += blockDim.x) {
+        sgeo[k] = S.geo[k];
+        soff[k] = S.off[k];
+    }
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int ix = (int)(i % S.nx), iy = (int)((i / S.nx) % S.ny), iz = (int)(i / ((int64_t)S.nx * S.ny));
+    const unsigned mi = S.pmask[i];
+    const T xi0 = xm[i], xi1 = xm[N + i], xi2 = xm[2 * N + i];
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    double a0, a1, a2;
+    const int R = S.radius;
+    const bool inner = ix >= R && ix < S.nx - R && iy >= R && iy < S.ny - R && iz >= R && iz < S.nz - R;
+    if (inner) stencil_sum<T, SFAC, false>(d, S, sgeo, soff, i, ix, iy, iz, xm, xi0, xi1, xi2, sfi, a0, a1, a2);
+    else stencil_sum<T, SFAC, true>(d, S, sgeo, soff, i, ix, iy, iz, xm, xi0, xi1, xi2, sfi, a0, a1, a2);
+    y[i] = (mi & 1) ? x[i] : a0;
+    y[N + i] = (mi & 2) ? x[N + i] : a1;
+    y[2 * N + i] = (mi & 4) ? x[2 * N + i] : a2;
 }
 
 // b = prescribed values on prescribed rows; on free rows the moved prescribed
@@ -239,10 +333,32 @@ void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y,
     else k_static_apply_f64<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
 }
 
-void launch_static_apply_f32(const Dev& d, double t, const float* x, float* y, cudaStream_t s) {
+void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y, cudaStream_t s) {
     if (d.n == 0) return;
-    if (d.sfac) k_static_apply_f32<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
-    else k_static_apply_f32<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+    if (d.sfac) k_static_apply_f32x<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+    else k_static_apply_f32x<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
+}
+
+void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s) {
+    if (d.n == 0) return;
+    k_static_pmask<<<blocks_for(d.n, 256), 256, 0, s>>>(d, pm);
+}
+
+void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const double* x, double* y, cudaStream_t s) {
+    if (d.n == 0) return;
+    const size_t sh = (size_t)S.ns * (sizeof(double4) + sizeof(int4));
+    const unsigned nb = blocks_for(d.n, 256);
+    if (f32) {
+        float* xm = reinterpret_cast<float*>(S.xm);
+        k_static_mask<float><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
+        if (d.sfac) k_static_stencil<float, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        else k_static_stencil<float, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+    } else {
+        double* xm = S.xm;
+        k_static_mask<double><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
+        if (d.sfac) k_static_stencil<double, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        else k_static_stencil<double, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+    }
 }
 
 void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s) {
@@ -308,26 +424,12 @@ __global__ void k_sub(const double* a, const double* b, double* o, int64_t n) {
         o[i] = a[i] - b[i];
 }
 
-__global__ void k_to_f32(const double* a, float* o, double scale, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        o[i] = (float)(a[i] * scale);
-}
-
-__global__ void k_add_f32(double* x, const float* dd, double scale, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        x[i] += scale * (double)dd[i];
-}
-
 constexpr int kStreamBlocks = 148 * 8;
 
 }  // namespace
 
 void launch_dot_f64(const double* a, const double* b, int64_t n, double* part, double* out, cudaStream_t s) {
     k_dot_partial<double><<<kDotBlocks, 256, 0, s>>>(a, b, n, part);
-    k_dot_final<<<1, 32, 0, s>>>(part, kDotBlocks, out);
-}
-void launch_dot_f32(const float* a, const float* b, int64_t n, double* part, double* out, cudaStream_t s) {
-    k_dot_partial<float><<<kDotBlocks, 256, 0, s>>>(a, b, n, part);
     k_dot_final<<<1, 32, 0, s>>>(part, kDotBlocks, out);
 }
 void launch_cg_update_x_f64(double* x, double* r, const double* p, const double* q, int64_t n, const double* scal,
@@ -337,22 +439,9 @@ void launch_cg_update_x_f64(double* x, double* r, const double* p, const double*
 void launch_cg_update_p_f64(const double* r, double* p, int64_t n, const double* scal, cudaStream_t s) {
     k_cg_p<double><<<kStreamBlocks, 256, 0, s>>>(r, p, n, scal);
 }
-void launch_cg_update_x_f32(float* x, float* r, const float* p, const float* q, int64_t n, const double* scal,
-                            cudaStream_t s) {
-    k_cg_x<float><<<kStreamBlocks, 256, 0, s>>>(x, r, p, q, n, scal);
-}
-void launch_cg_update_p_f32(const float* r, float* p, int64_t n, const double* scal, cudaStream_t s) {
-    k_cg_p<float><<<kStreamBlocks, 256, 0, s>>>(r, p, n, scal);
-}
 void launch_cg_swap(double* scal, cudaStream_t s) { k_cg_swap<<<1, 32, 0, s>>>(scal); }
 void launch_sub_f64(const double* a, const double* b, double* o, int64_t n, cudaStream_t s) {
     k_sub<<<kStreamBlocks, 256, 0, s>>>(a, b, o, n);
-}
-void launch_f64_to_f32(const double* a, float* o, double scale, int64_t n, cudaStream_t s) {
-    k_to_f32<<<kStreamBlocks, 256, 0, s>>>(a, o, scale, n);
-}
-void launch_add_f32_to_f64(double* x, const float* dd, double scale, int64_t n, cudaStream_t s) {
-    k_add_f32<<<kStreamBlocks, 256, 0, s>>>(x, dd, scale, n);
 }
 
 }  // namespace pd

@@ -102,6 +102,7 @@ struct Dev {
     float c0, e0;             // spring and critical stretch when there is one material
     int acc_stretch;          // FP64 force: extension as (2 xi.eta + eta.eta)/(p + r)
     int64_t f64_lanes_below;  // FGI FP64 force: eight lanes per node below this many nodes
+    int gather_per_point;     // FP32 gather: one thread per (node, point) instead of per 4 points
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -145,21 +146,29 @@ cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl*
 // CG helpers (pd_fast.cu): slots of the device scalar array
 enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_NSLOT = 8 };
 void launch_dot_f64(const double* a, const double* b, int64_t n, double* part, double* out, cudaStream_t s);
-void launch_dot_f32(const float* a, const float* b, int64_t n, double* part, double* out, cudaStream_t s);
 void launch_cg_update_x_f64(double* x, double* r, const double* p, const double* q, int64_t n, const double* scal, cudaStream_t s);
 void launch_cg_update_p_f64(const double* r, double* p, int64_t n, const double* scal, cudaStream_t s);
-void launch_cg_update_x_f32(float* x, float* r, const float* p, const float* q, int64_t n, const double* scal, cudaStream_t s);
-void launch_cg_update_p_f32(const float* r, float* p, int64_t n, const double* scal, cudaStream_t s);
 void launch_cg_swap(double* scal, cudaStream_t s);
 void launch_sub_f64(const double* a, const double* b, double* out, int64_t n, cudaStream_t s);
-void launch_f64_to_f32(const double* a, float* out, double scale, int64_t n, cudaStream_t s);
-void launch_add_f32_to_f64(double* x, const float* d, double scale, int64_t n, cudaStream_t s);
 constexpr int kDotBlocks = 296;
 
 // static operator (pd_fast.cu)
 void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
-void launch_static_apply_f32(const Dev& d, double t, const float* x, float* y, cudaStream_t s);
 void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s);
+void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
+// the static operator on a complete box lattice (node id = x + nx (y + ny z))
+// whose families are the horizon stencil clipped to the box
+constexpr int kMaxStencil = 1000;  // 48 B of shared memory each: under the 48 KB default
+struct StencilDev {
+    int nx, ny, nz, ns;
+    int radius;            // largest |offset| component
+    const int4* off;       // [ns] lattice offset and node-id offset, ascending id offset
+    const double4* geo;    // [ns] xi = offset * spacing, c V / r^3 of the one material
+    const uint8_t* pmask;  // [N] prescribed directions, bits 0..2
+    double* xm;            // [3N] scratch: the masked input (FP64, or FP32 in its first half)
+};
+void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s);
+void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const double* x, double* y, cudaStream_t s);
 
 // adjoint (pd_adjoint.cu): per-node adjoint vectors [3][N] of one RK4 step
 struct AdjBuf {

@@ -209,3 +209,66 @@ def test_static_operator_matches_oracle(tmp_path):
     u32, it32, r32 = ctx.static_solve(1e-8, P.PREC_FP32C, 1e-10)
     assert r32 <= 1e-10
     assert np.linalg.norm(u32 - u64) <= 1e-8 * np.linalg.norm(u64)
+
+
+def test_static_stencil_equals_family_kernel(tmp_path):
+    """On a complete box the static operator runs as a lattice stencil; it
+    agrees with the family-list kernel, and both solvers converge."""
+    d = D.config_bar(dims=(14, 8, 6), traction=1e6, bdry_eff=0)
+    d.write(str(tmp_path))
+    dm = gpu_model(str(tmp_path))
+    ctx = dm.context()
+    assert ctx.static_prepare()
+    n3 = 3 * ctx.n
+    xv = np.random.default_rng(5).standard_normal(n3) * 1e-7
+    y_st = ctx.static_matvec(1e-8, xv)
+    ctx.set_option(P.OPT_STATIC_STENCIL, 0)
+    y_fl = ctx.static_matvec(1e-8, xv)
+    assert np.linalg.norm(y_st - y_fl) <= 1e-13 * np.linalg.norm(y_fl)
+    u_fl, it_fl, r_fl = ctx.static_solve(1e-8, P.PREC_FP64, 1e-10)
+    ctx.set_option(P.OPT_STATIC_STENCIL, 1)
+    u64, it64, r64 = ctx.static_solve(1e-8, P.PREC_FP64, 1e-10)
+    u32, it32, r32 = ctx.static_solve(1e-8, P.PREC_FP32C, 1e-10)
+    assert r64 <= 1e-10 and r32 <= 1e-10
+    assert np.linalg.norm(u64 - u_fl) <= 1e-8 * np.linalg.norm(u_fl)
+    assert np.linalg.norm(u32 - u64) <= 1e-8 * np.linalg.norm(u64)
+    # the mixed-precision CG keeps its Krylov space: few extra iterations
+    assert it32 <= 1.5 * it64 + 20
+
+
+def test_static_operator_without_stencil_shape_matches_oracle():
+    """A specimen with a hole (deleted nodes) keeps the family-list kernel."""
+    g = load_golden("fgi1_hole")
+    dm = gpu_model("fgi1_hole")
+    x, mat, bc = dm.nodes()
+    rp, col, br = dm.family()
+    I = dm.info()
+    m = model_from_golden(g)
+    ctx = dm.context()
+    assert not ctx.static_prepare()
+    xv = np.random.default_rng(9).standard_normal(3 * I.num_nodes) * 1e-7
+    y_gpu = ctx.static_matvec(1e-8, xv)
+    y_or = m.static_apply(1e-8, xv)
+    assert np.linalg.norm(y_gpu - y_or) <= 1e-12 * np.linalg.norm(y_or)
+    u32, it32, r32 = ctx.static_solve(1e-8, P.PREC_FP32C, 1e-10)
+    assert r32 <= 1e-10
+    res = np.linalg.norm(m.static_apply(1e-8, u32) - m.static_rhs(1e-8)) / np.linalg.norm(m.static_rhs(1e-8))
+    assert res <= 2e-10
+
+
+@pytest.mark.parametrize("name", ["fgi_slit", "fgi3_ramp"])
+def test_fp32c_gather_variants_agree(name):
+    """The FP32-form gather per four points and per point: the same FMAs in
+    the same contributor order, so the same trajectory bit for bit."""
+    g = load_golden(name)
+    dt = g["dt"][0]
+    out = []
+    for per_point in (0, 1):
+        dm = gpu_model(name)
+        dm.SetPrecision(P.PREC_FP32C)
+        ctx = dm.context()
+        ctx.set_option(P.OPT_GATHER_PER_POINT, per_point)
+        ctx.rk4_steps(dt, 0.0, 20)
+        ctx.sync()
+        out.append(ctx.get_state())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
