@@ -130,62 +130,94 @@ __global__ void k_static_pmask(Dev d, uint8_t* __restrict__ pm) {
 // no coordinates are read.  Threads take nodes in lattice order, so for one
 // stencil slot a warp reads 32 consecutive neighbours; nodes at least the
 // stencil radius inside the box skip the box test.  The input arrives
-// masked (prescribed components zeroed, k_static_mask): FP64, or FP32 for
-// the FP32 operator, whose bond terms are FP32 and node sums FP64.
+// masked (prescribed components zeroed, k_static_mask): FP64, or rounded to
+// FP32 for the FP32 operator.  (An FP32 hi/lo split of the input, for
+// FP64-accurate neighbour differences, loads as many bytes as FP64 and did
+// not lower the CG iteration count on the 128^3 cube: 700 against 650.)
 template <typename T>
 __global__ void k_static_mask(const uint8_t* __restrict__ pmask, int64_t N, const double* __restrict__ x,
                               T* __restrict__ xm) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
     const unsigned m = pmask[i];
-    xm[i] = (m & 1) ? (T)0 : (T)x[i];
-    xm[N + i] = (m & 2) ? (T)0 : (T)x[N + i];
-    xm[2 * N + i] = (m & 4) ? (T)0 : (T)x[2 * N + i];
+    for (int a = 0; a < 3; ++a) {
+        const double v = (m & (1u << a)) ? 0.0 : x[a * N + i];
+        xm[a * N + i] = (T)v;
+    }
 }
 
+// FP64: bond terms and sums in FP64.  FP32: bond terms in FP32 from an FP32
+// copy of the table, summed in FP32 over runs of 16 stencil slots and then
+// added to the FP64 node sum (conversions run on the scarce XU pipe).
 template <typename T, bool SFAC, bool CHECK>
-__device__ __forceinline__ void stencil_sum(const Dev& d, const StencilDev& S, const double4* sgeo, const int4* soff,
-                                            int64_t i, int ix, int iy, int iz, const T* __restrict__ xm, T xi0,
-                                            T xi1, T xi2, double sfi, double& r0, double& r1, double& r2) {
+__device__ __forceinline__ void stencil_sum(const Dev& d, const StencilDev& S, const double4* sgeo,
+                                            const float4* sgeof, const int4* soff, int64_t i, int ix, int iy,
+                                            int iz, const T* __restrict__ xm, double sfi, double& a0, double& a1,
+                                            double& a2) {
     const int64_t N = d.n;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int k = 0; k < S.ns; ++k) {
-        const int4 o = soff[k];
-        if (CHECK && ((unsigned)(ix + o.x) >= (unsigned)S.nx || (unsigned)(iy + o.y) >= (unsigned)S.ny ||
-                      (unsigned)(iz + o.z) >= (unsigned)S.nz))
-            continue;
-        const int64_t j = i + o.w;
-        const double4 g = sgeo[k];
-        const T d0 = xi0 - xm[j], d1 = xi1 - xm[N + j], d2 = xi2 - xm[2 * N + j];
-        if (sizeof(T) == 4) {
-            float w = (float)g.w;
-            if (SFAC) w *= (float)(0.5 * (sfi + d.sfac[j]));
-            const float e0 = (float)g.x, e1 = (float)g.y, e2 = (float)g.z;
-            const float pr = w * fmaf(e0, (float)d0, fmaf(e1, (float)d1, e2 * (float)d2));
-            a0 += (double)(pr * e0);
-            a1 += (double)(pr * e1);
-            a2 += (double)(pr * e2);
-        } else {
+    a0 = a1 = a2 = 0.0;
+    if (sizeof(T) == 4) {
+        const float* __restrict__ h0 = reinterpret_cast<const float*>(xm);
+        const float* __restrict__ h1 = h0 + N;
+        const float* __restrict__ h2 = h0 + 2 * N;
+        const float hi0 = h0[i], hi1 = h1[i], hi2 = h2[i];
+        for (int k0 = 0; k0 < S.ns; k0 += 16) {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            const int ke = min(k0 + 16, S.ns);
+#pragma unroll 4
+            for (int k = k0; k < ke; ++k) {
+                const int4 o = soff[k];
+                if (CHECK && ((unsigned)(ix + o.x) >= (unsigned)S.nx || (unsigned)(iy + o.y) >= (unsigned)S.ny ||
+                              (unsigned)(iz + o.z) >= (unsigned)S.nz))
+                    continue;
+                const int64_t j = i + o.w;
+                const float4 g = sgeof[k];
+                float w = g.w;
+                if (SFAC) w *= (float)(0.5 * (sfi + d.sfac[j]));
+                const float d0 = hi0 - h0[j], d1 = hi1 - h1[j], d2 = hi2 - h2[j];
+                const float pr = w * fmaf(g.x, d0, fmaf(g.y, d1, g.z * d2));
+                s0 = fmaf(pr, g.x, s0);
+                s1 = fmaf(pr, g.y, s1);
+                s2 = fmaf(pr, g.z, s2);
+            }
+            a0 += (double)s0;
+            a1 += (double)s1;
+            a2 += (double)s2;
+        }
+    } else {
+        const double* __restrict__ x0p = reinterpret_cast<const double*>(xm);
+        const double* __restrict__ x1p = x0p + N;
+        const double* __restrict__ x2p = x0p + 2 * N;
+        const double xi0 = x0p[i], xi1 = x1p[i], xi2 = x2p[i];
+#pragma unroll 4
+        for (int k = 0; k < S.ns; ++k) {
+            const int4 o = soff[k];
+            if (CHECK && ((unsigned)(ix + o.x) >= (unsigned)S.nx || (unsigned)(iy + o.y) >= (unsigned)S.ny ||
+                          (unsigned)(iz + o.z) >= (unsigned)S.nz))
+                continue;
+            const int64_t j = i + o.w;
+            const double4 g = sgeo[k];
             double w = g.w;
             if (SFAC) w = w * (0.5 * (sfi + d.sfac[j]));
-            const double pr = w * (g.x * (double)d0 + g.y * (double)d1 + g.z * (double)d2);
+            const double d0 = xi0 - x0p[j], d1 = xi1 - x1p[j], d2 = xi2 - x2p[j];
+            const double pr = w * (g.x * d0 + g.y * d1 + g.z * d2);
             a0 += pr * g.x;
             a1 += pr * g.y;
             a2 += pr * g.z;
         }
     }
-    r0 = a0;
-    r1 = a1;
-    r2 = a2;
 }
 
 template <typename T, bool SFAC>
 __global__ void __launch_bounds__(256) k_static_stencil(Dev d, StencilDev S, const double* __restrict__ x,
                                                         const T* __restrict__ xm, double* __restrict__ y) {
     extern __shared__ double4 sgeo[];
-    int4* soff = reinterpret_cast<int4*>(sgeo + S.ns);
+    float4* sgeof = reinterpret_cast<float4*>(sgeo + S.ns);
+    int4* soff = reinterpret_cast<int4*>(sgeof + S.ns);
     for (int k = threadIdx.x; k < S.ns; k += blockDim.x) {
-        sgeo[k] = S.geo[k];
+        const double4 g = S.geo[k];
+        sgeo[k] = g;
+        sgeof[k] = make_float4((float)g.x, (float)g.y, (float)g.z, (float)g.w);
         soff[k] = S.off[k];
     }
     __syncthreads();
@@ -194,13 +226,12 @@ __global__ void __launch_bounds__(256) k_static_stencil(Dev d, StencilDev S, con
     if (i >= N) return;
     const int ix = (int)(i % S.nx), iy = (int)((i / S.nx) % S.ny), iz = (int)(i / ((int64_t)S.nx * S.ny));
     const unsigned mi = S.pmask[i];
-    const T xi0 = xm[i], xi1 = xm[N + i], xi2 = xm[2 * N + i];
     const double sfi = SFAC ? d.sfac[i] : 0.0;
     double a0, a1, a2;
     const int R = S.radius;
     const bool inner = ix >= R && ix < S.nx - R && iy >= R && iy < S.ny - R && iz >= R && iz < S.nz - R;
-    if (inner) stencil_sum<T, SFAC, false>(d, S, sgeo, soff, i, ix, iy, iz, xm, xi0, xi1, xi2, sfi, a0, a1, a2);
-    else stencil_sum<T, SFAC, true>(d, S, sgeo, soff, i, ix, iy, iz, xm, xi0, xi1, xi2, sfi, a0, a1, a2);
+    if (inner) stencil_sum<T, SFAC, false>(d, S, sgeo, sgeof, soff, i, ix, iy, iz, xm, sfi, a0, a1, a2);
+    else stencil_sum<T, SFAC, true>(d, S, sgeo, sgeof, soff, i, ix, iy, iz, xm, sfi, a0, a1, a2);
     y[i] = (mi & 1) ? x[i] : a0;
     y[N + i] = (mi & 2) ? x[N + i] : a1;
     y[2 * N + i] = (mi & 4) ? x[2 * N + i] : a2;
@@ -346,7 +377,7 @@ void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s) {
 
 void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const double* x, double* y, cudaStream_t s) {
     if (d.n == 0) return;
-    const size_t sh = (size_t)S.ns * (sizeof(double4) + sizeof(int4));
+    const size_t sh = (size_t)S.ns * (sizeof(double4) + sizeof(float4) + sizeof(int4));
     const unsigned nb = blocks_for(d.n, 256);
     if (f32) {
         float* xm = reinterpret_cast<float*>(S.xm);

@@ -158,7 +158,7 @@ void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s);
 void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
 // the static operator on a complete box lattice (node id = x + nx (y + ny z))
 // whose families are the horizon stencil clipped to the box
-constexpr int kMaxStencil = 1000;  // 48 B of shared memory each: under the 48 KB default
+constexpr int kMaxStencil = 768;  // 64 B of shared memory each: under the 48 KB default
 struct StencilDev {
     int nx, ny, nz, ns;
     int radius;            // largest |offset| component
