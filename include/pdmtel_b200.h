@@ -256,7 +256,12 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   no broken bond and stencil-shaped families (checked); 0 keeps the
  *   family-list kernel.
  * PD_OPT_GATHER_PER_POINT: 1 runs the FP32-form MLS gather with one thread
- *   per (node, Gauss point), 0 (default) with one per four points. */
+ *   per (node, Gauss point), 0 (default) with one per four points.
+ * PD_OPT_FORCE_TILE: the FP32-form force (2x2x2 points, nodes on one
+ *   lattice) stages lattice tiles of tx x ty x tz positions and their halo
+ *   in shared memory, value = tx | ty << 8 | tz << 16 (tx even, 32 to 256
+ *   pairs of positions per tile); 0 (default) reads neighbours from global
+ *   memory.  Reset to 0 whenever the family changes. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -264,7 +269,8 @@ enum {
     PD_OPT_PERSIST_FORCE_CHUNK = 4,
     PD_OPT_PERSIST_GATHER_CHUNK = 5,
     PD_OPT_STATIC_STENCIL = 6,
-    PD_OPT_GATHER_PER_POINT = 7
+    PD_OPT_GATHER_PER_POINT = 7,
+    PD_OPT_FORCE_TILE = 8
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -290,8 +296,10 @@ typedef struct pd_tune_result {
     double ms_per_step;    /* device time per step of the kept shape */
     int32_t gather_per_point; /* PD_OPT_GATHER_PER_POINT kept */
     int32_t pad;
+    int64_t force_tile;       /* PD_OPT_FORCE_TILE kept */
 } pd_tune_result;
-/* Times candidate launch shapes (node-order tiles, the FP32 gather variant;
+/* Times candidate launch shapes (node-order tiles, the FP32 gather variant,
+ * shared-memory force tiles;
  * for the persistent launch blocks per SM and queue chunks) over `steps`
  * steps each from the current state, keeps the fastest in the context and
  * restores the state. */

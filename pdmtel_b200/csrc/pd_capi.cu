@@ -477,6 +477,27 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
             if ((rc = dalloc(c, &dl, N)) != PD_OK || (rc = upload(c, dl, lat.data(), sizeof(int32_t) * N)) != PD_OK)
                 return bail(rc);
             d.lat = dl;
+            // the lattice box and, when it is not much larger than the node
+            // set, the position -> node id map of the tiled FP32 force
+            int64_t nx = 0, ny = 0, nz = 0;
+            for (int64_t i = 0; i < N; ++i) {
+                nx = std::max<int64_t>(nx, (lat[i] & 2047) + 1);
+                ny = std::max<int64_t>(ny, ((lat[i] >> 11) & 2047) + 1);
+                nz = std::max<int64_t>(nz, (lat[i] >> 22) + 1);
+            }
+            d.lat_nx = (int)nx;
+            d.lat_ny = (int)ny;
+            d.lat_nz = (int)nz;
+            if (nx * ny * nz <= 8 * N) {
+                std::vector<int32_t> map((size_t)(nx * ny * nz), -1);
+                for (int64_t i = 0; i < N; ++i)
+                    map[(lat[i] & 2047) + nx * (((lat[i] >> 11) & 2047) + ny * (lat[i] >> 22))] = (int32_t)i;
+                int32_t* dm = nullptr;
+                if ((rc = dalloc(c, &dm, map.size())) != PD_OK ||
+                    (rc = upload(c, dm, map.data(), sizeof(int32_t) * map.size())) != PD_OK)
+                    return bail(rc);
+                d.pos2id = dm;
+            }
         }
     }
     d.x = x;
@@ -550,6 +571,7 @@ static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr
     c->H = H;
     c->Ha = Ha;
     c->have_family = true;
+    c->d.tile_x = c->d.tile_y = c->d.tile_z = 0;  // its family radius may have changed
     c->generation++;
 }
 
@@ -749,6 +771,36 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.gather_per_point = (int)value;
             break;
+        case PD_OPT_FORCE_TILE: {
+            if (value == 0) {
+                c->d.tile_x = c->d.tile_y = c->d.tile_z = 0;
+                break;
+            }
+            const int tx = (int)(value & 0xff), ty = (int)((value >> 8) & 0xff), tz = (int)((value >> 16) & 0xff);
+            const int threads = tx / 2 * ty * tz;
+            if (tx < 2 || tx % 2 || ty < 1 || tz < 1 || threads < 32 || threads > 256)
+                return fail(PD_ERR_ARG, "pd_set_option: tile (x even, 32..256 node pairs)");
+            if (c->d.cci || c->npt != 8 || !c->d.lat || !c->d.pos2id || !c->have_family)
+                return fail(PD_ERR_ARG, "pd_set_option: the tiled force needs a lattice, 2x2x2 points and a family");
+            int* rad = reinterpret_cast<int*>(c->hscalar + 8);
+            pd::launch_family_radius(c->d, reinterpret_cast<int*>(c->scal + pd::CG_NSLOT - 1), c->stream);
+            PD_CUDA_TRY(cudaMemcpyAsync(rad, c->scal + pd::CG_NSLOT - 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                        c->stream));
+            PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            pd::Dev t = c->d;
+            t.fam_radius = *rad;
+            t.tile_x = tx;
+            t.tile_y = ty;
+            t.tile_z = tz;
+            const size_t smem = pd::tiled_smem_bytes(t);
+            int dev = 0, optin = 0;
+            PD_CUDA_TRY(cudaGetDevice(&dev));
+            PD_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            if (smem > (size_t)optin) return fail(PD_ERR_ARG, "pd_set_option: tile and halo exceed shared memory");
+            if (pd::prepare_tiled_force(smem) != PD_OK) return fail(PD_ERR_CUDA, "pd_set_option: shared memory opt-in");
+            c->d = t;
+            break;
+        }
         case PD_OPT_PERSIST_FORCE_CHUNK:
         case PD_OPT_PERSIST_GATHER_CHUNK:
             if (value < 128 || value > (1 << 20) || value % 128) return fail(PD_ERR_ARG, "pd_set_option: chunk");
@@ -770,6 +822,9 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_PERSIST_GATHER_CHUNK: *value = c->gather_chunk; return PD_OK;
         case PD_OPT_STATIC_STENCIL: *value = c->static_stencil_opt; return PD_OK;
         case PD_OPT_GATHER_PER_POINT: *value = c->d.gather_per_point; return PD_OK;
+        case PD_OPT_FORCE_TILE:
+            *value = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
+            return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
     }
 }
@@ -1749,6 +1804,23 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
         if ((rc = trial(T)) != PD_OK) return done(rc);
         if (!(best.ms < before)) c->d.gather_per_point = gp0;
         out->gather_per_point = c->d.gather_per_point;
+    }
+    if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && c->d.pos2id) {
+        // the shared-memory tiles of the force, on the best shape so far
+        const int tz = std::min(c->d.lat_nz, 4);
+        const int64_t cand[][3] = {{16, 8, tz}, {32, 4, tz}, {16, 4, tz}, {8, 8, tz}, {32, 8, tz}, {64, 2, tz}};
+        int64_t keep = 0;
+        const double before = best.ms;
+        for (auto& t3 : cand) {
+            const int64_t v = t3[0] | (t3[1] << 8) | (t3[2] << 16);
+            if (pd_set_option(c, PD_OPT_FORCE_TILE, v) != PD_OK) continue;  // does not fit: skip
+            Trial T{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+            const double prev = best.ms;
+            if ((rc = trial(T)) != PD_OK) return done(rc);
+            if (best.ms < prev) keep = v;
+        }
+        if ((rc = pd_set_option(c, PD_OPT_FORCE_TILE, best.ms < before ? keep : 0)) != PD_OK) return done(rc);
+        out->force_tile = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
     }
     if (persist_capable(c)) {
         int per_sm = 0, sms = 0;

@@ -17,6 +17,7 @@
 // unless both are tiny.  Coordinates are split the same way.  Per-bond forces
 // are summed in FP32 over the Gauss points, the family sum of each node is
 // Kahan-compensated, and the state update stays FP64.
+#include <algorithm>
 #include <climits>
 
 #include "pd_internal.cuh"
@@ -145,16 +146,24 @@ __device__ __forceinline__ void store_own(const Dev& d, int64_t i, const Own& o,
 // lists and loads every neighbour's block once for both bonds, which cuts
 // the L1 traffic per evaluation (the bound of this kernel) by the overlap of
 // the two families.  pdDataManager.cpp:1917-1962 in FP32 form.
-// The pair of work-order slots t2, t2+1.  PERSIST (inside the persistent
-// kernel) adds what the separate launches of a step do around the force: at
-// the first stage u1 = us = U and vbuf starts from V; after the force the
-// stage epilogue of both nodes at time t.
-template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT, bool PERSIST>
-__device__ __forceinline__ void force_pair(const Dev& d, const PointPack<8>& G, double dts, int64_t t2, int pstage,
-                                           double dt, double t) {
+// Node blocks staged in shared memory (the tiled kernel): a box of the
+// lattice [lo, lo + (lx, ly, ...)) with kTileStride floats per node.
+constexpr int kTileStride = 36;  // 144 B: 16-byte aligned, and lanes reading
+                                 // different nodes spread over the banks
+struct SmemTile {
+    const float* base;
+    int lox, loy, loz, lx, ly;
+};
+
+// Nodes ia and ib (ib may be -1).  PERSIST (inside the persistent kernel)
+// adds what the separate launches of a step do around the force: at the
+// first stage u1 = us = U and vbuf starts from V; after the force the stage
+// epilogue of both nodes at time t.  SMEM: neighbour blocks from a staged
+// tile T instead of global memory.
+template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT, bool PERSIST, bool SMEM>
+__device__ __forceinline__ void force_nodes(const Dev& d, const PointPack<8>& G, double dts, int64_t ia, int64_t ib,
+                                            int pstage, double dt, double t, const SmemTile& T) {
     const int64_t N = d.n;
-    const int64_t ia = d.order[t2];
-    const int64_t ib = (t2 + 1 < N) ? d.order[t2 + 1] : -1;
     if (PERSIST && pstage == 1) {
         for (int a = 0; a < 3; ++a) {
             const double ua = __ldcg(d.U + a * N + ia);
@@ -183,13 +192,17 @@ __device__ __forceinline__ void force_pair(const Dev& d, const PointPack<8>& G, 
         const int jb = pb < eb ? d.acol[pb] : INT_MAX;
         const int j = min(ja, jb);
         if (j == INT_MAX) break;
-        const float* bj = d.nblk + (int64_t)j * 32;
-        const float4 us0 = ld4m<PERSIST>(bj + 24), us1 = ld4m<PERSIST>(bj + 28);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
-        float pj[6];
         int lj = 0;
-        if (LAT) {
-            lj = d.lat[j];
-        } else {
+        if (LAT) lj = d.lat[j];
+        const float* bj = SMEM ? T.base + kTileStride * (((lj & 2047) - T.lox) +
+                                                         T.lx * ((((lj >> 11) & 2047) - T.loy) +
+                                                                 T.ly * ((lj >> 22) - T.loz)))
+                               : d.nblk + (int64_t)j * 32;
+        // hi0 hi1 hi2 lo0 | lo1 lo2 - -
+        const float4 us0 = SMEM ? *reinterpret_cast<const float4*>(bj + 24) : ld4m<PERSIST>(bj + 24);
+        const float4 us1 = SMEM ? *reinterpret_cast<const float4*>(bj + 28) : ld4m<PERSIST>(bj + 28);
+        float pj[6];
+        if (!LAT) {
             const float4 s0 = ld4(d.sblk + 8 * (int64_t)j), s1 = ld4(d.sblk + 8 * (int64_t)j + 4);
             pj[0] = s0.x; pj[1] = s0.y; pj[2] = s0.z; pj[3] = s0.w; pj[4] = s1.x; pj[5] = s1.y;
         }
@@ -235,7 +248,9 @@ __device__ __forceinline__ void force_pair(const Dev& d, const PointPack<8>& G, 
         // applied to both bonds
 #pragma unroll
         for (int q = 0; q < 8; q += 4) {
-            const float4 vx = ld4m<PERSIST>(bj + q), vy = ld4m<PERSIST>(bj + 8 + q), vz = ld4m<PERSIST>(bj + 16 + q);
+            const float4 vx = SMEM ? *reinterpret_cast<const float4*>(bj + q) : ld4m<PERSIST>(bj + q);
+            const float4 vy = SMEM ? *reinterpret_cast<const float4*>(bj + 8 + q) : ld4m<PERSIST>(bj + 8 + q);
+            const float4 vz = SMEM ? *reinterpret_cast<const float4*>(bj + 16 + q) : ld4m<PERSIST>(bj + 16 + q);
             const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
 #pragma unroll
             for (int side = 0; side < 2; ++side)
@@ -260,11 +275,85 @@ __device__ __forceinline__ void force_pair(const Dev& d, const PointPack<8>& G, 
     }
 }
 
+// the pair of work-order slots t2, t2 + 1
+template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT, bool PERSIST>
+__device__ __forceinline__ void force_pair(const Dev& d, const PointPack<8>& G, double dts, int64_t t2, int pstage,
+                                           double dt, double t) {
+    const int64_t ia = d.order[t2];
+    const int64_t ib = (t2 + 1 < d.n) ? d.order[t2 + 1] : -1;
+    force_nodes<HASFAIL, LAT, BDRY, SFAC, MULTIMAT, PERSIST, false>(d, G, dts, ia, ib, pstage, dt, t, SmemTile{});
+}
+
 template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
 __global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> G, double dts) {
     const int64_t t2 = 2 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
     if (t2 >= d.n) return;
     force_pair<HASFAIL, LAT, BDRY, SFAC, MULTIMAT, false>(d, G, dts, t2, 0, 0.0, 0.0);
+}
+
+// The same bond forces with the neighbour blocks of a lattice tile staged in
+// shared memory.  A block owns a tile of tile_x x tile_y x tile_z lattice
+// positions and copies the node blocks of the tile and of its halo (the
+// family radius around it, clipped to the box) into shared memory, 144 bytes
+// per node; every neighbour load of the force loop then reads shared memory,
+// where a warp's 32 loads of different nodes take a few wavefronts instead
+// of one L1 wavefront per node.  Thread t takes the x-adjacent pair of
+// positions (x0 + 2 px, x0 + 2 px + 1) of the tile.  Same arithmetic per node
+// as k_force_f32c_pair, so the same result bit for bit.
+template <bool HASFAIL, bool BDRY, bool SFAC, bool MULTIMAT>
+__global__ void __launch_bounds__(256, 1) k_force_f32c_tiled(Dev d, PointPack<8> G, double dts) {
+    extern __shared__ float4 smem4[];
+    float* smem = reinterpret_cast<float*>(smem4);
+    const int TX = d.tile_x, TY = d.tile_y, TZ = d.tile_z, R = d.fam_radius;
+    const int NX = d.lat_nx, NY = d.lat_ny, NZ = d.lat_nz;
+    const int ntx = (NX + TX - 1) / TX, nty = (NY + TY - 1) / TY;
+    const int b = blockIdx.x;
+    const int x0 = (b % ntx) * TX, y0 = ((b / ntx) % nty) * TY, z0 = (b / (ntx * nty)) * TZ;
+    const int lox = max(0, x0 - R), hix = min(NX, x0 + TX + R);
+    const int loy = max(0, y0 - R), hiy = min(NY, y0 + TY + R);
+    const int loz = max(0, z0 - R), hiz = min(NZ, z0 + TZ + R);
+    const int LX = hix - lox, LY = hiy - loy, LZ = hiz - loz;
+    const int L = LX * LY * LZ;
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        const int lx = l % LX, ly = (l / LX) % LY, lz = l / (LX * LY);
+        const int id = d.pos2id[(lox + lx) + (int64_t)NX * ((loy + ly) + (int64_t)NY * (loz + lz))];
+        if (id < 0) continue;
+        const float4* src = reinterpret_cast<const float4*>(d.nblk + (int64_t)id * 32);
+        float4* dst = reinterpret_cast<float4*>(smem + (int64_t)l * kTileStride);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) dst[q] = __ldg(src + q);
+    }
+    __syncthreads();
+    const int hx = TX / 2;
+    const int t = threadIdx.x;
+    if (t >= hx * TY * TZ) return;
+    const int gx = x0 + 2 * (t % hx), gy = y0 + (t / hx) % TY, gz = z0 + t / (hx * TY);
+    if (gx >= NX || gy >= NY || gz >= NZ) return;
+    const int64_t row = (int64_t)NX * (gy + (int64_t)NY * gz);
+    int64_t ia = d.pos2id[gx + row];
+    int64_t ib = gx + 1 < NX ? d.pos2id[gx + 1 + row] : -1;
+    if (ia < 0) {
+        ia = ib;
+        ib = -1;
+    }
+    if (ia < 0) return;
+    const SmemTile T{smem, lox, loy, loz, LX, LY};
+    force_nodes<HASFAIL, true, BDRY, SFAC, MULTIMAT, false, true>(d, G, dts, ia, ib, 0, 0.0, 0.0, T);
+}
+
+// the largest lattice offset along one axis over every active family entry
+__global__ void k_family_radius(Dev d, int* out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int li = d.lat[i];
+    int r = 0;
+    for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+        const int lj = d.lat[d.acol[p]];
+        r = max(r, abs((lj & 2047) - (li & 2047)));
+        r = max(r, abs(((lj >> 11) & 2047) - ((li >> 11) & 2047)));
+        r = max(r, abs((lj >> 22) - (li >> 22)));
+    }
+    atomicMax(out, r);
 }
 
 // The same for any number of Gauss points (constants from shared memory).
@@ -712,6 +801,30 @@ PointPack<NPT> pack_points(const Dev& d, const GaussConst* host_gc) {
 
 }  // namespace
 
+size_t tiled_smem_bytes(const Dev& d) {
+    const int R = d.fam_radius;
+    const int64_t lx = std::min(d.lat_nx, d.tile_x + 2 * R), ly = std::min(d.lat_ny, d.tile_y + 2 * R),
+                  lz = std::min(d.lat_nz, d.tile_z + 2 * R);
+    return (size_t)(lx * ly * lz) * kTileStride * sizeof(float);
+}
+
+int prepare_tiled_force(size_t smem) {
+    const void* fns[] = {(const void*)k_force_f32c_tiled<true, true, true, true>,
+                         (const void*)k_force_f32c_tiled<false, true, true, false>,
+                         (const void*)k_force_f32c_tiled<false, true, false, false>,
+                         (const void*)k_force_f32c_tiled<false, false, true, false>,
+                         (const void*)k_force_f32c_tiled<false, false, false, false>};
+    for (const void* f : fns)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return PD_ERR_CUDA;
+    return PD_OK;
+}
+
+void launch_family_radius(const Dev& d, int* out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(int), s);
+    if (d.n > 0 && d.lat) k_family_radius<<<blocks_for(d.n, 256), 256, 0, s>>>(d, out);
+}
+
 void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
     if (d.n == 0) return;
     const unsigned nb = blocks_for(d.n, 128);
@@ -719,6 +832,23 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
         k_pack_cci<<<blocks_for(d.n, 256), 256, 0, s>>>(d);
         if (d.sfac) k_force_f32c_cci<true><<<nb, 128, 0, s>>>(d, dts);
         else k_force_f32c_cci<false><<<nb, 128, 0, s>>>(d, dts);
+        return;
+    }
+    if (d.npt == 8 && d.gc_host && d.tile_x > 0 && d.lat && d.pos2id) {
+        const PointPack<8> P = pack_points<8>(d, d.gc_host);
+        const int nt = ((d.lat_nx + d.tile_x - 1) / d.tile_x) * ((d.lat_ny + d.tile_y - 1) / d.tile_y) *
+                       ((d.lat_nz + d.tile_z - 1) / d.tile_z);
+        const int bs = d.tile_x / 2 * d.tile_y * d.tile_z;
+        const size_t sh = tiled_smem_bytes(d);
+        const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
+        if (d.hasfail || d.multimat) k_force_f32c_tiled<true, true, true, true><<<nt, bs, sh, s>>>(d, P, dts);
+        else if (bd) {
+            if (sf) k_force_f32c_tiled<false, true, true, false><<<nt, bs, sh, s>>>(d, P, dts);
+            else k_force_f32c_tiled<false, true, false, false><<<nt, bs, sh, s>>>(d, P, dts);
+        } else {
+            if (sf) k_force_f32c_tiled<false, false, true, false><<<nt, bs, sh, s>>>(d, P, dts);
+            else k_force_f32c_tiled<false, false, false, false><<<nt, bs, sh, s>>>(d, P, dts);
+        }
         return;
     }
     if (d.npt == 8 && d.gc_host) {

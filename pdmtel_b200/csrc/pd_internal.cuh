@@ -103,6 +103,13 @@ struct Dev {
     int acc_stretch;          // FP64 force: extension as (2 xi.eta + eta.eta)/(p + r)
     int64_t f64_lanes_below;  // FGI FP64 force: eight lanes per node below this many nodes
     int gather_per_point;     // FP32 gather: one thread per (node, point) instead of per 4 points
+    // lattice box of the packed positions and the position -> node id map
+    // (-1: no node); the FP32 force stages tile_x x tile_y x tile_z tiles in
+    // shared memory when tile_x > 0 (fam_radius: largest family offset)
+    const int32_t* pos2id;
+    int lat_nx, lat_ny, lat_nz;
+    int fam_radius;
+    int tile_x, tile_y, tile_z;
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -129,6 +136,9 @@ int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int
 void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s);
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
+size_t tiled_smem_bytes(const Dev& d);
+int prepare_tiled_force(size_t smem);
+void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
 
 // persistent FP32C stepping (pd_f32c.cu): control block of one launch.
 // next[8*step + 2*(stage-1) + phase] are the work-queue counters; all of it

@@ -272,3 +272,42 @@ def test_fp32c_gather_variants_agree(name):
         ctx.sync()
         out.append(ctx.get_state())
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("name,tiles", [("fgi_slit", [(8, 8, 3), (4, 8, 3)]), ("fgi_velo", [(8, 8, 4), (4, 4, 4)])])
+def test_fp32c_tiled_force_equals_pair_kernel(name, tiles):
+    """The FP32 force with shared-memory lattice tiles: the same arithmetic
+    per node as the global-memory pair kernel, so the same trajectory."""
+    g = load_golden(name)
+    dt = g["dt"][0]
+
+    def run(tile):
+        dm = gpu_model(name)
+        dm.SetPrecision(P.PREC_FP32C)
+        ctx = dm.context()
+        if tile:
+            ctx.set_option(P.OPT_FORCE_TILE, tile[0] | (tile[1] << 8) | (tile[2] << 16))
+            assert ctx.get_option(P.OPT_FORCE_TILE) != 0
+        ctx.rk4_steps(dt, 0.0, 20)
+        ctx.sync()
+        return ctx.get_state()
+
+    U0, V0 = run(None)
+    assert np.abs(U0).max() > 0
+    for t in tiles:
+        U1, V1 = run(t)
+        assert np.array_equal(U0, U1) and np.array_equal(V0, V1), t
+
+
+def test_fp32c_tiled_force_rejects_bad_shapes():
+    dm = gpu_model("fgi_velo")
+    dm.SetPrecision(P.PREC_FP32C)
+    ctx = dm.context()
+    with pytest.raises(P.PdError):
+        ctx.set_option(P.OPT_FORCE_TILE, 3 | (8 << 8) | (4 << 16))  # odd x
+    with pytest.raises(P.PdError):
+        ctx.set_option(P.OPT_FORCE_TILE, 2 | (2 << 8) | (2 << 16))  # fewer than 32 pairs
+    d3 = gpu_model("fgi3_ramp")  # 3x3x3 points: the pair kernels do not apply
+    d3.SetPrecision(P.PREC_FP32C)
+    with pytest.raises(P.PdError):
+        d3.context().set_option(P.OPT_FORCE_TILE, 8 | (8 << 8) | (4 << 16))
