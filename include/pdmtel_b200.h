@@ -261,7 +261,10 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   lattice) stages lattice tiles of tx x ty x tz positions and their halo
  *   in shared memory, value = tx | ty << 8 | tz << 16 (tx even, 32 to 256
  *   pairs of positions per tile); 0 (default) reads neighbours from global
- *   memory.  Reset to 0 whenever the family changes. */
+ *   memory.  Reset to 0 whenever the family changes.
+ * PD_OPT_FORCE_QUAD: 1 runs the FP32-form force with four nodes per thread
+ *   (nodes on one lattice, one material, no critical stretch within reach;
+ *   otherwise ignored); 0 (default) with two. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -270,7 +273,8 @@ enum {
     PD_OPT_PERSIST_GATHER_CHUNK = 5,
     PD_OPT_STATIC_STENCIL = 6,
     PD_OPT_GATHER_PER_POINT = 7,
-    PD_OPT_FORCE_TILE = 8
+    PD_OPT_FORCE_TILE = 8,
+    PD_OPT_FORCE_QUAD = 9
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -297,6 +301,8 @@ typedef struct pd_tune_result {
     int32_t gather_per_point; /* PD_OPT_GATHER_PER_POINT kept */
     int32_t pad;
     int64_t force_tile;       /* PD_OPT_FORCE_TILE kept */
+    int32_t force_quad;       /* PD_OPT_FORCE_QUAD kept */
+    int32_t pad2;
 } pd_tune_result;
 /* Times candidate launch shapes (node-order tiles, the FP32 gather variant,
  * shared-memory force tiles;

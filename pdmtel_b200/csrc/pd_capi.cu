@@ -771,6 +771,10 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.gather_per_point = (int)value;
             break;
+        case PD_OPT_FORCE_QUAD:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            c->d.force_quad = (int)value;
+            break;
         case PD_OPT_FORCE_TILE: {
             if (value == 0) {
                 c->d.tile_x = c->d.tile_y = c->d.tile_z = 0;
@@ -825,6 +829,7 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_FORCE_TILE:
             *value = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
             return PD_OK;
+        case PD_OPT_FORCE_QUAD: *value = c->d.force_quad; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
     }
 }
@@ -1805,7 +1810,19 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
         if (!(best.ms < before)) c->d.gather_per_point = gp0;
         out->gather_per_point = c->d.gather_per_point;
     }
-    if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && c->d.pos2id) {
+    if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.hasfail &&
+        !c->d.multimat) {
+        // four nodes per thread in the force, on the best shape so far
+        const double before = best.ms;
+        c->d.force_quad = 1;
+        Trial T{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+        if ((rc = trial(T)) != PD_OK) return done(rc);
+        if (!(best.ms < before)) c->d.force_quad = 0;
+        c->generation++;
+        out->force_quad = c->d.force_quad;
+    }
+    if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && c->d.pos2id &&
+        !c->d.force_quad) {
         // the shared-memory tiles of the force, on the best shape so far
         const int tz = std::min(c->d.lat_nz, 4);
         const int64_t cand[][3] = {{16, 8, tz}, {32, 4, tz}, {16, 4, tz}, {8, 8, tz}, {32, 8, tz}, {64, 2, tz}};

@@ -291,6 +291,83 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_pair(Dev d, PointPack<8> 
     force_pair<HASFAIL, LAT, BDRY, SFAC, MULTIMAT, false>(d, G, dts, t2, 0, 0.0, 0.0);
 }
 
+// Four nodes per thread: the work-order slots t4 .. t4+3 (x-adjacent in a
+// node order whose tiles are at least four nodes wide) walk the merge of their
+// four ascending family lists, so a neighbour block loaded once serves up to
+// four bonds (the pair kernel: two).  Nodes on one lattice, one material, no
+// failure test.  Per node the same arithmetic in the same order as
+// k_force_f32c_pair, so the same result bit for bit.
+template <bool BDRY, bool SFAC>
+__global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> G, double dts) {
+    const int64_t N = d.n;
+    const int64_t t4 = 4 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+    if (t4 >= N) return;
+    int64_t id[4], p[4], e[4], nb[4];
+    Own O[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        id[k] = (t4 + k < N) ? d.order[t4 + k] : -1;
+        p[k] = e[k] = 0;
+        if (id[k] >= 0) {
+            load_own<true, BDRY, SFAC, false>(d, id[k], O[k]);
+            p[k] = d.arow[id[k]];
+            e[k] = d.arow[id[k] + 1];
+        }
+        nb[k] = e[k] - p[k];
+    }
+    const float h = (float)d.dx;
+    for (;;) {
+        int js[4];
+        int j = INT_MAX;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            js[k] = p[k] < e[k] ? d.acol[p[k]] : INT_MAX;
+            j = min(j, js[k]);
+        }
+        if (j == INT_MAX) break;
+        const float* bj = d.nblk + (int64_t)j * 32;
+        const float4 us0 = ld4(bj + 24), us1 = ld4(bj + 28);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
+        const int lj = d.lat[j];
+        float bej = 1.f, sfj = 1.f;
+        if (BDRY || SFAC) {
+            const float2 v = __ldg(reinterpret_cast<const float2*>(d.sblk + 8 * (int64_t)j + 6));
+            bej = v.x;
+            sfj = v.y;
+        }
+        const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
+        float dx[4][3], du[4][3], coef[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            dx[k][0] = (float)((lj & 2047) - (O[k].lat & 2047)) * h;
+            dx[k][1] = (float)(((lj >> 11) & 2047) - ((O[k].lat >> 11) & 2047)) * h;
+            dx[k][2] = (float)((lj >> 22) - (O[k].lat >> 22)) * h;
+            for (int a = 0; a < 3; ++a) du[k][a] = (ujh[a] - O[k].uh[a]) + (ujl[a] - O[k].ul[a]);
+            float c = O[k].c;
+            if (BDRY) c *= 0.5f * (O[k].be + bej);
+            if (SFAC) c *= 0.5f * (O[k].sf + sfj);
+            coef[k] = c;
+        }
+        float F[4][3] = {};
+#pragma unroll
+        for (int q = 0; q < 8; q += 4) {
+            const float4 vx = ld4(bj + q), vy = ld4(bj + 8 + q), vz = ld4(bj + 16 + q);
+            const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (js[k] == j) bond4<false>(G, q, u4, dx[k], du[k], O[k].e, F[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (js[k] == j) {
+                kahan_add(O[k], F[k][0] * coef[k], F[k][1] * coef[k], F[k][2] * coef[k]);
+                ++p[k];
+            }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (id[k] >= 0) store_own<false>(d, id[k], O[k], nb[k], dts, d.vbuf);
+}
+
 // The same bond forces with the neighbour blocks of a lattice tile staged in
 // shared memory.  A block owns a tile of tile_x x tile_y x tile_z lattice
 // positions and copies the node blocks of the tile and of its halo (the
@@ -848,6 +925,19 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
         } else {
             if (sf) k_force_f32c_tiled<false, false, true, false><<<nt, bs, sh, s>>>(d, P, dts);
             else k_force_f32c_tiled<false, false, false, false><<<nt, bs, sh, s>>>(d, P, dts);
+        }
+        return;
+    }
+    if (d.npt == 8 && d.gc_host && d.force_quad && d.lat && !d.hasfail && !d.multimat) {
+        const PointPack<8> P = pack_points<8>(d, d.gc_host);
+        const unsigned nq = blocks_for((d.n + 3) / 4, 128);
+        const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
+        if (bd) {
+            if (sf) k_force_f32c_quad<true, true><<<nq, 128, 0, s>>>(d, P, dts);
+            else k_force_f32c_quad<true, false><<<nq, 128, 0, s>>>(d, P, dts);
+        } else {
+            if (sf) k_force_f32c_quad<false, true><<<nq, 128, 0, s>>>(d, P, dts);
+            else k_force_f32c_quad<false, false><<<nq, 128, 0, s>>>(d, P, dts);
         }
         return;
     }

@@ -110,6 +110,7 @@ struct Dev {
     int lat_nx, lat_ny, lat_nz;
     int fam_radius;
     int tile_x, tile_y, tile_z;
+    int force_quad;           // FP32 force: four nodes per thread (lattice, one material, no failure)
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)

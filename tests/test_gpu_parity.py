@@ -311,3 +311,22 @@ def test_fp32c_tiled_force_rejects_bad_shapes():
     d3.SetPrecision(P.PREC_FP32C)
     with pytest.raises(P.PdError):
         d3.context().set_option(P.OPT_FORCE_TILE, 8 | (8 << 8) | (4 << 16))
+
+
+@pytest.mark.parametrize("name", ["fgi_slit", "fgi_velo"])
+def test_fp32c_quad_force_equals_pair_kernel(name):
+    """Four nodes per thread in the FP32 force: the same arithmetic per node
+    as two per thread, so the same trajectory bit for bit."""
+    g = load_golden(name)
+    dt = g["dt"][0]
+    out = []
+    for quad in (0, 1):
+        dm = gpu_model(name)
+        dm.SetPrecision(P.PREC_FP32C)
+        ctx = dm.context()
+        ctx.set_option(P.OPT_FORCE_QUAD, quad)
+        ctx.rk4_steps(dt, 0.0, 20)
+        ctx.sync()
+        out.append(ctx.get_state())
+    assert np.abs(out[0][0]).max() > 0
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
