@@ -32,6 +32,13 @@ factors (sigma 0.15, correlation 4 spacings), K RK4 steps of all specimens
 batched (launch shape from the autotuner: one persistent launch or the
 graph of a step) against the same specimens stepped one context at a time.
 
+--form identify: the differentiation config end to end: a hidden
+log-micromodulus field (Gaussian random field, sigma 0.2, correlation 5 mm)
+on the 64x64x8 specimen generates displacements from 1000 RK4 steps with
+1e-3 RMS noise; the adjoint gradient of the misfit at m = 0 is checked by
+central finite differences (h = 1e-6) along 32 random directions; L-BFGS
+runs 50 iterations (FP64A arithmetic, checkpoints every 50 steps).
+
 --form static: the 128^3 cube (bottom clamped, 1 MPa shear traction on top),
 CG to relative residual 1e-10: FP32 matvec inside FP64 iterative refinement
 against plain FP64 CG; time to solution and the difference of the solutions.
@@ -333,6 +340,88 @@ def run_batch(args):
     return 0
 
 
+def run_identify(args):
+    """--form identify"""
+    import numpy as np
+    import torch
+    import pdmtel_b200 as P
+    from pdmtel_b200 import adjoint as AD
+    from pdmtel_b200 import decks as D
+    torch.cuda.set_device(0)
+    c = IDENT
+    dims = tuple(int(v) for v in args.ident_dims.split("x"))
+    nsteps, every = args.ident_steps, c["every"]
+    tmp = tempfile.mkdtemp(prefix="pdident_")
+    D.config_identify(dims=dims, spacing=c["spacing"], vel=c["vel"], dt=c["dt"], steps=nsteps).write(tmp)
+    t0 = time.time()
+    dm = P.pdDataManager(tmp)
+    P.pdSolve.InitialProblem(dm)
+    ctx = dm.context()
+    ctx.set_precision(P.PREC_FP64A)
+    setup_s = time.time() - t0
+    x, _, _ = dm.nodes()
+    n = ctx.n
+    dt = c["dt"]
+    m_true = AD.gaussian_random_field(x, c["spacing"], c["corr"], c["sigma"], seed=2026)
+
+    def final_U(m):
+        ctx.set_spring_factor(np.exp(m))
+        ctx.reset_state()
+        ctx.rk4_steps(dt, 0.0, nsteps)
+        ctx.sync()
+        return ctx.get_state()[0]
+
+    U_true = final_U(m_true)
+    rng = np.random.default_rng(7)
+    U_obs = U_true + 1e-3 * np.sqrt(np.mean(U_true ** 2)) * rng.standard_normal(U_true.shape)
+    Uo = torch.from_numpy(U_obs.reshape(n, 3))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    # gradient at m = 0, timed
+    m0 = torch.zeros(n, dtype=torch.float64, requires_grad=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    U, _ = AD.trajectory(m0, ctx, dt, nsteps, every)
+    loss = AD.misfit(U, Uo)
+    loss.backward()
+    e1.record(stream)
+    e1.synchronize()
+    grad_s = e0.elapsed_time(e1) / 1e3
+    g = m0.grad.numpy().copy()
+    J0 = float(loss.detach())
+
+    def J(m):
+        Uf = final_U(m)
+        return 0.5 * np.sum((Uf - U_obs) ** 2) / np.sum(U_obs ** 2)
+
+    h = 1e-6
+    errs = []
+    drng = np.random.default_rng(11)
+    for _ in range(args.fd_dirs):
+        v = drng.standard_normal(n)
+        fd = (J(h * v) - J(-h * v)) / (2 * h)
+        errs.append(abs(fd - g @ v) / abs(g @ v))
+    res = AD.identify(ctx, U_obs, dt, nsteps, iters=args.lbfgs_iters, every=every)
+    rms = lambda a: float(np.sqrt(np.mean(np.asarray(a) ** 2)))
+    line = {"metric": "adjoint s/step, 64x64x8 identification (forward + reverse, FP64A)",
+            "value": grad_s / nsteps, "unit": "s/step", "n_gpus": 1, "steps": nsteps, "warmup": 0,
+            "ms_per_step": 1e3 * grad_s / nsteps, "higher_is_better": False, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{dims[0]}x{dims[1]}x{dims[2]} identification, fixed face + "
+                                   f"{c['vel']} m/s pulled face, dt {dt}, hidden GRF sigma {c['sigma']} "
+                                   f"corr {c['corr']} m, noise 1e-3 RMS", "nodes": n,
+                       "checkpoint_every": every},
+            "gradient_check": {"h": h, "directions": args.fd_dirs, "max_rel_err": max(errs) if errs else None,
+                               "median_rel_err": float(np.median(errs)) if errs else None},
+            "lbfgs": {"iterations": args.lbfgs_iters, "evaluations": res.evaluations, "seconds": res.seconds,
+                      "misfit_first": res.loss[0], "misfit_last": res.loss[-1],
+                      "m_rms_error_start": rms(m_true), "m_rms_error_end": rms(res.m - m_true)},
+            "misfit_at_zero": J0, "setup_s": setup_s}
+    print(json.dumps(line))
+    dm.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 def run_static(args):
     """--form static"""
     import numpy as np
@@ -539,7 +628,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=100)
-    ap.add_argument("--form", default="precision", choices=["precision", "batch", "static"])
+    ap.add_argument("--form", default="precision", choices=["precision", "batch", "static", "identify"])
+    ap.add_argument("--ident-dims", default="64x64x8")
+    ap.add_argument("--ident-steps", type=int, default=1000)
+    ap.add_argument("--fd-dirs", type=int, default=32)
+    ap.add_argument("--lbfgs-iters", type=int, default=50)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -549,6 +642,8 @@ def main():
         return run_batch(args)
     if args.form == "static":
         return run_static(args)
+    if args.form == "identify":
+        return run_identify(args)
     return run_ours(args)
 
 
