@@ -39,6 +39,10 @@ on the 64x64x8 specimen generates displacements from 1000 RK4 steps with
 central finite differences (h = 1e-6) along 32 random directions; L-BFGS
 runs 50 iterations (FP64A arithmetic, checkpoints every 50 steps).
 
+--form accuracy: the precision form's error over the plate run: 2000 RK4
+steps in FP32C and in the FP64 drop-in, relative displacement and velocity
+errors at steps 100, 500 and 2000.
+
 --form static: the 128^3 cube (bottom clamped, 1 MPa shear traction on top),
 CG to relative residual 1e-10: FP32 matvec inside FP64 iterative refinement
 against plain FP64 CG; time to solution and the difference of the solutions.
@@ -340,6 +344,48 @@ def run_batch(args):
     return 0
 
 
+def run_accuracy(args):
+    """--form accuracy"""
+    import numpy as np
+    import torch
+    import pdmtel_b200 as P
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp(prefix="pdacc_")
+    dm, ctx, setup_s = setup_plate(tmp, PLATE)
+    dt = PLATE["dt"]
+    marks = [100, 500, 2000]
+    states = {}
+    seconds = {}
+    for name, prec in (("fp32c", P.PREC_FP32C), ("fp64", P.PREC_FP64)):
+        ctx.set_precision(prec)
+        ctx.reset_state()
+        done, t = 0, 0.0
+        t0 = time.time()
+        for m in marks:
+            ctx.rk4_steps(dt, done * dt, m - done)
+            ctx.sync()
+            done = m
+            states[(name, m)] = ctx.get_state()
+        seconds[name] = time.time() - t0
+    err = {}
+    for m in marks:
+        U32, V32 = states[("fp32c", m)]
+        U64, V64 = states[("fp64", m)]
+        err[str(m)] = {"U": float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)),
+                       "V": float(np.linalg.norm(V32 - V64) / np.linalg.norm(V64)),
+                       "U_max_abs_fp64": float(np.abs(U64).max())}
+    line = {"metric": "relative displacement/velocity error of FP32C against the FP64 drop-in, plate",
+            "value": err["2000"]["U"], "unit": "relative L2", "n_gpus": 1, "steps": 2000, "warmup": 0,
+            "ms_per_step": None, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "plate 400x400x4, 2x2x2 Gauss+MLS, 40 mm slit, +-0.05 m/s, dt 5e-9"},
+            "errors": err, "wall_s": seconds, "setup_s": setup_s}
+    print(json.dumps(line))
+    dm.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 def run_identify(args):
     """--form identify"""
     import numpy as np
@@ -628,7 +674,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=100)
-    ap.add_argument("--form", default="precision", choices=["precision", "batch", "static", "identify"])
+    ap.add_argument("--form", default="precision", choices=["precision", "batch", "static", "identify", "accuracy"])
     ap.add_argument("--ident-dims", default="64x64x8")
     ap.add_argument("--ident-steps", type=int, default=1000)
     ap.add_argument("--fd-dirs", type=int, default=32)
@@ -644,6 +690,8 @@ def main():
         return run_static(args)
     if args.form == "identify":
         return run_identify(args)
+    if args.form == "accuracy":
+        return run_accuracy(args)
     return run_ours(args)
 
 
