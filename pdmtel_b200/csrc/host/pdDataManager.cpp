@@ -839,9 +839,27 @@ int pdDataManager::InitBatch(const std::vector<pdDataManager*>& sp) {
     _batchOffsets.assign(1, 0);
     bool anyFactor = false;
     for (const pdDataManager* m : sp) anyFactor = anyFactor || !m->_springFactor.empty();
+    // identical materials of different specimens become one entry, so that a
+    // batch of one material runs the single-material kernels
+    auto same = [](const Material& a, const Material& b) {
+        return a.type == b.type && a.ymod == b.ymod && a.sigmay == b.sigmay && a.nu == b.nu &&
+               a.ecrit == b.ecrit && a.density == b.density && a.grav[0] == b.grav[0] &&
+               a.grav[1] == b.grav[1] && a.grav[2] == b.grav[2];
+    };
     for (size_t k = 0; k < K; ++k) {
         const pdDataManager& m = *sp[k];
-        const int matBase = (int)_mats.size(), bcBase = (int)_bcs.size();
+        const int bcBase = (int)_bcs.size();
+        std::vector<int32_t> matMap(m._mats.size());
+        for (size_t q = 0; q < m._mats.size(); ++q) {
+            int found = -1;
+            for (size_t e = 0; e < _mats.size() && found < 0; ++e)
+                if (same(_mats[e], m._mats[q])) found = (int)e;
+            if (found < 0) {
+                found = (int)_mats.size();
+                _mats.push_back(m._mats[q]);
+            }
+            matMap[q] = found;
+        }
         double shift[3];
         for (int a = 0; a < 3; ++a) shift[a] = (double)origin[k][a] * h;
         for (int64_t i = 0; i < m._numNodes; ++i) {
@@ -850,11 +868,10 @@ int pdDataManager::InitBatch(const std::vector<pdDataManager*>& sp) {
                 _x.push_back(shift[a] + (xa - lo[k][a]));
                 _batchCoords.push_back(xa);
             }
-            _mat.push_back(m._mat[i] + matBase);
+            _mat.push_back(matMap[m._mat[i]]);
             _bc.push_back(m._bc[i] >= 0 ? m._bc[i] + bcBase : -1);
             if (anyFactor) _springFactor.push_back(m._springFactor.empty() ? 1.0 : m._springFactor[i]);
         }
-        for (const Material& q : m._mats) _mats.push_back(q);
         for (const BdryCondition& q : m._bcs) _bcs.push_back(q);
         for (size_t q = 0; q + 6 <= m._slits.size(); q += 6)
             for (int a = 0; a < 3; ++a)

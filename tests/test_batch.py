@@ -55,7 +55,8 @@ def test_batch_placement_offsets_and_tables(tmp_path):
     xb, mb, bb = bm.nodes()
     xb = xb.reshape(-1, 3)
     I = bm.info()
-    assert I.num_nodes == sum(counts) and I.num_materials == len(sp) and I.num_bcs == 2 * len(sp)
+    # the specimens share one material, merged into one entry
+    assert I.num_nodes == sum(counts) and I.num_materials == 1 and I.num_bcs == 2 * len(sp)
     boxes = []
     for k, s in enumerate(sp):
         xs, ms, bs = s.nodes()
@@ -67,7 +68,7 @@ def test_batch_placement_offsets_and_tables(tmp_path):
         assert np.allclose(shift, shift[0], rtol=0, atol=1e-12)
         steps = (seg[0] - xb[0]) / SPACING
         assert np.allclose(steps, np.rint(steps), atol=1e-6)
-        assert np.array_equal(mb[off[k]:off[k + 1]], ms + k)
+        assert np.array_equal(mb[off[k]:off[k + 1]], ms)
         assert np.array_equal(bb[off[k]:off[k + 1]], np.where(bs >= 0, bs + 2 * k, -1))
         boxes.append((seg.min(axis=0), seg.max(axis=0)))
     # every pair of specimens is further apart than the horizon plus a cell
@@ -76,7 +77,7 @@ def test_batch_placement_offsets_and_tables(tmp_path):
             gap = np.maximum(boxes[b][0] - boxes[a][1], boxes[a][0] - boxes[b][1]).max()
             assert gap > I.horizon + 1.5 * SPACING
     mats, bcs, ab, wt = bm.tables()
-    assert len(mats) == len(sp) and len(bcs) == 2 * len(sp)
+    assert len(mats) == 1 and len(bcs) == 2 * len(sp)
     assert np.allclose(ab, [1 / np.sqrt(3), -1 / np.sqrt(3)], rtol=1e-15) and np.all(wt == 1.0)
 
 
@@ -209,3 +210,25 @@ def test_persistent_launch_refuses_unsupported_setups(tmp_path):
     bt.ctx.set_energy(True)
     with pytest.raises(P.PdError):
         bt.ctx.rk4_steps_persistent(spec.dt, 0.0, 2)
+
+
+def test_batch_keeps_distinct_materials_apart(tmp_path):
+    """Identical materials of different specimens merge into one entry;
+    different ones stay distinct and each node keeps its own."""
+    from pdmtel_b200.decks import config_identify
+    sp = []
+    for k, E in enumerate((72e9, 72e9, 50e9)):
+        deck = config_identify(dims=(6, 5, 4), spacing=1e-3)
+        deck.materials = [(E, 1e20, 1e20, 2440.0)]
+        d = str(tmp_path / f"s{k}")
+        deck.write(d)
+        m = P.pdDataManager(d)
+        m.InitNode()
+        sp.append(m)
+    bm = P.pdDataManager.batch(str(tmp_path / "batch"), sp)
+    mats, _, _, _ = bm.tables()
+    assert len(mats) == 2
+    _, mb, _ = bm.nodes()
+    off = bm.batch_offsets()
+    assert set(mb[off[0]:off[2]]) == {0} and set(mb[off[2]:off[3]]) == {1}
+    assert mats[1]["spring"] < mats[0]["spring"]
