@@ -264,7 +264,12 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   memory.  Reset to 0 whenever the family changes.
  * PD_OPT_FORCE_QUAD: 1 runs the FP32-form force with four nodes per thread
  *   (nodes on one lattice, one material, no critical stretch within reach;
- *   otherwise ignored); 0 (default) with two. */
+ *   otherwise ignored); 0 (default) with two.
+ * PD_OPT_PERSIST_WAIT_US: how long a grid barrier of the persistent launch
+ *   waits before it gives up (default 4 s; 1 ms to 60 s).
+ * PD_OPT_PERSIST_TEST_STALL: 1 makes block 0 of the persistent launch skip
+ *   its first barrier, so that every wait there runs out and the call
+ *   returns PD_ERR_TIMEOUT; for tests of that path.  0 by default. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -274,7 +279,9 @@ enum {
     PD_OPT_STATIC_STENCIL = 6,
     PD_OPT_GATHER_PER_POINT = 7,
     PD_OPT_FORCE_TILE = 8,
-    PD_OPT_FORCE_QUAD = 9
+    PD_OPT_FORCE_QUAD = 9,
+    PD_OPT_PERSIST_WAIT_US = 10,
+    PD_OPT_PERSIST_TEST_STALL = 11
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);

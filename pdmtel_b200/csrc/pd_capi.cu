@@ -70,6 +70,8 @@ struct pd_ctx {
     int persist_steps = 0;
     uint64_t persist_generation = ~0ull;
     int tuned_persistent = 0;
+    int64_t persist_wait_us = 4000000;  // grid-barrier wait limit
+    int persist_stall = 0;
     // static operator: per-material springs, lattice stencil (static_prepare)
     std::vector<double> mat_spring;
     int static_stencil_opt = 1;
@@ -771,6 +773,14 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.gather_per_point = (int)value;
             break;
+        case PD_OPT_PERSIST_WAIT_US:
+            if (value < 1000 || value > 60000000) return fail(PD_ERR_ARG, "pd_set_option: wait 1e3..6e7 us");
+            c->persist_wait_us = value;
+            break;
+        case PD_OPT_PERSIST_TEST_STALL:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            c->persist_stall = (int)value;
+            break;
         case PD_OPT_FORCE_QUAD:
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.force_quad = (int)value;
@@ -830,6 +840,8 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
             *value = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
             return PD_OK;
         case PD_OPT_FORCE_QUAD: *value = c->d.force_quad; return PD_OK;
+        case PD_OPT_PERSIST_WAIT_US: *value = c->persist_wait_us; return PD_OK;
+        case PD_OPT_PERSIST_TEST_STALL: *value = c->persist_stall; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
     }
 }
@@ -1658,6 +1670,8 @@ extern "C" int pd_rk4_steps_persistent(pd_ctx* c, double dt, double t0, int nste
         cudaError_t e = cudaMemsetAsync(c->pctl, 0, bytes, c->stream);
         if (e == cudaSuccess)
             e = pd::launch_persist_f32c(c->d, dt, nsteps, c->pctl, blocks, c->force_chunk, c->gather_chunk,
+                                        pd::PersistWait{(unsigned long long)c->persist_wait_us * 1000ull,
+                                                        c->persist_stall},
                                         c->stream);
         cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
         if (e != cudaSuccess) {

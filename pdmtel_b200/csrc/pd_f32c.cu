@@ -778,10 +778,11 @@ __global__ void __launch_bounds__(256) k_gather_f32c_pt(Dev d, const double* __r
 
 // Grid barrier for one cooperative launch (all blocks co-resident).  The
 // arrival counter only grows: barrier k of the launch is passed once it
-// reaches (k+1) * gridDim.x.  The wait is bounded: after kBarrierNs without
-// completion the block sets the error word and every block leaves at its next
-// barrier; the host reads the word and reports PD_ERR_TIMEOUT.
-constexpr unsigned long long kBarrierNs = 4000000000ull;
+// reaches (k+1) * gridDim.x.  The wait is bounded: after W.ns nanoseconds
+// without completion the block sets the error word and every block leaves at
+// its next barrier; the host reads the word and reports PD_ERR_TIMEOUT.
+// W.stall (tests of that path only): block 0 does not arrive at the first
+// barrier, so every wait there runs out.
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -789,20 +790,20 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-__device__ __forceinline__ bool grid_barrier(PersistCtl* ctl, unsigned& passed) {
+__device__ __forceinline__ bool grid_barrier(PersistCtl* ctl, unsigned& passed, const PersistWait& W) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
         const unsigned target = (passed + 1) * gridDim.x;
         __threadfence();
-        atomicAdd(&ctl->arrive, 1u);
+        if (!(W.stall && blockIdx.x == 0 && passed == 0)) atomicAdd(&ctl->arrive, 1u);
         const unsigned long long t0 = global_ns();
         for (;;) {
             const unsigned a = *((volatile unsigned*)&ctl->arrive);
             if (a >= target) break;
             if (*((volatile int*)&ctl->error) != 0) { ok = 0; break; }
-            if (global_ns() - t0 > kBarrierNs) {
+            if (global_ns() - t0 > W.ns) {
                 atomicExch(&ctl->error, 1);
                 ok = 0;
                 break;
@@ -841,7 +842,7 @@ __device__ __forceinline__ void run_queue(unsigned* counter, int64_t nitems, uns
 template <bool HASFAIL, bool LAT, bool BDRY, bool SFAC, bool MULTIMAT>
 __global__ void __launch_bounds__(128, 4) k_persist_f32c(Dev d, PointPack<8> G, double dt, int nsteps,
                                                          PersistCtl* ctl, unsigned force_chunk,
-                                                         unsigned gather_chunk) {
+                                                         unsigned gather_chunk, PersistWait W) {
     const int64_t N = d.n;
     const int64_t npairs = (N + 1) / 2;
     const int64_t ngather = N * ((d.npt + 3) / 4);
@@ -858,10 +859,10 @@ __global__ void __launch_bounds__(128, 4) k_persist_f32c(Dev d, PointPack<8> G, 
             run_queue(q, npairs, force_chunk, [&](int64_t it) {
                 force_pair<HASFAIL, LAT, BDRY, SFAC, MULTIMAT, true>(d, G, dts, 2 * it, stage, dt, t);
             });
-            if (!grid_barrier(ctl, passed)) return;
+            if (!grid_barrier(ctl, passed, W)) return;
             const double* src = stage < 4 ? d.us : d.U;
             run_queue(q + 1, ngather, gather_chunk, [&](int64_t it) { gather_group<true>(d, src, it, t); });
-            if (!grid_barrier(ctl, passed)) return;
+            if (!grid_barrier(ctl, passed, W)) return;
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *d.tdev = t;
@@ -965,7 +966,7 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
 // The persistent kernel's variant for the problem, and how many of its
 // blocks fit on the device at once (a cooperative launch needs all resident).
 namespace {
-using PersistFn = void (*)(Dev, PointPack<8>, double, int, PersistCtl*, unsigned, unsigned);
+using PersistFn = void (*)(Dev, PointPack<8>, double, int, PersistCtl*, unsigned, unsigned, PersistWait);
 PersistFn persist_variant(const Dev& d) {
     const bool lat = d.lat != nullptr, bd = d.bdry_on != 0, sf = d.sfac != nullptr;
     if (d.hasfail || d.multimat) return k_persist_f32c<true, false, true, true, true>;
@@ -991,7 +992,7 @@ int persist_max_blocks(const Dev& d, int* per_sm, int* sms) {
 }
 
 cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl* ctl, int blocks,
-                                unsigned force_chunk, unsigned gather_chunk, cudaStream_t s) {
+                                unsigned force_chunk, unsigned gather_chunk, PersistWait W, cudaStream_t s) {
     const PointPack<8> P = pack_points<8>(d, d.gc_host);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)blocks);
@@ -1003,7 +1004,7 @@ cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl*
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, persist_variant(d), d, P, dt, nsteps, ctl, force_chunk, gather_chunk);
+    return cudaLaunchKernelEx(&cfg, persist_variant(d), d, P, dt, nsteps, ctl, force_chunk, gather_chunk, W);
 }
 
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {

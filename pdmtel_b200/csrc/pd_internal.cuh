@@ -150,9 +150,15 @@ struct PersistCtl {
     unsigned pad[30];
     unsigned next[1];  // [8 * nsteps]
 };
+// how long a grid barrier waits (ns) before giving up; stall: block 0 skips
+// the first barrier (tests of the give-up path)
+struct PersistWait {
+    unsigned long long ns;
+    int stall;
+};
 int persist_max_blocks(const Dev& d, int* per_sm, int* sms);
 cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl* ctl, int blocks,
-                                unsigned force_chunk, unsigned gather_chunk, cudaStream_t s);
+                                unsigned force_chunk, unsigned gather_chunk, PersistWait W, cudaStream_t s);
 
 // CG helpers (pd_fast.cu): slots of the device scalar array
 enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_NSLOT = 8 };

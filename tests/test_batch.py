@@ -232,3 +232,29 @@ def test_batch_keeps_distinct_materials_apart(tmp_path):
     off = bm.batch_offsets()
     assert set(mb[off[0]:off[2]]) == {0} and set(mb[off[2]:off[3]]) == {1}
     assert mats[1]["spring"] < mats[0]["spring"]
+
+
+@pytest.mark.gpu
+def test_persistent_barrier_wait_runs_out_and_the_context_recovers(tmp_path):
+    """The persistent launch's grid barriers give up after their wait limit:
+    with block 0 held back from the first barrier every wait runs out, the
+    call returns PD_ERR_TIMEOUT instead of hanging, and the next launch on the
+    same context runs normally."""
+    import time
+    spec = _small_spec(count=3, seed=23)
+    bt = B.Batch(str(tmp_path), spec, precision=P.PREC_FP32C)
+    bt.run(5, persistent=False)
+    Ug, Vg = _state(bt.ctx)
+    bt.ctx.set_option(P.OPT_PERSIST_WAIT_US, 200000)
+    bt.ctx.set_option(P.OPT_PERSIST_TEST_STALL, 1)
+    bt.ctx.reset_state()
+    t0 = time.time()
+    with pytest.raises(P.PdError) as e:
+        bt.ctx.rk4_steps_persistent(spec.dt, 0.0, 5)
+    assert e.value.code == -4  # PD_ERR_TIMEOUT
+    assert time.time() - t0 < 30
+    bt.ctx.set_option(P.OPT_PERSIST_TEST_STALL, 0)
+    bt.ctx.reset_state()
+    bt.run(5, persistent=True)
+    Up, Vp = _state(bt.ctx)
+    assert np.array_equal(Ug, Up) and np.array_equal(Vg, Vp)
