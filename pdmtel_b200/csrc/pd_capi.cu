@@ -86,6 +86,8 @@ struct pd_ctx {
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
+    double* adj_pool = nullptr;  // reverse-sweep work buffers and stage tape
+    int64_t adj_pool_count = 0;
     bool have_family = false, have_mls = false;
     // owned device buffers
     std::vector<void*> owned;
@@ -1516,13 +1518,22 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
     cudaStream_t s = c->stream;
     const pd::Dev& d = c->d;
     const double dt = c->adj_dt;
-    // work buffers
-    std::vector<double*> bufs;
+    // work buffers: carved from one pool that the context keeps between calls
+    // (an optimiser calls the pair again and again with the same sizes)
+    const int64_t pool_need = 13 * n3 + 3 * ng + N + (int64_t)c->adj_every * 4 * (2 * n3 + ng) + 32 * 19;
+    if (c->adj_pool_count < pool_need) {
+        dfree(c, c->adj_pool);
+        c->adj_pool = nullptr;
+        c->adj_pool_count = 0;
+        if (dalloc(c, &c->adj_pool, pool_need) != PD_OK)
+            return fail(PD_ERR_OOM, "pd_adjoint_backward: device memory for the tape");
+        c->adj_pool_count = pool_need;
+    }
+    int64_t carved = 0;
     auto get = [&](int64_t count) -> double* {
-        double* p = nullptr;
-        if (dalloc(c, &p, count) != PD_OK) return nullptr;
-        bufs.push_back(p);
-        return p;
+        double* p = c->adj_pool + carved;
+        carved += (count + 31) / 32 * 32;  // 256-byte aligned pieces
+        return carved <= c->adj_pool_count ? p : nullptr;
     };
     pd::AdjBuf A;
     double** fields[] = {&A.lU, &A.lV, &A.lvb, &A.lu1, &A.lk1, &A.lk2, &A.lk3, &A.lk4, &A.lus, &A.lF, &A.lueff};
@@ -1537,9 +1548,7 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
     const int every = c->adj_every;
     const int64_t per = 2 * n3 + ng;
     double* tape = get((int64_t)every * 4 * per);
-    auto release = [&]() {
-        for (double* p : bufs) dfree(c, p);
-    };
+    auto release = [&]() {};
     if (!ok || !lUp || !lVp || !lugSp || !lug || !lugSn || !gradf || !tape) {
         release();
         return fail(PD_ERR_OOM, "pd_adjoint_backward: device memory for the tape");
