@@ -265,6 +265,10 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  * PD_OPT_FORCE_QUAD: 1 runs the FP32-form force with four nodes per thread
  *   (nodes on one lattice, one material, no critical stretch within reach;
  *   otherwise ignored); 0 (default) with two.
+ * PD_OPT_GATHER_SELL: 1 keeps a sliced-ELLPACK copy of the FP32 gather's
+ *   contributor lists and coefficients (16 nodes of the work order side by
+ *   side per contributor slot: coalesced loads; 2x2x2 points), 0 (default)
+ *   reads the CSR lists.  Costs a second FP32 copy of the coefficients.
  * PD_OPT_PERSIST_WAIT_US: how long a grid barrier of the persistent launch
  *   waits before it gives up (default 4 s; 1 ms to 60 s).
  * PD_OPT_PERSIST_TEST_STALL: 1 makes block 0 of the persistent launch skip
@@ -281,7 +285,8 @@ enum {
     PD_OPT_FORCE_TILE = 8,
     PD_OPT_FORCE_QUAD = 9,
     PD_OPT_PERSIST_WAIT_US = 10,
-    PD_OPT_PERSIST_TEST_STALL = 11
+    PD_OPT_PERSIST_TEST_STALL = 11,
+    PD_OPT_GATHER_SELL = 12
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -309,7 +314,7 @@ typedef struct pd_tune_result {
     int32_t pad;
     int64_t force_tile;       /* PD_OPT_FORCE_TILE kept */
     int32_t force_quad;       /* PD_OPT_FORCE_QUAD kept */
-    int32_t pad2;
+    int32_t gather_sell;      /* PD_OPT_GATHER_SELL kept */
 } pd_tune_result;
 /* Times candidate launch shapes (node-order tiles, the FP32 gather variant,
  * shared-memory force tiles;

@@ -86,6 +86,9 @@ struct pd_ctx {
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
+    int64_t* sell_off = nullptr;  // SELL copy of the FP32 gather's lists
+    int32_t* sell_idx = nullptr;
+    float* sell_coef = nullptr;
     double* adj_pool = nullptr;  // reverse-sweep work buffers and stage tape
     int64_t adj_pool_count = 0;
     bool have_family = false, have_mls = false;
@@ -566,6 +569,41 @@ int pd_sync(pd_ctx* c) {
     return PD_OK;
 }
 
+// The SELL copy of the FP32 gather's contributor lists, in the current work
+// order (rebuilt after pd_set_mls and after a work-order change; freed when
+// the gather cannot use it).
+static int sell_prepare(pd_ctx* c) {
+    dfree(c, c->sell_off);
+    dfree(c, c->sell_idx);
+    dfree(c, c->sell_coef);
+    c->sell_off = nullptr;
+    c->sell_idx = nullptr;
+    c->sell_coef = nullptr;
+    c->d.sell_off = nullptr;
+    c->d.sell_idx = nullptr;
+    c->d.sell_coef = nullptr;
+    if (!c->d.sell_on || !c->have_mls || !c->d.mls || c->npt != 8 || c->n == 0) return PD_OK;
+    const int64_t S = pd::sell_slices(c->d);
+    int64_t* width = nullptr;
+    PD_TRY(dalloc(c, &width, S));
+    PD_TRY(dalloc(c, &c->sell_off, S + 1));
+    pd::launch_sell_width(c->d, width, c->stream);
+    int rc = pd::exclusive_scan_i64(width, c->sell_off, S, c->stream);
+    dfree(c, width);
+    if (rc != PD_OK) return fail(PD_ERR_CUDA, "SELL layout: scan");
+    int64_t total = 0;
+    PD_CUDA_TRY(cudaMemcpy(&total, c->sell_off + S, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    PD_TRY(dalloc(c, &c->sell_idx, total * 16));
+    PD_TRY(dalloc(c, &c->sell_coef, total * 16 * 8));
+    c->d.sell_off = c->sell_off;
+    c->d.sell_idx = c->sell_idx;
+    c->d.sell_coef = c->sell_coef;
+    pd::launch_sell_fill(c->d, c->sell_off, c->sell_idx, c->sell_coef, c->stream);
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->generation++;
+    return PD_OK;
+}
+
 static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr, int64_t* arow, int32_t* acol,
                            int64_t H, int64_t Ha) {
     dfree(c, c->frow); dfree(c, c->fcol); dfree(c, c->fbroken); dfree(c, c->arow); dfree(c, c->acol);
@@ -738,7 +776,7 @@ int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const do
     c->d.csum = c->csum;
     c->have_mls = true;
     c->generation++;
-    return PD_OK;
+    return sell_prepare(c);
 }
 
 int pd_set_precision(pd_ctx* c, int p) {
@@ -761,6 +799,7 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             PD_TRY(upload(c, (void*)c->d.order, ord.data(), sizeof(int32_t) * c->n));
             PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
             c->tile = value;
+            if (c->d.sell_on) PD_TRY(sell_prepare(c));
             break;
         }
         case PD_OPT_PERSIST_BLOCKS_PER_SM:
@@ -786,6 +825,13 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
         case PD_OPT_FORCE_QUAD:
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.force_quad = (int)value;
+            break;
+        case PD_OPT_GATHER_SELL:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            if ((int)value != c->d.sell_on) {
+                c->d.sell_on = (int)value;
+                PD_TRY(sell_prepare(c));
+            }
             break;
         case PD_OPT_FORCE_TILE: {
             if (value == 0) {
@@ -842,6 +888,7 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
             *value = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
             return PD_OK;
         case PD_OPT_FORCE_QUAD: *value = c->d.force_quad; return PD_OK;
+        case PD_OPT_GATHER_SELL: *value = c->d.sell_on; return PD_OK;
         case PD_OPT_PERSIST_WAIT_US: *value = c->persist_wait_us; return PD_OK;
         case PD_OPT_PERSIST_TEST_STALL: *value = c->persist_stall; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
@@ -1832,6 +1879,16 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
         if ((rc = trial(T)) != PD_OK) return done(rc);
         if (!(best.ms < before)) c->d.gather_per_point = gp0;
         out->gather_per_point = c->d.gather_per_point;
+        if (c->npt == 8 && !c->d.gather_per_point) {
+            // the SELL layout of the gather (rebuilt for every later order trial)
+            const int s0 = c->d.sell_on;
+            const double b2 = best.ms;
+            if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, !s0)) != PD_OK) return done(rc);
+            Trial T2{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+            if ((rc = trial(T2)) != PD_OK) return done(rc);
+            if (!(best.ms < b2) && (rc = pd_set_option(c, PD_OPT_GATHER_SELL, s0)) != PD_OK) return done(rc);
+            out->gather_sell = c->d.sell_on;
+        }
     }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.hasfail &&
         !c->d.multimat) {

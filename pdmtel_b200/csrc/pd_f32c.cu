@@ -148,6 +148,7 @@ __device__ __forceinline__ void store_own(const Dev& d, int64_t i, const Own& o,
 // the two families.  pdDataManager.cpp:1917-1962 in FP32 form.
 // Node blocks staged in shared memory (the tiled kernel): a box of the
 // lattice [lo, lo + (lx, ly, ...)) with kTileStride floats per node.
+constexpr int kSell = 16;        // nodes per SELL slice of the gather
 constexpr int kTileStride = 36;  // 144 B: 16-byte aligned, and lanes reading
                                  // different nodes spread over the banks
 struct SmemTile {
@@ -575,7 +576,12 @@ __global__ void k_pack_cci(Dev d) {
 // ill-conditioned moment matrices allow, hence the second term).  Nodes with a
 // boundary condition keep the reference's rules on the FP64 Gauss-point
 // displacement (pdDataManager.cpp:2604-2703) and store its difference.
-template <bool PERSIST>
+// SELL (sliced ELLPACK, 16 nodes per slice in the work order): contributor
+// slot k of the 16 nodes of a slice is stored side by side, so a warp's index
+// load reads 64 contiguous bytes and its coefficient load 512 (the CSR rows:
+// one 32-byte sector in each of 16 rows).  Every thread still walks only its
+// own node's contributors, in order: the same sums bit for bit.
+template <bool PERSIST, bool SELL = false>
 __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int64_t tid, double t) {
     const int64_t N = d.n;
     const int npt = d.npt, ngrp = (npt + 3) / 4;
@@ -623,8 +629,17 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
     }
     double a[4][3] = {};
     const int64_t c0 = d.cbptr[i], nc = d.cbptr[i + 1] - c0;
+    // contributor k: index cb[k * cs], coefficients cf[k * fs + q]
     const int32_t* cb = d.cbidx + c0;
     const float* cf = d.coeff32 + c0 * npt + g0;
+    int64_t cs = 1, fs = npt;
+    if (SELL) {
+        const int64_t slot = tid / ngrp, sl = slot / kSell, l = slot % kSell, base = d.sell_off[sl];
+        cb = d.sell_idx + base * kSell + l;
+        cf = d.sell_coef + (base * kSell + l) * 8 + g0;
+        cs = kSell;
+        fs = kSell * 8;
+    }
     const bool vec = (ng == 4) && ((npt & 3) == 0);
     int64_t k = 0;
     if (vec) {
@@ -635,8 +650,8 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
             float4 cv[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                m[u] = __ldg(cb + k + u);
-                cv[u] = ld4(cf + (k + u) * npt);
+                m[u] = __ldg(cb + (k + u) * cs);
+                cv[u] = ld4(cf + (k + u) * fs);
             }
             double dd[4][3];
 #pragma unroll
@@ -658,15 +673,15 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
         }
     }
     for (; k < nc; ++k) {
-        const int64_t m = cb[k];
+        const int64_t m = cb[k * cs];
         const double d0 = ldm<PERSIST>(us + m) - u0, d1 = ldm<PERSIST>(us + N + m) - u1,
                      d2 = ldm<PERSIST>(us + 2 * N + m) - u2;
         float c[4];
         if (vec) {
-            const float4 v = ld4(cf + k * npt);
+            const float4 v = ld4(cf + k * fs);
             c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
         } else {
-            for (int q = 0; q < 4; ++q) c[q] = q < ng ? cf[k * npt + q] : 0.f;
+            for (int q = 0; q < 4; ++q) c[q] = q < ng ? cf[k * fs + q] : 0.f;
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -683,10 +698,39 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
     }
 }
 
+template <bool SELL>
 __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __restrict__ us) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (tid >= d.n * ((d.npt + 3) / 4)) return;
-    gather_group<false>(d, us, tid, *d.tdev);
+    gather_group<false, SELL>(d, us, tid, *d.tdev);
+}
+
+// SELL layout: the widest contributor list of every slice, then the copy
+__global__ void k_sell_width(Dev d, int64_t* __restrict__ width, int64_t S) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    int64_t w = 0;
+    for (int l = 0; l < kSell; ++l) {
+        const int64_t slot = s * kSell + l;
+        if (slot >= d.n) break;
+        const int64_t i = d.order[slot];
+        w = max(w, d.cbptr[i + 1] - d.cbptr[i]);
+    }
+    width[s] = w;
+}
+
+__global__ void k_sell_fill(Dev d, const int64_t* __restrict__ off, int32_t* __restrict__ sidx,
+                            float* __restrict__ scoef) {
+    const int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (slot >= d.n) return;
+    const int64_t i = d.order[slot], sl = slot / kSell, l = slot % kSell, base = off[sl];
+    const int64_t c0 = d.cbptr[i], nc = d.cbptr[i + 1] - c0;
+    for (int64_t k = 0; k < nc; ++k) {
+        sidx[(base + k) * kSell + l] = d.cbidx[c0 + k];
+        const float* src = d.coeff32 + (c0 + k) * 8;
+        float* dst = scoef + ((base + k) * kSell + l) * 8;
+        for (int g = 0; g < 8; ++g) dst[g] = src[g];
+    }
 }
 
 // The same gather with one thread per (node, Gauss point): a third of the
@@ -1014,7 +1058,20 @@ void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
         return;
     }
     const int ngrp = (d.npt + 3) / 4;
-    k_gather_f32c<<<blocks_for(d.n * ngrp, 256), 256, 0, s>>>(d, us);
+    if (d.sell_on && d.sell_idx && d.mls && d.npt == 8)
+        k_gather_f32c<true><<<blocks_for(d.n * ngrp, 256), 256, 0, s>>>(d, us);
+    else k_gather_f32c<false><<<blocks_for(d.n * ngrp, 256), 256, 0, s>>>(d, us);
+}
+
+int64_t sell_slices(const Dev& d) { return (d.n + kSell - 1) / kSell; }
+
+void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s) {
+    const int64_t S = sell_slices(d);
+    if (S) k_sell_width<<<blocks_for(S, 256), 256, 0, s>>>(d, width, S);
+}
+
+void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s) {
+    if (d.n) k_sell_fill<<<blocks_for(d.n, 128), 128, 0, s>>>(d, off, sidx, scoef);
 }
 
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s) {

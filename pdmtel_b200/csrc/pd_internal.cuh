@@ -111,6 +111,11 @@ struct Dev {
     int fam_radius;
     int tile_x, tile_y, tile_z;
     int force_quad;           // FP32 force: four nodes per thread (lattice, one material, no failure)
+    // FP32 gather in SELL layout (16 nodes per slice of the work order, 2x2x2 points)
+    int sell_on;
+    const int64_t* sell_off;  // [slices + 1] first contributor slot of each slice
+    const int32_t* sell_idx;  // [slots][16]
+    const float* sell_coef;   // [slots][16][8]
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -138,6 +143,9 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s);
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
 size_t tiled_smem_bytes(const Dev& d);
+int64_t sell_slices(const Dev& d);
+void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s);
+void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s);
 int prepare_tiled_force(size_t smem);
 void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
 
