@@ -119,16 +119,23 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Samples carry nvidia-smi's own timestamp; start() returns once the first
+    sample has arrived, begin()/end() mark the timed region on the same wall
+    clock, and stop() keeps the samples inside it (or, for a region shorter
+    than the sampling interval, the nearest sample before and after it)."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=20):
         self.gpu = gpu_index
+        self.interval = interval_ms
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def start(self):
         if not shutil.which("nvidia-smi"):
@@ -137,35 +144,65 @@ class ClockSampler:
         os.close(fd)
         self.f = open(self.path, "w")
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
-                                     stderr=subprocess.DEVNULL)
+                                      "--format=csv,noheader,nounits", "-lms", str(self.interval)],
+                                     stdout=self.f, stderr=subprocess.DEVNULL)
+        deadline = time.time() + 5.0
+        while time.time() < deadline and os.path.getsize(self.path) == 0:
+            time.sleep(0.01)
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
+
+    @staticmethod
+    def _when(stamp):
+        import datetime
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(stamp, fmt).timestamp()
+            except ValueError:
+                pass
+        return None
 
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(2.5 * self.interval / 1000.0)  # one sample after the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.f.close()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
+            if len(p) < 10:
                 continue
             try:
-                sm.append(float(p[1]))
-                smax.append(float(p[2]))
+                rows.append((self._when(p[0]), float(p[2]), float(p[3]), p[6:10]))
             except ValueError:
                 continue
-            for k, n in enumerate(names):
-                if p[5 + k].lower().startswith("active"):
-                    reasons.add(n)
         os.unlink(self.path)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        inside = [r for r in rows if r[0] is not None and self.t0 is not None and self.t0 <= r[0] <= self.t1]
+        note = "samples inside the timed region"
+        if not inside and rows and self.t0 is not None:
+            before = [r for r in rows if r[0] is not None and r[0] < self.t0]
+            after = [r for r in rows if r[0] is not None and r[0] > self.t1]
+            inside = before[-1:] + after[:1]
+            note = "timed region shorter than the sampling interval: nearest samples before and after"
+        reasons = set()
+        for r in inside:
+            for k, n in enumerate(names):
+                if r[3][k].lower().startswith("active"):
+                    reasons.add(n)
+        sm = [r[1] for r in inside]
+        smax = [r[2] for r in inside]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": self.interval, "note": note}
 
 
 def setup_plate(workdir, cfg):
@@ -296,21 +333,25 @@ def run_batch(args):
     ev_step = bt.evals_per_step()
     tune = bt.tune(steps=2)
 
-    def timed(fn):
+    def timed(fn, sampler=None):
         bt.ctx.reset_state()
         fn(args.warmup)
         bt.ctx.reset_state()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        if sampler:
+            sampler.begin()
         e0.record(stream)
         fn(args.steps)
         e1.record(stream)
         e1.synchronize()
+        if sampler:
+            sampler.end()
         return e0.elapsed_time(e1) / 1e3
 
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
-    t_b = timed(lambda k: bt.run(k))
+    t_b = timed(lambda k: bt.run(k), sampler)
     clocks = sampler.stop()
     t_other = timed(lambda k: bt.run(k, persistent=not bt.persistent))
     # one context per specimen, stepped one after the other
@@ -552,10 +593,13 @@ def run_ours(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if sampler:
             sampler.start()
+            sampler.begin()
         e0.record(stream)
         ctx.rk4_steps(dt, args.warmup * dt, args.steps)
         e1.record(stream)
         e1.synchronize()
+        if sampler:
+            sampler.end()
         clocks = sampler.stop() if sampler else None
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1), ws)

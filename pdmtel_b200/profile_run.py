@@ -33,6 +33,9 @@ def main():
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--count", type=int, default=16)
     ap.add_argument("--nmax", type=int, default=20000)
+    ap.add_argument("--sell", action="store_true", help="plate: FP32 gather from the SELL copy")
+    ap.add_argument("--quad", action="store_true", help="plate: FP32 force with four nodes per thread")
+    ap.add_argument("--order-tile", default=None, help="plate: node-order tile exponents bx,by,bz")
     a = ap.parse_args()
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     import pdmtel_b200 as P
@@ -50,6 +53,13 @@ def main():
         ctx = dm.context()
         ctx.set_energy(False)
         ctx.set_precision(prec)
+        if a.order_tile:
+            bx, by, bz = (int(v) for v in a.order_tile.split(","))
+            ctx.set_option(P.OPT_TILE, bx | (by << 8) | (bz << 16))
+        if a.sell:
+            ctx.set_option(P.OPT_GATHER_SELL, 1)
+        if a.quad:
+            ctx.set_option(P.OPT_FORCE_QUAD, 1)
         setup = time.time() - t0
         dt = 5e-9
         ctx.rk4_steps(dt, 0.0, a.warmup)
