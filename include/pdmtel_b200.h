@@ -273,7 +273,21 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   waits before it gives up (default 4 s; 1 ms to 60 s).
  * PD_OPT_PERSIST_TEST_STALL: 1 makes block 0 of the persistent launch skip
  *   its first barrier, so that every wait there runs out and the call
- *   returns PD_ERR_TIMEOUT; for tests of that path.  0 by default. */
+ *   returns PD_ERR_TIMEOUT; for tests of that path.  0 by default.
+ * PD_OPT_FORCE_STENCIL: 1..4 runs the FP32-form force on the lattice
+ *   stencil: the family of every node becomes a bit mask over one list of
+ *   lattice offsets, the gather stores the node blocks chunk-major, and a
+ *   block covers 16 x-adjacent node pairs by (8x1, 4x2, 2x4, 1x8) rows x
+ *   layers for the values 1..4.  Needs 2x2x2 points, one material and a
+ *   complete box lattice whose node ids are x + nx (y + ny z) (checked on
+ *   the device: PD_ERR_ARG otherwise).  Takes precedence over the other
+ *   force variants; 0 (default) turns it off.  Reset to 0 whenever the
+ *   family changes.  Same results bit for bit as the other FP32 kernels
+ *   when no critical stretch is within reach (with one, those form bond
+ *   vectors from FP32 hi/lo coordinate splits instead of lattice offsets,
+ *   and the results agree to FP32 rounding).
+ *   Turning it on or off changes the layout of the node blocks that
+ *   pd_gather stores for pd_force_stage: gather again after the change. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -286,7 +300,8 @@ enum {
     PD_OPT_FORCE_QUAD = 9,
     PD_OPT_PERSIST_WAIT_US = 10,
     PD_OPT_PERSIST_TEST_STALL = 11,
-    PD_OPT_GATHER_SELL = 12
+    PD_OPT_GATHER_SELL = 12,
+    PD_OPT_FORCE_STENCIL = 13
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -315,8 +330,11 @@ typedef struct pd_tune_result {
     int64_t force_tile;       /* PD_OPT_FORCE_TILE kept */
     int32_t force_quad;       /* PD_OPT_FORCE_QUAD kept */
     int32_t gather_sell;      /* PD_OPT_GATHER_SELL kept */
+    int32_t force_stencil;    /* PD_OPT_FORCE_STENCIL kept */
+    int32_t pad2;
 } pd_tune_result;
-/* Times candidate launch shapes (node-order tiles, the FP32 gather variant,
+/* Times candidate launch shapes (node-order tiles, the FP32 gather variants,
+ * the FP32 force variants: lattice stencil, four nodes per thread,
  * shared-memory force tiles;
  * for the persistent launch blocks per SM and queue chunks) over `steps`
  * steps each from the current state, keeps the fastest in the context and

@@ -86,6 +86,10 @@ struct pd_ctx {
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
+    int fst_shape = 0;            // lattice-stencil FP32 force (PD_OPT_FORCE_STENCIL)
+    int4* fst_u2 = nullptr;
+    float4* fst_tab = nullptr;
+    uint32_t* fst_mask = nullptr;
     int64_t* sell_off = nullptr;  // SELL copy of the FP32 gather's lists
     int32_t* sell_idx = nullptr;
     float* sell_coef = nullptr;
@@ -604,6 +608,149 @@ static int sell_prepare(pd_ctx* c) {
     return PD_OK;
 }
 
+// The lattice-stencil FP32 force: off (buffers freed, contiguous node blocks).
+static void fsten_release(pd_ctx* c) {
+    dfree(c, c->fst_u2);
+    dfree(c, c->fst_tab);
+    dfree(c, c->fst_mask);
+    c->fst_u2 = nullptr;
+    c->fst_tab = nullptr;
+    c->fst_mask = nullptr;
+    c->fst_shape = 0;
+    c->d.blk_cm = 0;
+    c->d.sten_u2 = nullptr;
+    c->d.sten_tab = nullptr;
+    c->d.sten_mask = nullptr;
+    c->d.sten_nu = c->d.sten_nw = 0;
+    c->d.sten_np = 0;
+    c->generation++;
+}
+
+// Builds the stencil S (every offset an unbroken family entry takes), the
+// union list U2 = S u (S + e_x) of a node pair, the (offset, point) table and
+// the masks of every pair, checking on the device that the node ids follow
+// x + nx (y + ny z) and that every family maps onto U2 in ascending order.
+static int fsten_prepare(pd_ctx* c, int shape) {
+    static const int kBy[5] = {0, 8, 4, 2, 1};
+    if (shape < 0 || shape > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
+    if (shape == 0) {
+        fsten_release(c);
+        return PD_OK;
+    }
+    if (c->fst_mask) {  // built: only the block shape changes
+        c->fst_shape = shape;
+        c->d.sten_by = kBy[shape];
+        c->d.sten_bz = 8 / kBy[shape];
+        c->generation++;
+        return PD_OK;
+    }
+    const int64_t NX = c->d.lat_nx, NY = c->d.lat_ny, NZ = c->d.lat_nz;
+    if (c->d.cci || c->npt != 8 || !c->d.gc_host || !c->d.lat || !c->have_family || c->d.multimat || c->n == 0 ||
+        NX * NY * NZ != c->n)
+        return fail(PD_ERR_ARG,
+                    "pd_set_option: the stencil force needs 2x2x2 points, one material, a family and a complete "
+                    "box lattice");
+    int* rad = reinterpret_cast<int*>(c->hscalar + 8);
+    pd::launch_family_radius(c->d, reinterpret_cast<int*>(c->scal + pd::CG_NSLOT - 1), c->stream);
+    PD_CUDA_TRY(cudaMemcpyAsync(rad, c->scal + pd::CG_NSLOT - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const int R = *rad;
+    if (R > 16) return fail(PD_ERR_ARG, "pd_set_option: family radius too large for the stencil force");
+    const int W = 2 * R + 1;
+    int* dbits = nullptr;  // [W^3] bitmap, then the error word
+    PD_TRY(dalloc(c, &dbits, (size_t)W * W * W + 1));
+    int* derr = dbits + (size_t)W * W * W;
+    auto done = [&](int rc) {
+        dfree(c, dbits);
+        if (rc != PD_OK) fsten_release(c);
+        return rc;
+    };
+    if (cudaMemsetAsync(dbits, 0, sizeof(int) * ((size_t)W * W * W + 1), c->stream) != cudaSuccess)
+        return done(fail(PD_ERR_CUDA, "stencil force: memset"));
+    pd::launch_sten_offsets(c->d, R, dbits, derr, c->stream);
+    std::vector<int> bits((size_t)W * W * W + 1);
+    if (cudaMemcpyAsync(bits.data(), dbits, sizeof(int) * bits.size(), cudaMemcpyDeviceToHost, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return done(fail(PD_ERR_CUDA, "stencil force: offsets"));
+    if (bits.back() != 0)
+        return done(fail(PD_ERR_ARG, "pd_set_option: node ids do not follow the box lattice x + nx (y + ny z)"));
+    // S in ascending id offset, then U2 = S u (S + e_x)
+    auto lin = [&](int ox, int oy, int oz) { return (int64_t)ox + NX * ((int64_t)oy + NY * oz); };
+    std::vector<std::array<int, 3>> S;
+    for (int oz = -R; oz <= R; ++oz)
+        for (int oy = -R; oy <= R; ++oy)
+            for (int ox = -R; ox <= R; ++ox)
+                if (bits[(ox + R) + W * ((oy + R) + W * (oz + R))]) S.push_back({ox, oy, oz});
+    auto by_lin = [&](const std::array<int, 3>& a, const std::array<int, 3>& b) {
+        return lin(a[0], a[1], a[2]) < lin(b[0], b[1], b[2]);
+    };
+    std::sort(S.begin(), S.end(), by_lin);
+    const int WX = W + 1;
+    std::vector<int> sidx((size_t)WX * W * W, -1);  // offset from A over [-R, R+1] x [-R, R]^2 -> S index
+    for (size_t k = 0; k < S.size(); ++k) sidx[(S[k][0] + R) + WX * ((S[k][1] + R) + W * (S[k][2] + R))] = (int)k;
+    std::vector<std::array<int, 3>> U;
+    for (int oz = -R; oz <= R; ++oz)
+        for (int oy = -R; oy <= R; ++oy)
+            for (int ox = -R; ox <= R + 1; ++ox) {
+                const bool a = ox <= R && sidx[(ox + R) + WX * ((oy + R) + W * (oz + R))] >= 0;
+                const bool b = ox - 1 >= -R && sidx[(ox - 1 + R) + WX * ((oy + R) + W * (oz + R))] >= 0;
+                if (a || b) U.push_back({ox, oy, oz});
+            }
+    std::sort(U.begin(), U.end(), by_lin);
+    if (U.size() > 512) return done(fail(PD_ERR_ARG, "pd_set_option: stencil of more than 512 pair offsets"));
+    std::vector<int4> u2(U.size());
+    std::vector<int> lut((size_t)WX * W * W, -1);
+    for (size_t u = 0; u < U.size(); ++u) {
+        const int ox = U[u][0], oy = U[u][1], oz = U[u][2];
+        const int ka = ox <= R ? sidx[(ox + R) + WX * ((oy + R) + W * (oz + R))] : -1;
+        const int kb = ox - 1 >= -R ? sidx[(ox - 1 + R) + WX * ((oy + R) + W * (oz + R))] : -1;
+        u2[u] = make_int4((int)lin(ox, oy, oz), ka, kb, 0);
+        lut[(ox + R) + WX * ((oy + R) + W * (oz + R))] = (int)u;
+    }
+    std::vector<int4> offs(S.size());
+    for (size_t k = 0; k < S.size(); ++k) offs[k] = make_int4(S[k][0], S[k][1], S[k][2], 0);
+    const int nu = (int)U.size(), nw = (nu + 31) / 32, ns = (int)S.size();
+    const int64_t np = (NX + 1) / 2 * NY * NZ;
+    int4* doffs = nullptr;
+    int* dlut = nullptr;
+    int rc = PD_OK;
+    if ((rc = dalloc(c, &c->fst_u2, std::max<size_t>(u2.size(), 1))) ||
+        (rc = dalloc(c, &c->fst_tab, (size_t)ns * 16)) || (rc = dalloc(c, &c->fst_mask, (size_t)2 * nw * np)) ||
+        (rc = dalloc(c, &doffs, std::max<size_t>(offs.size(), 1))) || (rc = dalloc(c, &dlut, lut.size())))
+        return done(rc);
+    auto done2 = [&](int r) {
+        dfree(c, doffs);
+        dfree(c, dlut);
+        return done(r);
+    };
+    if ((rc = upload(c, c->fst_u2, u2.data(), sizeof(int4) * u2.size())) ||
+        (rc = upload(c, doffs, offs.data(), sizeof(int4) * offs.size())) ||
+        (rc = upload(c, dlut, lut.data(), sizeof(int) * lut.size())))
+        return done2(rc);
+    pd::Dev t = c->d;
+    t.sten_u2 = c->fst_u2;
+    t.sten_tab = c->fst_tab;
+    t.sten_mask = c->fst_mask;
+    t.sten_nu = nu;
+    t.sten_nw = nw;
+    t.sten_np = np;
+    pd::launch_sten_table(t, doffs, ns, c->fst_tab, c->stream);
+    pd::launch_sten_masks(t, dlut, R, c->fst_mask, derr, c->stream);
+    int err = 0;
+    if (cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return done2(fail(PD_ERR_CUDA, "stencil force: masks"));
+    if (err) return done2(fail(PD_ERR_ARG, "pd_set_option: a family does not map onto the lattice stencil"));
+    t.blk_cm = 1;
+    t.sten_by = kBy[shape];
+    t.sten_bz = 8 / kBy[shape];
+    c->d = t;
+    c->fst_shape = shape;
+    c->generation++;
+    return done2(PD_OK);
+}
+
 static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr, int64_t* arow, int32_t* acol,
                            int64_t H, int64_t Ha) {
     dfree(c, c->frow); dfree(c, c->fcol); dfree(c, c->fbroken); dfree(c, c->arow); dfree(c, c->acol);
@@ -614,6 +761,7 @@ static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr
     c->Ha = Ha;
     c->have_family = true;
     c->d.tile_x = c->d.tile_y = c->d.tile_z = 0;  // its family radius may have changed
+    if (c->fst_mask) fsten_release(c);
     c->generation++;
 }
 
@@ -826,6 +974,10 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.force_quad = (int)value;
             break;
+        case PD_OPT_FORCE_STENCIL:
+            if (value > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
+            PD_TRY(fsten_prepare(c, (int)value));
+            break;
         case PD_OPT_GATHER_SELL:
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             if ((int)value != c->d.sell_on) {
@@ -889,6 +1041,7 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
             return PD_OK;
         case PD_OPT_FORCE_QUAD: *value = c->d.force_quad; return PD_OK;
         case PD_OPT_GATHER_SELL: *value = c->d.sell_on; return PD_OK;
+        case PD_OPT_FORCE_STENCIL: *value = c->fst_shape; return PD_OK;
         case PD_OPT_PERSIST_WAIT_US: *value = c->persist_wait_us; return PD_OK;
         case PD_OPT_PERSIST_TEST_STALL: *value = c->persist_stall; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
@@ -1825,8 +1978,9 @@ int time_steps(pd_ctx* c, const Snapshot& S, double dt, int steps, bool persiste
 }  // namespace
 
 // Times candidate launch shapes on this context's own problem and keeps the
-// fastest: first the node-order tile with the graph-captured step, then (when
-// the persistent launch applies) its blocks per SM and queue chunk sizes.
+// fastest: first the node-order tile with the graph-captured step, then the
+// FP32 gather and force variants, then (when the persistent launch applies)
+// its blocks per SM and queue chunk sizes.
 // The state is restored after every trial, so tuning leaves it as it was.
 extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out) {
     if (!c || !out || steps < 1 || !(dt > 0.0)) return fail(PD_ERR_ARG, "pd_autotune: bad argument");
@@ -1890,8 +2044,23 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
             out->gather_sell = c->d.sell_on;
         }
     }
+    if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.multimat) {
+        // the lattice-stencil force in each block shape, on the best shape so far
+        const int f0 = c->fst_shape;
+        int keep = f0;
+        const double before = best.ms;
+        for (int sh = 1; sh <= 4; ++sh) {
+            if (pd_set_option(c, PD_OPT_FORCE_STENCIL, sh) != PD_OK) break;  // not a box lattice: skip
+            Trial T{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+            const double prev = best.ms;
+            if ((rc = trial(T)) != PD_OK) return done(rc);
+            if (best.ms < prev) keep = sh;
+        }
+        if ((rc = pd_set_option(c, PD_OPT_FORCE_STENCIL, best.ms < before ? keep : f0)) != PD_OK) return done(rc);
+        out->force_stencil = c->fst_shape;
+    }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.hasfail &&
-        !c->d.multimat) {
+        !c->d.multimat && !c->fst_shape) {
         // four nodes per thread in the force, on the best shape so far
         const double before = best.ms;
         c->d.force_quad = 1;
@@ -1902,7 +2071,7 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
         out->force_quad = c->d.force_quad;
     }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && c->d.pos2id &&
-        !c->d.force_quad) {
+        !c->d.force_quad && !c->fst_shape) {
         // the shared-memory tiles of the force, on the best shape so far
         const int tz = std::min(c->d.lat_nz, 4);
         const int64_t cand[][3] = {{16, 8, tz}, {32, 4, tz}, {16, 4, tz}, {8, 8, tz}, {32, 8, tz}, {64, 2, tz}};

@@ -73,7 +73,7 @@ __device__ __forceinline__ void bond4(const PointPack<8>& G, int q, const float*
         const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
         const float p2 = r2 + dd;
         const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
-        const float r = r2 * rinv;
+        const float r = __fmul_rn(r2, rinv);
         const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
         const float beta = __saturatef((P.A - r) * P.B);
         float fm = P.W * beta * s * pinv;
@@ -93,7 +93,10 @@ struct Own {
     float s[3], k[3];    // Kahan sum of the family force
 };
 
-__device__ __forceinline__ void kahan_add(Own& o, float F0, float F1, float F2) {
+// the bond force F c added to the family sum (products rounded on their own,
+// never contracted into the subtraction, so every kernel rounds alike)
+__device__ __forceinline__ void kahan_add(Own& o, const float* F, float c) {
+    const float F0 = __fmul_rn(F[0], c), F1 = __fmul_rn(F[1], c), F2 = __fmul_rn(F[2], c);
     float y = F0 - o.k[0], t = o.s[0] + y;
     o.k[0] = (t - o.s[0]) - y;
     o.s[0] = t;
@@ -227,9 +230,9 @@ __device__ __forceinline__ void force_nodes(const Dev& d, const PointPack<8>& G,
         for (int side = 0; side < 2; ++side) {
             const Own& O = side == 0 ? A : B;
             if (LAT) {
-                dx[side][0] = (float)((lj & 2047) - (O.lat & 2047)) * h;
-                dx[side][1] = (float)(((lj >> 11) & 2047) - ((O.lat >> 11) & 2047)) * h;
-                dx[side][2] = (float)((lj >> 22) - (O.lat >> 22)) * h;  // packed values are non-negative
+                dx[side][0] = __fmul_rn((float)((lj & 2047) - (O.lat & 2047)), h);
+                dx[side][1] = __fmul_rn((float)(((lj >> 11) & 2047) - ((O.lat >> 11) & 2047)), h);
+                dx[side][2] = __fmul_rn((float)((lj >> 22) - (O.lat >> 22)), h);  // packed values are non-negative
             } else {
                 for (int a = 0; a < 3; ++a) dx[side][a] = (pj[a] - O.ph[a]) + (pj[3 + a] - O.pl[a]);
             }
@@ -259,11 +262,11 @@ __device__ __forceinline__ void force_nodes(const Dev& d, const PointPack<8>& G,
                     bond4<HASFAIL>(G, q, u4, dx[side], du[side], ecrit[side], F[side]);
         }
         if (has[0]) {
-            kahan_add(A, F[0][0] * coef[0], F[0][1] * coef[0], F[0][2] * coef[0]);
+            kahan_add(A, F[0], coef[0]);
             ++pa;
         }
         if (has[1]) {
-            kahan_add(B, F[1][0] * coef[1], F[1][1] * coef[1], F[1][2] * coef[1]);
+            kahan_add(B, F[1], coef[1]);
             ++pb;
         }
     }
@@ -339,9 +342,9 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
         float dx[4][3], du[4][3], coef[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            dx[k][0] = (float)((lj & 2047) - (O[k].lat & 2047)) * h;
-            dx[k][1] = (float)(((lj >> 11) & 2047) - ((O[k].lat >> 11) & 2047)) * h;
-            dx[k][2] = (float)((lj >> 22) - (O[k].lat >> 22)) * h;
+            dx[k][0] = __fmul_rn((float)((lj & 2047) - (O[k].lat & 2047)), h);
+            dx[k][1] = __fmul_rn((float)(((lj >> 11) & 2047) - ((O[k].lat >> 11) & 2047)), h);
+            dx[k][2] = __fmul_rn((float)((lj >> 22) - (O[k].lat >> 22)), h);
             for (int a = 0; a < 3; ++a) du[k][a] = (ujh[a] - O[k].uh[a]) + (ujl[a] - O[k].ul[a]);
             float c = O[k].c;
             if (BDRY) c *= 0.5f * (O[k].be + bej);
@@ -360,13 +363,205 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (js[k] == j) {
-                kahan_add(O[k], F[k][0] * coef[k], F[k][1] * coef[k], F[k][2] * coef[k]);
+                kahan_add(O[k], F[k], coef[k]);
                 ++p[k];
             }
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k)
         if (id[k] >= 0) store_own<false>(d, id[k], O[k], nb[k], dts, d.vbuf);
+}
+
+// ------------------------------------------------------- lattice stencil
+//
+// On a complete box lattice the family of a node is a subset of one stencil
+// S of lattice offsets, and the geometric terms of a bond's Gauss points
+// (x = xi + h_g, r2, 1/r, r, W beta) depend on its offset only.  The stencil
+// kernel therefore reads them from a table instead of computing them, walks
+// a bit mask of the family instead of its column list, and reads the node
+// blocks chunk-major, so that the 16 pairs of a warp row read a neighbour
+// chunk from 512 contiguous bytes.  The table holds exactly the values bond4
+// computes (same expressions, same rounding; dx and r are rounded on their
+// own in both), the per-node sums run in the same ascending order, so the
+// result is that of the pair kernel's lattice variants bit for bit.
+
+// bond4 with the geometric terms of the bond's offset read from its table
+// row T (two float4 per Gauss point)
+template <bool HASFAIL>
+__device__ __forceinline__ void bond4_tab(const float4* __restrict__ T, const float* u4, const float* du,
+                                          float ecrit, float* F) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 a = __ldg(T + 2 * k), b = __ldg(T + 2 * k + 1);
+        const float x0 = a.x, x1 = a.y, x2 = a.z, r2 = a.w, rinv = b.x, r = b.y;
+        const float e0 = du[0] + u4[k], e1 = du[1] + u4[4 + k], e2 = du[2] + u4[8 + k];
+        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
+        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
+        const float p2 = r2 + dd;
+        const float pinv = rsqrtf(p2);
+        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
+        float fm = b.z * s * pinv;
+        if (HASFAIL && dd > 0.f && s > ecrit) fm = 0.f;
+        F[0] = fmaf(fm, y0, F[0]);
+        F[1] = fmaf(fm, y1, F[1]);
+        F[2] = fmaf(fm, y2, F[2]);
+    }
+}
+
+// One thread per x-adjacent node pair (A, B = A + 1) of a lattice row; a
+// block covers 16 pairs x sten_by rows x sten_bz layers.  The thread walks
+// the union list U2 in ascending offset (= ascending neighbour id) over the
+// set bits of the two masks; a warp's threads are in step wherever their
+// families have the same shape, so the U2 entry and the table rows are read
+// at one address by the whole warp.
+template <bool HASFAIL, bool BDRY, bool SFAC>
+__global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, double dts) {
+    const int NX = d.lat_nx, NY = d.lat_ny, NZ = d.lat_nz;
+    const int npx = (NX + 1) >> 1, BY = d.sten_by, BZ = d.sten_bz;
+    const int nbx = (npx + 15) >> 4, nby = (NY + BY - 1) / BY;
+    const int b = blockIdx.x;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int px = (b % nbx) * 16 + tx;
+    const int y = ((b / nbx) % nby) * BY + ty % BY;
+    const int z = (b / (nbx * nby)) * BZ + ty / BY;
+    if (px >= npx || y >= NY || z >= NZ) return;
+    const int64_t N = d.n, NP = d.sten_np;
+    const int64_t yz = y + (int64_t)NY * z;
+    const int64_t p = px + (int64_t)npx * yz;
+    const int64_t ia = 2 * px + (int64_t)NX * yz;
+    const bool hb = 2 * px + 1 < NX;
+    Own A, B;
+    load_own<true, BDRY, SFAC, false>(d, ia, A);
+    load_own<true, BDRY, SFAC, false>(d, hb ? ia + 1 : ia, B);
+    const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
+    const float4* __restrict__ tab = d.sten_tab;
+    const int nw = d.sten_nw;
+    int nba = 0, nbb = 0;
+    for (int w = 0; w < nw; ++w) {
+        const uint32_t ma = __ldg(d.sten_mask + (int64_t)w * NP + p);
+        const uint32_t mb = hb ? __ldg(d.sten_mask + (int64_t)(nw + w) * NP + p) : 0u;
+        nba += __popc(ma);
+        nbb += __popc(mb);
+        uint32_t m = ma | mb;
+        while (m) {
+            const int bit = __ffs(m) - 1;
+            m &= m - 1;
+            const int4 E = __ldg(d.sten_u2 + 32 * w + bit);
+            const bool has[2] = {((ma >> bit) & 1u) != 0, ((mb >> bit) & 1u) != 0};
+            const int64_t j = ia + E.x;
+            const float4 us0 = __ldg(blk + 6 * N + j), us1 = __ldg(blk + 7 * N + j);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
+            float bej = 1.f, sfj = 1.f;
+            if (BDRY || SFAC) {
+                const float2 v = __ldg(reinterpret_cast<const float2*>(d.sblk + 8 * j + 6));
+                bej = v.x;
+                sfj = v.y;
+            }
+            const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
+            float du[2][3], coef[2];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const Own& O = side == 0 ? A : B;
+                for (int a = 0; a < 3; ++a) du[side][a] = (ujh[a] - O.uh[a]) + (ujl[a] - O.ul[a]);
+                float c = O.c;
+                if (BDRY) c *= 0.5f * (O.be + bej);
+                if (SFAC) c *= 0.5f * (O.sf + sfj);
+                coef[side] = c;
+            }
+            const float4* TA = tab + 16 * (int64_t)max(E.y, 0);
+            const float4* TB = tab + 16 * (int64_t)max(E.z, 0);
+            float F[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll
+            for (int q = 0; q < 8; q += 4) {
+                const float4 vx = __ldg(blk + (q >> 2) * N + j), vy = __ldg(blk + (2 + (q >> 2)) * N + j),
+                             vz = __ldg(blk + (4 + (q >> 2)) * N + j);
+                const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
+                if (has[0]) bond4_tab<HASFAIL>(TA + 2 * q, u4, du[0], A.e, F[0]);
+                if (has[1]) bond4_tab<HASFAIL>(TB + 2 * q, u4, du[1], B.e, F[1]);
+            }
+            if (has[0]) kahan_add(A, F[0], coef[0]);
+            if (has[1]) kahan_add(B, F[1], coef[1]);
+        }
+    }
+    store_own<false>(d, ia, A, nba, dts, d.vbuf);
+    if (hb) store_own<false>(d, ia + 1, B, nbb, dts, d.vbuf);
+}
+
+// Setup: the offsets (from the node) of every unbroken family entry, over
+// [-R, R]^3.  err bit 1: a node id is not x + nx (y + ny z) of its lattice
+// position; bit 2: an offset beyond R.
+__global__ void k_sten_offsets(Dev d, int R, int* __restrict__ bitmap, int* __restrict__ err) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int li = d.lat[i];
+    const int xi = li & 2047, yi = (li >> 11) & 2047, zi = li >> 22;
+    if (i != xi + (int64_t)d.lat_nx * (yi + (int64_t)d.lat_ny * zi)) atomicOr(err, 1);
+    const int W = 2 * R + 1;
+    for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+        const int lj = d.lat[d.acol[p]];
+        const int ox = (lj & 2047) - xi, oy = ((lj >> 11) & 2047) - yi, oz = (lj >> 22) - zi;
+        if (abs(ox) > R || abs(oy) > R || abs(oz) > R) {
+            atomicOr(err, 2);
+            continue;
+        }
+        bitmap[(ox + R) + W * ((oy + R) + W * (oz + R))] = 1;  // same value from every writer
+    }
+}
+
+// Setup: the two masks of every pair.  lut: U2 index of an offset from node
+// A over [-R, R+1] x [-R, R] x [-R, R], or -1.  err bit 4: a family entry
+// that is not in U2 as a bond of its node, not at A + its offset, or out of
+// ascending order.
+__global__ void k_sten_masks(Dev d, const int* __restrict__ lut, int R, uint32_t* __restrict__ mask,
+                             int* __restrict__ err) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= d.sten_np) return;
+    const int NX = d.lat_nx, npx = (NX + 1) / 2;
+    const int px = (int)(p % npx);
+    const int64_t ia = 2 * px + (int64_t)NX * (p / npx);
+    const int la = d.lat[ia];
+    const int xa = la & 2047, ya = (la >> 11) & 2047, za = la >> 22;
+    const int WX = 2 * R + 2, W = 2 * R + 1;
+    for (int side = 0; side < 2; ++side) {
+        uint32_t m[16];
+        for (int w = 0; w < 16; ++w) m[w] = 0u;
+        if (side == 0 || 2 * px + 1 < NX) {
+            const int64_t i = ia + side;
+            int last = -1;
+            for (int64_t e = d.arow[i]; e < d.arow[i + 1]; ++e) {
+                const int64_t j = d.acol[e];
+                const int lj = d.lat[j];
+                const int ox = (lj & 2047) - xa, oy = ((lj >> 11) & 2047) - ya, oz = (lj >> 22) - za;
+                int u = -1;
+                if (ox >= -R && ox <= R + 1 && abs(oy) <= R && abs(oz) <= R)
+                    u = lut[(ox + R) + WX * ((oy + R) + W * (oz + R))];
+                if (u < 0 || u <= last || (side ? d.sten_u2[u].z : d.sten_u2[u].y) < 0 || j != ia + d.sten_u2[u].x) {
+                    atomicOr(err, 4);
+                    break;
+                }
+                m[u >> 5] |= 1u << (u & 31);
+                last = u;
+            }
+        }
+        for (int w = 0; w < d.sten_nw; ++w) mask[((int64_t)side * d.sten_nw + w) * d.sten_np + p] = m[w];
+    }
+}
+
+// Setup: the table row of stencil offset k, point g, by bond4's expressions.
+__global__ void k_sten_table(PointPack<8> G, const int4* __restrict__ offs, int ns, float h,
+                             float4* __restrict__ tab) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns * 8) return;
+    const int k = t >> 3, g = t & 7;
+    const int4 o = offs[k];
+    const PointF P = G.p[g];
+    const float dx0 = __fmul_rn((float)o.x, h), dx1 = __fmul_rn((float)o.y, h), dx2 = __fmul_rn((float)o.z, h);
+    const float x0 = dx0 + P.hx, x1 = dx1 + P.hy, x2 = dx2 + P.hz;
+    const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
+    const float rinv = rsqrtf(r2);
+    const float r = __fmul_rn(r2, rinv);
+    const float beta = __saturatef((P.A - r) * P.B);
+    tab[2 * t] = make_float4(x0, x1, x2, r2);
+    tab[2 * t + 1] = make_float4(rinv, r, P.W * beta, 0.f);
 }
 
 // The same bond forces with the neighbour blocks of a lattice tile staged in
@@ -569,6 +764,18 @@ __global__ void k_pack_cci(Dev d) {
 
 // ----------------------------------------------------------------- gather
 
+// Element e of node i's block: contiguous [N][bs], or chunk-major (float4
+// chunk e / 4 of node i at nblk + 4 (chunk N + i)) for the lattice-stencil
+// force, which reads chunk c of x-adjacent nodes side by side.
+struct BlkOut {
+    float* p;
+    int64_t cs;  // 0: contiguous block; else the chunk stride 4 N
+    __device__ __forceinline__ float& operator[](int e) const { return cs ? p[(e >> 2) * cs + (e & 3)] : p[e]; }
+};
+__device__ __forceinline__ BlkOut blk_out(const Dev& d, int64_t i) {
+    return d.blk_cm ? BlkOut{d.nblk + 4 * i, 4 * d.n} : BlkOut{d.nblk + i * d.bs, 0};
+}
+
 // One thread per (node, group of up to four Gauss points): the Gauss-point
 // displacement relative to the node, sum_k c_k (us_k - us_i) + (sum_k c_k - 1)
 // us_i, accumulated in FP64 from FP32 coefficients (the MLS coefficients
@@ -589,7 +796,7 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
     const int grp = (int)(tid % ngrp);
     const int g0 = 4 * grp, ng = min(4, npt - g0);
     const double u0 = ldm<PERSIST>(us + i), u1 = ldm<PERSIST>(us + N + i), u2 = ldm<PERSIST>(us + 2 * N + i);
-    float* o = d.nblk + i * d.bs;
+    const BlkOut o = blk_out(d, i);
     if (grp == 0) {
         const float h0 = (float)u0, h1 = (float)u1, h2 = (float)u2;
         o[3 * npt + 0] = h0;
@@ -746,7 +953,7 @@ __global__ void __launch_bounds__(256) k_gather_f32c_pt(Dev d, const double* __r
     const int g = (int)(tid % npt);
     const double t = *d.tdev;
     const double u0 = __ldg(us + i), u1 = __ldg(us + N + i), u2 = __ldg(us + 2 * N + i);
-    float* o = d.nblk + i * d.bs;
+    const BlkOut o = blk_out(d, i);
     if (g == 0) {
         const float h0 = (float)u0, h1 = (float)u1, h2 = (float)u2;
         o[3 * npt + 0] = h0;
@@ -956,6 +1163,23 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
         else k_force_f32c_cci<false><<<nb, 128, 0, s>>>(d, dts);
         return;
     }
+    if (d.blk_cm && d.sten_mask) {
+        // the gather stores chunk-major blocks: only this kernel reads them
+        const int npx = (d.lat_nx + 1) / 2;
+        const unsigned nbk = (unsigned)(((npx + 15) / 16) * ((d.lat_ny + d.sten_by - 1) / d.sten_by) *
+                                        ((d.lat_nz + d.sten_bz - 1) / d.sten_bz));
+        const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
+#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, dts)
+        if (d.hasfail) {
+            if (bd) { if (sf) PD_STEN(true, true, true); else PD_STEN(true, true, false); }
+            else { if (sf) PD_STEN(true, false, true); else PD_STEN(true, false, false); }
+        } else {
+            if (bd) { if (sf) PD_STEN(false, true, true); else PD_STEN(false, true, false); }
+            else { if (sf) PD_STEN(false, false, true); else PD_STEN(false, false, false); }
+        }
+#undef PD_STEN
+        return;
+    }
     if (d.npt == 8 && d.gc_host && d.tile_x > 0 && d.lat && d.pos2id) {
         const PointPack<8> P = pack_points<8>(d, d.gc_host);
         const int nt = ((d.lat_nx + d.tile_x - 1) / d.tile_x) * ((d.lat_ny + d.tile_y - 1) / d.tile_y) *
@@ -1048,7 +1272,10 @@ cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl*
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, persist_variant(d), d, P, dt, nsteps, ctl, force_chunk, gather_chunk, W);
+    // its gather and force phases use the contiguous node blocks
+    Dev t = d;
+    t.blk_cm = 0;
+    return cudaLaunchKernelEx(&cfg, persist_variant(t), t, P, dt, nsteps, ctl, force_chunk, gather_chunk, W);
 }
 
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
@@ -1064,6 +1291,19 @@ void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
 }
 
 int64_t sell_slices(const Dev& d) { return (d.n + kSell - 1) / kSell; }
+
+void launch_sten_offsets(const Dev& d, int R, int* bitmap, int* err, cudaStream_t s) {
+    if (d.n) k_sten_offsets<<<blocks_for(d.n, 256), 256, 0, s>>>(d, R, bitmap, err);
+}
+
+void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int* err, cudaStream_t s) {
+    if (d.sten_np) k_sten_masks<<<blocks_for(d.sten_np, 128), 128, 0, s>>>(d, lut, R, mask, err);
+}
+
+void launch_sten_table(const Dev& d, const int4* offs, int ns, float4* tab, cudaStream_t s) {
+    if (ns) k_sten_table<<<blocks_for((int64_t)ns * 8, 128), 128, 0, s>>>(pack_points<8>(d, d.gc_host), offs, ns,
+                                                                          (float)d.dx, tab);
+}
 
 void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s) {
     const int64_t S = sell_slices(d);

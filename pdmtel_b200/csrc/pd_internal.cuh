@@ -89,7 +89,8 @@ struct Dev {
     //  nblk [N][bs]: Gauss-point displacement relative to the node, component-
     //        major ([x:npt][y:npt][z:npt]), then the node's trial displacement
     //        split into FP32 hi and lo parts (hi[3], lo[3]); rewritten by every
-    //        gather (or, for CCI, by the pack kernel)
+    //        gather (or, for CCI, by the pack kernel); chunk-major when blk_cm
+    //        is set (below)
     //  sblk [N][8]:  coordinates split hi[3], lo[3], boundary factor, spring factor
     float* nblk;
     int bs;
@@ -116,6 +117,24 @@ struct Dev {
     const int64_t* sell_off;  // [slices + 1] first contributor slot of each slice
     const int32_t* sell_idx;  // [slots][16]
     const float* sell_coef;   // [slots][16][8]
+    // FP32 force on the lattice stencil (2x2x2 points, a complete box lattice
+    // with node id = x + nx (y + ny z), one material).  blk_cm: nblk is stored
+    // chunk-major, float4 chunk c of node j at nblk + 4 (c N + j), so that a
+    // warp reading chunk c of x-adjacent nodes reads contiguous memory.  Work
+    // unit: the x-adjacent node pair (2 px, 2 px + 1) of a row; a block covers
+    // 16 pairs x sten_by rows x sten_bz layers.  Union list U2 (sten_nu
+    // entries, ascending offset): .x offset of the neighbour from node A of the
+    // pair (node id units), .y its index in the stencil S as a bond of A (or
+    // -1), .z as a bond of B = A + 1 (or -1).  Table per (stencil offset k,
+    // point g): float4 (x0, x1, x2, r2), float4 (1/r, r, W beta, 0).  Masks
+    // [side][word][pair]: bit u of a side set when U2 entry u is an unbroken
+    // bond of that node.
+    int blk_cm;
+    int sten_nu, sten_nw, sten_by, sten_bz;
+    int64_t sten_np;
+    const int4* sten_u2;
+    const float4* sten_tab;
+    const uint32_t* sten_mask;
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -138,7 +157,7 @@ int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int
                 const double* slits_dev, int64_t** frow, int32_t** fcol, uint8_t** fbroken, int64_t** arow,
                 int32_t** acol, int64_t* nh, int64_t* nb, double* min_bond, cudaStream_t s);
 
-// FP32 compensated form (pd_fast.cu)
+// FP32 compensated form (pd_f32c.cu)
 void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);
 void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s);
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
@@ -148,6 +167,13 @@ void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s);
 void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s);
 int prepare_tiled_force(size_t smem);
 void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
+// lattice-stencil force setup: offsets present in the families (bitmap over
+// [-R, R]^3, R the family radius), the masks of every pair (err: set when a
+// family does not fit the union list or a node breaks the box numbering),
+// the table of (offset, point) terms
+void launch_sten_offsets(const Dev& d, int R, int* bitmap, int* err, cudaStream_t s);
+void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int* err, cudaStream_t s);
+void launch_sten_table(const Dev& d, const int4* offs, int ns, float4* tab, cudaStream_t s);
 
 // persistent FP32C stepping (pd_f32c.cu): control block of one launch.
 // next[8*step + 2*(stage-1) + phase] are the work-queue counters; all of it

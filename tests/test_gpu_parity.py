@@ -355,3 +355,94 @@ def test_fp32c_sell_gather_equals_csr_gather(name):
     for sell, tile in ((1, None), (1, 2 | (1 << 8) | (1 << 16))):
         U1, V1 = run(sell, tile)
         assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (sell, tile)
+
+
+def _fp32c_state(make_dm, dt, steps, stencil=0, sfac=None):
+    dm = make_dm()
+    dm.SetPrecision(P.PREC_FP32C)
+    ctx = dm.context()
+    if sfac is not None:
+        ctx.set_spring_factor(sfac)
+    if stencil:
+        ctx.set_option(P.OPT_FORCE_STENCIL, stencil)
+        assert ctx.get_option(P.OPT_FORCE_STENCIL) == stencil
+    ctx.rk4_steps(dt, 0.0, steps)
+    ctx.sync()
+    return ctx.get_state()
+
+
+@pytest.mark.parametrize("name", ["fgi_slit", "fgi_velo"])
+def test_fp32c_stencil_force_equals_pair_kernel(name):
+    """The FP32 force on the lattice stencil (family as a bit mask over one
+    offset list, geometric terms from a per-offset table, chunk-major node
+    blocks): the same terms in the same order per node as the pair kernel,
+    so the same trajectory bit for bit, in every block shape."""
+    g = load_golden(name)
+    dt = g["dt"][0]
+    U0, V0 = _fp32c_state(lambda: gpu_model(name), dt, 20)
+    assert np.abs(U0).max() > 0
+    for shape in (1, 2, 3, 4):
+        U1, V1 = _fp32c_state(lambda: gpu_model(name), dt, 20, stencil=shape)
+        assert np.array_equal(U0, U1) and np.array_equal(V0, V1), shape
+
+
+def _stencil_decks():
+    # odd row length (the last node of a row has no pair partner), a slit
+    yield "odd_rows_slit", D.config_plate(dims=(35, 22, 3), spacing=5e-4, slit_half_length=2.5e-3, dt=5e-9,
+                                           vel=5.0), None
+    # boundary-effect factors
+    d = D.config_plate(dims=(20, 16, 4), spacing=5e-4, slit_half_length=1.5e-3, dt=5e-9, vel=5.0)
+    d.bdry_eff = 1
+    yield "bdry", d, None
+    # a critical stretch that the loaded layers exceed
+    d = D.config_plate(dims=(20, 16, 4), spacing=5e-4, slit_half_length=1.5e-3, dt=5e-9, vel=5.0)
+    d.materials = [(72e9, 1e20, 2e-5, 2440.0)]
+    yield "ecrit", d, None
+    # per-node spring factors
+    d = D.config_plate(dims=(24, 12, 4), spacing=5e-4, slit_half_length=1.5e-3, dt=5e-9, vel=5.0)
+    yield "sfac", d, np.exp(0.2 * np.random.default_rng(3).standard_normal(24 * 12 * 4))
+
+
+@pytest.mark.parametrize("case", list(range(4)))
+def test_fp32c_stencil_force_variants_equal_pair_kernel(tmp_path, case):
+    """Odd rows, boundary factors, a critical stretch within reach and
+    spring factors: every template variant of the stencil kernel against
+    the pair kernel, bit for bit.  With a critical stretch the pair kernel
+    runs its general variant, which forms bond vectors from FP32 hi/lo
+    splits of the coordinates instead of lattice offsets; there the two
+    agree to 1e-6 (the FP32 form's bar against FP64)."""
+    name, deck, sfac = list(_stencil_decks())[case]
+    deck.write(str(tmp_path))
+    dt = 5e-9
+    make = lambda: gpu_model(str(tmp_path))  # noqa: E731
+    U0, V0 = _fp32c_state(make, dt, 30, sfac=sfac)
+    assert np.abs(U0).max() > 0
+    for shape in (1, 3):
+        U1, V1 = _fp32c_state(make, dt, 30, stencil=shape, sfac=sfac)
+        if name == "ecrit":
+            assert np.linalg.norm(U1 - U0) <= 1e-6 * np.linalg.norm(U0), shape
+            assert np.linalg.norm(V1 - V0) <= 1e-6 * np.linalg.norm(V0), shape
+        else:
+            assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (name, shape)
+
+
+def test_fp32c_stencil_force_rejects_and_resets(tmp_path):
+    """Problems off a complete box lattice are refused (deleted nodes, 3x3x3
+    points, CCI); a new bond search turns the stencil force off."""
+    d = D.config_plate(dims=(20, 16, 4), spacing=5e-4, slit_half_length=1.5e-3, dt=5e-9)
+    d.deletion_spaces = [D.Space(0, (1.2e-3, 0.0, 0.0, -1.0, 1.0), geo=2)]
+    hole = tmp_path / "hole"
+    d.write(str(hole))
+    for dm in (gpu_model(str(hole)), gpu_model("fgi3_ramp"), gpu_model("cci_grad")):
+        dm.SetPrecision(P.PREC_FP32C)
+        ctx = dm.context()
+        with pytest.raises(P.PdError):
+            ctx.set_option(P.OPT_FORCE_STENCIL, 1)
+        assert ctx.get_option(P.OPT_FORCE_STENCIL) == 0
+    dm = gpu_model("fgi_velo")
+    ctx = dm.context()
+    with pytest.raises(P.PdError):
+        ctx.set_option(P.OPT_FORCE_STENCIL, 5)
+    ctx.set_option(P.OPT_FORCE_STENCIL, 2)
+    ctx.bond_search()
+    assert ctx.get_option(P.OPT_FORCE_STENCIL) == 0
