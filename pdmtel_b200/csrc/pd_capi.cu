@@ -88,7 +88,6 @@ struct pd_ctx {
     int32_t *tj = nullptr, *tpos = nullptr;
     int fst_shape = 0;            // lattice-stencil FP32 force (PD_OPT_FORCE_STENCIL)
     int4* fst_u2 = nullptr;
-    float4* fst_tab = nullptr;
     uint32_t* fst_mask = nullptr;
     int64_t* sell_off = nullptr;  // SELL copy of the FP32 gather's lists
     int32_t* sell_idx = nullptr;
@@ -611,15 +610,12 @@ static int sell_prepare(pd_ctx* c) {
 // The lattice-stencil FP32 force: off (buffers freed, contiguous node blocks).
 static void fsten_release(pd_ctx* c) {
     dfree(c, c->fst_u2);
-    dfree(c, c->fst_tab);
     dfree(c, c->fst_mask);
     c->fst_u2 = nullptr;
-    c->fst_tab = nullptr;
     c->fst_mask = nullptr;
     c->fst_shape = 0;
     c->d.blk_cm = 0;
     c->d.sten_u2 = nullptr;
-    c->d.sten_tab = nullptr;
     c->d.sten_mask = nullptr;
     c->d.sten_nu = c->d.sten_nw = 0;
     c->d.sten_np = 0;
@@ -627,9 +623,9 @@ static void fsten_release(pd_ctx* c) {
 }
 
 // Builds the stencil S (every offset an unbroken family entry takes), the
-// union list U2 = S u (S + e_x) of a node pair, the (offset, point) table and
-// the masks of every pair, checking on the device that the node ids follow
-// x + nx (y + ny z) and that every family maps onto U2 in ascending order.
+// union list U2 = S u (S + e_x) of a node pair and the masks of every pair,
+// checking on the device that the node ids follow x + nx (y + ny z) and that
+// every family maps onto U2 in ascending order.
 static int fsten_prepare(pd_ctx* c, int shape) {
     static const int kBy[5] = {0, 8, 4, 2, 1};
     if (shape < 0 || shape > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
@@ -703,39 +699,29 @@ static int fsten_prepare(pd_ctx* c, int shape) {
     std::vector<int> lut((size_t)WX * W * W, -1);
     for (size_t u = 0; u < U.size(); ++u) {
         const int ox = U[u][0], oy = U[u][1], oz = U[u][2];
-        const int ka = ox <= R ? sidx[(ox + R) + WX * ((oy + R) + W * (oz + R))] : -1;
-        const int kb = ox - 1 >= -R ? sidx[(ox - 1 + R) + WX * ((oy + R) + W * (oz + R))] : -1;
-        u2[u] = make_int4((int)lin(ox, oy, oz), ka, kb, 0);
+        u2[u] = make_int4((int)lin(ox, oy, oz), ox, oy, oz);
         lut[(ox + R) + WX * ((oy + R) + W * (oz + R))] = (int)u;
     }
-    std::vector<int4> offs(S.size());
-    for (size_t k = 0; k < S.size(); ++k) offs[k] = make_int4(S[k][0], S[k][1], S[k][2], 0);
-    const int nu = (int)U.size(), nw = (nu + 31) / 32, ns = (int)S.size();
+    const int nu = (int)U.size(), nw = (nu + 31) / 32;
     const int64_t np = (NX + 1) / 2 * NY * NZ;
-    int4* doffs = nullptr;
     int* dlut = nullptr;
     int rc = PD_OK;
     if ((rc = dalloc(c, &c->fst_u2, std::max<size_t>(u2.size(), 1))) ||
-        (rc = dalloc(c, &c->fst_tab, (size_t)ns * 16)) || (rc = dalloc(c, &c->fst_mask, (size_t)2 * nw * np)) ||
-        (rc = dalloc(c, &doffs, std::max<size_t>(offs.size(), 1))) || (rc = dalloc(c, &dlut, lut.size())))
+        (rc = dalloc(c, &c->fst_mask, (size_t)2 * nw * np)) || (rc = dalloc(c, &dlut, lut.size())))
         return done(rc);
     auto done2 = [&](int r) {
-        dfree(c, doffs);
         dfree(c, dlut);
         return done(r);
     };
     if ((rc = upload(c, c->fst_u2, u2.data(), sizeof(int4) * u2.size())) ||
-        (rc = upload(c, doffs, offs.data(), sizeof(int4) * offs.size())) ||
         (rc = upload(c, dlut, lut.data(), sizeof(int) * lut.size())))
         return done2(rc);
     pd::Dev t = c->d;
     t.sten_u2 = c->fst_u2;
-    t.sten_tab = c->fst_tab;
     t.sten_mask = c->fst_mask;
     t.sten_nu = nu;
     t.sten_nw = nw;
     t.sten_np = np;
-    pd::launch_sten_table(t, doffs, ns, c->fst_tab, c->stream);
     pd::launch_sten_masks(t, dlut, R, c->fst_mask, derr, c->stream);
     int err = 0;
     if (cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||

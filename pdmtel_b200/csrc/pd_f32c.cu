@@ -375,47 +375,26 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 // ------------------------------------------------------- lattice stencil
 //
 // On a complete box lattice the family of a node is a subset of one stencil
-// S of lattice offsets, and the geometric terms of a bond's Gauss points
-// (x = xi + h_g, r2, 1/r, r, W beta) depend on its offset only.  The stencil
-// kernel therefore reads them from a table instead of computing them, walks
-// a bit mask of the family instead of its column list, and reads the node
-// blocks chunk-major, so that the 16 pairs of a warp row read a neighbour
-// chunk from 512 contiguous bytes.  The table holds exactly the values bond4
-// computes (same expressions, same rounding; dx and r are rounded on their
-// own in both), the per-node sums run in the same ascending order, so the
-// result is that of the pair kernel's lattice variants bit for bit.
-
-// bond4 with the geometric terms of the bond's offset read from its table
-// row T (two float4 per Gauss point)
-template <bool HASFAIL>
-__device__ __forceinline__ void bond4_tab(const float4* __restrict__ T, const float* u4, const float* du,
-                                          float ecrit, float* F) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float4 a = __ldg(T + 2 * k), b = __ldg(T + 2 * k + 1);
-        const float x0 = a.x, x1 = a.y, x2 = a.z, r2 = a.w, rinv = b.x, r = b.y;
-        const float e0 = du[0] + u4[k], e1 = du[1] + u4[4 + k], e2 = du[2] + u4[8 + k];
-        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
-        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
-        const float p2 = r2 + dd;
-        const float pinv = rsqrtf(p2);
-        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
-        float fm = b.z * s * pinv;
-        if (HASFAIL && dd > 0.f && s > ecrit) fm = 0.f;
-        F[0] = fmaf(fm, y0, F[0]);
-        F[1] = fmaf(fm, y1, F[1]);
-        F[2] = fmaf(fm, y2, F[2]);
-    }
-}
+// S of lattice offsets.  The stencil kernel walks a bit mask of the family
+// over the union list U2 = S u (S + e_x) of an x-adjacent node pair instead
+// of two column lists, takes the bond vector from the offset, and reads the
+// node blocks chunk-major, so that the 16 pairs of a warp row read a
+// neighbour chunk from 1 KB of contiguous memory (8 lines instead of 32).
+// Per node the same bond4 arithmetic in the same ascending neighbour order
+// as the pair kernel's lattice variants: the same result bit for bit.
+// (Reading the geometric terms of each offset and point from a table
+// instead of computing them was slower: a float4 that the whole warp reads
+// at one address still fills 512 bytes of registers, which costs the L1
+// data path as much as a coalesced load, and the table needs two per
+// evaluation.)
 
 // One thread per x-adjacent node pair (A, B = A + 1) of a lattice row; a
 // block covers 16 pairs x sten_by rows x sten_bz layers.  The thread walks
-// the union list U2 in ascending offset (= ascending neighbour id) over the
-// set bits of the two masks; a warp's threads are in step wherever their
-// families have the same shape, so the U2 entry and the table rows are read
-// at one address by the whole warp.
+// U2 in ascending offset (= ascending neighbour id) over the set bits of
+// the two masks; a warp's threads are in step wherever their families have
+// the same shape, so the U2 entry is read at one address by the whole warp.
 template <bool HASFAIL, bool BDRY, bool SFAC>
-__global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, double dts) {
+__global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
     const int NX = d.lat_nx, NY = d.lat_ny, NZ = d.lat_nz;
     const int npx = (NX + 1) >> 1, BY = d.sten_by, BZ = d.sten_bz;
     const int nbx = (npx + 15) >> 4, nby = (NY + BY - 1) / BY;
@@ -434,7 +413,7 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, double dts) {
     load_own<true, BDRY, SFAC, false>(d, ia, A);
     load_own<true, BDRY, SFAC, false>(d, hb ? ia + 1 : ia, B);
     const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
-    const float4* __restrict__ tab = d.sten_tab;
+    const float h = (float)d.dx;
     const int nw = d.sten_nw;
     int nba = 0, nbb = 0;
     for (int w = 0; w < nw; ++w) {
@@ -446,7 +425,7 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, double dts) {
         while (m) {
             const int bit = __ffs(m) - 1;
             m &= m - 1;
-            const int4 E = __ldg(d.sten_u2 + 32 * w + bit);
+            const int4 E = __ldg(d.sten_u2 + 32 * w + bit);  // id offset, ox, oy, oz from A
             const bool has[2] = {((ma >> bit) & 1u) != 0, ((mb >> bit) & 1u) != 0};
             const int64_t j = ia + E.x;
             const float4 us0 = __ldg(blk + 6 * N + j), us1 = __ldg(blk + 7 * N + j);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
@@ -457,26 +436,28 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, double dts) {
                 sfj = v.y;
             }
             const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
-            float du[2][3], coef[2];
+            float dx[2][3], du[2][3], coef[2];
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const Own& O = side == 0 ? A : B;
+                dx[side][0] = __fmul_rn((float)(E.y - side), h);
+                dx[side][1] = __fmul_rn((float)E.z, h);
+                dx[side][2] = __fmul_rn((float)E.w, h);
                 for (int a = 0; a < 3; ++a) du[side][a] = (ujh[a] - O.uh[a]) + (ujl[a] - O.ul[a]);
                 float c = O.c;
                 if (BDRY) c *= 0.5f * (O.be + bej);
                 if (SFAC) c *= 0.5f * (O.sf + sfj);
                 coef[side] = c;
             }
-            const float4* TA = tab + 16 * (int64_t)max(E.y, 0);
-            const float4* TB = tab + 16 * (int64_t)max(E.z, 0);
             float F[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
 #pragma unroll
             for (int q = 0; q < 8; q += 4) {
                 const float4 vx = __ldg(blk + (q >> 2) * N + j), vy = __ldg(blk + (2 + (q >> 2)) * N + j),
                              vz = __ldg(blk + (4 + (q >> 2)) * N + j);
                 const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
-                if (has[0]) bond4_tab<HASFAIL>(TA + 2 * q, u4, du[0], A.e, F[0]);
-                if (has[1]) bond4_tab<HASFAIL>(TB + 2 * q, u4, du[1], B.e, F[1]);
+#pragma unroll
+                for (int side = 0; side < 2; ++side)
+                    if (has[side]) bond4<HASFAIL>(G, q, u4, dx[side], du[side], side == 0 ? A.e : B.e, F[side]);
             }
             if (has[0]) kahan_add(A, F[0], coef[0]);
             if (has[1]) kahan_add(B, F[1], coef[1]);
@@ -509,8 +490,7 @@ __global__ void k_sten_offsets(Dev d, int R, int* __restrict__ bitmap, int* __re
 
 // Setup: the two masks of every pair.  lut: U2 index of an offset from node
 // A over [-R, R+1] x [-R, R] x [-R, R], or -1.  err bit 4: a family entry
-// that is not in U2 as a bond of its node, not at A + its offset, or out of
-// ascending order.
+// that is not in U2, not at A + its offset, or out of ascending order.
 __global__ void k_sten_masks(Dev d, const int* __restrict__ lut, int R, uint32_t* __restrict__ mask,
                              int* __restrict__ err) {
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -534,7 +514,7 @@ __global__ void k_sten_masks(Dev d, const int* __restrict__ lut, int R, uint32_t
                 int u = -1;
                 if (ox >= -R && ox <= R + 1 && abs(oy) <= R && abs(oz) <= R)
                     u = lut[(ox + R) + WX * ((oy + R) + W * (oz + R))];
-                if (u < 0 || u <= last || (side ? d.sten_u2[u].z : d.sten_u2[u].y) < 0 || j != ia + d.sten_u2[u].x) {
+                if (u < 0 || u <= last || j != ia + d.sten_u2[u].x) {
                     atomicOr(err, 4);
                     break;
                 }
@@ -544,24 +524,6 @@ __global__ void k_sten_masks(Dev d, const int* __restrict__ lut, int R, uint32_t
         }
         for (int w = 0; w < d.sten_nw; ++w) mask[((int64_t)side * d.sten_nw + w) * d.sten_np + p] = m[w];
     }
-}
-
-// Setup: the table row of stencil offset k, point g, by bond4's expressions.
-__global__ void k_sten_table(PointPack<8> G, const int4* __restrict__ offs, int ns, float h,
-                             float4* __restrict__ tab) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ns * 8) return;
-    const int k = t >> 3, g = t & 7;
-    const int4 o = offs[k];
-    const PointF P = G.p[g];
-    const float dx0 = __fmul_rn((float)o.x, h), dx1 = __fmul_rn((float)o.y, h), dx2 = __fmul_rn((float)o.z, h);
-    const float x0 = dx0 + P.hx, x1 = dx1 + P.hy, x2 = dx2 + P.hz;
-    const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
-    const float rinv = rsqrtf(r2);
-    const float r = __fmul_rn(r2, rinv);
-    const float beta = __saturatef((P.A - r) * P.B);
-    tab[2 * t] = make_float4(x0, x1, x2, r2);
-    tab[2 * t + 1] = make_float4(rinv, r, P.W * beta, 0.f);
 }
 
 // The same bond forces with the neighbour blocks of a lattice tile staged in
@@ -1163,13 +1125,14 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
         else k_force_f32c_cci<false><<<nb, 128, 0, s>>>(d, dts);
         return;
     }
-    if (d.blk_cm && d.sten_mask) {
+    if (d.blk_cm && d.sten_mask && d.npt == 8 && d.gc_host) {
         // the gather stores chunk-major blocks: only this kernel reads them
         const int npx = (d.lat_nx + 1) / 2;
         const unsigned nbk = (unsigned)(((npx + 15) / 16) * ((d.lat_ny + d.sten_by - 1) / d.sten_by) *
                                         ((d.lat_nz + d.sten_bz - 1) / d.sten_bz));
         const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
-#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, dts)
+        const PointPack<8> P = pack_points<8>(d, d.gc_host);
+#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, P, dts)
         if (d.hasfail) {
             if (bd) { if (sf) PD_STEN(true, true, true); else PD_STEN(true, true, false); }
             else { if (sf) PD_STEN(true, false, true); else PD_STEN(true, false, false); }
@@ -1300,10 +1263,6 @@ void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int*
     if (d.sten_np) k_sten_masks<<<blocks_for(d.sten_np, 128), 128, 0, s>>>(d, lut, R, mask, err);
 }
 
-void launch_sten_table(const Dev& d, const int4* offs, int ns, float4* tab, cudaStream_t s) {
-    if (ns) k_sten_table<<<blocks_for((int64_t)ns * 8, 128), 128, 0, s>>>(pack_points<8>(d, d.gc_host), offs, ns,
-                                                                          (float)d.dx, tab);
-}
 
 void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s) {
     const int64_t S = sell_slices(d);

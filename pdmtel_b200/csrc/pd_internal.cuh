@@ -122,18 +122,15 @@ struct Dev {
     // chunk-major, float4 chunk c of node j at nblk + 4 (c N + j), so that a
     // warp reading chunk c of x-adjacent nodes reads contiguous memory.  Work
     // unit: the x-adjacent node pair (2 px, 2 px + 1) of a row; a block covers
-    // 16 pairs x sten_by rows x sten_bz layers.  Union list U2 (sten_nu
-    // entries, ascending offset): .x offset of the neighbour from node A of the
-    // pair (node id units), .y its index in the stencil S as a bond of A (or
-    // -1), .z as a bond of B = A + 1 (or -1).  Table per (stencil offset k,
-    // point g): float4 (x0, x1, x2, r2), float4 (1/r, r, W beta, 0).  Masks
-    // [side][word][pair]: bit u of a side set when U2 entry u is an unbroken
-    // bond of that node.
+    // 16 pairs x sten_by rows x sten_bz layers.  Union list U2 = S u (S + e_x)
+    // (S: every lattice offset of a family entry; sten_nu entries, ascending):
+    // .x offset of the neighbour from node A of the pair in node ids, .y .z .w
+    // its lattice offset from A.  Masks [side][word][pair]: bit u of a side
+    // set when U2 entry u is an unbroken bond of that node.
     int blk_cm;
     int sten_nu, sten_nw, sten_by, sten_bz;
     int64_t sten_np;
     const int4* sten_u2;
-    const float4* sten_tab;
     const uint32_t* sten_mask;
 };
 
@@ -169,11 +166,9 @@ int prepare_tiled_force(size_t smem);
 void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
 // lattice-stencil force setup: offsets present in the families (bitmap over
 // [-R, R]^3, R the family radius), the masks of every pair (err: set when a
-// family does not fit the union list or a node breaks the box numbering),
-// the table of (offset, point) terms
+// family does not fit the union list or a node breaks the box numbering)
 void launch_sten_offsets(const Dev& d, int R, int* bitmap, int* err, cudaStream_t s);
 void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int* err, cudaStream_t s);
-void launch_sten_table(const Dev& d, const int4* offs, int ns, float4* tab, cudaStream_t s);
 
 // persistent FP32C stepping (pd_f32c.cu): control block of one launch.
 // next[8*step + 2*(stage-1) + phase] are the work-queue counters; all of it
