@@ -287,7 +287,15 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   vectors from FP32 hi/lo coordinate splits instead of lattice offsets,
  *   and the results agree to FP32 rounding).
  *   Turning it on or off changes the layout of the node blocks that
- *   pd_gather stores for pd_force_stage: gather again after the change. */
+ *   pd_gather stores for pd_force_stage: gather again after the change.
+ * PD_OPT_GATHER_STENCIL: 1 lets the FP32-form gather (one thread per four
+ *   points) take every node's MLS contributors from a pattern of id offsets
+ *   (nodes whose lists are translates of each other share one; kept with
+ *   the context and rebuilt by pd_set_mls) instead of its list, so the
+ *   contributor loads no longer wait on an index load from memory.  Same
+ *   contributors in the same order: same results bit for bit.  Refused
+ *   (PD_ERR_ARG) when the distinct patterns would hold more than 4M
+ *   entries; 0 (default) reads the lists. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -301,7 +309,8 @@ enum {
     PD_OPT_PERSIST_WAIT_US = 10,
     PD_OPT_PERSIST_TEST_STALL = 11,
     PD_OPT_GATHER_SELL = 12,
-    PD_OPT_FORCE_STENCIL = 13
+    PD_OPT_FORCE_STENCIL = 13,
+    PD_OPT_GATHER_STENCIL = 14
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -331,9 +340,10 @@ typedef struct pd_tune_result {
     int32_t force_quad;       /* PD_OPT_FORCE_QUAD kept */
     int32_t gather_sell;      /* PD_OPT_GATHER_SELL kept */
     int32_t force_stencil;    /* PD_OPT_FORCE_STENCIL kept */
-    int32_t pad2;
+    int32_t gather_stencil;   /* PD_OPT_GATHER_STENCIL kept */
 } pd_tune_result;
-/* Times candidate launch shapes (node-order tiles, the FP32 gather variants,
+/* Times candidate launch shapes (node-order tiles, the FP32 gather variants:
+ * per point, SELL copy, contributor patterns;
  * the FP32 force variants: lattice stencil, four nodes per thread,
  * shared-memory force tiles;
  * for the persistent launch blocks per SM and queue chunks) over `steps`

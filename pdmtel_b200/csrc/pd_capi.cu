@@ -8,6 +8,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "pd_internal.cuh"
@@ -86,6 +87,10 @@ struct pd_ctx {
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
+    int gpat_opt = 0;             // FP32 gather from contributor patterns (PD_OPT_GATHER_STENCIL)
+    int32_t* gpat_id = nullptr;
+    int64_t* gpat_ptr = nullptr;
+    int32_t* gpat_off = nullptr;
     int fst_shape = 0;            // lattice-stencil FP32 force (PD_OPT_FORCE_STENCIL)
     int4* fst_u2 = nullptr;
     uint32_t* fst_mask = nullptr;
@@ -607,6 +612,70 @@ static int sell_prepare(pd_ctx* c) {
     return PD_OK;
 }
 
+// The contributor patterns of the FP32 gather: every node's MLS contributor
+// list as id offsets from the node, identical lists stored once (on a box
+// lattice numbered x + nx (y + ny z) the lists of nodes with the same
+// position relative to the boundary are translates of each other).  Rebuilt
+// after pd_set_mls; freed when off.  Refused when the distinct patterns
+// would hold more than 4M entries (nothing repeats: no gain).
+static int gpat_prepare(pd_ctx* c) {
+    dfree(c, c->gpat_id);
+    dfree(c, c->gpat_ptr);
+    dfree(c, c->gpat_off);
+    c->gpat_id = nullptr;
+    c->gpat_ptr = nullptr;
+    c->gpat_off = nullptr;
+    c->d.gpat_id = nullptr;
+    c->d.gpat_ptr = nullptr;
+    c->d.gpat_off = nullptr;
+    c->generation++;
+    if (!c->gpat_opt || !c->have_mls || !c->d.mls || c->n == 0) return PD_OK;
+    const int64_t N = c->n;
+    const std::vector<int64_t>& cp = c->cbptr_host;
+    const std::vector<int32_t>& ci = c->cbidx_host;
+    std::vector<int32_t> pid((size_t)N);
+    std::vector<int64_t> ptr{0};
+    std::vector<int32_t> off;
+    std::unordered_map<uint64_t, std::vector<int32_t>> seen;  // content hash -> pattern ids
+    const size_t kMaxEntries = (size_t)4 << 20;
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t b = cp[i], e = cp[i + 1];
+        uint64_t h = 1469598103934665603ull ^ (uint64_t)(e - b);
+        for (int64_t k = b; k < e; ++k) h = (h ^ (uint64_t)(uint32_t)(ci[k] - (int32_t)i)) * 1099511628211ull;
+        auto& ids = seen[h];
+        int32_t found = -1;
+        for (int32_t q : ids) {
+            const int64_t pb = ptr[q], pe = ptr[q + 1];
+            if (pe - pb != e - b) continue;
+            bool same = true;
+            for (int64_t k = 0; k < e - b && same; ++k) same = off[pb + k] == ci[b + k] - (int32_t)i;
+            if (same) {
+                found = q;
+                break;
+            }
+        }
+        if (found < 0) {
+            if (off.size() + (size_t)(e - b) > kMaxEntries)
+                return fail(PD_ERR_ARG, "pd_set_option: the MLS contributor lists do not repeat (no patterns)");
+            found = (int32_t)(ptr.size() - 1);
+            for (int64_t k = b; k < e; ++k) off.push_back(ci[k] - (int32_t)i);
+            ptr.push_back((int64_t)off.size());
+            ids.push_back(found);
+        }
+        pid[i] = found;
+    }
+    PD_TRY(dalloc(c, &c->gpat_id, (size_t)N));
+    PD_TRY(dalloc(c, &c->gpat_ptr, ptr.size()));
+    PD_TRY(dalloc(c, &c->gpat_off, std::max<size_t>(off.size(), 1)));
+    PD_TRY(upload(c, c->gpat_id, pid.data(), sizeof(int32_t) * pid.size()));
+    PD_TRY(upload(c, c->gpat_ptr, ptr.data(), sizeof(int64_t) * ptr.size()));
+    if (!off.empty()) PD_TRY(upload(c, c->gpat_off, off.data(), sizeof(int32_t) * off.size()));
+    c->d.gpat_id = c->gpat_id;
+    c->d.gpat_ptr = c->gpat_ptr;
+    c->d.gpat_off = c->gpat_off;
+    return PD_OK;
+}
+
 // The lattice-stencil FP32 force: off (buffers freed, contiguous node blocks).
 static void fsten_release(pd_ctx* c) {
     dfree(c, c->fst_u2);
@@ -910,6 +979,7 @@ int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const do
     c->d.csum = c->csum;
     c->have_mls = true;
     c->generation++;
+    if (gpat_prepare(c) != PD_OK) c->gpat_opt = 0;  // the new lists do not repeat: plain lists
     return sell_prepare(c);
 }
 
@@ -959,6 +1029,17 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
         case PD_OPT_FORCE_QUAD:
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.force_quad = (int)value;
+            break;
+        case PD_OPT_GATHER_STENCIL:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            if ((int)value != c->gpat_opt) {
+                c->gpat_opt = (int)value;
+                const int rc = gpat_prepare(c);
+                if (rc != PD_OK) {
+                    c->gpat_opt = 0;
+                    return rc;
+                }
+            }
             break;
         case PD_OPT_FORCE_STENCIL:
             if (value > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
@@ -1028,6 +1109,7 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_FORCE_QUAD: *value = c->d.force_quad; return PD_OK;
         case PD_OPT_GATHER_SELL: *value = c->d.sell_on; return PD_OK;
         case PD_OPT_FORCE_STENCIL: *value = c->fst_shape; return PD_OK;
+        case PD_OPT_GATHER_STENCIL: *value = c->gpat_opt; return PD_OK;
         case PD_OPT_PERSIST_WAIT_US: *value = c->persist_wait_us; return PD_OK;
         case PD_OPT_PERSIST_TEST_STALL: *value = c->persist_stall; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
@@ -2029,6 +2111,15 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
             if (!(best.ms < b2) && (rc = pd_set_option(c, PD_OPT_GATHER_SELL, s0)) != PD_OK) return done(rc);
             out->gather_sell = c->d.sell_on;
         }
+        // contributor patterns instead of lists (refused when nothing repeats)
+        const int p0 = c->gpat_opt;
+        if (!c->d.gather_per_point && pd_set_option(c, PD_OPT_GATHER_STENCIL, !p0) == PD_OK) {
+            const double b3 = best.ms;
+            Trial T3{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+            if ((rc = trial(T3)) != PD_OK) return done(rc);
+            if (!(best.ms < b3) && (rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, p0)) != PD_OK) return done(rc);
+        }
+        out->gather_stencil = c->gpat_opt;
     }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.multimat) {
         // the lattice-stencil force in each block shape, on the best shape so far

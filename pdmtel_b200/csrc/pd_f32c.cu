@@ -750,15 +750,19 @@ __device__ __forceinline__ BlkOut blk_out(const Dev& d, int64_t i) {
 // load reads 64 contiguous bytes and its coefficient load 512 (the CSR rows:
 // one 32-byte sector in each of 16 rows).  Every thread still walks only its
 // own node's contributors, in order: the same sums bit for bit.
-template <bool PERSIST, bool SELL = false>
-__device__ __forceinline__ void gather_group(const Dev& d, const double* us, int64_t tid, double t) {
+// The part of a gather thread's work that needs no contributor: the node's
+// trial displacement (u0, u1, u2) and its FP32 hi/lo split (group 0), and the
+// whole job for nodes with a boundary condition or without MLS.  True when
+// the thread is done.
+template <bool PERSIST>
+__device__ __forceinline__ bool gather_head(const Dev& d, const double* us, int64_t i, int grp, double t,
+                                            const BlkOut& o, double& u0, double& u1, double& u2) {
     const int64_t N = d.n;
-    const int npt = d.npt, ngrp = (npt + 3) / 4;
-    const int64_t i = d.order[tid / ngrp];
-    const int grp = (int)(tid % ngrp);
+    const int npt = d.npt;
     const int g0 = 4 * grp, ng = min(4, npt - g0);
-    const double u0 = ldm<PERSIST>(us + i), u1 = ldm<PERSIST>(us + N + i), u2 = ldm<PERSIST>(us + 2 * N + i);
-    const BlkOut o = blk_out(d, i);
+    u0 = ldm<PERSIST>(us + i);
+    u1 = ldm<PERSIST>(us + N + i);
+    u2 = ldm<PERSIST>(us + 2 * N + i);
     if (grp == 0) {
         const float h0 = (float)u0, h1 = (float)u1, h2 = (float)u2;
         o[3 * npt + 0] = h0;
@@ -790,14 +794,40 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
             o[npt + g] = (float)(w1 - u1);
             o[2 * npt + g] = (float)(w2 - u2);
         }
-        return;
+        return true;
     }
     if (!d.mls) {
         for (int q = 0; q < ng; ++q) o[g0 + q] = o[npt + g0 + q] = o[2 * npt + g0 + q] = 0.f;
-        return;
+        return true;
     }
+    return false;
+}
+
+// PAT: contributor ids from the node's pattern (id offsets in an L1/L2-resident
+// table) instead of its list; the index load then no longer waits on memory.
+template <bool PERSIST, bool SELL = false, bool PAT = false>
+__device__ __forceinline__ void gather_group(const Dev& d, const double* us, int64_t tid, double t) {
+    const int64_t N = d.n;
+    const int npt = d.npt, ngrp = (npt + 3) / 4;
+    const int64_t i = d.order[tid / ngrp];
+    const int grp = (int)(tid % ngrp);
+    const int g0 = 4 * grp, ng = min(4, npt - g0);
+    const BlkOut o = blk_out(d, i);
+    double u0, u1, u2;
+    if (gather_head<PERSIST>(d, us, i, grp, t, o, u0, u1, u2)) return;
     double a[4][3] = {};
-    const int64_t c0 = d.cbptr[i], nc = d.cbptr[i + 1] - c0;
+    int64_t c0 = 0, nc = 0;
+    const int32_t* po = nullptr;  // PAT: contributor k is i + po[k]
+    if (PAT) {
+        const int pid = __ldg(d.gpat_id + i);
+        const int64_t q0 = __ldg(d.gpat_ptr + pid);
+        nc = __ldg(d.gpat_ptr + pid + 1) - q0;
+        po = d.gpat_off + q0;
+        if (!SELL) c0 = d.cbptr[i];
+    } else {
+        c0 = d.cbptr[i];
+        nc = d.cbptr[i + 1] - c0;
+    }
     // contributor k: index cb[k * cs], coefficients cf[k * fs + q]
     const int32_t* cb = d.cbidx + c0;
     const float* cf = d.coeff32 + c0 * npt + g0;
@@ -819,7 +849,7 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
             float4 cv[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                m[u] = __ldg(cb + (k + u) * cs);
+                m[u] = PAT ? (int)i + __ldg(po + k + u) : __ldg(cb + (k + u) * cs);
                 cv[u] = ld4(cf + (k + u) * fs);
             }
             double dd[4][3];
@@ -842,7 +872,7 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
         }
     }
     for (; k < nc; ++k) {
-        const int64_t m = cb[k * cs];
+        const int64_t m = PAT ? i + po[k] : cb[k * cs];
         const double d0 = ldm<PERSIST>(us + m) - u0, d1 = ldm<PERSIST>(us + N + m) - u1,
                      d2 = ldm<PERSIST>(us + 2 * N + m) - u2;
         float c[4];
@@ -867,11 +897,112 @@ __device__ __forceinline__ void gather_group(const Dev& d, const double* us, int
     }
 }
 
-template <bool SELL>
+template <bool SELL, bool PAT>
 __global__ void __launch_bounds__(256) k_gather_f32c(Dev d, const double* __restrict__ us) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (tid >= d.n * ((d.npt + 3) / 4)) return;
-    gather_group<false, SELL>(d, us, tid, *d.tdev);
+    gather_group<false, SELL, PAT>(d, us, tid, *d.tdev);
+}
+
+// 16-byte copy global -> shared that the thread waits for later (L2 only:
+// the coefficient stream is read once).
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+
+constexpr int kRing = 12;  // coefficient slots a thread keeps in flight
+
+// The SELL + pattern gather (2x2x2 points) with the coefficient stream run
+// through a shared-memory ring: each thread copies its own 16 bytes of each
+// contributor slot kRing slots ahead of the arithmetic (one commit group per
+// slot), so a warp keeps about 6 KB of the stream in flight without holding
+// it in registers, and the contributor ids come from the node's pattern
+// (L1-resident) without waiting on memory.  A thread reads back only what it
+// copied itself, after cp.async.wait_group, and refills a ring entry only
+// after the values read from it have been used.  Same FMAs in the same
+// contributor order as gather_group: the same result bit for bit.
+__global__ void __launch_bounds__(256) k_gather_f32c_ring(Dev d, const double* __restrict__ us) {
+    __shared__ float4 ring[8][kRing][32];
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= d.n * 2) return;
+    const int64_t N = d.n;
+    const int64_t slot = tid >> 1;
+    const int grp = (int)(tid & 1), g0 = 4 * grp;
+    const int64_t i = d.order[slot];
+    const BlkOut o = blk_out(d, i);
+    double u0, u1, u2;
+    if (gather_head<false>(d, us, i, grp, *d.tdev, o, u0, u1, u2)) return;
+    const int pid = __ldg(d.gpat_id + i);
+    const int64_t p0 = __ldg(d.gpat_ptr + pid);
+    const int nc = (int)(__ldg(d.gpat_ptr + pid + 1) - p0);
+    const int32_t* po = d.gpat_off + p0;
+    const int64_t sl = slot / kSell, ln = slot % kSell, base = d.sell_off[sl];
+    // contributor slot k of this thread: cf[32 k] (a slot is kSell nodes x 8 floats = 32 float4)
+    const float4* cf = reinterpret_cast<const float4*>(d.sell_coef + (base * kSell + ln) * 8 + g0);
+    float4* r = &ring[threadIdx.x >> 5][0][threadIdx.x & 31];  // ring entry e at r[32 e]
+#pragma unroll
+    for (int k = 0; k < kRing; ++k) {
+        if (k < nc) cp_async16(r + 32 * k, cf + (int64_t)32 * k);
+        cp_async_commit();
+    }
+    double a[4][3] = {};
+    int e = 0;  // ring entry of contributor k
+    for (int k = 0; k < nc; k += 4) {
+        cp_async_wait<kRing - 4>();  // slots k .. k+3 have landed
+        int m[4];
+        float4 cv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int eu = e + u < kRing ? e + u : e + u - kRing;
+            if (k + u < nc) {
+                cv[u] = r[32 * eu];
+                m[u] = (int)i + __ldg(po + k + u);
+            } else {
+                cv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                m[u] = (int)i;
+            }
+        }
+        double dd[4][3];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            dd[u][0] = __ldg(us + m[u]) - u0;
+            dd[u][1] = __ldg(us + N + m[u]) - u1;
+            dd[u][2] = __ldg(us + 2 * N + m[u]) - u2;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (k + u >= nc) break;
+            const float c[4] = {cv[u].x, cv[u].y, cv[u].z, cv[u].w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[q][0] = fma((double)c[q], dd[u][0], a[q][0]);
+                a[q][1] = fma((double)c[q], dd[u][1], a[q][1]);
+                a[q][2] = fma((double)c[q], dd[u][2], a[q][2]);
+            }
+        }
+        // refill the four entries just used with slots k + kRing .. k + kRing + 3
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int eu = e + u < kRing ? e + u : e + u - kRing;
+            const int kk = k + kRing + u;
+            if (kk < nc) cp_async16(r + 32 * eu, cf + (int64_t)32 * kk);
+            cp_async_commit();
+        }
+        e = e + 4 < kRing ? e + 4 : e + 4 - kRing;
+    }
+    cp_async_wait<0>();
+    for (int q = 0; q < 4; ++q) {
+        const double S = (double)d.csum[i * 8 + g0 + q];
+        o[g0 + q] = (float)fma(S, u0, a[q][0]);
+        o[8 + g0 + q] = (float)fma(S, u1, a[q][1]);
+        o[16 + g0 + q] = (float)fma(S, u2, a[q][2]);
+    }
 }
 
 // SELL layout: the widest contributor list of every slice, then the copy
@@ -1248,9 +1379,17 @@ void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
         return;
     }
     const int ngrp = (d.npt + 3) / 4;
-    if (d.sell_on && d.sell_idx && d.mls && d.npt == 8)
-        k_gather_f32c<true><<<blocks_for(d.n * ngrp, 256), 256, 0, s>>>(d, us);
-    else k_gather_f32c<false><<<blocks_for(d.n * ngrp, 256), 256, 0, s>>>(d, us);
+    const unsigned nb = blocks_for(d.n * ngrp, 256);
+    const bool sell = d.sell_on && d.sell_idx && d.mls && d.npt == 8, pat = d.gpat_id && d.mls;
+    if (sell && pat && d.npt == 8) {
+        k_gather_f32c_ring<<<nb, 256, 0, s>>>(d, us);
+    } else if (sell) {
+        if (pat) k_gather_f32c<true, true><<<nb, 256, 0, s>>>(d, us);
+        else k_gather_f32c<true, false><<<nb, 256, 0, s>>>(d, us);
+    } else {
+        if (pat) k_gather_f32c<false, true><<<nb, 256, 0, s>>>(d, us);
+        else k_gather_f32c<false, false><<<nb, 256, 0, s>>>(d, us);
+    }
 }
 
 int64_t sell_slices(const Dev& d) { return (d.n + kSell - 1) / kSell; }

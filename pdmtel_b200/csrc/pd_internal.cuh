@@ -131,7 +131,12 @@ struct Dev {
     int sten_nu, sten_nw, sten_by, sten_bz;
     int64_t sten_np;
     const int4* sten_u2;
-    const uint32_t* sten_mask;
+    const uint32_t* sten_mask;    // FP32 gather from contributor patterns: node i's contributors are
+    // i + gpat_off[gpat_ptr[p] ..] with p = gpat_id[i] (the same ids in the same
+    // order as its CSR list; nodes whose lists are translates share a pattern)
+    const int32_t* gpat_id;
+    const int64_t* gpat_ptr;
+    const int32_t* gpat_off;
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)

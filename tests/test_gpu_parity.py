@@ -446,3 +446,33 @@ def test_fp32c_stencil_force_rejects_and_resets(tmp_path):
     ctx.set_option(P.OPT_FORCE_STENCIL, 2)
     ctx.bond_search()
     assert ctx.get_option(P.OPT_FORCE_STENCIL) == 0
+
+
+@pytest.mark.parametrize("name", ["fgi_slit", "fgi_velo"])
+def test_fp32c_pattern_gather_equals_list_gather(name):
+    """The FP32 gather taking contributors from shared id-offset patterns:
+    the same contributors in the same order as the lists, so the same
+    trajectory bit for bit, with and without the SELL copy, and after the
+    MLS data are set again (the patterns are rebuilt)."""
+    g = load_golden(name)
+    dt = g["dt"][0]
+
+    def run(pat, sell, reset_mls=False):
+        dm = gpu_model(name)
+        dm.SetPrecision(P.PREC_FP32C)
+        ctx = dm.context()
+        ctx.set_option(P.OPT_GATHER_SELL, sell)
+        ctx.set_option(P.OPT_GATHER_STENCIL, pat)
+        assert ctx.get_option(P.OPT_GATHER_STENCIL) == pat
+        if reset_mls:
+            ctx.set_mls(*dm.mls())
+            assert ctx.get_option(P.OPT_GATHER_STENCIL) == pat
+        ctx.rk4_steps(dt, 0.0, 20)
+        ctx.sync()
+        return ctx.get_state()
+
+    U0, V0 = run(0, 0)
+    assert np.abs(U0).max() > 0
+    for pat, sell, reset in ((1, 0, False), (1, 1, False), (1, 1, True)):
+        U1, V1 = run(pat, sell, reset)
+        assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (pat, sell, reset)
