@@ -656,13 +656,22 @@ def run_ours(args):
     gather_ms = prof[1] / 4.0
     npt = I.num_gauss
     ncb = I.num_contrib
-    gather_bytes = ncb * npt * 4 + ncb * 4 + n * 8 * 4 + n * npt * 12 + n * npt * 4 + (n + 1) * 8
+    # the kernels the tuner kept
+    sten = bool(tune.get("force_stencil"))
+    force_kernel = ("k_force_f32c_sten" if sten else "k_force_f32c_quad" if tune.get("force_quad")
+                    else "k_force_f32c_tiled" if tune.get("force_tile") else "k_force_f32c_pair")
+    pat, sell = bool(tune.get("gather_stencil")), bool(tune.get("gather_sell"))
+    gather_kernel = "k_gather_f32c_ring" if (pat and sell) else "k_gather_f32c"
+    # coefficients, contributor ids (pattern ids instead with patterns), trial
+    # displacement, output blocks, partition-of-unity sums, row pointers
+    gather_bytes = (ncb * npt * 4 + (n * 4 if pat else ncb * 4 + (n + 1) * 8) + n * 8 * 4 + n * npt * 12
+                    + n * npt * 4)
     force_flops = FLOP_PER_EVAL * evals_stage
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get("force_f32c_bytes_per_launch")
+            traffic = json.load(f).get("force_f32c_sten_bytes_per_launch" if sten else "force_f32c_bytes_per_launch")
     value = replica_throughput(ws, evals_step * args.steps, ms32 / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -679,12 +688,12 @@ def run_ours(args):
         "e2e": {"value": ws * evals_step * args.steps / (ms_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 2 * 3 * n * 8, "d2h_bytes_per_step": 2 * 3 * n * 8},
         "gpu_launches": 13 * args.steps,
-        "roofline": {"bound": "fp32", "kernel": "k_force_f32c_pair", "achieved": force_flops / (force_ms / 1e3) / 1e12,
+        "roofline": {"bound": "fp32", "kernel": force_kernel, "achieved": force_flops / (force_ms / 1e3) / 1e12,
                      "peak": FP32_PEAK_NOMINAL / 1e12, "unit": "TFLOP/s",
                      "frac": force_flops / (force_ms / 1e3) / FP32_PEAK_NOMINAL, "traffic": traffic,
                      "peak_kind": "nominal FP32 (148 SMs x 128 lanes x FMA x 1965 MHz); no measured FP32 peak",
                      "launch_ms": force_ms, "flop_per_launch": force_flops},
-        "roofline_gather": {"bound": "hbm", "kernel": "k_gather_f32c",
+        "roofline_gather": {"bound": "hbm", "kernel": gather_kernel,
                             "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                             "frac": gather_bytes / (gather_ms / 1e3) / 1e9 / hbm_peak,
                             "peak_kind": peak_kind, "launch_ms": gather_ms, "bytes_per_launch": gather_bytes},
