@@ -922,12 +922,13 @@ constexpr int kRing = 12;  // coefficient slots a thread keeps in flight
 // through a shared-memory ring: each thread copies its own 16 bytes of each
 // contributor slot kRing slots ahead of the arithmetic (one commit group per
 // slot), so a warp keeps about 6 KB of the stream in flight without holding
-// it in registers, and the contributor ids come from the node's pattern
-// (L1-resident) without waiting on memory.  A thread reads back only what it
+// it in registers; the contributor ids come from the node's pattern
+// (L1-resident), and the contributors' trial displacements of the next group
+// of four are loaded while the current group is summed.  A thread reads back only what it
 // copied itself, after cp.async.wait_group, and refills a ring entry only
 // after the values read from it have been used.  Same FMAs in the same
 // contributor order as gather_group: the same result bit for bit.
-__global__ void __launch_bounds__(256) k_gather_f32c_ring(Dev d, const double* __restrict__ us) {
+__global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double* __restrict__ us) {
     __shared__ float4 ring[8][kRing][32];
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (tid >= d.n * 2) return;
@@ -951,29 +952,35 @@ __global__ void __launch_bounds__(256) k_gather_f32c_ring(Dev d, const double* _
         if (k < nc) cp_async16(r + 32 * k, cf + (int64_t)32 * k);
         cp_async_commit();
     }
+    // trial displacements of contributors k .. k+3, loaded one group ahead
+    double un[4][3];
+    auto load_group = [&](int k) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int m = (int)i + (k + u < nc ? __ldg(po + k + u) : 0);
+            un[u][0] = __ldg(us + m);
+            un[u][1] = __ldg(us + N + m);
+            un[u][2] = __ldg(us + 2 * N + m);
+        }
+    };
+    load_group(0);
     double a[4][3] = {};
     int e = 0;  // ring entry of contributor k
     for (int k = 0; k < nc; k += 4) {
+        double dd[4][3];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            dd[u][0] = un[u][0] - u0;
+            dd[u][1] = un[u][1] - u1;
+            dd[u][2] = un[u][2] - u2;
+        }
+        if (k + 4 < nc) load_group(k + 4);
         cp_async_wait<kRing - 4>();  // slots k .. k+3 have landed
-        int m[4];
         float4 cv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int eu = e + u < kRing ? e + u : e + u - kRing;
-            if (k + u < nc) {
-                cv[u] = r[32 * eu];
-                m[u] = (int)i + __ldg(po + k + u);
-            } else {
-                cv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                m[u] = (int)i;
-            }
-        }
-        double dd[4][3];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            dd[u][0] = __ldg(us + m[u]) - u0;
-            dd[u][1] = __ldg(us + N + m[u]) - u1;
-            dd[u][2] = __ldg(us + 2 * N + m[u]) - u2;
+            cv[u] = k + u < nc ? r[32 * eu] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {

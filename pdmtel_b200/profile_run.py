@@ -37,6 +37,7 @@ def main():
     ap.add_argument("--quad", action="store_true", help="plate: FP32 force with four nodes per thread")
     ap.add_argument("--order-tile", default=None, help="plate: node-order tile exponents bx,by,bz")
     ap.add_argument("--stencil", type=int, default=0, help="plate: lattice-stencil force, block shape 1..4")
+    ap.add_argument("--patterns", action="store_true", help="plate: FP32 gather from contributor patterns")
     a = ap.parse_args()
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     import pdmtel_b200 as P
@@ -63,6 +64,8 @@ def main():
             ctx.set_option(P.OPT_FORCE_QUAD, 1)
         if a.stencil:
             ctx.set_option(P.OPT_FORCE_STENCIL, a.stencil)
+        if a.patterns:
+            ctx.set_option(P.OPT_GATHER_STENCIL, 1)
         setup = time.time() - t0
         dt = 5e-9
         ctx.rk4_steps(dt, 0.0, a.warmup)
