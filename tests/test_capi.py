@@ -50,3 +50,26 @@ def test_null_context_is_rejected():
     assert L.pd_sync(None) == -1
     assert L.pd_rk4_steps(None, 1e-8, 0.0, 1) == -1
     assert L.pd_static_solve(None, 0.0, 0, 1e-10, 10, None, None, None) == -1
+
+
+def _header_text():
+    return re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "pdmtel_b200.h")).read(), flags=re.S)
+
+
+def test_option_constants_match_the_header():
+    """Every PD_OPT_* of the header has the same value in the Python layer."""
+    opts = {m.group(1): int(m.group(2)) for m in re.finditer(r"\bPD_OPT_(\w+)\s*=\s*(\d+)", _header_text())}
+    assert len(opts) >= 14
+    for name, v in opts.items():
+        assert getattr(P, "OPT_" + name) == v, name
+
+
+def test_tune_result_layout_matches_the_header():
+    """pd_tune_result: same fields, order and sizes in the header and ctypes."""
+    body = re.search(r"typedef struct pd_tune_result \{(.*?)\} pd_tune_result;", _header_text(), flags=re.S).group(1)
+    fields = []
+    for m in re.finditer(r"\b(int64_t|int32_t|double)\s+([\w\s,]+);", body):
+        for n in m.group(2).split(","):
+            fields.append((n.strip(), {"int64_t": 8, "int32_t": 4, "double": 8}[m.group(1)]))
+    py = [(n, C.sizeof(t)) for n, t in P.pd_tune_result._fields_]
+    assert fields == py
