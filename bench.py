@@ -608,7 +608,7 @@ def run_ours(args):
 
     # launch shapes for this plate (pd_autotune: tiles, gather variant; state restored)
     ctx.set_precision(P.PREC_FP32C)
-    tune = ctx.autotune(dt, 3)
+    tune = ctx.autotune(dt, 5)
     sampler = ClockSampler(dev)
     ms32, U32, V32, clocks = timed(P.PREC_FP32C, sampler)
     ms64, U64, V64, _ = timed(P.PREC_FP64)

@@ -2102,23 +2102,28 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
         if (!(best.ms < before)) c->d.gather_per_point = gp0;
         out->gather_per_point = c->d.gather_per_point;
         if (c->npt == 8 && !c->d.gather_per_point) {
-            // the SELL layout of the gather (rebuilt for every later order trial)
-            const int s0 = c->d.sell_on;
-            const double b2 = best.ms;
-            if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, !s0)) != PD_OK) return done(rc);
-            Trial T2{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
-            if ((rc = trial(T2)) != PD_OK) return done(rc);
-            if (!(best.ms < b2) && (rc = pd_set_option(c, PD_OPT_GATHER_SELL, s0)) != PD_OK) return done(rc);
-            out->gather_sell = c->d.sell_on;
+            // every combination of the SELL copy (rebuilt for every later order
+            // trial) and the contributor patterns (refused when nothing
+            // repeats); both together run the coefficient ring
+            const int s0 = c->d.sell_on, p0 = c->gpat_opt;
+            int ks = s0, kp = p0;
+            for (int sv = 0; sv <= 1; ++sv)
+                for (int pv = 0; pv <= 1; ++pv) {
+                    if (sv == s0 && pv == p0) continue;  // the shape timed so far
+                    if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, sv)) != PD_OK) return done(rc);
+                    if (pd_set_option(c, PD_OPT_GATHER_STENCIL, pv) != PD_OK) continue;
+                    const double prev = best.ms;
+                    Trial T2{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+                    if ((rc = trial(T2)) != PD_OK) return done(rc);
+                    if (best.ms < prev) {
+                        ks = sv;
+                        kp = pv;
+                    }
+                }
+            if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, ks)) != PD_OK) return done(rc);
+            if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, kp)) != PD_OK) return done(rc);
         }
-        // contributor patterns instead of lists (refused when nothing repeats)
-        const int p0 = c->gpat_opt;
-        if (!c->d.gather_per_point && pd_set_option(c, PD_OPT_GATHER_STENCIL, !p0) == PD_OK) {
-            const double b3 = best.ms;
-            Trial T3{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
-            if ((rc = trial(T3)) != PD_OK) return done(rc);
-            if (!(best.ms < b3) && (rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, p0)) != PD_OK) return done(rc);
-        }
+        out->gather_sell = c->d.sell_on;
         out->gather_stencil = c->gpat_opt;
     }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.multimat) {

@@ -476,3 +476,26 @@ def test_fp32c_pattern_gather_equals_list_gather(name):
     for pat, sell, reset in ((1, 0, False), (1, 1, False), (1, 1, True)):
         U1, V1 = run(pat, sell, reset)
         assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (pat, sell, reset)
+
+
+def test_autotune_on_a_box_lattice_changes_no_result(tmp_path):
+    """The tuner's trials on a plate (node orders, every gather variant, the
+    stencil force, the persistent launch) keep the state and leave a choice
+    whose trajectory equals the untuned one bit for bit."""
+    D.config_plate(dims=(48, 40, 4), spacing=5e-4, slit_half_length=3e-3, dt=5e-9, vel=5.0).write(str(tmp_path))
+    dt = 5e-9
+    U0, V0 = _fp32c_state(lambda: gpu_model(str(tmp_path)), dt, 12)
+    dm = gpu_model(str(tmp_path))
+    dm.SetPrecision(P.PREC_FP32C)
+    ctx = dm.context()
+    r = ctx.autotune(dt, 2)
+    assert r["trials"] >= 10
+    U1, V1 = ctx.get_state()
+    assert not U1.any() and not V1.any()
+    if r["persistent"]:
+        ctx.rk4_steps_persistent(dt, 0.0, 12)
+    else:
+        ctx.rk4_steps(dt, 0.0, 12)
+    ctx.sync()
+    U2, V2 = ctx.get_state()
+    assert np.array_equal(U0, U2) and np.array_equal(V0, V2), r
