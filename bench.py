@@ -559,6 +559,19 @@ def run_static(args):
     return 0
 
 
+def apply_shape(ctx, shape):
+    """Sets the launch-shape options a pd_autotune result names (for runs
+    whose timing must not depend on a tuner, e.g. under a profiler)."""
+    import pdmtel_b200 as P
+    opts = [("tile", P.OPT_TILE), ("gather_per_point", P.OPT_GATHER_PER_POINT), ("gather_sell", P.OPT_GATHER_SELL),
+            ("gather_stencil", P.OPT_GATHER_STENCIL), ("force_stencil", P.OPT_FORCE_STENCIL),
+            ("force_quad", P.OPT_FORCE_QUAD), ("force_tile", P.OPT_FORCE_TILE)]
+    for key, opt in opts:
+        if key in shape:
+            ctx.set_option(opt, int(shape[key]))
+    return dict(shape, applied=True)
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -606,9 +619,13 @@ def run_ours(args):
         U, V = ctx.get_state()
         return ms, U, V, clocks
 
-    # launch shapes for this plate (pd_autotune: tiles, gather variant; state restored)
+    # launch shapes for this plate (pd_autotune: node order, gather and force
+    # variants, persistent launch; state restored), or the shapes given
     ctx.set_precision(P.PREC_FP32C)
-    tune = ctx.autotune(dt, 5)
+    if args.shape:
+        tune = apply_shape(ctx, json.loads(args.shape))
+    else:
+        tune = ctx.autotune(dt, 5)
     sampler = ClockSampler(dev)
     ms32, U32, V32, clocks = timed(P.PREC_FP32C, sampler)
     ms64, U64, V64, _ = timed(P.PREC_FP64)
@@ -731,6 +748,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--shape", default=None,
+                    help="skip pd_autotune and apply these launch shapes, a JSON object with keys of its result "
+                         "(tile, gather_per_point, gather_sell, gather_stencil, force_stencil, force_quad, force_tile)")
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--form", default="precision", choices=["precision", "batch", "static", "identify", "accuracy"])
     ap.add_argument("--ident-dims", default="64x64x8")

@@ -84,6 +84,46 @@ __device__ __forceinline__ void bond4(const PointPack<8>& G, int q, const float*
     }
 }
 
+// bond4 for the two nodes of an x-adjacent pair: their bonds to one
+// neighbour share xi's y and z components, so x1 = xi_1 + h_y, x2 = xi_2 + h_z
+// and the inner term fmaf(x1, x1, x2 x2) of r2 are formed once per point
+// (X1, X2, T12) and bond4s adds only the pair-specific x0; the same values
+// as bond4 computes.
+__device__ __forceinline__ void pair_terms(const PointPack<8>& G, int q, float dx1, float dx2, float* X1, float* X2,
+                                           float* T12) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const PointF& P = G.p[q + k];
+        X1[k] = dx1 + P.hy;
+        X2[k] = dx2 + P.hz;
+        T12[k] = fmaf(X1[k], X1[k], X2[k] * X2[k]);
+    }
+}
+
+template <bool HASFAIL>
+__device__ __forceinline__ void bond4s(const PointPack<8>& G, int q, const float* u4, float dx0, const float* X1,
+                                       const float* X2, const float* T12, const float* du, float ecrit, float* F) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const PointF& P = G.p[q + k];
+        const float x0 = dx0 + P.hx, x1 = X1[k], x2 = X2[k];
+        const float e0 = du[0] + u4[k], e1 = du[1] + u4[4 + k], e2 = du[2] + u4[8 + k];
+        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
+        const float r2 = fmaf(x0, x0, T12[k]);
+        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
+        const float p2 = r2 + dd;
+        const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
+        const float r = __fmul_rn(r2, rinv);
+        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
+        const float beta = __saturatef((P.A - r) * P.B);
+        float fm = P.W * beta * s * pinv;
+        if (HASFAIL && dd > 0.f && s > ecrit) fm = 0.f;
+        F[0] = fmaf(fm, y0, F[0]);
+        F[1] = fmaf(fm, y1, F[1]);
+        F[2] = fmaf(fm, y2, F[2]);
+    }
+}
+
 struct Own {
     float uh[3], ul[3];  // displacement of the node, FP32 hi/lo
     float ph[3], pl[3];  // position hi/lo (off the lattice path)
@@ -455,9 +495,12 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
                 const float4 vx = __ldg(blk + (q >> 2) * N + j), vy = __ldg(blk + (2 + (q >> 2)) * N + j),
                              vz = __ldg(blk + (4 + (q >> 2)) * N + j);
                 const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
+                float X1[4], X2[4], T12[4];
+                pair_terms(G, q, dx[0][1], dx[0][2], X1, X2, T12);
 #pragma unroll
                 for (int side = 0; side < 2; ++side)
-                    if (has[side]) bond4<HASFAIL>(G, q, u4, dx[side], du[side], side == 0 ? A.e : B.e, F[side]);
+                    if (has[side])
+                        bond4s<HASFAIL>(G, q, u4, dx[side][0], X1, X2, T12, du[side], side == 0 ? A.e : B.e, F[side]);
             }
             if (has[0]) kahan_add(A, F[0], coef[0]);
             if (has[1]) kahan_add(B, F[1], coef[1]);
