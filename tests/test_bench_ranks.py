@@ -64,3 +64,25 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
 
     assert bench.run_reference_arm(A()) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_shape_option_sets_the_named_launch_shapes():
+    """bench --shape: every key of a tuner result it names becomes one
+    pd_set_option call with the matching option; other keys are ignored."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import pdmtel_b200 as P
+
+    class Ctx:
+        def __init__(self):
+            self.calls = []
+
+        def set_option(self, opt, v):
+            self.calls.append((opt, v))
+
+    c = Ctx()
+    out = bench.apply_shape(c, {"tile": 261, "gather_sell": 1, "gather_stencil": 1, "force_stencil": 3,
+                                "trials": 27})
+    assert sorted(c.calls) == sorted([(P.OPT_TILE, 261), (P.OPT_GATHER_SELL, 1), (P.OPT_GATHER_STENCIL, 1),
+                                      (P.OPT_FORCE_STENCIL, 3)])
+    assert out["applied"] and out["tile"] == 261
