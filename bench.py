@@ -46,6 +46,12 @@ errors at steps 100, 500 and 2000.
 --form static: the 128^3 cube (bottom clamped, 1 MPa shear traction on top),
 CG to relative residual 1e-10: FP32 matvec inside FP64 iterative refinement
 against plain FP64 CG; time to solution and the difference of the solutions.
+(--cube N changes the cube, --maxit caps the CG iterations.)
+
+--form steps: W + K device-resident RK4 steps of the plate (--plate-dims,
+--prec, launch shapes from --shape or the tuner) and nothing else: the run
+profiler captures are taken on.  --form adjoint: the adjoint pair alone on the
+identification specimen (--adjoint-steps).
 
 Multi-GPU: replicas (one full plate per rank, no data-path collective);
 weak scaling; time = max over ranks of the device-timed region.
@@ -69,8 +75,27 @@ METRIC = "bond-force evals/s on 1 B200: FP32-comp vs FP64 at ≤1e-6 rel err; ad
 UNIT = "bond-force evals/s"
 PLATE = dict(dims=(400, 400, 4), spacing=5e-4, slit_half_length=0.02, vel=0.05, dt=5e-9)
 SUBPLATE = dict(dims=(40, 40, 4), spacing=5e-4, slit_half_length=0.004, vel=0.05, dt=5e-9)
-FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9  # FP32 lanes x FMA x max SM clock
+FP32_LANES_PER_SM = 128  # sm_100: 4 SM sub-partitions x 32 FP32 lanes
 FLOP_PER_EVAL = 22
+
+
+def fp32_peak(sm_max_mhz):
+    """Nominal FP32 rate of the device: SMs (from the device) x FP32 lanes x
+    2 (FMA) x the maximum SM clock nvidia-smi reports (1965 MHz on B200 when
+    nvidia-smi is unavailable)."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = sm_max_mhz or 1965.0
+    return sms * FP32_LANES_PER_SM * 2 * mhz * 1e6, sms, mhz
+
+
+def plate_cfg(dims_text):
+    """The plate workload at other dimensions (for profiler captures): the
+    slit keeps a tenth of the plate width on each side of the centre."""
+    dims = tuple(int(v) for v in dims_text.split("x"))
+    cfg = dict(PLATE, dims=dims)
+    cfg["slit_half_length"] = 0.1 * dims[0] * PLATE["spacing"]
+    return cfg
 
 
 def dist_env():
@@ -522,7 +547,7 @@ def run_static(args):
     from pdmtel_b200 import decks as D
     torch.cuda.set_device(0)
     tmp = tempfile.mkdtemp(prefix="pdstatic_")
-    D.config_cube(n=128, intg_point=1).write(tmp)
+    D.config_cube(n=args.cube, intg_point=1).write(tmp)
     t0 = time.time()
     dm = P.pdDataManager(tmp)
     dm.InitNode()
@@ -537,24 +562,73 @@ def run_static(args):
     for name, prec in (("fp64", P.PREC_FP64), ("fp32c", P.PREC_FP32C)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        x, it, rr = ctx.static_solve(1.0, precision=prec, rtol=1e-10)
+        try:
+            x, it, rr = ctx.static_solve(1.0, precision=prec, rtol=1e-10, maxit=args.maxit)
+        except P.PdError:
+            if args.maxit >= 100000:
+                raise
+            x, it, rr = np.zeros(3 * ctx.n), args.maxit, float("nan")  # capped on purpose
         e1.record(stream)
         e1.synchronize()
         res[name] = {"s": e0.elapsed_time(e1) / 1e3, "iterations": it, "rel_residual": rr, "x": x}
     err = float(np.linalg.norm(res["fp32c"]["x"] - res["fp64"]["x"]) / np.linalg.norm(res["fp64"]["x"]))
     for r in res.values():
         r.pop("x")
-    line = {"metric": "static solve time to relative residual 1e-10, 128^3 cube", "value": res["fp32c"]["s"],
+    line = {"metric": f"static solve time to relative residual 1e-10, {args.cube}^3 cube", "value": res["fp32c"]["s"],
             "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * res["fp32c"]["s"],
             "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "cube 128^3, bottom clamped, 1 MPa shear traction on top",
+            "config": {"workload": f"cube {args.cube}^3, bottom clamped, 1 MPa shear traction on top",
                        "nodes": I.num_nodes, "bond_halves": I.num_halves,
                        "operator": "lattice stencil" if stencil else "family lists"},
             "fp32_ir": res["fp32c"], "fp64_cg": res["fp64"], "speedup_fp32ir_over_fp64": res["fp64"]["s"] / res["fp32c"]["s"],
             "rel_diff_fp32ir_vs_fp64": err, "setup_s": setup_s}
     print(json.dumps(line))
     dm.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def run_steps(args):
+    """--form steps: device-resident RK4 steps of the plate and nothing else
+    (the command profiler captures are taken on)."""
+    import torch
+    import pdmtel_b200 as P
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp(prefix="pdsteps_")
+    cfg = plate_cfg(args.plate_dims)
+    dm, ctx, setup_s = setup_plate(tmp, cfg)
+    prec = {"fp32c": P.PREC_FP32C, "fp64": P.PREC_FP64}[args.prec]
+    ctx.set_precision(prec)
+    tune = apply_shape(ctx, json.loads(args.shape)) if args.shape else (
+        ctx.autotune(cfg["dt"], 5) if prec == P.PREC_FP32C else {})
+    dt = cfg["dt"]
+    ctx.reset_state()
+    ctx.rk4_steps(dt, 0.0, args.warmup)
+    ctx.sync()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.rk4_steps(dt, args.warmup * dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ev = 4 * ctx.evals_per_stage()
+    print(json.dumps({"form": "steps", "workload": "plate {}x{}x{}".format(*cfg["dims"]), "prec": args.prec,
+                      "nodes": ctx.n, "ms_per_step": ms / args.steps, "value": ev * args.steps / (ms / 1e3),
+                      "unit": UNIT, "shape": tune, "setup_s": setup_s}))
+    dm.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def run_adjoint(args):
+    """--form adjoint: the adjoint pair alone (profiler captures)."""
+    import torch
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp(prefix="pdadj_")
+    res = adjoint_leg(tmp, args.adjoint_steps)
+    print(json.dumps({"form": "adjoint", **res}))
     shutil.rmtree(tmp, ignore_errors=True)
     return 0
 
@@ -586,7 +660,7 @@ def run_ours(args):
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     tmp = tempfile.mkdtemp(prefix=f"pdbench{rank}_")
-    cfg = PLATE
+    cfg = plate_cfg(args.plate_dims)
     dm, ctx, setup_s = setup_plate(tmp, cfg)
     dt = cfg["dt"]
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -669,6 +743,7 @@ def run_ours(args):
 
     I = dm.info()
     hbm_peak, peak_kind = load_peaks()
+    peak32, sms, mhz = fp32_peak((clocks or {}).get("sm_max_mhz"))
     force_ms = prof[0] / 4.0  # one launch per stage
     gather_ms = prof[1] / 4.0
     npt = I.num_gauss
@@ -694,7 +769,8 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "plate 400x400x4, 2x2x2 Gauss+MLS, 40 mm slit, +-0.05 m/s, dt 5e-9",
+        "config": {"workload": "plate {}x{}x{}, 2x2x2 Gauss+MLS, {:g} mm slit, +-0.05 m/s, dt 5e-9".format(
+                       *cfg["dims"], 2e3 * cfg["slit_half_length"]),
                    "nodes": n, "bond_halves": I.num_halves, "broken_halves": I.num_broken,
                    "evals_per_step": evals_step, "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (MLS coefficients and family lists are GBs per step)",
@@ -706,9 +782,10 @@ def run_ours(args):
                 "h2d_bytes_per_step": 2 * 3 * n * 8, "d2h_bytes_per_step": 2 * 3 * n * 8},
         "gpu_launches": 13 * args.steps,
         "roofline": {"bound": "fp32", "kernel": force_kernel, "achieved": force_flops / (force_ms / 1e3) / 1e12,
-                     "peak": FP32_PEAK_NOMINAL / 1e12, "unit": "TFLOP/s",
-                     "frac": force_flops / (force_ms / 1e3) / FP32_PEAK_NOMINAL, "traffic": traffic,
-                     "peak_kind": "nominal FP32 (148 SMs x 128 lanes x FMA x 1965 MHz); no measured FP32 peak",
+                     "peak": peak32 / 1e12, "unit": "TFLOP/s",
+                     "frac": force_flops / (force_ms / 1e3) / peak32, "traffic": traffic,
+                     "peak_kind": f"nominal FP32 ({sms} SMs x {FP32_LANES_PER_SM} lanes x FMA x {mhz:.0f} MHz, "
+                                  "the maximum SM clock); no measured FP32 peak",
                      "launch_ms": force_ms, "flop_per_launch": force_flops},
         "roofline_gather": {"bound": "hbm", "kernel": gather_kernel,
                             "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
@@ -752,7 +829,12 @@ def main():
                     help="skip pd_autotune and apply these launch shapes, a JSON object with keys of its result "
                          "(tile, gather_per_point, gather_sell, gather_stencil, force_stencil, force_quad, force_tile)")
     ap.add_argument("--adjoint-steps", type=int, default=100)
-    ap.add_argument("--form", default="precision", choices=["precision", "batch", "static", "identify", "accuracy"])
+    ap.add_argument("--form", default="precision",
+                    choices=["precision", "batch", "static", "identify", "accuracy", "steps", "adjoint"])
+    ap.add_argument("--plate-dims", default="400x400x4", help="plate lattice of the precision/steps forms")
+    ap.add_argument("--prec", default="fp32c", choices=["fp32c", "fp64"], help="arithmetic of --form steps")
+    ap.add_argument("--cube", type=int, default=128, help="cube side of --form static")
+    ap.add_argument("--maxit", type=int, default=100000, help="CG iteration cap of --form static")
     ap.add_argument("--ident-dims", default="64x64x8")
     ap.add_argument("--ident-steps", type=int, default=1000)
     ap.add_argument("--fd-dirs", type=int, default=32)
@@ -770,6 +852,10 @@ def main():
         return run_identify(args)
     if args.form == "accuracy":
         return run_accuracy(args)
+    if args.form == "steps":
+        return run_steps(args)
+    if args.form == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

@@ -136,7 +136,10 @@ int pd_set_precision(pd_ctx* ctx, int precision);
 int pd_set_energy(pd_ctx* ctx, int on);
 
 /* Nodal state U and V ([3N] each; either may be NULL).  Setting the state
- * also sets the velocity buffer to V (InitDynamicSolve). */
+ * also sets the velocity buffer to V (InitDynamicSolve).  Like the
+ * reference's pdNode::SetU1..3, it leaves the Gauss-point displacements
+ * alone: the next step's first stage reads the ones the last gather derived.
+ * Call pd_gather(ctx, t, NULL) to derive them from the new U. */
 int pd_set_state(pd_ctx* ctx, const double* U, const double* V);
 int pd_get_state(pd_ctx* ctx, double* U, double* V);
 int pd_get_vbuf(pd_ctx* ctx, double* vbuf);
@@ -165,7 +168,11 @@ int pd_rk4_step(pd_ctx* ctx, double dt, double time, double* ke, double* ee);
  * steps are captured once into a CUDA graph and replayed. */
 int pd_rk4_steps(pd_ctx* ctx, double dt, double t0, int nsteps);
 /* The same through host buffers: U,V in [3N] are uploaded, nsteps run and
- * the new state written to U_out,V_out. */
+ * the new state written to U_out,V_out.  When U_in differs from the device's
+ * displacement, the Gauss-point displacements are first derived from U_in at
+ * t0 (pd_gather), so the steps continue from U_in exactly as from a state the
+ * device reached by stepping; when it is the same (a round trip of the
+ * previous call's output), nothing is recomputed. */
 int pd_rk4_steps_host(pd_ctx* ctx, double dt, double t0, int nsteps, const double* U_in, const double* V_in,
                       double* U_out, double* V_out);
 /* number of Gauss-point force evaluations of one RK4 stage (unbroken
@@ -201,7 +208,12 @@ int pd_profile_step(pd_ctx* ctx, double dt, double time, double* ms);
  * broken (broken may be NULL): device, [capacity]; when the family is larger
  * than capacity the call returns PD_ERR_CAPACITY after writing row_ptr and
  * *num_halves, so the caller can size col and call again.  slits: host,
- * [num_slits][6].  stream: a cudaStream_t or NULL; the call synchronises it.
+ * [num_slits][6].  stream: a cudaStream_t or NULL.  The call waits for its
+ * stream several times (it reads the bounding box, the family size and the
+ * longest family back to the host between its launches) and returns with the
+ * stream idle.  A non-finite coordinate returns PD_ERR_ARG; the cell count is
+ * checked axis by axis, so a horizon tiny next to the extent returns
+ * PD_ERR_CAPACITY instead of overflowing.
  *
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call

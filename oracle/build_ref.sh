@@ -3,7 +3,7 @@
 # into oracle/_ref/ (git-ignored).  The result is test infrastructure only: the
 # reference harness that produces golden vectors and the timed CPU baseline.
 #
-#   sh oracle/build_ref.sh [REFERENCE_DIR]
+#   sh oracle/build_ref.sh REFERENCE_DIR     (or PDMTEL_REFERENCE=REFERENCE_DIR)
 #
 # The shipped reference does not compile as-is under g++ 13; three minimal
 # patches are applied to a scratch copy under oracle/_ref/src (never committed):
@@ -15,7 +15,11 @@
 # pdBCTract.cpp / pdBCVelocTime.cpp and debug_new.cpp are not compiled.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-${PDMTEL_REFERENCE:-/root/reference}}
+REF=${1:-${PDMTEL_REFERENCE:-}}
+if [ -z "$REF" ]; then
+    echo "build_ref.sh: give the reference source folder as the first argument or PDMTEL_REFERENCE" >&2
+    exit 2
+fi
 OUT="$HERE/_ref"
 if [ ! -f "$REF/pdDataManager.cpp" ]; then
     echo "build_ref.sh: reference sources not found at $REF" >&2

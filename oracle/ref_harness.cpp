@@ -16,6 +16,14 @@
 //   pdref_harness force <dir> <out.bin> <t> <dt_stage>
 //   pdref_harness traj  <dir> <out.bin> <nsteps> <dump_every>
 //   pdref_harness time  <dir> <nsteps>
+//   pdref_harness damp  <dir> <out.bin> <dt>
+//
+// damp: the reference's matrix-free linearised stiffness pass,
+// pdDataManager::CalcDampingCoeff (pdDataManager2.cpp:1616-1907), at three
+// displacement fields: the per-dof sum of |K_ij| (absKVector, returned scaled
+// by dt^2/4) and the damping coefficient 2 sqrt(u.Ku / u.Mu) of each field.
+// These pin the static operator of pdSolve::AssembleEquation
+// (pdSolve.cpp:195-527), whose coefficients are the same.
 //
 // <dir>/pds_input.txt is the deck.  An optional slit block
 //   number_of_slits / k   and   slit_i / 1 x1lo x1hi x2lo x2hi x3lo x3hi
@@ -35,6 +43,7 @@
 #define protected public
 #include "pdDataManager.h"
 #include "pdSolve.h"
+#include "pdVector.h"
 #undef private
 #undef protected
 
@@ -364,6 +373,36 @@ int main(int argc, char** argv) {
         w.d("ke", ke);
         w.d("ee", ee);
         w.d("times", times);
+    } else if (mode == "damp") {
+        double dt = std::atof(argv[4]);
+        setup(dat, dir);
+        Writer w(argv[3]);
+        dump_setup(dat, w);
+        const int N = dat.GetNumNode();
+        std::vector<double> u, v;
+        test_fields(dat, u, v);
+        std::vector<double> damp;
+        for (int f = 0; f < 3; ++f) {
+            // field 0: the smooth test field; 1: the test velocity field used
+            // as a displacement; 2: their sum with a node-wise alternating sign
+            std::vector<double> uf(3 * (size_t)N);
+            for (int i = 0; i < 3 * N; ++i)
+                uf[i] = f == 0 ? u[i] : f == 1 ? 1e-3 * v[i] : u[i] + ((i / 3) % 2 ? -1e-3 : 1e-3) * v[i];
+            for (int i = 0; i < N; ++i) {
+                pdNode* n = dat.GetNode(i);
+                n->SetU1(uf[3 * i]); n->SetU2(uf[3 * i + 1]); n->SetU3(uf[3 * i + 2]);
+            }
+            pdVector absK(3 * N);
+            damp.push_back(dat.CalcDampingCoeff(dt, &absK));
+            w.d("u_field_" + std::to_string(f), uf);
+            if (f == 0) {
+                std::vector<double> a(3 * (size_t)N);
+                for (int i = 0; i < 3 * N; ++i) a[i] = absK.GetCoeff(i);
+                w.d("absK", a);
+            }
+        }
+        w.d("damp_coeff", damp);
+        w.d1("damp_dt", dt);
     } else if (mode == "time") {
         int nsteps = std::atoi(argv[3]);
         double t0 = now();

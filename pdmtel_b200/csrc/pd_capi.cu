@@ -109,6 +109,7 @@ struct pd_ctx {
     float *coeff32 = nullptr, *csum = nullptr;
     double* hstage = nullptr;  // pinned host staging, 3N doubles x 2
     double* hscalar = nullptr; // pinned host scalars
+    int* dflag = nullptr;      // device flags (pd_rk4_steps_host: the uploaded U differs)
     // CUDA graph of one RK4 step
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;
@@ -380,6 +381,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     double* bdry = nullptr;
     int rc = PD_OK;
     if ((rc = dalloc(c, &c->scratch, n3 * 2)) != PD_OK) return bail(rc);
+    if ((rc = dalloc(c, &c->dflag, 4)) != PD_OK) return bail(rc);
     if ((rc = dalloc(c, &x, n3)) != PD_OK) return bail(rc);
     if ((rc = dalloc(c, &mat, N)) != PD_OK) return bail(rc);
     if ((rc = dalloc(c, &bc, N)) != PD_OK) return bail(rc);
@@ -1275,10 +1277,27 @@ int pd_rk4_steps(pd_ctx* c, double dt, double t0, int nsteps) {
 int pd_rk4_steps_host(pd_ctx* c, double dt, double t0, int nsteps, const double* U_in, const double* V_in,
                       double* U_out, double* V_out) {
     if (!c) return fail(PD_ERR_ARG, "pd_rk4_steps_host: null context");
+    if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_rk4_steps_host: family/MLS data not set");
     const size_t b3 = sizeof(double) * 3 * c->n;
-    if (U_in) {
+    if (U_in && c->n > 0) {
+        // The first stage reads the Gauss-point displacements (and, in FP32C,
+        // the node blocks) that the previous step's closing gather derived
+        // from the device's U.  When the uploaded U differs from that U, they
+        // are derived again from U_in at t0 (CalcIntgPointDisplRK4,
+        // pdDataManager.cpp:2402-2495), so the steps start from U_in
+        // throughout; a round trip of the device state skips the gather.
+        PD_CUDA_TRY(cudaMemsetAsync(c->dflag, 0, sizeof(int), c->stream));
         PD_CUDA_TRY(cudaMemcpyAsync(c->scratch, U_in, b3, cudaMemcpyHostToDevice, c->stream));
-        pd::launch_to_soa(c->scratch, c->d.U, c->n, 3, c->stream);
+        pd::launch_to_soa_changed(c->scratch, c->d.U, c->n, 3, c->dflag, c->stream);
+        int* hflag = reinterpret_cast<int*>(c->hscalar + 12);
+        PD_CUDA_TRY(cudaMemcpyAsync(hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (*hflag) {
+            PD_TRY(set_time(c, t0));
+            if (c->precision == PD_PREC_FP32C) pd::launch_gather_f32c(c->d, c->d.U, c->stream);
+            else pd::launch_gather_f64(c->d, c->d.U, c->stream);
+            PD_CUDA_TRY(cudaGetLastError());
+        }
     }
     if (V_in) {
         PD_CUDA_TRY(cudaMemcpyAsync(c->scratch + 3 * c->n, V_in, b3, cudaMemcpyHostToDevice, c->stream));

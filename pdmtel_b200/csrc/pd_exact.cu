@@ -370,6 +370,19 @@ __global__ void k_to_soa(const double* __restrict__ aos, double* __restrict__ so
     soa[c * n + i] = aos[t];
 }
 
+// k_to_soa that also records whether any value changed (bit pattern), so a
+// caller can tell a round trip of the device state from a new state
+__global__ void k_to_soa_changed(const double* __restrict__ aos, double* __restrict__ soa, int64_t n, int comps,
+                                 int* __restrict__ changed) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n * comps) return;
+    const int64_t i = t / comps;
+    const int c = (int)(t - i * comps);
+    const double v = aos[t];
+    if (__double_as_longlong(soa[c * n + i]) != __double_as_longlong(v)) *changed = 1;
+    soa[c * n + i] = v;
+}
+
 __global__ void k_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int64_t n, int comps) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= n * comps) return;
@@ -449,6 +462,11 @@ void launch_energy_reduce(const Dev& d, cudaStream_t s) {
 void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s) {
     if (n == 0) return;
     k_to_soa<<<blocks_for(n * comps, 256), 256, 0, s>>>(aos, soa, n, comps);
+}
+
+void launch_to_soa_changed(const double* aos, double* soa, int64_t n, int comps, int* changed, cudaStream_t s) {
+    if (n == 0) return;
+    k_to_soa_changed<<<blocks_for(n * comps, 256), 256, 0, s>>>(aos, soa, n, comps, changed);
 }
 
 void launch_to_aos(const double* soa, double* aos, int64_t n, int comps, cudaStream_t s) {
@@ -854,12 +872,18 @@ __device__ __forceinline__ double* na_scal(unsigned char* s) { return (double*)(
 // bounding box of the nodes into scal[0..5]; one block
 __global__ void k_na_bbox(const double* __restrict__ x, int64_t n, unsigned char* s) {
     __shared__ double red[6][32];
+    __shared__ int nonfinite;
+    if (threadIdx.x == 0) nonfinite = 0;
+    __syncthreads();
     double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    bool bad = false;
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
         for (int a = 0; a < 3; ++a) {
+            bad = bad || !isfinite(x[3 * i + a]);
             lo[a] = dmin(lo[a], x[3 * i + a]);
             hi[a] = -dmin(-hi[a], -x[3 * i + a]);
         }
+    if (bad) nonfinite = 1;
     for (int o = 16; o > 0; o >>= 1)
         for (int a = 0; a < 3; ++a) {
             lo[a] = dmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
@@ -880,7 +904,7 @@ __global__ void k_na_bbox(const double* __restrict__ x, int64_t n, unsigned char
                 l = dmin(l, red[a][k]);
                 h = -dmin(-h, -red[3 + a][k]);
             }
-            sc[a] = l;
+            sc[a] = nonfinite ? __longlong_as_double(0x7ff8000000000000LL) : l;  // a non-finite coordinate is reported as a NaN box
             sc[3 + a] = h;
         }
         ((unsigned long long*)sc)[6] = (unsigned long long)__double_as_longlong(0.0);
@@ -1061,13 +1085,23 @@ extern "C" int pd_bond_search_noalloc(const double* coords, int64_t n, double gr
     A.s = s;
     A.nslit = num_slits;
     A.g.h = horizon + grid_spacing;
+    // Cells per axis are counted in double and checked against the array's
+    // limit before any conversion to an integer: a non-finite coordinate or a
+    // horizon tiny next to the extent must not reach an undefined cast or an
+    // overflowing product.
     int64_t ncell = 1;
     for (int a = 0; a < 3; ++a) {
+        if (!std::isfinite(bb[a]) || !std::isfinite(bb[3 + a]))
+            return fail(PD_ERR_ARG, "pd_bond_search_noalloc: non-finite coordinate");
+        const double cells = std::floor((bb[3 + a] - bb[a]) / A.g.h) + 1.0;
+        if (!(cells >= 1.0) || cells > (double)na::kCells)
+            return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: more cells than PD_NOALLOC_MAX_CELLS");
         A.g.lo[a] = bb[a];
-        A.g.nc[a] = (int64_t)std::floor((bb[3 + a] - bb[a]) / A.g.h) + 1;
-        ncell *= A.g.nc[a];
+        A.g.nc[a] = (int64_t)cells;
+        ncell *= A.g.nc[a];  // each factor <= kCells and the partial product too: no overflow
+        if (ncell > na::kCells)
+            return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: more cells than PD_NOALLOC_MAX_CELLS");
     }
-    if (ncell > na::kCells) return fail(PD_ERR_CAPACITY, "pd_bond_search_noalloc: more cells than PD_NOALLOC_MAX_CELLS");
     // the regions read before they are written start at zero
     PD_CUDA_TRY(cudaMemsetAsync(s + na::kOffCellCnt, 0, sizeof(int64_t) * (ncell + 1), st));
     PD_CUDA_TRY(cudaMemsetAsync(s + na::kOffFill, 0, sizeof(int64_t) * (ncell + 1), st));

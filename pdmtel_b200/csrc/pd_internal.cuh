@@ -146,6 +146,7 @@ void launch_epilogue(const Dev& d, int stage, double dts, double dt, cudaStream_
 void launch_advance_time(double* t, double dt, cudaStream_t s);
 void launch_energy_reduce(const Dev& d, cudaStream_t s);
 void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s);
+void launch_to_soa_changed(const double* aos, double* soa, int64_t n, int comps, int* changed, cudaStream_t s);
 void launch_to_aos(const double* soa, double* aos, int64_t n, int comps, cudaStream_t s);
 void launch_fill(double* p, double v, int64_t n, cudaStream_t s);
 

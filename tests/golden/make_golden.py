@@ -1,7 +1,10 @@
 """Generates the golden fixtures of tests/golden/ from the reference itself.
 
-    make -C oracle            # builds oracle/_ref/pdref_harness from the reference sources
-    python tests/golden/make_golden.py
+    make -C oracle REF=<reference dir>   # builds oracle/_ref/pdref_harness
+    python tests/golden/make_golden.py           # the small decks, tests/golden/*.npz
+    python tests/golden/make_golden.py --kat     # known answers of larger decks, kat.json
+    python tests/golden/make_golden.py --long    # the 20x10x10 bar over 100 steps, long/*.npz
+    python tests/golden/make_golden.py --static  # the linearised stiffness pass, static/*.npz
 
 Each case is a small synthetic deck written by pdmtel_b200.decks into
 tests/golden/decks/<case>/pds_input.txt; the reference harness
@@ -11,10 +14,12 @@ state is stored as tests/golden/<case>.npz.  The fixtures are what the oracle
 and the CUDA path are pinned against; nothing at test time needs the
 reference sources.
 """
+import hashlib
 import os
 import shutil
 import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
@@ -79,8 +84,7 @@ def run(mode, workdir, out, *args):
 def main():
     if not os.path.exists(HARNESS):
         raise SystemExit("oracle/_ref/pdref_harness missing: run `make -C oracle` first")
-    tmp = os.path.join(ROOT, "_work", "golden_tmp")
-    os.makedirs(tmp, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix="pdgolden_")
     for name, (deck, spec) in cases().items():
         ddir = os.path.join(HERE, "decks", name)
         deck.write(ddir)
@@ -100,9 +104,10 @@ def main():
         data["force_args"] = np.array([t, dts])
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
         print(name, int(data["n"][0]), "nodes", len(data["fam_col"]), "halves")
+    shutil.rmtree(tmp, ignore_errors=True)
 
 
-if __name__ == "__main__" and "--kat" not in sys.argv:
+if __name__ == "__main__" and not {"--kat", "--long", "--static"} & set(sys.argv):
     main()
 
 
@@ -124,7 +129,7 @@ def make_kat():
     """Known answers of larger decks: bond counts and energies of the first
     steps, from the reference harness."""
     import json
-    tmp = os.path.join(ROOT, "_work", "golden_tmp")
+    tmp = tempfile.mkdtemp(prefix="pdgolden_")
     kat = {}
     wd = os.path.join(tmp, "sample_like")
     sample_like_deck().write(wd)
@@ -143,7 +148,160 @@ def make_kat():
     with open(os.path.join(HERE, "kat.json"), "w") as f:
         json.dump(kat, f, indent=1)
     print(kat)
+    shutil.rmtree(tmp, ignore_errors=True)
 
 
 if __name__ == "__main__" and "--kat" in sys.argv:
     make_kat()
+
+
+# ---- the 20x10x10 bar over 100 RK4 steps (tests/golden/long/) ----
+#
+# The plain-FP64 config: 20x10x10 nodes, spacing 1 mm, horizon 3.015 mm, FGI
+# 2x2x2 points with MLS, dt 1e-8 s, 100 steps from rest, with the boundary-
+# effect factor off and on.  The reference applies no traction load (type 4 is
+# parsed and never used, pdDataManager.cpp:2534-2592), so the right face is
+# pulled with a velocity condition instead; the left face is fixed.  These
+# decks hold full 250-node families and, with bdryEff on, nodes of all three
+# branches of InitBdryEffectFactor (full family, one face, several faces,
+# pdDataManager.cpp:1412-1461).
+#
+# Arrays that are compared bit for bit are stored as SHA-256 digests of their
+# little-endian bytes (family lists, contributor lists, MLS coefficients,
+# Gauss-point displacements); the state every 10 steps is stored as digests,
+# and in full at steps 10, 50 and 100 together with the boundary-effect
+# factors, the stage-1 k vector at a non-trivial displacement and the
+# energies of every step, so that a mismatch can be measured.
+
+LONG_STEPS = 100
+LONG_EVERY = 10
+LONG_FULL = (10, 50, 100)
+
+
+def digest(a):
+    a = np.ascontiguousarray(a)
+    return hashlib.sha256(a.astype(a.dtype.newbyteorder("<")).tobytes()).hexdigest()
+
+
+def long_cases():
+    return {f"bar20_bE{b}": D.config_bar(dims=(20, 10, 10), spacing=1e-3, traction_as_veloc=0.05, dt=1e-8,
+                                         steps=LONG_STEPS, bdry_eff=b) for b in (0, 1)}
+
+
+def sample_nodes(n, dims):
+    """Nodes whose MLS coefficients are stored in full: a corner, an edge, a
+    face and interior nodes, and a seeded handful of others."""
+    nx, ny, nz = dims
+    pick = lambda x, y, z: x + nx * (y + ny * z)
+    fixed = [pick(0, 0, 0), pick(10, 0, 0), pick(10, 5, 0), pick(10, 5, 5), pick(19, 9, 9), pick(3, 4, 5),
+             pick(16, 5, 4), pick(1, 1, 1)]
+    rng = np.random.default_rng(20)
+    return np.unique(np.concatenate([fixed, rng.choice(n, 24, replace=False)])).astype(np.int64)
+
+
+def make_long():
+    out_dir = os.path.join(HERE, "long")
+    os.makedirs(out_dir, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix="pdgolden_long_")
+    for name, deck in long_cases().items():
+        ddir = os.path.join(out_dir, "decks", name)
+        deck.write(ddir)
+        wd = os.path.join(tmp, name)
+        os.makedirs(wd, exist_ok=True)
+        shutil.copy(os.path.join(ddir, "pds_input.txt"), os.path.join(wd, "pds_input.txt"))
+        t, dts = 2e-8, 1e-8
+        run("force", wd, os.path.join(wd, "force.bin"), t, dts)
+        f = read_pdb(os.path.join(wd, "force.bin"))
+        n = int(f["n"][0])
+        npt = int(f["num_gauss"][0])
+        keep = sample_nodes(n, deck.dims)
+        cb_ptr = f["cb_ptr"]
+        co = f["coeff"]
+        samples = []
+        for i in keep:
+            b, e = cb_ptr[i], cb_ptr[i + 1]
+            samples.append(co[b * npt:e * npt])
+        data = {
+            "n": f["n"], "dims": np.array(deck.dims, dtype=np.int64), "num_bonds": f["num_bonds"],
+            "min_bond": f["min_bond"], "dt": f["dt"], "params": f["params"], "iparams": f["iparams"],
+            **{k: f[k] for k in ("mat", "bc", "spring", "mat_ymod", "mat_density", "mat_ecrit", "mat_grav", "bc_type",
+                                 "bc_dir", "bc_val", "bc_end", "bc_load", "gw")},
+            "fam_ptr": f["fam_ptr"], "bdry_eff": f["bdry_eff"], "cb_ptr": cb_ptr,
+            "sha_fam_col": np.array(digest(f["fam_col"])), "sha_broken": np.array(digest(f["broken"])),
+            "sha_cb_idx": np.array(digest(f["cb_idx"])), "sha_coeff": np.array(digest(co)),
+            "sha_gauss_x": np.array(digest(f["gauss_x"])),
+            "coeff_nodes": keep, "coeff_samples": np.concatenate(samples),
+            "force_args": np.array([t, dts]), "u_test": f["u_test"], "v_test": f["v_test"],
+            "k": f["k"], "vbuf": f["vbuf"], "eed": f["eed"],
+            "sha_ug_force": np.array(digest(f["ug"])),
+        }
+        if "num_max_family" in f:
+            data["num_max_family"] = f["num_max_family"]
+        run("traj", wd, os.path.join(wd, "traj.bin"), LONG_STEPS, LONG_EVERY)
+        tr = read_pdb(os.path.join(wd, "traj.bin"))
+        for s in range(LONG_EVERY, LONG_STEPS + 1, LONG_EVERY):
+            for q in ("U", "V", "ug"):
+                data[f"sha_{q}_{s}"] = np.array(digest(tr[f"{q}_{s}"]))
+            if s in LONG_FULL:
+                data[f"U_{s}"] = tr[f"U_{s}"]
+                data[f"V_{s}"] = tr[f"V_{s}"]
+        data["ke"], data["ee"], data["times"] = tr["ke"], tr["ee"], tr["times"]
+        np.savez_compressed(os.path.join(out_dir, name + ".npz"), **data)
+        print(name, n, "nodes", int(f["num_bonds"][0]), "bonds", "max family", int(np.diff(f["fam_ptr"]).max()))
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__" and "--long" in sys.argv:
+    make_long()
+
+
+# ---- the linearised stiffness operator (tests/golden/static/) ----
+#
+# pdDataManager::CalcDampingCoeff (pdDataManager2.cpp:1616-1907) forms K u
+# matrix-free with the coefficients of pdSolve::AssembleEquation (pdSolve.cpp:
+# 195-527) and returns the per-dof sum of |K_ij| (times dt^2/4) and
+# 2 sqrt(u.Ku / u.Mu).  The decks carry no boundary condition and no slit, so
+# that K is the unconstrained operator of the whole family: two materials (the
+# min spring rule), Gauss-point and CCI decks, and a deletion hole.  dt = 2
+# makes the dt^2/4 scale exactly 1.
+
+STATIC_DT = 2.0
+
+
+def static_cases():
+    h = 1e-3
+    out = {}
+    dims = (8, 5, 4)
+    out["static_bar"] = D.Deck(dims=dims, spacing=h, horizon=3.015 * h, total_time=1.0, total_step=10,
+                               fixed_dt=1e-8, intg_point=1)
+    dims = (7, 6, 4)
+    out["static_cci"] = D.Deck(dims=dims, spacing=2.0, horizon=6.0, total_time=1.0, total_step=10, fixed_dt=1e-3,
+                               materials=[(1.0e5, 1e14, 6e10, 2e-6)], cci=(1, 0))
+    dims = (9, 7, 3)
+    out["static_hole"] = D.Deck(dims=dims, spacing=h, horizon=3.015 * h, total_time=1.0, total_step=10,
+                                fixed_dt=1e-8, intg_point=1,
+                                deletion_spaces=[D.Space(0, (1.6e-3, 0.0, 0.0, -1.0, 1.0), geo=2)])
+    return out
+
+
+def make_static():
+    out_dir = os.path.join(HERE, "static")
+    os.makedirs(out_dir, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix="pdgolden_static_")
+    for name, deck in static_cases().items():
+        ddir = os.path.join(out_dir, "decks", name)
+        deck.write(ddir)
+        wd = os.path.join(tmp, name)
+        os.makedirs(wd, exist_ok=True)
+        shutil.copy(os.path.join(ddir, "pds_input.txt"), os.path.join(wd, "pds_input.txt"))
+        run("damp", wd, os.path.join(wd, "damp.bin"), STATIC_DT)
+        f = read_pdb(os.path.join(wd, "damp.bin"))
+        keep = ("n", "coords", "mat", "fam_ptr", "fam_col", "broken", "spring", "mat_density", "params", "iparams",
+                "absK", "damp_coeff", "damp_dt", "u_field_0", "u_field_1", "u_field_2")
+        np.savez_compressed(os.path.join(out_dir, name + ".npz"), **{k: f[k] for k in keep})
+        print(name, int(f["n"][0]), "nodes", "damping coefficients", f["damp_coeff"])
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__" and "--static" in sys.argv:
+    make_static()

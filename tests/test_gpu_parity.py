@@ -101,6 +101,34 @@ def test_host_buffer_steps_equal_device_steps():
     assert np.array_equal(Ua, U1) and np.array_equal(Va, V1)
 
 
+@pytest.mark.parametrize("prec", [P.PREC_FP64, P.PREC_FP32C])
+def test_host_buffer_steps_continue_from_an_uploaded_state(prec):
+    """A context handed a mid-run state through host buffers steps exactly
+    like the context that reached that state by stepping: the uploaded U
+    replaces the Gauss-point displacements (and FP32 node blocks) too, not
+    only the nodal state."""
+    g = load_golden("fgi_velo")
+    dt = g["dt"][0]
+    a = gpu_model("fgi_velo").context()
+    a.set_precision(prec)
+    a.rk4_steps(dt, 0.0, 4)
+    a.sync()
+    Ua, Va = a.get_state()
+    a.rk4_steps(dt, 4 * dt, 2)
+    a.sync()
+    Ua6, Va6 = a.get_state()
+    b = gpu_model("fgi_velo").context()  # at rest: its Gauss points are all zero
+    b.set_precision(prec)
+    n3 = 3 * b.n
+    U1, V1 = np.zeros(n3), np.zeros(n3)
+    b.rk4_steps_host(dt, 4 * dt, 1, Ua, Va, U1, V1)
+    # second call: a round trip of the first call's output
+    U2, V2 = np.zeros(n3), np.zeros(n3)
+    b.rk4_steps_host(dt, 5 * dt, 1, U1, V1, U2, V2)
+    assert np.array_equal(U2, Ua6) and np.array_equal(V2, Va6)
+    assert np.abs(Ua).max() > 0
+
+
 def test_sample_like_deck_known_answers():
     """The reference sample deck's parameters: 1,655,072 bonds and the
     energies of the first two steps (CCI, displacement-gradient layers)."""

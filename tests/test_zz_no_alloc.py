@@ -102,3 +102,71 @@ def test_noalloc_reports_capacity_and_size(tmp_path):
     rc = f(d_x.data_ptr(), too_many, info.grid_spacing, info.horizon, 0, None, d_rp.data_ptr(),
            d_col.data_ptr(), None, 10, None, C.byref(nh), C.byref(mb))
     assert rc == -6
+
+
+def _search(f, x, spacing, horizon, slits=None, cap=0):
+    """Runs the entry point on coordinates x [n][3]; returns (status, halves)."""
+    import torch
+    n = len(x)
+    d_x = torch.tensor(np.ascontiguousarray(x, dtype=np.float64), device="cuda")
+    d_rp = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    d_col = torch.zeros(max(cap, 1), dtype=torch.int32, device="cuda")
+    sl = None if slits is None else np.ascontiguousarray(slits, dtype=np.float64).reshape(-1)
+    ns = 0 if sl is None else sl.size // 6
+    nh = C.c_int64(0)
+    mb = C.c_double(0.0)
+    rc = f(d_x.data_ptr(), n, spacing, horizon, ns, sl.ctypes.data_as(C.POINTER(C.c_double)) if ns else None,
+           d_rp.data_ptr(), d_col.data_ptr(), None, cap, None, C.byref(nh), C.byref(mb))
+    torch.cuda.synchronize()
+    return rc, nh.value
+
+
+def _still_usable(f):
+    """After a refused call the library still searches a small bar correctly."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        D.config_bar(dims=(8, 5, 4), traction_as_veloc=0.05).write(td)
+        dm = P.pdDataManager(td)
+        dm.InitNode()
+        dm.InitBond()
+        info = dm.info()
+        x, _, _ = dm.nodes()
+        rc, nh = _search(f, x.reshape(-1, 3), info.grid_spacing, info.horizon, cap=info.num_halves)
+        assert rc == 0 and nh == info.num_halves
+
+
+def test_noalloc_refuses_too_many_cells():
+    f = _entry()
+    # two nodes 1 m apart with a 1 nm horizon: 5e8 cells along x
+    x = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    assert _search(f, x, 1e-9, 1e-9)[0] == -6
+    # three axes of 1e9 cells each: the product would overflow a 64-bit integer
+    x = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]])
+    assert _search(f, x, 1e-10, 1e-9)[0] == -6
+    # 301 cells per axis: each axis is within the limit, their product is not
+    assert _search(f, x, 1e-3, 1.0 / 300.0 - 1e-3)[0] == -6
+    # a non-finite coordinate is an argument error, not a cell count
+    x = np.array([[0.0, 0.0, 0.0], [np.nan, 0.0, 0.0]])
+    assert _search(f, x, 1e-3, 3e-3)[0] == -1
+    _still_usable(f)
+
+
+def test_noalloc_refuses_too_many_slits():
+    f = _entry()
+    x = np.array([[0.0, 0.0, 0.0], [1e-3, 0.0, 0.0]])
+    slits = np.tile([-1.0, 1.0, 0.0, 0.0, -1.0, 1.0], 17)
+    assert _search(f, x, 1e-3, 3e-3, slits=slits)[0] == -1  # above PD_NOALLOC_MAX_SLITS
+    _still_usable(f)
+
+
+def test_noalloc_refuses_family_beyond_shared_buffer():
+    f = _entry()
+    # 14^3 nodes all within one horizon: families of 2743 exceed the 48 KB
+    # shared buffer of four warps
+    g = np.arange(14, dtype=np.float64) * 1e-3
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    n = len(x)
+    rc, nh = _search(f, x, 1e-3, 0.05, cap=n * (n - 1))
+    assert nh == n * (n - 1)
+    assert rc == -6
+    _still_usable(f)
