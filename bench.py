@@ -638,7 +638,8 @@ def apply_shape(ctx, shape):
     whose timing must not depend on a tuner, e.g. under a profiler)."""
     import pdmtel_b200 as P
     opts = [("tile", P.OPT_TILE), ("gather_per_point", P.OPT_GATHER_PER_POINT), ("gather_sell", P.OPT_GATHER_SELL),
-            ("gather_stencil", P.OPT_GATHER_STENCIL), ("force_stencil", P.OPT_FORCE_STENCIL),
+            ("gather_stencil", P.OPT_GATHER_STENCIL), ("gather_delta", P.OPT_GATHER_DELTA),
+            ("force_stencil", P.OPT_FORCE_STENCIL),
             ("force_quad", P.OPT_FORCE_QUAD), ("force_tile", P.OPT_FORCE_TILE)]
     for key, opt in opts:
         if key in shape:
@@ -753,10 +754,14 @@ def run_ours(args):
     force_kernel = ("k_force_f32c_sten" if sten else "k_force_f32c_quad" if tune.get("force_quad")
                     else "k_force_f32c_tiled" if tune.get("force_tile") else "k_force_f32c_pair")
     pat, sell = bool(tune.get("gather_stencil")), bool(tune.get("gather_sell"))
-    gather_kernel = "k_gather_f32c_ring" if (pat and sell) else "k_gather_f32c"
-    # coefficients, contributor ids (pattern ids instead with patterns), trial
-    # displacement, output blocks, partition-of-unity sums, row pointers
-    gather_bytes = (ncb * npt * 4 + (n * 4 if pat else ncb * 4 + (n + 1) * 8) + n * 8 * 4 + n * npt * 12
+    delta = pat and sell and bool(tune.get("gather_delta"))
+    gather_kernel = ("k_gather_f32c_dring" if delta else "k_gather_f32c_ring") if (pat and sell) else "k_gather_f32c"
+    # coefficients (2-byte deltas and a 4-byte scale per node and point with
+    # the delta form; the pattern table stays in L2), contributor ids (pattern
+    # ids instead with patterns), trial displacement, output blocks,
+    # partition-of-unity sums, row pointers
+    coef_bytes = ncb * npt * 2 + n * npt * 4 if delta else ncb * npt * 4
+    gather_bytes = (coef_bytes + (n * 4 if pat else ncb * 4 + (n + 1) * 8) + n * 8 * 4 + n * npt * 12
                     + n * npt * 4)
     force_flops = FLOP_PER_EVAL * evals_stage
     traffic = None
@@ -827,7 +832,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--shape", default=None,
                     help="skip pd_autotune and apply these launch shapes, a JSON object with keys of its result "
-                         "(tile, gather_per_point, gather_sell, gather_stencil, force_stencil, force_quad, force_tile)")
+                         "(tile, gather_per_point, gather_sell, gather_stencil, gather_delta, force_stencil, force_quad, "
+                         "force_tile)")
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--form", default="precision",
                     choices=["precision", "batch", "static", "identify", "accuracy", "steps", "adjoint"])

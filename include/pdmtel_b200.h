@@ -128,6 +128,24 @@ int pd_set_bdry_eff(pd_ctx* ctx, const double* bdry_eff);
  * (pdDataManager2.cpp:118-256): cb_ptr [N+1], cb_idx, coeff laid out per
  * node as [point][contributor]. */
 int pd_set_mls(pd_ctx* ctx, const int64_t* cb_ptr, const int32_t* cb_idx, const double* coeff);
+/* The same MLS data computed on the device from the context's family (the
+ * contributor rule of pdDataManager2.cpp:118-171: the node, then family
+ * members within rw, within 1.5 rw when fewer than 10) and coordinates, or
+ * from mls_coords ([N][3] host, may be NULL: each node's coordinates in the
+ * frame its MLS is solved in, e.g. a batch specimen's own frame).  Moment
+ * matrices and their full-pivot solve follow pdDataManager2.cpp:173-256 and
+ * pdMatrix.cpp:251-391 operation for operation; only the spline weight's
+ * d^3 and d^4 (glibc pow in the reference, off the correctly rounded value
+ * for ~4e-4 of the arguments) are rounded once, so the coefficients equal
+ * the reference's where those agree and differ by the moment matrix's
+ * round-off elsewhere.  PD_ERR_SINGULAR on a singular moment matrix.
+ * *num_contrib (may be NULL) receives the number of contributor entries. */
+int pd_mls_setup(pd_ctx* ctx, double rw, const double* mls_coords, int64_t* num_contrib);
+/* The context's MLS data out in the layout of pd_set_mls: cb_ptr [N+1],
+ * cb_idx [entries] and coeff [entries x points] (either may be NULL). */
+int pd_get_mls(pd_ctx* ctx, int64_t* cb_ptr, int32_t* cb_idx, double* coeff);
+/* number of MLS contributor entries held (0 without MLS data) */
+int pd_mls_size(pd_ctx* ctx, int64_t* num_contrib);
 
 /* Arithmetic of the subsequent force/gather/step calls (pd_precision). */
 int pd_set_precision(pd_ctx* ctx, int precision);
@@ -252,7 +270,8 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
                     double* relres);
 
 /* ---- Tuning options (no counterpart in the reference) ----
- * None of them changes a result; they change launch shapes only.
+ * None of them changes a result (PD_OPT_STATIC_PRECOND: beyond the solve's
+ * tolerance); they change launch shapes only.
  * PD_OPT_F64_LANES_BELOW: the FP64 Gauss-point force runs eight lanes per
  *   node (same arithmetic, same order) when the problem has fewer nodes than
  *   this, one thread per node otherwise.  Default 131072.
@@ -307,7 +326,18 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   contributor loads no longer wait on an index load from memory.  Same
  *   contributors in the same order: same results bit for bit.  Refused
  *   (PD_ERR_ARG) when the distinct patterns would hold more than 4M
- *   entries; 0 (default) reads the lists. */
+ *   entries; 0 (default) reads the lists.
+ * PD_OPT_GATHER_DELTA: 1 makes the FP32-form gather with the SELL copy and
+ *   the patterns both on (the coefficient ring) read each coefficient as a
+ *   2-byte delta from its pattern's coefficient (half the bytes of the
+ *   FP32 stream).  The FP32 coefficients of every 2x2x2-point problem with
+ *   patterns are defined this way (pattern coefficient + per-point scale x
+ *   int16 delta, within FP32 rounding of the FP64 ones), so every FP32
+ *   gather gives the same result bit for bit.  Refused (PD_ERR_ARG) without
+ *   that form; 0 (default) off.
+ * PD_OPT_STATIC_PRECOND: 1 (default) preconditions the static CG with the
+ *   inverses of the operator's 3x3 diagonal blocks (block Jacobi); 0 runs
+ *   plain CG.  Changes the iterates, not the solution beyond the tolerance. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -322,7 +352,9 @@ enum {
     PD_OPT_PERSIST_TEST_STALL = 11,
     PD_OPT_GATHER_SELL = 12,
     PD_OPT_FORCE_STENCIL = 13,
-    PD_OPT_GATHER_STENCIL = 14
+    PD_OPT_GATHER_STENCIL = 14,
+    PD_OPT_GATHER_DELTA = 15,
+    PD_OPT_STATIC_PRECOND = 16
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -353,6 +385,8 @@ typedef struct pd_tune_result {
     int32_t gather_sell;      /* PD_OPT_GATHER_SELL kept */
     int32_t force_stencil;    /* PD_OPT_FORCE_STENCIL kept */
     int32_t gather_stencil;   /* PD_OPT_GATHER_STENCIL kept */
+    int32_t gather_delta;     /* PD_OPT_GATHER_DELTA kept */
+    int32_t pad2;
 } pd_tune_result;
 /* Times candidate launch shapes (node-order tiles, the FP32 gather variants:
  * per point, SELL copy, contributor patterns;

@@ -84,6 +84,10 @@ int pdh_get_tables(pdh_model* m, pd_material* materials, pd_bc* bcs, double* abs
 /* the device context of the model (uploads the setup on first use) */
 int pdh_context(pdh_model* m, pd_ctx** ctx);
 int pdh_set_precision(pdh_model* m, int precision);
+/* InitIntegrationPoint (pdDataManager2.cpp:106-309) on the device
+ * (pd_mls_setup) when on != 0; set before InitIntegrationPoint.  Off by
+ * default: the host setup reproduces the reference bit for bit. */
+int pdh_set_device_setup(pdh_model* m, int on);
 
 /* pdSolve::SolveDynamic (pdSolve.cpp:24-130); write_files selects the
  * reference's per-step log, probe and Tecplot output */

@@ -17,6 +17,11 @@
 //   pdref_harness traj  <dir> <out.bin> <nsteps> <dump_every>
 //   pdref_harness time  <dir> <nsteps>
 //   pdref_harness damp  <dir> <out.bin> <dt>
+//   pdref_harness solve <dir>
+//
+// solve: pdSolve::SolveDynamic (pdSolve.cpp:24-130) itself, which writes the
+// reference's pds_output.dat log, pds_steps.dat probe and pds_tecplot_<step>
+// files into <dir>.
 //
 // damp: the reference's matrix-free linearised stiffness pass,
 // pdDataManager::CalcDampingCoeff (pdDataManager2.cpp:1616-1907), at three
@@ -403,6 +408,9 @@ int main(int argc, char** argv) {
         }
         w.d("damp_coeff", damp);
         w.d1("damp_dt", dt);
+    } else if (mode == "solve") {
+        setup(dat, dir);
+        pdSolve::SolveDynamic(dat);
     } else if (mode == "time") {
         int nsteps = std::atoi(argv[3]);
         double t0 = now();

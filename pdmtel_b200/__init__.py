@@ -31,7 +31,8 @@ PREC_FP64, PREC_FP32C, PREC_FP64A = 0, 1, 2
 OPT_F64_LANES_BELOW, OPT_TILE, OPT_PERSIST_BLOCKS_PER_SM = 1, 2, 3
 OPT_PERSIST_FORCE_CHUNK, OPT_PERSIST_GATHER_CHUNK, OPT_STATIC_STENCIL, OPT_GATHER_PER_POINT = 4, 5, 6, 7
 OPT_FORCE_TILE, OPT_FORCE_QUAD, OPT_PERSIST_WAIT_US, OPT_PERSIST_TEST_STALL = 8, 9, 10, 11
-OPT_GATHER_SELL, OPT_FORCE_STENCIL, OPT_GATHER_STENCIL = 12, 13, 14
+OPT_GATHER_SELL, OPT_FORCE_STENCIL, OPT_GATHER_STENCIL, OPT_GATHER_DELTA = 12, 13, 14, 15
+OPT_STATIC_PRECOND = 16
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}
@@ -84,7 +85,8 @@ class pd_tune_result(C.Structure):
                 ("force_chunk", C.c_int32), ("gather_chunk", C.c_int32), ("trials", C.c_int32),
                 ("ms_per_step", C.c_double), ("gather_per_point", C.c_int32), ("pad", C.c_int32),
                 ("force_tile", C.c_int64), ("force_quad", C.c_int32), ("gather_sell", C.c_int32),
-                ("force_stencil", C.c_int32), ("gather_stencil", C.c_int32)]
+                ("force_stencil", C.c_int32), ("gather_stencil", C.c_int32), ("gather_delta", C.c_int32),
+                ("pad2", C.c_int32)]
 
 
 # name -> argtypes; every entry point returns int
@@ -99,6 +101,9 @@ _SIGS = {
     "pd_set_family": [_vp, _i64, _i32, _u8],
     "pd_set_bdry_eff": [_vp, _d],
     "pd_set_mls": [_vp, _i64, _i32, _d],
+    "pd_mls_setup": [_vp, C.c_double, _d, _i64],
+    "pd_get_mls": [_vp, _i64, _i32, _d],
+    "pd_mls_size": [_vp, _i64],
     "pd_set_precision": [_vp, C.c_int],
     "pd_set_energy": [_vp, C.c_int],
     "pd_set_state": [_vp, _d, _d],
@@ -143,6 +148,7 @@ _SIGS = {
     "pdh_get_mls": [_vp, _i64, _i32, _d],
     "pdh_context": [_vp, C.POINTER(_vp)],
     "pdh_set_precision": [_vp, C.c_int],
+    "pdh_set_device_setup": [_vp, C.c_int],
     "pdh_solve_dynamic": [_vp, C.c_int],
     "pdh_solve_static": [_vp, C.c_int, C.c_double, C.POINTER(C.c_int), _d],
     "pdh_batch_create": [C.c_char_p, C.POINTER(_vp), C.c_int, C.POINTER(_vp)],
@@ -316,6 +322,24 @@ class DeviceContext:
         ci = np.ascontiguousarray(cb_idx, dtype=np.int32)
         co = _f64(coeff)
         _check(lib().pd_set_mls(self.h, _p(cp, _i64), _p(ci, _i32), _p(co, _d)), "pd_set_mls")
+
+    def mls_setup(self, rw, mls_coords=None):
+        """InitIntegrationPoint on the device (pd_mls_setup); returns the
+        number of contributor entries."""
+        x = None if mls_coords is None else _f64(mls_coords, 3 * self.n)
+        T = C.c_int64(0)
+        _check(lib().pd_mls_setup(self.h, float(rw), _p(x, _d), C.byref(T)), "pd_mls_setup")
+        return T.value
+
+    def get_mls(self):
+        """(cb_ptr, cb_idx, coeff) held by the context, in pd_set_mls's layout"""
+        T = C.c_int64(0)
+        _check(lib().pd_mls_size(self.h, C.byref(T)), "pd_mls_size")
+        cp = np.zeros(self.n + 1, np.int64)
+        ci = np.zeros(max(T.value, 1), np.int32)
+        co = np.zeros(max(T.value * self.npt, 1))
+        _check(lib().pd_get_mls(self.h, _p(cp, _i64), _p(ci, _i32), _p(co, _d)), "pd_get_mls")
+        return cp, ci[:T.value], co[:T.value * self.npt]
 
     def set_precision(self, p):
         _check(lib().pd_set_precision(self.h, int(p)), "pd_set_precision")
@@ -545,6 +569,13 @@ class pdDataManager:
 
     def SetPrecision(self, p):
         self._call("pdh_set_precision", int(p))
+
+    def SetDeviceSetup(self, on=True):
+        """InitIntegrationPoint on the device (pd_mls_setup); set it before
+        InitIntegrationPoint.  The host setup (default) is the reference's
+        arithmetic bit for bit; the device one differs only where glibc's pow
+        is not correctly rounded."""
+        self._call("pdh_set_device_setup", int(bool(on)))
 
     def CalcStableTimeStep(self) -> float:
         return self.info().stable_dt

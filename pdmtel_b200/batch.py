@@ -58,7 +58,7 @@ class Batch:
     their micromodulus fields and assembles the batch model (device bond
     search, per-specimen MLS)."""
 
-    def __init__(self, workdir: str, spec: BatchSpec, precision: int = PREC_FP32C):
+    def __init__(self, workdir: str, spec: BatchSpec, precision: int = PREC_FP32C, device_setup: bool = False):
         self.spec = spec
         self.specimens: List[pdDataManager] = []
         self.factors: List[np.ndarray] = []
@@ -76,6 +76,9 @@ class Batch:
             self.factors.append(f)
         self.model = pdDataManager.batch(os.path.join(workdir, "batch"), self.specimens)
         self.model.InitBond()
+        # device_setup: every specimen's MLS solved on the device (pd_mls_setup,
+        # each in its own frame) instead of on the host
+        self.model.SetDeviceSetup(device_setup)
         self.model.InitIntegrationPoint()
         self.model.SetPrecision(precision)
         self.ctx = self.model.context()

@@ -114,6 +114,9 @@ int pdDataManager::ReadInputFile() {
         PDH_TRY(rd("fixed_time_step", 1, _fixedTimeStep));
     }
     if (D.Find("grid_file")) return Error(PD_ERR_ARG, "ReadInputFile: external grid files are not supported");
+    _forcePlaneOn = D.Find("total_force_plane");
+    if (_forcePlaneOn)
+        for (int a = 0; a < 3; ++a) PDH_TRY(rd("total_force_plane", a + 1, _forcePlane[a]));
     // materials
     PDH_TRY(req("number_of_materials"));
     int nm = 0;
@@ -194,7 +197,8 @@ int pdDataManager::ReadInputFile() {
     for (int i = 0; i < nms; ++i)
         PDH_TRY(read_space(keyword_append("material_space_", i + 1), true, nm, _matSpaces[i]));
     _delSpaces.clear();
-    if (D.Find("number_of_deletion_spaces")) {
+    const bool hasDelKeyword = D.Find("number_of_deletion_spaces");
+    if (hasDelKeyword) {
         int nd = 0;
         PDH_TRY(rd("number_of_deletion_spaces", 1, nd));
         _delSpaces.assign(std::max(nd, 0), Space());
@@ -253,12 +257,90 @@ int pdDataManager::ReadInputFile() {
     const int n1 = _cciOn ? 1 : _intgPoint;
     _npt = n1 * n1 * n1;
     gauss_rule(n1, _abscis, _weights);
-    log << "ReadInputFile: Problem title = " << _title << "\n"
-        << "ReadInputFile: Grid dimension = " << _dims[0] << " * " << _dims[1] << " * " << _dims[2] << "\n"
-        << "ReadInputFile: Global grid spacing = " << _gridSpacing << "\n"
-        << "ReadInputFile: Global grid horizon = " << _horizon << "\n";
+    EchoDeck(log, hasDelKeyword);
     _stage = true;
     return PD_OK;
+}
+
+namespace {
+
+// pdBdryCondition::Print and the subclasses' type line (pdBdryCondition.cpp:
+// 55-74, pdBdryConditionDispl.cpp:29-33, ...Veloc.cpp:20-24,
+// ...DisplGrad.cpp:30-34, ...Tract.cpp:29-33)
+void print_bc(std::ostream& os, int k, const BdryCondition& b) {
+    os << "Boundary Condition " << k + 1 << "\n";
+    os << "  Direction flag = " << b.dir[0] << "\t" << b.dir[1] << "\t" << b.dir[2] << "\n";
+    os << "  Value = ";
+    for (double v : b.value) os << v << "\t";
+    os << "\n" << "  End time = " << b.end_time << "\t";
+    os << (b.load_type == 1.0 ? "Loading type = Ramp loading" : "Loading type = Step loading") << "\n";
+    switch (b.type) {
+        case DISPL: os << "  Type: Prescribed Displacement\n"; break;
+        case VELOC: os << "  Type: Prescribed Velocity\n"; break;
+        case DISPLGRAD: os << "  Type: Prescribed Displacement Gradient \n"; break;
+        default: os << "  Type: Traction Force\n"; break;
+    }
+}
+
+// pdSpace::Print (pdSpace.cpp:87-100)
+void print_space(std::ostream& os, int k, const Space& s) {
+    os << "Space " << k + 1 << "\n";
+    if (s.geo == 1)
+        os << "  x1= " << s.lo[0] << "\t" << s.hi[0] << "\t" << " x2= " << s.lo[1] << "\t" << s.hi[1] << "\t"
+           << " x3= " << s.lo[2] << "\t" << s.hi[2];
+    else
+        os << "  center= " << s.c1 << "\t" << s.c2 << "\t" << " radius= " << s.rad << "\t" << " x3= " << s.lo[2]
+           << "\t" << s.hi[2];
+}
+
+}  // namespace
+
+// The deck echo of ReadInputFile into pds_output.dat, line for line the
+// reference's (pdDataManager.cpp:89-112,281-288,349-356,411-418,536-543,
+// 733-753).
+void pdDataManager::EchoDeck(std::ostream& log, bool deletion_keyword) const {
+    log << "ReadInputFile: Problem title = " << _title << "\n"
+        << "ReadInputFile: Grid center: x1 = " << _center[0] << ", x2 = " << _center[1] << ", x3 = " << _center[2]
+        << "\n"
+        << "ReadInputFile: Grid dimension = " << _dims[0] << " * " << _dims[1] << " * " << _dims[2] << "\n"
+        << "ReadInputFile: Global grid spacing = " << _gridSpacing << "\n"
+        << "ReadInputFile: Global grid horizon = " << _horizon << "\n"
+        << "ReadInputFile: Total run time = " << _totalTime << "\n"
+        << "ReadInputFile: Total run steps = " << _totalStep << "\n"
+        << "ReadInputFile: Step dump frequency = " << _stepDumpFrequency << "\n";
+    if (_fixedTimeStepOn) log << "ReadInputFile: Fixed time step = " << _fixedTimeStep << "\n";
+    log << "\nReadInputFile: Total boundary condition number = " << _bcs.size() << "\n";
+    for (size_t k = 0; k < _bcs.size(); ++k) {
+        print_bc(log, (int)k, _bcs[k]);
+        log << "\n";
+    }
+    log << "\nReadInputFile: Total material space number = " << _matSpaces.size() << "\n";
+    for (size_t k = 0; k < _matSpaces.size(); ++k) {
+        print_space(log, (int)k, _matSpaces[k]);
+        log << "\n  Type: material space associates with material id = " << _matSpaces[k].ref << "\n\n";
+    }
+    if (deletion_keyword) {
+        log << "\nReadInputFile: Total deletion space number = " << _delSpaces.size() << "\n";
+        for (size_t k = 0; k < _delSpaces.size(); ++k) {
+            print_space(log, (int)k, _delSpaces[k]);
+            log << "\n";
+        }
+    }
+    log << "\nReadInputFile: Total boundary space number = " << _bdrySpaces.size() << "\n";
+    for (size_t k = 0; k < _bdrySpaces.size(); ++k) {
+        print_space(log, (int)k, _bdrySpaces[k]);
+        log << "\n  Type: boundary condition space associates with BC id = " << _bdrySpaces[k].ref << "\n\n";
+    }
+    log << "\nReadInputFile: Linear damping coefficient = " << _dampCoeff << "\n";
+    log << "\nReadInputFile: Boundary effect compensation factor flag = " << _bdryEffOn << "\n";
+    log << "\nReadInputFile: CCI integration method flag = " << _cciOn << "\n";
+    if (_cciOn) log << "\nReadInputFile: Modified CCI beta flag = " << _cciMdf << "\n";
+    log << "\nReadInputFile: Integration with fixed Gaussian points method flag = " << _fgiOn << "\n";
+    if (_fgiOn) {
+        log << "\nReadInputFile: Starting Gaussian points = " << _intgPoint << "\n";
+        log << "\nReadInputFile: Moving least square flag = " << _mlsOn << "\n";
+    }
+    log << "\nReadInputFile: Adaptive integration method flag = " << 0 << "\n";
 }
 
 // pdDataManager::InitNode, pdDataManager.cpp:813-1098
@@ -300,7 +382,10 @@ int pdDataManager::InitNode() {
     _bdryEff.assign(_numNodes, 1.0);
     _nodesDone = true;
     std::ofstream log(_outFilePath.c_str(), std::ios::app);
-    log << "\nInitNode: total node number = " << _numNodes << "\n";
+    log << "\nInitNode: total node number = " << _numNodes << "\n"
+        << "\nInitNode: Material association done \n"
+        << "\nInitNode: boundary condition association done \n"
+        << "\nInitNode: nodes initialization done \n";
     return PD_OK;
 }
 
@@ -378,7 +463,8 @@ int pdDataManager::InitBond() {
     _bondsDone = true;
     _familyOnDevice = true;
     std::ofstream log(_outFilePath.c_str(), std::ios::app);
-    log << "\nInitBond: total bonds number = " << nh / 2 << "\n";
+    log << "\nInitBond: total bonds number = " << nh / 2 << "\n"
+        << "\nInitBond: bonds initialization done \n";
     return PD_OK;
 }
 
@@ -406,6 +492,20 @@ int pdDataManager::SetFamily(const std::vector<int64_t>& row_ptr, const std::vec
 // pdDataManager::InitMaterial, pdDataManager.cpp:1297-1338
 int pdDataManager::InitMaterial() {
     for (Material& m : _mats) m.spring = m.type == 1 ? 18 * m.BulkModulus() / (kPI * std::pow(_horizon, 4.0)) : 0.0;
+    {
+        // pdMaterial::Print and the type line (pdMaterial.cpp:100-106,
+        // pdMaterialBond.cpp:15-19, pdMaterialState.cpp:16-20)
+        std::ofstream log(_outFilePath.c_str(), std::ios::app);
+        log << "\nInitMatieral: Total material number = " << _mats.size() << "\n";
+        for (size_t k = 0; k < _mats.size(); ++k) {
+            const Material& m = _mats[k];
+            log << "Material " << k + 1 << "\n"
+                << "  Young's modulus= " << m.ymod << "\t" << "Yield strength= " << m.sigmay << "\n"
+                << "  Poisson's ratio= " << m.nu << "\t" << "Density= " << m.density << "\n"
+                << "  Critical stretch= " << m.ecrit << "\t" << "Spring constant= " << m.spring << "\n"
+                << (m.type == 1 ? "  Type: Bond-Based Material (PMB) \n" : "  Type: State-Based Material\n") << "\n";
+        }
+    }
     _minMaterialDensity = 1.0e10;
     _maxBulkSoundSpeed = 0.0;
     for (const Material& m : _mats) {
@@ -498,14 +598,66 @@ int pdDataManager::InitBdryEffectFactor() {
 
 // pdDataManager::InitGridBoundary, pdDataManager.cpp:1100-1295: the model
 // bounds are only used by output planes, which this build does not write.
-int pdDataManager::InitGridBoundary() { return PD_OK; }
+int pdDataManager::InitGridBoundary() {
+    // pdDataManager::InitGridBoundary, pdDataManager.cpp:1100-1170: the
+    // lattice bounds, the force planes (total_force_plane, or the middle) and
+    // the model space 50 spacings around; only the log uses them here
+    double a[3], b[3], plane[3];
+    for (int k = 0; k < 3; ++k) {
+        a[k] = -(_dims[k] - 1) * 0.5 * _gridSpacing + _center[k];
+        b[k] = (_dims[k] - 1) * 0.5 * _gridSpacing + _center[k];
+        plane[k] = _forcePlaneOn ? _forcePlane[k] : 0.5 * (a[k] + b[k]);
+    }
+    const double deformed = 50.0 * _gridSpacing;
+    std::ofstream log(_outFilePath.c_str(), std::ios::app);
+    log << "\nInitGridBoundary: grid boundaries: x1a = " << a[0] << ", x1b = " << b[0] << "\n"
+        << "InitGridBoundary: grid boundaries: x2a = " << a[1] << ", x2b = " << b[1] << "\n"
+        << "InitGridBoundary: grid boundaries: x3a = " << a[2] << ", x3b = " << b[2] << "\n"
+        << "\nInitGridBoundary: total force planes: x1= " << plane[0] << ", x2= " << plane[1] << ", x3= " << plane[2]
+        << "\n"
+        << "\nInitGridBoundary: model space boundaries: x1clo = " << a[0] - deformed << ", x1chi = " << b[0] + deformed
+        << "\n"
+        << "InitGridBoundary: model space boundaries: x2clo = " << a[1] - deformed << ", x2chi = " << b[1] + deformed
+        << "\n"
+        << "InitGridBoundary: model space boundaries: x3clo = " << a[2] - deformed << ", x3chi = " << b[2] + deformed
+        << "\n";
+    return PD_OK;
+}
 
 // pdDataManager::InitIntegrationPoint, pdDataManager2.cpp:106-309
 int pdDataManager::InitIntegrationPoint() {
+    const int rc = SetupIntegrationPoints();
+    if (rc == PD_OK) {
+        std::ofstream log(_outFilePath.c_str(), std::ios::app);
+        log << "\nInitIntegrationPoint: integration points initialization done \n";
+    }
+    return rc;
+}
+
+int pdDataManager::SetupIntegrationPoints() {
     if (!_mlsOn) return PD_OK;
     if (!_bondsDone) return Error(PD_ERR_ARG, "InitIntegrationPoint: bonds first");
     int64_t bad = -1;
     int rc = PD_OK;
+    _mlsOnDevice = false;
+    if (_deviceMls) {
+        // the contributors and coefficients computed on the device; a batch
+        // solves every specimen in its own frame, as BatchMLS does
+        if ((rc = EnsureContext()) != PD_OK) return rc;
+        if (!_familyOnDevice) {
+            if ((rc = pd_set_family(_ctx, _famPtr.data(), _famCol.data(), _famBroken.data())) != PD_OK)
+                return Cuda(rc, "pd_set_family");
+            _familyOnDevice = true;
+        }
+        _cbPtr.clear();
+        _cbIdx.clear();
+        _coeff.clear();
+        int64_t T = 0;
+        rc = pd_mls_setup(_ctx, _rw, _batch ? _batchCoords.data() : nullptr, &T);
+        if (rc != PD_OK) return Error(rc, std::string("pd_mls_setup: ") + pd_last_error());
+        _mlsOnDevice = true;
+        return PD_OK;
+    }
     if (_batch) {
         rc = BatchMLS(&bad);
     } else {
@@ -526,6 +678,27 @@ int pdDataManager::InitIntegrationPoint() {
     return PD_OK;
 }
 
+int64_t pdDataManager::NumContrib() const {
+    if (_mlsOnDevice && _ctx) {
+        int64_t T = 0;
+        pd_mls_size(_ctx, &T);
+        return T;
+    }
+    return _cbPtr.empty() ? 0 : _cbPtr.back();
+}
+
+int pdDataManager::FetchMLS() {
+    if (!_mlsOnDevice || !_ctx || !_cbPtr.empty()) return PD_OK;
+    int64_t T = 0;
+    int rc = pd_mls_size(_ctx, &T);
+    if (rc != PD_OK) return Cuda(rc, "pd_mls_size");
+    _cbPtr.assign(_numNodes + 1, 0);
+    _cbIdx.assign(T, 0);
+    _coeff.assign((size_t)T * _npt, 0.0);
+    rc = pd_get_mls(_ctx, _cbPtr.data(), _cbIdx.data(), _coeff.data());
+    return rc == PD_OK ? PD_OK : Cuda(rc, "pd_get_mls");
+}
+
 int pdDataManager::UploadSetup() {
     int rc = EnsureContext();
     if (rc != PD_OK) return rc;
@@ -538,7 +711,7 @@ int pdDataManager::UploadSetup() {
         _familyOnDevice = true;
     }
     if ((rc = pd_set_bdry_eff(_ctx, _bdryEff.data())) != PD_OK) return Cuda(rc, "pd_set_bdry_eff");
-    if (_mlsOn) {
+    if (_mlsOn && !_mlsOnDevice) {
         if (_cbPtr.empty()) return Error(PD_ERR_ARG, "no MLS data: InitIntegrationPoint first");
         if ((rc = pd_set_mls(_ctx, _cbPtr.data(), _cbIdx.data(), _coeff.data())) != PD_OK) return Cuda(rc, "pd_set_mls");
     }
@@ -644,7 +817,10 @@ static void print_node(std::ostream& os, int64_t i, const pdDataManager& dat, co
     const auto& x = dat.Coords();
     os << i << "\t" << x[3 * i] << "\t" << x[3 * i + 1] << "\t" << x[3 * i + 2] << "\t" << U[3 * i] << "\t"
        << U[3 * i + 1] << "\t" << U[3 * i + 2] << "\t" << V[3 * i] << "\t" << V[3 * i + 1] << "\t" << V[3 * i + 2]
-       << "\t" << dat.MatIds()[i] << "\t" << dat.BcIds()[i] << "\t" << dat.BdryEff()[i] << "\t" << 0;
+       << "\t" << dat.MatIds()[i] << "\t" << dat.BcIds()[i] << "\t" << dat.BdryEff()[i] << "\t" << 0.0;
+    // DmgFrac: pdNode::GetDmgFraction (pdNode.cpp:225-232), an int count of
+    // damaged bonds over the family size; nothing on the RK4 path counts a
+    // damaged bond, so the reference writes 0 as a double
 }
 
 int pdSolve::WriteTecplot(pdDataManager& dat, int step, double time) {
@@ -683,8 +859,9 @@ int pdSolve::SolveDynamic(pdDataManager& dat, bool write_files) {
         steps.open((dat.GetWkDir() + "pds_steps.dat").c_str());
         steps << "Data at given node for each time step output mode\n\n";
         steps << "Step Time ID X1 X2 X3 U1 U2 U3 V1 V2 V3 MatID BCID bdryEff DmgFrac \n";
-        steps.setf(std::ios::scientific);
-        steps.precision(5);
+        // the probe rows keep the stream's default format: the reference's
+        // WriteEachStep (pdSolve.cpp:752-774) sets scientific notation on a
+        // second stream but writes through the one SolveDynamic opened
     }
     int rc = dat.SetEnergy(write_files);
     if (rc != PD_OK) return rc;

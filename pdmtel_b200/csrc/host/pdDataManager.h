@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cstdint>
+#include <ostream>
 #include <string>
 #include <vector>
 
@@ -131,6 +132,14 @@ public:
     const std::vector<int64_t>& ContribPtr() const { return _cbPtr; }
     const std::vector<int32_t>& ContribIdx() const { return _cbIdx; }
     const std::vector<double>& Coeff() const { return _coeff; }
+    // InitIntegrationPoint on the device (pd_mls_setup) instead of the host;
+    // off by default: the host setup reproduces the reference bit for bit,
+    // the device one up to the rounding of two powers (see pd_mls_setup)
+    void SetDeviceSetup(bool on) { _deviceMls = on; }
+    bool MLSOnDevice() const { return _mlsOnDevice; }
+    int64_t NumContrib() const;
+    // the MLS data of a device setup, copied to the host vectors above
+    int FetchMLS();
     const std::vector<Material>& Materials() const { return _mats; }
     const std::vector<BdryCondition>& BCs() const { return _bcs; }
     pd_ctx* Context() { return _ctx; }
@@ -149,6 +158,8 @@ private:
     int Cuda(int rc, const char* what);
     int UploadSetup();
     int BatchMLS(int64_t* bad_node);
+    void EchoDeck(std::ostream& log, bool deletion_keyword) const;
+    int SetupIntegrationPoints();
 
     std::string _workDir, _inFilePath, _outFilePath, _title, _err;
     std::vector<std::string> _deck;  // lines, trimmed
@@ -156,6 +167,8 @@ private:
     double _center[3] = {0, 0, 0};
     double _gridSpacing = 0, _horizon = 0, _totalTime = 0, _fixedTimeStep = 0, _safeFactor = 0.8;
     double _tolerance = 0, _dampCoeff = 0, _rw = 0;
+    bool _forcePlaneOn = false;
+    double _forcePlane[3] = {0, 0, 0};
     int _totalStep = 0, _stepDumpFrequency = 1, _intgPoint = 0, _npt = 1;
     bool _fixedTimeStepOn = false, _bdryEffOn = false, _cciOn = false, _cciMdf = false, _fgiOn = false,
          _mlsOn = false;
@@ -193,6 +206,7 @@ private:
     pd_ctx* _ctx = nullptr;
     bool _uploaded = false;
     bool _familyOnDevice = false;
+    bool _deviceMls = false, _mlsOnDevice = false;
     int _precision = PD_PREC_FP64;
     bool _energy = true;
     bool _stage = false;  // ReadInputFile done

@@ -85,7 +85,7 @@ int pdh_get_info(pdh_model* m, pdh_info* I) {
     I->num_nodes = d.GetNumNode();
     I->num_halves = d.GetNumHalves();
     I->num_broken = d.GetNumBroken();
-    I->num_contrib = d.ContribPtr().empty() ? 0 : d.ContribPtr().back();
+    I->num_contrib = d.NumContrib();
     I->num_gauss = d.GetNumGaussPoints();
     I->cci = d.IsCCI();
     I->mls = d.IsMLSOn();
@@ -187,6 +187,8 @@ int pdh_get_bdry_eff(pdh_model* m, double* bE) {
 
 int pdh_get_mls(pdh_model* m, int64_t* cp, int32_t* ci, double* co) {
     if (!m) return PD_ERR_ARG;
+    const int rc = track(m, m->dat.FetchMLS());
+    if (rc != PD_OK) return rc;
     const auto& d = m->dat;
     if (cp) std::memcpy(cp, d.ContribPtr().data(), sizeof(int64_t) * d.ContribPtr().size());
     if (ci) std::memcpy(ci, d.ContribIdx().data(), sizeof(int32_t) * d.ContribIdx().size());
@@ -202,6 +204,12 @@ int pdh_context(pdh_model* m, pd_ctx** ctx) {
 }
 
 int pdh_set_precision(pdh_model* m, int p) { return m ? track(m, m->dat.SetPrecision(p)) : PD_ERR_ARG; }
+
+int pdh_set_device_setup(pdh_model* m, int on) {
+    if (!m) return PD_ERR_ARG;
+    m->dat.SetDeviceSetup(on != 0);
+    return PD_OK;
+}
 
 int pdh_solve_dynamic(pdh_model* m, int write_files) {
     return m ? track(m, pdh::pdSolve::SolveDynamic(m->dat, write_files != 0)) : PD_ERR_ARG;

@@ -45,6 +45,7 @@ struct pd_ctx {
     int precision = PD_PREC_FP64;
     int nslit = 0;
     std::vector<double> coords;  // [N][3] host copy
+    std::vector<double> abscis;  // 1-D Gauss abscissae (FGI)
     std::vector<double> slits;
     double* dslits = nullptr;   // [nslit][6] on the device
     std::vector<pd::GaussConst> gch;            // Gauss constants (host copy)
@@ -76,6 +77,9 @@ struct pd_ctx {
     // static operator: per-material springs, lattice stencil (static_prepare)
     std::vector<double> mat_spring;
     int static_stencil_opt = 1;
+    int static_precond = 1;        // block-Jacobi preconditioner of the static CG (PD_OPT_STATIC_PRECOND)
+    double* bj_minv = nullptr;
+    uint64_t bj_gen = ~0ull;
     int static_replacements = 0;
     bool sten_ok = false;
     uint64_t sten_gen = ~0ull;
@@ -88,12 +92,19 @@ struct pd_ctx {
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
     int gpat_opt = 0;             // FP32 gather from contributor patterns (PD_OPT_GATHER_STENCIL)
+    bool have_gpat = false;       // patterns built (with the MLS data; refused when nothing repeats)
+    bool have_delta = false;      // delta form of the FP32 coefficients built
+    float* cpat = nullptr;        // delta form: pattern table, scales, CSR deltas, SELL copy
+    float* cscale = nullptr;
+    int16_t* cd16 = nullptr;
+    int16_t* sell_d16 = nullptr;
     int32_t* gpat_id = nullptr;
     int64_t* gpat_ptr = nullptr;
     int32_t* gpat_off = nullptr;
     int fst_shape = 0;            // lattice-stencil FP32 force (PD_OPT_FORCE_STENCIL)
     int4* fst_u2 = nullptr;
     uint32_t* fst_mask = nullptr;
+    float4* fst_tab = nullptr;
     int64_t* sell_off = nullptr;  // SELL copy of the FP32 gather's lists
     int32_t* sell_idx = nullptr;
     float* sell_coef = nullptr;
@@ -355,6 +366,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     c->n = N;
     c->npt = n1 * n1 * n1;
     c->coords.assign(P->coords, P->coords + 3 * N);
+    if (P->integration == PD_INTG_FGI && P->abscissae) c->abscis.assign(P->abscissae, P->abscissae + n1);
     c->nslit = P->num_slits > 0 ? P->num_slits : 0;
     if (c->nslit) c->slits.assign(P->slits, P->slits + 6 * c->nslit);
     pd::Dev& d = c->d;
@@ -586,12 +598,15 @@ static int sell_prepare(pd_ctx* c) {
     dfree(c, c->sell_off);
     dfree(c, c->sell_idx);
     dfree(c, c->sell_coef);
+    dfree(c, c->sell_d16);
     c->sell_off = nullptr;
     c->sell_idx = nullptr;
     c->sell_coef = nullptr;
+    c->sell_d16 = nullptr;
     c->d.sell_off = nullptr;
     c->d.sell_idx = nullptr;
     c->d.sell_coef = nullptr;
+    c->d.sell_d16 = nullptr;
     if (!c->d.sell_on || !c->have_mls || !c->d.mls || c->npt != 8 || c->n == 0) return PD_OK;
     const int64_t S = pd::sell_slices(c->d);
     int64_t* width = nullptr;
@@ -605,10 +620,12 @@ static int sell_prepare(pd_ctx* c) {
     PD_CUDA_TRY(cudaMemcpy(&total, c->sell_off + S, sizeof(int64_t), cudaMemcpyDeviceToHost));
     PD_TRY(dalloc(c, &c->sell_idx, total * 16));
     PD_TRY(dalloc(c, &c->sell_coef, total * 16 * 8));
+    if (c->have_delta) PD_TRY(dalloc(c, &c->sell_d16, total * 16 * 8));
     c->d.sell_off = c->sell_off;
     c->d.sell_idx = c->sell_idx;
     c->d.sell_coef = c->sell_coef;
-    pd::launch_sell_fill(c->d, c->sell_off, c->sell_idx, c->sell_coef, c->stream);
+    c->d.sell_d16 = c->sell_d16;
+    pd::launch_sell_fill(c->d, c->sell_off, c->sell_idx, c->sell_coef, c->sell_d16, c->stream);
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->generation++;
     return PD_OK;
@@ -617,21 +634,141 @@ static int sell_prepare(pd_ctx* c) {
 // The contributor patterns of the FP32 gather: every node's MLS contributor
 // list as id offsets from the node, identical lists stored once (on a box
 // lattice numbered x + nx (y + ny z) the lists of nodes with the same
-// position relative to the boundary are translates of each other).  Rebuilt
-// after pd_set_mls; freed when off.  Refused when the distinct patterns
-// would hold more than 4M entries (nothing repeats: no gain).
-static int gpat_prepare(pd_ctx* c) {
-    dfree(c, c->gpat_id);
-    dfree(c, c->gpat_ptr);
-    dfree(c, c->gpat_off);
+// position relative to the boundary are translates of each other).  Built
+// with the MLS data (pd_set_mls), whether or not a gather uses them, because
+// the FP32 coefficients of 2x2x2-point problems are defined from them (the
+// delta form below).  No patterns when the distinct lists would hold more
+// than 4M entries (nothing repeats).
+static void gpat_free(pd_ctx* c) {
+    for (void* p : {(void*)c->gpat_id, (void*)c->gpat_ptr, (void*)c->gpat_off, (void*)c->cpat, (void*)c->cscale,
+                    (void*)c->cd16})
+        dfree(c, p);
     c->gpat_id = nullptr;
     c->gpat_ptr = nullptr;
     c->gpat_off = nullptr;
+    c->cpat = nullptr;
+    c->cscale = nullptr;
+    c->cd16 = nullptr;
+    c->have_gpat = c->have_delta = false;
     c->d.gpat_id = nullptr;
     c->d.gpat_ptr = nullptr;
     c->d.gpat_off = nullptr;
+    c->d.cpat = nullptr;
+    c->d.cscale = nullptr;
+    c->d.cd16 = nullptr;
     c->generation++;
-    if (!c->gpat_opt || !c->have_mls || !c->d.mls || c->n == 0) return PD_OK;
+}
+
+// the patterns are read by the gathers only while PD_OPT_GATHER_STENCIL is on
+static void gpat_apply(pd_ctx* c) {
+    const bool on = c->gpat_opt && c->have_gpat;
+    c->d.gpat_id = on ? c->gpat_id : nullptr;
+    c->d.gpat_ptr = on ? c->gpat_ptr : nullptr;
+    c->d.gpat_off = on ? c->gpat_off : nullptr;
+    c->generation++;
+}
+
+// The delta form of the FP32 coefficients (2x2x2 points; see k_delta_build):
+// a node whose coefficients stray more than 2^-10 from its pattern
+// representative's gets a pattern of its own.  On success coeff32 holds
+// cpat + scale * delta for every coefficient.
+static int delta_build(pd_ctx* c, std::vector<int32_t>& pid, std::vector<int64_t>& ptr, std::vector<int32_t>& off,
+                       size_t max_entries) {
+    const int64_t N = c->n;
+    const int32_t P0 = (int32_t)(ptr.size() - 1);
+    std::vector<int32_t> rep((size_t)P0, -1);
+    for (int64_t i = 0; i < N; ++i)
+        if (rep[pid[i]] < 0) rep[pid[i]] = (int32_t)i;
+    int32_t *dpid = nullptr, *drep = nullptr;
+    int64_t* dptr = nullptr;
+    uint8_t* dfar = nullptr;
+    auto cleanup = [&]() { dfree(c, dpid); dfree(c, drep); dfree(c, dptr); dfree(c, dfar); };
+    int rc = PD_OK;
+    if ((rc = dalloc(c, &dpid, (size_t)N)) || (rc = dalloc(c, &drep, rep.size() + (size_t)N)) ||
+        (rc = dalloc(c, &dfar, (size_t)N)) || (rc = upload(c, dpid, pid.data(), sizeof(int32_t) * N)) ||
+        (rc = upload(c, drep, rep.data(), sizeof(int32_t) * rep.size()))) {
+        cleanup();
+        return rc;
+    }
+    pd::launch_delta_check(c->d, dpid, drep, dfar, c->stream);
+    std::vector<uint8_t> far((size_t)N);
+    if (cudaMemcpyAsync(far.data(), dfar, N, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        cleanup();
+        return fail(PD_ERR_CUDA, "delta form: check");
+    }
+    for (int64_t i = 0; i < N; ++i) {
+        if (!far[i]) continue;
+        const int64_t b = c->cbptr_host[i], e = c->cbptr_host[i + 1];
+        if (off.size() + (size_t)(e - b) > max_entries) {
+            cleanup();
+            return PD_ERR_CAPACITY;  // too irregular: no delta form
+        }
+        pid[i] = (int32_t)(ptr.size() - 1);
+        rep.push_back((int32_t)i);
+        for (int64_t k = b; k < e; ++k) off.push_back(c->cbidx_host[k] - (int32_t)i);
+        ptr.push_back((int64_t)off.size());
+    }
+    const size_t T = (size_t)c->cbptr_host[N];
+    if ((rc = upload(c, dpid, pid.data(), sizeof(int32_t) * N)) ||
+        (rc = upload(c, drep, rep.data(), sizeof(int32_t) * rep.size())) || (rc = dalloc(c, &dptr, ptr.size())) ||
+        (rc = upload(c, dptr, ptr.data(), sizeof(int64_t) * ptr.size())) ||
+        (rc = dalloc(c, &c->cpat, std::max<size_t>(off.size(), 1) * 8)) ||
+        (rc = dalloc(c, &c->cscale, (size_t)N * 8)) || (rc = dalloc(c, &c->cd16, std::max<size_t>(T, 1) * 8))) {
+        cleanup();
+        return rc;
+    }
+    pd::launch_delta_build(c->d, dpid, dptr, drep, c->cpat, c->cscale, c->cd16, c->coeff32, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cleanup();
+    if (e != cudaSuccess) return pd::fail_cuda(e, "delta form: build", __FILE__, __LINE__);
+    c->d.cpat = c->cpat;
+    c->d.cscale = c->cscale;
+    c->d.cd16 = c->cd16;
+    c->have_delta = true;
+    return PD_OK;
+}
+
+// the MLS data and what is derived from them, freed
+static void mls_release(pd_ctx* c) {
+    for (void* p : {(void*)c->tptr, (void*)c->tj, (void*)c->tpos, (void*)c->cbptr, (void*)c->cbidx, (void*)c->coeff,
+                    (void*)c->coeff32, (void*)c->csum})
+        dfree(c, p);
+    c->tptr = nullptr;
+    c->tj = c->tpos = nullptr;
+    c->cbptr = nullptr;
+    c->cbidx = nullptr;
+    c->coeff = nullptr;
+    c->coeff32 = c->csum = nullptr;
+    c->d.cbptr = nullptr;
+    c->d.cbidx = nullptr;
+    c->d.coeff = nullptr;
+    c->d.coeff32 = c->d.csum = nullptr;
+    c->have_mls = false;
+    c->generation++;
+}
+
+static int gpat_build(pd_ctx* c);
+
+// after new MLS data: the patterns, the delta form and the SELL copy
+static int mls_installed(pd_ctx* c) {
+    c->d.cbptr = c->cbptr;
+    c->d.cbidx = c->cbidx;
+    c->d.coeff = c->coeff;
+    c->d.coeff32 = c->coeff32;
+    c->d.csum = c->csum;
+    c->have_mls = true;
+    c->generation++;
+    PD_TRY(gpat_build(c));
+    if (!c->have_gpat) c->gpat_opt = 0;  // the new lists do not repeat: plain lists
+    if (!c->have_delta) c->d.gather_delta = 0;
+    gpat_apply(c);
+    return sell_prepare(c);
+}
+
+static int gpat_build(pd_ctx* c) {
+    gpat_free(c);
+    if (!c->have_mls || !c->d.mls || c->n == 0) return PD_OK;
     const int64_t N = c->n;
     const std::vector<int64_t>& cp = c->cbptr_host;
     const std::vector<int32_t>& ci = c->cbidx_host;
@@ -657,8 +794,7 @@ static int gpat_prepare(pd_ctx* c) {
             }
         }
         if (found < 0) {
-            if (off.size() + (size_t)(e - b) > kMaxEntries)
-                return fail(PD_ERR_ARG, "pd_set_option: the MLS contributor lists do not repeat (no patterns)");
+            if (off.size() + (size_t)(e - b) > kMaxEntries) return PD_OK;  // the lists do not repeat
             found = (int32_t)(ptr.size() - 1);
             for (int64_t k = b; k < e; ++k) off.push_back(ci[k] - (int32_t)i);
             ptr.push_back((int64_t)off.size());
@@ -666,15 +802,27 @@ static int gpat_prepare(pd_ctx* c) {
         }
         pid[i] = found;
     }
+    if (c->npt == 8) {
+        const int rc = delta_build(c, pid, ptr, off, kMaxEntries);
+        if (rc != PD_OK && rc != PD_ERR_CAPACITY) return rc;
+        if (rc == PD_ERR_CAPACITY) {  // no delta form: the plain FP32 coefficients stay
+            for (void* p : {(void*)c->cpat, (void*)c->cscale, (void*)c->cd16}) dfree(c, p);
+            c->cpat = nullptr;
+            c->cscale = nullptr;
+            c->cd16 = nullptr;
+            c->d.cpat = c->d.cscale = nullptr;
+            c->d.cd16 = nullptr;
+            c->have_delta = false;
+        }
+    }
     PD_TRY(dalloc(c, &c->gpat_id, (size_t)N));
     PD_TRY(dalloc(c, &c->gpat_ptr, ptr.size()));
     PD_TRY(dalloc(c, &c->gpat_off, std::max<size_t>(off.size(), 1)));
     PD_TRY(upload(c, c->gpat_id, pid.data(), sizeof(int32_t) * pid.size()));
     PD_TRY(upload(c, c->gpat_ptr, ptr.data(), sizeof(int64_t) * ptr.size()));
     if (!off.empty()) PD_TRY(upload(c, c->gpat_off, off.data(), sizeof(int32_t) * off.size()));
-    c->d.gpat_id = c->gpat_id;
-    c->d.gpat_ptr = c->gpat_ptr;
-    c->d.gpat_off = c->gpat_off;
+    c->have_gpat = true;
+    gpat_apply(c);
     return PD_OK;
 }
 
@@ -682,12 +830,15 @@ static int gpat_prepare(pd_ctx* c) {
 static void fsten_release(pd_ctx* c) {
     dfree(c, c->fst_u2);
     dfree(c, c->fst_mask);
+    dfree(c, c->fst_tab);
     c->fst_u2 = nullptr;
     c->fst_mask = nullptr;
+    c->fst_tab = nullptr;
     c->fst_shape = 0;
     c->d.blk_cm = 0;
     c->d.sten_u2 = nullptr;
     c->d.sten_mask = nullptr;
+    c->d.sten_tab = nullptr;
     c->d.sten_nu = c->d.sten_nw = 0;
     c->d.sten_np = 0;
     c->generation++;
@@ -778,7 +929,8 @@ static int fsten_prepare(pd_ctx* c, int shape) {
     int* dlut = nullptr;
     int rc = PD_OK;
     if ((rc = dalloc(c, &c->fst_u2, std::max<size_t>(u2.size(), 1))) ||
-        (rc = dalloc(c, &c->fst_mask, (size_t)2 * nw * np)) || (rc = dalloc(c, &dlut, lut.size())))
+        (rc = dalloc(c, &c->fst_mask, (size_t)2 * nw * np)) || (rc = dalloc(c, &dlut, lut.size())) ||
+        (rc = dalloc(c, &c->fst_tab, (size_t)8 * nu)))
         return done(rc);
     auto done2 = [&](int r) {
         dfree(c, dlut);
@@ -799,6 +951,10 @@ static int fsten_prepare(pd_ctx* c, int shape) {
         cudaStreamSynchronize(c->stream) != cudaSuccess)
         return done2(fail(PD_ERR_CUDA, "stencil force: masks"));
     if (err) return done2(fail(PD_ERR_ARG, "pd_set_option: a family does not map onto the lattice stencil"));
+    t.sten_tab = c->fst_tab;
+    if ((rc = pd::launch_sten_table(t, c->fst_tab, c->stream)) != PD_OK ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return done2(fail(PD_ERR_CUDA, "stencil force: geometry table"));
     t.blk_cm = 1;
     t.sten_by = kBy[shape];
     t.sten_bz = 8 / kBy[shape];
@@ -960,10 +1116,7 @@ int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const do
     }
     c->cbptr_host.assign(cb_ptr, cb_ptr + N + 1);
     c->cbidx_host.assign(cb_idx, cb_idx + T);
-    dfree(c, c->tptr); dfree(c, c->tj); dfree(c, c->tpos);
-    c->tptr = nullptr; c->tj = nullptr; c->tpos = nullptr;
-    dfree(c, c->cbptr); dfree(c, c->cbidx); dfree(c, c->coeff); dfree(c, c->coeff32); dfree(c, c->csum);
-    c->cbptr = nullptr; c->cbidx = nullptr; c->coeff = nullptr; c->coeff32 = nullptr; c->csum = nullptr;
+    mls_release(c);
     PD_TRY(dalloc(c, &c->cbptr, N + 1));
     PD_TRY(dalloc(c, &c->cbidx, T));
     PD_TRY(dalloc(c, &c->coeff, (size_t)T * npt));
@@ -974,15 +1127,89 @@ int pd_set_mls(pd_ctx* c, const int64_t* cb_ptr, const int32_t* cb_idx, const do
     if (T) PD_TRY(upload(c, c->coeff, co.data(), sizeof(double) * co.size()));
     if (T) PD_TRY(upload(c, c->coeff32, co32.data(), sizeof(float) * co32.size()));
     PD_TRY(upload(c, c->csum, cs.data(), sizeof(float) * cs.size()));
-    c->d.cbptr = c->cbptr;
-    c->d.cbidx = c->cbidx;
-    c->d.coeff = c->coeff;
-    c->d.coeff32 = c->coeff32;
-    c->d.csum = c->csum;
-    c->have_mls = true;
-    c->generation++;
-    if (gpat_prepare(c) != PD_OK) c->gpat_opt = 0;  // the new lists do not repeat: plain lists
-    return sell_prepare(c);
+    return mls_installed(c);
+}
+
+// The MLS data of InitIntegrationPoint computed on the device (k_mls_contrib,
+// k_mls_coeff) from the context's family and coordinates, or from the given
+// MLS coordinates (a batch: every specimen in its own frame).
+int pd_mls_setup(pd_ctx* c, double rw, const double* mls_coords, int64_t* num_contrib) {
+    if (!c) return fail(PD_ERR_ARG, "pd_mls_setup: null context");
+    if (!c->d.mls || c->d.cci) return fail(PD_ERR_ARG, "pd_mls_setup: MLS is off for this integration scheme");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_mls_setup: no family (pd_bond_search or pd_set_family first)");
+    if (!(rw > 0.0) || c->abscis.empty()) return fail(PD_ERR_ARG, "pd_mls_setup: support size or Gauss rule");
+    const int64_t N = c->n;
+    const int n1 = (int)c->abscis.size();
+    mls_release(c);
+    double *xm = nullptr, *dab = nullptr;
+    int64_t* cnt = nullptr;
+    auto cleanup = [&]() { dfree(c, xm); dfree(c, dab); dfree(c, cnt); };
+    int rc = PD_OK;
+    if ((rc = dalloc(c, &cnt, (size_t)std::max<int64_t>(N, 1))) || (rc = dalloc(c, &dab, (size_t)n1)) ||
+        (rc = dalloc(c, &c->cbptr, (size_t)N + 1)) || (rc = upload(c, dab, c->abscis.data(), sizeof(double) * n1))) {
+        cleanup();
+        return rc;
+    }
+    const double* xsrc = c->d.x;
+    if (mls_coords) {
+        if ((rc = dalloc(c, &xm, (size_t)(3 * N))) || (rc = upload_vec3(c, xm, mls_coords))) {
+            cleanup();
+            return rc;
+        }
+        xsrc = xm;
+    }
+    struct Alloc {
+        static void* fn(void* ctx, size_t bytes) {
+            char* p = nullptr;
+            return dalloc(static_cast<pd_ctx*>(ctx), &p, bytes) == PD_OK ? (void*)p : nullptr;
+        }
+    };
+    int64_t T = 0, bad = -1;
+    rc = pd::mls_setup(c->d, xsrc, rw, dab, n1, cnt, c->cbptr, &c->cbidx, &c->coeff, &c->coeff32, &c->csum, &T, &bad,
+                       &Alloc::fn, c, c->stream);
+    cleanup();
+    if (rc == PD_ERR_SINGULAR) {
+        mls_release(c);
+        const std::string msg =
+            "pdMatrix::Gauss: Singular Matrix (MLS moment matrix of node " + std::to_string(bad) + ")";
+        return fail(PD_ERR_SINGULAR, msg.c_str());
+    }
+    if (rc != PD_OK) {
+        mls_release(c);
+        return fail(rc, "pd_mls_setup: device setup failed");
+    }
+    c->cbptr_host.resize((size_t)N + 1);
+    c->cbidx_host.resize((size_t)T);
+    PD_CUDA_TRY(cudaMemcpy(c->cbptr_host.data(), c->cbptr, sizeof(int64_t) * (N + 1), cudaMemcpyDeviceToHost));
+    if (T) PD_CUDA_TRY(cudaMemcpy(c->cbidx_host.data(), c->cbidx, sizeof(int32_t) * T, cudaMemcpyDeviceToHost));
+    if (num_contrib) *num_contrib = T;
+    return mls_installed(c);
+}
+
+// The MLS data out, in the layout pd_set_mls takes (coeff [node][point][contributor]).
+int pd_get_mls(pd_ctx* c, int64_t* cb_ptr, int32_t* cb_idx, double* coeff) {
+    if (!c || !cb_ptr) return fail(PD_ERR_ARG, "pd_get_mls: null argument");
+    if (!c->have_mls) return fail(PD_ERR_ARG, "pd_get_mls: no MLS data");
+    const int64_t N = c->n, T = c->cbptr_host.empty() ? 0 : c->cbptr_host[N];
+    const int npt = c->npt;
+    std::memcpy(cb_ptr, c->cbptr_host.data(), sizeof(int64_t) * (N + 1));
+    if (cb_idx && T) std::memcpy(cb_idx, c->cbidx_host.data(), sizeof(int32_t) * T);
+    if (coeff && T) {
+        std::vector<double> co((size_t)T * npt);
+        PD_CUDA_TRY(cudaMemcpy(co.data(), c->coeff, sizeof(double) * co.size(), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < N; ++i) {
+            const int64_t b = c->cbptr_host[i], nc = c->cbptr_host[i + 1] - b;
+            for (int64_t k = 0; k < nc; ++k)
+                for (int g = 0; g < npt; ++g) coeff[b * npt + (int64_t)g * nc + k] = co[(b + k) * npt + g];
+        }
+    }
+    return PD_OK;
+}
+
+int pd_mls_size(pd_ctx* c, int64_t* num_contrib) {
+    if (!c || !num_contrib) return fail(PD_ERR_ARG, "pd_mls_size: null argument");
+    *num_contrib = c->have_mls && !c->cbptr_host.empty() ? c->cbptr_host[c->n] : 0;
+    return PD_OK;
 }
 
 int pd_set_precision(pd_ctx* c, int p) {
@@ -1034,13 +1261,22 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             break;
         case PD_OPT_GATHER_STENCIL:
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
-            if ((int)value != c->gpat_opt) {
-                c->gpat_opt = (int)value;
-                const int rc = gpat_prepare(c);
-                if (rc != PD_OK) {
-                    c->gpat_opt = 0;
-                    return rc;
-                }
+            if (value && !c->have_gpat)
+                return fail(PD_ERR_ARG, "pd_set_option: the MLS contributor lists do not repeat (no patterns)");
+            c->gpat_opt = (int)value;
+            gpat_apply(c);
+            break;
+        case PD_OPT_STATIC_PRECOND:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            c->static_precond = (int)value;
+            break;
+        case PD_OPT_GATHER_DELTA:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            if (value && !c->have_delta)
+                return fail(PD_ERR_ARG, "pd_set_option: no delta form of the coefficients (2x2x2 points, patterns)");
+            if ((int)value != c->d.gather_delta) {
+                c->d.gather_delta = (int)value;
+                c->generation++;
             }
             break;
         case PD_OPT_FORCE_STENCIL:
@@ -1112,6 +1348,8 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_GATHER_SELL: *value = c->d.sell_on; return PD_OK;
         case PD_OPT_FORCE_STENCIL: *value = c->fst_shape; return PD_OK;
         case PD_OPT_GATHER_STENCIL: *value = c->gpat_opt; return PD_OK;
+        case PD_OPT_GATHER_DELTA: *value = c->d.gather_delta; return PD_OK;
+        case PD_OPT_STATIC_PRECOND: *value = c->static_precond; return PD_OK;
         case PD_OPT_PERSIST_WAIT_US: *value = c->persist_wait_us; return PD_OK;
         case PD_OPT_PERSIST_TEST_STALL: *value = c->persist_stall; return PD_OK;
         default: return fail(PD_ERR_ARG, "pd_get_option: unknown option");
@@ -1543,16 +1781,18 @@ int pd_static_rhs(pd_ctx* c, double time, double* b) {
 
 namespace {
 
-// CG on K x = b with FP64 vectors and device scalars; the residual is read
-// back every 10 iterations.  f32: the matvec of the iterations has FP32 bond
-// terms, and the residual is replaced by the FP64 true residual b - K x
-// whenever the recurred one has fallen by 1e-2 since the last replacement
-// and when it reaches the tolerance ("reliable updates", van der Vorst & Ye,
-// SIAM J. Sci. Comput. 22 (2000) 1716-1731): the FP64 refinement of the
-// FP32 iterations, without restarting the Krylov space.  Convergence is
-// decided on the true residual.
-int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, double* p, double* q, bool f32,
-              double rtol, int maxit, int* iters, double* relres, int* replacements) {
+// Preconditioned CG on K x = b with FP64 vectors and device scalars; the
+// residual is read back every 10 iterations.  minv: the block-Jacobi
+// preconditioner (3x3 diagonal blocks, k_static_bjacobi), or null for plain
+// CG.  f32: the matvec of the iterations has FP32 bond terms, and the
+// residual is replaced by the FP64 true residual b - K x whenever the
+// recurred one has fallen by 1e-2 since the last replacement and when it
+// reaches the tolerance ("reliable updates", van der Vorst & Ye, SIAM J. Sci.
+// Comput. 22 (2000) 1716-1731): the FP64 refinement of the FP32 iterations,
+// without restarting the Krylov space.  Convergence is decided on the true
+// residual.  scal: CG_RR = r.z, CG_RRN = the next r.z, CG_RES = r.r.
+int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, double* p, double* q, double* z,
+              const double* minv, bool f32, double rtol, int maxit, int* iters, double* relres, int* replacements) {
     const int64_t n3 = 3 * c->n;
     cudaStream_t s = c->stream;
     double* scal = c->scal;
@@ -1561,22 +1801,29 @@ int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, dou
     };
     auto read = [&]() -> int {
         PD_CUDA_TRY(cudaGetLastError());
-        PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+        PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, scal, sizeof(double) * 5, cudaMemcpyDeviceToHost, s));
         PD_CUDA_TRY(cudaStreamSynchronize(s));
         return PD_OK;
     };
-    // true residual into r, |r|^2 into scal[CG_RR]
+    // z = M^-1 r (z aliases r without a preconditioner) and r.z into slot
+    const double* zz = minv ? z : r;
+    auto precond = [&](double* slot) {
+        if (minv) pd::launch_bj_apply(minv, r, z, c->n, s);
+        dot(r, zz, slot);
+    };
+    // true residual into r, |r|^2 into scal[CG_RES], r.z into scal[CG_RR]
     auto true_residual = [&]() {
         static_apply(c, time, false, x, q);
         pd::launch_sub_f64(b, q, r, n3, s);
-        dot(r, r, scal + pd::CG_RR);
+        dot(r, r, scal + pd::CG_RES);
+        precond(scal + pd::CG_RR);
     };
     dot(b, b, scal + pd::CG_BB);
     true_residual();
-    PD_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    PD_CUDA_TRY(cudaMemcpyAsync(p, zz, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     PD_TRY(read());
     const double bb = c->hscalar[pd::CG_BB] > 0.0 ? c->hscalar[pd::CG_BB] : 1.0;
-    double rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+    double rel = std::sqrt(c->hscalar[pd::CG_RES] / bb);
     double since = rel;  // largest recurred residual since the last replacement
     int it = 0, nrep = 0;
     const int check = 10;
@@ -1585,19 +1832,20 @@ int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, dou
             static_apply(c, time, f32, p, q);
             dot(p, q, scal + pd::CG_PQ);
             pd::launch_cg_update_x_f64(x, r, p, q, n3, scal, s);
-            dot(r, r, scal + pd::CG_RRN);
-            pd::launch_cg_update_p_f64(r, p, n3, scal, s);
+            precond(scal + pd::CG_RRN);
+            pd::launch_cg_update_p_f64(zz, p, n3, scal, s);
             pd::launch_cg_swap(scal, s);
         }
+        dot(r, r, scal + pd::CG_RES);
         PD_TRY(read());
-        rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+        rel = std::sqrt(c->hscalar[pd::CG_RES] / bb);
         if (!std::isfinite(rel)) break;
         since = std::max(since, rel);
         if (f32 && (rel <= rtol || rel < 1e-2 * since)) {
             // replace: r = b - K x in FP64; p keeps its direction
             true_residual();
             PD_TRY(read());
-            rel = std::sqrt(c->hscalar[pd::CG_RR] / bb);
+            rel = std::sqrt(c->hscalar[pd::CG_RES] / bb);
             since = rel;
             ++nrep;
         }
@@ -1620,19 +1868,26 @@ extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rto
         return fail(PD_ERR_ARG, "pd_static_solve: precision");
     PD_TRY(static_prepare(c));
     const int64_t n3 = 3 * c->n;
-    double *b = nullptr, *xd = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    double *b = nullptr, *xd = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr;
     PD_TRY(dalloc(c, &b, n3));
     PD_TRY(dalloc(c, &xd, n3));
     PD_TRY(dalloc(c, &r, n3));
     PD_TRY(dalloc(c, &p, n3));
     PD_TRY(dalloc(c, &q, n3));
-    auto cleanup = [&]() { dfree(c, b); dfree(c, xd); dfree(c, r); dfree(c, p); dfree(c, q); };
+    if (c->static_precond) PD_TRY(dalloc(c, &z, n3));
+    auto cleanup = [&]() { dfree(c, b); dfree(c, xd); dfree(c, r); dfree(c, p); dfree(c, q); dfree(c, z); };
     int rc = upload_vec3(c, xd, x);
     if (rc != PD_OK) { cleanup(); return rc; }
+    if (c->static_precond && (!c->bj_minv || c->bj_gen != c->generation)) {
+        if (!c->bj_minv && (rc = dalloc(c, &c->bj_minv, (size_t)(6 * c->n))) != PD_OK) { cleanup(); return rc; }
+        pd::launch_static_bjacobi(c->d, c->bj_minv, c->stream);
+        c->bj_gen = c->generation;
+    }
     pd::launch_static_rhs(c->d, time, b, c->stream);
     int it = 0, nrep = 0;
     double rel = 0.0;
-    rc = cg_static(c, time, b, xd, r, p, q, precision == PD_PREC_FP32C, rtol, maxit, &it, &rel, &nrep);
+    rc = cg_static(c, time, b, xd, r, p, q, z, c->static_precond ? c->bj_minv : nullptr,
+                   precision == PD_PREC_FP32C, rtol, maxit, &it, &rel, &nrep);
     c->static_replacements = nrep;
     int rc2 = download_vec3(c, x, xd);
     cleanup();
@@ -2141,9 +2396,26 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
                 }
             if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, ks)) != PD_OK) return done(rc);
             if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, kp)) != PD_OK) return done(rc);
+            if (c->have_delta) {
+                // the coefficient ring on the delta form, with both on
+                const int d0 = c->d.gather_delta;
+                const int s1 = c->d.sell_on, p1 = c->gpat_opt;
+                if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, 1)) != PD_OK) return done(rc);
+                if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, 1)) != PD_OK) return done(rc);
+                if ((rc = pd_set_option(c, PD_OPT_GATHER_DELTA, 1)) != PD_OK) return done(rc);
+                const double prev = best.ms;
+                Trial T3{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
+                if ((rc = trial(T3)) != PD_OK) return done(rc);
+                if (!(best.ms < prev)) {
+                    if ((rc = pd_set_option(c, PD_OPT_GATHER_DELTA, d0)) != PD_OK) return done(rc);
+                    if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, s1)) != PD_OK) return done(rc);
+                    if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, p1)) != PD_OK) return done(rc);
+                }
+            }
         }
         out->gather_sell = c->d.sell_on;
         out->gather_stencil = c->gpat_opt;
+        out->gather_delta = c->d.gather_delta;
     }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.multimat) {
         // the lattice-stencil force in each block shape, on the best shape so far

@@ -6,6 +6,7 @@
 // one node and sums its family in ascending id order, which is the order of
 // the reference's loops, so the force, gather and state vectors are bit-for-
 // bit those of the reference CPU path (pdDataManager.cpp:1767-2134).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -457,6 +458,247 @@ void launch_energy_reduce(const Dev& d, cudaStream_t s) {
     double* part = d.red + 2 * d.n + 2;
     k_energy_partial<<<nb, 256, 0, s>>>(d.red, d.n, part);
     k_energy_final<<<1, 32, 0, s>>>(part, nb, d.red + 2 * d.n);
+}
+
+// ============================================================ MLS setup
+//
+// InitIntegrationPoint (pdDataManager2.cpp:118-256) on the device: the
+// contributor lists and the coefficients of every Gauss point, in the
+// reference's operation order (this unit is compiled with -fmad=false).  The
+// one difference: the spline weight's d^3 and d^4, which the reference takes
+// from glibc's pow, are rounded once here (Dekker's exact product, formed with
+// FMA), and glibc's pow is off the correctly rounded value for about 4 in
+// 10,000 arguments; through the ill-conditioned moment matrix (global
+// coordinates) such a weight moves the coefficients by round-off amplified
+// like the reference's own (1e-10..1e-5 of the largest coefficient).
+
+__device__ __forceinline__ double cube_rn(double d) {
+    const double p = d * d, ep = fma(d, d, -p);  // d^2 = p + ep exactly
+    const double h = p * d, eh = fma(p, d, -h);  // p d = h + eh exactly
+    return h + (eh + ep * d);
+}
+
+__device__ __forceinline__ double quart_rn(double d) {
+    const double p = d * d, ep = fma(d, d, -p);
+    const double q = p * p, eq = fma(p, p, -q);  // d^4 = q + eq + 2 p ep + ep^2
+    return q + (eq + 2.0 * p * ep);
+}
+
+// quadratic basis in global coordinates, pdDataManager2.cpp:1547-1563
+__device__ __forceinline__ void mls_basis(double q0, double q1, double q2, double* p) {
+    p[0] = 1.0;
+    p[1] = q0;
+    p[2] = q1;
+    p[3] = q2;
+    p[4] = q0 * q1;
+    p[5] = q0 * q2;
+    p[6] = q1 * q2;
+    p[7] = q0 * q0;
+    p[8] = q1 * q1;
+    p[9] = q2 * q2;
+}
+
+// quartic spline of |q - node| / rw, pdDataManager2.cpp:1565-1578
+__device__ __forceinline__ double mls_weight(double n0, double n1, double n2, double q0, double q1, double q2,
+                                             double rw) {
+    const double e1 = q0 - n0, e2 = q1 - n1, e3 = q2 - n2;
+    const double r = sqrt(e1 * e1 + e2 * e2 + e3 * e3);
+    const double d = r / rw;
+    if (d > 1.0) return 0.0;
+    return (1 - 6.0 * d * d + 8.0 * cube_rn(d) - 3.0 * quart_rn(d));
+}
+
+// contributors: the node, then its family members (ascending id) within rw,
+// or within 1.5 rw when fewer than 10 qualify (pdDataManager2.cpp:118-171)
+template <bool FILL>
+__global__ void k_mls_contrib(Dev d, const double* __restrict__ xm, double rw, int64_t* __restrict__ cnt,
+                              const int64_t* __restrict__ cbptr, int32_t* __restrict__ cbidx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int64_t N = d.n;
+    const double x0 = xm[i], x1 = xm[N + i], x2 = xm[2 * N + i];
+    double radius = rw;
+    int64_t c = 1;
+    for (int pass = 0; pass < 2; ++pass) {
+        radius = pass == 0 ? rw : rw * 1.5;
+        c = 1;
+        for (int64_t p = d.frow[i]; p < d.frow[i + 1]; ++p) {
+            const int64_t j = d.fcol[p];
+            const double d1 = xm[j] - x0, d2 = xm[N + j] - x1, d3 = xm[2 * N + j] - x2;
+            if (sqrt(d1 * d1 + d2 * d2 + d3 * d3) <= radius) ++c;
+        }
+        if (c >= 10) break;
+    }
+    if (!FILL) {
+        cnt[i] = c;
+        return;
+    }
+    int64_t o = cbptr[i];
+    cbidx[o++] = (int32_t)i;
+    for (int64_t p = d.frow[i]; p < d.frow[i + 1]; ++p) {
+        const int64_t j = d.fcol[p];
+        const double d1 = xm[j] - x0, d2 = xm[N + j] - x1, d3 = xm[2 * N + j] - x2;
+        if (sqrt(d1 * d1 + d2 * d2 + d3 * d3) <= radius) cbidx[o++] = (int32_t)j;
+    }
+}
+
+// One thread per (node, Gauss point): the 10x10 moment matrix sum_k w_k p_k
+// p_k^T (held in shared memory, entry-major so that a warp's accesses hit
+// distinct banks), the full-pivot Gauss-Jordan solve of pdMatrix::Gauss
+// (pdMatrix.cpp:251-391) for A s = p(x_g), and coeff_k = w_k p_k^T s, laid
+// out [node][contributor][point].  A singular matrix records its node in *bad.
+__global__ void __launch_bounds__(128) k_mls_coeff(Dev d, const double* __restrict__ xm, double rw,
+                                                   const double* __restrict__ absc, int n1,
+                                                   const int64_t* __restrict__ cbptr,
+                                                   const int32_t* __restrict__ cbidx, double* __restrict__ coeff,
+                                                   unsigned long long* __restrict__ bad) {
+    extern __shared__ double smA[];
+    const int bs = blockDim.x, tl = threadIdx.x;
+    const int npt = n1 * n1 * n1;
+    const int64_t t = blockIdx.x * (int64_t)bs + tl;
+    if (t >= d.n * npt) return;
+    const int64_t N = d.n;
+    const int64_t i = t / npt;
+    const int g = (int)(t - i * npt);
+    const int gi = g / (n1 * n1), gj = (g / n1) % n1, gk = g % n1;
+    const double q0 = 0.5 * d.dx * absc[gi] + xm[i];
+    const double q1 = 0.5 * d.dx * absc[gj] + xm[N + i];
+    const double q2 = 0.5 * d.dx * absc[gk] + xm[2 * N + i];
+#define PD_A(r, c) smA[((r) * 10 + (c)) * bs + tl]
+    for (int k = 0; k < 100; ++k) smA[k * bs + tl] = 0.0;
+    const int64_t b = cbptr[i], nc = cbptr[i + 1] - b;
+    for (int64_t k = 0; k < nc; ++k) {
+        const int64_t m = cbidx[b + k];
+        double e[10];
+        mls_basis(xm[m], xm[N + m], xm[2 * N + m], e);
+        const double w = mls_weight(xm[m], xm[N + m], xm[2 * N + m], q0, q1, q2, rw);
+        for (int r = 0; r < 10; ++r) {
+            const double wr = w * e[r];
+            for (int c = 0; c < 10; ++c) PD_A(r, c) = PD_A(r, c) + wr * e[c];
+        }
+    }
+    double s[10];
+    mls_basis(q0, q1, q2, s);
+    int piv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool ok = true;
+    for (int step = 0; step < 10 && ok; ++step) {
+        double big = 0.0;
+        int prow = 0, pcol = 0;
+        for (int r = 0; r < 10 && ok; ++r) {
+            if (piv[r] == 1) continue;
+            for (int c = 0; c < 10; ++c) {
+                if (piv[c] == 0) {
+                    if (fabs(PD_A(r, c)) >= big) {
+                        big = fabs(PD_A(r, c));
+                        prow = r;
+                        pcol = c;
+                    }
+                } else if (piv[c] > 1) {
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        if (!ok) break;
+        ++piv[pcol];
+        if (prow != pcol) {
+            for (int c = 0; c < 10; ++c) {
+                const double tmp = PD_A(prow, c);
+                PD_A(prow, c) = PD_A(pcol, c);
+                PD_A(pcol, c) = tmp;
+            }
+            const double tmp = s[prow];
+            s[prow] = s[pcol];
+            s[pcol] = tmp;
+        }
+        if (PD_A(pcol, pcol) == 0.0) {
+            ok = false;
+            break;
+        }
+        const double inv = 1.0 / PD_A(pcol, pcol);
+        PD_A(pcol, pcol) = 1.0;
+        for (int c = 0; c < 10; ++c) PD_A(pcol, c) = PD_A(pcol, c) * inv;
+        s[pcol] = s[pcol] * inv;
+        for (int r = 0; r < 10; ++r) {
+            if (r == pcol) continue;
+            const double mm = PD_A(r, pcol);
+            PD_A(r, pcol) = 0.0;
+            for (int c = 0; c < 10; ++c) PD_A(r, c) = PD_A(r, c) - PD_A(pcol, c) * mm;
+            s[r] = s[r] + -mm * s[pcol];
+        }
+    }
+#undef PD_A
+    if (!ok) {
+        atomicMin(bad, (unsigned long long)i);
+        for (int64_t k = 0; k < nc; ++k) coeff[(b + k) * npt + g] = 0.0;
+        return;
+    }
+    for (int64_t k = 0; k < nc; ++k) {
+        const int64_t m = cbidx[b + k];
+        double e[10];
+        mls_basis(xm[m], xm[N + m], xm[2 * N + m], e);
+        const double w = mls_weight(xm[m], xm[N + m], xm[2 * N + m], q0, q1, q2, rw);
+        double sum = 0.0;
+        for (int r = 0; r < 10; ++r) sum += (e[r] * w) * s[r];
+        coeff[(b + k) * npt + g] = sum;
+    }
+}
+
+// partition-of-unity defect sum_k c_k - 1 per (node, point), and the FP32
+// copy of the coefficients
+__global__ void k_mls_finish(Dev d, int npt, const int64_t* __restrict__ cbptr, const double* __restrict__ coeff,
+                             float* __restrict__ coeff32, float* __restrict__ csum) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= d.n * npt) return;
+    const int64_t i = t / npt;
+    const int g = (int)(t - i * npt);
+    double sum = 0.0;
+    for (int64_t k = cbptr[i]; k < cbptr[i + 1]; ++k) {
+        const double v = coeff[k * npt + g];
+        coeff32[k * npt + g] = (float)v;
+        sum += v;
+    }
+    csum[t] = (float)(sum - 1.0);
+}
+
+int mls_setup(const Dev& d, const double* xm, double rw, const double* absc, int n1, int64_t* cnt, int64_t* cbptr,
+              int32_t** cbidx, double** coeff, float** coeff32, float** csum, int64_t* total, int64_t* bad_node,
+              void* (*alloc)(void*, size_t), void* actx, cudaStream_t s) {
+    const int64_t N = d.n;
+    const int npt = n1 * n1 * n1;
+    *bad_node = -1;
+    if (N == 0) return PD_OK;
+    k_mls_contrib<false><<<(unsigned)((N + 127) / 128), 128, 0, s>>>(d, xm, rw, cnt, nullptr, nullptr);
+    if (exclusive_scan_i64(cnt, cbptr, N, s) != PD_OK) return PD_ERR_CUDA;
+    if (cudaMemcpyAsync(total, cbptr + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return PD_ERR_CUDA;
+    const int64_t T = *total;
+    *cbidx = (int32_t*)alloc(actx, sizeof(int32_t) * (size_t)std::max<int64_t>(T, 1));
+    *coeff = (double*)alloc(actx, sizeof(double) * (size_t)std::max<int64_t>(T * npt, 1));
+    *coeff32 = (float*)alloc(actx, sizeof(float) * (size_t)std::max<int64_t>(T * npt, 1));
+    *csum = (float*)alloc(actx, sizeof(float) * (size_t)(N * npt));
+    if (!*cbidx || !*coeff || !*coeff32 || !*csum) return PD_ERR_OOM;
+    k_mls_contrib<true><<<(unsigned)((N + 127) / 128), 128, 0, s>>>(d, xm, rw, nullptr, cbptr, *cbidx);
+    unsigned long long* dbad = reinterpret_cast<unsigned long long*>(cnt);  // the counts are no longer needed
+    const unsigned long long none = ~0ull;
+    if (cudaMemcpyAsync(dbad, &none, sizeof none, cudaMemcpyHostToDevice, s) != cudaSuccess) return PD_ERR_CUDA;
+    const int bs = 128;
+    const size_t smem = sizeof(double) * 100 * bs;
+    if (cudaFuncSetAttribute(k_mls_coeff, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return PD_ERR_CUDA;
+    k_mls_coeff<<<(unsigned)((N * npt + bs - 1) / bs), bs, smem, s>>>(d, xm, rw, absc, n1, cbptr, *cbidx, *coeff,
+                                                                      dbad);
+    k_mls_finish<<<(unsigned)((N * npt + 255) / 256), 256, 0, s>>>(d, npt, cbptr, *coeff, *coeff32, *csum);
+    unsigned long long hb = none;
+    if (cudaMemcpyAsync(&hb, dbad, sizeof hb, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return PD_ERR_CUDA;
+    if (hb != none) {
+        *bad_node = (int64_t)hb;
+        return PD_ERR_SINGULAR;
+    }
+    return cudaGetLastError() == cudaSuccess ? PD_OK : PD_ERR_CUDA;
 }
 
 void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s) {

@@ -57,71 +57,183 @@ struct PointPack {
     PointF p[NPT > 0 ? NPT : 1];
 };
 
+// FP32 operations with explicit rounding (round to nearest, denormals
+// flushed, never contracted), written once so that the scalar and the packed
+// code paths below round identically
+__device__ __forceinline__ float fadd(float a, float b) {
+    float d;
+    asm("add.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float fmul(float a, float b) {
+    float d;
+    asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float ffma(float a, float b, float c) {
+    float d;
+    asm("fma.rn.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Two FP32 values in one 64-bit register, and sm_100's packed FP32
+// arithmetic on them (one instruction for both lanes, each lane rounded as
+// the scalar operation above rounds)
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2_make(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_split(f2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// ---- per-point force of the FP32 form ----
+//
+// For a bond vector x (cell j's Gauss point minus node i) and relative
+// displacement e, with y = x + e, r = |x|, p = |y| and dd = p^2 - r^2 =
+// e.(2x + e) = e.(x + y), the point force of pdDataManager2.cpp:1320-1343 is
+//     f = W beta(r) s y / p,   s = (p - r) / r,
+// and W beta s / p = K h(eps) with K = W beta(r) / r and eps = dd / r^2:
+//     h(eps) = dd / ((p + r) p) = 1 - (1 + eps)^(-1/2).
+// K and 1/r^2 depend on the bond's lattice offset and the point only (pt_geo),
+// so the lattice kernels can take them from a table.  For |eps| < 1/64,
+// h is the binomial series eps (1/2 - 3/8 eps + 5/16 eps^2 - 35/128 eps^3),
+// whose truncation error is below 0.5 eps^4 relative (3e-8 at the bound, under
+// half an FP32 ulp); strains of 1e-5..1e-3 give eps of 2e-5..2e-3.  Larger
+// |eps| takes the exact form dd / ((p + r) p) with reciprocal square roots.
+// Every operation is written with an explicit rounding intrinsic, so that the
+// scalar kernels and the packed (two points per instruction) stencil kernel
+// round alike, and the forces of the eight points of a bond are summed in
+// two chains, the even points and the odd points, added at the end.
+// The critical-stretch test s > ecrit reads eps > ecrit (2 + ecrit).
+constexpr float kSeriesMax = 1.0f / 64.0f;
+constexpr float kH1 = 0.5f, kH2 = -0.375f, kH3 = 0.3125f, kH4 = -0.2734375f;
+
+__device__ __forceinline__ void pt_geo(const PointF& P, float x0, float x1, float x2, float& K, float& r2inv) {
+    const float r2 = ffma(x0, x0, ffma(x1, x1, fmul(x2, x2)));
+    const float rinv = rsqrtf(r2);
+    const float r = fmul(r2, rinv);
+    const float beta = __saturatef(fmul(fadd(P.A, -r), P.B));
+    K = fmul(fmul(P.W, beta), rinv);
+    r2inv = fmul(rinv, rinv);
+}
+
+__device__ __forceinline__ float pt_series(float eps) {
+    float c = ffma(eps, kH4, kH3);
+    c = ffma(eps, c, kH2);
+    c = ffma(eps, c, kH1);
+    return fmul(eps, c);
+}
+
+__device__ __forceinline__ float pt_exact(float x0, float x1, float x2, float dd) {
+    const float r2 = ffma(x0, x0, ffma(x1, x1, fmul(x2, x2)));
+    const float p2 = fadd(r2, dd);
+    const float pinv = rsqrtf(p2), rinv = rsqrtf(r2);
+    const float p = fmul(p2, pinv), r = fmul(r2, rinv);
+    return fmul(fmul(dd, pinv), __frcp_rn(fadd(p, r)));
+}
+
+// one point: F (three components of its chain) += f
+template <bool HASFAIL>
+__device__ __forceinline__ void pt_force(float x0, float x1, float x2, float K, float r2inv, float e0, float e1,
+                                         float e2, float epsc, float* F) {
+    const float y0 = fadd(x0, e0), y1 = fadd(x1, e1), y2 = fadd(x2, e2);
+    const float dd = ffma(e0, fadd(x0, y0), ffma(e1, fadd(x1, y1), fmul(e2, fadd(x2, y2))));
+    const float eps = fmul(dd, r2inv);
+    const float h = fabsf(eps) < kSeriesMax ? pt_series(eps) : pt_exact(x0, x1, x2, dd);
+    float fm = fmul(K, h);
+    if (HASFAIL && eps > epsc) fm = 0.f;
+    F[0] = ffma(fm, y0, F[0]);
+    F[1] = ffma(fm, y1, F[1]);
+    F[2] = ffma(fm, y2, F[2]);
+}
+
+// The same for two points at once (lo and hi lanes), lane by lane the
+// operations of pt_force; a lane outside the series range takes pt_exact.
+template <bool HASFAIL>
+__device__ __forceinline__ void pt_force2(f2 x0, f2 x1, f2 x2, f2 K, f2 r2inv, f2 e0, f2 e1, f2 e2, float epsc,
+                                          f2* F) {
+    const f2 y0 = f2_add(x0, e0), y1 = f2_add(x1, e1), y2 = f2_add(x2, e2);
+    const f2 dd = f2_fma(e0, f2_add(x0, y0), f2_fma(e1, f2_add(x1, y1), f2_mul(e2, f2_add(x2, y2))));
+    const f2 eps = f2_mul(dd, r2inv);
+    f2 c = f2_fma(eps, f2_make(kH4, kH4), f2_make(kH3, kH3));
+    c = f2_fma(eps, c, f2_make(kH2, kH2));
+    c = f2_fma(eps, c, f2_make(kH1, kH1));
+    f2 h = f2_mul(eps, c);
+    float el, eh;
+    f2_split(eps, el, eh);
+    if (!(fabsf(el) < kSeriesMax) || !(fabsf(eh) < kSeriesMax)) {
+        float hl, hh, dl, dh, a0, b0, a1, b1, a2, b2;
+        f2_split(h, hl, hh);
+        f2_split(dd, dl, dh);
+        f2_split(x0, a0, b0);
+        f2_split(x1, a1, b1);
+        f2_split(x2, a2, b2);
+        if (!(fabsf(el) < kSeriesMax)) hl = pt_exact(a0, a1, a2, dl);
+        if (!(fabsf(eh) < kSeriesMax)) hh = pt_exact(b0, b1, b2, dh);
+        h = f2_make(hl, hh);
+    }
+    f2 fm = f2_mul(K, h);
+    if (HASFAIL) {
+        float fl, fh;
+        f2_split(fm, fl, fh);
+        if (el > epsc) fl = 0.f;
+        if (eh > epsc) fh = 0.f;
+        fm = f2_make(fl, fh);
+    }
+    F[0] = f2_fma(fm, y0, F[0]);
+    F[1] = f2_fma(fm, y1, F[1]);
+    F[2] = f2_fma(fm, y2, F[2]);
+}
+
+// eps above which a bond has failed: s > ecrit  <=>  eps > ecrit (2 + ecrit)
+__device__ __forceinline__ float eps_crit(float ecrit) { return fmul(ecrit, fadd(2.0f, ecrit)); }
+
+// us_j - u_i from FP32 hi/lo splits
+__device__ __forceinline__ float split_diff(float jh, float jl, float ih, float il) {
+    return fadd(fadd(jh, -ih), fadd(jl, -il));
+}
+
 // Four Gauss points q..q+3 of cell j on one bond (without the pair
 // coefficient), given xi_ij (dx), us_j - u_i (du) and the Gauss-point
-// displacements of j relative to us_j (u4: x[4], y[4], z[4]).
+// displacements of j relative to us_j (u4: x[4], y[4], z[4]).  F[0..2] is the
+// chain of the even points, F[3..5] that of the odd points.
 template <bool HASFAIL>
 __device__ __forceinline__ void bond4(const PointPack<8>& G, int q, const float* u4, const float* dx,
-                                      const float* du, float ecrit, float* F) {
+                                      const float* du, float epsc, float* F) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const PointF& P = G.p[q + k];
-        const float x0 = dx[0] + P.hx, x1 = dx[1] + P.hy, x2 = dx[2] + P.hz;
-        const float e0 = du[0] + u4[k], e1 = du[1] + u4[4 + k], e2 = du[2] + u4[8 + k];
-        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
-        const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
-        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
-        const float p2 = r2 + dd;
-        const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
-        const float r = __fmul_rn(r2, rinv);
-        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
-        const float beta = __saturatef((P.A - r) * P.B);
-        float fm = P.W * beta * s * pinv;
-        if (HASFAIL && dd > 0.f && s > ecrit) fm = 0.f;
-        F[0] = fmaf(fm, y0, F[0]);
-        F[1] = fmaf(fm, y1, F[1]);
-        F[2] = fmaf(fm, y2, F[2]);
+        const float x0 = fadd(dx[0], P.hx), x1 = fadd(dx[1], P.hy), x2 = fadd(dx[2], P.hz);
+        float K, r2inv;
+        pt_geo(P, x0, x1, x2, K, r2inv);
+        const float e0 = fadd(du[0], u4[k]), e1 = fadd(du[1], u4[4 + k]), e2 = fadd(du[2], u4[8 + k]);
+        pt_force<HASFAIL>(x0, x1, x2, K, r2inv, e0, e1, e2, epsc, F + 3 * (k & 1));
     }
 }
 
-// bond4 for the two nodes of an x-adjacent pair: their bonds to one
-// neighbour share xi's y and z components, so x1 = xi_1 + h_y, x2 = xi_2 + h_z
-// and the inner term fmaf(x1, x1, x2 x2) of r2 are formed once per point
-// (X1, X2, T12) and bond4s adds only the pair-specific x0; the same values
-// as bond4 computes.
-__device__ __forceinline__ void pair_terms(const PointPack<8>& G, int q, float dx1, float dx2, float* X1, float* X2,
-                                           float* T12) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const PointF& P = G.p[q + k];
-        X1[k] = dx1 + P.hy;
-        X2[k] = dx2 + P.hz;
-        T12[k] = fmaf(X1[k], X1[k], X2[k] * X2[k]);
-    }
-}
-
-template <bool HASFAIL>
-__device__ __forceinline__ void bond4s(const PointPack<8>& G, int q, const float* u4, float dx0, const float* X1,
-                                       const float* X2, const float* T12, const float* du, float ecrit, float* F) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const PointF& P = G.p[q + k];
-        const float x0 = dx0 + P.hx, x1 = X1[k], x2 = X2[k];
-        const float e0 = du[0] + u4[k], e1 = du[1] + u4[4 + k], e2 = du[2] + u4[8 + k];
-        const float y0 = x0 + e0, y1 = x1 + e1, y2 = x2 + e2;
-        const float r2 = fmaf(x0, x0, T12[k]);
-        const float dd = fmaf(e0, x0 + y0, fmaf(e1, x1 + y1, e2 * (x2 + y2)));
-        const float p2 = r2 + dd;
-        const float rinv = rsqrtf(r2), pinv = rsqrtf(p2);
-        const float r = __fmul_rn(r2, rinv);
-        const float s = dd * rinv * __fdividef(1.0f, fmaf(p2, pinv, r));
-        const float beta = __saturatef((P.A - r) * P.B);
-        float fm = P.W * beta * s * pinv;
-        if (HASFAIL && dd > 0.f && s > ecrit) fm = 0.f;
-        F[0] = fmaf(fm, y0, F[0]);
-        F[1] = fmaf(fm, y1, F[1]);
-        F[2] = fmaf(fm, y2, F[2]);
-    }
+// the bond force of the two chains
+__device__ __forceinline__ void chains_sum(const float* F6, float* F) {
+    F[0] = fadd(F6[0], F6[3]);
+    F[1] = fadd(F6[1], F6[4]);
+    F[2] = fadd(F6[2], F6[5]);
 }
 
 struct Own {
@@ -276,7 +388,7 @@ __device__ __forceinline__ void force_nodes(const Dev& d, const PointPack<8>& G,
             } else {
                 for (int a = 0; a < 3; ++a) dx[side][a] = (pj[a] - O.ph[a]) + (pj[3 + a] - O.pl[a]);
             }
-            for (int a = 0; a < 3; ++a) du[side][a] = (ujh[a] - O.uh[a]) + (ujl[a] - O.ul[a]);
+            for (int a = 0; a < 3; ++a) du[side][a] = split_diff(ujh[a], ujl[a], O.uh[a], O.ul[a]);
             float c = O.c;
             ecrit[side] = O.e;
             if (MULTIMAT) {
@@ -287,7 +399,8 @@ __device__ __forceinline__ void force_nodes(const Dev& d, const PointPack<8>& G,
             if (SFAC) c *= 0.5f * (O.sf + sfj);
             coef[side] = c;
         }
-        float F[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float F[2][6] = {{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+        const float epsc[2] = {HASFAIL ? eps_crit(ecrit[0]) : 0.f, HASFAIL ? eps_crit(ecrit[1]) : 0.f};
         // the eight Gauss points of cell j in two halves of four, each half
         // applied to both bonds
 #pragma unroll
@@ -299,14 +412,18 @@ __device__ __forceinline__ void force_nodes(const Dev& d, const PointPack<8>& G,
 #pragma unroll
             for (int side = 0; side < 2; ++side)
                 if (has[side])
-                    bond4<HASFAIL>(G, q, u4, dx[side], du[side], ecrit[side], F[side]);
+                    bond4<HASFAIL>(G, q, u4, dx[side], du[side], epsc[side], F[side]);
         }
         if (has[0]) {
-            kahan_add(A, F[0], coef[0]);
+            float Fb[3];
+            chains_sum(F[0], Fb);
+            kahan_add(A, Fb, coef[0]);
             ++pa;
         }
         if (has[1]) {
-            kahan_add(B, F[1], coef[1]);
+            float Fb[3];
+            chains_sum(F[1], Fb);
+            kahan_add(B, Fb, coef[1]);
             ++pb;
         }
     }
@@ -385,25 +502,27 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
             dx[k][0] = __fmul_rn((float)((lj & 2047) - (O[k].lat & 2047)), h);
             dx[k][1] = __fmul_rn((float)(((lj >> 11) & 2047) - ((O[k].lat >> 11) & 2047)), h);
             dx[k][2] = __fmul_rn((float)((lj >> 22) - (O[k].lat >> 22)), h);
-            for (int a = 0; a < 3; ++a) du[k][a] = (ujh[a] - O[k].uh[a]) + (ujl[a] - O[k].ul[a]);
+            for (int a = 0; a < 3; ++a) du[k][a] = split_diff(ujh[a], ujl[a], O[k].uh[a], O[k].ul[a]);
             float c = O[k].c;
             if (BDRY) c *= 0.5f * (O[k].be + bej);
             if (SFAC) c *= 0.5f * (O[k].sf + sfj);
             coef[k] = c;
         }
-        float F[4][3] = {};
+        float F[4][6] = {};
 #pragma unroll
         for (int q = 0; q < 8; q += 4) {
             const float4 vx = ld4(bj + q), vy = ld4(bj + 8 + q), vz = ld4(bj + 16 + q);
             const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                if (js[k] == j) bond4<false>(G, q, u4, dx[k], du[k], O[k].e, F[k]);
+                if (js[k] == j) bond4<false>(G, q, u4, dx[k], du[k], 0.f, F[k]);
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (js[k] == j) {
-                kahan_add(O[k], F[k], coef[k]);
+                float Fb[3];
+                chains_sum(F[k], Fb);
+                kahan_add(O[k], Fb, coef[k]);
                 ++p[k];
             }
     }
@@ -422,19 +541,32 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 // neighbour chunk from 1 KB of contiguous memory (8 lines instead of 32).
 // Per node the same bond4 arithmetic in the same ascending neighbour order
 // as the pair kernel's lattice variants: the same result bit for bit.
-// (Reading the geometric terms of each offset and point from a table
-// instead of computing them was slower: a float4 that the whole warp reads
-// at one address still fills 512 bytes of registers, which costs the L1
-// data path as much as a coalesced load, and the table needs two per
-// evaluation.)
+// (A first table of the geometric terms in global memory, read one float4
+// per point, was slower than computing them: a warp-wide broadcast from L1
+// still costs a wavefront per load.  The table below lives in shared memory,
+// holds only what the series form needs, and serves two points per load.)
 
 // One thread per x-adjacent node pair (A, B = A + 1) of a lattice row; a
-// block covers 16 pairs x sten_by rows x sten_bz layers.  The thread walks
-// U2 in ascending offset (= ascending neighbour id) over the set bits of
-// the two masks; a warp's threads are in step wherever their families have
-// the same shape, so the U2 entry is read at one address by the whole warp.
+// block covers 16 pairs x sten_by rows x sten_bz layers.  A warp walks the
+// union of its threads' masks over U2 in ascending offset (= ascending
+// neighbour id for every thread), so the U2 entry and the table row are the
+// same for the whole warp; a thread takes the bonds its own masks hold.
+// Geometry per (entry, side, point pair) comes from the table of pt_geo
+// values staged in shared memory (sten_tab, 16 bytes per two points: one
+// broadcast load), and the eight points of a bond are evaluated two per
+// packed instruction (pt_force2: the even point in the low lane, the odd in
+// the high lane, which are the two chains of bond4).  Per node the same
+// operations in the same order as bond4 on the lattice path: the same
+// result bit for bit as the pair, quad and tiled kernels.
 template <bool HASFAIL, bool BDRY, bool SFAC>
 __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
+    extern __shared__ float4 sm4[];
+    const int nu = d.sten_nu;
+    float4* tab = sm4;                                   // [2][nu][4]
+    int4* u2s = reinterpret_cast<int4*>(sm4 + 8 * nu);  // [nu]
+    for (int k = threadIdx.x; k < 8 * nu; k += blockDim.x) tab[k] = __ldg(d.sten_tab + k);
+    for (int k = threadIdx.x; k < nu; k += blockDim.x) u2s[k] = __ldg(d.sten_u2 + k);
+    __syncthreads();
     const int NX = d.lat_nx, NY = d.lat_ny, NZ = d.lat_nz;
     const int npx = (NX + 1) >> 1, BY = d.sten_by, BZ = d.sten_bz;
     const int nbx = (npx + 15) >> 4, nby = (NY + BY - 1) / BY;
@@ -443,30 +575,41 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
     const int px = (b % nbx) * 16 + tx;
     const int y = ((b / nbx) % nby) * BY + ty % BY;
     const int z = (b / (nbx * nby)) * BZ + ty / BY;
-    if (px >= npx || y >= NY || z >= NZ) return;
+    // threads past the box stay in the warp's walk with empty masks
+    const bool valid = px < npx && y < NY && z < NZ;
     const int64_t N = d.n, NP = d.sten_np;
-    const int64_t yz = y + (int64_t)NY * z;
-    const int64_t p = px + (int64_t)npx * yz;
-    const int64_t ia = 2 * px + (int64_t)NX * yz;
-    const bool hb = 2 * px + 1 < NX;
+    const int64_t yz = valid ? y + (int64_t)NY * z : 0;
+    const int64_t p = valid ? px + (int64_t)npx * yz : 0;
+    const int64_t ia = valid ? 2 * px + (int64_t)NX * yz : 0;
+    const bool hb = valid && 2 * px + 1 < NX;
     Own A, B;
     load_own<true, BDRY, SFAC, false>(d, ia, A);
     load_own<true, BDRY, SFAC, false>(d, hb ? ia + 1 : ia, B);
+    const float epsc[2] = {HASFAIL ? eps_crit(A.e) : 0.f, HASFAIL ? eps_crit(B.e) : 0.f};
     const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
     const float h = (float)d.dx;
+    f2 hx[4], hy[4], hz[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        hx[k] = f2_make(G.p[2 * k].hx, G.p[2 * k + 1].hx);
+        hy[k] = f2_make(G.p[2 * k].hy, G.p[2 * k + 1].hy);
+        hz[k] = f2_make(G.p[2 * k].hz, G.p[2 * k + 1].hz);
+    }
     const int nw = d.sten_nw;
     int nba = 0, nbb = 0;
     for (int w = 0; w < nw; ++w) {
-        const uint32_t ma = __ldg(d.sten_mask + (int64_t)w * NP + p);
+        const uint32_t ma = valid ? __ldg(d.sten_mask + (int64_t)w * NP + p) : 0u;
         const uint32_t mb = hb ? __ldg(d.sten_mask + (int64_t)(nw + w) * NP + p) : 0u;
         nba += __popc(ma);
         nbb += __popc(mb);
-        uint32_t m = ma | mb;
+        uint32_t m = __reduce_or_sync(0xffffffffu, ma | mb);
         while (m) {
             const int bit = __ffs(m) - 1;
             m &= m - 1;
-            const int4 E = __ldg(d.sten_u2 + 32 * w + bit);  // id offset, ox, oy, oz from A
             const bool has[2] = {((ma >> bit) & 1u) != 0, ((mb >> bit) & 1u) != 0};
+            if (!(has[0] || has[1])) continue;
+            const int u = 32 * w + bit;
+            const int4 E = u2s[u];  // id offset, ox, oy, oz from A
             const int64_t j = ia + E.x;
             const float4 us0 = __ldg(blk + 6 * N + j), us1 = __ldg(blk + 7 * N + j);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
             float bej = 1.f, sfj = 1.f;
@@ -476,38 +619,81 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
                 sfj = v.y;
             }
             const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
-            float dx[2][3], du[2][3], coef[2];
+            const float dx1 = __fmul_rn((float)E.z, h), dx2 = __fmul_rn((float)E.w, h);
+            f2 dx0s[2], du[2][3];
+            float coef[2];
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const Own& O = side == 0 ? A : B;
-                dx[side][0] = __fmul_rn((float)(E.y - side), h);
-                dx[side][1] = __fmul_rn((float)E.z, h);
-                dx[side][2] = __fmul_rn((float)E.w, h);
-                for (int a = 0; a < 3; ++a) du[side][a] = (ujh[a] - O.uh[a]) + (ujl[a] - O.ul[a]);
+                const float dx0 = __fmul_rn((float)(E.y - side), h);
+                dx0s[side] = f2_make(dx0, dx0);
+                for (int a = 0; a < 3; ++a) {
+                    const float v = split_diff(ujh[a], ujl[a], O.uh[a], O.ul[a]);
+                    du[side][a] = f2_make(v, v);
+                }
                 float c = O.c;
                 if (BDRY) c *= 0.5f * (O.be + bej);
                 if (SFAC) c *= 0.5f * (O.sf + sfj);
                 coef[side] = c;
             }
-            float F[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+            const f2 dx1s = f2_make(dx1, dx1), dx2s = f2_make(dx2, dx2);
+            f2 F[2][3] = {{0ull, 0ull, 0ull}, {0ull, 0ull, 0ull}};
 #pragma unroll
             for (int q = 0; q < 8; q += 4) {
                 const float4 vx = __ldg(blk + (q >> 2) * N + j), vy = __ldg(blk + (2 + (q >> 2)) * N + j),
                              vz = __ldg(blk + (4 + (q >> 2)) * N + j);
-                const float u4[12] = {vx.x, vx.y, vx.z, vx.w, vy.x, vy.y, vy.z, vy.w, vz.x, vz.y, vz.z, vz.w};
-                float X1[4], X2[4], T12[4];
-                pair_terms(G, q, dx[0][1], dx[0][2], X1, X2, T12);
 #pragma unroll
-                for (int side = 0; side < 2; ++side)
-                    if (has[side])
-                        bond4s<HASFAIL>(G, q, u4, dx[side][0], X1, X2, T12, du[side], side == 0 ? A.e : B.e, F[side]);
+                for (int kk = 0; kk < 2; ++kk) {
+                    const int k = (q >> 1) + kk;  // point pair (2k, 2k + 1)
+                    const f2 gx = kk ? f2_make(vx.z, vx.w) : f2_make(vx.x, vx.y);
+                    const f2 gy = kk ? f2_make(vy.z, vy.w) : f2_make(vy.x, vy.y);
+                    const f2 gz = kk ? f2_make(vz.z, vz.w) : f2_make(vz.x, vz.y);
+                    const f2 x1 = f2_add(dx1s, hy[k]), x2 = f2_add(dx2s, hz[k]);
+#pragma unroll
+                    for (int side = 0; side < 2; ++side)
+                        if (has[side]) {
+                            const float4 T = tab[(side * nu + u) * 4 + k];  // K lo hi, 1/r^2 lo hi
+                            const f2 x0 = f2_add(dx0s[side], hx[k]);
+                            pt_force2<HASFAIL>(x0, x1, x2, f2_make(T.x, T.y), f2_make(T.z, T.w),
+                                               f2_add(du[side][0], gx), f2_add(du[side][1], gy),
+                                               f2_add(du[side][2], gz), epsc[side], F[side]);
+                        }
+                }
             }
-            if (has[0]) kahan_add(A, F[0], coef[0]);
-            if (has[1]) kahan_add(B, F[1], coef[1]);
+#pragma unroll
+            for (int side = 0; side < 2; ++side)
+                if (has[side]) {
+                    float F6[6];
+                    f2_split(F[side][0], F6[0], F6[3]);
+                    f2_split(F[side][1], F6[1], F6[4]);
+                    f2_split(F[side][2], F6[2], F6[5]);
+                    float Fb[3];
+                    chains_sum(F6, Fb);
+                    kahan_add(side == 0 ? A : B, Fb, coef[side]);
+                }
         }
     }
-    store_own<false>(d, ia, A, nba, dts, d.vbuf);
+    if (valid) store_own<false>(d, ia, A, nba, dts, d.vbuf);
     if (hb) store_own<false>(d, ia + 1, B, nbb, dts, d.vbuf);
+}
+
+// Setup of the stencil force's table: per U2 entry u, side (node A: offset
+// o_u; node B = A + 1: o_u - e_x) and point pair k, K and 1/r^2 of the points
+// 2k and 2k + 1 (pt_geo, from the same lattice-offset bond vector that bond4
+// forms), laid out [side][u][k] as (K_2k, K_2k+1, 1/r2_2k, 1/r2_2k+1).
+__global__ void k_sten_table(const int4* __restrict__ u2, int nu, PointPack<8> G, float h, float4* __restrict__ tab) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8 * nu) return;
+    const int k = t & 3, u = (t >> 2) % nu, side = t / (4 * nu);
+    const int4 E = u2[u];
+    const float dx0 = __fmul_rn((float)(E.y - side), h), dx1 = __fmul_rn((float)E.z, h),
+                dx2 = __fmul_rn((float)E.w, h);
+    float K[2], r2i[2];
+    for (int l = 0; l < 2; ++l) {
+        const PointF& P = G.p[2 * k + l];
+        pt_geo(P, fadd(dx0, P.hx), fadd(dx1, P.hy), fadd(dx2, P.hz), K[l], r2i[l]);
+    }
+    tab[t] = make_float4(K[0], K[1], r2i[0], r2i[1]);
 }
 
 // Setup: the offsets (from the node) of every unbroken family entry, over
@@ -1055,6 +1241,112 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
     }
 }
 
+// 8-byte copy global -> shared (the delta ring's slot of four int16)
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gsrc) : "memory");
+}
+
+constexpr int kRingD = 20;  // delta slots a thread keeps in flight (8 bytes each)
+
+// k_gather_f32c_ring on the delta form of the coefficients: the stream of
+// int16 deltas (8 bytes per contributor slot and thread) runs through the
+// shared-memory ring, the pattern coefficients and the thread's four scales
+// come through L1, and every coefficient is rebuilt as fma(scale, delta,
+// c_pattern), the value coeff32 holds, before the same FMAs in the same
+// order as gather_group: the same result bit for bit.
+__global__ void __launch_bounds__(256, 2) k_gather_f32c_dring(Dev d, const double* __restrict__ us) {
+    __shared__ uint2 ring[8][kRingD][32];
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (tid >= d.n * 2) return;
+    const int64_t N = d.n;
+    const int64_t slot = tid >> 1;
+    const int grp = (int)(tid & 1), g0 = 4 * grp;
+    const int64_t i = d.order[slot];
+    const BlkOut o = blk_out(d, i);
+    double u0, u1, u2;
+    if (gather_head<false>(d, us, i, grp, *d.tdev, o, u0, u1, u2)) return;
+    const int pid = __ldg(d.gpat_id + i);
+    const int64_t p0 = __ldg(d.gpat_ptr + pid);
+    const int nc = (int)(__ldg(d.gpat_ptr + pid + 1) - p0);
+    const int32_t* po = d.gpat_off + p0;
+    const float* cpt = d.cpat + p0 * 8 + g0;  // contributor k: cpt[8 k .. 8 k + 3]
+    const float4 sc4 = ld4(d.cscale + i * 8 + g0);
+    const float sc[4] = {sc4.x, sc4.y, sc4.z, sc4.w};
+    const int64_t sl = slot / kSell, ln = slot % kSell, base = d.sell_off[sl];
+    // contributor slot k of this thread: cf[32 k] (a slot is kSell nodes x 8 int16 = 32 x 8 bytes)
+    const uint2* cf = reinterpret_cast<const uint2*>(d.sell_d16 + (base * kSell + ln) * 8 + g0);
+    uint2* r = &ring[threadIdx.x >> 5][0][threadIdx.x & 31];  // ring entry e at r[32 e]
+#pragma unroll
+    for (int k = 0; k < kRingD; ++k) {
+        if (k < nc) cp_async8(r + 32 * k, cf + (int64_t)32 * k);
+        cp_async_commit();
+    }
+    double un[4][3];
+    auto load_group = [&](int k) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int m = (int)i + (k + u < nc ? __ldg(po + k + u) : 0);
+            un[u][0] = __ldg(us + m);
+            un[u][1] = __ldg(us + N + m);
+            un[u][2] = __ldg(us + 2 * N + m);
+        }
+    };
+    load_group(0);
+    double a[4][3] = {};
+    int e = 0;
+    for (int k = 0; k < nc; k += 4) {
+        double dd[4][3];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            dd[u][0] = un[u][0] - u0;
+            dd[u][1] = un[u][1] - u1;
+            dd[u][2] = un[u][2] - u2;
+        }
+        if (k + 4 < nc) load_group(k + 4);
+        float4 cv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            cv[u] = k + u < nc ? ld4(cpt + 8 * (k + u)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        cp_async_wait<kRingD - 4>();  // slots k .. k+3 have landed
+        uint2 dv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int eu = e + u < kRingD ? e + u : e + u - kRingD;
+            dv[u] = k + u < nc ? r[32 * eu] : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (k + u >= nc) break;
+            const float dq[4] = {(float)(short)(dv[u].x & 0xffffu), (float)((int)dv[u].x >> 16),
+                                 (float)(short)(dv[u].y & 0xffffu), (float)((int)dv[u].y >> 16)};
+            const float cpv[4] = {cv[u].x, cv[u].y, cv[u].z, cv[u].w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float c = ffma(sc[q], dq[q], cpv[q]);
+                a[q][0] = fma((double)c, dd[u][0], a[q][0]);
+                a[q][1] = fma((double)c, dd[u][1], a[q][1]);
+                a[q][2] = fma((double)c, dd[u][2], a[q][2]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int eu = e + u < kRingD ? e + u : e + u - kRingD;
+            const int kk = k + kRingD + u;
+            if (kk < nc) cp_async8(r + 32 * eu, cf + (int64_t)32 * kk);
+            cp_async_commit();
+        }
+        e = e + 4 < kRingD ? e + 4 : e + 4 - kRingD;
+    }
+    cp_async_wait<0>();
+    for (int q = 0; q < 4; ++q) {
+        const double S = (double)d.csum[i * 8 + g0 + q];
+        o[g0 + q] = (float)fma(S, u0, a[q][0]);
+        o[8 + g0 + q] = (float)fma(S, u1, a[q][1]);
+        o[16 + g0 + q] = (float)fma(S, u2, a[q][2]);
+    }
+}
+
 // SELL layout: the widest contributor list of every slice, then the copy
 __global__ void k_sell_width(Dev d, int64_t* __restrict__ width, int64_t S) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1070,7 +1362,7 @@ __global__ void k_sell_width(Dev d, int64_t* __restrict__ width, int64_t S) {
 }
 
 __global__ void k_sell_fill(Dev d, const int64_t* __restrict__ off, int32_t* __restrict__ sidx,
-                            float* __restrict__ scoef) {
+                            float* __restrict__ scoef, int16_t* __restrict__ sd16) {
     const int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (slot >= d.n) return;
     const int64_t i = d.order[slot], sl = slot / kSell, l = slot % kSell, base = off[sl];
@@ -1080,6 +1372,77 @@ __global__ void k_sell_fill(Dev d, const int64_t* __restrict__ off, int32_t* __r
         const float* src = d.coeff32 + (c0 + k) * 8;
         float* dst = scoef + ((base + k) * kSell + l) * 8;
         for (int g = 0; g < 8; ++g) dst[g] = src[g];
+        if (sd16) {
+            const int16_t* s16 = d.cd16 + (c0 + k) * 8;
+            int16_t* d16 = sd16 + ((base + k) * kSell + l) * 8;
+            for (int g = 0; g < 8; ++g) d16[g] = s16[g];
+        }
+    }
+}
+
+// ---- delta form of the FP32 MLS coefficients (2x2x2 points) ----
+//
+// On a lattice, nodes whose contributor lists are translates of each other
+// (one pattern) have the same coefficients up to the round-off the
+// ill-conditioned moment matrix of InitIntegrationPoint (pdDataManager2.cpp:
+// 173-256, global coordinates) adds: 1e-10..1e-5 of the largest coefficient,
+// growing with the distance from the origin.  The FP32 form stores each
+// coefficient as the pattern representative's FP32 coefficient plus an
+// int16 multiple of a per-(node, point) scale, max |c - c_rep| / 32767, so
+// the quantisation error (below 2^-16 of the largest delta) is far below the
+// FP32 rounding of the result, fma(scale, delta, c_rep): the FP32
+// coefficient of every FP32 gather.  The gather from deltas streams 2 bytes
+// per coefficient instead of 4 and reads the pattern table from L1/L2.
+
+// nodes whose coefficients stray more than 2^-10 of their largest from their
+// representative's (the pattern then does not describe the geometry)
+__global__ void k_delta_check(Dev d, const int32_t* __restrict__ pid, const int32_t* __restrict__ rep,
+                              uint8_t* __restrict__ far) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int64_t r = rep[pid[i]];
+    const int64_t a = d.cbptr[i], b = d.cbptr[r], nc = d.cbptr[i + 1] - a;
+    double dev = 0.0, cm = 0.0;
+    for (int64_t k = 0; k < 8 * nc; ++k) {
+        const double ci = d.coeff[a * 8 + k], cr = d.coeff[b * 8 + k];
+        dev = fmax(dev, fabs(ci - cr));
+        cm = fmax(cm, fabs(ci));
+    }
+    far[i] = dev > 0x1p-10 * cm ? 1 : 0;
+}
+
+// the pattern table: the representative's coefficients in FP32
+__global__ void k_delta_pat(Dev d, const int32_t* __restrict__ pid, const int64_t* __restrict__ ptr,
+                            const int32_t* __restrict__ rep, float* __restrict__ cpat) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n || rep[pid[i]] != i) return;
+    const int64_t a = d.cbptr[i], nc = d.cbptr[i + 1] - a;
+    float* dst = cpat + ptr[pid[i]] * 8;
+    for (int64_t k = 0; k < 8 * nc; ++k) dst[k] = (float)d.coeff[a * 8 + k];
+}
+
+// one thread per (node, point): scale, deltas, and the FP32 coefficients
+__global__ void k_delta_build(Dev d, const int32_t* __restrict__ pid, const int64_t* __restrict__ ptr,
+                              const float* __restrict__ cpat, float* __restrict__ cscale, int16_t* __restrict__ cd16,
+                              float* __restrict__ coeff32) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= d.n * 8) return;
+    const int64_t i = t >> 3;
+    const int g = (int)(t & 7);
+    const int64_t a = d.cbptr[i], nc = d.cbptr[i + 1] - a;
+    const float* cp = cpat + ptr[pid[i]] * 8 + g;
+    double m = 0.0;
+    for (int64_t k = 0; k < nc; ++k) m = fmax(m, fabs(d.coeff[(a + k) * 8 + g] - (double)cp[8 * k]));
+    const float sf = (float)(m / 32767.0);
+    cscale[t] = sf;
+    for (int64_t k = 0; k < nc; ++k) {
+        int q = 0;
+        if (sf > 0.f) {
+            const double v = rint((d.coeff[(a + k) * 8 + g] - (double)cp[8 * k]) / (double)sf);
+            q = (int)fmax(-32767.0, fmin(32767.0, v));
+        }
+        cd16[(a + k) * 8 + g] = (int16_t)q;
+        coeff32[(a + k) * 8 + g] = ffma(sf, (float)q, cp[8 * k]);
     }
 }
 
@@ -1273,6 +1636,9 @@ PointPack<NPT> pack_points(const Dev& d, const GaussConst* host_gc) {
 
 }  // namespace
 
+// shared memory of the stencil force: the table and the U2 entries
+static size_t sten_smem_bytes(int nu) { return (size_t)nu * (8 * sizeof(float4) + sizeof(int4)); }
+
 size_t tiled_smem_bytes(const Dev& d) {
     const int R = d.fam_radius;
     const int64_t lx = std::min(d.lat_nx, d.tile_x + 2 * R), ly = std::min(d.lat_ny, d.tile_y + 2 * R),
@@ -1313,7 +1679,8 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
                                         ((d.lat_nz + d.sten_bz - 1) / d.sten_bz));
         const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
         const PointPack<8> P = pack_points<8>(d, d.gc_host);
-#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, P, dts)
+        const size_t sh = sten_smem_bytes(d.sten_nu);
+#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, sh, s>>>(d, P, dts)
         if (d.hasfail) {
             if (bd) { if (sf) PD_STEN(true, true, true); else PD_STEN(true, true, false); }
             else { if (sf) PD_STEN(true, false, true); else PD_STEN(true, false, false); }
@@ -1432,7 +1799,8 @@ void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
     const unsigned nb = blocks_for(d.n * ngrp, 256);
     const bool sell = d.sell_on && d.sell_idx && d.mls && d.npt == 8, pat = d.gpat_id && d.mls;
     if (sell && pat && d.npt == 8) {
-        k_gather_f32c_ring<<<nb, 256, 0, s>>>(d, us);
+        if (d.gather_delta && d.sell_d16 && d.cpat && d.cscale) k_gather_f32c_dring<<<nb, 256, 0, s>>>(d, us);
+        else k_gather_f32c_ring<<<nb, 256, 0, s>>>(d, us);
     } else if (sell) {
         if (pat) k_gather_f32c<true, true><<<nb, 256, 0, s>>>(d, us);
         else k_gather_f32c<true, false><<<nb, 256, 0, s>>>(d, us);
@@ -1453,13 +1821,41 @@ void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int*
 }
 
 
+int launch_sten_table(const Dev& d, float4* tab, cudaStream_t s) {
+    if (d.sten_nu <= 0 || !d.gc_host) return PD_ERR_ARG;
+    const PointPack<8> P = pack_points<8>(d, d.gc_host);
+    k_sten_table<<<blocks_for(8 * d.sten_nu, 128), 128, 0, s>>>(d.sten_u2, d.sten_nu, P, (float)d.dx, tab);
+    const int smem = (int)sten_smem_bytes(d.sten_nu);
+    const void* fns[8] = {
+        (const void*)k_force_f32c_sten<false, false, false>, (const void*)k_force_f32c_sten<false, false, true>,
+        (const void*)k_force_f32c_sten<false, true, false>,  (const void*)k_force_f32c_sten<false, true, true>,
+        (const void*)k_force_f32c_sten<true, false, false>,  (const void*)k_force_f32c_sten<true, false, true>,
+        (const void*)k_force_f32c_sten<true, true, false>,   (const void*)k_force_f32c_sten<true, true, true>};
+    for (const void* f : fns)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return PD_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? PD_OK : PD_ERR_CUDA;
+}
+
+
 void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s) {
     const int64_t S = sell_slices(d);
     if (S) k_sell_width<<<blocks_for(S, 256), 256, 0, s>>>(d, width, S);
 }
 
-void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s) {
-    if (d.n) k_sell_fill<<<blocks_for(d.n, 128), 128, 0, s>>>(d, off, sidx, scoef);
+void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, int16_t* sd16, cudaStream_t s) {
+    if (d.n) k_sell_fill<<<blocks_for(d.n, 128), 128, 0, s>>>(d, off, sidx, scoef, sd16);
+}
+
+void launch_delta_check(const Dev& d, const int32_t* pid, const int32_t* rep, uint8_t* far, cudaStream_t s) {
+    if (d.n) k_delta_check<<<blocks_for(d.n, 128), 128, 0, s>>>(d, pid, rep, far);
+}
+
+void launch_delta_build(const Dev& d, const int32_t* pid, const int64_t* ptr, const int32_t* rep, float* cpat,
+                        float* cscale, int16_t* cd16, float* coeff32, cudaStream_t s) {
+    if (!d.n) return;
+    k_delta_pat<<<blocks_for(d.n, 128), 128, 0, s>>>(d, pid, ptr, rep, cpat);
+    k_delta_build<<<blocks_for(d.n * 8, 128), 128, 0, s>>>(d, pid, ptr, cpat, cscale, cd16, coeff32);
 }
 
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s) {

@@ -237,6 +237,69 @@ __global__ void __launch_bounds__(256) k_static_stencil(Dev d, StencilDev S, con
     y[2 * N + i] = (mi & 4) ? x[2 * N + i] : a2;
 }
 
+// Block-Jacobi preconditioner of the static operator: per node the inverse
+// of its 3x3 diagonal block sum_j c V_j xi xi^T / r^3 over the unbroken
+// family (the coefficients of pdSolve::AssembleEquation), with prescribed
+// directions as identity rows and columns; stored symmetric [6][N] (xx yy zz
+// xy xz yz).  A singular block (a node without bonds) keeps the identity.
+template <bool SFAC>
+__global__ void k_static_bjacobi(Dev d, double* __restrict__ minv) {
+    const int64_t N = d.n;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    bool pi[3];
+    double pv[3];
+    prescribed(d, i, 0.0, pi, pv);
+    const double X0 = d.x[i], X1 = d.x[N + i], X2 = d.x[2 * N + i];
+    const double ci = d.mats[d.mat[i]].spring;
+    const double sfi = SFAC ? d.sfac[i] : 0.0;
+    double D[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+        const int64_t j = d.acol[p];
+        const double e[3] = {d.x[j] - X0, d.x[N + j] - X1, d.x[2 * N + j] - X2};
+        const double r2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+        const double r = sqrt(r2);
+        const double cj = d.mats[d.mat[j]].spring;
+        double c = (cj < ci) ? cj : ci;
+        if (SFAC) c = c * (0.5 * (sfi + d.sfac[j]));
+        const double w = c * d.vol / (r2 * r);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) D[a][b] += w * e[a] * e[b];
+    }
+    for (int a = 0; a < 3; ++a)
+        if (pi[a])
+            for (int b = 0; b < 3; ++b) D[a][b] = D[b][a] = (a == b) ? 1.0 : 0.0;
+    // inverse by cofactors (D symmetric)
+    const double c00 = D[1][1] * D[2][2] - D[1][2] * D[2][1];
+    const double c01 = D[1][2] * D[2][0] - D[1][0] * D[2][2];
+    const double c02 = D[1][0] * D[2][1] - D[1][1] * D[2][0];
+    const double det = D[0][0] * c00 + D[0][1] * c01 + D[0][2] * c02;
+    double m[6] = {1.0, 1.0, 1.0, 0.0, 0.0, 0.0};
+    if (det > 0.0 && isfinite(det)) {
+        const double id = 1.0 / det;
+        m[0] = c00 * id;
+        m[1] = (D[0][0] * D[2][2] - D[0][2] * D[2][0]) * id;
+        m[2] = (D[0][0] * D[1][1] - D[0][1] * D[1][0]) * id;
+        m[3] = c01 * id;
+        m[4] = c02 * id;
+        m[5] = (D[0][2] * D[1][0] - D[0][0] * D[1][2]) * id;
+    }
+    for (int k = 0; k < 6; ++k) minv[k * N + i] = m[k];
+}
+
+// z = M^-1 r with the blocks of k_static_bjacobi
+__global__ void k_bj_apply(const double* __restrict__ minv, const double* __restrict__ r, double* __restrict__ z,
+                           int64_t N) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double r0 = r[i], r1 = r[N + i], r2 = r[2 * N + i];
+        const double m0 = minv[i], m1 = minv[N + i], m2 = minv[2 * N + i];
+        const double m3 = minv[3 * N + i], m4 = minv[4 * N + i], m5 = minv[5 * N + i];
+        z[i] = m0 * r0 + m3 * r1 + m4 * r2;
+        z[N + i] = m3 * r0 + m1 * r1 + m5 * r2;
+        z[2 * N + i] = m4 * r0 + m5 * r1 + m2 * r2;
+    }
+}
+
 // b = prescribed values on prescribed rows; on free rows the moved prescribed
 // columns (pdSolve.cpp:296-363 sign pattern) plus the traction load.
 template <bool SFAC>
@@ -390,6 +453,16 @@ void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const do
         if (d.sfac) k_static_stencil<double, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
         else k_static_stencil<double, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
     }
+}
+
+void launch_static_bjacobi(const Dev& d, double* minv, cudaStream_t s) {
+    if (d.n == 0) return;
+    if (d.sfac) k_static_bjacobi<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, minv);
+    else k_static_bjacobi<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, minv);
+}
+
+void launch_bj_apply(const double* minv, const double* r, double* z, int64_t n, cudaStream_t s) {
+    if (n) k_bj_apply<<<148 * 8, 256, 0, s>>>(minv, r, z, n);
 }
 
 void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s) {

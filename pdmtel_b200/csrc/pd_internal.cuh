@@ -130,7 +130,16 @@ struct Dev {
     int blk_cm;
     int sten_nu, sten_nw, sten_by, sten_bz;
     int64_t sten_np;
+    // FP32 MLS coefficients as a pattern coefficient plus an int16 delta:
+    // c32 = fma(cscale[i][g], (float)delta, cpat[(gpat_ptr[pid] + k) * 8 + g])
+    // (2x2x2 points; coeff32 holds the same c32 values for the other gathers)
+    const float* cpat;            // per pattern entry and point: the representative's coefficient
+    const float* cscale;          // [N][8] delta scale of every node and point
+    const int16_t* sell_d16;      // SELL copy of the deltas [slots][16][8]
+    const int16_t* cd16;          // the deltas in the CSR layout [T][8] (setup of the SELL copy)
+    int gather_delta;             // FP32 gather from the deltas (PD_OPT_GATHER_DELTA)
     const int4* sten_u2;
+    const float4* sten_tab;       // [2][sten_nu][4] geometry of the stencil force (k_sten_table)
     const uint32_t* sten_mask;    // FP32 gather from contributor patterns: node i's contributors are
     // i + gpat_off[gpat_ptr[p] ..] with p = gpat_id[i] (the same ids in the same
     // order as its CSR list; nodes whose lists are translates share a pattern)
@@ -145,6 +154,14 @@ void launch_gather_f64(const Dev& d, const double* us, cudaStream_t s);
 void launch_epilogue(const Dev& d, int stage, double dts, double dt, cudaStream_t s);
 void launch_advance_time(double* t, double dt, cudaStream_t s);
 void launch_energy_reduce(const Dev& d, cudaStream_t s);
+// InitIntegrationPoint on the device (k_mls_contrib, k_mls_coeff): contributor
+// CSR and coefficients [node][contributor][point] from the family and the MLS
+// coordinates xm [3][N]; cnt [N] is scratch, cbptr [N+1] is written; the
+// other arrays are allocated through alloc(actx, bytes).  PD_ERR_SINGULAR
+// with *bad_node on a singular moment matrix.
+int mls_setup(const Dev& d, const double* xm, double rw, const double* absc, int n1, int64_t* cnt, int64_t* cbptr,
+              int32_t** cbidx, double** coeff, float** coeff32, float** csum, int64_t* total, int64_t* bad_node,
+              void* (*alloc)(void*, size_t), void* actx, cudaStream_t s);
 void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s);
 void launch_to_soa_changed(const double* aos, double* soa, int64_t n, int comps, int* changed, cudaStream_t s);
 void launch_to_aos(const double* soa, double* aos, int64_t n, int comps, cudaStream_t s);
@@ -167,7 +184,7 @@ void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
 size_t tiled_smem_bytes(const Dev& d);
 int64_t sell_slices(const Dev& d);
 void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s);
-void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s);
+void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, int16_t* sd16, cudaStream_t s);
 int prepare_tiled_force(size_t smem);
 void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
 // lattice-stencil force setup: offsets present in the families (bitmap over
@@ -175,6 +192,18 @@ void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
 // family does not fit the union list or a node breaks the box numbering)
 void launch_sten_offsets(const Dev& d, int R, int* bitmap, int* err, cudaStream_t s);
 void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int* err, cudaStream_t s);
+// geometry table of the stencil force (d.sten_u2, d.sten_nu, the Gauss
+// constants) into tab [2][nu][4]; sets the kernel's shared-memory limit
+int launch_sten_table(const Dev& d, float4* tab, cudaStream_t s);
+// Delta form of the FP32 coefficients (2x2x2 points): per node whether its
+// coefficients stay within 2^-10 of the largest one of its pattern's
+// representative (rep[pid]), the pattern table cpat, then for every node the
+// scales, the int16 deltas cd16 ([T][8], CSR) and coeff32 rebuilt as
+// cpat + scale * delta.  pid/ptr/rep: pattern of each node, first entry of
+// each pattern, representative node of each pattern.
+void launch_delta_check(const Dev& d, const int32_t* pid, const int32_t* rep, uint8_t* far, cudaStream_t s);
+void launch_delta_build(const Dev& d, const int32_t* pid, const int64_t* ptr, const int32_t* rep, float* cpat,
+                        float* cscale, int16_t* cd16, float* coeff32, cudaStream_t s);
 
 // persistent FP32C stepping (pd_f32c.cu): control block of one launch.
 // next[8*step + 2*(stage-1) + phase] are the work-queue counters; all of it
@@ -196,7 +225,7 @@ cudaError_t launch_persist_f32c(const Dev& d, double dt, int nsteps, PersistCtl*
                                 unsigned force_chunk, unsigned gather_chunk, PersistWait W, cudaStream_t s);
 
 // CG helpers (pd_fast.cu): slots of the device scalar array
-enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_NSLOT = 8 };
+enum { CG_RR = 0, CG_PQ = 1, CG_RRN = 2, CG_BB = 3, CG_RES = 4, CG_NSLOT = 8 };
 void launch_dot_f64(const double* a, const double* b, int64_t n, double* part, double* out, cudaStream_t s);
 void launch_cg_update_x_f64(double* x, double* r, const double* p, const double* q, int64_t n, const double* scal, cudaStream_t s);
 void launch_cg_update_p_f64(const double* r, double* p, int64_t n, const double* scal, cudaStream_t s);
@@ -206,6 +235,10 @@ constexpr int kDotBlocks = 296;
 
 // static operator (pd_fast.cu)
 void launch_static_apply_f64(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
+// block-Jacobi preconditioner of the static operator ([6][N] symmetric
+// inverses of the 3x3 diagonal blocks) and its application z = M^-1 r
+void launch_static_bjacobi(const Dev& d, double* minv, cudaStream_t s);
+void launch_bj_apply(const double* minv, const double* r, double* z, int64_t n, cudaStream_t s);
 void launch_static_rhs(const Dev& d, double t, double* b, cudaStream_t s);
 void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y, cudaStream_t s);
 // the static operator on a complete box lattice (node id = x + nx (y + ny z))

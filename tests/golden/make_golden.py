@@ -5,6 +5,7 @@
     python tests/golden/make_golden.py --kat     # known answers of larger decks, kat.json
     python tests/golden/make_golden.py --long    # the 20x10x10 bar over 100 steps, long/*.npz
     python tests/golden/make_golden.py --static  # the linearised stiffness pass, static/*.npz
+    python tests/golden/make_golden.py --outputs # the reference's output files, outputs/<case>/
 
 Each case is a small synthetic deck written by pdmtel_b200.decks into
 tests/golden/decks/<case>/pds_input.txt; the reference harness
@@ -107,7 +108,7 @@ def main():
     shutil.rmtree(tmp, ignore_errors=True)
 
 
-if __name__ == "__main__" and not {"--kat", "--long", "--static"} & set(sys.argv):
+if __name__ == "__main__" and not {"--kat", "--long", "--static", "--outputs"} & set(sys.argv):
     main()
 
 
@@ -305,3 +306,57 @@ def make_static():
 
 if __name__ == "__main__" and "--static" in sys.argv:
     make_static()
+
+
+# ---- the reference's output files (tests/golden/outputs/) ----
+#
+# pdSolve::SolveDynamic (pdSolve.cpp:24-130) writes the pds_output.dat log
+# (the deck echo of ReadInputFile and one line per step), the pds_steps.dat
+# probe of the node at (dx/2, dx/2, dx/2) and pds_tecplot_<step>.dat at the
+# first, the last and every dump step (pdSolve.cpp:708-774, pdNode.cpp:418-
+# 433).  The harness runs it on two small decks (Gauss points with MLS and a
+# shortened last step; CCI with a ramped displacement gradient) and the files
+# are kept under outputs/<case>/ with a ref_ prefix.
+
+def output_cases():
+    h = 1e-3
+    out = {}
+    dims = (8, 6, 4)
+    out["out_fgi"] = D.Deck(dims=dims, spacing=h, horizon=3.015 * h, total_time=6.5e-8, total_step=7, dump=3,
+                            fixed_dt=1e-8, damping=0.01, bdry_eff=1, intg_point=2,
+                            bcs=[D.BC(D.DISPL, (1, 1, 1), (0.0, 0.0, 0.0), 1.0, 2.0),
+                                 D.BC(D.VELOC, (1, 0, 0), (0.05, 0.0, 0.0), 1.0, 2.0)],
+                            bc_spaces=[D.Space(1, D.face_box(dims, h, 0, -1)), D.Space(2, D.face_box(dims, h, 0, +1))],
+                            title="output check gauss")
+    dims = (6, 6, 4)
+    out["out_cci"] = D.Deck(dims=dims, spacing=2.0, horizon=6.0, total_time=2.0, total_step=5, dump=2, safety=1.1,
+                            materials=[(1.0e5, 1e14, 6e10, 2e-6)], damping=0.06, bdry_eff=1, cci=(1, 0),
+                            bcs=[D.BC(D.DISPLGRAD, (1, 1, 1), (-2.5e-5, 0, 0, 0, 1e-4, 0, 0, 0, -2.5e-5), 8e-4, 1.0)],
+                            bc_spaces=[D.Space(1, D.face_box(dims, 2.0, 1, -1)), D.Space(1, D.face_box(dims, 2.0, 1, +1))],
+                            title="output check cci")
+    return out
+
+
+def make_outputs():
+    import glob
+    out_dir = os.path.join(HERE, "outputs")
+    tmp = tempfile.mkdtemp(prefix="pdgolden_out_")
+    for name, deck in output_cases().items():
+        cdir = os.path.join(out_dir, name)
+        deck.write(cdir)
+        wd = os.path.join(tmp, name)
+        deck.write(wd)
+        r = subprocess.run([HARNESS, "solve", wd], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"harness solve {name} failed: {r.stderr[-400:]}")
+        for old in glob.glob(os.path.join(cdir, "ref_*")):
+            os.remove(old)
+        files = sorted(glob.glob(os.path.join(wd, "pds_*.dat")))
+        for f in files:
+            shutil.copy(f, os.path.join(cdir, "ref_" + os.path.basename(f)))
+        print(name, [os.path.basename(f) for f in files])
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__" and "--outputs" in sys.argv:
+    make_outputs()
