@@ -147,6 +147,22 @@ int pd_get_mls(pd_ctx* ctx, int64_t* cb_ptr, int32_t* cb_idx, double* coeff);
 /* number of MLS contributor entries held (0 without MLS data) */
 int pd_mls_size(pd_ctx* ctx, int64_t* num_contrib);
 
+/* The areal-force-density sums of pdSolve::PostAFD (pdSolve.cpp:810-834,
+ * pdDataManager3.cpp:442-635,1101-1223, replacing CalcForceOfPlusSpace).
+ * U [N][3] and bdry_eff [N] (host) are the nodal displacements and
+ * boundary factors PostAFD reads from a Tecplot dump; the Gauss-point
+ * displacements are derived from U as PostAFD derives them
+ * (CalcApproxDispl, pdDataManager.cpp:2704-2752: flagged directions of
+ * boundary-condition nodes stay zero).  Item k (node item_i, source
+ * item_s, direction item_dir 1..3) receives in force[3k..3k+2] the sum, over
+ * the family members j of node item_i (ascending id) with x_j >= x_source
+ * along the direction, of the bond force integrated over cell j: the fixed
+ * Gauss rule nested as pdIntgManager::CalcConfigurationType3 nests it, or
+ * the one-point CCI force with the node volume.  The caller adds the items
+ * of a source into its stress tensor (x ds, in the reference's order). */
+int pd_afd(pd_ctx* ctx, const double* U, const double* bdry_eff, int64_t num_items, const int64_t* item_i,
+           const int64_t* item_s, const int32_t* item_dir, double* force);
+
 /* Arithmetic of the subsequent force/gather/step calls (pd_precision). */
 int pd_set_precision(pd_ctx* ctx, int precision);
 /* Whether the elastic-energy diagnostic (pdDataManager2.cpp:1340-1342,

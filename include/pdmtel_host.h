@@ -88,6 +88,13 @@ int pdh_set_precision(pdh_model* m, int precision);
  * (pd_mls_setup) when on != 0; set before InitIntegrationPoint.  Off by
  * default: the host setup reproduces the reference bit for bit. */
 int pdh_set_device_setup(pdh_model* m, int on);
+/* pdSolve::PostAFD (pdSolve.cpp:810-834) without the console: reads
+ * pds_tecplot_<step>.dat of the working folder and writes the areal force
+ * density stress of n requests to pds_AFD_<step>.dat; request k is a plane
+ * (kind 1: nodes whose coordinate along norm[k] equals coord[k]) or a node
+ * (kind 2: node[k]). */
+int pdh_post_afd(pdh_model* m, int step, int n, const int32_t* kind, const int32_t* norm, const double* coord,
+                 const int64_t* node);
 
 /* pdSolve::SolveDynamic (pdSolve.cpp:24-130); write_files selects the
  * reference's per-step log, probe and Tecplot output */

@@ -18,10 +18,16 @@
 //   pdref_harness time  <dir> <nsteps>
 //   pdref_harness damp  <dir> <out.bin> <dt>
 //   pdref_harness solve <dir>
+//   pdref_harness afd   <dir> <script>
 //
 // solve: pdSolve::SolveDynamic (pdSolve.cpp:24-130) itself, which writes the
 // reference's pds_output.dat log, pds_steps.dat probe and pds_tecplot_<step>
 // files into <dir>.
+//
+// afd: pdSolve::PostAFD (pdSolve.cpp:810-834, pdDataManager3.cpp:442-635,
+// 1101-1223), which asks the console for the Tecplot step to read and for the
+// planes or nodes to evaluate; the answers come from the <script> file, and
+// it writes pds_AFD_<step>.dat into <dir>.
 //
 // damp: the reference's matrix-free linearised stiffness pass,
 // pdDataManager::CalcDampingCoeff (pdDataManager2.cpp:1616-1907), at three
@@ -40,6 +46,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <iostream>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -408,6 +415,16 @@ int main(int argc, char** argv) {
         }
         w.d("damp_coeff", damp);
         w.d1("damp_dt", dt);
+    } else if (mode == "afd") {
+        if (argc < 4) {
+            std::fprintf(stderr, "afd needs a script file\n");
+            return 2;
+        }
+        setup(dat, dir);
+        std::ifstream script(argv[3]);
+        std::streambuf* console = std::cin.rdbuf(script.rdbuf());
+        pdSolve::PostAFD(dat);
+        std::cin.rdbuf(console);
     } else if (mode == "solve") {
         setup(dat, dir);
         pdSolve::SolveDynamic(dat);

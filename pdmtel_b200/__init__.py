@@ -149,6 +149,8 @@ _SIGS = {
     "pdh_context": [_vp, C.POINTER(_vp)],
     "pdh_set_precision": [_vp, C.c_int],
     "pdh_set_device_setup": [_vp, C.c_int],
+    "pdh_post_afd": [_vp, C.c_int, C.c_int, _i32, _i32, _d, _i64],
+    "pd_afd": [_vp, _d, _d, C.c_int64, _i64, _i64, _i32, _d],
     "pdh_solve_dynamic": [_vp, C.c_int],
     "pdh_solve_static": [_vp, C.c_int, C.c_double, C.POINTER(C.c_int), _d],
     "pdh_batch_create": [C.c_char_p, C.POINTER(_vp), C.c_int, C.POINTER(_vp)],
@@ -626,6 +628,25 @@ class pdSolve:
     @staticmethod
     def SolveDynamic(dat: pdDataManager, write_files: bool = True):
         dat._call("pdh_solve_dynamic", int(bool(write_files)))
+
+    @staticmethod
+    def PostAFD(dat: pdDataManager, step: int, requests):
+        """pdSolve::PostAFD without the console: the areal force density of
+        pds_tecplot_<step>.dat on planes ("plane", normal 1..3, location)
+        and nodes ("node", id), written to pds_AFD_<step>.dat."""
+        n = len(requests)
+        kind = np.zeros(max(n, 1), np.int32)
+        norm = np.zeros(max(n, 1), np.int32)
+        coord = np.zeros(max(n, 1))
+        node = np.zeros(max(n, 1), np.int64)
+        for k, r in enumerate(requests):
+            if r[0] == "plane":
+                kind[k], norm[k], coord[k] = 1, int(r[1]), float(r[2])
+            elif r[0] == "node":
+                kind[k], node[k] = 2, int(r[1])
+            else:
+                raise ValueError(f"unknown PostAFD request {r!r}")
+        dat._call("pdh_post_afd", int(step), n, _p(kind, _i32), _p(norm, _i32), _p(coord, _d), _p(node, _i64))
 
     @staticmethod
     def SolveStatic(dat: pdDataManager, precision=PREC_FP64, rtol=1e-10):

@@ -2,6 +2,7 @@
 #include "pdDataManager.h"
 
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -839,6 +840,132 @@ int pdSolve::WriteTecplot(pdDataManager& dat, int step, double time) {
         out << "\n";
     }
     (void)time;
+    return PD_OK;
+}
+
+// ------------------------------------------------------------ PostAFD
+
+namespace {
+
+struct CoordKey {
+    uint64_t a, b, c;
+    bool operator==(const CoordKey& o) const { return a == o.a && b == o.b && c == o.c; }
+};
+struct CoordHash {
+    size_t operator()(const CoordKey& k) const {
+        return (size_t)((k.a * 0x9E3779B97F4A7C15ull) ^ (k.b * 0xC2B2AE3D27D4EB4Full) ^ (k.c * 0x165667B19E3779F9ull));
+    }
+};
+CoordKey coord_key(double x1, double x2, double x3) {
+    CoordKey k;
+    std::memcpy(&k.a, &x1, 8);
+    std::memcpy(&k.b, &x2, 8);
+    std::memcpy(&k.c, &x3, 8);
+    return k;
+}
+
+}  // namespace
+
+int pdSolve::PostAFD(pdDataManager& dat, int step, const std::vector<AfdRequest>& requests) {
+    int rc = dat.UploadSetup();
+    if (rc != PD_OK) return rc;
+    const int64_t N = dat.GetNumNode();
+    const std::string in_path = dat.GetWkDir() + keyword_append("pds_tecplot_", step) + ".dat";
+    std::ifstream in(in_path.c_str());
+    if (!in) return dat.Error(PD_ERR_ARG, "ReadTecplotFile: pdMTEL tecplot output file not exist!");
+    // the dump: four header lines, then one row per node
+    // (pdDataManager3.cpp:1108-1130); displacements and boundary factors are
+    // taken from it as written
+    std::string line;
+    for (int k = 0; k < 4; ++k) std::getline(in, line);
+    std::vector<double> U(3 * (size_t)N, 0.0), bE(N, 1.0);
+    for (int64_t k = 0; k < N; ++k) {
+        int64_t id, mat, bc;
+        double x1, x2, x3, u1, u2, u3, v1, v2, v3, be, dmg;
+        if (!(in >> id >> x1 >> x2 >> x3 >> u1 >> u2 >> u3 >> v1 >> v2 >> v3 >> mat >> bc >> be >> dmg) || id < 0 ||
+            id >= N)
+            return dat.Error(PD_ERR_ARG, "PostAFD: " + in_path + " does not hold this model's nodes");
+        U[3 * id] = u1;
+        U[3 * id + 1] = u2;
+        U[3 * id + 2] = u3;
+        bE[id] = be;
+    }
+    const std::vector<double>& X = dat.Coords();
+    std::unordered_map<CoordKey, int64_t, CoordHash> at;
+    at.reserve((size_t)N * 2);
+    for (int64_t i = 0; i < N; ++i) at.emplace(coord_key(X[3 * i], X[3 * i + 1], X[3 * i + 2]), i);
+    const double h = dat.GetGridSpacing(), delta = dat.GetHorizon();
+    const int ns = int(delta / h);
+    const double ds = delta / ns;
+    // items of one source: per direction the nodes at x_s - h (1 + is) e_d in
+    // ascending id (the order CalcArealForceDensity lists them in,
+    // pdDataManager3.cpp:463-480)
+    auto sigma_of = [&](const std::vector<int64_t>& sources, std::vector<std::array<double, 9>>& sig) -> int {
+        std::vector<int64_t> it_i, it_s;
+        std::vector<int32_t> it_d;
+        for (int64_t s : sources) {
+            const double* xs = &X[3 * s];
+            for (int d = 0; d < 3; ++d) {
+                std::vector<int64_t> col;
+                for (int is = 0; is != ns; ++is) {
+                    double q[3] = {xs[0], xs[1], xs[2]};
+                    q[d] = xs[d] - h * (1 + is);
+                    auto f = at.find(coord_key(q[0], q[1], q[2]));
+                    if (f != at.end()) col.push_back(f->second);
+                }
+                std::sort(col.begin(), col.end());
+                for (int64_t i : col) {
+                    it_i.push_back(i);
+                    it_s.push_back(s);
+                    it_d.push_back(d + 1);
+                }
+            }
+        }
+        std::vector<double> force(3 * it_i.size(), 0.0);
+        const int r = pd_afd(dat.Context(), U.data(), bE.data(), (int64_t)it_i.size(), it_i.data(), it_s.data(),
+                             it_d.data(), force.data());
+        if (r != PD_OK) return dat.Cuda(r, "pd_afd");
+        sig.assign(sources.size(), std::array<double, 9>{});
+        size_t src = 0;
+        for (size_t m = 0; m < it_i.size(); ++m) {
+            while (it_s[m] != sources[src]) ++src;
+            const int d = it_d[m] - 1;
+            for (int a = 0; a < 3; ++a) sig[src][3 * d + a] += force[3 * m + a] * ds;
+        }
+        return PD_OK;
+    };
+    std::ofstream out((dat.GetWkDir() + keyword_append("pds_AFD_", step) + ".dat").c_str());
+    for (const AfdRequest& q : requests) {
+        std::vector<int64_t> src;
+        if (q.kind == 1) {
+            if (q.norm < 1 || q.norm > 3) return dat.Error(PD_ERR_ARG, "PostAFD: plane normal 1, 2 or 3");
+            out << " norm = " << q.norm << ", location = " << q.coord << "\n";
+            for (int64_t i = 0; i < N; ++i)
+                if (X[3 * i + q.norm - 1] == q.coord) src.push_back(i);
+        } else if (q.kind == 2) {
+            if (q.node < 0 || q.node >= N) return dat.Error(PD_ERR_ARG, "PostAFD: node id out of range");
+            src.push_back(q.node);
+        } else {
+            return dat.Error(PD_ERR_ARG, "PostAFD: request kind 1 (plane) or 2 (node)");
+        }
+        std::vector<std::array<double, 9>> sig;
+        if ((rc = sigma_of(src, sig)) != PD_OK) return rc;
+        for (size_t k = 0; k < src.size(); ++k) {
+            const int64_t i = src[k];
+            const double* x = &X[3 * i];
+            const auto& g = sig[k];
+            if (q.kind == 1) {
+                out << i << "\t" << x[0] << "\t" << x[1] << "\t" << x[2];
+                for (int a = 0; a < 9; ++a) out << "\t" << g[a];
+                out << "\n";
+            } else {
+                out << " AFD at node " << x[0] << "\t" << x[1] << "\t" << x[2] << "\n";
+                out << " sigma11 = " << g[0] << " sigma12 = " << g[1] << " sigma13 = " << g[2] << "\n"
+                    << " sigma21 = " << g[3] << " sigma22 = " << g[4] << " sigma23 = " << g[5] << "\n"
+                    << " sigma31 = " << g[6] << " sigma32 = " << g[7] << " sigma33 = " << g[8] << "\n\n";
+            }
+        }
+    }
     return PD_OK;
 }
 

@@ -225,6 +225,18 @@ public:
     static int SolveStatic(pdDataManager& dat, int precision = PD_PREC_FP64, double rtol = 1e-10,
                            bool write_files = true);
     static int WriteTecplot(pdDataManager& dat, int step, double time);
+    // pdSolve::PostAFD (pdSolve.cpp:810-834, pdDataManager3.cpp:1101-1223)
+    // without the console: reads pds_tecplot_<step>.dat and writes the areal
+    // force density stress of every request to pds_AFD_<step>.dat.  A
+    // request is a plane (kind 1: every node whose coordinate along `norm`
+    // equals `coord`) or one node (kind 2: `node`).
+    struct AfdRequest {
+        int kind;
+        int norm;
+        double coord;
+        int64_t node;
+    };
+    static int PostAFD(pdDataManager& dat, int step, const std::vector<AfdRequest>& requests);
 };
 
 // MLS/bdryEff/search helpers shared by the setup code (pd_setup.cpp)

@@ -205,6 +205,14 @@ int pdh_context(pdh_model* m, pd_ctx** ctx) {
 
 int pdh_set_precision(pdh_model* m, int p) { return m ? track(m, m->dat.SetPrecision(p)) : PD_ERR_ARG; }
 
+int pdh_post_afd(pdh_model* m, int step, int n, const int32_t* kind, const int32_t* norm, const double* coord,
+                 const int64_t* node) {
+    if (!m || n < 0 || (n > 0 && (!kind || !norm || !coord || !node))) return PD_ERR_ARG;
+    std::vector<pdh::pdSolve::AfdRequest> req((size_t)n);
+    for (int k = 0; k < n; ++k) req[k] = {kind[k], norm[k], coord[k], node[k]};
+    return track(m, pdh::pdSolve::PostAFD(m->dat, step, req));
+}
+
 int pdh_set_device_setup(pdh_model* m, int on) {
     if (!m) return PD_ERR_ARG;
     m->dat.SetDeviceSetup(on != 0);

@@ -45,7 +45,8 @@ struct pd_ctx {
     int precision = PD_PREC_FP64;
     int nslit = 0;
     std::vector<double> coords;  // [N][3] host copy
-    std::vector<double> abscis;  // 1-D Gauss abscissae (FGI)
+    std::vector<double> abscis;  // 1-D Gauss abscissae and weights (FGI)
+    std::vector<double> gweights;
     std::vector<double> slits;
     double* dslits = nullptr;   // [nslit][6] on the device
     std::vector<pd::GaussConst> gch;            // Gauss constants (host copy)
@@ -367,6 +368,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     c->npt = n1 * n1 * n1;
     c->coords.assign(P->coords, P->coords + 3 * N);
     if (P->integration == PD_INTG_FGI && P->abscissae) c->abscis.assign(P->abscissae, P->abscissae + n1);
+    if (P->integration == PD_INTG_FGI && P->weights) c->gweights.assign(P->weights, P->weights + n1);
     c->nslit = P->num_slits > 0 ? P->num_slits : 0;
     if (c->nslit) c->slits.assign(P->slits, P->slits + 6 * c->nslit);
     pd::Dev& d = c->d;
@@ -1184,6 +1186,57 @@ int pd_mls_setup(pd_ctx* c, double rw, const double* mls_coords, int64_t* num_co
     if (T) PD_CUDA_TRY(cudaMemcpy(c->cbidx_host.data(), c->cbidx, sizeof(int32_t) * T, cudaMemcpyDeviceToHost));
     if (num_contrib) *num_contrib = T;
     return mls_installed(c);
+}
+
+// Half-space bond-force sums of PostAFD (k_afd_gauss, k_afd_items).
+int pd_afd(pd_ctx* c, const double* U, const double* bdry_eff, int64_t n_items, const int64_t* item_i,
+           const int64_t* item_s, const int32_t* item_dir, double* force) {
+    if (!c || !U || !bdry_eff || n_items < 0 || (n_items > 0 && (!item_i || !item_s || !item_dir || !force)))
+        return fail(PD_ERR_ARG, "pd_afd: null argument");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_afd: no family");
+    if (!c->d.cci && c->d.mls && !c->have_mls) return fail(PD_ERR_ARG, "pd_afd: no MLS data");
+    if (!c->d.cci && (c->abscis.empty() || c->gweights.size() != c->abscis.size()))
+        return fail(PD_ERR_ARG, "pd_afd: no Gauss rule");
+    const int64_t N = c->n;
+    for (int64_t k = 0; k < n_items; ++k)
+        if (item_i[k] < 0 || item_i[k] >= N || item_s[k] < 0 || item_s[k] >= N || item_dir[k] < 1 || item_dir[k] > 3)
+            return fail(PD_ERR_ARG, "pd_afd: item out of range");
+    if (n_items == 0 || N == 0) return PD_OK;
+    const int n1 = c->d.cci ? 1 : (int)c->abscis.size();
+    double *Ud = nullptr, *bEd = nullptr, *ug = nullptr, *ab = nullptr, *wt = nullptr, *out = nullptr;
+    int64_t *ii = nullptr, *ss = nullptr;
+    int32_t* dd = nullptr;
+    auto cleanup = [&]() {
+        for (void* p : {(void*)Ud, (void*)bEd, (void*)ug, (void*)ab, (void*)wt, (void*)out, (void*)ii, (void*)ss,
+                        (void*)dd})
+            dfree(c, p);
+    };
+    const std::vector<double> one{0.0};
+    const std::vector<double> two{2.0};
+    const std::vector<double>& av = c->d.cci ? one : c->abscis;
+    const std::vector<double>& wv = c->d.cci ? two : c->gweights;
+    int rc = PD_OK;
+    if ((rc = dalloc(c, &Ud, (size_t)(3 * N))) || (rc = dalloc(c, &bEd, (size_t)N)) ||
+        (rc = dalloc(c, &ug, (size_t)(3 * N * c->npt))) || (rc = dalloc(c, &ab, (size_t)n1)) ||
+        (rc = dalloc(c, &wt, (size_t)n1)) || (rc = dalloc(c, &out, (size_t)(3 * n_items))) ||
+        (rc = dalloc(c, &ii, (size_t)n_items)) || (rc = dalloc(c, &ss, (size_t)n_items)) ||
+        (rc = dalloc(c, &dd, (size_t)n_items)) || (rc = upload_vec3(c, Ud, U)) ||
+        (rc = upload(c, bEd, bdry_eff, sizeof(double) * N)) || (rc = upload(c, ab, av.data(), sizeof(double) * n1)) ||
+        (rc = upload(c, wt, wv.data(), sizeof(double) * n1)) ||
+        (rc = upload(c, ii, item_i, sizeof(int64_t) * n_items)) ||
+        (rc = upload(c, ss, item_s, sizeof(int64_t) * n_items)) ||
+        (rc = upload(c, dd, item_dir, sizeof(int32_t) * n_items))) {
+        cleanup();
+        return rc;
+    }
+    rc = pd::afd_forces(c->d, Ud, bEd, ug, ab, wt, n1, n_items, ii, ss, dd, out, c->stream);
+    if (rc == PD_OK) {
+        const cudaError_t e = cudaMemcpyAsync(force, out, sizeof(double) * 3 * n_items, cudaMemcpyDeviceToHost,
+                                              c->stream);
+        if (e != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) rc = PD_ERR_CUDA;
+    }
+    cleanup();
+    return rc == PD_OK ? PD_OK : fail(rc, "pd_afd: device computation failed");
 }
 
 // The MLS data out, in the layout pd_set_mls takes (coeff [node][point][contributor]).

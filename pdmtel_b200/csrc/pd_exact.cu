@@ -1377,3 +1377,188 @@ extern "C" int pd_bond_search_noalloc(const double* coords, int64_t n, double gr
     PD_CUDA_TRY(cudaStreamSynchronize(st));
     return PD_OK;
 }
+
+namespace pd {
+
+// ================================================== areal force density
+//
+// pdSolve::PostAFD (pdSolve.cpp:810-834, pdDataManager3.cpp:442-635,
+// 1101-1223): the stress tensor at a source node s from the areal force
+// density.  For each direction d and each node i at s - (1 + is) dx e_d
+// (is < int(horizon / dx)), the bond forces of i with every node j of its
+// family that lies in the source's half space x_j,d >= x_s,d are summed.
+// Here one thread takes one (i, s, d) item; the host builds the items and
+// adds them up in the reference's order.
+
+// Gauss-point displacements as PostAFD derives them from a Tecplot dump
+// (pdDataManager.cpp:2704-2752, CalcApproxDispl, or the copy of the one-point
+// rule): the MLS sum of the nodal displacements u_k c_k on every node, except
+// that a direction a boundary condition flags keeps its Gauss points at zero
+// (they are never set in a post-processing run).
+__global__ void k_afd_gauss(Dev d, const double* __restrict__ U, double* __restrict__ ug) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int64_t N = d.n;
+    const int npt = d.npt;
+    bool flagged[3] = {false, false, false};
+    if (d.bc[i] >= 0)
+        for (int a = 0; a < 3; ++a) flagged[a] = d.bcs[d.bc[i]].dir[a] == 1;
+    for (int g = 0; g < npt; ++g) {
+        double v[3] = {0.0, 0.0, 0.0};
+        if (d.mls) {
+            const int64_t b = d.cbptr[i], nc = d.cbptr[i + 1] - b;
+            for (int64_t k = 0; k < nc; ++k) {
+                const int64_t m = d.cbidx[b + k];
+                const double c = d.coeff[(b + k) * npt + g];
+                v[0] += U[m] * c;
+                v[1] += U[N + m] * c;
+                v[2] += U[2 * N + m] * c;
+            }
+            for (int a = 0; a < 3; ++a)
+                if (flagged[a]) v[a] = 0.0;
+        } else {
+            for (int a = 0; a < 3; ++a) v[a] = U[a * N + i];
+        }
+        for (int a = 0; a < 3; ++a) ug[(int64_t)(3 * g + a) * N + i] = v[a];
+    }
+}
+
+// pdIntgManager::CalcBondBasedForce (pdIntgManager2.cpp:92-310), fixed
+// Gauss points: the point at local position (X, Y, Z) from node i, with the
+// displacement of cell j's point g
+__device__ __forceinline__ void afd_point(const Dev& d, double X, double Y, double Z, const double* ugj, double ui0,
+                                          double ui1, double ui2, double bE, double spring, double ecrit,
+                                          double dxe, double* f) {
+    const double xi1 = X - 0.0, xi2 = Y - 0.0, xi3 = Z - 0.0;
+    const double eta1 = ugj[0] - ui0, eta2 = ugj[1] - ui1, eta3 = ugj[2] - ui2;
+    const double r = sqrt(xi1 * xi1 + xi2 * xi2 + xi3 * xi3);
+    const double y1 = xi1 + eta1, y2 = xi2 + eta2, y3 = xi3 + eta3;
+    const double p = sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+    const double beta = beta_factor(r, d.delta, dxe, false);
+    const double u = p - r;
+    const double stretch = u / r;
+    if (u <= 0.0 || (u > 0.0 && stretch <= ecrit)) {
+        f[0] = bE * beta * spring * stretch * y1 / p;
+        f[1] = bE * beta * spring * stretch * y2 / p;
+        f[2] = bE * beta * spring * stretch * y3 / p;
+    } else {
+        f[0] = f[1] = f[2] = 0.0;
+    }
+}
+
+__global__ void k_afd_items(Dev d, const double* __restrict__ U, const double* __restrict__ bE,
+                            const double* __restrict__ ug, const double* __restrict__ absc,
+                            const double* __restrict__ wts, int n1, int64_t n_items,
+                            const int64_t* __restrict__ item_i, const int64_t* __restrict__ item_s,
+                            const int32_t* __restrict__ item_d, double* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n_items) return;
+    const int64_t N = d.n;
+    const int64_t i = item_i[t], s = item_s[t];
+    const int dir = item_d[t] - 1;
+    const double pi[3] = {d.x[i], d.x[N + i], d.x[2 * N + i]};
+    const double xs_d = d.x[dir * N + s];
+    const double ui0 = U[i], ui1 = U[N + i], ui2 = U[2 * N + i];
+    const MatDev& Mi = d.mats[d.mat[i]];
+    const double dx = d.dx, tol = 1.0e-4 * dx;
+    double sum0 = 0.0, sum1 = 0.0, sum2 = 0.0;
+    for (int64_t p = d.frow[i]; p < d.frow[i + 1]; ++p) {
+        const int64_t j = d.fcol[p];
+        const double pj[3] = {d.x[j], d.x[N + j], d.x[2 * N + j]};
+        if (!(pj[dir] - xs_d >= 0.0)) continue;  // the source's R+ space
+        const MatDev& Mj = d.mats[d.mat[j]];
+        const double ecrit = dmin(Mi.ecrit, Mj.ecrit);
+        const double spring = dmin(Mi.spring, Mj.spring);
+        const double bEij = 0.5 * (bE[i] + bE[j]);
+        double f[3] = {0.0, 0.0, 0.0};
+        if (d.cci) {
+            // pdDataManager::CalcBondForceCCI(bond, i, j), pdDataManager2.cpp:1087-1154
+            const double xi1 = pj[0] - pi[0], xi2 = pj[1] - pi[1], xi3 = pj[2] - pi[2];
+            const double eta1 = U[j] - ui0, eta2 = U[N + j] - ui1, eta3 = U[2 * N + j] - ui2;
+            const double r = sqrt(xi1 * xi1 + xi2 * xi2 + xi3 * xi3);
+            const double y1 = xi1 + eta1, y2 = xi2 + eta2, y3 = xi3 + eta3;
+            const double pl = sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+            const double u = pl - r;
+            const double stretch = u / r;
+            if (u <= 0.0 || (u > 0.0 && stretch <= ecrit)) {
+                const double beta = beta_factor(r, d.delta, dx, !d.cci_mdf);
+                const double vol = d.vol;
+                f[0] = bEij * vol * beta * spring * stretch * y1 / pl;
+                f[1] = bEij * vol * beta * spring * stretch * y2 / pl;
+                f[2] = bEij * vol * beta * spring * stretch * y3 / pl;
+            }
+        } else {
+            // CalcBondForceIntg (pdDataManager2.cpp:1156-1215): nothing when
+            // the cell lies beyond the horizon, else the cell's fixed Gauss
+            // rule as pdIntgManager::CalcConfigurationType3 / CalcIntg3D /
+            // CalcGaussianQuad nest it (pdIntgManager.cpp:49-128,453-509,
+            // 3471-3482), in local coordinates x_j - x_i
+            double mn = kMega, a, b;
+            for (int ax = 0; ax < 3; ++ax) {
+                dist_to_face(ax + 1, pj[ax] - 0.5 * dx, pi, pj, dx, &a, &b);
+                mn = dmin(mn, a);
+                dist_to_face(ax + 1, pj[ax] + 0.5 * dx, pi, pj, dx, &a, &b);
+                mn = dmin(mn, a);
+            }
+            if (!(d.delta <= mn)) {
+                const double x1j = pj[0] - pi[0], x2j = pj[1] - pi[1], x3j = pj[2] - pi[2];
+                const double lo1 = x1j - 0.5 * dx, hi1 = x1j + 0.5 * dx;
+                const double lo2 = x2j - 0.5 * dx, hi2 = x2j + 0.5 * dx;
+                const double lo3 = x3j - 0.5 * dx, hi3 = x3j + 0.5 * dx;
+                int counter = 0;  // _intgPointCounter: the Gauss point of cell j
+                if (fabs(lo1 - hi1) > 1.0e-10) {
+                    double S1[3] = {0.0, 0.0, 0.0};
+                    for (int q1 = 0; q1 < n1; ++q1) {
+                        const double X = 0.5 * dx * absc[q1] + x1j;
+                        double F2[3] = {0.0, 0.0, 0.0};
+                        if (fabs(lo2 - hi2) > 1.0e-10) {
+                            double S2[3] = {0.0, 0.0, 0.0};
+                            for (int q2 = 0; q2 < n1; ++q2) {
+                                const double Y = 0.5 * dx * absc[q2] + x2j;
+                                double F3[3] = {0.0, 0.0, 0.0};
+                                if (fabs(lo3 - hi3) > 1.0e-10) {
+                                    double S3[3] = {0.0, 0.0, 0.0};
+                                    for (int q3 = 0; q3 < n1; ++q3) {
+                                        const double Z = 0.5 * dx * absc[q3] + x3j;
+                                        const double ugj[3] = {ug[(int64_t)(3 * counter) * N + j],
+                                                               ug[(int64_t)(3 * counter + 1) * N + j],
+                                                               ug[(int64_t)(3 * counter + 2) * N + j]};
+                                        double fp[3];
+                                        afd_point(d, X, Y, Z, ugj, ui0, ui1, ui2, bEij, spring, ecrit,
+                                                  d.gc[counter].dxe, fp);
+                                        ++counter;
+                                        for (int c = 0; c < 3; ++c) S3[c] += wts[q3] * fp[c];
+                                    }
+                                    for (int c = 0; c < 3; ++c) F3[c] = S3[c] * (0.5 * (hi3 - lo3));
+                                }
+                                for (int c = 0; c < 3; ++c) S2[c] += wts[q2] * F3[c];
+                            }
+                            for (int c = 0; c < 3; ++c) F2[c] = S2[c] * (0.5 * (hi2 - lo2));
+                        }
+                        for (int c = 0; c < 3; ++c) S1[c] += wts[q1] * F2[c];
+                    }
+                    for (int c = 0; c < 3; ++c) f[c] = S1[c] * (0.5 * (hi1 - lo1));
+                }
+            }
+        }
+        sum0 += f[0];
+        sum1 += f[1];
+        sum2 += f[2];
+    }
+    (void)tol;
+    out[3 * t] = sum0;
+    out[3 * t + 1] = sum1;
+    out[3 * t + 2] = sum2;
+}
+
+int afd_forces(const Dev& d, const double* U, const double* bE, double* ug, const double* absc, const double* wts,
+               int n1, int64_t n_items, const int64_t* item_i, const int64_t* item_s, const int32_t* item_d,
+               double* out, cudaStream_t s) {
+    if (d.n == 0 || n_items == 0) return PD_OK;
+    k_afd_gauss<<<(unsigned)((d.n + 127) / 128), 128, 0, s>>>(d, U, ug);
+    k_afd_items<<<(unsigned)((n_items + 63) / 64), 64, 0, s>>>(d, U, bE, ug, absc, wts, n1, n_items, item_i, item_s,
+                                                               item_d, out);
+    return cudaGetLastError() == cudaSuccess ? PD_OK : PD_ERR_CUDA;
+}
+
+}  // namespace pd

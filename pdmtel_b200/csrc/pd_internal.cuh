@@ -162,6 +162,13 @@ void launch_energy_reduce(const Dev& d, cudaStream_t s);
 int mls_setup(const Dev& d, const double* xm, double rw, const double* absc, int n1, int64_t* cnt, int64_t* cbptr,
               int32_t** cbidx, double** coeff, float** coeff32, float** csum, int64_t* total, int64_t* bad_node,
               void* (*alloc)(void*, size_t), void* actx, cudaStream_t s);
+// PostAFD on the device (k_afd_gauss, k_afd_items): Gauss-point displacements
+// of the nodal U [3][N] into ug [npt*3][N], then per item (node i, source s,
+// direction 1..3) the half-space bond-force sum into out [items][3]; bE [N]
+// the boundary factors to use, absc / wts the 1-D Gauss rule (n1 points).
+int afd_forces(const Dev& d, const double* U, const double* bE, double* ug, const double* absc, const double* wts,
+               int n1, int64_t n_items, const int64_t* item_i, const int64_t* item_s, const int32_t* item_d,
+               double* out, cudaStream_t s);
 void launch_to_soa(const double* aos, double* soa, int64_t n, int comps, cudaStream_t s);
 void launch_to_soa_changed(const double* aos, double* soa, int64_t n, int comps, int* changed, cudaStream_t s);
 void launch_to_aos(const double* soa, double* aos, int64_t n, int comps, cudaStream_t s);

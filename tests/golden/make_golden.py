@@ -337,6 +337,23 @@ def output_cases():
     return out
 
 
+# PostAFD's console answers per case: the Tecplot step to read, then planes
+# (1, normal, location) and single nodes (2, id), "y" between runs, "n" last
+AFD_SCRIPTS = {
+    "out_fgi": ("7", [("1", "1", "0.0005"), ("1", "2", "-0.0005"), ("1", "3", "0.0005"), ("2", "10"), ("2", "100")]),
+    "out_cci": ("5", [("1", "1", "1"), ("1", "2", "-1"), ("1", "3", "1"), ("2", "20")]),
+}
+
+
+def afd_script(case):
+    step, runs = AFD_SCRIPTS[case]
+    lines = [step]
+    for k, r in enumerate(runs):
+        lines += list(r)
+        lines.append("y" if k + 1 < len(runs) else "n")
+    return "\n".join(lines) + "\n"
+
+
 def make_outputs():
     import glob
     out_dir = os.path.join(HERE, "outputs")
@@ -355,6 +372,14 @@ def make_outputs():
         for f in files:
             shutil.copy(f, os.path.join(cdir, "ref_" + os.path.basename(f)))
         print(name, [os.path.basename(f) for f in files])
+        # PostAFD on the last Tecplot dump (the answers it reads from the console)
+        with open(os.path.join(wd, "afd_script.txt"), "w") as f:
+            f.write(afd_script(name))
+        r = subprocess.run([HARNESS, "afd", wd, os.path.join(wd, "afd_script.txt")], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"harness afd {name} failed: {r.stderr[-400:]}")
+        step = AFD_SCRIPTS[name][0]
+        shutil.copy(os.path.join(wd, f"pds_AFD_{step}.dat"), os.path.join(cdir, f"ref_afd_pds_AFD_{step}.dat"))
     shutil.rmtree(tmp, ignore_errors=True)
 
 
