@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -89,6 +90,8 @@ struct pd_ctx {
     double4* sten_geo = nullptr;
     uint8_t* sten_pmask = nullptr;
     double* sten_xm = nullptr;
+    int4* sten_col = nullptr;
+    double4* sten_colgeo = nullptr;
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
@@ -1776,18 +1779,50 @@ int static_prepare(pd_ctx* c) {
         geo[k] = make_double4(e0, e1, e2, cv / (r2 * r));
         for (int a = 0; a < 3; ++a) radius = std::max(radius, std::abs(o[a]));
     }
+    // the same stencil by (ox, oy) columns with a dense oz window (the
+    // z-blocked kernel), when no offset reaches beyond 4 along z
+    int rz = 0;
+    for (const auto& o : offs) rz = std::max(rz, std::abs(o[2]));
+    std::vector<int4> cols;
+    std::vector<double4> colgeo;
+    if (rz >= 1 && rz <= 4) {
+        const int W = 2 * rz + 1;
+        std::map<std::pair<int, int>, int> at;  // (oy, ox) -> column
+        for (int k = 0; k < ns; ++k) {
+            const auto key = std::make_pair(offs[k][1], offs[k][0]);
+            if (!at.count(key)) at[key] = 0;
+        }
+        int nc = 0;
+        for (auto& kv : at) {
+            kv.second = nc++;
+            cols.push_back(make_int4(kv.first.second, kv.first.first, (int)(kv.first.second + nx * kv.first.first), 0));
+        }
+        colgeo.assign((size_t)nc * W, make_double4(0.0, 0.0, 0.0, 0.0));
+        for (int k = 0; k < ns; ++k) {
+            const int cidx = at[std::make_pair(offs[k][1], offs[k][0])];
+            colgeo[(size_t)cidx * W + offs[k][2] + rz] = geo[k];
+        }
+    }
     if (!c->sten_off) {
         PD_TRY(dalloc(c, &c->sten_off, pd::kMaxStencil));
         PD_TRY(dalloc(c, &c->sten_geo, pd::kMaxStencil));
         PD_TRY(dalloc(c, &c->sten_pmask, N));
         PD_TRY(dalloc(c, &c->sten_xm, 3 * N));
+        PD_TRY(dalloc(c, &c->sten_col, pd::kMaxStencil));
+        PD_TRY(dalloc(c, &c->sten_colgeo, (size_t)pd::kMaxStencil * 9));
     }
     PD_TRY(upload(c, c->sten_off, off.data(), sizeof(int4) * ns));
     PD_TRY(upload(c, c->sten_geo, geo.data(), sizeof(double4) * ns));
+    if (!cols.empty() && cols.size() <= (size_t)pd::kMaxStencil && colgeo.size() <= (size_t)pd::kMaxStencil * 9) {
+        PD_TRY(upload(c, c->sten_col, cols.data(), sizeof(int4) * cols.size()));
+        PD_TRY(upload(c, c->sten_colgeo, colgeo.data(), sizeof(double4) * colgeo.size()));
+    } else {
+        cols.clear();
+    }
     pd::launch_static_pmask(c->d, c->sten_pmask, c->stream);
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->sten = pd::StencilDev{(int)nx, (int)ny, (int)nz, ns, radius, c->sten_off, c->sten_geo, c->sten_pmask,
-                             c->sten_xm};
+                             c->sten_xm, (int)cols.size(), rz, c->sten_col, c->sten_colgeo};
     c->sten_ok = true;
     return PD_OK;
 }

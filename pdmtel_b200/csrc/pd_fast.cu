@@ -1,6 +1,7 @@
 // The static operator (FP64 and FP32 matvec, right-hand side), the CG pieces,
 // scans and reductions.
 #include <cstdio>
+#include <type_traits>
 
 #include "pd_internal.cuh"
 
@@ -300,6 +301,107 @@ __global__ void k_bj_apply(const double* __restrict__ minv, const double* __rest
     }
 }
 
+// The same operator blocked along z: a thread owns R consecutive nodes of a
+// z column, (ix, iy, iz0 .. iz0 + R - 1), and walks the stencil by (ox, oy)
+// columns; every neighbour value of a column window z in [iz0 - rz, iz0 + R
+// - 1 + rz] is loaded once and serves the up to 2 rz + 1 bonds of the R nodes
+// that reach it, so a node needs (R + 2 rz) / R loads per column instead of
+// one per bond.  The oz window is padded with zero weights where an offset is
+// not in the stencil.  Sums per node in column order; FP32 bond terms are
+// added in FP32 over four columns, then to the FP64 sum.
+template <typename T, bool SFAC, int RZ, int R>
+__global__ void __launch_bounds__(128) k_static_zcol(Dev d, StencilDev S, const double* __restrict__ x,
+                                                     const T* __restrict__ xm, double* __restrict__ y) {
+    constexpr int W = 2 * RZ + 1;
+    using G = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
+    extern __shared__ double4 zsm[];
+    G* geo = reinterpret_cast<G*>(zsm);
+    int4* cols = reinterpret_cast<int4*>(geo + S.ncol * W);
+    for (int k = threadIdx.x; k < S.ncol * W; k += blockDim.x) {
+        const double4 g = S.colgeo[k];
+        geo[k] = G{(T)g.x, (T)g.y, (T)g.z, (T)g.w};
+    }
+    for (int k = threadIdx.x; k < S.ncol; k += blockDim.x) cols[k] = S.col[k];
+    __syncthreads();
+    const int64_t N = d.n, nxy = (int64_t)S.nx * S.ny;
+    const int ix = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int iy = blockIdx.y * 4 + (threadIdx.x >> 5);
+    const int iz0 = blockIdx.z * R;
+    const bool in_xy = ix < S.nx && iy < S.ny;
+    const int64_t i0 = ix + (int64_t)S.nx * iy + nxy * iz0;
+    T xi[R][3];
+    double sfi[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        const bool v = in_xy && iz0 + m < S.nz;
+        for (int a = 0; a < 3; ++a) xi[m][a] = v ? xm[a * N + i0 + m * nxy] : (T)0;
+        sfi[m] = (SFAC && v) ? d.sfac[i0 + m * nxy] : 0.0;
+    }
+    double acc[R][3];
+    T part[R][3];
+#pragma unroll
+    for (int m = 0; m < R; ++m)
+        for (int a = 0; a < 3; ++a) acc[m][a] = 0.0, part[m][a] = (T)0;
+    for (int c = 0; c < S.ncol; ++c) {
+        const int4 C = cols[c];
+        const bool cv = in_xy && (unsigned)(ix + C.x) < (unsigned)S.nx && (unsigned)(iy + C.y) < (unsigned)S.ny;
+        G g[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) g[q] = geo[c * W + q];
+#pragma unroll
+        for (int zz = -RZ; zz < R + RZ; ++zz) {
+            const int jz = iz0 + zz;
+            if (!cv || jz < 0 || jz >= S.nz) continue;
+            const int64_t j = i0 + C.z + nxy * zz;
+            const T xj0 = xm[j], xj1 = xm[N + j], xj2 = xm[2 * N + j];
+            const double sfj = SFAC ? d.sfac[j] : 0.0;
+#pragma unroll
+            for (int m = 0; m < R; ++m) {
+                const int oz = zz - m;
+                if (oz < -RZ || oz > RZ) continue;
+                const G& q = g[oz + RZ];
+                T w = q.w;
+                if (SFAC) w = w * (T)(0.5 * (sfi[m] + sfj));
+                const T d0 = xi[m][0] - xj0, d1 = xi[m][1] - xj1, d2 = xi[m][2] - xj2;
+                const T pr = w * (q.x * d0 + q.y * d1 + q.z * d2);
+                part[m][0] += pr * q.x;
+                part[m][1] += pr * q.y;
+                part[m][2] += pr * q.z;
+            }
+        }
+        if (sizeof(T) == 8 || (c & 3) == 3 || c + 1 == S.ncol) {
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                for (int a = 0; a < 3; ++a) {
+                    acc[m][a] += (double)part[m][a];
+                    part[m][a] = (T)0;
+                }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        if (!in_xy || iz0 + m >= S.nz) continue;
+        const int64_t i = i0 + m * nxy;
+        const unsigned mi = S.pmask[i];
+        y[i] = (mi & 1) ? x[i] : acc[m][0];
+        y[N + i] = (mi & 2) ? x[N + i] : acc[m][1];
+        y[2 * N + i] = (mi & 4) ? x[2 * N + i] : acc[m][2];
+    }
+}
+
+template <typename T, bool SFAC, int R>
+void launch_zcol(const Dev& d, const StencilDev& S, const double* x, const T* xm, double* y, cudaStream_t s) {
+    const dim3 grid((unsigned)((S.nx + 31) / 32), (unsigned)((S.ny + 3) / 4), (unsigned)((S.nz + R - 1) / R));
+    const size_t sh = (size_t)S.ncol * (2 * S.rz + 1) * (sizeof(T) == 4 ? sizeof(float4) : sizeof(double4)) +
+                      (size_t)S.ncol * sizeof(int4);
+    switch (S.rz) {
+        case 1: k_static_zcol<T, SFAC, 1, R><<<grid, 128, sh, s>>>(d, S, x, xm, y); break;
+        case 2: k_static_zcol<T, SFAC, 2, R><<<grid, 128, sh, s>>>(d, S, x, xm, y); break;
+        case 3: k_static_zcol<T, SFAC, 3, R><<<grid, 128, sh, s>>>(d, S, x, xm, y); break;
+        default: k_static_zcol<T, SFAC, 4, R><<<grid, 128, sh, s>>>(d, S, x, xm, y); break;
+    }
+}
+
 // b = prescribed values on prescribed rows; on free rows the moved prescribed
 // columns (pdSolve.cpp:296-363 sign pattern) plus the traction load.
 template <bool SFAC>
@@ -442,16 +544,29 @@ void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const do
     if (d.n == 0) return;
     const size_t sh = (size_t)S.ns * (sizeof(double4) + sizeof(float4) + sizeof(int4));
     const unsigned nb = blocks_for(d.n, 256);
+    const bool zcol = S.ncol > 0 && S.rz >= 1 && S.rz <= 4;
     if (f32) {
         float* xm = reinterpret_cast<float*>(S.xm);
         k_static_mask<float><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
-        if (d.sfac) k_static_stencil<float, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
-        else k_static_stencil<float, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        if (zcol) {
+            if (d.sfac) launch_zcol<float, true, 8>(d, S, x, xm, y, s);
+            else launch_zcol<float, false, 8>(d, S, x, xm, y, s);
+        } else if (d.sfac) {
+            k_static_stencil<float, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        } else {
+            k_static_stencil<float, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        }
     } else {
         double* xm = S.xm;
         k_static_mask<double><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
-        if (d.sfac) k_static_stencil<double, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
-        else k_static_stencil<double, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        if (zcol) {
+            if (d.sfac) launch_zcol<double, true, 4>(d, S, x, xm, y, s);
+            else launch_zcol<double, false, 4>(d, S, x, xm, y, s);
+        } else if (d.sfac) {
+            k_static_stencil<double, true><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        } else {
+            k_static_stencil<double, false><<<nb, 256, sh, s>>>(d, S, x, xm, y);
+        }
     }
 }
 

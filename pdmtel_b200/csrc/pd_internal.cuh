@@ -258,6 +258,12 @@ struct StencilDev {
     const double4* geo;    // [ns] xi = offset * spacing, c V / r^3 of the one material
     const uint8_t* pmask;  // [N] prescribed directions, bits 0..2
     double* xm;            // [3N] scratch: the masked input (FP64, or FP32 in its first half)
+    // the stencil regrouped into (ox, oy) columns: col[c] = (ox, oy, ox + nx oy,
+    // 0) and colgeo[c][oz + rz] for oz in [-rz, rz] (c V / r^3 = 0 where the
+    // offset is not in the stencil); ncol = 0 when rz is beyond 4
+    int ncol, rz;
+    const int4* col;
+    const double4* colgeo;
 };
 void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s);
 void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const double* x, double* y, cudaStream_t s);
