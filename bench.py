@@ -540,7 +540,7 @@ def run_identify(args):
     return 0
 
 
-def static_solves(tmp, n, maxit=100000):
+def static_solves(tmp, n, maxit=100000, precond=True):
     """The static config on an n^3 cube (bottom clamped, 1 MPa shear traction
     on top): FP32 matvec with FP64 reliable updates against plain FP64 CG,
     both to relative residual 1e-10 and block-Jacobi preconditioned; device
@@ -558,6 +558,7 @@ def static_solves(tmp, n, maxit=100000):
     dm.InitMaterial()
     ctx = dm.context()
     stencil = ctx.static_prepare()
+    ctx.set_option(P.OPT_STATIC_PRECOND, int(bool(precond)))
     setup_s = time.time() - t0
     stream = torch.cuda.ExternalStream(ctx.stream)
     I = dm.info()
@@ -581,7 +582,7 @@ def static_solves(tmp, n, maxit=100000):
         r["ms_per_iteration"] = 1e3 * r["s"] / max(r["iterations"], 1)
     out = {"workload": f"cube {n}^3, bottom clamped, 1 MPa shear traction on top", "nodes": I.num_nodes,
            "bond_halves": I.num_halves, "operator": "lattice stencil (z-blocked)" if stencil else "family lists",
-           "preconditioner": "block Jacobi (3x3 diagonal blocks)",
+           "preconditioner": "block Jacobi (3x3 diagonal blocks)" if precond else "none",
            "fp32_ir": res["fp32c"], "fp64_cg": res["fp64"],
            "speedup_fp32ir_over_fp64": res["fp64"]["s"] / res["fp32c"]["s"],
            "rel_diff_fp32ir_vs_fp64": err, "setup_s": setup_s}
@@ -594,7 +595,7 @@ def run_static(args):
     import torch
     torch.cuda.set_device(0)
     tmp = tempfile.mkdtemp(prefix="pdstatic_")
-    r = static_solves(tmp, args.cube, args.maxit)
+    r = static_solves(tmp, args.cube, args.maxit, precond=not args.no_precond)
     line = {"metric": f"static solve time to relative residual 1e-10, {args.cube}^3 cube",
             "value": r["fp32_ir"]["s"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
             "ms_per_step": 1e3 * r["fp32_ir"]["s"], "higher_is_better": False, "scaling": "strong",
@@ -657,7 +658,7 @@ def apply_shape(ctx, shape):
     whose timing must not depend on a tuner, e.g. under a profiler)."""
     import pdmtel_b200 as P
     opts = [("tile", P.OPT_TILE), ("gather_per_point", P.OPT_GATHER_PER_POINT), ("gather_sell", P.OPT_GATHER_SELL),
-            ("gather_stencil", P.OPT_GATHER_STENCIL), ("gather_delta", P.OPT_GATHER_DELTA),
+            ("gather_stencil", P.OPT_GATHER_STENCIL),
             ("force_stencil", P.OPT_FORCE_STENCIL),
             ("force_quad", P.OPT_FORCE_QUAD), ("force_tile", P.OPT_FORCE_TILE)]
     for key, opt in opts:
@@ -773,14 +774,10 @@ def run_ours(args):
     force_kernel = ("k_force_f32c_sten" if sten else "k_force_f32c_quad" if tune.get("force_quad")
                     else "k_force_f32c_tiled" if tune.get("force_tile") else "k_force_f32c_pair")
     pat, sell = bool(tune.get("gather_stencil")), bool(tune.get("gather_sell"))
-    delta = pat and sell and bool(tune.get("gather_delta"))
-    gather_kernel = ("k_gather_f32c_dring" if delta else "k_gather_f32c_ring") if (pat and sell) else "k_gather_f32c"
-    # coefficients (2-byte deltas and a 4-byte scale per node and point with
-    # the delta form; the pattern table stays in L2), contributor ids (pattern
-    # ids instead with patterns), trial displacement, output blocks,
-    # partition-of-unity sums, row pointers
-    coef_bytes = ncb * npt * 2 + n * npt * 4 if delta else ncb * npt * 4
-    gather_bytes = (coef_bytes + (n * 4 if pat else ncb * 4 + (n + 1) * 8) + n * 8 * 4 + n * npt * 12
+    gather_kernel = "k_gather_f32c_ring" if (pat and sell) else "k_gather_f32c"
+    # coefficients, contributor ids (pattern ids instead with patterns), trial
+    # displacement, output blocks, partition-of-unity sums, row pointers
+    gather_bytes = (ncb * npt * 4 + (n * 4 if pat else ncb * 4 + (n + 1) * 8) + n * 8 * 4 + n * npt * 12
                     + n * npt * 4)
     force_flops = FLOP_PER_EVAL * evals_stage
     traffic = None
@@ -854,7 +851,7 @@ def main():
     ap.add_argument("--no-static", action="store_true", help="leave the static solve out of the headline line")
     ap.add_argument("--shape", default=None,
                     help="skip pd_autotune and apply these launch shapes, a JSON object with keys of its result "
-                         "(tile, gather_per_point, gather_sell, gather_stencil, gather_delta, force_stencil, force_quad, "
+                         "(tile, gather_per_point, gather_sell, gather_stencil, force_stencil, force_quad, "
                          "force_tile)")
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--form", default="precision",
@@ -863,6 +860,7 @@ def main():
     ap.add_argument("--prec", default="fp32c", choices=["fp32c", "fp64"], help="arithmetic of --form steps")
     ap.add_argument("--cube", type=int, default=128, help="cube side of --form static")
     ap.add_argument("--maxit", type=int, default=100000, help="CG iteration cap of --form static")
+    ap.add_argument("--no-precond", action="store_true", help="--form static: plain CG, no block Jacobi")
     ap.add_argument("--ident-dims", default="64x64x8")
     ap.add_argument("--ident-steps", type=int, default=1000)
     ap.add_argument("--fd-dirs", type=int, default=32)

@@ -343,14 +343,6 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   contributors in the same order: same results bit for bit.  Refused
  *   (PD_ERR_ARG) when the distinct patterns would hold more than 4M
  *   entries; 0 (default) reads the lists.
- * PD_OPT_GATHER_DELTA: 1 makes the FP32-form gather with the SELL copy and
- *   the patterns both on (the coefficient ring) read each coefficient as a
- *   2-byte delta from its pattern's coefficient (half the bytes of the
- *   FP32 stream).  The FP32 coefficients of every 2x2x2-point problem with
- *   patterns are defined this way (pattern coefficient + per-point scale x
- *   int16 delta, within FP32 rounding of the FP64 ones), so every FP32
- *   gather gives the same result bit for bit.  Refused (PD_ERR_ARG) without
- *   that form; 0 (default) off.
  * PD_OPT_STATIC_PRECOND: 1 (default) preconditions the static CG with the
  *   inverses of the operator's 3x3 diagonal blocks (block Jacobi); 0 runs
  *   plain CG.  Changes the iterates, not the solution beyond the tolerance. */
@@ -369,8 +361,7 @@ enum {
     PD_OPT_GATHER_SELL = 12,
     PD_OPT_FORCE_STENCIL = 13,
     PD_OPT_GATHER_STENCIL = 14,
-    PD_OPT_GATHER_DELTA = 15,
-    PD_OPT_STATIC_PRECOND = 16
+    PD_OPT_STATIC_PRECOND = 15
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
@@ -401,8 +392,6 @@ typedef struct pd_tune_result {
     int32_t gather_sell;      /* PD_OPT_GATHER_SELL kept */
     int32_t force_stencil;    /* PD_OPT_FORCE_STENCIL kept */
     int32_t gather_stencil;   /* PD_OPT_GATHER_STENCIL kept */
-    int32_t gather_delta;     /* PD_OPT_GATHER_DELTA kept */
-    int32_t pad2;
 } pd_tune_result;
 /* Times candidate launch shapes (node-order tiles, the FP32 gather variants:
  * per point, SELL copy, contributor patterns;

@@ -31,8 +31,7 @@ PREC_FP64, PREC_FP32C, PREC_FP64A = 0, 1, 2
 OPT_F64_LANES_BELOW, OPT_TILE, OPT_PERSIST_BLOCKS_PER_SM = 1, 2, 3
 OPT_PERSIST_FORCE_CHUNK, OPT_PERSIST_GATHER_CHUNK, OPT_STATIC_STENCIL, OPT_GATHER_PER_POINT = 4, 5, 6, 7
 OPT_FORCE_TILE, OPT_FORCE_QUAD, OPT_PERSIST_WAIT_US, OPT_PERSIST_TEST_STALL = 8, 9, 10, 11
-OPT_GATHER_SELL, OPT_FORCE_STENCIL, OPT_GATHER_STENCIL, OPT_GATHER_DELTA = 12, 13, 14, 15
-OPT_STATIC_PRECOND = 16
+OPT_GATHER_SELL, OPT_FORCE_STENCIL, OPT_GATHER_STENCIL, OPT_STATIC_PRECOND = 12, 13, 14, 15
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}
@@ -85,8 +84,7 @@ class pd_tune_result(C.Structure):
                 ("force_chunk", C.c_int32), ("gather_chunk", C.c_int32), ("trials", C.c_int32),
                 ("ms_per_step", C.c_double), ("gather_per_point", C.c_int32), ("pad", C.c_int32),
                 ("force_tile", C.c_int64), ("force_quad", C.c_int32), ("gather_sell", C.c_int32),
-                ("force_stencil", C.c_int32), ("gather_stencil", C.c_int32), ("gather_delta", C.c_int32),
-                ("pad2", C.c_int32)]
+                ("force_stencil", C.c_int32), ("gather_stencil", C.c_int32)]
 
 
 # name -> argtypes; every entry point returns int

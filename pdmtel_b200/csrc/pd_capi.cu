@@ -97,11 +97,6 @@ struct pd_ctx {
     int32_t *tj = nullptr, *tpos = nullptr;
     int gpat_opt = 0;             // FP32 gather from contributor patterns (PD_OPT_GATHER_STENCIL)
     bool have_gpat = false;       // patterns built (with the MLS data; refused when nothing repeats)
-    bool have_delta = false;      // delta form of the FP32 coefficients built
-    float* cpat = nullptr;        // delta form: pattern table, scales, CSR deltas, SELL copy
-    float* cscale = nullptr;
-    int16_t* cd16 = nullptr;
-    int16_t* sell_d16 = nullptr;
     int32_t* gpat_id = nullptr;
     int64_t* gpat_ptr = nullptr;
     int32_t* gpat_off = nullptr;
@@ -603,15 +598,12 @@ static int sell_prepare(pd_ctx* c) {
     dfree(c, c->sell_off);
     dfree(c, c->sell_idx);
     dfree(c, c->sell_coef);
-    dfree(c, c->sell_d16);
     c->sell_off = nullptr;
     c->sell_idx = nullptr;
     c->sell_coef = nullptr;
-    c->sell_d16 = nullptr;
     c->d.sell_off = nullptr;
     c->d.sell_idx = nullptr;
     c->d.sell_coef = nullptr;
-    c->d.sell_d16 = nullptr;
     if (!c->d.sell_on || !c->have_mls || !c->d.mls || c->npt != 8 || c->n == 0) return PD_OK;
     const int64_t S = pd::sell_slices(c->d);
     int64_t* width = nullptr;
@@ -625,12 +617,10 @@ static int sell_prepare(pd_ctx* c) {
     PD_CUDA_TRY(cudaMemcpy(&total, c->sell_off + S, sizeof(int64_t), cudaMemcpyDeviceToHost));
     PD_TRY(dalloc(c, &c->sell_idx, total * 16));
     PD_TRY(dalloc(c, &c->sell_coef, total * 16 * 8));
-    if (c->have_delta) PD_TRY(dalloc(c, &c->sell_d16, total * 16 * 8));
     c->d.sell_off = c->sell_off;
     c->d.sell_idx = c->sell_idx;
     c->d.sell_coef = c->sell_coef;
-    c->d.sell_d16 = c->sell_d16;
-    pd::launch_sell_fill(c->d, c->sell_off, c->sell_idx, c->sell_coef, c->sell_d16, c->stream);
+    pd::launch_sell_fill(c->d, c->sell_off, c->sell_idx, c->sell_coef, c->stream);
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->generation++;
     return PD_OK;
@@ -640,27 +630,18 @@ static int sell_prepare(pd_ctx* c) {
 // list as id offsets from the node, identical lists stored once (on a box
 // lattice numbered x + nx (y + ny z) the lists of nodes with the same
 // position relative to the boundary are translates of each other).  Built
-// with the MLS data (pd_set_mls), whether or not a gather uses them, because
-// the FP32 coefficients of 2x2x2-point problems are defined from them (the
-// delta form below).  No patterns when the distinct lists would hold more
-// than 4M entries (nothing repeats).
+// with the MLS data (pd_set_mls), whether or not a gather uses them.  No
+// patterns when the distinct lists would hold more than 4M entries (nothing
+// repeats).
 static void gpat_free(pd_ctx* c) {
-    for (void* p : {(void*)c->gpat_id, (void*)c->gpat_ptr, (void*)c->gpat_off, (void*)c->cpat, (void*)c->cscale,
-                    (void*)c->cd16})
-        dfree(c, p);
+    for (void* p : {(void*)c->gpat_id, (void*)c->gpat_ptr, (void*)c->gpat_off}) dfree(c, p);
     c->gpat_id = nullptr;
     c->gpat_ptr = nullptr;
     c->gpat_off = nullptr;
-    c->cpat = nullptr;
-    c->cscale = nullptr;
-    c->cd16 = nullptr;
-    c->have_gpat = c->have_delta = false;
+    c->have_gpat = false;
     c->d.gpat_id = nullptr;
     c->d.gpat_ptr = nullptr;
     c->d.gpat_off = nullptr;
-    c->d.cpat = nullptr;
-    c->d.cscale = nullptr;
-    c->d.cd16 = nullptr;
     c->generation++;
 }
 
@@ -671,104 +652,6 @@ static void gpat_apply(pd_ctx* c) {
     c->d.gpat_ptr = on ? c->gpat_ptr : nullptr;
     c->d.gpat_off = on ? c->gpat_off : nullptr;
     c->generation++;
-}
-
-// The delta form of the FP32 coefficients (2x2x2 points; see k_delta_build):
-// a node whose coefficients stray more than 2^-10 from its pattern
-// representative's gets a pattern of its own.  On success coeff32 holds
-// cpat + scale * delta for every coefficient.
-static int delta_build(pd_ctx* c, std::vector<int32_t>& pid, std::vector<int64_t>& ptr, std::vector<int32_t>& off,
-                       size_t max_entries) {
-    const int64_t N = c->n;
-    const int32_t P0 = (int32_t)(ptr.size() - 1);
-    std::vector<int32_t> rep((size_t)P0, -1);
-    for (int64_t i = 0; i < N; ++i)
-        if (rep[pid[i]] < 0) rep[pid[i]] = (int32_t)i;
-    int32_t *dpid = nullptr, *drep = nullptr;
-    int64_t* dptr = nullptr;
-    uint8_t* dfar = nullptr;
-    auto cleanup = [&]() { dfree(c, dpid); dfree(c, drep); dfree(c, dptr); dfree(c, dfar); };
-    int rc = PD_OK;
-    if ((rc = dalloc(c, &dpid, (size_t)N)) || (rc = dalloc(c, &drep, rep.size() + (size_t)N)) ||
-        (rc = dalloc(c, &dfar, (size_t)N)) || (rc = upload(c, dpid, pid.data(), sizeof(int32_t) * N)) ||
-        (rc = upload(c, drep, rep.data(), sizeof(int32_t) * rep.size()))) {
-        cleanup();
-        return rc;
-    }
-    pd::launch_delta_check(c->d, dpid, drep, dfar, c->stream);
-    std::vector<uint8_t> far((size_t)N);
-    if (cudaMemcpyAsync(far.data(), dfar, N, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
-        cudaStreamSynchronize(c->stream) != cudaSuccess) {
-        cleanup();
-        return fail(PD_ERR_CUDA, "delta form: check");
-    }
-    for (int64_t i = 0; i < N; ++i) {
-        if (!far[i]) continue;
-        const int64_t b = c->cbptr_host[i], e = c->cbptr_host[i + 1];
-        if (off.size() + (size_t)(e - b) > max_entries) {
-            cleanup();
-            return PD_ERR_CAPACITY;  // too irregular: no delta form
-        }
-        pid[i] = (int32_t)(ptr.size() - 1);
-        rep.push_back((int32_t)i);
-        for (int64_t k = b; k < e; ++k) off.push_back(c->cbidx_host[k] - (int32_t)i);
-        ptr.push_back((int64_t)off.size());
-    }
-    const size_t T = (size_t)c->cbptr_host[N];
-    if ((rc = upload(c, dpid, pid.data(), sizeof(int32_t) * N)) ||
-        (rc = upload(c, drep, rep.data(), sizeof(int32_t) * rep.size())) || (rc = dalloc(c, &dptr, ptr.size())) ||
-        (rc = upload(c, dptr, ptr.data(), sizeof(int64_t) * ptr.size())) ||
-        (rc = dalloc(c, &c->cpat, std::max<size_t>(off.size(), 1) * 8)) ||
-        (rc = dalloc(c, &c->cscale, (size_t)N * 8)) || (rc = dalloc(c, &c->cd16, std::max<size_t>(T, 1) * 8))) {
-        cleanup();
-        return rc;
-    }
-    pd::launch_delta_build(c->d, dpid, dptr, drep, c->cpat, c->cscale, c->cd16, c->coeff32, c->stream);
-    const cudaError_t e = cudaStreamSynchronize(c->stream);
-    cleanup();
-    if (e != cudaSuccess) return pd::fail_cuda(e, "delta form: build", __FILE__, __LINE__);
-    c->d.cpat = c->cpat;
-    c->d.cscale = c->cscale;
-    c->d.cd16 = c->cd16;
-    c->have_delta = true;
-    return PD_OK;
-}
-
-// the MLS data and what is derived from them, freed
-static void mls_release(pd_ctx* c) {
-    for (void* p : {(void*)c->tptr, (void*)c->tj, (void*)c->tpos, (void*)c->cbptr, (void*)c->cbidx, (void*)c->coeff,
-                    (void*)c->coeff32, (void*)c->csum})
-        dfree(c, p);
-    c->tptr = nullptr;
-    c->tj = c->tpos = nullptr;
-    c->cbptr = nullptr;
-    c->cbidx = nullptr;
-    c->coeff = nullptr;
-    c->coeff32 = c->csum = nullptr;
-    c->d.cbptr = nullptr;
-    c->d.cbidx = nullptr;
-    c->d.coeff = nullptr;
-    c->d.coeff32 = c->d.csum = nullptr;
-    c->have_mls = false;
-    c->generation++;
-}
-
-static int gpat_build(pd_ctx* c);
-
-// after new MLS data: the patterns, the delta form and the SELL copy
-static int mls_installed(pd_ctx* c) {
-    c->d.cbptr = c->cbptr;
-    c->d.cbidx = c->cbidx;
-    c->d.coeff = c->coeff;
-    c->d.coeff32 = c->coeff32;
-    c->d.csum = c->csum;
-    c->have_mls = true;
-    c->generation++;
-    PD_TRY(gpat_build(c));
-    if (!c->have_gpat) c->gpat_opt = 0;  // the new lists do not repeat: plain lists
-    if (!c->have_delta) c->d.gather_delta = 0;
-    gpat_apply(c);
-    return sell_prepare(c);
 }
 
 static int gpat_build(pd_ctx* c) {
@@ -807,19 +690,6 @@ static int gpat_build(pd_ctx* c) {
         }
         pid[i] = found;
     }
-    if (c->npt == 8) {
-        const int rc = delta_build(c, pid, ptr, off, kMaxEntries);
-        if (rc != PD_OK && rc != PD_ERR_CAPACITY) return rc;
-        if (rc == PD_ERR_CAPACITY) {  // no delta form: the plain FP32 coefficients stay
-            for (void* p : {(void*)c->cpat, (void*)c->cscale, (void*)c->cd16}) dfree(c, p);
-            c->cpat = nullptr;
-            c->cscale = nullptr;
-            c->cd16 = nullptr;
-            c->d.cpat = c->d.cscale = nullptr;
-            c->d.cd16 = nullptr;
-            c->have_delta = false;
-        }
-    }
     PD_TRY(dalloc(c, &c->gpat_id, (size_t)N));
     PD_TRY(dalloc(c, &c->gpat_ptr, ptr.size()));
     PD_TRY(dalloc(c, &c->gpat_off, std::max<size_t>(off.size(), 1)));
@@ -829,6 +699,39 @@ static int gpat_build(pd_ctx* c) {
     c->have_gpat = true;
     gpat_apply(c);
     return PD_OK;
+}
+
+static void mls_release(pd_ctx* c) {
+    for (void* p : {(void*)c->tptr, (void*)c->tj, (void*)c->tpos, (void*)c->cbptr, (void*)c->cbidx, (void*)c->coeff,
+                    (void*)c->coeff32, (void*)c->csum})
+        dfree(c, p);
+    c->tptr = nullptr;
+    c->tj = c->tpos = nullptr;
+    c->cbptr = nullptr;
+    c->cbidx = nullptr;
+    c->coeff = nullptr;
+    c->coeff32 = c->csum = nullptr;
+    c->d.cbptr = nullptr;
+    c->d.cbidx = nullptr;
+    c->d.coeff = nullptr;
+    c->d.coeff32 = c->d.csum = nullptr;
+    c->have_mls = false;
+    c->generation++;
+}
+
+// after new MLS data: the patterns and the SELL copy
+static int mls_installed(pd_ctx* c) {
+    c->d.cbptr = c->cbptr;
+    c->d.cbidx = c->cbidx;
+    c->d.coeff = c->coeff;
+    c->d.coeff32 = c->coeff32;
+    c->d.csum = c->csum;
+    c->have_mls = true;
+    c->generation++;
+    PD_TRY(gpat_build(c));
+    if (!c->have_gpat) c->gpat_opt = 0;  // the new lists do not repeat: plain lists
+    gpat_apply(c);
+    return sell_prepare(c);
 }
 
 // The lattice-stencil FP32 force: off (buffers freed, contiguous node blocks).
@@ -1326,15 +1229,6 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->static_precond = (int)value;
             break;
-        case PD_OPT_GATHER_DELTA:
-            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
-            if (value && !c->have_delta)
-                return fail(PD_ERR_ARG, "pd_set_option: no delta form of the coefficients (2x2x2 points, patterns)");
-            if ((int)value != c->d.gather_delta) {
-                c->d.gather_delta = (int)value;
-                c->generation++;
-            }
-            break;
         case PD_OPT_FORCE_STENCIL:
             if (value > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
             PD_TRY(fsten_prepare(c, (int)value));
@@ -1404,7 +1298,6 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_GATHER_SELL: *value = c->d.sell_on; return PD_OK;
         case PD_OPT_FORCE_STENCIL: *value = c->fst_shape; return PD_OK;
         case PD_OPT_GATHER_STENCIL: *value = c->gpat_opt; return PD_OK;
-        case PD_OPT_GATHER_DELTA: *value = c->d.gather_delta; return PD_OK;
         case PD_OPT_STATIC_PRECOND: *value = c->static_precond; return PD_OK;
         case PD_OPT_PERSIST_WAIT_US: *value = c->persist_wait_us; return PD_OK;
         case PD_OPT_PERSIST_TEST_STALL: *value = c->persist_stall; return PD_OK;
@@ -2484,26 +2377,9 @@ extern "C" int pd_autotune(pd_ctx* c, double dt, int steps, pd_tune_result* out)
                 }
             if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, ks)) != PD_OK) return done(rc);
             if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, kp)) != PD_OK) return done(rc);
-            if (c->have_delta) {
-                // the coefficient ring on the delta form, with both on
-                const int d0 = c->d.gather_delta;
-                const int s1 = c->d.sell_on, p1 = c->gpat_opt;
-                if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, 1)) != PD_OK) return done(rc);
-                if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, 1)) != PD_OK) return done(rc);
-                if ((rc = pd_set_option(c, PD_OPT_GATHER_DELTA, 1)) != PD_OK) return done(rc);
-                const double prev = best.ms;
-                Trial T3{best.tile, 0, c->persist_per_sm, c->force_chunk, c->gather_chunk, 0.0};
-                if ((rc = trial(T3)) != PD_OK) return done(rc);
-                if (!(best.ms < prev)) {
-                    if ((rc = pd_set_option(c, PD_OPT_GATHER_DELTA, d0)) != PD_OK) return done(rc);
-                    if ((rc = pd_set_option(c, PD_OPT_GATHER_SELL, s1)) != PD_OK) return done(rc);
-                    if ((rc = pd_set_option(c, PD_OPT_GATHER_STENCIL, p1)) != PD_OK) return done(rc);
-                }
-            }
         }
         out->gather_sell = c->d.sell_on;
         out->gather_stencil = c->gpat_opt;
-        out->gather_delta = c->d.gather_delta;
     }
     if (c->precision == PD_PREC_FP32C && !c->d.cci && c->npt == 8 && c->d.lat && !c->d.multimat) {
         // the lattice-stencil force in each block shape, on the best shape so far

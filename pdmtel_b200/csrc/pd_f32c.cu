@@ -558,15 +558,83 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 // the high lane, which are the two chains of bond4).  Per node the same
 // operations in the same order as bond4 on the lattice path: the same
 // result bit for bit as the pair, quad and tiled kernels.
+// One U2 entry of the pair (A, B): SIDES bit 0 = node A holds the bond,
+// bit 1 = node B holds it.  Compiled for both sides together (the lattice
+// interior, where the sides' independent chains interleave) and for each
+// side alone.
+template <bool HASFAIL, bool BDRY, bool SFAC, int SIDES>
+__device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, const f2* hx, const f2* hy, const f2* hz,
+                                           const float* epsc, float h, Own& A, Own& B) {
+    const int64_t N = d.n;
+    const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
+    const int4 E = __ldg(d.sten_u2 + u);  // id offset, ox, oy, oz from A
+    const int64_t j = ia + E.x;
+    const float4 us0 = __ldg(blk + 6 * N + j), us1 = __ldg(blk + 7 * N + j);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
+    float bej = 1.f, sfj = 1.f;
+    if (BDRY || SFAC) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(d.sblk + 8 * j + 6));
+        bej = v.x;
+        sfj = v.y;
+    }
+    const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
+    const float dx1 = __fmul_rn((float)E.z, h), dx2 = __fmul_rn((float)E.w, h);
+    f2 dx0s[2], du[2][3];
+    float coef[2];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        if (!((SIDES >> side) & 1)) continue;
+        const Own& O = side == 0 ? A : B;
+        const float dx0 = __fmul_rn((float)(E.y - side), h);
+        dx0s[side] = f2_make(dx0, dx0);
+        for (int a = 0; a < 3; ++a) {
+            const float v = split_diff(ujh[a], ujl[a], O.uh[a], O.ul[a]);
+            du[side][a] = f2_make(v, v);
+        }
+        float c = O.c;
+        if (BDRY) c *= 0.5f * (O.be + bej);
+        if (SFAC) c *= 0.5f * (O.sf + sfj);
+        coef[side] = c;
+    }
+    const f2 dx1s = f2_make(dx1, dx1), dx2s = f2_make(dx2, dx2);
+    const float4* __restrict__ tab = d.sten_tab;
+    const int nu = d.sten_nu;
+    f2 F[2][3] = {{0ull, 0ull, 0ull}, {0ull, 0ull, 0ull}};
+#pragma unroll
+    for (int q = 0; q < 8; q += 4) {
+        const float4 vx = __ldg(blk + (q >> 2) * N + j), vy = __ldg(blk + (2 + (q >> 2)) * N + j),
+                     vz = __ldg(blk + (4 + (q >> 2)) * N + j);
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            const int k = (q >> 1) + kk;  // point pair (2k, 2k + 1)
+            const f2 gx = kk ? f2_make(vx.z, vx.w) : f2_make(vx.x, vx.y);
+            const f2 gy = kk ? f2_make(vy.z, vy.w) : f2_make(vy.x, vy.y);
+            const f2 gz = kk ? f2_make(vz.z, vz.w) : f2_make(vz.x, vz.y);
+            const f2 x1 = f2_add(dx1s, hy[k]), x2 = f2_add(dx2s, hz[k]);
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                if (!((SIDES >> side) & 1)) continue;
+                const float4 T = __ldg(tab + (side * nu + u) * 4 + k);  // K lo hi, 1/r^2 lo hi
+                const f2 x0 = f2_add(dx0s[side], hx[k]);
+                pt_force2<HASFAIL>(x0, x1, x2, f2_make(T.x, T.y), f2_make(T.z, T.w), f2_add(du[side][0], gx),
+                                   f2_add(du[side][1], gy), f2_add(du[side][2], gz), epsc[side], F[side]);
+            }
+        }
+    }
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        if (!((SIDES >> side) & 1)) continue;
+        float F6[6];
+        f2_split(F[side][0], F6[0], F6[3]);
+        f2_split(F[side][1], F6[1], F6[4]);
+        f2_split(F[side][2], F6[2], F6[5]);
+        float Fb[3];
+        chains_sum(F6, Fb);
+        kahan_add(side == 0 ? A : B, Fb, coef[side]);
+    }
+}
+
 template <bool HASFAIL, bool BDRY, bool SFAC>
 __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
-    extern __shared__ float4 sm4[];
-    const int nu = d.sten_nu;
-    float4* tab = sm4;                                   // [2][nu][4]
-    int4* u2s = reinterpret_cast<int4*>(sm4 + 8 * nu);  // [nu]
-    for (int k = threadIdx.x; k < 8 * nu; k += blockDim.x) tab[k] = __ldg(d.sten_tab + k);
-    for (int k = threadIdx.x; k < nu; k += blockDim.x) u2s[k] = __ldg(d.sten_u2 + k);
-    __syncthreads();
     const int NX = d.lat_nx, NY = d.lat_ny, NZ = d.lat_nz;
     const int npx = (NX + 1) >> 1, BY = d.sten_by, BZ = d.sten_bz;
     const int nbx = (npx + 15) >> 4, nby = (NY + BY - 1) / BY;
@@ -577,7 +645,7 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
     const int z = (b / (nbx * nby)) * BZ + ty / BY;
     // threads past the box stay in the warp's walk with empty masks
     const bool valid = px < npx && y < NY && z < NZ;
-    const int64_t N = d.n, NP = d.sten_np;
+    const int64_t NP = d.sten_np;
     const int64_t yz = valid ? y + (int64_t)NY * z : 0;
     const int64_t p = valid ? px + (int64_t)npx * yz : 0;
     const int64_t ia = valid ? 2 * px + (int64_t)NX * yz : 0;
@@ -586,7 +654,6 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
     load_own<true, BDRY, SFAC, false>(d, ia, A);
     load_own<true, BDRY, SFAC, false>(d, hb ? ia + 1 : ia, B);
     const float epsc[2] = {HASFAIL ? eps_crit(A.e) : 0.f, HASFAIL ? eps_crit(B.e) : 0.f};
-    const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
     const float h = (float)d.dx;
     f2 hx[4], hy[4], hz[4];
 #pragma unroll
@@ -606,71 +673,11 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
         while (m) {
             const int bit = __ffs(m) - 1;
             m &= m - 1;
-            const bool has[2] = {((ma >> bit) & 1u) != 0, ((mb >> bit) & 1u) != 0};
-            if (!(has[0] || has[1])) continue;
+            const bool ha = ((ma >> bit) & 1u) != 0, hbit = ((mb >> bit) & 1u) != 0;
             const int u = 32 * w + bit;
-            const int4 E = u2s[u];  // id offset, ox, oy, oz from A
-            const int64_t j = ia + E.x;
-            const float4 us0 = __ldg(blk + 6 * N + j), us1 = __ldg(blk + 7 * N + j);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
-            float bej = 1.f, sfj = 1.f;
-            if (BDRY || SFAC) {
-                const float2 v = __ldg(reinterpret_cast<const float2*>(d.sblk + 8 * j + 6));
-                bej = v.x;
-                sfj = v.y;
-            }
-            const float ujh[3] = {us0.x, us0.y, us0.z}, ujl[3] = {us0.w, us1.x, us1.y};
-            const float dx1 = __fmul_rn((float)E.z, h), dx2 = __fmul_rn((float)E.w, h);
-            f2 dx0s[2], du[2][3];
-            float coef[2];
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const Own& O = side == 0 ? A : B;
-                const float dx0 = __fmul_rn((float)(E.y - side), h);
-                dx0s[side] = f2_make(dx0, dx0);
-                for (int a = 0; a < 3; ++a) {
-                    const float v = split_diff(ujh[a], ujl[a], O.uh[a], O.ul[a]);
-                    du[side][a] = f2_make(v, v);
-                }
-                float c = O.c;
-                if (BDRY) c *= 0.5f * (O.be + bej);
-                if (SFAC) c *= 0.5f * (O.sf + sfj);
-                coef[side] = c;
-            }
-            const f2 dx1s = f2_make(dx1, dx1), dx2s = f2_make(dx2, dx2);
-            f2 F[2][3] = {{0ull, 0ull, 0ull}, {0ull, 0ull, 0ull}};
-#pragma unroll
-            for (int q = 0; q < 8; q += 4) {
-                const float4 vx = __ldg(blk + (q >> 2) * N + j), vy = __ldg(blk + (2 + (q >> 2)) * N + j),
-                             vz = __ldg(blk + (4 + (q >> 2)) * N + j);
-#pragma unroll
-                for (int kk = 0; kk < 2; ++kk) {
-                    const int k = (q >> 1) + kk;  // point pair (2k, 2k + 1)
-                    const f2 gx = kk ? f2_make(vx.z, vx.w) : f2_make(vx.x, vx.y);
-                    const f2 gy = kk ? f2_make(vy.z, vy.w) : f2_make(vy.x, vy.y);
-                    const f2 gz = kk ? f2_make(vz.z, vz.w) : f2_make(vz.x, vz.y);
-                    const f2 x1 = f2_add(dx1s, hy[k]), x2 = f2_add(dx2s, hz[k]);
-#pragma unroll
-                    for (int side = 0; side < 2; ++side)
-                        if (has[side]) {
-                            const float4 T = tab[(side * nu + u) * 4 + k];  // K lo hi, 1/r^2 lo hi
-                            const f2 x0 = f2_add(dx0s[side], hx[k]);
-                            pt_force2<HASFAIL>(x0, x1, x2, f2_make(T.x, T.y), f2_make(T.z, T.w),
-                                               f2_add(du[side][0], gx), f2_add(du[side][1], gy),
-                                               f2_add(du[side][2], gz), epsc[side], F[side]);
-                        }
-                }
-            }
-#pragma unroll
-            for (int side = 0; side < 2; ++side)
-                if (has[side]) {
-                    float F6[6];
-                    f2_split(F[side][0], F6[0], F6[3]);
-                    f2_split(F[side][1], F6[1], F6[4]);
-                    f2_split(F[side][2], F6[2], F6[5]);
-                    float Fb[3];
-                    chains_sum(F6, Fb);
-                    kahan_add(side == 0 ? A : B, Fb, coef[side]);
-                }
+            if (ha && hbit) sten_entry<HASFAIL, BDRY, SFAC, 3>(d, u, ia, hx, hy, hz, epsc, h, A, B);
+            else if (ha) sten_entry<HASFAIL, BDRY, SFAC, 1>(d, u, ia, hx, hy, hz, epsc, h, A, B);
+            else if (hbit) sten_entry<HASFAIL, BDRY, SFAC, 2>(d, u, ia, hx, hy, hz, epsc, h, A, B);
         }
     }
     if (valid) store_own<false>(d, ia, A, nba, dts, d.vbuf);
@@ -1241,112 +1248,6 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
     }
 }
 
-// 8-byte copy global -> shared (the delta ring's slot of four int16)
-__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gsrc) : "memory");
-}
-
-constexpr int kRingD = 20;  // delta slots a thread keeps in flight (8 bytes each)
-
-// k_gather_f32c_ring on the delta form of the coefficients: the stream of
-// int16 deltas (8 bytes per contributor slot and thread) runs through the
-// shared-memory ring, the pattern coefficients and the thread's four scales
-// come through L1, and every coefficient is rebuilt as fma(scale, delta,
-// c_pattern), the value coeff32 holds, before the same FMAs in the same
-// order as gather_group: the same result bit for bit.
-__global__ void __launch_bounds__(256, 2) k_gather_f32c_dring(Dev d, const double* __restrict__ us) {
-    __shared__ uint2 ring[8][kRingD][32];
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (tid >= d.n * 2) return;
-    const int64_t N = d.n;
-    const int64_t slot = tid >> 1;
-    const int grp = (int)(tid & 1), g0 = 4 * grp;
-    const int64_t i = d.order[slot];
-    const BlkOut o = blk_out(d, i);
-    double u0, u1, u2;
-    if (gather_head<false>(d, us, i, grp, *d.tdev, o, u0, u1, u2)) return;
-    const int pid = __ldg(d.gpat_id + i);
-    const int64_t p0 = __ldg(d.gpat_ptr + pid);
-    const int nc = (int)(__ldg(d.gpat_ptr + pid + 1) - p0);
-    const int32_t* po = d.gpat_off + p0;
-    const float* cpt = d.cpat + p0 * 8 + g0;  // contributor k: cpt[8 k .. 8 k + 3]
-    const float4 sc4 = ld4(d.cscale + i * 8 + g0);
-    const float sc[4] = {sc4.x, sc4.y, sc4.z, sc4.w};
-    const int64_t sl = slot / kSell, ln = slot % kSell, base = d.sell_off[sl];
-    // contributor slot k of this thread: cf[32 k] (a slot is kSell nodes x 8 int16 = 32 x 8 bytes)
-    const uint2* cf = reinterpret_cast<const uint2*>(d.sell_d16 + (base * kSell + ln) * 8 + g0);
-    uint2* r = &ring[threadIdx.x >> 5][0][threadIdx.x & 31];  // ring entry e at r[32 e]
-#pragma unroll
-    for (int k = 0; k < kRingD; ++k) {
-        if (k < nc) cp_async8(r + 32 * k, cf + (int64_t)32 * k);
-        cp_async_commit();
-    }
-    double un[4][3];
-    auto load_group = [&](int k) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int m = (int)i + (k + u < nc ? __ldg(po + k + u) : 0);
-            un[u][0] = __ldg(us + m);
-            un[u][1] = __ldg(us + N + m);
-            un[u][2] = __ldg(us + 2 * N + m);
-        }
-    };
-    load_group(0);
-    double a[4][3] = {};
-    int e = 0;
-    for (int k = 0; k < nc; k += 4) {
-        double dd[4][3];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            dd[u][0] = un[u][0] - u0;
-            dd[u][1] = un[u][1] - u1;
-            dd[u][2] = un[u][2] - u2;
-        }
-        if (k + 4 < nc) load_group(k + 4);
-        float4 cv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            cv[u] = k + u < nc ? ld4(cpt + 8 * (k + u)) : make_float4(0.f, 0.f, 0.f, 0.f);
-        cp_async_wait<kRingD - 4>();  // slots k .. k+3 have landed
-        uint2 dv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int eu = e + u < kRingD ? e + u : e + u - kRingD;
-            dv[u] = k + u < nc ? r[32 * eu] : make_uint2(0u, 0u);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (k + u >= nc) break;
-            const float dq[4] = {(float)(short)(dv[u].x & 0xffffu), (float)((int)dv[u].x >> 16),
-                                 (float)(short)(dv[u].y & 0xffffu), (float)((int)dv[u].y >> 16)};
-            const float cpv[4] = {cv[u].x, cv[u].y, cv[u].z, cv[u].w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float c = ffma(sc[q], dq[q], cpv[q]);
-                a[q][0] = fma((double)c, dd[u][0], a[q][0]);
-                a[q][1] = fma((double)c, dd[u][1], a[q][1]);
-                a[q][2] = fma((double)c, dd[u][2], a[q][2]);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int eu = e + u < kRingD ? e + u : e + u - kRingD;
-            const int kk = k + kRingD + u;
-            if (kk < nc) cp_async8(r + 32 * eu, cf + (int64_t)32 * kk);
-            cp_async_commit();
-        }
-        e = e + 4 < kRingD ? e + 4 : e + 4 - kRingD;
-    }
-    cp_async_wait<0>();
-    for (int q = 0; q < 4; ++q) {
-        const double S = (double)d.csum[i * 8 + g0 + q];
-        o[g0 + q] = (float)fma(S, u0, a[q][0]);
-        o[8 + g0 + q] = (float)fma(S, u1, a[q][1]);
-        o[16 + g0 + q] = (float)fma(S, u2, a[q][2]);
-    }
-}
-
 // SELL layout: the widest contributor list of every slice, then the copy
 __global__ void k_sell_width(Dev d, int64_t* __restrict__ width, int64_t S) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1362,7 +1263,7 @@ __global__ void k_sell_width(Dev d, int64_t* __restrict__ width, int64_t S) {
 }
 
 __global__ void k_sell_fill(Dev d, const int64_t* __restrict__ off, int32_t* __restrict__ sidx,
-                            float* __restrict__ scoef, int16_t* __restrict__ sd16) {
+                            float* __restrict__ scoef) {
     const int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (slot >= d.n) return;
     const int64_t i = d.order[slot], sl = slot / kSell, l = slot % kSell, base = off[sl];
@@ -1372,77 +1273,6 @@ __global__ void k_sell_fill(Dev d, const int64_t* __restrict__ off, int32_t* __r
         const float* src = d.coeff32 + (c0 + k) * 8;
         float* dst = scoef + ((base + k) * kSell + l) * 8;
         for (int g = 0; g < 8; ++g) dst[g] = src[g];
-        if (sd16) {
-            const int16_t* s16 = d.cd16 + (c0 + k) * 8;
-            int16_t* d16 = sd16 + ((base + k) * kSell + l) * 8;
-            for (int g = 0; g < 8; ++g) d16[g] = s16[g];
-        }
-    }
-}
-
-// ---- delta form of the FP32 MLS coefficients (2x2x2 points) ----
-//
-// On a lattice, nodes whose contributor lists are translates of each other
-// (one pattern) have the same coefficients up to the round-off the
-// ill-conditioned moment matrix of InitIntegrationPoint (pdDataManager2.cpp:
-// 173-256, global coordinates) adds: 1e-10..1e-5 of the largest coefficient,
-// growing with the distance from the origin.  The FP32 form stores each
-// coefficient as the pattern representative's FP32 coefficient plus an
-// int16 multiple of a per-(node, point) scale, max |c - c_rep| / 32767, so
-// the quantisation error (below 2^-16 of the largest delta) is far below the
-// FP32 rounding of the result, fma(scale, delta, c_rep): the FP32
-// coefficient of every FP32 gather.  The gather from deltas streams 2 bytes
-// per coefficient instead of 4 and reads the pattern table from L1/L2.
-
-// nodes whose coefficients stray more than 2^-10 of their largest from their
-// representative's (the pattern then does not describe the geometry)
-__global__ void k_delta_check(Dev d, const int32_t* __restrict__ pid, const int32_t* __restrict__ rep,
-                              uint8_t* __restrict__ far) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
-    const int64_t r = rep[pid[i]];
-    const int64_t a = d.cbptr[i], b = d.cbptr[r], nc = d.cbptr[i + 1] - a;
-    double dev = 0.0, cm = 0.0;
-    for (int64_t k = 0; k < 8 * nc; ++k) {
-        const double ci = d.coeff[a * 8 + k], cr = d.coeff[b * 8 + k];
-        dev = fmax(dev, fabs(ci - cr));
-        cm = fmax(cm, fabs(ci));
-    }
-    far[i] = dev > 0x1p-10 * cm ? 1 : 0;
-}
-
-// the pattern table: the representative's coefficients in FP32
-__global__ void k_delta_pat(Dev d, const int32_t* __restrict__ pid, const int64_t* __restrict__ ptr,
-                            const int32_t* __restrict__ rep, float* __restrict__ cpat) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= d.n || rep[pid[i]] != i) return;
-    const int64_t a = d.cbptr[i], nc = d.cbptr[i + 1] - a;
-    float* dst = cpat + ptr[pid[i]] * 8;
-    for (int64_t k = 0; k < 8 * nc; ++k) dst[k] = (float)d.coeff[a * 8 + k];
-}
-
-// one thread per (node, point): scale, deltas, and the FP32 coefficients
-__global__ void k_delta_build(Dev d, const int32_t* __restrict__ pid, const int64_t* __restrict__ ptr,
-                              const float* __restrict__ cpat, float* __restrict__ cscale, int16_t* __restrict__ cd16,
-                              float* __restrict__ coeff32) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= d.n * 8) return;
-    const int64_t i = t >> 3;
-    const int g = (int)(t & 7);
-    const int64_t a = d.cbptr[i], nc = d.cbptr[i + 1] - a;
-    const float* cp = cpat + ptr[pid[i]] * 8 + g;
-    double m = 0.0;
-    for (int64_t k = 0; k < nc; ++k) m = fmax(m, fabs(d.coeff[(a + k) * 8 + g] - (double)cp[8 * k]));
-    const float sf = (float)(m / 32767.0);
-    cscale[t] = sf;
-    for (int64_t k = 0; k < nc; ++k) {
-        int q = 0;
-        if (sf > 0.f) {
-            const double v = rint((d.coeff[(a + k) * 8 + g] - (double)cp[8 * k]) / (double)sf);
-            q = (int)fmax(-32767.0, fmin(32767.0, v));
-        }
-        cd16[(a + k) * 8 + g] = (int16_t)q;
-        coeff32[(a + k) * 8 + g] = ffma(sf, (float)q, cp[8 * k]);
     }
 }
 
@@ -1636,9 +1466,6 @@ PointPack<NPT> pack_points(const Dev& d, const GaussConst* host_gc) {
 
 }  // namespace
 
-// shared memory of the stencil force: the table and the U2 entries
-static size_t sten_smem_bytes(int nu) { return (size_t)nu * (8 * sizeof(float4) + sizeof(int4)); }
-
 size_t tiled_smem_bytes(const Dev& d) {
     const int R = d.fam_radius;
     const int64_t lx = std::min(d.lat_nx, d.tile_x + 2 * R), ly = std::min(d.lat_ny, d.tile_y + 2 * R),
@@ -1679,8 +1506,7 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
                                         ((d.lat_nz + d.sten_bz - 1) / d.sten_bz));
         const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
         const PointPack<8> P = pack_points<8>(d, d.gc_host);
-        const size_t sh = sten_smem_bytes(d.sten_nu);
-#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, sh, s>>>(d, P, dts)
+#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, P, dts)
         if (d.hasfail) {
             if (bd) { if (sf) PD_STEN(true, true, true); else PD_STEN(true, true, false); }
             else { if (sf) PD_STEN(true, false, true); else PD_STEN(true, false, false); }
@@ -1799,8 +1625,7 @@ void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
     const unsigned nb = blocks_for(d.n * ngrp, 256);
     const bool sell = d.sell_on && d.sell_idx && d.mls && d.npt == 8, pat = d.gpat_id && d.mls;
     if (sell && pat && d.npt == 8) {
-        if (d.gather_delta && d.sell_d16 && d.cpat && d.cscale) k_gather_f32c_dring<<<nb, 256, 0, s>>>(d, us);
-        else k_gather_f32c_ring<<<nb, 256, 0, s>>>(d, us);
+        k_gather_f32c_ring<<<nb, 256, 0, s>>>(d, us);
     } else if (sell) {
         if (pat) k_gather_f32c<true, true><<<nb, 256, 0, s>>>(d, us);
         else k_gather_f32c<true, false><<<nb, 256, 0, s>>>(d, us);
@@ -1825,15 +1650,6 @@ int launch_sten_table(const Dev& d, float4* tab, cudaStream_t s) {
     if (d.sten_nu <= 0 || !d.gc_host) return PD_ERR_ARG;
     const PointPack<8> P = pack_points<8>(d, d.gc_host);
     k_sten_table<<<blocks_for(8 * d.sten_nu, 128), 128, 0, s>>>(d.sten_u2, d.sten_nu, P, (float)d.dx, tab);
-    const int smem = (int)sten_smem_bytes(d.sten_nu);
-    const void* fns[8] = {
-        (const void*)k_force_f32c_sten<false, false, false>, (const void*)k_force_f32c_sten<false, false, true>,
-        (const void*)k_force_f32c_sten<false, true, false>,  (const void*)k_force_f32c_sten<false, true, true>,
-        (const void*)k_force_f32c_sten<true, false, false>,  (const void*)k_force_f32c_sten<true, false, true>,
-        (const void*)k_force_f32c_sten<true, true, false>,   (const void*)k_force_f32c_sten<true, true, true>};
-    for (const void* f : fns)
-        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-            return PD_ERR_CUDA;
     return cudaGetLastError() == cudaSuccess ? PD_OK : PD_ERR_CUDA;
 }
 
@@ -1843,19 +1659,8 @@ void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s) {
     if (S) k_sell_width<<<blocks_for(S, 256), 256, 0, s>>>(d, width, S);
 }
 
-void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, int16_t* sd16, cudaStream_t s) {
-    if (d.n) k_sell_fill<<<blocks_for(d.n, 128), 128, 0, s>>>(d, off, sidx, scoef, sd16);
-}
-
-void launch_delta_check(const Dev& d, const int32_t* pid, const int32_t* rep, uint8_t* far, cudaStream_t s) {
-    if (d.n) k_delta_check<<<blocks_for(d.n, 128), 128, 0, s>>>(d, pid, rep, far);
-}
-
-void launch_delta_build(const Dev& d, const int32_t* pid, const int64_t* ptr, const int32_t* rep, float* cpat,
-                        float* cscale, int16_t* cd16, float* coeff32, cudaStream_t s) {
-    if (!d.n) return;
-    k_delta_pat<<<blocks_for(d.n, 128), 128, 0, s>>>(d, pid, ptr, rep, cpat);
-    k_delta_build<<<blocks_for(d.n * 8, 128), 128, 0, s>>>(d, pid, ptr, cpat, cscale, cd16, coeff32);
+void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s) {
+    if (d.n) k_sell_fill<<<blocks_for(d.n, 128), 128, 0, s>>>(d, off, sidx, scoef);
 }
 
 void launch_pack_cci_f32c(const Dev& d, cudaStream_t s) {

@@ -130,14 +130,6 @@ struct Dev {
     int blk_cm;
     int sten_nu, sten_nw, sten_by, sten_bz;
     int64_t sten_np;
-    // FP32 MLS coefficients as a pattern coefficient plus an int16 delta:
-    // c32 = fma(cscale[i][g], (float)delta, cpat[(gpat_ptr[pid] + k) * 8 + g])
-    // (2x2x2 points; coeff32 holds the same c32 values for the other gathers)
-    const float* cpat;            // per pattern entry and point: the representative's coefficient
-    const float* cscale;          // [N][8] delta scale of every node and point
-    const int16_t* sell_d16;      // SELL copy of the deltas [slots][16][8]
-    const int16_t* cd16;          // the deltas in the CSR layout [T][8] (setup of the SELL copy)
-    int gather_delta;             // FP32 gather from the deltas (PD_OPT_GATHER_DELTA)
     const int4* sten_u2;
     const float4* sten_tab;       // [2][sten_nu][4] geometry of the stencil force (k_sten_table)
     const uint32_t* sten_mask;    // FP32 gather from contributor patterns: node i's contributors are
@@ -191,7 +183,7 @@ void launch_pack_cci_f32c(const Dev& d, cudaStream_t s);
 size_t tiled_smem_bytes(const Dev& d);
 int64_t sell_slices(const Dev& d);
 void launch_sell_width(const Dev& d, int64_t* width, cudaStream_t s);
-void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, int16_t* sd16, cudaStream_t s);
+void launch_sell_fill(const Dev& d, const int64_t* off, int32_t* sidx, float* scoef, cudaStream_t s);
 int prepare_tiled_force(size_t smem);
 void launch_family_radius(const Dev& d, int* out, cudaStream_t s);
 // lattice-stencil force setup: offsets present in the families (bitmap over
@@ -202,16 +194,6 @@ void launch_sten_masks(const Dev& d, const int* lut, int R, uint32_t* mask, int*
 // geometry table of the stencil force (d.sten_u2, d.sten_nu, the Gauss
 // constants) into tab [2][nu][4]; sets the kernel's shared-memory limit
 int launch_sten_table(const Dev& d, float4* tab, cudaStream_t s);
-// Delta form of the FP32 coefficients (2x2x2 points): per node whether its
-// coefficients stay within 2^-10 of the largest one of its pattern's
-// representative (rep[pid]), the pattern table cpat, then for every node the
-// scales, the int16 deltas cd16 ([T][8], CSR) and coeff32 rebuilt as
-// cpat + scale * delta.  pid/ptr/rep: pattern of each node, first entry of
-// each pattern, representative node of each pattern.
-void launch_delta_check(const Dev& d, const int32_t* pid, const int32_t* rep, uint8_t* far, cudaStream_t s);
-void launch_delta_build(const Dev& d, const int32_t* pid, const int64_t* ptr, const int32_t* rep, float* cpat,
-                        float* cscale, int16_t* cd16, float* coeff32, cudaStream_t s);
-
 // persistent FP32C stepping (pd_f32c.cu): control block of one launch.
 // next[8*step + 2*(stage-1) + phase] are the work-queue counters; all of it
 // is zeroed before every launch.

@@ -81,8 +81,8 @@ def test_shape_option_sets_the_named_launch_shapes():
             self.calls.append((opt, v))
 
     c = Ctx()
-    out = bench.apply_shape(c, {"tile": 261, "gather_sell": 1, "gather_stencil": 1, "gather_delta": 1,
+    out = bench.apply_shape(c, {"tile": 261, "gather_sell": 1, "gather_stencil": 1,
                                 "force_stencil": 3, "trials": 27})
     assert sorted(c.calls) == sorted([(P.OPT_TILE, 261), (P.OPT_GATHER_SELL, 1), (P.OPT_GATHER_STENCIL, 1),
-                                      (P.OPT_GATHER_DELTA, 1), (P.OPT_FORCE_STENCIL, 3)])
+                                      (P.OPT_FORCE_STENCIL, 3)])
     assert out["applied"] and out["tile"] == 261

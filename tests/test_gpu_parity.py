@@ -480,37 +480,30 @@ def test_fp32c_stencil_force_rejects_and_resets(tmp_path):
 def test_fp32c_pattern_gather_equals_list_gather(name):
     """The FP32 gather taking contributors from shared id-offset patterns:
     the same contributors in the same order as the lists, so the same
-    trajectory bit for bit, with and without the SELL copy, with the delta
-    form of the coefficients, and after the MLS data are set again (the
-    patterns and the delta form are rebuilt)."""
+    trajectory bit for bit, with and without the SELL copy, and after the
+    MLS data are set again (the patterns are rebuilt)."""
     g = load_golden(name)
     dt = g["dt"][0]
 
-    def run(pat, sell, reset_mls=False, delta=0):
+    def run(pat, sell, reset_mls=False):
         dm = gpu_model(name)
         dm.SetPrecision(P.PREC_FP32C)
         ctx = dm.context()
         ctx.set_option(P.OPT_GATHER_SELL, sell)
         ctx.set_option(P.OPT_GATHER_STENCIL, pat)
-        ctx.set_option(P.OPT_GATHER_DELTA, delta)
         assert ctx.get_option(P.OPT_GATHER_STENCIL) == pat
         if reset_mls:
             ctx.set_mls(*dm.mls())
             assert ctx.get_option(P.OPT_GATHER_STENCIL) == pat
-            assert ctx.get_option(P.OPT_GATHER_DELTA) == delta
         ctx.rk4_steps(dt, 0.0, 20)
         ctx.sync()
         return ctx.get_state()
 
     U0, V0 = run(0, 0)
     assert np.abs(U0).max() > 0
-    # the ring on the delta form of the coefficients (2-byte deltas from the
-    # pattern coefficients) rebuilds the FP32 coefficients every other
-    # gather reads: the same trajectory too
-    for pat, sell, reset, delta in ((1, 0, False, 0), (1, 1, False, 0), (1, 1, True, 0), (1, 1, False, 1),
-                                    (1, 1, True, 1)):
-        U1, V1 = run(pat, sell, reset, delta)
-        assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (pat, sell, reset, delta)
+    for pat, sell, reset in ((1, 0, False), (1, 1, False), (1, 1, True)):
+        U1, V1 = run(pat, sell, reset)
+        assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (pat, sell, reset)
 
 
 def test_autotune_on_a_box_lattice_changes_no_result(tmp_path):
