@@ -345,7 +345,15 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   entries; 0 (default) reads the lists.
  * PD_OPT_STATIC_PRECOND: 1 (default) preconditions the static CG with the
  *   inverses of the operator's 3x3 diagonal blocks (block Jacobi); 0 runs
- *   plain CG.  Changes the iterates, not the solution beyond the tolerance. */
+ *   plain CG.  Changes the iterates, not the solution beyond the tolerance.
+ * PD_OPT_STATIC_SPLIT: the FP64 lattice-stencil operator in the split form
+ *   K x = D_i x_i - sum_o W_o x_(i+o) (three FMAs per bond instead of ten;
+ *   the same operator to FP64 rounding) with 4 (default) or 8 nodes per
+ *   thread along z; 0 runs the difference form.  No effect on the FP32
+ *   operator, on spring factors (pd_set_spring_factor) or off the stencil.
+ * PD_OPT_STATIC_F32_BELOW: v; the FP32C static solve iterates with the FP64
+ *   operator until the relative residual is below 1/v, then with the FP32
+ *   one (default 10: below 0.1); 0 uses the FP32 operator from the start. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -361,7 +369,9 @@ enum {
     PD_OPT_GATHER_SELL = 12,
     PD_OPT_FORCE_STENCIL = 13,
     PD_OPT_GATHER_STENCIL = 14,
-    PD_OPT_STATIC_PRECOND = 15
+    PD_OPT_STATIC_PRECOND = 15,
+    PD_OPT_STATIC_SPLIT = 16,
+    PD_OPT_STATIC_F32_BELOW = 17
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);

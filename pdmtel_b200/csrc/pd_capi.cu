@@ -92,6 +92,11 @@ struct pd_ctx {
     double* sten_xm = nullptr;
     int4* sten_col = nullptr;
     double4* sten_colgeo = nullptr;
+    int static_split = 4;           // split-form nodes per thread (PD_OPT_STATIC_SPLIT; 0: difference form)
+    int64_t static_f32_below = 10;  // FP32 matvecs below relative residual 1/value (PD_OPT_STATIC_F32_BELOW)
+    int4* nd_col = nullptr;
+    double2* nd_tap = nullptr;
+    double* nd_diag = nullptr;
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
@@ -1202,6 +1207,15 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->static_stencil_opt = (int)value;
             break;
+        case PD_OPT_STATIC_F32_BELOW:
+            if (value > 1000000000) return fail(PD_ERR_ARG, "pd_set_option: 0..1e9");
+            c->static_f32_below = value;
+            return PD_OK;
+        case PD_OPT_STATIC_SPLIT:
+            if (value != 0 && value != 4 && value != 8) return fail(PD_ERR_ARG, "pd_set_option: 0, 4 or 8");
+            c->static_split = (int)value;
+            c->sten.ndr = c->sten.ndcol > 0 ? (int)value : 0;
+            return PD_OK;
         case PD_OPT_GATHER_PER_POINT:
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->d.gather_per_point = (int)value;
@@ -1225,10 +1239,10 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             c->gpat_opt = (int)value;
             gpat_apply(c);
             break;
-        case PD_OPT_STATIC_PRECOND:
+        case PD_OPT_STATIC_PRECOND:  // the static options leave the prepared stencil valid
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->static_precond = (int)value;
-            break;
+            return PD_OK;
         case PD_OPT_FORCE_STENCIL:
             if (value > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
             PD_TRY(fsten_prepare(c, (int)value));
@@ -1290,6 +1304,8 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_PERSIST_FORCE_CHUNK: *value = c->force_chunk; return PD_OK;
         case PD_OPT_PERSIST_GATHER_CHUNK: *value = c->gather_chunk; return PD_OK;
         case PD_OPT_STATIC_STENCIL: *value = c->static_stencil_opt; return PD_OK;
+        case PD_OPT_STATIC_SPLIT: *value = c->static_split; return PD_OK;
+        case PD_OPT_STATIC_F32_BELOW: *value = c->static_f32_below; return PD_OK;
         case PD_OPT_GATHER_PER_POINT: *value = c->d.gather_per_point; return PD_OK;
         case PD_OPT_FORCE_TILE:
             *value = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
@@ -1594,6 +1610,72 @@ namespace {
 // every lattice position of a box holds one node, node id = x + nx (y + ny z),
 // one material, no broken family entry, and every node's family is the union
 // stencil clipped to the box (checked node by node on the downloaded family).
+// The split form's tables (k_static_nd): the columns of the z-blocked
+// difference form sorted by half-height, (w, w oz spacing) per oz, and the
+// per-node diagonal blocks D_i built on the device from the same tables;
+// the interior block is read back from a node at least the stencil reach
+// inside the box.  Left off (ndcol = 0) when the tables would not fit the
+// 48 KB of shared memory a block gets by default.
+int split_prepare(pd_ctx* c, const std::vector<int4>& cols, const std::vector<double4>& colgeo) {
+    pd::StencilDev& S = c->sten;
+    S.ndcol = S.ndr = 0;
+    const int nc = (int)cols.size(), rz = S.rz;
+    if (nc == 0 || rz < 1 || rz > 4 || (size_t)nc * (9 * sizeof(double2) + sizeof(int4)) > 48 * 1024) return PD_OK;
+    const int W = 2 * rz + 1;
+    std::vector<int> h(nc, 0), order(nc);
+    for (int k = 0; k < nc; ++k) {
+        for (int q = 0; q < W; ++q)
+            if (colgeo[(size_t)k * W + q].w != 0.0) h[k] = std::max(h[k], std::abs(q - rz));
+        order[k] = k;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h[a] < h[b]; });
+    std::vector<int4> nd(nc);
+    std::vector<double2> tap((size_t)nc * 9, make_double2(0.0, 0.0));
+    int rx = 0, ry = 0;
+    for (int hh = 0; hh <= 5; ++hh) S.ndcls[hh] = nc;
+    for (int k = nc - 1; k >= 0; --k) S.ndcls[h[order[k]]] = k;
+    for (int hh = 4; hh >= 0; --hh) S.ndcls[hh] = std::min(S.ndcls[hh], S.ndcls[hh + 1]);
+    for (int k = 0; k < nc; ++k) {
+        const int o = order[k];
+        nd[k] = make_int4(cols[o].x, cols[o].y, cols[o].z, h[o]);
+        rx = std::max(rx, std::abs(cols[o].x));
+        ry = std::max(ry, std::abs(cols[o].y));
+        for (int q = 0; q < W; ++q) {
+            const double4 g = colgeo[(size_t)o * W + q];
+            tap[(size_t)k * 9 + 4 + (q - rz)] = make_double2(g.w, g.w * g.z);
+        }
+    }
+    if (!c->nd_col) {
+        PD_TRY(dalloc(c, &c->nd_col, pd::kMaxStencil));
+        PD_TRY(dalloc(c, &c->nd_tap, (size_t)pd::kMaxStencil * 9));
+    }
+    if (!c->nd_diag) PD_TRY(dalloc(c, &c->nd_diag, (size_t)6 * c->n));
+    PD_TRY(upload(c, c->nd_col, nd.data(), sizeof(int4) * nc));
+    PD_TRY(upload(c, c->nd_tap, tap.data(), sizeof(double2) * tap.size()));
+    S.ndcol = nc;
+    S.nrx = rx;
+    S.nry = ry;
+    S.sp = c->d.dx;
+    S.ndc = c->nd_col;
+    S.ndtap = c->nd_tap;
+    S.ndiag = c->nd_diag;
+    pd::launch_static_ndiag(S, c->n, c->nd_diag, c->stream);
+    PD_CUDA_TRY(cudaGetLastError());
+    if (S.nx > 2 * rx && S.ny > 2 * ry && S.nz > 2 * rz) {
+        const int64_t i = rx + (int64_t)S.nx * (ry + (int64_t)S.ny * rz);
+        double* hv = c->hscalar;
+        for (int k = 0; k < 6; ++k)
+            PD_CUDA_TRY(cudaMemcpyAsync(hv + k, c->nd_diag + k * c->n + i, sizeof(double), cudaMemcpyDeviceToHost,
+                                        c->stream));
+        PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < 6; ++k) S.ndint[k] = hv[k];
+    } else {
+        S.nrx = S.nx;  // no interior: every node reads its own block
+    }
+    S.ndr = c->static_split;
+    return PD_OK;
+}
+
 int static_prepare(pd_ctx* c) {
     if (c->sten_gen == c->generation) return PD_OK;
     c->sten_ok = false;
@@ -1716,6 +1798,7 @@ int static_prepare(pd_ctx* c) {
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->sten = pd::StencilDev{(int)nx, (int)ny, (int)nz, ns, radius, c->sten_off, c->sten_geo, c->sten_pmask,
                              c->sten_xm, (int)cols.size(), rz, c->sten_col, c->sten_colgeo};
+    PD_TRY(split_prepare(c, cols, colgeo));
     c->sten_ok = true;
     return PD_OK;
 }
@@ -1765,15 +1848,22 @@ namespace {
 // Preconditioned CG on K x = b with FP64 vectors and device scalars; the
 // residual is read back every 10 iterations.  minv: the block-Jacobi
 // preconditioner (3x3 diagonal blocks, k_static_bjacobi), or null for plain
-// CG.  f32: the matvec of the iterations has FP32 bond terms, and the
-// residual is replaced by the FP64 true residual b - K x whenever the
-// recurred one has fallen by 1e-2 since the last replacement and when it
-// reaches the tolerance ("reliable updates", van der Vorst & Ye, SIAM J. Sci.
-// Comput. 22 (2000) 1716-1731): the FP64 refinement of the FP32 iterations,
-// without restarting the Krylov space.  Convergence is decided on the true
-// residual.  scal: CG_RR = r.z, CG_RRN = the next r.z, CG_RES = r.r.
+// CG.  f32: once the relative residual is below f32_below, the matvec of the
+// iterations has FP32 bond terms, and the residual is replaced by the FP64
+// true residual b - K x whenever the recurred one has fallen by 1e-2 since
+// the last replacement and when it reaches the tolerance ("reliable
+// updates", van der Vorst & Ye, SIAM J. Sci. Comput. 22 (2000) 1716-1731):
+// the FP64 refinement of the FP32 iterations, without restarting the Krylov
+// space.  The first iterations stay FP64 because rounding errors there cost
+// the most: on block-Jacobi CG of clamped lattice cubes, FP32 matvecs from
+// the start took 1.2-1.5x the FP64 iteration count, FP32 matvecs only below
+// a relative residual of 0.1 took the FP64 count (inexact Krylov methods
+// tolerate matvec errors that grow as the residual falls: Simoncini & Szyld,
+// SIAM J. Sci. Comput. 25 (2003) 454-477).  Convergence is decided on the
+// true residual.  scal: CG_RR = r.z, CG_RRN = the next r.z, CG_RES = r.r.
 int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, double* p, double* q, double* z,
-              const double* minv, bool f32, double rtol, int maxit, int* iters, double* relres, int* replacements) {
+              const double* minv, bool f32, double f32_below, double rtol, int maxit, int* iters, double* relres,
+              int* replacements) {
     const int64_t n3 = 3 * c->n;
     cudaStream_t s = c->stream;
     double* scal = c->scal;
@@ -1809,8 +1899,9 @@ int cg_static(pd_ctx* c, double time, const double* b, double* x, double* r, dou
     int it = 0, nrep = 0;
     const int check = 10;
     while (rel > rtol && it < maxit) {
+        const bool use32 = f32 && rel < f32_below;
         for (int k = 0; k < check && it < maxit; ++k, ++it) {
-            static_apply(c, time, f32, p, q);
+            static_apply(c, time, use32, p, q);
             dot(p, q, scal + pd::CG_PQ);
             pd::launch_cg_update_x_f64(x, r, p, q, n3, scal, s);
             precond(scal + pd::CG_RRN);
@@ -1868,7 +1959,8 @@ extern "C" int pd_static_solve(pd_ctx* c, double time, int precision, double rto
     int it = 0, nrep = 0;
     double rel = 0.0;
     rc = cg_static(c, time, b, xd, r, p, q, z, c->static_precond ? c->bj_minv : nullptr,
-                   precision == PD_PREC_FP32C, rtol, maxit, &it, &rel, &nrep);
+                   precision == PD_PREC_FP32C, c->static_f32_below > 0 ? 1.0 / c->static_f32_below : 2.0, rtol,
+                   maxit, &it, &rel, &nrep);
     c->static_replacements = nrep;
     int rc2 = download_vec3(c, x, xd);
     cleanup();

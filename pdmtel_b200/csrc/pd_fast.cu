@@ -389,6 +389,147 @@ __global__ void __launch_bounds__(128) k_static_zcol(Dev d, StencilDev S, const 
     }
 }
 
+// The FP64 operator in the split form K x = D_i x_i - sum_o W_o x_(i+o), with
+// W_o = w_o xi_o xi_o^T and D_i = sum of W_o over the offsets that stay in the
+// box (k_static_ndiag; the same block for every node at least the stencil
+// radius inside the box).  A column (ox, oy) of the stencil contributes
+// -sum_oz w (a_j + ez pz_j) (ex, ey, ez) with a_j = ex px_j + ey py_j formed
+// once per loaded neighbour, so a bond costs three FMAs: s = a + ez pz,
+// T += w s, TZ += (w ez) s, and the column adds (ex T, ey T, TZ) to the node.
+// Neighbours outside the box are simply not loaded.  Columns come sorted by
+// their half-height h (the offsets of a column are oz in [-h, h]; missing
+// ones have w = 0), so every class runs with its own unrolled window and a
+// node does no work for padding.  FP64 only: in FP32 the cancellation of
+// D_i x_i against the neighbour sum is not a rounding of the input and
+// slows CG down.
+template <int H, int R>
+__device__ __forceinline__ void nd_column(const double* __restrict__ xm, int64_t N, int64_t nxy, int64_t jb, int iz0,
+                                          int nz, double sp, const double2* __restrict__ tap, int cx, int cy,
+                                          double (&acc)[R][3]) {
+    constexpr int W = 2 * H + 1;
+    double w[W], wz[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        const double2 t = tap[4 - H + q];
+        w[q] = t.x;
+        wz[q] = t.y;
+    }
+    double T[R], TZ[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) T[m] = TZ[m] = 0.0;
+    const double ex = cx * sp, ey = cy * sp;
+#pragma unroll
+    for (int zz = -H; zz < R + H; ++zz) {
+        const int jz = iz0 + zz;
+        if (jz < 0 || jz >= nz) continue;
+        const int64_t j = jb + nxy * zz;
+        const double px = xm[j], py = xm[N + j], pz = xm[2 * N + j];
+        const double a = fma(ey, py, ex * px);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const int oz = zz - m;
+            if (oz < -H || oz > H) continue;
+            const double s = fma(oz * sp, pz, a);
+            T[m] = fma(w[oz + H], s, T[m]);
+            TZ[m] = fma(wz[oz + H], s, TZ[m]);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        acc[m][0] = fma(-ex, T[m], acc[m][0]);
+        acc[m][1] = fma(-ey, T[m], acc[m][1]);
+        acc[m][2] -= TZ[m];
+    }
+}
+
+template <int H, int R>
+__device__ __forceinline__ void nd_class(const StencilDev& S, const int4* cols, const double2* taps, int c0, int c1,
+                                         const double* __restrict__ xm, int64_t N, int64_t nxy, int64_t i0, int ix,
+                                         int iy, int iz0, bool in_xy, double (&acc)[R][3]) {
+    for (int c = c0; c < c1; ++c) {
+        const int4 C = cols[c];
+        if (!in_xy || (unsigned)(ix + C.x) >= (unsigned)S.nx || (unsigned)(iy + C.y) >= (unsigned)S.ny) continue;
+        nd_column<H, R>(xm, N, nxy, i0 + C.z, iz0, S.nz, S.sp, taps + c * 9, C.x, C.y, acc);
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(128) k_static_nd(Dev d, StencilDev S, const double* __restrict__ x,
+                                                   const double* __restrict__ xm, double* __restrict__ y) {
+    extern __shared__ double2 ndsm[];
+    double2* taps = ndsm;
+    int4* cols = reinterpret_cast<int4*>(taps + S.ndcol * 9);
+    for (int k = threadIdx.x; k < S.ndcol * 9; k += blockDim.x) taps[k] = S.ndtap[k];
+    for (int k = threadIdx.x; k < S.ndcol; k += blockDim.x) cols[k] = S.ndc[k];
+    __syncthreads();
+    const int64_t N = d.n, nxy = (int64_t)S.nx * S.ny;
+    const int ix = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int iy = blockIdx.y * 4 + (threadIdx.x >> 5);
+    const int iz0 = blockIdx.z * R;
+    const bool in_xy = ix < S.nx && iy < S.ny;
+    const int64_t i0 = ix + (int64_t)S.nx * iy + nxy * iz0;
+    double acc[R][3];
+#pragma unroll
+    for (int m = 0; m < R; ++m) acc[m][0] = acc[m][1] = acc[m][2] = 0.0;
+    nd_class<0, R>(S, cols, taps, S.ndcls[0], S.ndcls[1], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
+    nd_class<1, R>(S, cols, taps, S.ndcls[1], S.ndcls[2], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
+    nd_class<2, R>(S, cols, taps, S.ndcls[2], S.ndcls[3], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
+    nd_class<3, R>(S, cols, taps, S.ndcls[3], S.ndcls[4], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
+    nd_class<4, R>(S, cols, taps, S.ndcls[4], S.ndcls[5], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
+    if (!in_xy) return;
+    const bool xy_inner = ix >= S.nrx && ix < S.nx - S.nrx && iy >= S.nry && iy < S.ny - S.nry;
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        const int iz = iz0 + m;
+        if (iz >= S.nz) continue;
+        const int64_t i = i0 + m * nxy;
+        const bool inner = xy_inner && iz >= S.rz && iz < S.nz - S.rz;
+        double D[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) D[k] = inner ? S.ndint[k] : S.ndiag[k * N + i];
+        const double u0 = xm[i], u1 = xm[N + i], u2 = xm[2 * N + i];
+        const double y0 = fma(D[0], u0, fma(D[3], u1, fma(D[4], u2, acc[m][0])));
+        const double y1 = fma(D[3], u0, fma(D[1], u1, fma(D[5], u2, acc[m][1])));
+        const double y2 = fma(D[4], u0, fma(D[5], u1, fma(D[2], u2, acc[m][2])));
+        const unsigned mi = S.pmask[i];
+        y[i] = (mi & 1) ? x[i] : y0;
+        y[N + i] = (mi & 2) ? x[N + i] : y1;
+        y[2 * N + i] = (mi & 4) ? x[2 * N + i] : y2;
+    }
+}
+
+// D_i = sum of w xi xi^T over the stencil offsets that stay in the box, from
+// the column tables k_static_nd reads: blocks (00, 11, 22, 01, 02, 12).
+__global__ void k_static_ndiag(StencilDev S, int64_t N, double* __restrict__ D) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int ix = (int)(i % S.nx), iy = (int)((i / S.nx) % S.ny), iz = (int)(i / ((int64_t)S.nx * S.ny));
+    double a[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int c = 0; c < S.ndcol; ++c) {
+        const int4 C = S.ndc[c];
+        if ((unsigned)(ix + C.x) >= (unsigned)S.nx || (unsigned)(iy + C.y) >= (unsigned)S.ny) continue;
+        const double ex = C.x * S.sp, ey = C.y * S.sp;
+        for (int oz = -C.w; oz <= C.w; ++oz) {
+            if ((unsigned)(iz + oz) >= (unsigned)S.nz) continue;
+            const double w = S.ndtap[c * 9 + 4 + oz].x, ez = oz * S.sp;
+            a[0] += w * ex * ex;
+            a[1] += w * ey * ey;
+            a[2] += w * ez * ez;
+            a[3] += w * ex * ey;
+            a[4] += w * ex * ez;
+            a[5] += w * ey * ez;
+        }
+    }
+    for (int k = 0; k < 6; ++k) D[k * N + i] = a[k];
+}
+
+template <int R>
+void launch_nd(const Dev& d, const StencilDev& S, const double* x, const double* xm, double* y, cudaStream_t s) {
+    const dim3 grid((unsigned)((S.nx + 31) / 32), (unsigned)((S.ny + 3) / 4), (unsigned)((S.nz + R - 1) / R));
+    const size_t sh = (size_t)S.ndcol * (9 * sizeof(double2) + sizeof(int4));
+    k_static_nd<R><<<grid, 128, sh, s>>>(d, S, x, xm, y);
+}
+
 template <typename T, bool SFAC, int R>
 void launch_zcol(const Dev& d, const StencilDev& S, const double* x, const T* xm, double* y, cudaStream_t s) {
     const dim3 grid((unsigned)((S.nx + 31) / 32), (unsigned)((S.ny + 3) / 4), (unsigned)((S.nz + R - 1) / R));
@@ -535,6 +676,10 @@ void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y
     else k_static_apply_f32x<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
 }
 
+void launch_static_ndiag(const StencilDev& S, int64_t n, double* D, cudaStream_t s) {
+    if (n) k_static_ndiag<<<blocks_for(n, 128), 128, 0, s>>>(S, n, D);
+}
+
 void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s) {
     if (d.n == 0) return;
     k_static_pmask<<<blocks_for(d.n, 256), 256, 0, s>>>(d, pm);
@@ -559,7 +704,11 @@ void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const do
     } else {
         double* xm = S.xm;
         k_static_mask<double><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
-        if (zcol) {
+        if (S.ndcol > 0 && !d.sfac && S.ndr == 8) {
+            launch_nd<8>(d, S, x, xm, y, s);
+        } else if (S.ndcol > 0 && !d.sfac && S.ndr == 4) {
+            launch_nd<4>(d, S, x, xm, y, s);
+        } else if (zcol) {
             if (d.sfac) launch_zcol<double, true, 4>(d, S, x, xm, y, s);
             else launch_zcol<double, false, 4>(d, S, x, xm, y, s);
         } else if (d.sfac) {
