@@ -898,7 +898,7 @@ def main():
     ap.add_argument("--plate-dims", default="400x400x4", help="plate lattice of the precision/steps forms")
     ap.add_argument("--prec", default="fp32c", choices=["fp32c", "fp64"], help="arithmetic of --form steps")
     ap.add_argument("--cube", type=int, default=128, help="cube side of --form static")
-    ap.add_argument("--split", type=int, default=4, choices=[0, 4, 8],
+    ap.add_argument("--split", type=int, default=4, choices=[0, 2, 4, 8],
                     help="nodes per thread of the split-form static operator (0: difference form)")
     ap.add_argument("--maxit", type=int, default=100000, help="CG iteration cap of --form static")
     ap.add_argument("--no-precond", action="store_true", help="--form static: plain CG, no block Jacobi")

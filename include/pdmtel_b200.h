@@ -348,7 +348,7 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   plain CG.  Changes the iterates, not the solution beyond the tolerance.
  * PD_OPT_STATIC_SPLIT: the FP64 lattice-stencil operator in the split form
  *   K x = D_i x_i - sum_o W_o x_(i+o) (three FMAs per bond instead of ten;
- *   the same operator to FP64 rounding) with 4 (default) or 8 nodes per
+ *   the same operator to FP64 rounding) with 2, 4 (default) or 8 nodes per
  *   thread along z; 0 runs the difference form.  No effect on the FP32
  *   operator, on spring factors (pd_set_spring_factor) or off the stencil.
  * PD_OPT_STATIC_F32_BELOW: v; the FP32C static solve iterates with the FP64

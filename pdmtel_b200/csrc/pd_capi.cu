@@ -1212,7 +1212,8 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             c->static_f32_below = value;
             return PD_OK;
         case PD_OPT_STATIC_SPLIT:
-            if (value != 0 && value != 4 && value != 8) return fail(PD_ERR_ARG, "pd_set_option: 0, 4 or 8");
+            if (value != 0 && value != 2 && value != 4 && value != 8)
+                return fail(PD_ERR_ARG, "pd_set_option: 0, 2, 4 or 8");
             c->static_split = (int)value;
             c->sten.ndr = c->sten.ndcol > 0 ? (int)value : 0;
             return PD_OK;
@@ -1614,8 +1615,8 @@ namespace {
 // difference form sorted by half-height, (w, w oz spacing) per oz, and the
 // per-node diagonal blocks D_i built on the device from the same tables;
 // the interior block is read back from a node at least the stencil reach
-// inside the box.  Left off (ndcol = 0) when the tables would not fit the
-// 48 KB of shared memory a block gets by default.
+// inside the box.  Left off (ndcol = 0) when the tables would take more than
+// 48 KB of shared memory (the staged tile comes on top of them).
 int split_prepare(pd_ctx* c, const std::vector<int4>& cols, const std::vector<double4>& colgeo) {
     pd::StencilDev& S = c->sten;
     S.ndcol = S.ndr = 0;
@@ -1669,8 +1670,9 @@ int split_prepare(pd_ctx* c, const std::vector<int4>& cols, const std::vector<do
                                         c->stream));
         PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
         for (int k = 0; k < 6; ++k) S.ndint[k] = hv[k];
+        S.ndin = 1;
     } else {
-        S.nrx = S.nx;  // no interior: every node reads its own block
+        S.ndin = 0;  // no interior: every node reads its own block
     }
     S.ndr = c->static_split;
     return PD_OK;

@@ -392,20 +392,44 @@ __global__ void __launch_bounds__(128) k_static_zcol(Dev d, StencilDev S, const 
 // The FP64 operator in the split form K x = D_i x_i - sum_o W_o x_(i+o), with
 // W_o = w_o xi_o xi_o^T and D_i = sum of W_o over the offsets that stay in the
 // box (k_static_ndiag; the same block for every node at least the stencil
-// radius inside the box).  A column (ox, oy) of the stencil contributes
+// reach inside the box).  A column (ox, oy) of the stencil contributes
 // -sum_oz w (a_j + ez pz_j) (ex, ey, ez) with a_j = ex px_j + ey py_j formed
 // once per loaded neighbour, so a bond costs three FMAs: s = a + ez pz,
 // T += w s, TZ += (w ez) s, and the column adds (ex T, ey T, TZ) to the node.
-// Neighbours outside the box are simply not loaded.  Columns come sorted by
-// their half-height h (the offsets of a column are oz in [-h, h]; missing
-// ones have w = 0), so every class runs with its own unrolled window and a
-// node does no work for padding.  FP64 only: in FP32 the cancellation of
-// D_i x_i against the neighbour sum is not a rounding of the input and
-// slows CG down.
-template <int H, int R>
-__device__ __forceinline__ void nd_column(const double* __restrict__ xm, int64_t N, int64_t nxy, int64_t jb, int iz0,
-                                          int nz, double sp, const double2* __restrict__ tap, int cx, int cy,
+// Columns come sorted by their half-height h (the offsets of a column are oz
+// in [-h, h]; missing ones have w = 0), so every class runs with its own
+// unrolled window.  FP64 only: in FP32 the cancellation of D_i x_i against
+// the neighbour sum is not a rounding of the input and slows CG down.
+//
+// A block owns a tile of 32 x 4 x R nodes (a thread: R consecutive nodes of a
+// z column) and first stages the tile and its stencil halo, (32 + 2 rx) x
+// (4 + 2 ry) x (R + 2 rz) nodes of the masked input (k_static_mask), in
+// shared memory with asynchronous copies that are all in flight before the
+// block waits once; positions outside the box are zero-filled, so a
+// neighbour there adds nothing and the bond loop has no box test.  Every
+// neighbour value is read from L2 once per block instead of once per column
+// window of every thread.  (Reading the neighbours straight from global
+// memory ran at a 54% L1 hit rate, latency-bound on the misses: 511 us per
+// 128^3 matvec.)
+__device__ __forceinline__ void cp_async8z(double* sdst, const double* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+// The tile has a halo of RH nodes on every side (RH = the stencil's largest
+// offset component), so every shared-memory offset below is a compile-time
+// constant.
+template <int R, int RH>
+struct NdTile {
+    static constexpr int LX = 32 + 2 * RH, LY = 4 + 2 * RH, LZ = R + 2 * RH;
+    static constexpr int SS = LX * LY, CS = SS * LZ;
+};
+
+template <int H, int R, int RH>
+__device__ __forceinline__ void nd_column(const double* __restrict__ b, const double* ez,
+                                          const double2* __restrict__ tap, double ex, double ey,
                                           double (&acc)[R][3]) {
+    using L = NdTile<R, RH>;
     constexpr int W = 2 * H + 1;
     double w[W], wz[W];
 #pragma unroll
@@ -417,19 +441,15 @@ __device__ __forceinline__ void nd_column(const double* __restrict__ xm, int64_t
     double T[R], TZ[R];
 #pragma unroll
     for (int m = 0; m < R; ++m) T[m] = TZ[m] = 0.0;
-    const double ex = cx * sp, ey = cy * sp;
 #pragma unroll
     for (int zz = -H; zz < R + H; ++zz) {
-        const int jz = iz0 + zz;
-        if (jz < 0 || jz >= nz) continue;
-        const int64_t j = jb + nxy * zz;
-        const double px = xm[j], py = xm[N + j], pz = xm[2 * N + j];
+        const double px = b[zz * L::SS], py = b[L::CS + zz * L::SS], pz = b[2 * L::CS + zz * L::SS];
         const double a = fma(ey, py, ex * px);
 #pragma unroll
         for (int m = 0; m < R; ++m) {
             const int oz = zz - m;
             if (oz < -H || oz > H) continue;
-            const double s = fma(oz * sp, pz, a);
+            const double s = fma(ez[oz + H], pz, a);
             T[m] = fma(w[oz + H], s, T[m]);
             TZ[m] = fma(wz[oz + H], s, TZ[m]);
         }
@@ -442,59 +462,124 @@ __device__ __forceinline__ void nd_column(const double* __restrict__ xm, int64_t
     }
 }
 
-template <int H, int R>
-__device__ __forceinline__ void nd_class(const StencilDev& S, const int4* cols, const double2* taps, int c0, int c1,
-                                         const double* __restrict__ xm, int64_t N, int64_t nxy, int64_t i0, int ix,
-                                         int iy, int iz0, bool in_xy, double (&acc)[R][3]) {
-    for (int c = c0; c < c1; ++c) {
+template <int H, int R, int RH>
+__device__ __forceinline__ void nd_class(const int4* cols, const double2* taps, int c0, int c1, int g,
+                                         const double* own, double sp, double (&acc)[R][3]) {
+    if (H > RH) return;
+    double ez[2 * H + 1];
+#pragma unroll
+    for (int q = 0; q <= 2 * H; ++q) ez[q] = (q - H) * sp;
+    for (int c = c0 + g; c < c1; c += 2) {
         const int4 C = cols[c];
-        if (!in_xy || (unsigned)(ix + C.x) >= (unsigned)S.nx || (unsigned)(iy + C.y) >= (unsigned)S.ny) continue;
-        nd_column<H, R>(xm, N, nxy, i0 + C.z, iz0, S.nz, S.sp, taps + c * 9, C.x, C.y, acc);
+        nd_column<H, R, RH>(own + C.y * NdTile<R, RH>::LX + C.x, ez, taps + c * 9, C.x * sp, C.y * sp, acc);
     }
 }
 
-template <int R>
-__global__ void __launch_bounds__(128) k_static_nd(Dev d, StencilDev S, const double* __restrict__ x,
+// the halo of the tile: the stencil's largest offset component (0 when it
+// is beyond 4: the difference form runs instead)
+inline int nd_halo(const StencilDev& S) {
+    const int h = S.nrx > S.nry ? (S.nrx > S.rz ? S.nrx : S.rz) : (S.nry > S.rz ? S.nry : S.rz);
+    return h <= 4 ? h : 0;
+}
+
+// shared memory of k_static_nd: tables, then the staged tile [3][LZ][LY][LX]
+inline size_t nd_smem(const StencilDev& S, int R) {
+    const size_t h = nd_halo(S);
+    const size_t LX = 32 + 2 * h, LY = 4 + 2 * h, LZ = R + 2 * h;
+    return (size_t)S.ndcol * (9 * sizeof(double2) + sizeof(int4)) + 3 * LX * LY * LZ * sizeof(double);
+}
+
+// 256 threads: two groups of 128 take the even and the odd columns of every
+// class for the same nodes (twice the warps per staged tile), and the second
+// group hands its sums to the first through shared memory.
+template <int R, int RH>
+__global__ void __launch_bounds__(256) k_static_nd(Dev d, StencilDev S, const double* __restrict__ x,
                                                    const double* __restrict__ xm, double* __restrict__ y) {
+    using L = NdTile<R, RH>;
     extern __shared__ double2 ndsm[];
     double2* taps = ndsm;
     int4* cols = reinterpret_cast<int4*>(taps + S.ndcol * 9);
+    double* P = reinterpret_cast<double*>(cols + S.ndcol);
     for (int k = threadIdx.x; k < S.ndcol * 9; k += blockDim.x) taps[k] = S.ndtap[k];
     for (int k = threadIdx.x; k < S.ndcol; k += blockDim.x) cols[k] = S.ndc[k];
-    __syncthreads();
     const int64_t N = d.n, nxy = (int64_t)S.nx * S.ny;
-    const int ix = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int iy = blockIdx.y * 4 + (threadIdx.x >> 5);
-    const int iz0 = blockIdx.z * R;
-    const bool in_xy = ix < S.nx && iy < S.ny;
-    const int64_t i0 = ix + (int64_t)S.nx * iy + nxy * iz0;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 4, z0 = blockIdx.z * R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // stage the tile and its halo: one row of LX nodes per warp at a time
+    for (int row = warp; row < L::LY * L::LZ; row += 8) {
+        const int ly = row % L::LY, lz = row / L::LY;
+        const int gy = y0 - RH + ly, gz = z0 - RH + lz;
+        const bool rv = gy >= 0 && gy < S.ny && gz >= 0 && gz < S.nz;
+        const int64_t jr = (int64_t)gy * S.nx + nxy * gz;
+#pragma unroll
+        for (int lx0 = 0; lx0 < L::LX; lx0 += 32) {
+            const int lx = lx0 + lane;
+            if (lx >= L::LX) break;
+            const int gx = x0 - RH + lx;
+            const bool v = rv && gx >= 0 && gx < S.nx;
+            const int64_t j = v ? jr + gx : 0;  // zero-filled copies read nothing
+            const int k = row * L::LX + lx;
+            cp_async8z(P + k, xm + j, v);
+            cp_async8z(P + L::CS + k, xm + N + j, v);
+            cp_async8z(P + 2 * L::CS + k, xm + 2 * N + j, v);
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    const int g = warp >> 2;  // column group
+    const int tx = lane, ty = warp & 3;
+    const int ix = x0 + tx, iy = y0 + ty;
+    // this thread's first node in the tile
+    const double* own = P + RH * L::SS + (ty + RH) * L::LX + (tx + RH);
     double acc[R][3];
 #pragma unroll
     for (int m = 0; m < R; ++m) acc[m][0] = acc[m][1] = acc[m][2] = 0.0;
-    nd_class<0, R>(S, cols, taps, S.ndcls[0], S.ndcls[1], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
-    nd_class<1, R>(S, cols, taps, S.ndcls[1], S.ndcls[2], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
-    nd_class<2, R>(S, cols, taps, S.ndcls[2], S.ndcls[3], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
-    nd_class<3, R>(S, cols, taps, S.ndcls[3], S.ndcls[4], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
-    nd_class<4, R>(S, cols, taps, S.ndcls[4], S.ndcls[5], xm, N, nxy, i0, ix, iy, iz0, in_xy, acc);
-    if (!in_xy) return;
-    const bool xy_inner = ix >= S.nrx && ix < S.nx - S.nrx && iy >= S.nry && iy < S.ny - S.nry;
+    const double sp = S.sp;
+    nd_class<0, R, RH>(cols, taps, S.ndcls[0], S.ndcls[1], g, own, sp, acc);
+    nd_class<1, R, RH>(cols, taps, S.ndcls[1], S.ndcls[2], g, own, sp, acc);
+    nd_class<2, R, RH>(cols, taps, S.ndcls[2], S.ndcls[3], g, own, sp, acc);
+    nd_class<3, R, RH>(cols, taps, S.ndcls[3], S.ndcls[4], g, own, sp, acc);
+    nd_class<4, R, RH>(cols, taps, S.ndcls[4], S.ndcls[5], g, own, sp, acc);
+    // the own values the first group still needs, then the second group's
+    // sums through the (no longer read) tile
+    double u[R][3];
 #pragma unroll
     for (int m = 0; m < R; ++m) {
-        const int iz = iz0 + m;
+        u[m][0] = own[m * L::SS];
+        u[m][1] = own[L::CS + m * L::SS];
+        u[m][2] = own[2 * L::CS + m * L::SS];
+    }
+    __syncthreads();
+    double* xch = P + (threadIdx.x & 127);
+    if (g == 1) {
+#pragma unroll
+        for (int m = 0; m < R; ++m)
+            for (int a = 0; a < 3; ++a) xch[(3 * m + a) * 128] = acc[m][a];
+    }
+    __syncthreads();
+    if (g == 1 || ix >= S.nx || iy >= S.ny) return;
+#pragma unroll
+    for (int m = 0; m < R; ++m)
+        for (int a = 0; a < 3; ++a) acc[m][a] += xch[(3 * m + a) * 128];
+    const bool xy_inner = S.ndin && ix >= S.nrx && ix < S.nx - S.nrx && iy >= S.nry && iy < S.ny - S.nry;
+    const int64_t i0 = ix + (int64_t)S.nx * iy + nxy * z0;
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        const int iz = z0 + m;
         if (iz >= S.nz) continue;
         const int64_t i = i0 + m * nxy;
         const bool inner = xy_inner && iz >= S.rz && iz < S.nz - S.rz;
         double D[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) D[k] = inner ? S.ndint[k] : S.ndiag[k * N + i];
-        const double u0 = xm[i], u1 = xm[N + i], u2 = xm[2 * N + i];
-        const double y0 = fma(D[0], u0, fma(D[3], u1, fma(D[4], u2, acc[m][0])));
-        const double y1 = fma(D[3], u0, fma(D[1], u1, fma(D[5], u2, acc[m][1])));
-        const double y2 = fma(D[4], u0, fma(D[5], u1, fma(D[2], u2, acc[m][2])));
+        const double u0 = u[m][0], u1 = u[m][1], u2 = u[m][2];
+        const double y0v = fma(D[0], u0, fma(D[3], u1, fma(D[4], u2, acc[m][0])));
+        const double y1v = fma(D[3], u0, fma(D[1], u1, fma(D[5], u2, acc[m][1])));
+        const double y2v = fma(D[4], u0, fma(D[5], u1, fma(D[2], u2, acc[m][2])));
         const unsigned mi = S.pmask[i];
-        y[i] = (mi & 1) ? x[i] : y0;
-        y[N + i] = (mi & 2) ? x[N + i] : y1;
-        y[2 * N + i] = (mi & 4) ? x[2 * N + i] : y2;
+        y[i] = (mi & 1) ? x[i] : y0v;
+        y[N + i] = (mi & 2) ? x[N + i] : y1v;
+        y[2 * N + i] = (mi & 4) ? x[2 * N + i] : y2v;
     }
 }
 
@@ -523,11 +608,25 @@ __global__ void k_static_ndiag(StencilDev S, int64_t N, double* __restrict__ D) 
     for (int k = 0; k < 6; ++k) D[k * N + i] = a[k];
 }
 
+template <int R, int RH>
+void launch_nd_h(const Dev& d, const StencilDev& S, const double* x, const double* xm, double* y, cudaStream_t s) {
+    const dim3 grid((unsigned)((S.nx + 31) / 32), (unsigned)((S.ny + 3) / 4), (unsigned)((S.nz + R - 1) / R));
+    static bool attr = false;  // once per process: the tile needs more than the 48 KB default
+    if (!attr) {
+        cudaFuncSetAttribute(k_static_nd<R, RH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    k_static_nd<R, RH><<<grid, 256, nd_smem(S, R), s>>>(d, S, x, xm, y);
+}
+
 template <int R>
 void launch_nd(const Dev& d, const StencilDev& S, const double* x, const double* xm, double* y, cudaStream_t s) {
-    const dim3 grid((unsigned)((S.nx + 31) / 32), (unsigned)((S.ny + 3) / 4), (unsigned)((S.nz + R - 1) / R));
-    const size_t sh = (size_t)S.ndcol * (9 * sizeof(double2) + sizeof(int4));
-    k_static_nd<R><<<grid, 128, sh, s>>>(d, S, x, xm, y);
+    switch (nd_halo(S)) {
+        case 1: launch_nd_h<R, 1>(d, S, x, xm, y, s); break;
+        case 2: launch_nd_h<R, 2>(d, S, x, xm, y, s); break;
+        case 3: launch_nd_h<R, 3>(d, S, x, xm, y, s); break;
+        default: launch_nd_h<R, 4>(d, S, x, xm, y, s); break;
+    }
 }
 
 template <typename T, bool SFAC, int R>
@@ -676,6 +775,8 @@ void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y
     else k_static_apply_f32x<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, t, x, y);
 }
 
+size_t static_nd_smem(const StencilDev& S, int R) { return nd_smem(S, R); }
+
 void launch_static_ndiag(const StencilDev& S, int64_t n, double* D, cudaStream_t s) {
     if (n) k_static_ndiag<<<blocks_for(n, 128), 128, 0, s>>>(S, n, D);
 }
@@ -704,10 +805,11 @@ void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const do
     } else {
         double* xm = S.xm;
         k_static_mask<double><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
-        if (S.ndcol > 0 && !d.sfac && S.ndr == 8) {
-            launch_nd<8>(d, S, x, xm, y, s);
-        } else if (S.ndcol > 0 && !d.sfac && S.ndr == 4) {
-            launch_nd<4>(d, S, x, xm, y, s);
+        if (S.ndcol > 0 && !d.sfac && (S.ndr == 2 || S.ndr == 4 || S.ndr == 8) && nd_halo(S) > 0 &&
+            nd_smem(S, S.ndr) <= 227 * 1024) {
+            if (S.ndr == 2) launch_nd<2>(d, S, x, xm, y, s);
+            else if (S.ndr == 4) launch_nd<4>(d, S, x, xm, y, s);
+            else launch_nd<8>(d, S, x, xm, y, s);
         } else if (zcol) {
             if (d.sfac) launch_zcol<double, true, 4>(d, S, x, xm, y, s);
             else launch_zcol<double, false, 4>(d, S, x, xm, y, s);

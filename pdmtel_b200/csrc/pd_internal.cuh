@@ -249,9 +249,10 @@ struct StencilDev {
     // the split form (k_static_nd): columns (ox, oy, ox + nx oy, h) sorted by
     // h, ndcls[h] .. ndcls[h + 1] - 1 the columns of half-height h; ndtap[c][oz
     // + 4] = (w, w oz sp); ndiag [6][N] the per-node diagonal blocks, ndint
-    // the block of every node at least (nrx, nry, rz) inside the box; ndr the
+    // the block of every node at least (nrx, nry, rz) inside the box (when
+    // ndin: the box has such nodes); ndr the
     // nodes per thread along z (0: the difference form runs instead)
-    int ndcol, ndr, nrx, nry;
+    int ndcol, ndr, nrx, nry, ndin;
     int ndcls[6];
     double sp;
     double ndint[6];
@@ -262,6 +263,7 @@ struct StencilDev {
 void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s);
 void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const double* x, double* y, cudaStream_t s);
 void launch_static_ndiag(const StencilDev& S, int64_t n, double* D, cudaStream_t s);
+size_t static_nd_smem(const StencilDev& S, int R);  // shared memory of the split-form kernel
 
 // adjoint (pd_adjoint.cu): per-node adjoint vectors [3][N] of one RK4 step
 struct AdjBuf {

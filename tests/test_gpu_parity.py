@@ -242,7 +242,7 @@ def test_static_operator_matches_oracle(tmp_path):
 @pytest.mark.parametrize("dims", [(14, 8, 6), (16, 12, 10)])
 def test_static_stencil_equals_family_kernel(tmp_path, dims):
     """On a complete box the static operator runs as a lattice stencil: the
-    split form (D_i x_i - sum W_o x_j; 4 or 8 nodes per thread) and the
+    split form (D_i x_i - sum W_o x_j; 2, 4 or 8 nodes per thread) and the
     difference form agree with the family-list kernel, and the solvers
     converge.  The larger box has interior nodes (the shared diagonal block),
     the smaller one none."""
@@ -255,7 +255,7 @@ def test_static_stencil_equals_family_kernel(tmp_path, dims):
     n3 = 3 * ctx.n
     xv = np.random.default_rng(5).standard_normal(n3) * 1e-7
     ys = {}
-    for split in (4, 8, 0):
+    for split in (4, 2, 8, 0):
         ctx.set_option(P.OPT_STATIC_SPLIT, split)
         ys[split] = ctx.static_matvec(1e-8, xv)
     # a rigid translation of the free nodes: no force on nodes away from the
