@@ -97,6 +97,7 @@ struct pd_ctx {
     int4* nd_col = nullptr;
     double2* nd_tap = nullptr;
     double* nd_diag = nullptr;
+    std::unique_ptr<pd::NdTab> nd_host;
     double adj_dt = 0.0;
     int64_t *tptr = nullptr;
     int32_t *tj = nullptr, *tpos = nullptr;
@@ -1615,13 +1616,12 @@ namespace {
 // difference form sorted by half-height, (w, w oz spacing) per oz, and the
 // per-node diagonal blocks D_i built on the device from the same tables;
 // the interior block is read back from a node at least the stencil reach
-// inside the box.  Left off (ndcol = 0) when the tables would take more than
-// 48 KB of shared memory (the staged tile comes on top of them).
+// inside the box.  Left off (ndcol = 0) beyond kNdMaxCol columns.
 int split_prepare(pd_ctx* c, const std::vector<int4>& cols, const std::vector<double4>& colgeo) {
     pd::StencilDev& S = c->sten;
     S.ndcol = S.ndr = 0;
     const int nc = (int)cols.size(), rz = S.rz;
-    if (nc == 0 || rz < 1 || rz > 4 || (size_t)nc * (9 * sizeof(double2) + sizeof(int4)) > 48 * 1024) return PD_OK;
+    if (nc == 0 || nc > pd::kNdMaxCol || rz < 1 || rz > 4) return PD_OK;
     const int W = 2 * rz + 1;
     std::vector<int> h(nc, 0), order(nc);
     for (int k = 0; k < nc; ++k) {
@@ -1660,6 +1660,10 @@ int split_prepare(pd_ctx* c, const std::vector<int4>& cols, const std::vector<do
     S.ndc = c->nd_col;
     S.ndtap = c->nd_tap;
     S.ndiag = c->nd_diag;
+    if (!c->nd_host) c->nd_host.reset(new pd::NdTab());
+    std::copy(tap.begin(), tap.end(), c->nd_host->tap);
+    std::copy(nd.begin(), nd.end(), c->nd_host->col);
+    S.ndhost = c->nd_host.get();
     pd::launch_static_ndiag(S, c->n, c->nd_diag, c->stream);
     PD_CUDA_TRY(cudaGetLastError());
     if (S.nx > 2 * rx && S.ny > 2 * ry && S.nz > 2 * rz) {

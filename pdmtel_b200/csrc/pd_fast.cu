@@ -463,15 +463,15 @@ __device__ __forceinline__ void nd_column(const double* __restrict__ b, const do
 }
 
 template <int H, int R, int RH>
-__device__ __forceinline__ void nd_class(const int4* cols, const double2* taps, int c0, int c1, int g,
-                                         const double* own, double sp, double (&acc)[R][3]) {
+__device__ __forceinline__ void nd_class(const NdTab& tb, int c0, int c1, int g, const double* own, double sp,
+                                         double (&acc)[R][3]) {
     if (H > RH) return;
     double ez[2 * H + 1];
 #pragma unroll
     for (int q = 0; q <= 2 * H; ++q) ez[q] = (q - H) * sp;
     for (int c = c0 + g; c < c1; c += 2) {
-        const int4 C = cols[c];
-        nd_column<H, R, RH>(own + C.y * NdTile<R, RH>::LX + C.x, ez, taps + c * 9, C.x * sp, C.y * sp, acc);
+        const int4 C = tb.col[c];
+        nd_column<H, R, RH>(own + C.y * NdTile<R, RH>::LX + C.x, ez, tb.tap + c * 9, C.x * sp, C.y * sp, acc);
     }
 }
 
@@ -482,26 +482,23 @@ inline int nd_halo(const StencilDev& S) {
     return h <= 4 ? h : 0;
 }
 
-// shared memory of k_static_nd: tables, then the staged tile [3][LZ][LY][LX]
+// shared memory of k_static_nd: the staged tile [3][LZ][LY][LX]
 inline size_t nd_smem(const StencilDev& S, int R) {
     const size_t h = nd_halo(S);
     const size_t LX = 32 + 2 * h, LY = 4 + 2 * h, LZ = R + 2 * h;
-    return (size_t)S.ndcol * (9 * sizeof(double2) + sizeof(int4)) + 3 * LX * LY * LZ * sizeof(double);
+    return 3 * LX * LY * LZ * sizeof(double);
 }
 
 // 256 threads: two groups of 128 take the even and the odd columns of every
 // class for the same nodes (twice the warps per staged tile), and the second
 // group hands its sums to the first through shared memory.
 template <int R, int RH>
-__global__ void __launch_bounds__(256) k_static_nd(Dev d, StencilDev S, const double* __restrict__ x,
-                                                   const double* __restrict__ xm, double* __restrict__ y) {
+__global__ void __launch_bounds__(256) k_static_nd(Dev d, StencilDev S, const __grid_constant__ NdTab tb,
+                                                   const double* __restrict__ x, const double* __restrict__ xm,
+                                                   double* __restrict__ y) {
     using L = NdTile<R, RH>;
     extern __shared__ double2 ndsm[];
-    double2* taps = ndsm;
-    int4* cols = reinterpret_cast<int4*>(taps + S.ndcol * 9);
-    double* P = reinterpret_cast<double*>(cols + S.ndcol);
-    for (int k = threadIdx.x; k < S.ndcol * 9; k += blockDim.x) taps[k] = S.ndtap[k];
-    for (int k = threadIdx.x; k < S.ndcol; k += blockDim.x) cols[k] = S.ndc[k];
+    double* P = reinterpret_cast<double*>(ndsm);
     const int64_t N = d.n, nxy = (int64_t)S.nx * S.ny;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 4, z0 = blockIdx.z * R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -535,11 +532,11 @@ __global__ void __launch_bounds__(256) k_static_nd(Dev d, StencilDev S, const do
 #pragma unroll
     for (int m = 0; m < R; ++m) acc[m][0] = acc[m][1] = acc[m][2] = 0.0;
     const double sp = S.sp;
-    nd_class<0, R, RH>(cols, taps, S.ndcls[0], S.ndcls[1], g, own, sp, acc);
-    nd_class<1, R, RH>(cols, taps, S.ndcls[1], S.ndcls[2], g, own, sp, acc);
-    nd_class<2, R, RH>(cols, taps, S.ndcls[2], S.ndcls[3], g, own, sp, acc);
-    nd_class<3, R, RH>(cols, taps, S.ndcls[3], S.ndcls[4], g, own, sp, acc);
-    nd_class<4, R, RH>(cols, taps, S.ndcls[4], S.ndcls[5], g, own, sp, acc);
+    nd_class<0, R, RH>(tb, S.ndcls[0], S.ndcls[1], g, own, sp, acc);
+    nd_class<1, R, RH>(tb, S.ndcls[1], S.ndcls[2], g, own, sp, acc);
+    nd_class<2, R, RH>(tb, S.ndcls[2], S.ndcls[3], g, own, sp, acc);
+    nd_class<3, R, RH>(tb, S.ndcls[3], S.ndcls[4], g, own, sp, acc);
+    nd_class<4, R, RH>(tb, S.ndcls[4], S.ndcls[5], g, own, sp, acc);
     // the own values the first group still needs, then the second group's
     // sums through the (no longer read) tile
     double u[R][3];
@@ -616,7 +613,7 @@ void launch_nd_h(const Dev& d, const StencilDev& S, const double* x, const doubl
         cudaFuncSetAttribute(k_static_nd<R, RH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr = true;
     }
-    k_static_nd<R, RH><<<grid, 256, nd_smem(S, R), s>>>(d, S, x, xm, y);
+    k_static_nd<R, RH><<<grid, 256, nd_smem(S, R), s>>>(d, S, *S.ndhost, x, xm, y);
 }
 
 template <int R>
@@ -805,7 +802,7 @@ void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const do
     } else {
         double* xm = S.xm;
         k_static_mask<double><<<nb, 256, 0, s>>>(S.pmask, d.n, x, xm);
-        if (S.ndcol > 0 && !d.sfac && (S.ndr == 2 || S.ndr == 4 || S.ndr == 8) && nd_halo(S) > 0 &&
+        if (S.ndcol > 0 && S.ndhost && !d.sfac && (S.ndr == 2 || S.ndr == 4 || S.ndr == 8) && nd_halo(S) > 0 &&
             nd_smem(S, S.ndr) <= 227 * 1024) {
             if (S.ndr == 2) launch_nd<2>(d, S, x, xm, y, s);
             else if (S.ndr == 4) launch_nd<4>(d, S, x, xm, y, s);

@@ -259,6 +259,14 @@ struct StencilDev {
     const int4* ndc;
     const double2* ndtap;
     const double* ndiag;
+    const struct NdTab* ndhost;  // host copy of the tables, passed as a kernel parameter
+};
+// The split form's tables as one kernel parameter (constant bank: warp-uniform
+// reads through the constant cache, no shared-memory traffic).
+constexpr int kNdMaxCol = 64;
+struct NdTab {
+    double2 tap[kNdMaxCol * 9];
+    int4 col[kNdMaxCol];
 };
 void launch_static_pmask(const Dev& d, uint8_t* pm, cudaStream_t s);
 void launch_static_stencil(const Dev& d, const StencilDev& S, bool f32, const double* x, double* y, cudaStream_t s);
