@@ -387,6 +387,14 @@ int pd_get_option(pd_ctx* ctx, int option, int64_t* value);
  * graph per (dt, nsteps, launch shape).  Needs PD_PREC_FP32C, 2x2x2 Gauss
  * points and energy accumulation off; same result bit for bit as
  * pd_rk4_steps.  Synchronous. */
+/* Declares that the node ranges offsets[b] .. offsets[b + 1] - 1 (b < nbox,
+ * offsets[0] = 0, offsets[nbox] = the node count) each form a complete box
+ * lattice whose node ids follow x + nx (y + ny z) from the range's first
+ * node, as the specimens of a batch do; the box dimensions are read from the
+ * coordinates.  PD_OPT_FORCE_STENCIL then runs the lattice-stencil FP32 force
+ * on every box.  nbox = 0 returns to one box.  PD_ERR_ARG when a range is
+ * not such a box. */
+int pd_set_boxes(pd_ctx* ctx, int nbox, const int64_t* offsets);
 int pd_rk4_steps_persistent(pd_ctx* ctx, double dt, double t0, int nsteps);
 typedef struct pd_tune_result {
     int64_t tile;          /* PD_OPT_TILE value kept */

@@ -157,6 +157,7 @@ _SIGS = {
     "pdh_batch_count": [_vp, C.POINTER(C.c_int)],
     "pdh_get_tables": [_vp, C.POINTER(pd_material), C.POINTER(pd_bc), _d, _d],
     "pd_rk4_steps_persistent": [_vp, C.c_double, C.c_double, C.c_int],
+    "pd_set_boxes": [_vp, C.c_int, _i64],
     "pd_autotune": [_vp, C.c_double, C.c_int, C.POINTER(pd_tune_result)],
 }
 
@@ -443,6 +444,13 @@ class DeviceContext:
 
     def set_option(self, option, value):
         _check(lib().pd_set_option(self.h, int(option), int(value)), "pd_set_option")
+
+    def set_boxes(self, offsets):
+        """pd_set_boxes: node ranges offsets[b] .. offsets[b + 1] - 1 that are
+        complete box lattices (an empty list returns to one box)."""
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+        nb = max(len(o) - 1, 0)
+        _check(lib().pd_set_boxes(self.h, nb, _p(o, _i64) if nb else None), "pd_set_boxes")
 
     def get_option(self, option):
         v = C.c_int64(0)

@@ -442,6 +442,9 @@ int pdDataManager::EnsureContext() {
     if (rc != PD_OK) return Cuda(rc, "pd_ctx_create");
     pd_set_precision(_ctx, _precision);
     pd_set_energy(_ctx, _energy ? 1 : 0);
+    // specimens that are complete boxes let the batch run the stencil force;
+    // any other batch keeps the general kernels (the refusal changes nothing)
+    if (_batch) pd_set_boxes(_ctx, (int)(_batchOffsets.size() - 1), _batchOffsets.data());
     _uploaded = false;
     return PD_OK;
 }

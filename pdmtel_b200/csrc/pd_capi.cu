@@ -110,6 +110,10 @@ struct pd_ctx {
     int4* fst_u2 = nullptr;
     uint32_t* fst_mask = nullptr;
     float4* fst_tab = nullptr;
+    int4* fst_box = nullptr;         // stencil force boxes (dims, first tile) and (first node, first pair)
+    longlong2* fst_boxb = nullptr;
+    std::vector<int64_t> box_first;  // pd_set_boxes: node ranges that are complete box lattices
+    std::vector<int4> box_dims;
     int64_t* sell_off = nullptr;  // SELL copy of the FP32 gather's lists
     int32_t* sell_idx = nullptr;
     float* sell_coef = nullptr;
@@ -745,6 +749,14 @@ static void fsten_release(pd_ctx* c) {
     dfree(c, c->fst_u2);
     dfree(c, c->fst_mask);
     dfree(c, c->fst_tab);
+    dfree(c, c->fst_box);
+    dfree(c, c->fst_boxb);
+    c->fst_box = nullptr;
+    c->fst_boxb = nullptr;
+    c->d.sten_box = nullptr;
+    c->d.sten_boxb = nullptr;
+    c->d.sten_nbox = 0;
+    c->d.sten_ntiles = 0;
     c->fst_u2 = nullptr;
     c->fst_mask = nullptr;
     c->fst_tab = nullptr;
@@ -762,6 +774,24 @@ static void fsten_release(pd_ctx* c) {
 // union list U2 = S u (S + e_x) of a node pair and the masks of every pair,
 // checking on the device that the node ids follow x + nx (y + ny z) and that
 // every family maps onto U2 in ascending order.
+// The tiles of every box for the block shape (16 pairs x by rows x bz
+// layers): first tile of each box into fst_box, their total into
+// d.sten_ntiles.
+static int fsten_tiles(pd_ctx* c, int by, int bz) {
+    std::vector<int4> bx(c->box_dims.size());
+    int64_t t = 0;
+    for (size_t b = 0; b < bx.size(); ++b) {
+        const int4 D = c->box_dims[b];
+        const int64_t npx = (D.x + 1) / 2;
+        bx[b] = make_int4(D.x, D.y, D.z, (int)t);
+        t += ((npx + 15) / 16) * ((D.y + by - 1) / by) * ((D.z + bz - 1) / bz);
+        if (t > INT32_MAX) return fail(PD_ERR_ARG, "pd_set_option: too many stencil force tiles");
+    }
+    PD_TRY(upload(c, c->fst_box, bx.data(), sizeof(int4) * bx.size()));
+    c->d.sten_ntiles = t;
+    return PD_OK;
+}
+
 static int fsten_prepare(pd_ctx* c, int shape) {
     static const int kBy[5] = {0, 8, 4, 2, 1};
     if (shape < 0 || shape > 4) return fail(PD_ERR_ARG, "pd_set_option: stencil force shape 0..4");
@@ -770,6 +800,7 @@ static int fsten_prepare(pd_ctx* c, int shape) {
         return PD_OK;
     }
     if (c->fst_mask) {  // built: only the block shape changes
+        PD_TRY(fsten_tiles(c, kBy[shape], 8 / kBy[shape]));
         c->fst_shape = shape;
         c->d.sten_by = kBy[shape];
         c->d.sten_bz = 8 / kBy[shape];
@@ -777,17 +808,51 @@ static int fsten_prepare(pd_ctx* c, int shape) {
         return PD_OK;
     }
     const int64_t NX = c->d.lat_nx, NY = c->d.lat_ny, NZ = c->d.lat_nz;
+    const bool one_box = c->box_first.empty();
     if (c->d.cci || c->npt != 8 || !c->d.gc_host || !c->d.lat || !c->have_family || c->d.multimat || c->n == 0 ||
-        NX * NY * NZ != c->n)
+        (one_box && NX * NY * NZ != c->n))
         return fail(PD_ERR_ARG,
-                    "pd_set_option: the stencil force needs 2x2x2 points, one material, a family and a complete "
-                    "box lattice");
+                    "pd_set_option: the stencil force needs 2x2x2 points, one material, a family and complete "
+                    "box lattices");
+    if (one_box) {
+        c->box_dims.assign(1, make_int4((int)NX, (int)NY, (int)NZ, 0));
+    }
+    const std::vector<int64_t> firsts = one_box ? std::vector<int64_t>{0} : c->box_first;
+    const int nbox = (int)c->box_dims.size();
+    std::vector<longlong2> boxb(nbox);
+    int64_t np = 0;
+    for (int b = 0; b < nbox; ++b) {
+        boxb[b] = make_longlong2(firsts[b], np);
+        np += (int64_t)(c->box_dims[b].x + 1) / 2 * c->box_dims[b].y * c->box_dims[b].z;
+    }
+    {
+        int rc0 = PD_OK;
+        if ((rc0 = dalloc(c, &c->fst_box, nbox)) || (rc0 = dalloc(c, &c->fst_boxb, nbox)) ||
+            (rc0 = upload(c, c->fst_boxb, boxb.data(), sizeof(longlong2) * nbox))) {
+            fsten_release(c);
+            return rc0;
+        }
+        c->d.sten_box = c->fst_box;
+        c->d.sten_boxb = c->fst_boxb;
+        c->d.sten_nbox = nbox;
+        if ((rc0 = fsten_tiles(c, kBy[shape], 8 / kBy[shape])) != PD_OK) {
+            fsten_release(c);
+            return rc0;
+        }
+    }
     int* rad = reinterpret_cast<int*>(c->hscalar + 8);
     pd::launch_family_radius(c->d, reinterpret_cast<int*>(c->scal + pd::CG_NSLOT - 1), c->stream);
-    PD_CUDA_TRY(cudaMemcpyAsync(rad, c->scal + pd::CG_NSLOT - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (cudaMemcpyAsync(rad, c->scal + pd::CG_NSLOT - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        fsten_release(c);
+        return fail(PD_ERR_CUDA, "stencil force: family radius");
+    }
     const int R = *rad;
-    if (R > 16) return fail(PD_ERR_ARG, "pd_set_option: family radius too large for the stencil force");
+    if (R > 16) {
+        fsten_release(c);
+        return fail(PD_ERR_ARG, "pd_set_option: family radius too large for the stencil force");
+    }
     const int W = 2 * R + 1;
     int* dbits = nullptr;  // [W^3] bitmap, then the error word
     PD_TRY(dalloc(c, &dbits, (size_t)W * W * W + 1));
@@ -807,6 +872,10 @@ static int fsten_prepare(pd_ctx* c, int shape) {
         return done(fail(PD_ERR_CUDA, "stencil force: offsets"));
     if (bits.back() != 0)
         return done(fail(PD_ERR_ARG, "pd_set_option: node ids do not follow the box lattice x + nx (y + ny z)"));
+    // U2 in lin() order is ascending neighbour id for every node of every box:
+    // two offsets that stay in a box of width nx differ by at most nx - 1 in
+    // x, so their order by (oz, oy, ox) is their order by id in that box, and
+    // lin() with the lattice's nx >= every box's nx keeps that order too.
     // S in ascending id offset, then U2 = S u (S + e_x)
     auto lin = [&](int ox, int oy, int oz) { return (int64_t)ox + NX * ((int64_t)oy + NY * oz); };
     std::vector<std::array<int, 3>> S;
@@ -839,7 +908,6 @@ static int fsten_prepare(pd_ctx* c, int shape) {
         lut[(ox + R) + WX * ((oy + R) + W * (oz + R))] = (int)u;
     }
     const int nu = (int)U.size(), nw = (nu + 31) / 32;
-    const int64_t np = (NX + 1) / 2 * NY * NZ;
     int* dlut = nullptr;
     int rc = PD_OK;
     if ((rc = dalloc(c, &c->fst_u2, std::max<size_t>(u2.size(), 1))) ||
@@ -890,6 +958,55 @@ static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr
     c->d.tile_x = c->d.tile_y = c->d.tile_z = 0;  // its family radius may have changed
     if (c->fst_mask) fsten_release(c);
     c->generation++;
+}
+
+// Node ranges offsets[b] .. offsets[b + 1] - 1 that each form a complete box
+// lattice in id order (the specimens of a batch): the lattice-stencil force
+// then runs on every box.  The dimensions come from the coordinates.
+int pd_set_boxes(pd_ctx* c, int nbox, const int64_t* offsets) {
+    if (!c) return fail(PD_ERR_ARG, "pd_set_boxes: null context");
+    if (nbox < 0 || (nbox > 0 && !offsets)) return fail(PD_ERR_ARG, "pd_set_boxes: null offsets");
+    std::vector<int64_t> first;
+    std::vector<int4> dims;
+    if (nbox > 0) {
+        if (offsets[0] != 0 || offsets[nbox] != c->n)
+            return fail(PD_ERR_ARG, "pd_set_boxes: the ranges must cover the nodes in order");
+        std::vector<int32_t> lat;
+        if (!lattice_positions(c->coords, c->n, c->d.dx, lat))
+            return fail(PD_ERR_ARG, "pd_set_boxes: the nodes are not on one lattice");
+        auto pos = [&](int64_t i, int* q) {
+            q[0] = lat[i] & 2047;
+            q[1] = (lat[i] >> 11) & 2047;
+            q[2] = lat[i] >> 22;
+        };
+        for (int b = 0; b < nbox; ++b) {
+            const int64_t f0 = offsets[b], f1 = offsets[b + 1];
+            if (f1 <= f0) return fail(PD_ERR_ARG, "pd_set_boxes: empty or descending range");
+            int o[3], q[3], ext[3] = {0, 0, 0};
+            pos(f0, o);
+            for (int64_t i = f0; i < f1; ++i) {
+                pos(i, q);
+                for (int a = 0; a < 3; ++a) {
+                    if (q[a] < o[a]) return fail(PD_ERR_ARG, "pd_set_boxes: a range does not start at its corner");
+                    ext[a] = std::max(ext[a], q[a] - o[a] + 1);
+                }
+            }
+            if ((int64_t)ext[0] * ext[1] * ext[2] != f1 - f0)
+                return fail(PD_ERR_ARG, "pd_set_boxes: a range is not a complete box");
+            for (int64_t i = f0; i < f1; ++i) {
+                pos(i, q);
+                if (i != f0 + (q[0] - o[0]) + (int64_t)ext[0] * ((q[1] - o[1]) + (int64_t)ext[1] * (q[2] - o[2])))
+                    return fail(PD_ERR_ARG, "pd_set_boxes: node ids do not follow x + nx (y + ny z) in a box");
+            }
+            first.push_back(f0);
+            dims.push_back(make_int4(ext[0], ext[1], ext[2], 0));
+        }
+    }
+    if (c->fst_mask) fsten_release(c);  // the next PD_OPT_FORCE_STENCIL builds on the boxes
+    c->box_first = first;
+    c->box_dims = dims;
+    c->generation++;
+    return PD_OK;
 }
 
 int pd_bond_search(pd_ctx* c, int64_t* num_halves, int64_t* num_broken, double* min_bond_length) {

@@ -563,12 +563,12 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 // interior, where the sides' independent chains interleave) and for each
 // side alone.
 template <bool HASFAIL, bool BDRY, bool SFAC, int SIDES>
-__device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, const f2* hx, const f2* hy, const f2* hz,
-                                           const float* epsc, float h, Own& A, Own& B) {
+__device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, int NX, int64_t NXY, const f2* hx,
+                                           const f2* hy, const f2* hz, const float* epsc, float h, Own& A, Own& B) {
     const int64_t N = d.n;
     const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
-    const int4 E = __ldg(d.sten_u2 + u);  // id offset, ox, oy, oz from A
-    const int64_t j = ia + E.x;
+    const int4 E = __ldg(d.sten_u2 + u);  // (id offset in one box), ox, oy, oz from A
+    const int64_t j = ia + E.y + (int64_t)NX * E.z + NXY * E.w;
     const float4 us0 = __ldg(blk + 6 * N + j), us1 = __ldg(blk + 7 * N + j);  // hi0 hi1 hi2 lo0 | lo1 lo2 - -
     float bej = 1.f, sfj = 1.f;
     if (BDRY || SFAC) {
@@ -635,10 +635,20 @@ __device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, cons
 
 template <bool HASFAIL, bool BDRY, bool SFAC>
 __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
-    const int NX = d.lat_nx, NY = d.lat_ny, NZ = d.lat_nz;
+    // the box of this tile: the last whose first tile is at most blockIdx.x
+    int lo = 0, hi = d.sten_nbox - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&d.sten_box[mid].w) <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const int4 BX = __ldg(d.sten_box + lo);
+    const longlong2 BB = __ldg(d.sten_boxb + lo);
+    const int NX = BX.x, NY = BX.y, NZ = BX.z;
+    const int64_t NXY = (int64_t)NX * NY;
     const int npx = (NX + 1) >> 1, BY = d.sten_by, BZ = d.sten_bz;
     const int nbx = (npx + 15) >> 4, nby = (NY + BY - 1) / BY;
-    const int b = blockIdx.x;
+    const int b = (int)blockIdx.x - BX.w;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int px = (b % nbx) * 16 + tx;
     const int y = ((b / nbx) % nby) * BY + ty % BY;
@@ -647,8 +657,8 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
     const bool valid = px < npx && y < NY && z < NZ;
     const int64_t NP = d.sten_np;
     const int64_t yz = valid ? y + (int64_t)NY * z : 0;
-    const int64_t p = valid ? px + (int64_t)npx * yz : 0;
-    const int64_t ia = valid ? 2 * px + (int64_t)NX * yz : 0;
+    const int64_t p = valid ? BB.y + px + (int64_t)npx * yz : 0;
+    const int64_t ia = valid ? BB.x + 2 * px + (int64_t)NX * yz : 0;
     const bool hb = valid && 2 * px + 1 < NX;
     Own A, B;
     load_own<true, BDRY, SFAC, false>(d, ia, A);
@@ -675,9 +685,9 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
             m &= m - 1;
             const bool ha = ((ma >> bit) & 1u) != 0, hbit = ((mb >> bit) & 1u) != 0;
             const int u = 32 * w + bit;
-            if (ha && hbit) sten_entry<HASFAIL, BDRY, SFAC, 3>(d, u, ia, hx, hy, hz, epsc, h, A, B);
-            else if (ha) sten_entry<HASFAIL, BDRY, SFAC, 1>(d, u, ia, hx, hy, hz, epsc, h, A, B);
-            else if (hbit) sten_entry<HASFAIL, BDRY, SFAC, 2>(d, u, ia, hx, hy, hz, epsc, h, A, B);
+            if (ha && hbit) sten_entry<HASFAIL, BDRY, SFAC, 3>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B);
+            else if (ha) sten_entry<HASFAIL, BDRY, SFAC, 1>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B);
+            else if (hbit) sten_entry<HASFAIL, BDRY, SFAC, 2>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B);
         }
     }
     if (valid) store_own<false>(d, ia, A, nba, dts, d.vbuf);
@@ -706,12 +716,31 @@ __global__ void k_sten_table(const int4* __restrict__ u2, int nu, PointPack<8> G
 // Setup: the offsets (from the node) of every unbroken family entry, over
 // [-R, R]^3.  err bit 1: a node id is not x + nx (y + ny z) of its lattice
 // position; bit 2: an offset beyond R.
+// the box of node i (boxes in node order)
+__device__ __forceinline__ int sten_box_of_node(const Dev& d, int64_t i) {
+    int lo = 0, hi = d.sten_nbox - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d.sten_boxb[mid].x <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 __global__ void k_sten_offsets(Dev d, int R, int* __restrict__ bitmap, int* __restrict__ err) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= d.n) return;
     const int li = d.lat[i];
     const int xi = li & 2047, yi = (li >> 11) & 2047, zi = li >> 22;
-    if (i != xi + (int64_t)d.lat_nx * (yi + (int64_t)d.lat_ny * zi)) atomicOr(err, 1);
+    // node id = first + x + nx (y + ny z) of its position in its box
+    const int bx = sten_box_of_node(d, i);
+    const int4 BX = d.sten_box[bx];
+    const int64_t f = d.sten_boxb[bx].x;
+    const int l0 = d.lat[f];
+    const int lx = xi - (l0 & 2047), ly = yi - ((l0 >> 11) & 2047), lz = zi - (l0 >> 22);
+    if (lx < 0 || lx >= BX.x || ly < 0 || ly >= BX.y || lz < 0 || lz >= BX.z ||
+        i != f + lx + (int64_t)BX.x * (ly + (int64_t)BX.y * lz))
+        atomicOr(err, 1);
     const int W = 2 * R + 1;
     for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
         const int lj = d.lat[d.acol[p]];
@@ -731,9 +760,18 @@ __global__ void k_sten_masks(Dev d, const int* __restrict__ lut, int R, uint32_t
                              int* __restrict__ err) {
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= d.sten_np) return;
-    const int NX = d.lat_nx, npx = (NX + 1) / 2;
-    const int px = (int)(p % npx);
-    const int64_t ia = 2 * px + (int64_t)NX * (p / npx);
+    int bx = 0, hi = d.sten_nbox - 1;  // the box of pair p
+    while (bx < hi) {
+        const int mid = (bx + hi + 1) >> 1;
+        if (d.sten_boxb[mid].y <= p) bx = mid;
+        else hi = mid - 1;
+    }
+    const int4 BX = d.sten_box[bx];
+    const int64_t lp = p - d.sten_boxb[bx].y;
+    const int NX = BX.x, npx = (NX + 1) / 2;
+    const int64_t NXY = (int64_t)NX * BX.y;
+    const int px = (int)(lp % npx);
+    const int64_t ia = d.sten_boxb[bx].x + 2 * px + (int64_t)NX * (lp / npx);
     const int la = d.lat[ia];
     const int xa = la & 2047, ya = (la >> 11) & 2047, za = la >> 22;
     const int WX = 2 * R + 2, W = 2 * R + 1;
@@ -750,7 +788,8 @@ __global__ void k_sten_masks(Dev d, const int* __restrict__ lut, int R, uint32_t
                 int u = -1;
                 if (ox >= -R && ox <= R + 1 && abs(oy) <= R && abs(oz) <= R)
                     u = lut[(ox + R) + WX * ((oy + R) + W * (oz + R))];
-                if (u < 0 || u <= last || j != ia + d.sten_u2[u].x) {
+                if (u < 0 || u <= last ||
+                    j != ia + d.sten_u2[u].y + (int64_t)NX * d.sten_u2[u].z + NXY * d.sten_u2[u].w) {
                     atomicOr(err, 4);
                     break;
                 }
@@ -1501,9 +1540,7 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
     }
     if (d.blk_cm && d.sten_mask && d.npt == 8 && d.gc_host) {
         // the gather stores chunk-major blocks: only this kernel reads them
-        const int npx = (d.lat_nx + 1) / 2;
-        const unsigned nbk = (unsigned)(((npx + 15) / 16) * ((d.lat_ny + d.sten_by - 1) / d.sten_by) *
-                                        ((d.lat_nz + d.sten_bz - 1) / d.sten_bz));
+        const unsigned nbk = (unsigned)d.sten_ntiles;
         const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
         const PointPack<8> P = pack_points<8>(d, d.gc_host);
 #define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, P, dts)

@@ -117,19 +117,27 @@ struct Dev {
     const int64_t* sell_off;  // [slices + 1] first contributor slot of each slice
     const int32_t* sell_idx;  // [slots][16]
     const float* sell_coef;   // [slots][16][8]
-    // FP32 force on the lattice stencil (2x2x2 points, a complete box lattice
-    // with node id = x + nx (y + ny z), one material).  blk_cm: nblk is stored
-    // chunk-major, float4 chunk c of node j at nblk + 4 (c N + j), so that a
-    // warp reading chunk c of x-adjacent nodes reads contiguous memory.  Work
-    // unit: the x-adjacent node pair (2 px, 2 px + 1) of a row; a block covers
-    // 16 pairs x sten_by rows x sten_bz layers.  Union list U2 = S u (S + e_x)
-    // (S: every lattice offset of a family entry; sten_nu entries, ascending):
-    // .x offset of the neighbour from node A of the pair in node ids, .y .z .w
-    // its lattice offset from A.  Masks [side][word][pair]: bit u of a side
-    // set when U2 entry u is an unbroken bond of that node.
+    // FP32 force on the lattice stencil (2x2x2 points, one material, nodes
+    // that form complete box lattices: box b holds the nodes first_b ..
+    // first_b + nx ny nz - 1 with node id = first_b + x + nx (y + ny z); one
+    // box, or the specimens of a batch).  blk_cm: nblk is stored chunk-major,
+    // float4 chunk c of node j at nblk + 4 (c N + j), so that a warp reading
+    // chunk c of x-adjacent nodes reads contiguous memory.  Work unit: the
+    // x-adjacent node pair (2 px, 2 px + 1) of a row; a block covers 16 pairs
+    // x sten_by rows x sten_bz layers of one box.  Union list U2 = S u (S +
+    // e_x) (S: every lattice offset of a family entry; sten_nu entries, in
+    // ascending neighbour id for every box): .x offset of the neighbour from
+    // node A of the pair in node ids (one box), .y .z .w its lattice offset
+    // from A.  Masks [side][word][pair]: bit u of a side set when U2 entry u
+    // is an unbroken bond of that node.  sten_box[b] = (nx, ny, nz, first
+    // tile), sten_boxb[b] = (first node, first pair), boxes in node order.
     int blk_cm;
     int sten_nu, sten_nw, sten_by, sten_bz;
     int64_t sten_np;
+    int sten_nbox;
+    int64_t sten_ntiles;
+    const int4* sten_box;
+    const longlong2* sten_boxb;
     const int4* sten_u2;
     const float4* sten_tab;       // [2][sten_nu][4] geometry of the stencil force (k_sten_table)
     const uint32_t* sten_mask;    // FP32 gather from contributor patterns: node i's contributors are

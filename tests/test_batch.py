@@ -258,3 +258,46 @@ def test_persistent_barrier_wait_runs_out_and_the_context_recovers(tmp_path):
     bt.run(5, persistent=True)
     Up, Vp = _state(bt.ctx)
     assert np.array_equal(Ug, Up) and np.array_equal(Vg, Vp)
+
+
+@pytest.mark.gpu
+def test_batch_stencil_force_equals_pair_force(tmp_path):
+    """Specimens that are complete boxes run the lattice-stencil force box by
+    box (pd_set_boxes, called by the batch setup): every block shape gives the
+    trajectory of the general pair kernel bit for bit, thin boxes (narrower
+    than the family reach) included."""
+    dims = [(12, 9, 5), (10, 8, 8), (20, 10, 4), (4, 7, 6), (16, 3, 3), (9, 12, 3)]
+    spec = B.BatchSpec(dims=dims, spacing=SPACING, seed=23)
+    bt = B.Batch(str(tmp_path), spec, precision=P.PREC_FP32C)
+    assert bt.ctx.get_option(P.OPT_FORCE_STENCIL) == 0
+    nsteps = 20
+    bt.run(nsteps, persistent=False)
+    U0, V0 = _state(bt.ctx)
+    assert np.abs(U0).max() > 0
+    for shape in (1, 2, 3, 4):
+        bt.ctx.reset_state()
+        bt.ctx.set_option(P.OPT_FORCE_STENCIL, shape)
+        assert bt.ctx.get_option(P.OPT_FORCE_STENCIL) == shape
+        bt.run(nsteps, persistent=False)
+        U1, V1 = _state(bt.ctx)
+        assert np.array_equal(U0, U1) and np.array_equal(V0, V1), shape
+
+
+@pytest.mark.gpu
+def test_batch_stencil_force_refuses_undeclared_boxes(tmp_path):
+    spec = B.BatchSpec(dims=[(12, 9, 5), (10, 8, 8)], spacing=SPACING, seed=31)
+    bt = B.Batch(str(tmp_path), spec, precision=P.PREC_FP32C)
+    n0 = bt.offsets[1]
+    # ranges that are not boxes are refused
+    with pytest.raises(P.PdError):
+        bt.ctx.set_boxes([0, n0 - 5, bt.offsets[2]])
+    with pytest.raises(P.PdError):
+        bt.ctx.set_boxes([0, n0])
+    # without boxes the batch is no box lattice
+    bt.ctx.set_boxes([])
+    with pytest.raises(P.PdError):
+        bt.ctx.set_option(P.OPT_FORCE_STENCIL, 1)
+    assert bt.ctx.get_option(P.OPT_FORCE_STENCIL) == 0
+    bt.ctx.set_boxes(bt.offsets)
+    bt.ctx.set_option(P.OPT_FORCE_STENCIL, 1)
+    assert bt.ctx.get_option(P.OPT_FORCE_STENCIL) == 1
