@@ -386,7 +386,7 @@ def run_batch(args):
     tmp = tempfile.mkdtemp(prefix=f"pdbatch{rank}_")
     t0 = time.time()
     spec = B.BatchSpec(dims=B.draw_dims(256, 2026 + rank), seed=2026 + rank)
-    bt = B.Batch(tmp, spec, precision=P.PREC_FP32C)
+    bt = B.Batch(tmp, spec, precision=P.PREC_FP32C, device_setup=True)  # MLS solved on the device
     setup_s = time.time() - t0
     stream = torch.cuda.ExternalStream(bt.ctx.stream)
     ev_step = bt.evals_per_step()

@@ -341,8 +341,9 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   the context and rebuilt by pd_set_mls) instead of its list, so the
  *   contributor loads no longer wait on an index load from memory.  Same
  *   contributors in the same order: same results bit for bit.  Refused
- *   (PD_ERR_ARG) when the distinct patterns would hold more than 4M
- *   entries; 0 (default) reads the lists.
+ *   (PD_ERR_ARG) when the distinct patterns would hold more than a quarter
+ *   of all list entries (at least 4M allowed, at most 64M); 0 (default)
+ *   reads the lists.
  * PD_OPT_STATIC_PRECOND: 1 (default) preconditions the static CG with the
  *   inverses of the operator's 3x3 diagonal blocks (block Jacobi); 0 runs
  *   plain CG.  Changes the iterates, not the solution beyond the tolerance.

@@ -639,10 +639,9 @@ static int sell_prepare(pd_ctx* c) {
 // The contributor patterns of the FP32 gather: every node's MLS contributor
 // list as id offsets from the node, identical lists stored once (on a box
 // lattice numbered x + nx (y + ny z) the lists of nodes with the same
-// position relative to the boundary are translates of each other).  Built
-// with the MLS data (pd_set_mls), whether or not a gather uses them.  No
-// patterns when the distinct lists would hold more than 4M entries (nothing
-// repeats).
+// position relative to the boundary are translates of each other; in a
+// batch, per specimen).  Built with the MLS data (pd_set_mls), whether or not
+// a gather uses them.
 static void gpat_free(pd_ctx* c) {
     for (void* p : {(void*)c->gpat_id, (void*)c->gpat_ptr, (void*)c->gpat_off}) dfree(c, p);
     c->gpat_id = nullptr;
@@ -674,7 +673,11 @@ static int gpat_build(pd_ctx* c) {
     std::vector<int64_t> ptr{0};
     std::vector<int32_t> off;
     std::unordered_map<uint64_t, std::vector<int32_t>> seen;  // content hash -> pattern ids
-    const size_t kMaxEntries = (size_t)4 << 20;
+    // refused when the distinct lists would hold more than a quarter of all
+    // entries (little repeats: the table would not stay in cache), or above
+    // 64M entries; at least 4M are allowed
+    const size_t kMaxEntries =
+        std::min<size_t>((size_t)64 << 20, std::max<size_t>((size_t)4 << 20, (size_t)cp[N] / 4));
     for (int64_t i = 0; i < N; ++i) {
         const int64_t b = cp[i], e = cp[i + 1];
         uint64_t h = 1469598103934665603ull ^ (uint64_t)(e - b);
@@ -774,17 +777,17 @@ static void fsten_release(pd_ctx* c) {
 // union list U2 = S u (S + e_x) of a node pair and the masks of every pair,
 // checking on the device that the node ids follow x + nx (y + ny z) and that
 // every family maps onto U2 in ascending order.
-// The tiles of every box for the block shape (16 pairs x by rows x bz
-// layers): first tile of each box into fst_box, their total into
-// d.sten_ntiles.
+// The tiles of every box for the block shape (tw pairs x by 16 / tw rows x
+// bz layers, tw = sten_tw of the box): first tile of each box into fst_box,
+// their total into d.sten_ntiles.
 static int fsten_tiles(pd_ctx* c, int by, int bz) {
     std::vector<int4> bx(c->box_dims.size());
     int64_t t = 0;
     for (size_t b = 0; b < bx.size(); ++b) {
         const int4 D = c->box_dims[b];
-        const int64_t npx = (D.x + 1) / 2;
+        const int npx = (D.x + 1) / 2, tw = pd::sten_tw(npx), byw = by * (16 / tw);
         bx[b] = make_int4(D.x, D.y, D.z, (int)t);
-        t += ((npx + 15) / 16) * ((D.y + by - 1) / by) * ((D.z + bz - 1) / bz);
+        t += (int64_t)((npx + tw - 1) / tw) * ((D.y + byw - 1) / byw) * ((D.z + bz - 1) / bz);
         if (t > INT32_MAX) return fail(PD_ERR_ARG, "pd_set_option: too many stencil force tiles");
     }
     PD_TRY(upload(c, c->fst_box, bx.data(), sizeof(int4) * bx.size()));

@@ -547,7 +547,8 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 // holds only what the series form needs, and serves two points per load.)
 
 // One thread per x-adjacent node pair (A, B = A + 1) of a lattice row; a
-// block covers 16 pairs x sten_by rows x sten_bz layers.  A warp walks the
+// block covers tw pairs x (sten_by 16 / tw) rows x sten_bz layers (tw =
+// sten_tw: 16, or 8 / 4 for narrow boxes).  A warp walks the
 // union of its threads' masks over U2 in ascending offset (= ascending
 // neighbour id for every thread), so the U2 entry and the table row are the
 // same for the whole warp; a thread takes the bonds its own masks hold.
@@ -646,11 +647,11 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
     const longlong2 BB = __ldg(d.sten_boxb + lo);
     const int NX = BX.x, NY = BX.y, NZ = BX.z;
     const int64_t NXY = (int64_t)NX * NY;
-    const int npx = (NX + 1) >> 1, BY = d.sten_by, BZ = d.sten_bz;
-    const int nbx = (npx + 15) >> 4, nby = (NY + BY - 1) / BY;
+    const int npx = (NX + 1) >> 1, TW = sten_tw(npx), BY = d.sten_by * (16 / TW), BZ = d.sten_bz;
+    const int nbx = (npx + TW - 1) / TW, nby = (NY + BY - 1) / BY;
     const int b = (int)blockIdx.x - BX.w;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int px = (b % nbx) * 16 + tx;
+    const int tx = threadIdx.x & (TW - 1), ty = threadIdx.x / TW;
+    const int px = (b % nbx) * TW + tx;
     const int y = ((b / nbx) % nby) * BY + ty % BY;
     const int z = (b / (nbx * nby)) * BZ + ty / BY;
     // threads past the box stay in the warp's walk with empty masks

@@ -123,8 +123,9 @@ struct Dev {
     // box, or the specimens of a batch).  blk_cm: nblk is stored chunk-major,
     // float4 chunk c of node j at nblk + 4 (c N + j), so that a warp reading
     // chunk c of x-adjacent nodes reads contiguous memory.  Work unit: the
-    // x-adjacent node pair (2 px, 2 px + 1) of a row; a block covers 16 pairs
-    // x sten_by rows x sten_bz layers of one box.  Union list U2 = S u (S +
+    // x-adjacent node pair (2 px, 2 px + 1) of a row; a block covers tw pairs
+    // x (sten_by 16 / tw) rows x sten_bz layers of one box, tw = sten_tw(the
+    // box's pairs per row).  Union list U2 = S u (S +
     // e_x) (S: every lattice offset of a family entry; sten_nu entries, in
     // ascending neighbour id for every box): .x offset of the neighbour from
     // node A of the pair in node ids (one box), .y .z .w its lattice offset
@@ -241,6 +242,15 @@ void launch_static_apply_f32x(const Dev& d, double t, const double* x, double* y
 // the static operator on a complete box lattice (node id = x + nx (y + ny z))
 // whose families are the horizon stencil clipped to the box
 constexpr int kMaxStencil = 768;  // 64 B of shared memory each: under the 48 KB default
+// Pairs per tile row of the stencil force for a box row of npx pairs: the
+// widest of 16, 8, 4 whose padded row is within 1/8 of the least padded one
+// (narrow boxes waste fewer lanes; wide ones keep 16).
+__host__ __device__ inline int sten_tw(int npx) {
+    const int p16 = (npx + 15) / 16 * 16, p8 = (npx + 7) / 8 * 8, p4 = (npx + 3) / 4 * 4;
+    const int lim = p4 + p4 / 8;  // p4 is the least padded
+    return p16 <= lim ? 16 : (p8 <= lim ? 8 : 4);
+}
+
 struct StencilDev {
     int nx, ny, nz, ns;
     int radius;            // largest |offset| component
