@@ -87,6 +87,42 @@ __device__ __forceinline__ bool point_terms(const Dev& d, const GaussConst& G, d
     return true;
 }
 
+// The same terms in FP32 (the adjoint of the FP32-compensated form): the
+// bond vector and the relative displacement are formed in FP64 from the tape
+// and rounded once; 1/r, 1/p from rsqrtf; the extension from the
+// cancellation-free form.  The derivative is that of the exact force, which
+// the FP32 form's series approximates to FP32 rounding.
+struct PointTermsF {
+    float y0, y1, y2, a, q, bw;
+};
+
+__device__ __forceinline__ float beta_ff(float dist, float delta, float dx) {
+    const float inner = delta - 0.5f * dx, outer = delta + 0.5f * dx;
+    if (dist <= inner) return 1.f;
+    if (dist <= outer) return (outer - dist) / dx;
+    return 0.f;
+}
+
+__device__ __forceinline__ bool point_terms_f(const Dev& d, const GaussConst& G, float x0, float x1, float x2,
+                                              float e0, float e1, float e2, float l0, float l1, float l2,
+                                              float ecrit, float bE, PointTermsF& T) {
+    T.y0 = x0 + e0;
+    T.y1 = x1 + e1;
+    T.y2 = x2 + e2;
+    const float r2 = fmaf(x0, x0, fmaf(x1, x1, x2 * x2));
+    const float p2 = fmaf(T.y0, T.y0, fmaf(T.y1, T.y1, T.y2 * T.y2));
+    const float rinv = rsqrtf(r2), ip = rsqrtf(p2);
+    const float r = r2 * rinv, pl = p2 * ip;
+    const float qx = fmaf(e0, 2.f * x0 + e0, fmaf(e1, 2.f * x1 + e1, e2 * (2.f * x2 + e2)));
+    const float ext = __fdividef(qx, pl + r);
+    if (ext > 0.f && ext * rinv > ecrit) return false;
+    T.bw = bE * beta_ff(r, (float)d.delta, (float)G.dxe) * (float)G.W;
+    T.a = ext * rinv * ip;  // 1/r - 1/p
+    const float yl = fmaf(T.y0, l0, fmaf(T.y1, l1, T.y2 * l2));
+    T.q = yl * ip * ip * ip;
+    return true;
+}
+
 template <int L>
 __global__ void __launch_bounds__(256) k_vjp_own(Dev d, const double* __restrict__ teU,
                                                  const double* __restrict__ teus, const double* __restrict__ teug,
@@ -197,6 +233,119 @@ __global__ void __launch_bounds__(256) k_vjp_partner(Dev d, const double* __rest
     }
     gf = lane_sum<L>(gf);
     if (live && lane == 0 && d.sfac) gradf[j] += gf;
+}
+
+// FP32 versions of the two VJP halves (same traversal, FP32 point terms and
+// FP32 sums per lane, closed in FP64 across the lanes)
+template <int L>
+__global__ void __launch_bounds__(256) k_vjp_own_f32(Dev d, const double* __restrict__ teU,
+                                                     const double* __restrict__ teus, const double* __restrict__ teug,
+                                                     const double* __restrict__ lamF, double* __restrict__ lam_u,
+                                                     double* __restrict__ gradf) {
+    extern __shared__ GaussConst sg[];
+    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t slot = t / L;
+    const int lane = (int)(t % L);
+    const bool live = slot < N;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, gf = 0.f;
+    const int64_t i = live ? d.order[slot] : 0;
+    if (live) {
+        const float l0 = (float)lamF[i], l1 = (float)lamF[N + i], l2 = (float)lamF[2 * N + i];
+        double ui[3];
+        ueff(d, teU, teus, i, ui);
+        const double xi0 = d.x[i], xi1 = d.x[N + i], xi2 = d.x[2 * N + i];
+        const MatDev& Mi = d.mats[d.mat[i]];
+        for (int64_t p = d.arow[i]; p < d.arow[i + 1]; ++p) {
+            const int64_t j = d.acol[p];
+            double cmin;
+            const float c = (float)pair_c(d, i, j, &cmin);
+            const float ecrit = (float)fmin(Mi.ecrit, d.mats[d.mat[j]].ecrit);
+            const float bE = (float)(0.5 * (d.bdry[i] + d.bdry[j]));
+            const double dx0 = d.x[j] - xi0, dx1 = d.x[N + j] - xi1, dx2 = d.x[2 * N + j] - xi2;
+            float gc = 0.f;
+            for (int g = lane; g < d.npt; g += L) {
+                const GaussConst& G = sg[g];
+                const double* ug = teug + (int64_t)(3 * g) * N + j;
+                PointTermsF T;
+                if (!point_terms_f(d, G, (float)(G.hg[0] + dx0), (float)(G.hg[1] + dx1), (float)(G.hg[2] + dx2),
+                                   (float)(ug[0] - ui[0]), (float)(ug[N] - ui[1]), (float)(ug[2 * N] - ui[2]), l0,
+                                   l1, l2, ecrit, bE, T))
+                    continue;
+                const float k = T.bw * c;
+                a0 -= k * fmaf(T.a, l0, T.y0 * T.q);
+                a1 -= k * fmaf(T.a, l1, T.y1 * T.q);
+                a2 -= k * fmaf(T.a, l2, T.y2 * T.q);
+                gc += T.bw * T.a * fmaf(T.y0, l0, fmaf(T.y1, l1, T.y2 * l2));
+            }
+            gf += gc * (float)(0.5 * cmin);
+        }
+    }
+    const double s0 = lane_sum<L>((double)a0), s1 = lane_sum<L>((double)a1), s2 = lane_sum<L>((double)a2);
+    const double sf = lane_sum<L>((double)gf);
+    if (live && lane == 0) {
+        lam_u[i] = s0;
+        lam_u[N + i] = s1;
+        lam_u[2 * N + i] = s2;
+        if (d.sfac) gradf[i] += sf;
+    }
+}
+
+template <int L>
+__global__ void __launch_bounds__(256) k_vjp_partner_f32(Dev d, const double* __restrict__ teU,
+                                                         const double* __restrict__ teus,
+                                                         const double* __restrict__ teug,
+                                                         const double* __restrict__ lamF, double* __restrict__ lam_ug,
+                                                         double* __restrict__ gradf) {
+    extern __shared__ GaussConst sg[];
+    for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
+    __syncthreads();
+    const int64_t N = d.n;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t slot = t / L;
+    const int lane = (int)(t % L);
+    const bool live = slot < N;
+    float gf = 0.f;
+    const int64_t j = live ? d.order[slot] : 0;
+    if (live) {
+        const double xj0 = d.x[j], xj1 = d.x[N + j], xj2 = d.x[2 * N + j];
+        const MatDev& Mj = d.mats[d.mat[j]];
+        for (int g = lane; g < d.npt; g += L) {
+            const GaussConst& G = sg[g];
+            const double* ug = teug + (int64_t)(3 * g) * N + j;
+            const double ug0 = ug[0], ug1 = ug[N], ug2 = ug[2 * N];
+            const double q0 = G.hg[0] + xj0, q1 = G.hg[1] + xj1, q2 = G.hg[2] + xj2;
+            float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+            for (int64_t p = d.arow[j]; p < d.arow[j + 1]; ++p) {
+                const int64_t i = d.acol[p];
+                const float l0 = (float)lamF[i], l1 = (float)lamF[N + i], l2 = (float)lamF[2 * N + i];
+                double ui[3];
+                ueff(d, teU, teus, i, ui);
+                double cmin;
+                const float c = (float)pair_c(d, i, j, &cmin);
+                const float ecrit = (float)fmin(d.mats[d.mat[i]].ecrit, Mj.ecrit);
+                const float bE = (float)(0.5 * (d.bdry[i] + d.bdry[j]));
+                PointTermsF T;
+                if (!point_terms_f(d, G, (float)(q0 - d.x[i]), (float)(q1 - d.x[N + i]), (float)(q2 - d.x[2 * N + i]),
+                                   (float)(ug0 - ui[0]), (float)(ug1 - ui[1]), (float)(ug2 - ui[2]), l0, l1, l2,
+                                   ecrit, bE, T))
+                    continue;
+                const float k = T.bw * c;
+                o0 += k * fmaf(T.a, l0, T.y0 * T.q);
+                o1 += k * fmaf(T.a, l1, T.y1 * T.q);
+                o2 += k * fmaf(T.a, l2, T.y2 * T.q);
+                gf += T.bw * T.a * fmaf(T.y0, l0, fmaf(T.y1, l1, T.y2 * l2)) * (float)(0.5 * cmin);
+            }
+            double* o = lam_ug + (int64_t)(3 * g) * N + j;
+            o[0] = o0;
+            o[N] = o1;
+            o[2 * N] = o2;
+        }
+    }
+    const double sf = lane_sum<L>((double)gf);
+    if (live && lane == 0 && d.sfac) gradf[j] += sf;
 }
 
 // transpose of the MLS gather: lam_us[k] += sum over the Gauss points (j,g)
@@ -332,19 +481,31 @@ __global__ void k_adj_stage1_end(Dev d, AdjBuf A) {
 
 }  // namespace
 
-// lanes per node: 8 for the multi-point rules, 1 for one point
+// lanes per node: 8 for the multi-point rules, 1 for one point; f32: the
+// FP32 point terms (adjoint of the FP32-compensated form)
 void launch_vjp_own(const Dev& d, const double* teU, const double* teus, const double* teug, const double* lamF,
-                    double* lam_u, double* gradf, cudaStream_t s) {
+                    double* lam_u, double* gradf, cudaStream_t s, bool f32) {
     const size_t sh = (size_t)d.npt * sizeof(GaussConst);
-    if (d.npt >= 8) k_vjp_own<8><<<blocks_for(8 * d.n, 256), 256, sh, s>>>(d, teU, teus, teug, lamF, lam_u, gradf);
-    else k_vjp_own<1><<<blocks_for(d.n, 256), 256, sh, s>>>(d, teU, teus, teug, lamF, lam_u, gradf);
+    const unsigned b8 = blocks_for(8 * d.n, 256), b1 = blocks_for(d.n, 256);
+    if (f32) {
+        if (d.npt >= 8) k_vjp_own_f32<8><<<b8, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_u, gradf);
+        else k_vjp_own_f32<1><<<b1, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_u, gradf);
+    } else {
+        if (d.npt >= 8) k_vjp_own<8><<<b8, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_u, gradf);
+        else k_vjp_own<1><<<b1, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_u, gradf);
+    }
 }
 void launch_vjp_partner(const Dev& d, const double* teU, const double* teus, const double* teug, const double* lamF,
-                        double* lam_ug, double* gradf, cudaStream_t s) {
+                        double* lam_ug, double* gradf, cudaStream_t s, bool f32) {
     const size_t sh = (size_t)d.npt * sizeof(GaussConst);
-    if (d.npt >= 8)
-        k_vjp_partner<8><<<blocks_for(8 * d.n, 256), 256, sh, s>>>(d, teU, teus, teug, lamF, lam_ug, gradf);
-    else k_vjp_partner<1><<<blocks_for(d.n, 256), 256, sh, s>>>(d, teU, teus, teug, lamF, lam_ug, gradf);
+    const unsigned b8 = blocks_for(8 * d.n, 256), b1 = blocks_for(d.n, 256);
+    if (f32) {
+        if (d.npt >= 8) k_vjp_partner_f32<8><<<b8, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_ug, gradf);
+        else k_vjp_partner_f32<1><<<b1, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_ug, gradf);
+    } else {
+        if (d.npt >= 8) k_vjp_partner<8><<<b8, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_ug, gradf);
+        else k_vjp_partner<1><<<b1, 256, sh, s>>>(d, teU, teus, teug, lamF, lam_ug, gradf);
+    }
 }
 void launch_gather_T(const Dev& d, const int64_t* tptr, const int32_t* tj, const int32_t* tpos, const double* lam_ug,
                      double* lam_us, cudaStream_t s) {

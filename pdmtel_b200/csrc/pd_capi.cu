@@ -62,6 +62,7 @@ struct pd_ctx {
     };
     std::vector<Checkpoint> ckpt;
     int adj_steps = 0, adj_every = 0, adj_acc = 0;
+    bool adj_f32 = false;  // the last forward run was the FP32-compensated form
     // launch shapes (pd_set_option / pd_autotune)
     int64_t tile = 3 | (2 << 8) | (2 << 16);
     int persist_per_sm = 0;  // 0: as many as fit
@@ -2115,10 +2116,11 @@ extern "C" int pd_set_spring_factor(pd_ctx* c, const double* f) {
 
 namespace {
 
-// one RK4 step (as enqueue_step_body, FP64) that copies, before every force
+// one RK4 step (as enqueue_step_body) that copies, before every force
 // evaluation, the state the force reads: U, the trial displacement and the
-// Gauss-point displacements (tape[s] = {U, us, ug} of stage s)
-void enqueue_step_tape(pd_ctx* c, double dt, double* tape) {
+// Gauss-point displacements (tape[s] = {U, us, ug} of stage s; in the FP32
+// form ug is rebuilt in FP64 from the node blocks the force reads)
+void enqueue_step_tape(pd_ctx* c, double dt, double* tape, bool f32) {
     cudaStream_t s = c->stream;
     const pd::Dev& d = c->d;
     const int64_t n3 = 3 * c->n, ng = n3 * c->npt;
@@ -2127,7 +2129,16 @@ void enqueue_step_tape(pd_ctx* c, double dt, double* tape) {
         double* t = tape + (int64_t)(st - 1) * per;
         cudaMemcpyAsync(t, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(t + n3, d.us, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(t + 2 * n3, d.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+        if (f32) pd::launch_blocks_to_ug(d, t + 2 * n3, s);
+        else cudaMemcpyAsync(t + 2 * n3, d.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+    };
+    auto force = [&](double dts) {
+        if (f32) pd::launch_force_f32c(d, dts, s);
+        else pd::launch_force_f64(d, dts, s);
+    };
+    auto gather = [&](const double* us) {
+        if (f32) pd::launch_gather_f32c(d, us, s);
+        else pd::launch_gather_f64(d, us, s);
     };
     const double h = 0.5 * dt;
     pd::launch_advance_time(d.tdev, dt, s);
@@ -2135,21 +2146,21 @@ void enqueue_step_tape(pd_ctx* c, double dt, double* tape) {
     cudaMemcpyAsync(d.u1, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(d.us, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
     copy(1);
-    pd::launch_force_f64(d, h, s);
+    force(h);
     pd::launch_epilogue(d, 1, h, dt, s);
-    pd::launch_gather_f64(d, d.us, s);
+    gather(d.us);
     copy(2);
-    pd::launch_force_f64(d, h, s);
+    force(h);
     pd::launch_epilogue(d, 2, h, dt, s);
-    pd::launch_gather_f64(d, d.us, s);
+    gather(d.us);
     copy(3);
-    pd::launch_force_f64(d, dt, s);
+    force(dt);
     pd::launch_epilogue(d, 3, dt, dt, s);
-    pd::launch_gather_f64(d, d.us, s);
+    gather(d.us);
     copy(4);
-    pd::launch_force_f64(d, dt, s);
+    force(dt);
     pd::launch_epilogue(d, 4, dt, dt, s);
-    pd::launch_gather_f64(d, d.U, s);
+    gather(d.U);
 }
 
 // transpose of the contributor lists of nodes without a boundary condition
@@ -2210,22 +2221,25 @@ int save_checkpoint(pd_ctx* c, pd_ctx::Checkpoint& k) {
 
 }  // namespace
 
-// Forward run of nsteps FP64 RK4 steps from the current state, keeping a
+// Forward run of nsteps RK4 steps from the current state, keeping a
 // checkpoint (U, V, Gauss-point u, time) every checkpoint_every steps for
-// pd_adjoint_backward.  PD_PREC_FP64A stays FP64A; any other precision
-// runs as PD_PREC_FP64.
+// pd_adjoint_backward.  PD_PREC_FP64A stays FP64A and PD_PREC_FP32C stays
+// FP32C (its node blocks are re-gathered from U at every checkpoint, as the
+// step before would have left them); PD_PREC_FP64 runs as PD_PREC_FP64.
 extern "C" int pd_adjoint_forward(pd_ctx* c, double dt, double t0, int nsteps, int every) {
     if (!c || nsteps < 1 || every < 1) return fail(PD_ERR_ARG, "pd_adjoint_forward: bad argument");
     if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_adjoint_forward: family/MLS data not set");
     if (c->d.cci) return fail(PD_ERR_ARG, "pd_adjoint_forward: the adjoint covers the Gauss-point (FGI) scheme");
     const int prec = c->precision, energy = c->d.energy;
-    if (prec != PD_PREC_FP64A) c->precision = PD_PREC_FP64;
+    if (prec != PD_PREC_FP64A && prec != PD_PREC_FP32C) c->precision = PD_PREC_FP64;
     c->adj_acc = c->d.acc_stretch = prec == PD_PREC_FP64A;
+    c->adj_f32 = prec == PD_PREC_FP32C;
     c->d.energy = 0;
     free_checkpoints(c);
     const int nck = (nsteps + every - 1) / every;
     c->ckpt.resize(nck);
     int rc = set_time(c, t0);
+    if (rc == PD_OK && c->adj_f32) pd::launch_gather_f32c(c->d, c->d.U, c->stream);
     int done = 0;
     for (int k = 0; k < nck && rc == PD_OK; ++k) {
         rc = save_checkpoint(c, c->ckpt[k]);
@@ -2295,6 +2309,7 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
         return fail(PD_ERR_OOM, "pd_adjoint_backward: device memory for the tape");
     }
     const int energy = c->d.energy, acc = c->d.acc_stretch;
+    const bool f32 = c->adj_f32;
     c->d.energy = 0;  // the recomputed steps need no energy density
     c->d.acc_stretch = c->adj_acc;  // and use the forward run's arithmetic
     int rc = upload_vec3(c, lUp, lam_U);
@@ -2311,7 +2326,8 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
         cudaMemcpyAsync(d.V, K.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.ug, K.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
         rc = set_time(c, K.t);
-        for (int n = 0; n < S && rc == PD_OK; ++n) enqueue_step_tape(c, dt, tape + (int64_t)n * 4 * per);
+        if (rc == PD_OK && f32) pd::launch_gather_f32c(d, d.U, s);  // the node blocks the segment started from
+        for (int n = 0; n < S && rc == PD_OK; ++n) enqueue_step_tape(c, dt, tape + (int64_t)n * 4 * per, f32);
         // reverse the segment's steps
         for (int n = S - 1; n >= 0 && rc == PD_OK; --n) {
             const double* tp = tape + (int64_t)n * 4 * per;
@@ -2325,15 +2341,15 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
             for (int st = 4; st >= 2; --st) {
                 const double dts = st >= 3 ? dt : 0.5 * dt;
                 pd::launch_adj_stage_pre(d, dts, lk_of[st], A, s);
-                pd::launch_vjp_own(d, teU(st), teus(st), teug(st), A.lF, A.lueff, gradf, s);
-                pd::launch_vjp_partner(d, teU(st), teus(st), teug(st), A.lF, lug, gradf, s);
+                pd::launch_vjp_own(d, teU(st), teus(st), teug(st), A.lF, A.lueff, gradf, s, f32);
+                pd::launch_vjp_partner(d, teU(st), teus(st), teug(st), A.lF, lug, gradf, s, f32);
                 pd::launch_adj_stage_node(d, A, s);
                 pd::launch_gather_T(d, c->tptr, c->tj, c->tpos, lug, A.lus, s);
                 pd::launch_adj_stage_post(d, alpha[st], lk_of[st - 1], A, s);
             }
             pd::launch_adj_stage_pre(d, 0.5 * dt, A.lk1, A, s);
-            pd::launch_vjp_own(d, teU(1), teus(1), teug(1), A.lF, A.lueff, gradf, s);
-            pd::launch_vjp_partner(d, teU(1), teus(1), teug(1), A.lF, lugSn, gradf, s);
+            pd::launch_vjp_own(d, teU(1), teus(1), teug(1), A.lF, A.lueff, gradf, s, f32);
+            pd::launch_vjp_partner(d, teU(1), teus(1), teug(1), A.lF, lugSn, gradf, s, f32);
             pd::launch_adj_stage1_end(d, A, s);
             cudaMemcpyAsync(lUp, A.lU, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
             cudaMemcpyAsync(lVp, A.lV, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
@@ -2348,6 +2364,7 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
         cudaMemcpyAsync(d.U, K.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.V, K.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.ug, K.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
+        if (f32 && (rc = set_time(c, K.t)) == PD_OK) pd::launch_gather_f32c(d, d.U, s);
         cudaMemcpyAsync(grad_f, gradf, sizeof(double) * N, cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) rc = pd::fail_cuda(e, "adjoint backward", __FILE__, __LINE__);

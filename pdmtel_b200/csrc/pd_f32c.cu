@@ -1288,6 +1288,21 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
     }
 }
 
+// FP64 Gauss-point displacements from the node blocks the FP32 gather wrote:
+// us_j (hi + lo) plus the point's FP32 offset (the adjoint's stage tape of
+// the FP32-compensated form).
+__global__ void k_blocks_to_ug(Dev d, double* __restrict__ ug) {
+    const int64_t N = d.n;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const int npt = d.npt;
+    const BlkOut o = blk_out(d, j);
+    for (int a = 0; a < 3; ++a) {
+        const double u = (double)o[3 * npt + a] + (double)o[3 * npt + 3 + a];
+        for (int g = 0; g < npt; ++g) ug[(int64_t)(3 * g + a) * N + j] = u + (double)o[a * npt + g];
+    }
+}
+
 // SELL layout: the widest contributor list of every slice, then the copy
 __global__ void k_sell_width(Dev d, int64_t* __restrict__ width, int64_t S) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1528,6 +1543,10 @@ int prepare_tiled_force(size_t smem) {
 void launch_family_radius(const Dev& d, int* out, cudaStream_t s) {
     cudaMemsetAsync(out, 0, sizeof(int), s);
     if (d.n > 0 && d.lat) k_family_radius<<<blocks_for(d.n, 256), 256, 0, s>>>(d, out);
+}
+
+void launch_blocks_to_ug(const Dev& d, double* ug, cudaStream_t s) {
+    if (d.n) k_blocks_to_ug<<<blocks_for(d.n, 256), 256, 0, s>>>(d, ug);
 }
 
 void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {

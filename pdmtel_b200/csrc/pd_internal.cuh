@@ -296,9 +296,12 @@ struct AdjBuf {
     double *lU, *lV, *lvb, *lu1, *lk1, *lk2, *lk3, *lk4, *lus, *lF, *lueff;
 };
 void launch_vjp_own(const Dev& d, const double* teU, const double* teus, const double* teug, const double* lamF,
-                    double* lam_u, double* gradf, cudaStream_t s);
+                    double* lam_u, double* gradf, cudaStream_t s, bool f32);
 void launch_vjp_partner(const Dev& d, const double* teU, const double* teus, const double* teug, const double* lamF,
-                        double* lam_ug, double* gradf, cudaStream_t s);
+                        double* lam_ug, double* gradf, cudaStream_t s, bool f32);
+// FP64 Gauss-point displacements [3 npt][N] from the FP32 form's node blocks
+// (the node's trial displacement hi + lo plus each point's FP32 offset)
+void launch_blocks_to_ug(const Dev& d, double* ug, cudaStream_t s);
 void launch_gather_T(const Dev& d, const int64_t* tptr, const int32_t* tj, const int32_t* tpos, const double* lam_ug,
                      double* lam_us, cudaStream_t s);
 void launch_adj_combine(const Dev& d, double dt, const double* lUp, const double* lVp, const AdjBuf& A,
