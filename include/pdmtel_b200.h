@@ -354,7 +354,11 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   operator, on spring factors (pd_set_spring_factor) or off the stencil.
  * PD_OPT_STATIC_F32_BELOW: v; the FP32C static solve iterates with the FP64
  *   operator until the relative residual is below 1/v, then with the FP32
- *   one (default 10: below 0.1); 0 uses the FP32 operator from the start. */
+ *   one (default 10: below 0.1); 0 uses the FP32 operator from the start.
+ * PD_OPT_ADJOINT_VJP32: 1 makes the reverse sweep of an FP32C forward run
+ *   (pd_adjoint_backward) evaluate its point terms in FP32 (faster; the
+ *   family sums of a smooth adjoint cancel, so its gradient is good to about
+ *   1e-3); 0 (default) keeps them FP64 on the FP32C tape. */
 enum {
     PD_OPT_F64_LANES_BELOW = 1,
     PD_OPT_TILE = 2,
@@ -372,7 +376,8 @@ enum {
     PD_OPT_GATHER_STENCIL = 14,
     PD_OPT_STATIC_PRECOND = 15,
     PD_OPT_STATIC_SPLIT = 16,
-    PD_OPT_STATIC_F32_BELOW = 17
+    PD_OPT_STATIC_F32_BELOW = 17,
+    PD_OPT_ADJOINT_VJP32 = 18
 };
 int pd_set_option(pd_ctx* ctx, int option, int64_t value);
 int pd_get_option(pd_ctx* ctx, int option, int64_t* value);

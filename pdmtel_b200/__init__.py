@@ -32,7 +32,7 @@ OPT_F64_LANES_BELOW, OPT_TILE, OPT_PERSIST_BLOCKS_PER_SM = 1, 2, 3
 OPT_PERSIST_FORCE_CHUNK, OPT_PERSIST_GATHER_CHUNK, OPT_STATIC_STENCIL, OPT_GATHER_PER_POINT = 4, 5, 6, 7
 OPT_FORCE_TILE, OPT_FORCE_QUAD, OPT_PERSIST_WAIT_US, OPT_PERSIST_TEST_STALL = 8, 9, 10, 11
 OPT_GATHER_SELL, OPT_FORCE_STENCIL, OPT_GATHER_STENCIL, OPT_STATIC_PRECOND = 12, 13, 14, 15
-OPT_STATIC_SPLIT, OPT_STATIC_F32_BELOW = 16, 17
+OPT_STATIC_SPLIT, OPT_STATIC_F32_BELOW, OPT_ADJOINT_VJP32 = 16, 17, 18
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}

@@ -58,11 +58,13 @@ struct pd_ctx {
     // adjoint: checkpoints (U, V, Gauss-point u, time) of the last forward
     struct Checkpoint {
         double *U = nullptr, *V = nullptr, *ug = nullptr;
+        float* blk = nullptr;  // the FP32 form's node blocks (FP32C forward runs)
         double t = 0.0;
     };
     std::vector<Checkpoint> ckpt;
     int adj_steps = 0, adj_every = 0, adj_acc = 0;
     bool adj_f32 = false;  // the last forward run was the FP32-compensated form
+    int adj_vjp32 = 0;     // PD_OPT_ADJOINT_VJP32: FP32 point terms in its reverse sweep
     // launch shapes (pd_set_option / pd_autotune)
     int64_t tile = 3 | (2 << 8) | (2 << 16);
     int persist_per_sm = 0;  // 0: as many as fit
@@ -1329,6 +1331,10 @@ int pd_set_option(pd_ctx* c, int option, int64_t value) {
             if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
             c->static_stencil_opt = (int)value;
             break;
+        case PD_OPT_ADJOINT_VJP32:
+            if (value > 1) return fail(PD_ERR_ARG, "pd_set_option: 0 or 1");
+            c->adj_vjp32 = (int)value;
+            return PD_OK;
         case PD_OPT_STATIC_F32_BELOW:
             if (value > 1000000000) return fail(PD_ERR_ARG, "pd_set_option: 0..1e9");
             c->static_f32_below = value;
@@ -1429,6 +1435,7 @@ int pd_get_option(pd_ctx* c, int option, int64_t* value) {
         case PD_OPT_STATIC_STENCIL: *value = c->static_stencil_opt; return PD_OK;
         case PD_OPT_STATIC_SPLIT: *value = c->static_split; return PD_OK;
         case PD_OPT_STATIC_F32_BELOW: *value = c->static_f32_below; return PD_OK;
+        case PD_OPT_ADJOINT_VJP32: *value = c->adj_vjp32; return PD_OK;
         case PD_OPT_GATHER_PER_POINT: *value = c->d.gather_per_point; return PD_OK;
         case PD_OPT_FORCE_TILE:
             *value = c->d.tile_x | (c->d.tile_y << 8) | ((int64_t)c->d.tile_z << 16);
@@ -2198,6 +2205,7 @@ void free_checkpoints(pd_ctx* c) {
         dfree(c, k.U);
         dfree(c, k.V);
         dfree(c, k.ug);
+        dfree(c, k.blk);
     }
     c->ckpt.clear();
 }
@@ -2213,6 +2221,11 @@ int save_checkpoint(pd_ctx* c, pd_ctx::Checkpoint& k) {
     PD_CUDA_TRY(cudaMemcpyAsync(k.U, c->d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     PD_CUDA_TRY(cudaMemcpyAsync(k.V, c->d.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     PD_CUDA_TRY(cudaMemcpyAsync(k.ug, c->d.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s));
+    if (c->adj_f32) {
+        const size_t nb = (size_t)c->n * c->d.bs;
+        if (!k.blk) PD_TRY(dalloc(c, &k.blk, nb));
+        PD_CUDA_TRY(cudaMemcpyAsync(k.blk, c->d.nblk, sizeof(float) * nb, cudaMemcpyDeviceToDevice, s));
+    }
     PD_CUDA_TRY(cudaMemcpyAsync(c->hscalar, c->d.tdev, sizeof(double), cudaMemcpyDeviceToHost, s));
     PD_CUDA_TRY(cudaStreamSynchronize(s));
     k.t = c->hscalar[0];
@@ -2224,8 +2237,8 @@ int save_checkpoint(pd_ctx* c, pd_ctx::Checkpoint& k) {
 // Forward run of nsteps RK4 steps from the current state, keeping a
 // checkpoint (U, V, Gauss-point u, time) every checkpoint_every steps for
 // pd_adjoint_backward.  PD_PREC_FP64A stays FP64A and PD_PREC_FP32C stays
-// FP32C (its node blocks are re-gathered from U at every checkpoint, as the
-// step before would have left them); PD_PREC_FP64 runs as PD_PREC_FP64.
+// FP32C (its checkpoints also keep the node blocks the next step reads);
+// PD_PREC_FP64 runs as PD_PREC_FP64.
 extern "C" int pd_adjoint_forward(pd_ctx* c, double dt, double t0, int nsteps, int every) {
     if (!c || nsteps < 1 || every < 1) return fail(PD_ERR_ARG, "pd_adjoint_forward: bad argument");
     if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_adjoint_forward: family/MLS data not set");
@@ -2239,7 +2252,6 @@ extern "C" int pd_adjoint_forward(pd_ctx* c, double dt, double t0, int nsteps, i
     const int nck = (nsteps + every - 1) / every;
     c->ckpt.resize(nck);
     int rc = set_time(c, t0);
-    if (rc == PD_OK && c->adj_f32) pd::launch_gather_f32c(c->d, c->d.U, c->stream);
     int done = 0;
     for (int k = 0; k < nck && rc == PD_OK; ++k) {
         rc = save_checkpoint(c, c->ckpt[k]);
@@ -2309,7 +2321,7 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
         return fail(PD_ERR_OOM, "pd_adjoint_backward: device memory for the tape");
     }
     const int energy = c->d.energy, acc = c->d.acc_stretch;
-    const bool f32 = c->adj_f32;
+    const bool f32 = c->adj_f32, vjp32 = f32 && c->adj_vjp32;
     c->d.energy = 0;  // the recomputed steps need no energy density
     c->d.acc_stretch = c->adj_acc;  // and use the forward run's arithmetic
     int rc = upload_vec3(c, lUp, lam_U);
@@ -2326,7 +2338,8 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
         cudaMemcpyAsync(d.V, K.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.ug, K.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
         rc = set_time(c, K.t);
-        if (rc == PD_OK && f32) pd::launch_gather_f32c(d, d.U, s);  // the node blocks the segment started from
+        if (f32)  // the node blocks the segment started from
+            cudaMemcpyAsync(d.nblk, K.blk, sizeof(float) * (size_t)N * d.bs, cudaMemcpyDeviceToDevice, s);
         for (int n = 0; n < S && rc == PD_OK; ++n) enqueue_step_tape(c, dt, tape + (int64_t)n * 4 * per, f32);
         // reverse the segment's steps
         for (int n = S - 1; n >= 0 && rc == PD_OK; --n) {
@@ -2341,15 +2354,15 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
             for (int st = 4; st >= 2; --st) {
                 const double dts = st >= 3 ? dt : 0.5 * dt;
                 pd::launch_adj_stage_pre(d, dts, lk_of[st], A, s);
-                pd::launch_vjp_own(d, teU(st), teus(st), teug(st), A.lF, A.lueff, gradf, s, f32);
-                pd::launch_vjp_partner(d, teU(st), teus(st), teug(st), A.lF, lug, gradf, s, f32);
+                pd::launch_vjp_own(d, teU(st), teus(st), teug(st), A.lF, A.lueff, gradf, s, vjp32);
+                pd::launch_vjp_partner(d, teU(st), teus(st), teug(st), A.lF, lug, gradf, s, vjp32);
                 pd::launch_adj_stage_node(d, A, s);
                 pd::launch_gather_T(d, c->tptr, c->tj, c->tpos, lug, A.lus, s);
                 pd::launch_adj_stage_post(d, alpha[st], lk_of[st - 1], A, s);
             }
             pd::launch_adj_stage_pre(d, 0.5 * dt, A.lk1, A, s);
-            pd::launch_vjp_own(d, teU(1), teus(1), teug(1), A.lF, A.lueff, gradf, s, f32);
-            pd::launch_vjp_partner(d, teU(1), teus(1), teug(1), A.lF, lugSn, gradf, s, f32);
+            pd::launch_vjp_own(d, teU(1), teus(1), teug(1), A.lF, A.lueff, gradf, s, vjp32);
+            pd::launch_vjp_partner(d, teU(1), teus(1), teug(1), A.lF, lugSn, gradf, s, vjp32);
             pd::launch_adj_stage1_end(d, A, s);
             cudaMemcpyAsync(lUp, A.lU, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
             cudaMemcpyAsync(lVp, A.lV, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
@@ -2364,7 +2377,7 @@ extern "C" int pd_adjoint_backward(pd_ctx* c, const double* lam_U, const double*
         cudaMemcpyAsync(d.U, K.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.V, K.V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.ug, K.ug, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s);
-        if (f32 && (rc = set_time(c, K.t)) == PD_OK) pd::launch_gather_f32c(d, d.U, s);
+        if (f32) cudaMemcpyAsync(d.nblk, K.blk, sizeof(float) * (size_t)N * d.bs, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(grad_f, gradf, sizeof(double) * N, cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) rc = pd::fail_cuda(e, "adjoint backward", __FILE__, __LINE__);

@@ -115,11 +115,12 @@ def test_device_adjoint_matches_oracle_gradient(name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["fgi_velo", "fgi3_ramp", "fgi_slit"])
 def test_fp32c_adjoint_matches_fp64_gradient(name):
-    """The adjoint of the FP32-compensated form (FP32C forward steps, FP32
-    point terms in the reverse sweep, FP64 sums across points and stages):
-    its forward run is the FP32C trajectory, its gradient agrees with the
-    FP64 adjoint's to 1e-4 relative, and it leaves the state (and the node
-    blocks the next FP32C step reads) at the start of the forward run."""
+    """The adjoint of the FP32-compensated form: FP32C forward steps (the
+    FP32C trajectory bit for bit) and segment recompute, reverse sweep with
+    FP64 point terms on that tape (default) or FP32 ones
+    (PD_OPT_ADJOINT_VJP32).  Its gradient agrees with the FP64 adjoint's to
+    1e-5 (1e-3 with FP32 point terms), and it leaves the state and the node
+    blocks the next FP32C step reads at the start of the forward run."""
     g = load_golden(name)
     n = int(g["n"][0])
     dt = DT
@@ -127,6 +128,7 @@ def test_fp32c_adjoint_matches_fp64_gradient(name):
     f = _factors(n, 3)
     a, b = _functional(n, 3)
     dm, ctx = _gpu_ctx(name)
+    ctx.set_energy(False)
     ctx.set_spring_factor(f)
     ctx.set_precision(P.PREC_FP64)
     ctx.reset_state()
@@ -134,19 +136,21 @@ def test_fp32c_adjoint_matches_fp64_gradient(name):
     g64 = ctx.adjoint_backward(a, b)
     ctx.set_precision(P.PREC_FP32C)
     U32, V32 = _gpu_final(ctx, f, dt, nsteps)
-    ctx.reset_state()
-    ctx.adjoint_forward(dt, 0.0, nsteps, every)
-    U, V = ctx.get_state()
-    assert np.array_equal(U, U32) and np.array_equal(V, V32)
-    g32 = ctx.adjoint_backward(a, b)
-    err = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
-    assert err <= 1e-4, err
-    U0, V0 = ctx.get_state()
-    assert not U0.any() and not V0.any()
-    # a forward run after the reverse sweep repeats the first one
-    ctx.adjoint_forward(dt, 0.0, nsteps, every)
-    U2, V2 = ctx.get_state()
-    assert np.array_equal(U2, U32) and np.array_equal(V2, V32)
+    for vjp32, bar in ((0, 1e-5), (1, 1e-3)):
+        ctx.set_option(P.OPT_ADJOINT_VJP32, vjp32)
+        ctx.reset_state()
+        ctx.adjoint_forward(dt, 0.0, nsteps, every)
+        U, V = ctx.get_state()
+        assert np.array_equal(U, U32) and np.array_equal(V, V32)
+        g32 = ctx.adjoint_backward(a, b)
+        err = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
+        assert err <= bar, (vjp32, err)
+        U0, V0 = ctx.get_state()
+        assert not U0.any() and not V0.any()
+        # a forward run after the reverse sweep repeats the first one
+        ctx.adjoint_forward(dt, 0.0, nsteps, every)
+        U2, V2 = ctx.get_state()
+        assert np.array_equal(U2, U32) and np.array_equal(V2, V32)
 
 
 @pytest.mark.gpu
