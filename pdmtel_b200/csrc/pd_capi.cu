@@ -781,8 +781,8 @@ static void fsten_release(pd_ctx* c) {
 // checking on the device that the node ids follow x + nx (y + ny z) and that
 // every family maps onto U2 in ascending order.
 // The tiles of every box for the block shape (tw pairs x by 16 / tw rows x
-// bz layers, tw = sten_tw of the box): first tile of each box into fst_box,
-// their total into d.sten_ntiles.
+// bz layers, tw = sten_tw of the box; runs of 128 pairs where sten_linear):
+// first tile of each box into fst_box, their total into d.sten_ntiles.
 static int fsten_tiles(pd_ctx* c, int by, int bz) {
     std::vector<int4> bx(c->box_dims.size());
     int64_t t = 0;
@@ -790,7 +790,10 @@ static int fsten_tiles(pd_ctx* c, int by, int bz) {
         const int4 D = c->box_dims[b];
         const int npx = (D.x + 1) / 2, tw = pd::sten_tw(npx), byw = by * (16 / tw);
         bx[b] = make_int4(D.x, D.y, D.z, (int)t);
-        t += (int64_t)((npx + tw - 1) / tw) * ((D.y + byw - 1) / byw) * ((D.z + bz - 1) / bz);
+        if (pd::sten_linear(npx, D.y, D.z, tw, byw, bz))
+            t += ((int64_t)npx * D.y * D.z + 127) / 128;
+        else
+            t += (int64_t)((npx + tw - 1) / tw) * ((D.y + byw - 1) / byw) * ((D.z + bz - 1) / bz);
         if (t > INT32_MAX) return fail(PD_ERR_ARG, "pd_set_option: too many stencil force tiles");
     }
     PD_TRY(upload(c, c->fst_box, bx.data(), sizeof(int4) * bx.size()));

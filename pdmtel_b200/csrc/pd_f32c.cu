@@ -648,12 +648,20 @@ __global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> 
     const int NX = BX.x, NY = BX.y, NZ = BX.z;
     const int64_t NXY = (int64_t)NX * NY;
     const int npx = (NX + 1) >> 1, TW = sten_tw(npx), BY = d.sten_by * (16 / TW), BZ = d.sten_bz;
-    const int nbx = (npx + TW - 1) / TW, nby = (NY + BY - 1) / BY;
     const int b = (int)blockIdx.x - BX.w;
-    const int tx = threadIdx.x & (TW - 1), ty = threadIdx.x / TW;
-    const int px = (b % nbx) * TW + tx;
-    const int y = ((b / nbx) % nby) * BY + ty % BY;
-    const int z = (b / (nbx * nby)) * BZ + ty / BY;
+    int px, y, z;
+    if (sten_linear(npx, NY, NZ, TW, BY, BZ)) {  // 128 consecutive pairs of the box
+        const int64_t lp = (int64_t)b * 128 + threadIdx.x;
+        px = (int)(lp % npx);
+        y = (int)((lp / npx) % NY);
+        z = (int)(lp / ((int64_t)npx * NY));
+    } else {
+        const int nbx = (npx + TW - 1) / TW, nby = (NY + BY - 1) / BY;
+        const int tx = threadIdx.x & (TW - 1), ty = threadIdx.x / TW;
+        px = (b % nbx) * TW + tx;
+        y = ((b / nbx) % nby) * BY + ty % BY;
+        z = (b / (nbx * nby)) * BZ + ty / BY;
+    }
     // threads past the box stay in the warp's walk with empty masks
     const bool valid = px < npx && y < NY && z < NZ;
     const int64_t NP = d.sten_np;

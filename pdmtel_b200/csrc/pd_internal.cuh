@@ -251,6 +251,17 @@ __host__ __device__ inline int sten_tw(int npx) {
     return p16 <= lim ? 16 : (p8 <= lim ? 8 : 4);
 }
 
+// Whether a box of npx pairs x ny rows x nz layers takes its stencil-force
+// tiles as runs of 128 consecutive pairs in (x, y, z) order instead of 3D
+// tiles of tw x by x bz: when the 3D tiles would leave more than a tenth of
+// the lanes past the box (small specimens of a batch).
+__host__ __device__ inline bool sten_linear(int npx, int ny, int nz, int tw, int by, int bz) {
+    const long long np = (long long)npx * ny * nz;
+    const long long pad =
+        (long long)((npx + tw - 1) / tw * tw) * ((ny + by - 1) / by * by) * (long long)((nz + bz - 1) / bz * bz);
+    return np * 10 < pad * 9;
+}
+
 struct StencilDev {
     int nx, ny, nz, ns;
     int radius;            // largest |offset| component
