@@ -1194,6 +1194,19 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gsrc) : "memory");
 }
+// the same with an L2 eviction policy (the coefficient stream is read once
+// per gather: evict it first, so that the node blocks the force reads next
+// stay in L2)
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void cp_async16_pol(void* sdst, const void* gsrc, uint64_t pol) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(sa), "l"(gsrc), "l"(pol)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int NPEND>
 __device__ __forceinline__ void cp_async_wait() {
@@ -1231,9 +1244,10 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
     // contributor slot k of this thread: cf[32 k] (a slot is kSell nodes x 8 floats = 32 float4)
     const float4* cf = reinterpret_cast<const float4*>(d.sell_coef + (base * kSell + ln) * 8 + g0);
     float4* r = &ring[threadIdx.x >> 5][0][threadIdx.x & 31];  // ring entry e at r[32 e]
+    const uint64_t pol = l2_evict_first();
 #pragma unroll
     for (int k = 0; k < kRing; ++k) {
-        if (k < nc) cp_async16(r + 32 * k, cf + (int64_t)32 * k);
+        if (k < nc) cp_async16_pol(r + 32 * k, cf + (int64_t)32 * k, pol);
         cp_async_commit();
     }
     // trial displacements of contributors k .. k+3, loaded one group ahead
@@ -1282,7 +1296,7 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
         for (int u = 0; u < 4; ++u) {
             const int eu = e + u < kRing ? e + u : e + u - kRing;
             const int kk = k + kRing + u;
-            if (kk < nc) cp_async16(r + 32 * eu, cf + (int64_t)32 * kk);
+            if (kk < nc) cp_async16_pol(r + 32 * eu, cf + (int64_t)32 * kk, pol);
             cp_async_commit();
         }
         e = e + 4 < kRing ? e + 4 : e + 4 - kRing;
