@@ -1213,20 +1213,25 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
 }
 
-constexpr int kRing = 12;  // coefficient slots a thread keeps in flight
+// coefficient slots a thread keeps in flight: 64 KB of ring per block, two
+// blocks per SM (12 slots in static shared memory: 1.84 ms per plate step;
+// 16: 1.78; 24: 1.78)
+constexpr int kRingSlots = 16;
 
 // The SELL + pattern gather (2x2x2 points) with the coefficient stream run
 // through a shared-memory ring: each thread copies its own 16 bytes of each
 // contributor slot kRing slots ahead of the arithmetic (one commit group per
-// slot), so a warp keeps about 6 KB of the stream in flight without holding
+// slot), so a warp keeps about 8 KB of the stream in flight without holding
 // it in registers; the contributor ids come from the node's pattern
 // (L1-resident), and the contributors' trial displacements of the next group
 // of four are loaded while the current group is summed.  A thread reads back only what it
 // copied itself, after cp.async.wait_group, and refills a ring entry only
 // after the values read from it have been used.  Same FMAs in the same
 // contributor order as gather_group: the same result bit for bit.
+template <int kRing>
 __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double* __restrict__ us) {
-    __shared__ float4 ring[8][kRing][32];
+    extern __shared__ float4 ring_sm[];  // [8 warps][kRing][32 lanes]
+    float4 (*ring)[kRing][32] = reinterpret_cast<float4 (*)[kRing][32]>(ring_sm);
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (tid >= d.n * 2) return;
     const int64_t N = d.n;
@@ -1704,7 +1709,13 @@ void launch_gather_f32c(const Dev& d, const double* us, cudaStream_t s) {
     const unsigned nb = blocks_for(d.n * ngrp, 256);
     const bool sell = d.sell_on && d.sell_idx && d.mls && d.npt == 8, pat = d.gpat_id && d.mls;
     if (sell && pat && d.npt == 8) {
-        k_gather_f32c_ring<<<nb, 256, 0, s>>>(d, us);
+        static bool attr = false;  // once per process: the ring needs more than the 48 KB default
+        const size_t sh = (size_t)8 * kRingSlots * 32 * sizeof(float4);
+        if (!attr) {
+            cudaFuncSetAttribute(k_gather_f32c_ring<kRingSlots>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+            attr = true;
+        }
+        k_gather_f32c_ring<kRingSlots><<<nb, 256, sh, s>>>(d, us);
     } else if (sell) {
         if (pat) k_gather_f32c<true, true><<<nb, 256, 0, s>>>(d, us);
         else k_gather_f32c<true, false><<<nb, 256, 0, s>>>(d, us);
