@@ -634,8 +634,11 @@ __device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, int 
     }
 }
 
+// Five blocks per SM (96 registers, 20 warps; 8 bytes of spill): the walk is
+// latency-bound, and 4 blocks at 110 registers measured 5.00 against 4.70 ms
+// per plate step (6 blocks at 80 registers: 4.71, with 104 bytes of spill).
 template <bool HASFAIL, bool BDRY, bool SFAC>
-__global__ void __launch_bounds__(128, 4) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
+__global__ void __launch_bounds__(128, 5) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
     // the box of this tile: the last whose first tile is at most blockIdx.x
     int lo = 0, hi = d.sten_nbox - 1;
     while (lo < hi) {
