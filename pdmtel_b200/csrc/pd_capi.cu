@@ -40,6 +40,8 @@ struct pd_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t copy_stream = nullptr;  // pd_rk4_steps_host: result copies beside the closing gather
+    cudaEvent_t ev_final = nullptr, ev_copied = nullptr;
     pd::Dev d{};
     int64_t n = 0, H = 0, Ha = 0;
     int npt = 1;
@@ -290,7 +292,7 @@ bool ready_dynamic(pd_ctx* c) {
 }
 
 // the four stages of pdDataManager::RK4 and the closing gather
-void enqueue_step_body(pd_ctx* c, double dt) {
+void enqueue_step_body(pd_ctx* c, double dt, bool closing_gather = true) {
     cudaStream_t s = c->stream;
     const pd::Dev& d = c->d;
     const int64_t n3 = 3 * c->n;
@@ -321,7 +323,13 @@ void enqueue_step_body(pd_ctx* c, double dt) {
     force(dt);
     pd::launch_epilogue(d, 4, dt, dt, s);
     if (d.energy) pd::launch_energy_reduce(d, s);
-    gather(d.U);
+    if (closing_gather) gather(d.U);
+}
+
+// the closing gather of a step alone (CalcIntgPointDisplRK4 at the new U)
+void enqueue_closing_gather(pd_ctx* c) {
+    if (c->precision == PD_PREC_FP32C) pd::launch_gather_f32c(c->d, c->d.U, c->stream);
+    else pd::launch_gather_f64(c->d, c->d.U, c->stream);
 }
 
 }  // namespace
@@ -587,6 +595,12 @@ int pd_ctx_destroy(pd_ctx* c) {
         if (p) cudaFree(p);
     if (c->hstage) cudaFreeHost(c->hstage);
     if (c->hscalar) cudaFreeHost(c->hscalar);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    if (c->ev_final) cudaEventDestroy(c->ev_final);
+    if (c->ev_copied) cudaEventDestroy(c->ev_copied);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PD_OK;
@@ -1639,16 +1653,47 @@ int pd_rk4_steps_host(pd_ctx* c, double dt, double t0, int nsteps, const double*
         PD_CUDA_TRY(cudaMemcpyAsync(c->scratch + 3 * c->n, V_in, b3, cudaMemcpyHostToDevice, c->stream));
         pd::launch_to_soa(c->scratch + 3 * c->n, c->d.V, c->n, 3, c->stream);
     }
-    PD_TRY(pd_rk4_steps(c, dt, t0, nsteps));
-    if (U_out) {
-        pd::launch_to_aos(c->d.U, c->scratch, c->n, 3, c->stream);
-        PD_CUDA_TRY(cudaMemcpyAsync(U_out, c->scratch, b3, cudaMemcpyDeviceToHost, c->stream));
-    }
-    if (V_out) {
-        pd::launch_to_aos(c->d.V, c->scratch + 3 * c->n, c->n, 3, c->stream);
-        PD_CUDA_TRY(cudaMemcpyAsync(V_out, c->scratch + 3 * c->n, b3, cudaMemcpyDeviceToHost, c->stream));
+    // nsteps - 1 steps from the step graph, the last one launched directly so
+    // that U and V (final after its fourth stage) are copied out on a second
+    // stream while its closing gather, which only reads U, runs
+    if (nsteps > 1) PD_TRY(pd_rk4_steps(c, dt, t0, nsteps - 1));
+    if (nsteps >= 1) {
+        if (nsteps == 1) PD_TRY(set_time(c, t0));
+        if (!c->copy_stream) {
+            PD_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+            PD_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_final, cudaEventDisableTiming));
+            PD_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+        }
+        pd::launch_advance_time(c->d.tdev, dt, c->stream);
+        enqueue_step_body(c, dt, false);
+        PD_CUDA_TRY(cudaEventRecord(c->ev_final, c->stream));
+        PD_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->ev_final, 0));
+        enqueue_closing_gather(c);
+        cudaStream_t cs = c->copy_stream;
+        if (U_out) {
+            pd::launch_to_aos(c->d.U, c->scratch, c->n, 3, cs);
+            PD_CUDA_TRY(cudaMemcpyAsync(U_out, c->scratch, b3, cudaMemcpyDeviceToHost, cs));
+        }
+        if (V_out) {
+            pd::launch_to_aos(c->d.V, c->scratch + 3 * c->n, c->n, 3, cs);
+            PD_CUDA_TRY(cudaMemcpyAsync(V_out, c->scratch + 3 * c->n, b3, cudaMemcpyDeviceToHost, cs));
+        }
+        // the next call's uploads into scratch wait for these copies
+        PD_CUDA_TRY(cudaEventRecord(c->ev_copied, cs));
+        PD_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_copied, 0));
+        PD_CUDA_TRY(cudaGetLastError());
+    } else {
+        if (U_out) {
+            pd::launch_to_aos(c->d.U, c->scratch, c->n, 3, c->stream);
+            PD_CUDA_TRY(cudaMemcpyAsync(U_out, c->scratch, b3, cudaMemcpyDeviceToHost, c->stream));
+        }
+        if (V_out) {
+            pd::launch_to_aos(c->d.V, c->scratch + 3 * c->n, c->n, 3, c->stream);
+            PD_CUDA_TRY(cudaMemcpyAsync(V_out, c->scratch + 3 * c->n, b3, cudaMemcpyDeviceToHost, c->stream));
+        }
     }
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->copy_stream) PD_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
     return PD_OK;
 }
 
