@@ -58,8 +58,11 @@ __device__ __forceinline__ double extension(double x0, double x1, double x2, dou
 // CalcBondBasedMotionRK4 (pdDataManager.cpp:1917-1962) with the per-point
 // CalcBondForceCCI (pdDataManager2.cpp:1293-1351).  CCI: the one-point
 // branch (pdDataManager.cpp:1818-1866).
+// Eight blocks per SM (64 registers, ~200 bytes of spill to L1): the
+// evaluation is a chain of IEEE square roots and divisions, so more resident
+// warps hide more of it (plate step 77 -> 64.5 ms; 6 blocks 70, 12 blocks 67).
 template <bool CCI, bool ENERGY, bool SFAC, bool ACC>
-__global__ void __launch_bounds__(128) k_force_f64(Dev d, double dts) {
+__global__ void __launch_bounds__(128, 8) k_force_f64(Dev d, double dts) {
     extern __shared__ GaussConst sg[];
     for (int g = threadIdx.x; g < d.npt; g += blockDim.x) sg[g] = d.gc[g];
     __syncthreads();
