@@ -434,10 +434,14 @@ int pd_autotune(pd_ctx* ctx, double dt, int steps, pd_tune_result* out);
  * differentiable in f; f = exp(m) gives a log-micromodulus field m. */
 /* replace the per-node spring factors f [N] (host, positive) */
 int pd_set_spring_factor(pd_ctx* ctx, const double* f);
-/* Forward half of the adjoint pair: nsteps FP64 RK4 steps of the scheme of
+/* Forward half of the adjoint pair: nsteps RK4 steps of the scheme of
  * pdDataManager::RK4 (pdDataManager.cpp:1994-2134) from the current state at
  * time t0, storing (U, V, Gauss-point displacements, time) every
  * checkpoint_every steps in the context.  The state ends at step nsteps.
+ * The steps run in the context's precision: FP64 (PD_PREC_FP64A stays
+ * FP64A), or at PD_PREC_FP32C the
+ * compensated FP32 step (checkpoints then hold its node blocks, so the
+ * reverse sweep recomputes the forward bit for bit).
  * FGI (Gauss-point) scheme only. */
 int pd_adjoint_forward(pd_ctx* ctx, double dt, double t0, int nsteps, int checkpoint_every);
 /* Backward half: the vector-Jacobian product of the last forward run.
