@@ -22,7 +22,8 @@ sources) on a 40x40x4 sub-plate of the same workload, one process per host
 core, each step one RK4 step of every process.
 
 The headline line also carries `adjoint`: seconds per RK4 step of the
-differentiation form (forward with checkpoints + reverse sweep, FP64) on the
+differentiation form (forward with checkpoints + reverse sweep; FP64, FP64A,
+FP32C with FP64 point terms, FP32C with FP32 point terms) on the
 64x64x8 identification specimen (spacing 1 mm, fixed face and 0.02 m/s pulled
 face, log-micromodulus a Gaussian random field, sigma 0.2, correlation 5 mm).
 
