@@ -39,7 +39,14 @@ enum pd_status {
 /* boundary-condition types, pdDataManager.h:231 / pdBdryCondition.h:25 */
 enum pd_bc_type { PD_BC_DISPL = 1, PD_BC_VELOC = 2, PD_BC_DISPLGRAD = 3, PD_BC_TRACTION = 4 };
 /* volume integration scheme, pdDataManager.cpp:571-730 */
-enum pd_integration { PD_INTG_CCI = 0, PD_INTG_FGI = 1 };
+enum pd_integration {
+    PD_INTG_CCI = 0,
+    PD_INTG_FGI = 1,
+    /* adaptive trapezoid over the family cell cut by the horizon sphere
+     * (ai_on, pdIntgManager types 1-3); intg_point is the trapezoid index
+     * (1..3: 2, 3 or 5 points per direction); data from pd_set_ai */
+    PD_INTG_AI = 2
+};
 /* arithmetic of the force / gather / matvec kernels */
 enum pd_precision {
     PD_PREC_FP64 = 0,  /* the drop-in: bit-faithful to the reference CPU path */
@@ -144,6 +151,69 @@ int pd_mls_setup(pd_ctx* ctx, double rw, const double* mls_coords, int64_t* num_
 /* The context's MLS data out in the layout of pd_set_mls: cb_ptr [N+1],
  * cb_idx [entries] and coeff [entries x points] (either may be NULL). */
 int pd_get_mls(pd_ctx* ctx, int64_t* cb_ptr, int32_t* cb_idx, double* coeff);
+/* Adaptive-trapezoid (AI) integration (pdDataManager::CalcBondForceIntg,
+ * pdDataManager2.cpp:1227-1291; pdIntgManager.cpp:49-3491).  A bond's force is
+ * a sum of regions, each a nested trapezoid rule: the outer direction axis[0]
+ * over [a, b], the middle direction axis[1] between the limit functions
+ * lim[0], lim[1] of the outer value, the inner direction axis[2] between
+ * lim[2], lim[3] of the outer and middle values.  Limit codes (dx spacing,
+ * x_j the family node relative to node i, delta the horizon):
+ *   middle: 2 axis + side          x_j[axis] -/+ dx/2 (side 0 low, 1 high)
+ *           8 + 4 (3 A + B) + 2 side + sign
+ *                                  +/- sqrt(r^2 - t^2) (0 where negative),
+ *                                  r^2 = delta^2 - (x_j[C] -/+ dx/2)^2, t the
+ *                                  outer value, C the axis other than A, B
+ *   inner:  2 axis + side          x_j[axis] -/+ dx/2
+ *           8 + 2 axis + sign      +/- sqrt(delta^2 - t^2 - s^2) (0 where
+ *                                  negative), s the middle value
+ * sign 1 is +.  PD_AI_ASSIGN on a bond's first region: the force is that
+ * region's integral (the reference writes it), else the regions are added to
+ * a sum that starts at 0.0. */
+#define PD_AI_ASSIGN 1
+typedef struct pd_ai_region {
+    double a, b;
+    uint8_t axis[3];
+    uint8_t lim[4];
+    uint8_t flags;
+} pd_ai_region;
+/* The regions of every full-family entry (pd_get_family order; the bond
+ * classification of CalcBondForceIntg and the case analysis of
+ * pdIntgManager::AdaptiveIntegration, pdIntgManager.cpp:523-3482, from the
+ * coordinates coords [N][3]): reg_ptr [entries + 1], regions (NULL to size
+ * the list: *num_regions receives the count; PD_ERR_CAPACITY when capacity is
+ * smaller).  Host only; needs no device. */
+int pd_ai_plan(int64_t num_nodes, const double* coords, const int64_t* row_ptr, const int32_t* col,
+               double grid_spacing, double horizon, int64_t* reg_ptr, pd_ai_region* regions, int64_t capacity,
+               int64_t* num_regions);
+/* The per-node MLS coefficient lists of the AI form (InitIntegrationPoint's
+ * trapezoid pass, pdDataManager2.cpp:257-300, and
+ * pdIntgManager::InitMLSCoeff, pdIntgManager2.cpp:1879-1939): node j's list
+ * holds the coefficients of the trapezoid points of the bonds i -> j in the
+ * order the reference's setup pass visits them, and the force pass reads
+ * entry k for a region's k-th point, whichever bond it integrates.  Only the
+ * entries the force pass can reach are kept: tab_ptr [N+1] (entries per node,
+ * cumulative), tab_coeff [entry][contributor of the node] (NULL to size:
+ * *num_coeff receives the count of doubles).  cb_ptr / cb_idx: the MLS
+ * contributors (pd_get_mls layout); rw the support radius; trap_index 1..3.
+ * PD_ERR_SINGULAR with the node in *bad_node on a singular moment matrix.
+ * Host only. */
+int pd_ai_mls_table(int64_t num_nodes, const double* coords, const int64_t* row_ptr, const int32_t* col,
+                    const int64_t* reg_ptr, const pd_ai_region* regions, double grid_spacing, double horizon,
+                    int trap_index, const int64_t* cb_ptr, const int32_t* cb_idx, double rw, int64_t* tab_ptr,
+                    double* tab_coeff, int64_t capacity, int64_t* num_coeff, int64_t* bad_node);
+/* Upload the AI data to a context created with PD_INTG_AI, after its family:
+ * the regions of every full-family entry (pd_ai_plan layout) and, with
+ * mls = 1, the MLS contributors cb_ptr / cb_idx (pd_get_mls layout) and
+ * tables (pd_ai_mls_table layout).  A new family drops the AI data.  With
+ * mls = 0 every family node carries a displacement-gradient boundary
+ * condition and eta = G xi (pdIntgManager2.cpp:211-235).  With MLS, a family
+ * node with a boundary condition gives its prescribed value in the DISPL /
+ * DISPLGRAD directions it flags; its other directions take the MLS value
+ * (the reference reads an unset local there).
+ * A bond whose point passes the critical stretch is broken from then on for
+ * both of its nodes (pdIntgManager2.cpp:301-308); the FP64 arithmetic only. */
+int pd_set_ai(pd_ctx* ctx, int mls, const int64_t* reg_ptr, const pd_ai_region* regions, const int64_t* cb_ptr,
+              const int32_t* cb_idx, const int64_t* tab_ptr, const double* tab_coeff);
 /* number of MLS contributor entries held (0 without MLS data) */
 int pd_mls_size(pd_ctx* ctx, int64_t* num_contrib);
 

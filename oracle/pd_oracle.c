@@ -646,6 +646,265 @@ static void rk4_step_taped(or_model* m, double dt, double t, double* tape) {
 
 void or_rk4_step(or_model* m, double dt, double t) { rk4_step_taped(m, dt, t, NULL); }
 
+/* ------------------------------------------------------------ AI form -- */
+
+/* pd_ai_region's layout (pdmtel_b200.h) */
+typedef struct {
+    double a, b;
+    uint8_t axis[3];
+    uint8_t lim[4];
+    uint8_t flags;
+} or_ai_region;
+
+typedef struct {
+    or_model* m;
+    int trap;
+    double xj[3];               /* node j in the family coordinates of node i */
+    int64_t i, j;
+    const double* ui;
+    double ecrit, spring, be, t;
+    const double* us;
+    const double* tab;          /* node j's coefficient list */
+    int64_t ncb;
+    const int32_t* cb;
+    const or_ai_region* R;
+    int counter;                /* _intgPointCounter */
+    int failed;
+} ai_state;
+
+/* SolveBinaryQuadric with its centre at the origin (pdIntgManager2.cpp:812-834) */
+static double ai_quadric(double r_sq, double xy) {
+    double v = r_sq - (xy - 0.0) * (xy - 0.0);
+    if (v < 0.0) return -1.0;
+    return sqrt(v);
+}
+
+/* middle-direction limits (pdIntgManager2.cpp:440-617) */
+static double ai_ylimit(const ai_state* s, int code, double x) {
+    const double dx = s->m->dx, delta = s->m->delta;
+    if (code < 8) {
+        int ax = code / 2;
+        return (code % 2) ? s->xj[ax] + 0.5 * dx : s->xj[ax] - 0.5 * dx;
+    }
+    int c = code - 8;
+    int pos = c % 2, high = (c / 2) % 2, solved = (c / 4) / 3, arg = (c / 4) % 3;
+    int third = 3 - solved - arg;
+    double plane = high ? s->xj[third] + 0.5 * dx : s->xj[third] - 0.5 * dx;
+    double v = ai_quadric(delta * delta - plane * plane, x);
+    if (v < 0.0) v = 0.0;
+    return pos ? v : -v;
+}
+
+/* inner-direction limits (pdIntgManager2.cpp:622-682) */
+static double ai_zlimit(const ai_state* s, int code, double x, double y) {
+    const double dx = s->m->dx, delta = s->m->delta;
+    if (code < 8) {
+        int ax = code / 2;
+        return (code % 2) ? s->xj[ax] + 0.5 * dx : s->xj[ax] - 0.5 * dx;
+    }
+    double sq = delta * delta - x * x - y * y;
+    double v = (sq < 0.0) ? 0.0 : sqrt(sq);
+    return (code % 2) ? v : -v;
+}
+
+/* the integrand CalcBondBasedForce (pdIntgManager2.cpp:92-310) at the local
+ * point (x1, x2, x3) */
+static void ai_integrand(ai_state* s, double x1, double x2, double x3, double* f) {
+    or_model* m = s->m;
+    double xi1 = x1 - 0.0, xi2 = x2 - 0.0, xi3 = x3 - 0.0;
+    double eta[3];
+    int b = m->bc[s->j];
+    if (m->mls) {
+        double u[3] = {0.0, 0.0, 0.0};
+        /* the MLS value; a boundary-condition node overrides its prescribed directions */
+        const double* c = s->tab + (int64_t)s->counter * s->ncb;
+        for (int64_t q = 0; q < s->ncb; ++q) {
+            const double* d = s->us + 3 * (int64_t)s->cb[q];
+            u[0] += d[0] * c[q];
+            u[1] += d[1] * c[q];
+            u[2] += d[2] * c[q];
+        }
+        if (b >= 0) {
+            double fac = time_factor(m, b, s->t);
+            const int32_t* dir = m->bc_dir + 3 * b;
+            const double* v = m->bc_val + 9 * b;
+            const double* X = m->x + 3 * s->i;
+            double xg[3] = {x1 + X[0], x2 + X[1], x3 + X[2]};
+            for (int a = 0; a < 3; ++a) {
+                if (dir[a] != 1) continue;
+                if (m->bc_type[b] == OR_DISPL) u[a] = v[a] * fac;
+                else if (m->bc_type[b] == OR_DISPLGRAD)
+                    u[a] = (v[3 * a] * xg[0] + v[3 * a + 1] * xg[1] + v[3 * a + 2] * xg[2]) * fac;
+            }
+        }
+        eta[0] = u[0] - s->ui[0];
+        eta[1] = u[1] - s->ui[1];
+        eta[2] = u[2] - s->ui[2];
+    } else {
+        const double* v = m->bc_val + 9 * b;
+        for (int a = 0; a < 3; ++a) eta[a] = v[3 * a] * xi1 + v[3 * a + 1] * xi2 + v[3 * a + 2] * xi3;
+    }
+    double r = sqrt(xi1 * xi1 + xi2 * xi2 + xi3 * xi3);
+    double y1 = xi1 + eta[0], y2 = xi2 + eta[1], y3 = xi3 + eta[2];
+    double p = sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+    double beta = 1.0;
+    double u = p - r;
+    double stretch = u / r;
+    if (u <= 0.0 || (u > 0.0 && stretch <= s->ecrit)) {
+        f[0] = s->be * beta * s->spring * stretch * (xi1 + eta[0]) / p;
+        f[1] = s->be * beta * s->spring * stretch * (xi2 + eta[1]) / p;
+        f[2] = s->be * beta * s->spring * stretch * (xi3 + eta[2]) / p;
+        m->eed[s->i] += s->be * 0.5 * (0.5 * beta * (s->spring / r) * u * u);
+    } else {
+        f[0] = f[1] = f[2] = 0.0;
+        s->failed += 1;
+    }
+}
+
+static void ai_x1(ai_state* s, double x, double* f);
+static void ai_x2(ai_state* s, double x, double y, double* f);
+
+/* CalcIntgX3 (pdIntgManager.cpp:282-345): the point in x, y, z order */
+static void ai_x3(ai_state* s, double x, double y, double z, double* f) {
+    double p[3];
+    p[s->R->axis[0]] = x;
+    p[s->R->axis[1]] = y;
+    p[s->R->axis[2]] = z;
+    ai_integrand(s, p[0], p[1], p[2], f);
+    ++s->counter;
+}
+
+static void ai_eval(ai_state* s, int level, double v, double x, double y, double* f) {
+    if (level == 1) ai_x1(s, v, f);
+    else if (level == 2) ai_x2(s, x, v, f);
+    else ai_x3(s, x, y, v, f);
+}
+
+/* CalcTrapzdQuad, cases 1-3 (pdIntgManager.cpp:347-451) */
+static void ai_trapz(ai_state* s, int level, double a, double b, double x, double y, double* out) {
+    double f1[3], f2[3], f3[3], f4[3], f5[3];
+    if (s->trap == 1) {
+        ai_eval(s, level, a, x, y, f1);
+        ai_eval(s, level, b, x, y, f2);
+        for (int c = 0; c < 3; ++c) out[c] = (b - a) * (0.5 * f1[c] + 0.5 * f2[c]);
+    } else if (s->trap == 2) {
+        ai_eval(s, level, a, x, y, f1);
+        ai_eval(s, level, 0.5 * (a + b), x, y, f2);
+        ai_eval(s, level, b, x, y, f3);
+        for (int c = 0; c < 3; ++c) out[c] = 0.5 * (b - a) * (0.5 * f1[c] + f2[c] + 0.5 * f3[c]);
+    } else {
+        ai_eval(s, level, a, x, y, f1);
+        ai_eval(s, level, 0.25 * (3.0 * a + b), x, y, f2);
+        ai_eval(s, level, 0.5 * (a + b), x, y, f3);
+        ai_eval(s, level, 0.25 * (a + 3.0 * b), x, y, f4);
+        ai_eval(s, level, b, x, y, f5);
+        for (int c = 0; c < 3; ++c)
+            out[c] = 0.25 * (b - a) * (0.5 * f1[c] + f2[c] + f3[c] + f4[c] + 0.5 * f5[c]);
+    }
+}
+
+/* CalcIntgX1 (pdIntgManager.cpp:130-204) */
+static void ai_x1(ai_state* s, double x, double* f) {
+    double a = ai_ylimit(s, s->R->lim[0], x), b = ai_ylimit(s, s->R->lim[1], x);
+    if (fabs(a - b) <= 1.0e-10) { f[0] = f[1] = f[2] = 0.0; return; }
+    ai_trapz(s, 2, a, b, x, 0.0, f);
+}
+
+/* CalcIntgX2 (pdIntgManager.cpp:206-280) */
+static void ai_x2(ai_state* s, double x, double y, double* f) {
+    double a = ai_zlimit(s, s->R->lim[2], x, y), b = ai_zlimit(s, s->R->lim[3], x, y);
+    if (fabs(a - b) <= 1.0e-10) { f[0] = f[1] = f[2] = 0.0; return; }
+    ai_trapz(s, 3, a, b, x, y, f);
+}
+
+/* CalcIntg3D (pdIntgManager.cpp:49-128) over one region */
+static void ai_region3d(ai_state* s, const or_ai_region* R, double* f) {
+    s->R = R;
+    s->counter = 0;
+    if (fabs(R->a - R->b) <= 1.0e-10) { f[0] = f[1] = f[2] = 0.0; return; }
+    ai_trapz(s, 1, R->a, R->b, 0.0, 0.0, f);
+}
+
+static int64_t ai_entry(const or_model* m, int64_t i, int64_t j) {
+    int64_t lo = m->fam_ptr[i], hi = m->fam_ptr[i + 1];
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (m->fam_col[mid] < j) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < m->fam_ptr[i + 1] && m->fam_col[lo] == j) ? lo : -1;
+}
+
+void or_ai_force_stage(or_model* m, int trap, const int64_t* reg_ptr, const void* regs, const int64_t* tab_ptr,
+                       const double* tab_coeff, uint8_t* ai_broken, int32_t* dmg, double dts, double t,
+                       const double* us, double* k) {
+    const or_ai_region* RG = (const or_ai_region*)regs;
+    for (int64_t i = 0; i < m->n; ++i) {
+        int mi = m->mat[i];
+        double rho = m->mat_density[mi];
+        double body[3] = {m->mat_grav[3 * mi] * rho, m->mat_grav[3 * mi + 1] * rho, m->mat_grav[3 * mi + 2] * rho};
+        const double* ui = (m->bc[i] >= 0) ? m->U + 3 * i : us + 3 * i;
+        for (int64_t p = m->fam_ptr[i]; p < m->fam_ptr[i + 1]; ++p) {
+            if (ai_broken[p]) continue;
+            int64_t j = m->fam_col[p];
+            int mj = m->mat[j];
+            ai_state s;
+            memset(&s, 0, sizeof(s));
+            s.m = m;
+            s.trap = trap;
+            for (int a = 0; a < 3; ++a) s.xj[a] = m->x[3 * j + a] - m->x[3 * i + a];
+            s.i = i;
+            s.j = j;
+            s.ui = ui;
+            s.ecrit = (m->mat_ecrit[mj] < m->mat_ecrit[mi]) ? m->mat_ecrit[mj] : m->mat_ecrit[mi];
+            s.spring = pair_spring(m, i, j);
+            s.be = 0.5 * (m->bdry_eff[i] + m->bdry_eff[j]);
+            s.t = t;
+            s.us = us;
+            if (m->mls) {
+                s.ncb = m->cb_ptr[j + 1] - m->cb_ptr[j];
+                s.cb = m->cb_idx + m->cb_ptr[j];
+                int64_t off = 0;
+                for (int64_t q = 0; q < j; ++q) off += (tab_ptr[q + 1] - tab_ptr[q]) * (m->cb_ptr[q + 1] - m->cb_ptr[q]);
+                s.tab = tab_coeff + off;
+            }
+            double F[3] = {0.0, 0.0, 0.0};
+            int64_t r0 = reg_ptr[p], r1 = reg_ptr[p + 1];
+            if (r1 > r0 && (RG[r0].flags & 1)) {
+                ai_region3d(&s, &RG[r0], F);
+            } else {
+                for (int64_t r = r0; r < r1; ++r) {
+                    double st[3];
+                    ai_region3d(&s, &RG[r], st);
+                    F[0] += st[0];
+                    F[1] += st[1];
+                    F[2] += st[2];
+                }
+            }
+            if (s.failed) {
+                int64_t q = ai_entry(m, j, i);
+                ai_broken[p] = 1;
+                if (q >= 0) ai_broken[q] = 1;
+                dmg[i] += s.failed;
+            }
+            m->vbuf[3 * i + 0] += (F[0] + body[0]) * dts / rho;
+            m->vbuf[3 * i + 1] += (F[1] + body[1]) * dts / rho;
+            m->vbuf[3 * i + 2] += (F[2] + body[2]) * dts / rho;
+        }
+        int b = m->bc[i];
+        if (b >= 0 && m->bc_type[b] == OR_TRACTION) {
+            double fac = time_factor(m, b, t);
+            for (int a = 0; a < 3; ++a)
+                if (m->bc_dir[3 * b + a] == 1) {
+                    double tb = m->bc_val[9 * b + a] * fac / m->dx;
+                    m->vbuf[3 * i + a] += tb * dts / rho;
+                }
+        }
+    }
+    update_node_bc(m, t);
+    for (int64_t i = 0; i < 3 * m->n; ++i) k[i] = m->vbuf[i] * dts;
+}
+
 /* ------------------------------------------------------------ adjoint -- */
 
 /* Project rule, no counterpart in the reference: reverse accumulation of

@@ -106,6 +106,25 @@ void or_force_stage(or_model* m, double dts, double t, const double* us, double*
 /* pdDataManager2.cpp:410-439 + pdDataManager.cpp:1994-2134. */
 void or_rk4_step(or_model* m, double dt, double t);
 
+/* Adaptive-trapezoid (AI) force stage: the ai_on branch of
+ * CalcBondBasedMotionRK4 (pdDataManager.cpp:1886-1915) with
+ * CalcBondForceIntg (pdDataManager2.cpp:1227-1291) and the nested trapezoid
+ * rule of pdIntgManager (pdIntgManager.cpp:49-451; integrand
+ * pdIntgManager2.cpp:92-310), node by node in the reference's order.  The
+ * regions of every family entry come from reg_ptr / regs (the layout of
+ * pd_ai_plan: 24 bytes per region, a, b, axis[3], lim[4], flags); with
+ * m->mls the displacement of a region's k-th point is the MLS sum over node
+ * j's contributors with coefficient list entry k (tab_ptr [n+1] entries,
+ * tab_coeff [entry][contributor]); a boundary-condition node j gives its
+ * prescribed value in flagged DISPL / DISPLGRAD directions.  Without MLS
+ * every family node carries a displacement gradient G and eta = G xi.  A
+ * point past the critical stretch gives no force, breaks the bond for both
+ * nodes (ai_broken [entries], updated in place) and adds 1 to dmg [n].
+ * k [3n] out, as or_force_stage. */
+void or_ai_force_stage(or_model* m, int trap, const int64_t* reg_ptr, const void* regs, const int64_t* tab_ptr,
+                       const double* tab_coeff, uint8_t* ai_broken, int32_t* dmg, double dts, double t,
+                       const double* us, double* k);
+
 /* pdSolve.cpp:195-527 restated as an operator on the 3n system: free rows
  * sum c*V_j*xi xi^T/r^3 (x_i - x_j) over unbroken family members, with
  * prescribed columns masked; prescribed rows are identity. */

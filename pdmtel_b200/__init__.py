@@ -34,6 +34,7 @@ OPT_FORCE_TILE, OPT_FORCE_QUAD, OPT_PERSIST_WAIT_US, OPT_PERSIST_TEST_STALL = 8,
 OPT_GATHER_SELL, OPT_FORCE_STENCIL, OPT_GATHER_STENCIL, OPT_STATIC_PRECOND = 12, 13, 14, 15
 OPT_STATIC_SPLIT, OPT_STATIC_F32_BELOW, OPT_ADJOINT_VJP32 = 16, 17, 18
 BC_DISPL, BC_VELOC, BC_DISPLGRAD, BC_TRACTION = 1, 2, 3, 4
+INTG_CCI, INTG_FGI, INTG_AI = 0, 1, 2
 _ERRS = {-1: "PD_ERR_ARG", -2: "PD_ERR_OOM", -3: "PD_ERR_CUDA", -4: "PD_ERR_TIMEOUT", -5: "PD_ERR_SINGULAR",
          -6: "PD_ERR_CAPACITY", -7: "PD_ERR_NOCONV", -8: "PD_ERR_NODEV"}
 
@@ -53,6 +54,11 @@ _vp = C.c_void_p
 
 class pd_material(C.Structure):
     _fields_ = [("spring", C.c_double), ("density", C.c_double), ("ecrit", C.c_double), ("grav", C.c_double * 3)]
+
+
+class pd_ai_region(C.Structure):
+    _fields_ = [("a", C.c_double), ("b", C.c_double), ("axis", C.c_uint8 * 3), ("lim", C.c_uint8 * 4),
+                ("flags", C.c_uint8)]
 
 
 class pd_bc(C.Structure):
@@ -158,6 +164,11 @@ _SIGS = {
     "pdh_get_tables": [_vp, C.POINTER(pd_material), C.POINTER(pd_bc), _d, _d],
     "pd_rk4_steps_persistent": [_vp, C.c_double, C.c_double, C.c_int],
     "pd_set_boxes": [_vp, C.c_int, _i64],
+    "pd_ai_plan": [C.c_int64, _d, _i64, _i32, C.c_double, C.c_double, _i64, C.POINTER(pd_ai_region), C.c_int64,
+                   _i64],
+    "pd_ai_mls_table": [C.c_int64, _d, _i64, _i32, _i64, C.POINTER(pd_ai_region), C.c_double, C.c_double, C.c_int,
+                        _i64, _i32, C.c_double, _i64, _d, C.c_int64, _i64, _i64],
+    "pd_set_ai": [_vp, C.c_int, _i64, C.POINTER(pd_ai_region), _i64, _i32, _i64, _d],
     "pd_autotune": [_vp, C.c_double, C.c_int, C.POINTER(pd_tune_result)],
 }
 
@@ -202,6 +213,42 @@ def device_count() -> int:
     n = C.c_int(0)
     lib().pd_device_count(C.byref(n))
     return n.value
+
+
+def ai_plan(coords, row_ptr, col, grid_spacing, horizon):
+    """Regions of every family entry of the adaptive-trapezoid form
+    (pd_ai_plan; host only): (reg_ptr [entries + 1], regions array)."""
+    x = _f64(coords)
+    n = x.size // 3
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    ptr = np.zeros(int(rp[-1]) + 1, np.int64)
+    cnt = C.c_int64(0)
+    args = (n, _p(x, _d), _p(rp, _i64), _p(cl, _i32), float(grid_spacing), float(horizon), _p(ptr, _i64))
+    _check(lib().pd_ai_plan(*args, None, 0, C.byref(cnt)), "pd_ai_plan")
+    regs = (pd_ai_region * max(cnt.value, 1))()
+    _check(lib().pd_ai_plan(*args, regs, cnt.value, C.byref(cnt)), "pd_ai_plan")
+    return ptr, regs
+
+
+def ai_mls_table(coords, row_ptr, col, reg_ptr, regions, grid_spacing, horizon, trap_index, cb_ptr, cb_idx, rw):
+    """The per-node MLS coefficient lists of the adaptive-trapezoid form
+    (pd_ai_mls_table; host only): (tab_ptr [n + 1], tab_coeff)."""
+    x = _f64(coords)
+    n = x.size // 3
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    gp = np.ascontiguousarray(reg_ptr, dtype=np.int64)
+    cp = np.ascontiguousarray(cb_ptr, dtype=np.int64)
+    ci = np.ascontiguousarray(cb_idx, dtype=np.int32)
+    tp = np.zeros(n + 1, np.int64)
+    cnt, bad = C.c_int64(0), C.c_int64(-1)
+    head = (n, _p(x, _d), _p(rp, _i64), _p(cl, _i32), _p(gp, _i64), regions, float(grid_spacing), float(horizon),
+            int(trap_index), _p(cp, _i64), _p(ci, _i32), float(rw), _p(tp, _i64))
+    _check(lib().pd_ai_mls_table(*head, None, 0, C.byref(cnt), C.byref(bad)), "pd_ai_mls_table")
+    co = np.zeros(max(cnt.value, 1))
+    _check(lib().pd_ai_mls_table(*head, _p(co, _d), cnt.value, C.byref(cnt), C.byref(bad)), "pd_ai_mls_table")
+    return tp, co[:cnt.value]
 
 
 def _f64(a, n=None):
@@ -318,6 +365,17 @@ class DeviceContext:
     def set_bdry_eff(self, bE):
         b = _f64(bE, self.n)
         _check(lib().pd_set_bdry_eff(self.h, _p(b, _d)), "pd_set_bdry_eff")
+
+    def set_ai(self, reg_ptr, regions, cb_ptr=None, cb_idx=None, tab_ptr=None, tab_coeff=None):
+        """pd_set_ai: MLS on when the contributors and tables are given"""
+        gp = np.ascontiguousarray(reg_ptr, dtype=np.int64)
+        mls = cb_ptr is not None
+        cp = np.ascontiguousarray(cb_ptr, dtype=np.int64) if mls else None
+        ci = np.ascontiguousarray(cb_idx, dtype=np.int32) if mls else None
+        tp = np.ascontiguousarray(tab_ptr, dtype=np.int64) if mls else None
+        tc = _f64(tab_coeff) if mls else None
+        _check(lib().pd_set_ai(self.h, int(mls), _p(gp, _i64), regions, _p(cp, _i64), _p(ci, _i32), _p(tp, _i64),
+                               _p(tc, _d)), "pd_set_ai")
 
     def set_mls(self, cb_ptr, cb_idx, coeff):
         cp = np.ascontiguousarray(cb_ptr, dtype=np.int64)

@@ -31,12 +31,14 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
 
 CUDA_UNITS = {
     "pd_exact.cu": ["-fmad=false"],
+    "pd_ai.cu": ["-fmad=false"],
     "pd_f32c.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "pd_fast.cu": [],
     "pd_capi.cu": [],
     "pd_adjoint.cu": [],
 }
-HOST_UNITS = ["host/pd_deck.cpp", "host/pd_setup.cpp", "host/pdDataManager.cpp", "host/pd_host_capi.cpp"]
+HOST_UNITS = ["host/pd_deck.cpp", "host/pd_setup.cpp", "host/pd_ai_plan.cpp", "host/pdDataManager.cpp",
+              "host/pd_host_capi.cpp"]
 
 
 def _newer(src_list, out):

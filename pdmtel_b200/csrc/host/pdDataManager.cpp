@@ -245,17 +245,43 @@ int pdDataManager::ReadInputFile() {
         PDH_TRY(req("fgi_on"));
         PDH_TRY(rd("fgi_on", 1, _fgiOn));
         _cciMdf = false;
-        if (!_fgiOn) return Error(PD_ERR_ARG, "ReadInputFile: adaptive integration (ai_on) is not supported");
-        _intgPoint = 3;
-        if (D.Find("intg_point")) PDH_TRY(rd("intg_point", 1, _intgPoint));
-        _mlsOn = _intgPoint != 1;
-        _rw = 3.0 * _gridSpacing;
-        if (D.Find("support_domain_size")) PDH_TRY(rd("support_domain_size", 1, _rw));
-        if (_intgPoint < 1 || _intgPoint > 8 || _intgPoint == 7)
-            return Error(PD_ERR_ARG, "ReadInputFile: intg_point must be 1-6 or 8");
+        if (_fgiOn) {
+            _intgPoint = 3;
+            if (D.Find("intg_point")) PDH_TRY(rd("intg_point", 1, _intgPoint));
+            _mlsOn = _intgPoint != 1;
+            _rw = 3.0 * _gridSpacing;
+            if (D.Find("support_domain_size")) PDH_TRY(rd("support_domain_size", 1, _rw));
+            if (_intgPoint < 1 || _intgPoint > 8 || _intgPoint == 7)
+                return Error(PD_ERR_ARG, "ReadInputFile: intg_point must be 1-6 or 8");
+        } else {
+            // adaptive trapezoid integration, pdDataManager.cpp:656-717
+            PDH_TRY(req("ai_on"));
+            PDH_TRY(rd("ai_on", 1, _aiOn));
+            if (!_aiOn) return Error(PD_ERR_ARG, "ReadInputFile: no integration method is used! ");
+            PDH_TRY(rd("ai_on", 2, _mlsOn));
+            _rw = 3.0 * _gridSpacing;
+            if (D.Find("support_domain_size")) PDH_TRY(rd("support_domain_size", 1, _rw));
+            _intgPoint = 3;
+            if (D.Find("intg_point")) PDH_TRY(rd("intg_point", 1, _intgPoint));
+            _errorControlOn = false;
+            _eps = 0.0;
+            if (D.Find("error_control_on")) {
+                PDH_TRY(rd("error_control_on", 1, _errorControlOn));
+                if (_errorControlOn) {
+                    _eps = 0.01;
+                    if (D.Find("error_control_eps")) PDH_TRY(rd("error_control_eps", 1, _eps));
+                }
+            }
+            if (_errorControlOn)
+                return Error(PD_ERR_ARG, "ReadInputFile: error_control_on is not supported: the refinement reads MLS "
+                                         "list entries the setup pass never filled (pdIntgManager2.cpp:174)");
+            if (_intgPoint < 1 || _intgPoint > 3)
+                return Error(PD_ERR_ARG, "ReadInputFile: the AI trapezoid index (intg_point) must be 1-3: above 3 "
+                                         "the reference's rule refines a sum left by the previous integral");
+        }
     }
 #undef PDH_TRY
-    const int n1 = _cciOn ? 1 : _intgPoint;
+    const int n1 = (_cciOn || _aiOn) ? 1 : _intgPoint;
     _npt = n1 * n1 * n1;
     gauss_rule(n1, _abscis, _weights);
     EchoDeck(log, hasDelKeyword);
@@ -341,7 +367,13 @@ void pdDataManager::EchoDeck(std::ostream& log, bool deletion_keyword) const {
         log << "\nReadInputFile: Starting Gaussian points = " << _intgPoint << "\n";
         log << "\nReadInputFile: Moving least square flag = " << _mlsOn << "\n";
     }
-    log << "\nReadInputFile: Adaptive integration method flag = " << 0 << "\n";
+    log << "\nReadInputFile: Adaptive integration method flag = " << _aiOn << "\n";
+    if (_aiOn) {
+        log << "\nReadInputFile: Moving least square flag = " << _mlsOn << "\n";
+        log << "\nReadInputFile: Error control method flag = " << _errorControlOn << "\n";
+        log << "\nReadInputFile: Error control accuracy = " << _eps << "\n";
+        log << "\nReadInputFile: Starting trapezoidal index = " << _intgPoint << "\n";
+    }
 }
 
 // pdDataManager::InitNode, pdDataManager.cpp:813-1098
@@ -429,7 +461,7 @@ int pdDataManager::EnsureContext() {
     P.bcs = bcs.empty() ? nullptr : bcs.data();
     P.grid_spacing = _gridSpacing;
     P.horizon = _horizon;
-    P.integration = _cciOn ? PD_INTG_CCI : PD_INTG_FGI;
+    P.integration = _cciOn ? PD_INTG_CCI : (_aiOn ? PD_INTG_AI : PD_INTG_FGI);
     P.cci_modified = _cciMdf ? 1 : 0;
     P.intg_point = _cciOn ? 1 : _intgPoint;
     P.abscissae = _abscis.data();
@@ -638,7 +670,55 @@ int pdDataManager::InitIntegrationPoint() {
     return rc;
 }
 
+// The adaptive-trapezoid form: the regions of every bond, and with MLS the
+// contributors and the per-node coefficient lists of the trapezoid points
+// (pdDataManager2.cpp:257-300), all on the host.
+int pdDataManager::SetupAI() {
+    if (!_bondsDone) return Error(PD_ERR_ARG, "InitIntegrationPoint: bonds first");
+    const int64_t H = _famPtr.empty() ? 0 : _famPtr.back();
+    int64_t R = 0;
+    _aiRegPtr.assign(H + 1, 0);
+    int rc = pd_ai_plan(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _gridSpacing, _horizon,
+                        _aiRegPtr.data(), nullptr, 0, &R);
+    if (rc != PD_OK) return Error(rc, "pd_ai_plan: bad family");
+    _aiRegs.resize(std::max<int64_t>(R, 1));
+    rc = pd_ai_plan(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _gridSpacing, _horizon, _aiRegPtr.data(),
+                    _aiRegs.data(), R, &R);
+    if (rc != PD_OK) return Error(rc, "pd_ai_plan");
+    _aiTabPtr.clear();
+    _aiTab.clear();
+    if (_mlsOn) {
+        mls_contributors(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _rw, _cbPtr, _cbIdx);
+        _aiTabPtr.assign(_numNodes + 1, 0);
+        int64_t nc = 0, bad = -1;
+        rc = pd_ai_mls_table(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _aiRegPtr.data(), _aiRegs.data(),
+                             _gridSpacing, _horizon, _intgPoint, _cbPtr.data(), _cbIdx.data(), _rw, _aiTabPtr.data(),
+                             nullptr, 0, &nc, &bad);
+        if (rc != PD_OK) return Error(rc, "pd_ai_mls_table");
+        _aiTab.assign(std::max<int64_t>(nc, 1), 0.0);
+        rc = pd_ai_mls_table(_numNodes, _x.data(), _famPtr.data(), _famCol.data(), _aiRegPtr.data(), _aiRegs.data(),
+                             _gridSpacing, _horizon, _intgPoint, _cbPtr.data(), _cbIdx.data(), _rw, _aiTabPtr.data(),
+                             _aiTab.data(), nc, &nc, &bad);
+        if (rc == PD_ERR_SINGULAR) {
+            std::ostringstream o;
+            o << "pdMatrix::Gauss: Singular Matrix (MLS moment matrix of node " << bad << ")";
+            return Error(rc, o.str());
+        }
+        if (rc != PD_OK) return Error(rc, "pd_ai_mls_table");
+    }
+    if (_ctx && _familyOnDevice) return UploadAI();
+    return PD_OK;
+}
+
+int pdDataManager::UploadAI() {
+    const bool m = _mlsOn;
+    const int rc = pd_set_ai(_ctx, m ? 1 : 0, _aiRegPtr.data(), _aiRegs.data(), m ? _cbPtr.data() : nullptr,
+                             m ? _cbIdx.data() : nullptr, m ? _aiTabPtr.data() : nullptr, m ? _aiTab.data() : nullptr);
+    return rc == PD_OK ? PD_OK : Cuda(rc, "pd_set_ai");
+}
+
 int pdDataManager::SetupIntegrationPoints() {
+    if (_aiOn) return SetupAI();
     if (!_mlsOn) return PD_OK;
     if (!_bondsDone) return Error(PD_ERR_ARG, "InitIntegrationPoint: bonds first");
     int64_t bad = -1;
@@ -715,7 +795,10 @@ int pdDataManager::UploadSetup() {
         _familyOnDevice = true;
     }
     if ((rc = pd_set_bdry_eff(_ctx, _bdryEff.data())) != PD_OK) return Cuda(rc, "pd_set_bdry_eff");
-    if (_mlsOn && !_mlsOnDevice) {
+    if (_aiOn) {
+        if (_aiRegPtr.empty()) return Error(PD_ERR_ARG, "no AI data: InitIntegrationPoint first");
+        if ((rc = UploadAI()) != PD_OK) return rc;
+    } else if (_mlsOn && !_mlsOnDevice) {
         if (_cbPtr.empty()) return Error(PD_ERR_ARG, "no MLS data: InitIntegrationPoint first");
         if ((rc = pd_set_mls(_ctx, _cbPtr.data(), _cbIdx.data(), _coeff.data())) != PD_OK) return Cuda(rc, "pd_set_mls");
     }
@@ -1061,6 +1144,7 @@ int pdDataManager::InitBatch(const std::vector<pdDataManager*>& sp) {
         if (!m->_nodesDone && (rc = m->InitNode()) != PD_OK) return Error(rc, "InitBatch: specimen: " + m->_err);
         if (!m->_matDone && (rc = m->InitMaterial()) != PD_OK) return Error(rc, "InitBatch: specimen: " + m->_err);
         const pdDataManager& f = *sp[0];
+        if (m->_aiOn) return Error(PD_ERR_ARG, "InitBatch: the batching form runs the Gauss-point and CCI schemes");
         if (m->_gridSpacing != f._gridSpacing || m->_horizon != f._horizon || m->_cciOn != f._cciOn ||
             m->_cciMdf != f._cciMdf || m->_fgiOn != f._fgiOn || m->_mlsOn != f._mlsOn ||
             m->_intgPoint != f._intgPoint || m->_rw != f._rw || m->_dampCoeff != f._dampCoeff)

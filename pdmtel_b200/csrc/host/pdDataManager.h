@@ -160,6 +160,8 @@ private:
     int BatchMLS(int64_t* bad_node);
     void EchoDeck(std::ostream& log, bool deletion_keyword) const;
     int SetupIntegrationPoints();
+    int SetupAI();
+    int UploadAI();
 
     std::string _workDir, _inFilePath, _outFilePath, _title, _err;
     std::vector<std::string> _deck;  // lines, trimmed
@@ -171,7 +173,12 @@ private:
     double _forcePlane[3] = {0, 0, 0};
     int _totalStep = 0, _stepDumpFrequency = 1, _intgPoint = 0, _npt = 1;
     bool _fixedTimeStepOn = false, _bdryEffOn = false, _cciOn = false, _cciMdf = false, _fgiOn = false,
-         _mlsOn = false;
+         _mlsOn = false, _aiOn = false, _errorControlOn = false;
+    double _eps = 0;
+    // adaptive-trapezoid form: regions of every family entry, MLS tables
+    std::vector<int64_t> _aiRegPtr, _aiTabPtr;
+    std::vector<pd_ai_region> _aiRegs;
+    std::vector<double> _aiTab;
     std::vector<Material> _mats;
     std::vector<BdryCondition> _bcs;
     std::vector<Space> _matSpaces, _delSpaces, _bdrySpaces;
@@ -245,6 +252,8 @@ int mls_contributors(int64_t n, const double* x, const int64_t* row_ptr, const i
 int mls_coefficients(int64_t n, const double* x, const double* abscis, int n1, double dx,
                      const std::vector<int64_t>& cb_ptr, const std::vector<int32_t>& cb_idx, double rw,
                      std::vector<double>& coeff, int nthreads, int64_t* bad_node);
+bool mls_point(const double* x, const int32_t* cb, int64_t nc, const double q[3], double rw, double* pw,
+               double* out);
 void gauss_rule(int n, std::vector<double>& abscis, std::vector<double>& weights);
 void cube_distance(const double* pi, const double* pj, double dx, double* dmin, double* dmax);
 double beta_factor(double dist, double delta, double dx, bool cci_original);

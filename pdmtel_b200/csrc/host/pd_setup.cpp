@@ -259,6 +259,33 @@ bool solve10(double A[10][10], double rhs[10]) {
 
 }  // namespace
 
+// MLS coefficients of node contributors cb [nc] at the global point q
+// (pdDataManager2.cpp:173-256, pdIntgManager2.cpp:1879-1939): moment matrix
+// sum_k w_k p_k p_k^T, solved against p(q), coefficient k = (w_k p_k) . sol.
+// pw: scratch of 11 nc doubles.  False on a singular moment matrix.
+bool mls_point(const double* x, const int32_t* cb, int64_t nc, const double q[3], double rw, double* pw,
+               double* out) {
+    double A[10][10] = {};
+    for (int64_t k = 0; k < nc; ++k) {
+        const double* node = x + 3 * (int64_t)cb[k];
+        double* e = pw + 11 * k;
+        basis(node, e);
+        e[10] = spline_weight(node, q, rw);
+        for (int r = 0; r < 10; ++r)
+            for (int cc = 0; cc < 10; ++cc) A[r][cc] = A[r][cc] + e[10] * e[r] * e[cc];
+    }
+    double s[10];
+    basis(q, s);
+    if (!solve10(A, s)) return false;
+    for (int64_t k = 0; k < nc; ++k) {
+        const double* e = pw + 11 * k;
+        double sum = 0.0;
+        for (int r = 0; r < 10; ++r) sum += (e[r] * e[10]) * s[r];
+        out[k] = sum;
+    }
+    return true;
+}
+
 // MLS shape coefficients of every Gauss point, pdDataManager2.cpp:173-256.
 // Output per node: npt blocks of ncb values (the point's coefficient vector).
 int mls_coefficients(int64_t n, const double* x, const double* abscis, int n1, double dx,
@@ -280,28 +307,11 @@ int mls_coefficients(int64_t n, const double* x, const double* abscis, int n1, d
                     const int gi = g / (n1 * n1), gj = (g / n1) % n1, gk = g % n1;
                     const double q[3] = {0.5 * dx * abscis[gi] + x[3 * i], 0.5 * dx * abscis[gj] + x[3 * i + 1],
                                          0.5 * dx * abscis[gk] + x[3 * i + 2]};
-                    double A[10][10] = {};
-                    for (int64_t k = 0; k < nc; ++k) {
-                        const double* node = x + 3 * (int64_t)cb_idx[b + k];
-                        double* e = pw.data() + 11 * k;
-                        basis(node, e);
-                        e[10] = spline_weight(node, q, rw);
-                        for (int r = 0; r < 10; ++r)
-                            for (int cc = 0; cc < 10; ++cc) A[r][cc] = A[r][cc] + e[10] * e[r] * e[cc];
-                    }
-                    double s[10];
-                    basis(q, s);
-                    if (!solve10(A, s)) {
+                    double* out = coeff.data() + b * npt + (int64_t)g * nc;
+                    if (!mls_point(x, cb_idx.data() + b, nc, q, rw, pw.data(), out)) {
                         int64_t exp = -1;
                         bad.compare_exchange_strong(exp, i);
                         return;
-                    }
-                    double* out = coeff.data() + b * npt + (int64_t)g * nc;
-                    for (int64_t k = 0; k < nc; ++k) {
-                        const double* e = pw.data() + 11 * k;
-                        double sum = 0.0;
-                        for (int r = 0; r < 10; ++r) sum += (e[r] * e[10]) * s[r];
-                        out[k] = sum;
                     }
                 }
             }

@@ -1,0 +1,246 @@
+// Adaptive-trapezoid (AI) form on the device: the ai_on branch of
+// CalcBondBasedMotionRK4 (pdDataManager.cpp:1886-1915) with
+// CalcBondForceIntg (pdDataManager2.cpp:1227-1291) and the integrand
+// pdIntgManager::CalcBondBasedForce (pdIntgManager2.cpp:92-310).
+//
+// Compiled with -fmad=false: the nested trapezoid sums (pd_ai_eval.h), the
+// MLS sums and the force are rounded operation by operation in the
+// reference's order, so the stage's velocity buffer is the reference's bit
+// for bit.
+//
+// One stage is three launches:
+//  k_ai_gather  one thread per MLS table entry: the displacement of the
+//               entry's point from the trial displacements (the reference
+//               forms it point by point inside the integrand; the sum is the
+//               same, so it is formed once per entry here and read by every
+//               bond to the node);
+//  k_ai_bond    one thread per full-family entry i -> j: the bond's force and
+//               the count of its points past the critical stretch;
+//  k_ai_sum     one thread per node: the velocity update bond by bond in
+//               family order.  A failing point breaks the bond object the two
+//               nodes share (pdIntgManager2.cpp:301-308), and the reference
+//               visits node i's bonds after those of every lower node: a bond
+//               to a lower node j is skipped when j's evaluation of it failed
+//               in this stage.  Breaks are committed here for the next stage.
+#include <cfloat>
+#include <cmath>
+
+#include "pd_ai_eval.h"
+#include "pd_internal.cuh"
+#include "pd_stage.cuh"
+
+namespace pd {
+
+namespace {
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+
+__global__ void k_ai_gather(Dev d, const double* __restrict__ us) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= d.ai_ntab) return;
+    const int64_t N = d.n;
+    const int64_t j = d.ai_tnode[e];
+    const int64_t k = e - d.ai_tptr[j];
+    const int64_t c0 = d.cbptr[j], nc = d.cbptr[j + 1] - c0;
+    const double* cf = d.ai_tcoef + d.ai_coff[j] + k * nc;
+    const int32_t* cb = d.cbidx + c0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int64_t q = 0; q < nc; ++q) {
+        const int64_t m = cb[q];
+        const double c = cf[q];
+        a0 += us[m] * c;
+        a1 += us[N + m] * c;
+        a2 += us[2 * N + m] * c;
+    }
+    d.ai_u[3 * e] = a0;
+    d.ai_u[3 * e + 1] = a1;
+    d.ai_u[3 * e + 2] = a2;
+}
+
+// the integrand at one trapezoid point of bond i -> j
+struct ForceFn {
+    const Dev* d;
+    double ui[3];
+    double xi[3];        // node i (global): a DISPLGRAD point sits at local + x_i
+    double ecrit, c, be;
+    const double* tab;   // node j's table entries [K][3]
+    int64_t K;
+    const BcDev* B;      // node j's boundary condition or null
+    double fac;
+    int fail;
+    double eacc;
+    bool energy;
+
+    __device__ void operator()(const double* p, int k, double* f) {
+        double eta[3];
+        if (d->ai_mls) {
+            double u[3];
+            if (k < K) {
+                u[0] = tab[3 * k];
+                u[1] = tab[3 * k + 1];
+                u[2] = tab[3 * k + 2];
+            } else {
+                u[0] = u[1] = u[2] = 0.0;
+                *d->ai_err = 1;
+            }
+            if (B) {
+                for (int a = 0; a < 3; ++a) {
+                    if (B->dir[a] != 1) continue;
+                    if (B->type == PD_BC_DISPL) {
+                        u[a] = B->val[a] * fac;
+                    } else if (B->type == PD_BC_DISPLGRAD) {
+                        const double g0 = p[0] + xi[0], g1 = p[1] + xi[1], g2 = p[2] + xi[2];
+                        u[a] = (B->val[3 * a] * g0 + B->val[3 * a + 1] * g1 + B->val[3 * a + 2] * g2) * fac;
+                    }
+                }
+            }
+            eta[0] = u[0] - ui[0];
+            eta[1] = u[1] - ui[1];
+            eta[2] = u[2] - ui[2];
+        } else {
+            // every family node carries a displacement gradient (checked at upload)
+            for (int a = 0; a < 3; ++a)
+                eta[a] = B->val[3 * a] * (p[0] - 0.0) + B->val[3 * a + 1] * (p[1] - 0.0) +
+                         B->val[3 * a + 2] * (p[2] - 0.0);
+        }
+        const double x0 = p[0] - 0.0, x1 = p[1] - 0.0, x2 = p[2] - 0.0;
+        const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+        const double y0 = x0 + eta[0], y1 = x1 + eta[1], y2 = x2 + eta[2];
+        const double pl = sqrt(y0 * y0 + y1 * y1 + y2 * y2);
+        const double u = pl - r;
+        const double s = u / r;
+        if (u <= 0.0 || (u > 0.0 && s <= ecrit)) {
+            const double t = be * 1.0 * c * s;
+            f[0] = t * y0 / pl;
+            f[1] = t * y1 / pl;
+            f[2] = t * y2 / pl;
+            if (energy) eacc += be * 0.5 * (0.5 * 1.0 * (c / r) * u * u);
+        } else {
+            f[0] = f[1] = f[2] = 0.0;
+            ++fail;
+        }
+    }
+};
+
+__device__ __noinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, int64_t j, const double* ui, double t, bool energy,
+                          double F[3], int* fail, double* eacc) {
+    const int64_t N = d.n;
+    const MatDev& Mi = d.mats[d.mat[i]];
+    const MatDev& Mj = d.mats[d.mat[j]];
+    ForceFn fn;
+    fn.d = &d;
+    for (int a = 0; a < 3; ++a) fn.ui[a] = ui[a];
+    fn.xi[0] = d.x[i];
+    fn.xi[1] = d.x[N + i];
+    fn.xi[2] = d.x[2 * N + i];
+    fn.ecrit = dmin(Mi.ecrit, Mj.ecrit);
+    fn.c = dmin(Mi.spring, Mj.spring);
+    if (d.sfac) fn.c = fn.c * (0.5 * (d.sfac[i] + d.sfac[j]));
+    fn.be = 0.5 * (d.bdry[i] + d.bdry[j]);
+    const int b = d.bc[j];
+    fn.B = b >= 0 ? &d.bcs[b] : nullptr;
+    fn.fac = b >= 0 ? bc_time_factor(d.bcs[b], t) : 0.0;
+    if (d.ai_mls) {
+        fn.tab = d.ai_u + 3 * d.ai_tptr[j];
+        fn.K = d.ai_tptr[j + 1] - d.ai_tptr[j];
+    } else {
+        fn.tab = nullptr;
+        fn.K = 0;
+    }
+    fn.fail = 0;
+    fn.eacc = energy ? *eacc : 0.0;
+    fn.energy = energy;
+    const double xj[3] = {d.x[j] - d.x[i], d.x[N + j] - d.x[N + i], d.x[2 * N + j] - d.x[2 * N + i]};
+    pd_ai::bond(d.ai_reg, d.ai_rptr[p], d.ai_rptr[p + 1], d.ai_n, xj, d.delta, d.dx, fn, F);
+    *fail = fn.fail;
+    if (energy) *eacc = fn.eacc;
+}
+
+__device__ __forceinline__ void node_u(const Dev& d, int64_t i, double* u) {
+    const int64_t N = d.n;
+    const double* src = d.bc[i] >= 0 ? d.U : d.us;
+    u[0] = src[i];
+    u[1] = src[N + i];
+    u[2] = src[2 * N + i];
+}
+
+__global__ void __launch_bounds__(128) k_ai_bond(Dev d) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= d.ai_nent) return;
+    if (d.ai_brk[p]) {
+        d.ai_fail[p] = 0;
+        return;
+    }
+    const int64_t i = d.ai_row[p], j = d.fcol[p];
+    double ui[3], F[3];
+    node_u(d, i, ui);
+    int fail = 0;
+    eval_bond(d, p, i, j, ui, *d.tdev, false, F, &fail, nullptr);
+    d.ai_F[3 * p] = F[0];
+    d.ai_F[3 * p + 1] = F[1];
+    d.ai_F[3 * p + 2] = F[2];
+    d.ai_fail[p] = fail;
+}
+
+template <bool ENERGY>
+__global__ void k_ai_sum(Dev d, double dts) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int64_t N = d.n;
+    const MatDev Mi = d.mats[d.mat[i]];
+    const double rho = Mi.density;
+    const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
+    double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
+    double eacc = ENERGY ? d.eed[i] : 0.0;
+    int dmg = d.ai_dmg[i];
+    double ui[3];
+    if (ENERGY) node_u(d, i, ui);
+    const double t = *d.tdev;
+    const int64_t pe = d.frow[i + 1];
+    for (int64_t p = d.frow[i]; p < pe; ++p) {
+        if (d.ai_brk[p]) continue;
+        const int64_t j = d.fcol[p];
+        const int64_t q = d.ai_mirror[p];
+        if (j < i && d.ai_fail[q] > 0) {
+            d.ai_brk[p] = 1;  // broken by node j's visit of this bond in this stage
+            continue;
+        }
+        double F[3];
+        if (ENERGY) {
+            int fail = 0;
+            eval_bond(d, p, i, j, ui, t, true, F, &fail, &eacc);
+        } else {
+            F[0] = d.ai_F[3 * p];
+            F[1] = d.ai_F[3 * p + 1];
+            F[2] = d.ai_F[3 * p + 2];
+        }
+        dmg += d.ai_fail[p];
+        v0 += (F[0] + b0) * dts / rho;
+        v1 += (F[1] + b1) * dts / rho;
+        v2 += (F[2] + b2) * dts / rho;
+        if (d.ai_fail[p] > 0 || (j > i && d.ai_fail[q] > 0)) d.ai_brk[p] = 1;
+    }
+    d.vbuf[i] = v0;
+    d.vbuf[N + i] = v1;
+    d.vbuf[2 * N + i] = v2;
+    d.ai_dmg[i] = dmg;
+    if (ENERGY) d.eed[i] = eacc;
+}
+
+inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+void launch_ai_gather(const Dev& d, const double* us, cudaStream_t s) {
+    if (!d.ai_mls || d.ai_ntab == 0) return;
+    k_ai_gather<<<blocks_for(d.ai_ntab, 256), 256, 0, s>>>(d, us);
+}
+
+void launch_ai_force(const Dev& d, double dts, cudaStream_t s) {
+    if (d.n == 0) return;
+    if (d.ai_nent > 0) k_ai_bond<<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
+    if (d.energy) k_ai_sum<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
+    else k_ai_sum<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
+}
+
+}  // namespace pd

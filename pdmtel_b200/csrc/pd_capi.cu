@@ -125,6 +125,9 @@ struct pd_ctx {
     double* adj_pool = nullptr;  // reverse-sweep work buffers and stage tape
     int64_t adj_pool_count = 0;
     bool have_family = false, have_mls = false;
+    bool have_ai = false;                   // pd_set_ai data for the current family
+    std::vector<void*> ai_bufs;             // device buffers of the AI form
+    std::vector<int32_t> bctype_host;       // per bc: its type
     // owned device buffers
     std::vector<void*> owned;
     int64_t *frow = nullptr, *arow = nullptr, *cbptr = nullptr;
@@ -287,6 +290,7 @@ uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
 
 bool ready_dynamic(pd_ctx* c) {
     if (!c->have_family) return false;
+    if (c->d.ai) return c->have_ai;
     if (!c->d.cci && c->d.mls && !c->have_mls) return false;
     return true;
 }
@@ -311,6 +315,7 @@ void enqueue_step_body(pd_ctx* c, double dt, bool closing_gather = true) {
     cudaMemcpyAsync(d.u1, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(d.us, d.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s);
     if (d.energy) cudaMemsetAsync(d.eed, 0, sizeof(double) * c->n, s);
+    if (d.ai) cudaMemsetAsync(d.ai_dmg, 0, sizeof(int32_t) * c->n, s);
     force(dtHalf);
     pd::launch_epilogue(d, 1, dtHalf, dt, s);
     gather(d.us);
@@ -357,8 +362,11 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     if (P->num_materials <= 0 || !P->materials) return fail(PD_ERR_ARG, "pd_ctx_create: no materials");
     if (P->num_bcs < 0 || (P->num_bcs > 0 && !P->bcs)) return fail(PD_ERR_ARG, "pd_ctx_create: bad bc table");
     if (!(P->grid_spacing > 0.0) || !(P->horizon > 0.0)) return fail(PD_ERR_ARG, "pd_ctx_create: bad spacing/horizon");
-    if (P->integration != PD_INTG_CCI && P->integration != PD_INTG_FGI)
+    if (P->integration != PD_INTG_CCI && P->integration != PD_INTG_FGI && P->integration != PD_INTG_AI)
         return fail(PD_ERR_ARG, "pd_ctx_create: unknown integration scheme");
+    if (P->integration == PD_INTG_AI && (P->intg_point < 1 || P->intg_point > 3))
+        return fail(PD_ERR_ARG, "pd_ctx_create: the AI trapezoid index must be 1..3 (above 3 the reference's rule "
+                                "refines a sum left by the previous integral)");
     int n1 = P->integration == PD_INTG_FGI ? P->intg_point : 1;
     if (n1 < 1 || n1 > 8) return fail(PD_ERR_ARG, "pd_ctx_create: intg_point must be 1..8");
     if (P->integration == PD_INTG_FGI && (!P->abscissae || !P->weights))
@@ -395,7 +403,9 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     d.npt = c->npt;
     d.cci = P->integration == PD_INTG_CCI;
     d.cci_mdf = P->cci_modified ? 1 : 0;
-    d.mls = (!d.cci && n1 > 1) ? 1 : 0;
+    d.mls = (P->integration == PD_INTG_FGI && n1 > 1) ? 1 : 0;
+    d.ai = P->integration == PD_INTG_AI;
+    d.ai_n = d.ai ? P->intg_point : 0;
     d.energy = 1;
     d.dx = P->grid_spacing;
     d.delta = P->horizon;
@@ -460,7 +470,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     {
         const double vol8 = std::pow(d.dx, 3.0) / 8.0;  // pow(_gridSpacing, 3)/8.0, pdDataManager.cpp:1953
         std::vector<double> a(n1, 0.0), w(n1, 2.0);
-        if (!d.cci) {
+        if (P->integration == PD_INTG_FGI) {
             for (int k = 0; k < n1; ++k) { a[k] = P->abscissae[k]; w[k] = P->weights[k]; }
         }
         for (int i = 0; i < n1; ++i)
@@ -487,6 +497,7 @@ int pd_ctx_create(const pd_problem* P, pd_ctx** out) {
     std::vector<int32_t> bcv(N, -1);
     if (P->bc_id) std::copy(P->bc_id, P->bc_id + N, bcv.begin());
     c->bc_host = bcv;
+    for (int k = 0; k < P->num_bcs; ++k) c->bctype_host.push_back(P->bcs[k].type);
     std::vector<double> ones(N, 1.0);
     if ((rc = upload(c, x, xs.data(), sizeof(double) * n3)) || (rc = upload(c, mat, P->mat_id, sizeof(int32_t) * N)) ||
         (rc = upload(c, bc, bcv.data(), sizeof(int32_t) * N)) ||
@@ -978,6 +989,7 @@ static void install_family(pd_ctx* c, int64_t* frow, int32_t* fcol, uint8_t* fbr
     c->H = H;
     c->Ha = Ha;
     c->have_family = true;
+    c->have_ai = false;                            // its regions follow the family
     c->d.tile_x = c->d.tile_y = c->d.tile_z = 0;  // its family radius may have changed
     if (c->fst_mask) fsten_release(c);
     c->generation++;
@@ -1291,6 +1303,141 @@ int pd_afd(pd_ctx* c, const double* U, const double* bdry_eff, int64_t n_items, 
     return rc == PD_OK ? PD_OK : fail(rc, "pd_afd: device computation failed");
 }
 
+// Adaptive-trapezoid data: the regions of every full-family entry, the MLS
+// contributors and tables (or, without MLS, the check that every family node
+// carries a displacement gradient), and the per-entry work buffers.
+int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* regions, const int64_t* cb_ptr,
+              const int32_t* cb_idx, const int64_t* tab_ptr, const double* tab_coeff) {
+    if (!c || !reg_ptr) return fail(PD_ERR_ARG, "pd_set_ai: null argument");
+    if (!c->d.ai) return fail(PD_ERR_ARG, "pd_set_ai: the context was not created with PD_INTG_AI");
+    if (!c->have_family) return fail(PD_ERR_ARG, "pd_set_ai: no family (pd_bond_search or pd_set_family first)");
+    const int64_t N = c->n, H = c->H;
+    if (reg_ptr[0] != 0) return fail(PD_ERR_ARG, "pd_set_ai: bad reg_ptr");
+    for (int64_t p = 0; p < H; ++p)
+        if (reg_ptr[p + 1] < reg_ptr[p]) return fail(PD_ERR_ARG, "pd_set_ai: reg_ptr not monotone");
+    const int64_t R = reg_ptr[H];
+    if (R > 0 && !regions) return fail(PD_ERR_ARG, "pd_set_ai: null regions");
+    for (int64_t r = 0; r < R; ++r) {
+        const pd_ai_region& g = regions[r];
+        const int a0 = g.axis[0], a1 = g.axis[1], a2 = g.axis[2];
+        bool ok = a0 < 3 && a1 < 3 && a2 < 3 && a0 != a1 && a0 != a2 && a1 != a2;
+        for (int k = 0; k < 2; ++k) ok = ok && (g.lim[k] < 6 || (g.lim[k] >= 8 && g.lim[k] < 44));
+        for (int k = 2; k < 4; ++k) ok = ok && (g.lim[k] < 6 || (g.lim[k] >= 8 && g.lim[k] < 14));
+        if (!ok) return fail(PD_ERR_ARG, "pd_set_ai: bad region axes or limit codes");
+    }
+    std::vector<int64_t> frow(N + 1);
+    std::vector<int32_t> fcol(std::max<int64_t>(H, 1));
+    PD_TRY(pd_get_family(c, frow.data(), fcol.data(), nullptr));
+    std::vector<int32_t> row(std::max<int64_t>(H, 1));
+    std::vector<int64_t> mirror(std::max<int64_t>(H, 1));
+    for (int64_t i = 0; i < N; ++i)
+        for (int64_t p = frow[i]; p < frow[i + 1]; ++p) {
+            row[p] = (int32_t)i;
+            const int64_t j = fcol[p];
+            const int32_t* b = fcol.data() + frow[j];
+            const int32_t* e = fcol.data() + frow[j + 1];
+            const int32_t* q = std::lower_bound(b, e, (int32_t)i);
+            if (q == e || *q != i) return fail(PD_ERR_ARG, "pd_set_ai: the family is not symmetric");
+            mirror[p] = q - fcol.data();
+        }
+    int64_t T = 0, ncoef = 0;
+    std::vector<int32_t> tnode;
+    std::vector<int64_t> coff(N + 1, 0);
+    if (mls) {
+        if (!cb_ptr || !cb_idx || !tab_ptr || !tab_coeff) return fail(PD_ERR_ARG, "pd_set_ai: null MLS data");
+        if (cb_ptr[0] != 0 || tab_ptr[0] != 0) return fail(PD_ERR_ARG, "pd_set_ai: bad cb_ptr / tab_ptr");
+        for (int64_t i = 0; i < N; ++i) {
+            if (cb_ptr[i + 1] < cb_ptr[i] || tab_ptr[i + 1] < tab_ptr[i])
+                return fail(PD_ERR_ARG, "pd_set_ai: cb_ptr / tab_ptr not monotone");
+            coff[i + 1] = coff[i] + (tab_ptr[i + 1] - tab_ptr[i]) * (cb_ptr[i + 1] - cb_ptr[i]);
+        }
+        for (int64_t k = 0; k < cb_ptr[N]; ++k)
+            if (cb_idx[k] < 0 || cb_idx[k] >= N) return fail(PD_ERR_ARG, "pd_set_ai: contributor out of range");
+        T = tab_ptr[N];
+        ncoef = coff[N];
+        tnode.resize(std::max<int64_t>(T, 1));
+        for (int64_t i = 0; i < N; ++i)
+            for (int64_t e = tab_ptr[i]; e < tab_ptr[i + 1]; ++e) tnode[e] = (int32_t)i;
+    } else {
+        for (int64_t p = 0; p < H; ++p) {
+            const int b = c->bc_host[fcol[p]];
+            if (b < 0 || c->bctype_host[b] != PD_BC_DISPLGRAD)
+                return fail(PD_ERR_ARG, "pd_set_ai: without MLS every family node needs a displacement-gradient "
+                                        "condition (pdIntgManager2.cpp:211-235)");
+        }
+    }
+    for (void* q : c->ai_bufs) dfree(c, q);
+    c->ai_bufs.clear();
+    c->have_ai = false;
+    pd::Dev& d = c->d;
+    int64_t *rptr = nullptr, *mir = nullptr, *tptr = nullptr, *cof = nullptr, *cbp = nullptr;
+    int32_t *rw = nullptr, *tn = nullptr, *cbi = nullptr, *fl = nullptr, *dmg = nullptr;
+    pd_ai_region* reg = nullptr;
+    double *tco = nullptr, *au = nullptr, *F = nullptr;
+    uint8_t* brk = nullptr;
+    int* err = nullptr;
+    auto track = [&](void* q) { c->ai_bufs.push_back(q); };
+    PD_TRY(dalloc(c, &rptr, H + 1)); track(rptr);
+    PD_TRY(dalloc(c, &reg, R)); track(reg);
+    PD_TRY(dalloc(c, &rw, H)); track(rw);
+    PD_TRY(dalloc(c, &mir, H)); track(mir);
+    PD_TRY(dalloc(c, &F, 3 * H)); track(F);
+    PD_TRY(dalloc(c, &fl, H)); track(fl);
+    PD_TRY(dalloc(c, &brk, H)); track(brk);
+    PD_TRY(dalloc(c, &dmg, N)); track(dmg);
+    PD_TRY(dalloc(c, &err, 1)); track(err);
+    PD_TRY(upload(c, rptr, reg_ptr, sizeof(int64_t) * (H + 1)));
+    if (R) PD_TRY(upload(c, reg, regions, sizeof(pd_ai_region) * R));
+    if (H) {
+        PD_TRY(upload(c, rw, row.data(), sizeof(int32_t) * H));
+        PD_TRY(upload(c, mir, mirror.data(), sizeof(int64_t) * H));
+        PD_CUDA_TRY(cudaMemcpyAsync(brk, c->fbroken, H, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    PD_CUDA_TRY(cudaMemsetAsync(dmg, 0, sizeof(int32_t) * N, c->stream));
+    PD_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), c->stream));
+    if (mls) {
+        PD_TRY(dalloc(c, &cbp, N + 1)); track(cbp);
+        PD_TRY(dalloc(c, &cbi, cb_ptr[N])); track(cbi);
+        PD_TRY(dalloc(c, &tptr, N + 1)); track(tptr);
+        PD_TRY(dalloc(c, &cof, N + 1)); track(cof);
+        PD_TRY(dalloc(c, &tn, T)); track(tn);
+        PD_TRY(dalloc(c, &tco, ncoef)); track(tco);
+        PD_TRY(dalloc(c, &au, 3 * T)); track(au);
+        PD_TRY(upload(c, cbp, cb_ptr, sizeof(int64_t) * (N + 1)));
+        if (cb_ptr[N]) PD_TRY(upload(c, cbi, cb_idx, sizeof(int32_t) * cb_ptr[N]));
+        PD_TRY(upload(c, tptr, tab_ptr, sizeof(int64_t) * (N + 1)));
+        PD_TRY(upload(c, cof, coff.data(), sizeof(int64_t) * (N + 1)));
+        if (T) PD_TRY(upload(c, tn, tnode.data(), sizeof(int32_t) * T));
+        if (ncoef) PD_TRY(upload(c, tco, tab_coeff, sizeof(double) * ncoef));
+        PD_CUDA_TRY(cudaMemsetAsync(au, 0, sizeof(double) * 3 * std::max<int64_t>(T, 1), c->stream));
+        c->cbptr_host.assign(cb_ptr, cb_ptr + N + 1);
+        c->cbidx_host.assign(cb_idx, cb_idx + cb_ptr[N]);
+    }
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    d.ai_mls = mls ? 1 : 0;
+    d.ai_nent = H;
+    d.ai_ntab = T;
+    d.ai_rptr = rptr;
+    d.ai_reg = reg;
+    d.ai_row = rw;
+    d.ai_mirror = mir;
+    d.ai_F = F;
+    d.ai_fail = fl;
+    d.ai_brk = brk;
+    d.ai_dmg = dmg;
+    d.ai_err = err;
+    d.ai_tptr = tptr;
+    d.ai_coff = cof;
+    d.ai_tnode = tn;
+    d.ai_tcoef = tco;
+    d.ai_u = au;
+    d.cbptr = cbp;
+    d.cbidx = cbi;
+    c->have_ai = true;
+    c->generation++;
+    return PD_OK;
+}
+
 // The MLS data out, in the layout pd_set_mls takes (coeff [node][point][contributor]).
 int pd_get_mls(pd_ctx* c, int64_t* cb_ptr, int32_t* cb_idx, double* coeff) {
     if (!c || !cb_ptr) return fail(PD_ERR_ARG, "pd_get_mls: null argument");
@@ -1320,6 +1467,8 @@ int pd_mls_size(pd_ctx* c, int64_t* num_contrib) {
 int pd_set_precision(pd_ctx* c, int p) {
     if (!c || (p != PD_PREC_FP64 && p != PD_PREC_FP32C && p != PD_PREC_FP64A))
         return fail(PD_ERR_ARG, "pd_set_precision: bad argument");
+    if (c->d.ai && p != PD_PREC_FP64)
+        return fail(PD_ERR_ARG, "pd_set_precision: the AI form runs the FP64 drop-in arithmetic only");
     c->precision = p;
     c->d.acc_stretch = p == PD_PREC_FP64A;
     return PD_OK;
@@ -1544,6 +1693,7 @@ int pd_init_dynamic(pd_ctx* c) {
     const size_t b3 = sizeof(double) * 3 * c->n;
     PD_CUDA_TRY(cudaMemcpyAsync(c->d.vbuf, c->d.V, b3, cudaMemcpyDeviceToDevice, c->stream));
     PD_CUDA_TRY(cudaMemsetAsync(c->d.eed, 0, sizeof(double) * c->n, c->stream));
+    if (c->d.ai && c->have_ai) PD_CUDA_TRY(cudaMemsetAsync(c->d.ai_dmg, 0, sizeof(int32_t) * c->n, c->stream));
     PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return PD_OK;
 }
@@ -1705,6 +1855,11 @@ int pd_reset_state(pd_ctx* c) {
     PD_CUDA_TRY(cudaMemsetAsync(c->d.ug, 0, b3 * c->npt, s));
     PD_CUDA_TRY(cudaMemsetAsync(c->d.nblk, 0, sizeof(float) * c->n * c->d.bs, s));
     PD_CUDA_TRY(cudaMemsetAsync(c->d.eed, 0, sizeof(double) * c->n, s));
+    if (c->d.ai && c->have_ai) {
+        // the bonds the AI form broke heal: back to the family's own flags
+        PD_CUDA_TRY(cudaMemcpyAsync(c->d.ai_brk, c->fbroken, c->H, cudaMemcpyDeviceToDevice, s));
+        PD_CUDA_TRY(cudaMemsetAsync(c->d.ai_dmg, 0, sizeof(int32_t) * c->n, s));
+    }
     PD_CUDA_TRY(cudaStreamSynchronize(s));
     return PD_OK;
 }
@@ -2290,7 +2445,8 @@ int save_checkpoint(pd_ctx* c, pd_ctx::Checkpoint& k) {
 extern "C" int pd_adjoint_forward(pd_ctx* c, double dt, double t0, int nsteps, int every) {
     if (!c || nsteps < 1 || every < 1) return fail(PD_ERR_ARG, "pd_adjoint_forward: bad argument");
     if (!ready_dynamic(c)) return fail(PD_ERR_ARG, "pd_adjoint_forward: family/MLS data not set");
-    if (c->d.cci) return fail(PD_ERR_ARG, "pd_adjoint_forward: the adjoint covers the Gauss-point (FGI) scheme");
+    if (c->d.cci || c->d.ai)
+        return fail(PD_ERR_ARG, "pd_adjoint_forward: the adjoint covers the Gauss-point (FGI) scheme");
     const int prec = c->precision, energy = c->d.energy;
     if (prec != PD_PREC_FP64A && prec != PD_PREC_FP32C) c->precision = PD_PREC_FP64;
     c->adj_acc = c->d.acc_stretch = prec == PD_PREC_FP64A;

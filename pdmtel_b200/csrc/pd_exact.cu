@@ -406,6 +406,10 @@ inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) /
 
 void launch_force_f64(const Dev& d, double dts, cudaStream_t s) {
     if (d.n == 0) return;
+    if (d.ai) {
+        launch_ai_force(d, dts, s);
+        return;
+    }
     const int bs = 128;
     size_t sh = (size_t)d.npt * sizeof(GaussConst);
     unsigned nb = blocks_for(d.n, bs);
@@ -438,6 +442,10 @@ void launch_force_f64(const Dev& d, double dts, cudaStream_t s) {
 }
 
 void launch_gather_f64(const Dev& d, const double* us, cudaStream_t s) {
+    if (d.ai) {
+        launch_ai_gather(d, us, s);
+        return;
+    }
     if (d.cci || d.n == 0) return;
     const int bs = 256;
     k_gather_f64<<<blocks_for(d.n * d.npt, bs), bs, 0, s>>>(d, us);

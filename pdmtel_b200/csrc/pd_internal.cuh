@@ -147,6 +147,24 @@ struct Dev {
     const int32_t* gpat_id;
     const int64_t* gpat_ptr;
     const int32_t* gpat_off;
+    // adaptive-trapezoid (AI) integration (pd_ai.cu): the force of a bond is
+    // the sum of its regions' nested trapezoid integrals (pd_ai_eval.h)
+    int ai, ai_n, ai_mls;         // on, trapezoid index 1..3, MLS on
+    int64_t ai_nent, ai_ntab;     // full-family entries, MLS table entries
+    const int64_t* ai_rptr;       // [H+1] regions of each full-family entry
+    const pd_ai_region* ai_reg;
+    const int32_t* ai_row;        // [H] node i of full-family entry i -> j
+    const int64_t* ai_mirror;     // [H] entry j -> i
+    const int64_t* ai_tptr;       // [N+1] MLS table entries of each node
+    const int64_t* ai_coff;       // [N] first coefficient of each node's table
+    const int32_t* ai_tnode;      // [T] node of each table entry
+    const double* ai_tcoef;       // [entry][contributor of the node]
+    double* ai_u;                 // [T][3] displacement of each table entry (per stage)
+    double* ai_F;                 // [H][3] bond force of the stage
+    int32_t* ai_fail;             // [H] points past the critical stretch in the stage's evaluation
+    uint8_t* ai_brk;              // [H] broken: an AI bond breaks for good
+    int32_t* ai_dmg;              // [N] failed points of the step (pdNode's damaged-bond count)
+    int* ai_err;                  // a table entry out of range was asked for
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
@@ -184,6 +202,11 @@ struct SearchGrid {
 int bond_search(const Dev& d, const SearchGrid& g, const int32_t* cell_rank, int64_t ncell, int nslit,
                 const double* slits_dev, int64_t** frow, int32_t** fcol, uint8_t** fbroken, int64_t** arow,
                 int32_t** acol, int64_t* nh, int64_t* nb, double* min_bond, cudaStream_t s);
+
+// adaptive-trapezoid (AI) form (pd_ai.cu, compiled without FMA contraction):
+// the MLS table gather of a stage and the force stage
+void launch_ai_gather(const Dev& d, const double* us, cudaStream_t s);
+void launch_ai_force(const Dev& d, double dts, cudaStream_t s);
 
 // FP32 compensated form (pd_f32c.cu)
 void launch_force_f32c(const Dev& d, double dts, cudaStream_t s);

@@ -110,13 +110,32 @@ def test_deletion_space_renumbers_nodes(tmp_path):
     assert np.all(np.abs(x.reshape(-1, 3)[:, 0]) > 1e-3)
 
 
-def test_unsupported_adaptive_integration(tmp_path):
+def _ai_deck(tmp_path, extra=""):
     d = D.config_bar(dims=(5, 4, 4))
-    text = d.text().replace("fgi_on\n 1\n", "fgi_on\n 0\nai_on\n 1 1\n")
+    text = d.text().replace("fgi_on\n 1\n", "fgi_on\n 0\nai_on\n 1 1\n" + extra)
     (tmp_path / "pds_input.txt").write_text(text)
+    return str(tmp_path)
+
+
+def test_adaptive_integration_deck(tmp_path):
+    """ai_on decks are read (pdDataManager.cpp:656-717) and echoed with the
+    reference's AI lines (:747-753)."""
+    path = _ai_deck(tmp_path, "intg_point\n 2\n")
+    P.pdDataManager(path)
+    log = (tmp_path / "pds_output.dat").read_text()
+    assert "Adaptive integration method flag = 1" in log
+    assert "Starting trapezoidal index = 2" in log
+    assert "Error control method flag = 0" in log
+
+
+@pytest.mark.parametrize("extra,word", [("error_control_on\n 1\n", "error_control_on"),
+                                        ("intg_point\n 4\n", "trapezoid index")])
+def test_adaptive_integration_refusals(tmp_path, extra, word):
+    """The refinement with error control reads MLS list entries the setup pass
+    never stored, and an index above 3 refines a stale sum: both refused."""
     with pytest.raises(P.PdError) as e:
-        P.pdDataManager(str(tmp_path))
-    assert "adaptive" in str(e.value)
+        P.pdDataManager(_ai_deck(tmp_path, extra))
+    assert word in str(e.value)
 
 
 def test_no_gpu_fails_loudly(tmp_path):
