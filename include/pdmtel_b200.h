@@ -214,6 +214,13 @@ int pd_ai_mls_table(int64_t num_nodes, const double* coords, const int64_t* row_
  * both of its nodes (pdIntgManager2.cpp:301-308); the FP64 arithmetic only. */
 int pd_set_ai(pd_ctx* ctx, int mls, const int64_t* reg_ptr, const pd_ai_region* regions, const int64_t* cb_ptr,
               const int32_t* cb_idx, const int64_t* tab_ptr, const double* tab_coeff);
+/* The AI form's damage state: broken [full-family entries] (the family's
+ * flags plus the bonds the AI integrand broke) and count [N], the points of
+ * node i past the critical stretch in the last step (pdNode's damaged-bond
+ * count, pdIntgManager2.cpp:308; reset by pdDataManager::InitDynamicSolve,
+ * pdDataManager2.cpp:426).  Either may be NULL; other schemes report their
+ * family's flags and zero counts. */
+int pd_get_damage(pd_ctx* ctx, uint8_t* broken, int32_t* count);
 /* number of MLS contributor entries held (0 without MLS data) */
 int pd_mls_size(pd_ctx* ctx, int64_t* num_contrib);
 

@@ -356,6 +356,16 @@ int main(int argc, char** argv) {
         std::vector<double> eed;
         for (int i = 0; i < dat.GetNumNode(); ++i) eed.push_back(dat.GetNode(i)->GetElastEnergyDensity());
         w.d("eed", eed);
+        // bonds broken by the stage (the AI integrand breaks them,
+        // pdIntgManager2.cpp:301-308) and the per-node damaged-point counts
+        std::vector<int32_t> broken_after, dmg;
+        for (int i = 0; i < dat.GetNumNode(); ++i) {
+            pdNode* n = dat.GetNode(i);
+            for (int f = 0; f < n->GetNumFamily(); ++f) broken_after.push_back(n->GetFamilyBond(f)->IsBreak() ? 1 : 0);
+            dmg.push_back(n->GetNumDmgBond());
+        }
+        w.i("broken_after", broken_after);
+        w.i("dmg", dmg);
     } else if (mode == "traj") {
         int nsteps = std::atoi(argv[4]), every = std::atoi(argv[5]);
         setup(dat, dir);
@@ -375,6 +385,12 @@ int main(int argc, char** argv) {
             ee.push_back(dat.GetElastStep());
             times.push_back(t);
             if (it % every == 0 || it == nsteps) {
+                std::vector<int32_t> br;
+                for (int i = 0; i < dat.GetNumNode(); ++i) {
+                    pdNode* n = dat.GetNode(i);
+                    for (int f = 0; f < n->GetNumFamily(); ++f) br.push_back(n->GetFamilyBond(f)->IsBreak() ? 1 : 0);
+                }
+                w.i("broken_" + std::to_string(it), br);
                 w.d("U_" + std::to_string(it), node_state(dat, 0));
                 w.d("V_" + std::to_string(it), node_state(dat, 1));
                 w.d("ug_" + std::to_string(it), gauss_u(dat));

@@ -169,6 +169,7 @@ _SIGS = {
     "pd_ai_mls_table": [C.c_int64, _d, _i64, _i32, _i64, C.POINTER(pd_ai_region), C.c_double, C.c_double, C.c_int,
                         _i64, _i32, C.c_double, _i64, _d, C.c_int64, _i64, _i64],
     "pd_set_ai": [_vp, C.c_int, _i64, C.POINTER(pd_ai_region), _i64, _i32, _i64, _d],
+    "pd_get_damage": [_vp, _u8, _i32],
     "pd_autotune": [_vp, C.c_double, C.c_int, C.POINTER(pd_tune_result)],
 }
 
@@ -376,6 +377,13 @@ class DeviceContext:
         tc = _f64(tab_coeff) if mls else None
         _check(lib().pd_set_ai(self.h, int(mls), _p(gp, _i64), regions, _p(cp, _i64), _p(ci, _i32), _p(tp, _i64),
                                _p(tc, _d)), "pd_set_ai")
+
+    def get_damage(self, num_halves):
+        """(broken flags per family entry, failed points per node of the last step)"""
+        br = np.zeros(max(num_halves, 1), np.uint8)
+        cnt = np.zeros(self.n, np.int32)
+        _check(lib().pd_get_damage(self.h, _p(br, _u8), _p(cnt, _i32)), "pd_get_damage")
+        return br[:num_halves], cnt
 
     def set_mls(self, cb_ptr, cb_idx, coeff):
         cp = np.ascontiguousarray(cb_ptr, dtype=np.int64)

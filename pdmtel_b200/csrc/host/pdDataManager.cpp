@@ -898,22 +898,37 @@ int pdSolve::InitialProblem(pdDataManager& dat) {
     return PD_OK;
 }
 
+// DmgFrac of every node: pdNode::GetDmgFraction (pdNode.cpp:225-232), the
+// int count of damaged bonds over the family size in int arithmetic.  Only
+// the AI integrand counts (one per point past the critical stretch,
+// pdIntgManager2.cpp:308); the Gauss-point and CCI paths leave it 0.
+int pdDataManager::DamageFractions(std::vector<double>& f) {
+    f.assign(_numNodes, 0.0);
+    if (!_aiOn || !_ctx) return PD_OK;
+    std::vector<int32_t> cnt(_numNodes, 0);
+    const int rc = pd_get_damage(_ctx, nullptr, cnt.data());
+    if (rc != PD_OK) return Cuda(rc, "pd_get_damage");
+    for (int64_t i = 0; i < _numNodes; ++i) {
+        const int nf = (int)(_famPtr[i + 1] - _famPtr[i]);
+        f[i] = nf != 0 ? (double)(cnt[i] / nf) : 0.0;
+    }
+    return PD_OK;
+}
+
 // one node record as pdNode::Print writes it (pdNode.cpp:418-433)
 static void print_node(std::ostream& os, int64_t i, const pdDataManager& dat, const std::vector<double>& U,
-                       const std::vector<double>& V) {
+                       const std::vector<double>& V, const std::vector<double>& dmg) {
     const auto& x = dat.Coords();
     os << i << "\t" << x[3 * i] << "\t" << x[3 * i + 1] << "\t" << x[3 * i + 2] << "\t" << U[3 * i] << "\t"
        << U[3 * i + 1] << "\t" << U[3 * i + 2] << "\t" << V[3 * i] << "\t" << V[3 * i + 1] << "\t" << V[3 * i + 2]
-       << "\t" << dat.MatIds()[i] << "\t" << dat.BcIds()[i] << "\t" << dat.BdryEff()[i] << "\t" << 0.0;
-    // DmgFrac: pdNode::GetDmgFraction (pdNode.cpp:225-232), an int count of
-    // damaged bonds over the family size; nothing on the RK4 path counts a
-    // damaged bond, so the reference writes 0 as a double
+       << "\t" << dat.MatIds()[i] << "\t" << dat.BcIds()[i] << "\t" << dat.BdryEff()[i] << "\t" << dmg[i];
 }
 
 int pdSolve::WriteTecplot(pdDataManager& dat, int step, double time) {
-    std::vector<double> U, V;
+    std::vector<double> U, V, dmg;
     int rc;
-    if ((rc = dat.GetDispl(U)) != PD_OK || (rc = dat.GetVeloc(V)) != PD_OK) return rc;
+    if ((rc = dat.GetDispl(U)) != PD_OK || (rc = dat.GetVeloc(V)) != PD_OK || (rc = dat.DamageFractions(dmg)) != PD_OK)
+        return rc;
     std::ofstream out((dat.GetWkDir() + keyword_append("pds_tecplot_", step) + ".dat").c_str());
     out << "Tecplot formatting output mode\n";
     out.setf(std::ios::scientific);
@@ -922,7 +937,7 @@ int pdSolve::WriteTecplot(pdDataManager& dat, int step, double time) {
         << "ZONE I=" << dat.GetGridDimension(0) << ", J=" << dat.GetGridDimension(1)
         << ", K=" << dat.GetGridDimension(2) << ", F=POINT\n\n";
     for (int64_t i = 0; i < dat.GetNumNode(); ++i) {
-        print_node(out, i, dat, U, V);
+        print_node(out, i, dat, U, V, dmg);
         out << "\n";
     }
     (void)time;
@@ -1094,11 +1109,12 @@ int pdSolve::SolveDynamic(pdDataManager& dat, bool write_files) {
             if (iter == 1 || iter == lastStep || iter % dump == 0)
                 if ((rc = WriteTecplot(dat, iter, t)) != PD_OK) return rc;
             if (probe >= 0) {
-                std::vector<double> U, V;
+                std::vector<double> U, V, dmg;
                 dat.GetDispl(U);
                 dat.GetVeloc(V);
+                if ((rc = dat.DamageFractions(dmg)) != PD_OK) return rc;
                 steps << iter << "\t" << t << "\t";
-                print_node(steps, probe, dat, U, V);
+                print_node(steps, probe, dat, U, V, dmg);
                 steps << "\n";
             }
         } else {

@@ -96,6 +96,7 @@ public:
                     double* relres);
 
     // state
+    int DamageFractions(std::vector<double>& frac);  // DmgFrac of every node
     int GetDispl(std::vector<double>& U);
     int GetVeloc(std::vector<double>& V);
     int SetState(const std::vector<double>& U, const std::vector<double>& V);

@@ -1438,6 +1438,24 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     return PD_OK;
 }
 
+int pd_get_damage(pd_ctx* c, uint8_t* broken, int32_t* count) {
+    if (!c) return fail(PD_ERR_ARG, "pd_get_damage: null context");
+    const bool ai = c->d.ai && c->have_ai;
+    if (broken) {
+        if (!c->have_family) return fail(PD_ERR_ARG, "pd_get_damage: no family");
+        if (c->H)
+            PD_CUDA_TRY(cudaMemcpyAsync(broken, ai ? c->d.ai_brk : c->fbroken, c->H, cudaMemcpyDeviceToHost,
+                                        c->stream));
+    }
+    if (count) {
+        if (ai) PD_CUDA_TRY(cudaMemcpyAsync(count, c->d.ai_dmg, sizeof(int32_t) * c->n, cudaMemcpyDeviceToHost,
+                                            c->stream));
+        else std::fill(count, count + c->n, 0);
+    }
+    PD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return PD_OK;
+}
+
 // The MLS data out, in the layout pd_set_mls takes (coeff [node][point][contributor]).
 int pd_get_mls(pd_ctx* c, int64_t* cb_ptr, int32_t* cb_idx, double* coeff) {
     if (!c || !cb_ptr) return fail(PD_ERR_ARG, "pd_get_mls: null argument");

@@ -65,6 +65,7 @@ class Deck:
     cci: Optional[Sequence[int]] = None  # (on, modified); None -> FGI
     intg_point: int = 2
     support_domain: Optional[float] = None
+    ai_mls: Optional[int] = None  # adaptive trapezoid (ai_on 1 <mls>); intg_point is its trapezoid index
     title: str = "pdmtel_b200 synthetic deck"
 
     def text(self) -> str:
@@ -112,6 +113,13 @@ class Deck:
         kv("bdryEff_on", str(int(self.bdry_eff)))
         if self.cci is not None:
             kv("cci_on", f"{int(self.cci[0])} {int(self.cci[1])}")
+        elif self.ai_mls is not None:
+            kv("cci_on", "0 0")
+            kv("fgi_on", "0")
+            kv("ai_on", f"1 {int(self.ai_mls)}")
+            kv("intg_point", str(int(self.intg_point)))
+            if self.support_domain is not None:
+                kv("support_domain_size", repr(float(self.support_domain)))
         else:
             kv("cci_on", "0 0")
             kv("fgi_on", "1")

@@ -6,6 +6,7 @@
     python tests/golden/make_golden.py --long    # the 20x10x10 bar over 100 steps, long/*.npz
     python tests/golden/make_golden.py --static  # the linearised stiffness pass, static/*.npz
     python tests/golden/make_golden.py --outputs # the reference's output files, outputs/<case>/
+    python tests/golden/make_golden.py --ai      # adaptive-trapezoid decks, tests/golden/ai/*.npz
 
 Each case is a small synthetic deck written by pdmtel_b200.decks into
 tests/golden/decks/<case>/pds_input.txt; the reference harness
@@ -108,8 +109,81 @@ def main():
     shutil.rmtree(tmp, ignore_errors=True)
 
 
-if __name__ == "__main__" and not {"--kat", "--long", "--static", "--outputs"} & set(sys.argv):
+if __name__ == "__main__" and not {"--kat", "--long", "--static", "--outputs", "--ai"} & set(sys.argv):
     main()
+
+
+def ai_cases():
+    """Adaptive-trapezoid (ai_on) decks.  Boundary conditions prescribe every
+    direction (DISPL or DISPLGRAD with flags 1 1 1): a family node with a
+    VELOC condition, or an unflagged direction, makes the reference's
+    integrand read an unset local (pdIntgManager2.cpp:122-174), which no
+    fixture can pin."""
+    h = 1e-3
+    out = {}
+    dims = (7, 5, 5)
+    grad = D.BC(D.DISPLGRAD, (1, 1, 1), (1e-4, 0, 0, 0, 0, 0, 0, 2e-5, -5e-5), 5e-8, 1.0)
+    pull = D.BC(D.DISPL, (1, 1, 1), (1e-7, 3e-9, -2e-8), 1.0, 2.0)
+    spaces = [D.Space(1, D.face_box(dims, h, 2, -1)), D.Space(2, D.face_box(dims, h, 0, +1))]
+    # trapezoid index 3 (5 points per direction), MLS, boundary factors
+    d = D.Deck(dims=dims, spacing=h, horizon=3.015 * h, total_time=1.0, total_step=100, fixed_dt=1e-8,
+               damping=0.02, bdry_eff=1, ai_mls=1, intg_point=3, bcs=[grad, pull], bc_spaces=spaces)
+    out["ai_mls3"] = (d, dict(force=(1e-8, 1e-8), traj=(2, 1)))
+    # trapezoid index 2, a wider horizon (other cuts of the cell by the sphere)
+    dims2 = (8, 6, 5)
+    d = D.Deck(dims=dims2, spacing=h, horizon=3.5 * h, total_time=1.0, total_step=100, fixed_dt=1e-8,
+               bdry_eff=0, ai_mls=1, intg_point=2, bcs=[pull, D.BC(D.DISPL, (1, 1, 1), (0, 0, 0), 1.0, 2.0)],
+               bc_spaces=[D.Space(1, D.face_box(dims2, h, 0, +1)), D.Space(2, D.face_box(dims2, h, 0, -1))])
+    out["ai_mls2_d35"] = (d, dict(force=(2e-8, 1e-8), traj=(2, 2)))
+    # trapezoid index 1, horizon 2.515 dx, a slit
+    dims3 = (9, 6, 4)
+    d = D.Deck(dims=dims3, spacing=h, horizon=2.515 * h, total_time=1.0, total_step=100, fixed_dt=1e-8,
+               slits=[(-0.0015, -0.0005, -1.0, 0.0002, -1.0, 1.0)],
+               bdry_eff=1, ai_mls=1, intg_point=1, bcs=[pull], bc_spaces=[D.Space(1, D.face_box(dims3, h, 0, +1))])
+    out["ai_mls1_slit"] = (d, dict(force=(2e-8, 1e-8), traj=(3, 3)))
+    # (ai_on 1 0, without MLS, is left out: the reference's RK4 path deletes
+    # element 0 of a zero-length contributor array in ~pdIntgManager
+    # (pdIntgManager.cpp:37-46, pdDataManager.cpp:1892-1901) and crashes)
+    # a small critical stretch: points past it break their bonds
+    d = D.Deck(dims=dims, spacing=h, horizon=3.015 * h, total_time=1.0, total_step=100, fixed_dt=1e-8,
+               materials=[(72e9, 1e20, 2.0e-4, 2440.0)], bdry_eff=0, ai_mls=1, intg_point=1,
+               bcs=[D.BC(D.DISPL, (1, 1, 1), (4e-6, 0, 0), 3e-8, 1.0), D.BC(D.DISPL, (1, 1, 1), (0, 0, 0), 1.0, 2.0)],
+               bc_spaces=[D.Space(1, D.face_box(dims, h, 0, +1)), D.Space(2, D.face_box(dims, h, 0, -1))])
+    out["ai_break"] = (d, dict(force=(1e-8, 1e-8), traj=(4, 1)))
+    return out
+
+
+def _ai_one(args):
+    name, deck, spec, tmp = args
+    ddir = os.path.join(HERE, "decks", name)
+    deck.write(ddir)
+    wd = os.path.join(tmp, name)
+    os.makedirs(wd, exist_ok=True)
+    shutil.copy(os.path.join(ddir, "pds_input.txt"), os.path.join(wd, "pds_input.txt"))
+    data = {}
+    t, dts = spec["force"]
+    run("force", wd, os.path.join(wd, "force.bin"), t, dts)
+    data.update(read_pdb(os.path.join(wd, "force.bin")))
+    if spec["traj"]:
+        nsteps, every = spec["traj"]
+        run("traj", wd, os.path.join(wd, "traj.bin"), nsteps, every)
+        for k, v in read_pdb(os.path.join(wd, "traj.bin")).items():
+            if k.startswith(("U_", "V_", "broken_")) or k in ("ke", "ee", "times"):
+                data["traj_" + k] = v
+    data["force_args"] = np.array([t, dts])
+    os.makedirs(os.path.join(HERE, "ai"), exist_ok=True)
+    np.savez_compressed(os.path.join(HERE, "ai", name + ".npz"), **data)
+    return name, int(data["n"][0]), len(data["fam_col"])
+
+
+def make_ai():
+    from multiprocessing import get_context
+    tmp = tempfile.mkdtemp(prefix="pdgolden_ai_")
+    jobs = [(name, deck, spec, tmp) for name, (deck, spec) in ai_cases().items()]
+    with get_context("spawn").Pool(len(jobs)) as pool:
+        for name, n, h in pool.imap_unordered(_ai_one, jobs):
+            print(name, n, "nodes", h, "halves", flush=True)
+    shutil.rmtree(tmp, ignore_errors=True)
 
 
 def sample_like_deck():
@@ -385,3 +459,7 @@ def make_outputs():
 
 if __name__ == "__main__" and "--outputs" in sys.argv:
     make_outputs()
+
+
+if __name__ == "__main__" and "--ai" in sys.argv:
+    make_ai()
