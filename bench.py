@@ -55,6 +55,11 @@ line carries the same comparison under "static" (--no-static leaves it out).
 profiler captures are taken on.  --form adjoint: the adjoint pair alone on the
 identification specimen (--adjoint-steps).
 
+--form ai: the adaptive-trapezoid (ai_on) form on the 20x10x10 bar (FP64
+drop-in, trapezoid index 3, MLS): RK4 steps on the device, in trapezoid-point
+force evaluations per second, against one stage of the oracle port on the
+host (the reference's own AI setup on this bar runs for tens of minutes).
+
 Multi-GPU: replicas (one full plate per rank, no data-path collective);
 weak scaling; time = max over ranks of the device-timed region.
 """
@@ -697,6 +702,99 @@ def run_steps(args):
     return 0
 
 
+def ai_deck(dims):
+    """The 20x10x10 bar of the plain-FP64 config with adaptive-trapezoid
+    integration (ai_on, trapezoid index 3, MLS): left face held, right face
+    pulled by a ramped displacement."""
+    from pdmtel_b200 import decks as D
+    h = 1e-3
+    return D.Deck(dims=dims, spacing=h, horizon=3.015 * h, total_time=1.0, total_step=100, fixed_dt=1e-8,
+                  bdry_eff=1, ai_mls=1, intg_point=3,
+                  bcs=[D.BC(D.DISPL, (1, 1, 1), (0, 0, 0), 1.0, 2.0), D.BC(D.DISPL, (1, 1, 1), (2e-6, 0, 0), 2e-7, 1.0)],
+                  bc_spaces=[D.Space(1, D.face_box(dims, h, 0, -1)), D.Space(2, D.face_box(dims, h, 0, +1))])
+
+
+def ai_oracle_stage_seconds(dm, dims, trap=3):
+    """One AI force stage of the oracle port (single thread) on the same deck:
+    the CPU baseline of the AI form."""
+    import ctypes as C
+    import numpy as np
+    import pdmtel_b200 as P
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as OL
+    x, mat, bc = dm.nodes()
+    rp, col, br = dm.family()
+    cp, ci, _ = dm.mls()
+    mats, bcs, _, _ = dm.tables()
+    h = 1e-3
+    ptr, regs = P.ai_plan(x, rp, col, h, 3.015 * h)
+    tp, tc = P.ai_mls_table(x, rp, col, ptr, regs, h, 3.015 * h, trap, cp, ci, 3.0 * h)
+    n = x.size // 3
+    rng = np.random.default_rng(1)
+    u = 1e-7 * rng.standard_normal(3 * n)
+    m = OL.Model(n=n, x=x, dx=h, delta=3.015 * h, mls=1, npt=1, fam_ptr=rp, fam_col=col, broken=br,
+                 cb_ptr=cp, cb_idx=ci, bdry_eff=dm.bdry_eff(), mat=mat, mat_spring=[q["spring"] for q in mats],
+                 mat_ecrit=[q["ecrit"] for q in mats], mat_density=[q["density"] for q in mats],
+                 mat_ymod=[72e9] * len(mats), bc=bc, bc_type=[b["type"] for b in bcs],
+                 bc_dir=[d for b in bcs for d in b["dir"]], bc_val=[v for b in bcs for v in b["value"]],
+                 bc_end=[b["end_time"] for b in bcs], bc_load=[b["load_type"] for b in bcs], U=u)
+    L = OL.lib()
+    L.or_ai_force_stage.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 6 + [C.c_double, C.c_double,
+                                                                              C.c_void_p, C.c_void_p]
+    brk = np.ascontiguousarray(br, np.uint8).copy()
+    dmg = np.zeros(n, np.int32)
+    k = np.zeros(3 * n)
+    tp = np.ascontiguousarray(tp, np.int64)
+    tc = np.ascontiguousarray(tc, np.float64)
+    t0 = time.perf_counter()
+    L.or_ai_force_stage(C.addressof(m.m), trap, ptr.ctypes.data, C.addressof(regs), tp.ctypes.data, tc.ctypes.data,
+                        brk.ctypes.data, dmg.ctypes.data, 1e-8, 1e-8, u.ctypes.data, k.ctypes.data)
+    return time.perf_counter() - t0
+
+
+def run_ai(args):
+    """--form ai: the adaptive-trapezoid (ai_on) form, FP64 drop-in, on the
+    20x10x10 bar: W + K device RK4 steps (graph of one step), trapezoid-point
+    force evaluations per second, against one stage of the oracle port."""
+    import torch
+    import pdmtel_b200 as P
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp(prefix="pdai_")
+    dims = (20, 10, 10)
+    ai_deck(dims).write(tmp)
+    t0 = time.perf_counter()
+    dm = P.pdDataManager(tmp)
+    P.pdSolve.InitialProblem(dm)
+    ctx = dm.context()
+    setup_s = time.perf_counter() - t0
+    dt = 1e-8
+    ctx.rk4_steps(dt, 0.0, args.warmup)
+    ctx.sync()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.rk4_steps(dt, args.warmup * dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    pts = 4 * ctx.evals_per_stage()
+    cpu_stage = None if args.no_cpu_baseline else ai_oracle_stage_seconds(dm, dims)
+    line = {"form": "ai", "metric": "AI trapezoid-point force evaluations per second (FP64 drop-in)",
+            "value": pts / (ms / 1e3), "unit": "point evals/s", "ms_per_step": ms, "steps": args.steps,
+            "warmup": args.warmup, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "bar 20x10x10, spacing 1 mm, horizon 3.015 spacings, ai_on with MLS, "
+                                   "trapezoid index 3", "nodes": ctx.n, "points_per_step": pts},
+            "setup_s": setup_s}
+    if cpu_stage is not None:
+        line["cpu_baseline"] = {"value": pts / 4 / cpu_stage, "unit": "point evals/s", "cores": 1, "kind": "port",
+                                "sample": "one force stage of the oracle port on the same deck",
+                                "s_per_step": 4 * cpu_stage}
+    print(json.dumps(line))
+    dm.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 def run_adjoint(args):
     """--form adjoint: the adjoint pair alone (profiler captures)."""
     import torch
@@ -912,7 +1010,7 @@ def main():
                          "force_tile)")
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--form", default="precision",
-                    choices=["precision", "batch", "static", "identify", "accuracy", "steps", "adjoint"])
+                    choices=["precision", "batch", "static", "identify", "accuracy", "steps", "adjoint", "ai"])
     ap.add_argument("--plate-dims", default="400x400x4", help="plate lattice of the precision/steps forms")
     ap.add_argument("--prec", default="fp32c", choices=["fp32c", "fp64"], help="arithmetic of --form steps")
     ap.add_argument("--cube", type=int, default=128, help="cube side of --form static")
@@ -941,6 +1039,8 @@ def main():
         return run_steps(args)
     if args.form == "adjoint":
         return run_adjoint(args)
+    if args.form == "ai":
+        return run_ai(args)
     return run_ours(args)
 
 

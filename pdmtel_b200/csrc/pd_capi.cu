@@ -12,6 +12,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "pd_ai_eval.h"
 #include "pd_internal.cuh"
 
 namespace pd {
@@ -126,6 +127,7 @@ struct pd_ctx {
     int64_t adj_pool_count = 0;
     bool have_family = false, have_mls = false;
     bool have_ai = false;                   // pd_set_ai data for the current family
+    int64_t ai_points = 0;                  // trapezoid points of the unbroken bonds per stage
     std::vector<void*> ai_bufs;             // device buffers of the AI form
     std::vector<int32_t> bctype_host;       // per bc: its type
     // owned device buffers
@@ -1327,7 +1329,24 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     }
     std::vector<int64_t> frow(N + 1);
     std::vector<int32_t> fcol(std::max<int64_t>(H, 1));
-    PD_TRY(pd_get_family(c, frow.data(), fcol.data(), nullptr));
+    std::vector<uint8_t> fbr(std::max<int64_t>(H, 1));
+    PD_TRY(pd_get_family(c, frow.data(), fcol.data(), fbr.data()));
+    // points per stage of the unbroken bonds (the work of one force stage)
+    int64_t points = 0;
+    {
+        struct Count {
+            void operator()(const double*, int, double* f) const { f[0] = f[1] = f[2] = 0.0; }
+        } none;
+        for (int64_t i = 0; i < N; ++i)
+            for (int64_t p = frow[i]; p < frow[i + 1]; ++p) {
+                if (fbr[p]) continue;
+                const int64_t j = fcol[p];
+                double xj[3], f[3];
+                for (int a = 0; a < 3; ++a) xj[a] = c->coords[3 * j + a] - c->coords[3 * i + a];
+                for (int64_t r = reg_ptr[p]; r < reg_ptr[p + 1]; ++r)
+                    points += pd_ai::region(regions[r], c->d.ai_n, xj, c->d.delta, c->d.dx, none, f);
+            }
+    }
     std::vector<int32_t> row(std::max<int64_t>(H, 1));
     std::vector<int64_t> mirror(std::max<int64_t>(H, 1));
     for (int64_t i = 0; i < N; ++i)
@@ -1434,6 +1453,7 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     d.cbptr = cbp;
     d.cbidx = cbi;
     c->have_ai = true;
+    c->ai_points = points;
     c->generation++;
     return PD_OK;
 }
@@ -1947,6 +1967,11 @@ int pd_profile_step(pd_ctx* c, double dt, double time, double* ms) {
 int pd_evals_per_stage(pd_ctx* c, int64_t* ev) {
     if (!c || !ev) return fail(PD_ERR_ARG, "pd_evals_per_stage: null argument");
     if (!c->have_family) return fail(PD_ERR_ARG, "pd_evals_per_stage: no family");
+    if (c->d.ai) {
+        if (!c->have_ai) return fail(PD_ERR_ARG, "pd_evals_per_stage: no AI data");
+        *ev = c->ai_points;  // trapezoid points of the unbroken bonds
+        return PD_OK;
+    }
     *ev = c->d.cci ? c->Ha : c->Ha * c->npt;
     return PD_OK;
 }
