@@ -122,7 +122,7 @@ struct ForceFn {
     }
 };
 
-__device__ __noinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, int64_t j, const double* ui, double t, bool energy,
+__device__ __forceinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, int64_t j, const double* ui, double t, bool energy,
                           double F[3], int* fail, double* eacc) {
     const int64_t N = d.n;
     const MatDev& Mi = d.mats[d.mat[i]];
