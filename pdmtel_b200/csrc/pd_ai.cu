@@ -15,9 +15,12 @@
 //               same, so it is formed once per entry here and read by every
 //               bond to the node);
 //  k_ai_bond    one thread per full-family entry i -> j: the bond's force and
-//               the count of its points past the critical stretch;
+//               the count of its points past the critical stretch; with the
+//               energy on, every point's energy term in the bond's slots of a
+//               per-point buffer (0.0 for a failed point);
 //  k_ai_sum     one thread per node: the velocity update bond by bond in
-//               family order.  A failing point breaks the bond object the two
+//               family order, and the energy terms added point by point in
+//               the reference's order (a sequential sum, formed exactly).  A failing point breaks the bond object the two
 //               nodes share (pdIntgManager2.cpp:301-308), and the reference
 //               visits node i's bonds after those of every lower node: a bond
 //               to a lower node j is skipped when j's evaluation of it failed
@@ -68,8 +71,8 @@ struct ForceFn {
     const BcDev* B;      // node j's boundary condition or null
     double fac;
     int fail;
-    double eacc;
-    bool energy;
+    double* ebuf;        // the bond's energy terms, point by point (or null)
+    int64_t q;
 
     __device__ void operator()(const double* p, int k, double* f) {
         double eta[3];
@@ -114,16 +117,17 @@ struct ForceFn {
             f[0] = t * y0 / pl;
             f[1] = t * y1 / pl;
             f[2] = t * y2 / pl;
-            if (energy) eacc += be * 0.5 * (0.5 * 1.0 * (c / r) * u * u);
+            if (ebuf) ebuf[q++] = be * 0.5 * (0.5 * 1.0 * (c / r) * u * u);
         } else {
             f[0] = f[1] = f[2] = 0.0;
             ++fail;
+            if (ebuf) ebuf[q++] = 0.0;
         }
     }
 };
 
-__device__ __forceinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, int64_t j, const double* ui, double t, bool energy,
-                          double F[3], int* fail, double* eacc) {
+__device__ __forceinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, int64_t j, const double* ui, double t,
+                                          double* ebuf, double F[3], int* fail) {
     const int64_t N = d.n;
     const MatDev& Mi = d.mats[d.mat[i]];
     const MatDev& Mj = d.mats[d.mat[j]];
@@ -148,12 +152,11 @@ __device__ __forceinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, in
         fn.K = 0;
     }
     fn.fail = 0;
-    fn.eacc = energy ? *eacc : 0.0;
-    fn.energy = energy;
+    fn.ebuf = ebuf;
+    fn.q = 0;
     const double xj[3] = {d.x[j] - d.x[i], d.x[N + j] - d.x[N + i], d.x[2 * N + j] - d.x[2 * N + i]};
     pd_ai::bond(d.ai_reg, d.ai_rptr[p], d.ai_rptr[p + 1], d.ai_n, xj, d.delta, d.dx, fn, F);
     *fail = fn.fail;
-    if (energy) *eacc = fn.eacc;
 }
 
 __device__ __forceinline__ void node_u(const Dev& d, int64_t i, double* u) {
@@ -164,9 +167,11 @@ __device__ __forceinline__ void node_u(const Dev& d, int64_t i, double* u) {
     u[2] = src[2 * N + i];
 }
 
+template <bool ENERGY>
 __global__ void __launch_bounds__(128) k_ai_bond(Dev d) {
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= d.ai_nent) return;
+    const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (w >= d.ai_nent) return;
+    const int64_t p = d.ai_order[w];
     if (d.ai_brk[p]) {
         d.ai_fail[p] = 0;
         return;
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(128) k_ai_bond(Dev d) {
     double ui[3], F[3];
     node_u(d, i, ui);
     int fail = 0;
-    eval_bond(d, p, i, j, ui, *d.tdev, false, F, &fail, nullptr);
+    eval_bond(d, p, i, j, ui, *d.tdev, ENERGY ? d.ai_e + d.ai_eptr[p] : nullptr, F, &fail);
     d.ai_F[3 * p] = F[0];
     d.ai_F[3 * p + 1] = F[1];
     d.ai_F[3 * p + 2] = F[2];
@@ -193,9 +198,6 @@ __global__ void k_ai_sum(Dev d, double dts) {
     double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
     double eacc = ENERGY ? d.eed[i] : 0.0;
     int dmg = d.ai_dmg[i];
-    double ui[3];
-    if (ENERGY) node_u(d, i, ui);
-    const double t = *d.tdev;
     const int64_t pe = d.frow[i + 1];
     for (int64_t p = d.frow[i]; p < pe; ++p) {
         if (d.ai_brk[p]) continue;
@@ -205,14 +207,10 @@ __global__ void k_ai_sum(Dev d, double dts) {
             d.ai_brk[p] = 1;  // broken by node j's visit of this bond in this stage
             continue;
         }
-        double F[3];
+        const double F[3] = {d.ai_F[3 * p], d.ai_F[3 * p + 1], d.ai_F[3 * p + 2]};
         if (ENERGY) {
-            int fail = 0;
-            eval_bond(d, p, i, j, ui, t, true, F, &fail, &eacc);
-        } else {
-            F[0] = d.ai_F[3 * p];
-            F[1] = d.ai_F[3 * p + 1];
-            F[2] = d.ai_F[3 * p + 2];
+            const int64_t e1 = d.ai_eptr[p + 1];
+            for (int64_t e = d.ai_eptr[p]; e < e1; ++e) eacc += d.ai_e[e];
         }
         dmg += d.ai_fail[p];
         v0 += (F[0] + b0) * dts / rho;
@@ -238,7 +236,10 @@ void launch_ai_gather(const Dev& d, const double* us, cudaStream_t s) {
 
 void launch_ai_force(const Dev& d, double dts, cudaStream_t s) {
     if (d.n == 0) return;
-    if (d.ai_nent > 0) k_ai_bond<<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
+    if (d.ai_nent > 0) {
+        if (d.energy) k_ai_bond<true><<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
+        else k_ai_bond<false><<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
+    }
     if (d.energy) k_ai_sum<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
     else k_ai_sum<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
 }

@@ -1331,22 +1331,35 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     std::vector<int32_t> fcol(std::max<int64_t>(H, 1));
     std::vector<uint8_t> fbr(std::max<int64_t>(H, 1));
     PD_TRY(pd_get_family(c, frow.data(), fcol.data(), fbr.data()));
-    // points per stage of the unbroken bonds (the work of one force stage)
+    // trapezoid points of every entry: the energy slots, and the work of
+    // one force stage (the unbroken entries)
     int64_t points = 0;
+    std::vector<int64_t> eptr(H + 1, 0);
     {
         struct Count {
             void operator()(const double*, int, double* f) const { f[0] = f[1] = f[2] = 0.0; }
         } none;
         for (int64_t i = 0; i < N; ++i)
             for (int64_t p = frow[i]; p < frow[i + 1]; ++p) {
-                if (fbr[p]) continue;
                 const int64_t j = fcol[p];
                 double xj[3], f[3];
+                int64_t np = 0;
                 for (int a = 0; a < 3; ++a) xj[a] = c->coords[3 * j + a] - c->coords[3 * i + a];
                 for (int64_t r = reg_ptr[p]; r < reg_ptr[p + 1]; ++r)
-                    points += pd_ai::region(regions[r], c->d.ai_n, xj, c->d.delta, c->d.dx, none, f);
+                    np += pd_ai::region(regions[r], c->d.ai_n, xj, c->d.delta, c->d.dx, none, f);
+                eptr[p + 1] = eptr[p] + np;
+                if (!fbr[p]) points += np;
             }
     }
+    // work order of the bond kernel: entries grouped by region count and
+    // points, so the threads of a warp walk the same loop structure
+    std::vector<int32_t> order(std::max<int64_t>(H, 1));
+    for (int64_t p = 0; p < H; ++p) order[p] = (int32_t)p;
+    std::stable_sort(order.begin(), order.begin() + H, [&](int32_t a, int32_t b) {
+        const int64_t ra = reg_ptr[a + 1] - reg_ptr[a], rb = reg_ptr[b + 1] - reg_ptr[b];
+        if (ra != rb) return ra > rb;
+        return (eptr[a + 1] - eptr[a]) > (eptr[b + 1] - eptr[b]);
+    });
     std::vector<int32_t> row(std::max<int64_t>(H, 1));
     std::vector<int64_t> mirror(std::max<int64_t>(H, 1));
     for (int64_t i = 0; i < N; ++i)
@@ -1392,7 +1405,8 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     int64_t *rptr = nullptr, *mir = nullptr, *tptr = nullptr, *cof = nullptr, *cbp = nullptr;
     int32_t *rw = nullptr, *tn = nullptr, *cbi = nullptr, *fl = nullptr, *dmg = nullptr;
     pd_ai_region* reg = nullptr;
-    double *tco = nullptr, *au = nullptr, *F = nullptr;
+    double *tco = nullptr, *au = nullptr, *F = nullptr, *ae = nullptr;
+    int64_t* ep = nullptr;
     uint8_t* brk = nullptr;
     int* err = nullptr;
     auto track = [&](void* q) { c->ai_bufs.push_back(q); };
@@ -1405,6 +1419,12 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     PD_TRY(dalloc(c, &brk, H)); track(brk);
     PD_TRY(dalloc(c, &dmg, N)); track(dmg);
     PD_TRY(dalloc(c, &err, 1)); track(err);
+    PD_TRY(dalloc(c, &ep, H + 1)); track(ep);
+    int32_t* ord = nullptr;
+    PD_TRY(dalloc(c, &ord, H)); track(ord);
+    if (H) PD_TRY(upload(c, ord, order.data(), sizeof(int32_t) * H));
+    PD_TRY(dalloc(c, &ae, eptr[H])); track(ae);
+    PD_TRY(upload(c, ep, eptr.data(), sizeof(int64_t) * (H + 1)));
     PD_TRY(upload(c, rptr, reg_ptr, sizeof(int64_t) * (H + 1)));
     if (R) PD_TRY(upload(c, reg, regions, sizeof(pd_ai_region) * R));
     if (H) {
@@ -1445,6 +1465,9 @@ int pd_set_ai(pd_ctx* c, int mls, const int64_t* reg_ptr, const pd_ai_region* re
     d.ai_brk = brk;
     d.ai_dmg = dmg;
     d.ai_err = err;
+    d.ai_eptr = ep;
+    d.ai_order = ord;
+    d.ai_e = ae;
     d.ai_tptr = tptr;
     d.ai_coff = cof;
     d.ai_tnode = tn;

@@ -165,6 +165,9 @@ struct Dev {
     uint8_t* ai_brk;              // [H] broken: an AI bond breaks for good
     int32_t* ai_dmg;              // [N] failed points of the step (pdNode's damaged-bond count)
     int* ai_err;                  // a table entry out of range was asked for
+    const int64_t* ai_eptr;       // [H+1] per-point energy slots of each entry (its trapezoid points)
+    double* ai_e;                 // energy term of every point of the stage
+    const int32_t* ai_order;      // [H] entries in the bond kernel's work order
 };
 
 // kernel launchers (pd_exact.cu: compiled without FMA contraction)
