@@ -18,9 +18,11 @@
 //               the count of its points past the critical stretch; with the
 //               energy on, every point's energy term in the bond's slots of a
 //               per-point buffer (0.0 for a failed point);
-//  k_ai_sum     one thread per node: the velocity update bond by bond in
-//               family order, and the energy terms added point by point in
-//               the reference's order (a sequential sum, formed exactly).  A failing point breaks the bond object the two
+//  k_ai_sum     one thread per node (one warp with the energy on,
+//               k_ai_sum_energy): the velocity update bond by bond in family
+//               order, and the energy terms added point by point in the
+//               reference's order (a sequential sum, formed exactly).
+//               A failing point breaks the bond object the two
 //               nodes share (pdIntgManager2.cpp:301-308), and the reference
 //               visits node i's bonds after those of every lower node: a bond
 //               to a lower node j is skipped when j's evaluation of it failed
@@ -187,7 +189,6 @@ __global__ void __launch_bounds__(128) k_ai_bond(Dev d) {
     d.ai_fail[p] = fail;
 }
 
-template <bool ENERGY>
 __global__ void k_ai_sum(Dev d, double dts) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= d.n) return;
@@ -196,7 +197,6 @@ __global__ void k_ai_sum(Dev d, double dts) {
     const double rho = Mi.density;
     const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
     double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
-    double eacc = ENERGY ? d.eed[i] : 0.0;
     int dmg = d.ai_dmg[i];
     const int64_t pe = d.frow[i + 1];
     for (int64_t p = d.frow[i]; p < pe; ++p) {
@@ -208,10 +208,6 @@ __global__ void k_ai_sum(Dev d, double dts) {
             continue;
         }
         const double F[3] = {d.ai_F[3 * p], d.ai_F[3 * p + 1], d.ai_F[3 * p + 2]};
-        if (ENERGY) {
-            const int64_t e1 = d.ai_eptr[p + 1];
-            for (int64_t e = d.ai_eptr[p]; e < e1; ++e) eacc += d.ai_e[e];
-        }
         dmg += d.ai_fail[p];
         v0 += (F[0] + b0) * dts / rho;
         v1 += (F[1] + b1) * dts / rho;
@@ -222,7 +218,61 @@ __global__ void k_ai_sum(Dev d, double dts) {
     d.vbuf[N + i] = v1;
     d.vbuf[2 * N + i] = v2;
     d.ai_dmg[i] = dmg;
-    if (ENERGY) d.eed[i] = eacc;
+}
+
+// With the energy on: one warp per node.  The warp streams each counted
+// bond's energy terms 32 at a time through shared memory and lane 0 adds
+// them in point order (the reference's sequential sum), so the memory reads
+// are coalesced while the sum stays exact; lane 0 also does the velocity
+// update and the break bookkeeping of k_ai_sum.
+__global__ void __launch_bounds__(128) k_ai_sum_energy(Dev d, double dts) {
+    __shared__ double buf[4][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (i >= d.n) return;
+    const int64_t N = d.n;
+    const MatDev Mi = d.mats[d.mat[i]];
+    const double rho = Mi.density;
+    const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
+    double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
+    double eacc = d.eed[i];
+    int dmg = d.ai_dmg[i];
+    const int64_t pe = d.frow[i + 1];
+    for (int64_t p = d.frow[i]; p < pe; ++p) {
+        if (d.ai_brk[p]) continue;
+        const int64_t j = d.fcol[p];
+        const int64_t q = d.ai_mirror[p];
+        __syncwarp();
+        if (j < i && d.ai_fail[q] > 0) {
+            if (lane == 0) d.ai_brk[p] = 1;
+            continue;
+        }
+        const int64_t e0 = d.ai_eptr[p], e1 = d.ai_eptr[p + 1];
+        for (int64_t base = e0; base < e1; base += 32) {
+            const int64_t e = base + lane;
+            buf[wib][lane] = e < e1 ? d.ai_e[e] : 0.0;
+            __syncwarp();
+            if (lane == 0) {
+                const int m = (e1 - base) < 32 ? (int)(e1 - base) : 32;
+                for (int k = 0; k < m; ++k) eacc += buf[wib][k];
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            dmg += d.ai_fail[p];
+            v0 += (d.ai_F[3 * p] + b0) * dts / rho;
+            v1 += (d.ai_F[3 * p + 1] + b1) * dts / rho;
+            v2 += (d.ai_F[3 * p + 2] + b2) * dts / rho;
+            if (d.ai_fail[p] > 0 || (j > i && d.ai_fail[q] > 0)) d.ai_brk[p] = 1;
+        }
+    }
+    if (lane == 0) {
+        d.vbuf[i] = v0;
+        d.vbuf[N + i] = v1;
+        d.vbuf[2 * N + i] = v2;
+        d.ai_dmg[i] = dmg;
+        d.eed[i] = eacc;
+    }
 }
 
 inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -240,8 +290,8 @@ void launch_ai_force(const Dev& d, double dts, cudaStream_t s) {
         if (d.energy) k_ai_bond<true><<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
         else k_ai_bond<false><<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
     }
-    if (d.energy) k_ai_sum<true><<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
-    else k_ai_sum<false><<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
+    if (d.energy) k_ai_sum_energy<<<blocks_for(32 * d.n, 128), 128, 0, s>>>(d, dts);
+    else k_ai_sum<<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
 }
 
 }  // namespace pd
