@@ -176,6 +176,8 @@ __global__ void __launch_bounds__(128) k_ai_bond(Dev d) {
     const int64_t p = d.ai_order[w];
     if (d.ai_brk[p]) {
         d.ai_fail[p] = 0;
+        if (ENERGY)  // no terms: the node's sum streams over these slots
+            for (int64_t e = d.ai_eptr[p]; e < d.ai_eptr[p + 1]; ++e) d.ai_e[e] = 0.0;
         return;
     }
     const int64_t i = d.ai_row[p], j = d.fcol[p];
@@ -220,59 +222,92 @@ __global__ void k_ai_sum(Dev d, double dts) {
     d.ai_dmg[i] = dmg;
 }
 
-// With the energy on: one warp per node.  The warp streams each counted
-// bond's energy terms 32 at a time through shared memory and lane 0 adds
-// them in point order (the reference's sequential sum), so the memory reads
-// are coalesced while the sum stays exact; lane 0 also does the velocity
-// update and the break bookkeeping of k_ai_sum.
+// With the energy on: one warp per node.  The node's energy terms are
+// contiguous (its entries' slots in family order; k_ai_bond zeroes the slots
+// of bonds broken before the stage, and adding +0.0 to a non-negative sum
+// changes nothing), so the warp streams them 128 at a time through shared
+// memory, the next round's loads in flight while lane 0 adds the current
+// round in point order: the reference's sequential sum, formed exactly.  A
+// node with a bond its lower node broke in this stage (rare) takes the terms
+// bond by bond instead.  Lane 0 then does the velocity update and the break
+// bookkeeping of k_ai_sum.
 __global__ void __launch_bounds__(128) k_ai_sum_energy(Dev d, double dts) {
-    __shared__ double buf[4][32];
+    constexpr int kRound = 128;
+    __shared__ double buf[4][2][kRound];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (i >= d.n) return;
     const int64_t N = d.n;
+    const int64_t pb = d.frow[i], pe = d.frow[i + 1];
+    // a bond skipped because node j's visit of it failed in this stage?
+    int skip = 0;
+    for (int64_t p = pb + lane; p < pe; p += 32) {
+        const int64_t j = d.fcol[p];
+        if (!d.ai_brk[p] && j < i && d.ai_fail[d.ai_mirror[p]] > 0) skip = 1;
+    }
+    skip = __any_sync(0xffffffffu, skip);
+    double eacc = d.eed[i];
+    auto stream = [&](int64_t E0, int64_t E1) {
+        double nxt[kRound / 32];
+#pragma unroll
+        for (int u = 0; u < kRound / 32; ++u) {
+            const int64_t e = E0 + 32 * u + lane;
+            nxt[u] = e < E1 ? d.ai_e[e] : 0.0;
+        }
+        int cur = 0;
+        for (int64_t base = E0; base < E1; base += kRound) {
+#pragma unroll
+            for (int u = 0; u < kRound / 32; ++u) buf[wib][cur][32 * u + lane] = nxt[u];
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < kRound / 32; ++u) {
+                const int64_t e = base + kRound + 32 * u + lane;
+                nxt[u] = e < E1 ? d.ai_e[e] : 0.0;
+            }
+            if (lane == 0) {
+                const int m = (E1 - base) < kRound ? (int)(E1 - base) : kRound;
+                const double* b = buf[wib][cur];
+                for (int k = 0; k < m; ++k) eacc += b[k];
+            }
+            cur ^= 1;
+        }
+        __syncwarp();
+    };
+    if (!skip) {
+        stream(d.ai_eptr[pb], d.ai_eptr[pe]);
+    } else {
+        for (int64_t p = pb; p < pe; ++p) {
+            if (d.ai_brk[p]) continue;
+            const int64_t j = d.fcol[p];
+            if (j < i && d.ai_fail[d.ai_mirror[p]] > 0) continue;
+            stream(d.ai_eptr[p], d.ai_eptr[p + 1]);
+        }
+    }
+    if (lane != 0) return;
     const MatDev Mi = d.mats[d.mat[i]];
     const double rho = Mi.density;
     const double b0 = Mi.grav[0] * rho, b1 = Mi.grav[1] * rho, b2 = Mi.grav[2] * rho;
     double v0 = d.vbuf[i], v1 = d.vbuf[N + i], v2 = d.vbuf[2 * N + i];
-    double eacc = d.eed[i];
     int dmg = d.ai_dmg[i];
-    const int64_t pe = d.frow[i + 1];
-    for (int64_t p = d.frow[i]; p < pe; ++p) {
+    for (int64_t p = pb; p < pe; ++p) {
         if (d.ai_brk[p]) continue;
         const int64_t j = d.fcol[p];
         const int64_t q = d.ai_mirror[p];
-        __syncwarp();
         if (j < i && d.ai_fail[q] > 0) {
-            if (lane == 0) d.ai_brk[p] = 1;
+            d.ai_brk[p] = 1;  // broken by node j's visit of this bond in this stage
             continue;
         }
-        const int64_t e0 = d.ai_eptr[p], e1 = d.ai_eptr[p + 1];
-        for (int64_t base = e0; base < e1; base += 32) {
-            const int64_t e = base + lane;
-            buf[wib][lane] = e < e1 ? d.ai_e[e] : 0.0;
-            __syncwarp();
-            if (lane == 0) {
-                const int m = (e1 - base) < 32 ? (int)(e1 - base) : 32;
-                for (int k = 0; k < m; ++k) eacc += buf[wib][k];
-            }
-            __syncwarp();
-        }
-        if (lane == 0) {
-            dmg += d.ai_fail[p];
-            v0 += (d.ai_F[3 * p] + b0) * dts / rho;
-            v1 += (d.ai_F[3 * p + 1] + b1) * dts / rho;
-            v2 += (d.ai_F[3 * p + 2] + b2) * dts / rho;
-            if (d.ai_fail[p] > 0 || (j > i && d.ai_fail[q] > 0)) d.ai_brk[p] = 1;
-        }
+        dmg += d.ai_fail[p];
+        v0 += (d.ai_F[3 * p] + b0) * dts / rho;
+        v1 += (d.ai_F[3 * p + 1] + b1) * dts / rho;
+        v2 += (d.ai_F[3 * p + 2] + b2) * dts / rho;
+        if (d.ai_fail[p] > 0 || (j > i && d.ai_fail[q] > 0)) d.ai_brk[p] = 1;
     }
-    if (lane == 0) {
-        d.vbuf[i] = v0;
-        d.vbuf[N + i] = v1;
-        d.vbuf[2 * N + i] = v2;
-        d.ai_dmg[i] = dmg;
-        d.eed[i] = eacc;
-    }
+    d.vbuf[i] = v0;
+    d.vbuf[N + i] = v1;
+    d.vbuf[2 * N + i] = v2;
+    d.ai_dmg[i] = dmg;
+    d.eed[i] = eacc;
 }
 
 inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
