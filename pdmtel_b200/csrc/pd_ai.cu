@@ -14,7 +14,7 @@
 //               forms it point by point inside the integrand; the sum is the
 //               same, so it is formed once per entry here and read by every
 //               bond to the node);
-//  k_ai_bond    one thread per full-family entry i -> j: the bond's force and
+//  k_ai_bond    one warp per full-family entry i -> j: the bond's force and
 //               the count of its points past the critical stretch; with the
 //               energy on, every point's energy term in the bond's slots of a
 //               per-point buffer (0.0 for a failed point);
@@ -62,7 +62,10 @@ __global__ void k_ai_gather(Dev d, const double* __restrict__ us) {
     d.ai_u[3 * e + 2] = a2;
 }
 
-// the integrand at one trapezoid point of bond i -> j
+// The integrand at one trapezoid point of bond i -> j: the force density into
+// f, the energy term into *e (0.0 for a point past the critical stretch);
+// returns 1 for such a point.  k: the point's index in its region (the entry
+// of node j's MLS list the reference reads).
 struct ForceFn {
     const Dev* d;
     double ui[3];
@@ -72,11 +75,8 @@ struct ForceFn {
     int64_t K;
     const BcDev* B;      // node j's boundary condition or null
     double fac;
-    int fail;
-    double* ebuf;        // the bond's energy terms, point by point (or null)
-    int64_t q;
 
-    __device__ void operator()(const double* p, int k, double* f) {
+    __device__ int eval(const double* p, int k, double* f, double* e) const {
         double eta[3];
         if (d->ai_mls) {
             double u[3];
@@ -119,47 +119,14 @@ struct ForceFn {
             f[0] = t * y0 / pl;
             f[1] = t * y1 / pl;
             f[2] = t * y2 / pl;
-            if (ebuf) ebuf[q++] = be * 0.5 * (0.5 * 1.0 * (c / r) * u * u);
-        } else {
-            f[0] = f[1] = f[2] = 0.0;
-            ++fail;
-            if (ebuf) ebuf[q++] = 0.0;
+            *e = be * 0.5 * (0.5 * 1.0 * (c / r) * u * u);
+            return 0;
         }
+        f[0] = f[1] = f[2] = 0.0;
+        *e = 0.0;
+        return 1;
     }
 };
-
-__device__ __forceinline__ void eval_bond(const Dev& d, int64_t p, int64_t i, int64_t j, const double* ui, double t,
-                                          double* ebuf, double F[3], int* fail) {
-    const int64_t N = d.n;
-    const MatDev& Mi = d.mats[d.mat[i]];
-    const MatDev& Mj = d.mats[d.mat[j]];
-    ForceFn fn;
-    fn.d = &d;
-    for (int a = 0; a < 3; ++a) fn.ui[a] = ui[a];
-    fn.xi[0] = d.x[i];
-    fn.xi[1] = d.x[N + i];
-    fn.xi[2] = d.x[2 * N + i];
-    fn.ecrit = dmin(Mi.ecrit, Mj.ecrit);
-    fn.c = dmin(Mi.spring, Mj.spring);
-    if (d.sfac) fn.c = fn.c * (0.5 * (d.sfac[i] + d.sfac[j]));
-    fn.be = 0.5 * (d.bdry[i] + d.bdry[j]);
-    const int b = d.bc[j];
-    fn.B = b >= 0 ? &d.bcs[b] : nullptr;
-    fn.fac = b >= 0 ? bc_time_factor(d.bcs[b], t) : 0.0;
-    if (d.ai_mls) {
-        fn.tab = d.ai_u + 3 * d.ai_tptr[j];
-        fn.K = d.ai_tptr[j + 1] - d.ai_tptr[j];
-    } else {
-        fn.tab = nullptr;
-        fn.K = 0;
-    }
-    fn.fail = 0;
-    fn.ebuf = ebuf;
-    fn.q = 0;
-    const double xj[3] = {d.x[j] - d.x[i], d.x[N + j] - d.x[N + i], d.x[2 * N + j] - d.x[2 * N + i]};
-    pd_ai::bond(d.ai_reg, d.ai_rptr[p], d.ai_rptr[p + 1], d.ai_n, xj, d.delta, d.dx, fn, F);
-    *fail = fn.fail;
-}
 
 __device__ __forceinline__ void node_u(const Dev& d, int64_t i, double* u) {
     const int64_t N = d.n;
@@ -169,26 +136,174 @@ __device__ __forceinline__ void node_u(const Dev& d, int64_t i, double* u) {
     u[2] = src[2 * N + i];
 }
 
+constexpr int kAiWarps = 4;  // warps per block of k_ai_bond
+
+// One warp per bond, region by region.  Lane r < np^2 owns row r = (k, l) of
+// the region (outer point k, middle point l): its limits, whether its inner
+// interval is empty, and by a warp prefix sum the region index of its first
+// point.  The np^3 points are then spread over the lanes, each point's
+// integrand written to shared memory; the row, middle and outer trapezoid
+// sums follow in the order of pdIntgManager::CalcTrapzdQuad (lane = row,
+// lane = outer point, lane 0), so the integral is the serial one bit for bit.
 template <bool ENERGY>
 __global__ void __launch_bounds__(128) k_ai_bond(Dev d) {
-    const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    using namespace pd_ai;
+    constexpr unsigned full = 0xffffffffu;
+    __shared__ double sf[kAiWarps][kMaxRegionPoints][3];
+    __shared__ double sh[kAiWarps][kMaxPerDir * kMaxPerDir][3];
+    __shared__ double sg[kAiWarps][kMaxPerDir][3];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (w >= d.ai_nent) return;
     const int64_t p = d.ai_order[w];
     if (d.ai_brk[p]) {
-        d.ai_fail[p] = 0;
+        if (lane == 0) d.ai_fail[p] = 0;
         if (ENERGY)  // no terms: the node's sum streams over these slots
-            for (int64_t e = d.ai_eptr[p]; e < d.ai_eptr[p + 1]; ++e) d.ai_e[e] = 0.0;
+            for (int64_t e = d.ai_eptr[p] + lane; e < d.ai_eptr[p + 1]; e += 32) d.ai_e[e] = 0.0;
         return;
     }
+    const int64_t N = d.n;
     const int64_t i = d.ai_row[p], j = d.fcol[p];
-    double ui[3], F[3];
-    node_u(d, i, ui);
+    const double t_now = *d.tdev;
+    ForceFn fn;
+    fn.d = &d;
+    node_u(d, i, fn.ui);
+    fn.xi[0] = d.x[i];
+    fn.xi[1] = d.x[N + i];
+    fn.xi[2] = d.x[2 * N + i];
+    const MatDev& Mi = d.mats[d.mat[i]];
+    const MatDev& Mj = d.mats[d.mat[j]];
+    fn.ecrit = dmin(Mi.ecrit, Mj.ecrit);
+    fn.c = dmin(Mi.spring, Mj.spring);
+    if (d.sfac) fn.c = fn.c * (0.5 * (d.sfac[i] + d.sfac[j]));
+    fn.be = 0.5 * (d.bdry[i] + d.bdry[j]);
+    const int b = d.bc[j];
+    fn.B = b >= 0 ? &d.bcs[b] : nullptr;
+    fn.fac = b >= 0 ? bc_time_factor(d.bcs[b], t_now) : 0.0;
+    fn.tab = d.ai_mls ? d.ai_u + 3 * d.ai_tptr[j] : nullptr;
+    fn.K = d.ai_mls ? d.ai_tptr[j + 1] - d.ai_tptr[j] : 0;
+    const double xj[3] = {d.x[j] - d.x[i], d.x[N + j] - d.x[N + i], d.x[2 * N + j] - d.x[2 * N + i]};
+    const double delta = d.delta, dx = d.dx;
+    const int n = d.ai_n, np = points_per_dir(n), nrow = np * np;
+    double F[3] = {0.0, 0.0, 0.0};
     int fail = 0;
-    eval_bond(d, p, i, j, ui, *d.tdev, ENERGY ? d.ai_e + d.ai_eptr[p] : nullptr, F, &fail);
-    d.ai_F[3 * p] = F[0];
-    d.ai_F[3 * p + 1] = F[1];
-    d.ai_F[3 * p + 2] = F[2];
-    d.ai_fail[p] = fail;
+    int64_t q0 = ENERGY ? d.ai_eptr[p] : 0;
+    const int64_t r0 = d.ai_rptr[p], r1 = d.ai_rptr[p + 1];
+    const bool assign = r1 > r0 && (d.ai_reg[r0].flags & PD_AI_ASSIGN);
+    for (int64_t r = r0; r < r1; ++r) {
+        const pd_ai_region R = d.ai_reg[r];
+        double out[3] = {0.0, 0.0, 0.0};
+        if (!(fabs(R.a - R.b) <= 1.0e-10)) {
+            // rows
+            double t = 0.0, s = 0.0, ml = 0.0, mh = 0.0, zl = 0.0, zh = 0.0;
+            int mid_ok = 0, row_ok = 0;
+            if (lane < nrow) {
+                t = point(n, lane / np, R.a, R.b);
+                ml = mid_limit(R.lim[0], t, xj, delta, dx);
+                mh = mid_limit(R.lim[1], t, xj, delta, dx);
+                mid_ok = !(fabs(ml - mh) <= 1.0e-10);
+                if (mid_ok) {
+                    s = point(n, lane % np, ml, mh);
+                    zl = in_limit(R.lim[2], t, s, xj, delta, dx);
+                    zh = in_limit(R.lim[3], t, s, xj, delta, dx);
+                    row_ok = !(fabs(zl - zh) <= 1.0e-10);
+                }
+            }
+            const int cnt = row_ok ? np : 0;
+            int incl = cnt;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int v = __shfl_up_sync(full, incl, off);
+                if (lane >= off) incl += v;
+            }
+            const int base = incl - cnt;
+            const int total = __shfl_sync(full, incl, 31);
+            // points
+            const int nslot = nrow * np;
+            for (int s0 = 0; s0 < nslot; s0 += 32) {
+                const int slot = s0 + lane;
+                const int row = slot < nslot ? slot / np : 0;
+                const double rt = __shfl_sync(full, t, row), rs = __shfl_sync(full, s, row);
+                const double rzl = __shfl_sync(full, zl, row), rzh = __shfl_sync(full, zh, row);
+                const int rok = __shfl_sync(full, row_ok, row), rbase = __shfl_sync(full, base, row);
+                if (slot < nslot && rok) {
+                    const int m = slot - row * np;
+                    double pp[3], f[3], e;
+                    pp[R.axis[0]] = rt;
+                    pp[R.axis[1]] = rs;
+                    pp[R.axis[2]] = point(n, m, rzl, rzh);
+                    fail += fn.eval(pp, rbase + m, f, &e);
+                    sf[wib][slot][0] = f[0];
+                    sf[wib][slot][1] = f[1];
+                    sf[wib][slot][2] = f[2];
+                    if (ENERGY) d.ai_e[q0 + rbase + m] = e;
+                }
+            }
+            __syncwarp();
+            // inner sums, one lane per row
+            if (lane < nrow) {
+                double h[3] = {0.0, 0.0, 0.0};
+                if (row_ok) {
+                    double acc[3];
+                    for (int m = 0; m < np; ++m) accumulate(m, np, sf[wib][lane * np + m], acc);
+                    const double wgt = scale(n, zl, zh);
+                    h[0] = wgt * acc[0];
+                    h[1] = wgt * acc[1];
+                    h[2] = wgt * acc[2];
+                }
+                sh[wib][lane][0] = h[0];
+                sh[wib][lane][1] = h[1];
+                sh[wib][lane][2] = h[2];
+            }
+            __syncwarp();
+            // middle sums, one lane per outer point (row k np holds its limits)
+            const int src = lane < np ? lane * np : 0;
+            const double kml = __shfl_sync(full, ml, src), kmh = __shfl_sync(full, mh, src);
+            const int kok = __shfl_sync(full, mid_ok, src);
+            if (lane < np) {
+                double g[3] = {0.0, 0.0, 0.0};
+                if (kok) {
+                    double acc[3];
+                    for (int l = 0; l < np; ++l) accumulate(l, np, sh[wib][lane * np + l], acc);
+                    const double wgt = scale(n, kml, kmh);
+                    g[0] = wgt * acc[0];
+                    g[1] = wgt * acc[1];
+                    g[2] = wgt * acc[2];
+                }
+                sg[wib][lane][0] = g[0];
+                sg[wib][lane][1] = g[1];
+                sg[wib][lane][2] = g[2];
+            }
+            __syncwarp();
+            if (lane == 0) {
+                double acc[3];
+                for (int k = 0; k < np; ++k) accumulate(k, np, sg[wib][k], acc);
+                const double wgt = scale(n, R.a, R.b);
+                out[0] = wgt * acc[0];
+                out[1] = wgt * acc[1];
+                out[2] = wgt * acc[2];
+            }
+            __syncwarp();
+            q0 += total;
+        }
+        if (assign) {
+            F[0] = out[0];
+            F[1] = out[1];
+            F[2] = out[2];
+        } else {
+            F[0] = F[0] + out[0];
+            F[1] = F[1] + out[1];
+            F[2] = F[2] + out[2];
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) fail += __shfl_down_sync(full, fail, off);
+    if (lane == 0) {
+        d.ai_F[3 * p] = F[0];
+        d.ai_F[3 * p + 1] = F[1];
+        d.ai_F[3 * p + 2] = F[2];
+        d.ai_fail[p] = fail;
+    }
 }
 
 __global__ void k_ai_sum(Dev d, double dts) {
@@ -267,7 +382,16 @@ __global__ void __launch_bounds__(128) k_ai_sum_energy(Dev d, double dts) {
             if (lane == 0) {
                 const int m = (E1 - base) < kRound ? (int)(E1 - base) : kRound;
                 const double* b = buf[wib][cur];
-                for (int k = 0; k < m; ++k) eacc += b[k];
+                int k = 0;
+                // eight shared-memory loads in flight ahead of the in-order adds
+                for (; k + 8 <= m; k += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) v[u] = b[k + u];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) eacc += v[u];
+                }
+                for (; k < m; ++k) eacc += b[k];
             }
             cur ^= 1;
         }
@@ -322,8 +446,9 @@ void launch_ai_gather(const Dev& d, const double* us, cudaStream_t s) {
 void launch_ai_force(const Dev& d, double dts, cudaStream_t s) {
     if (d.n == 0) return;
     if (d.ai_nent > 0) {
-        if (d.energy) k_ai_bond<true><<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
-        else k_ai_bond<false><<<blocks_for(d.ai_nent, 128), 128, 0, s>>>(d);
+        const unsigned nb = blocks_for(d.ai_nent, kAiWarps);
+        if (d.energy) k_ai_bond<true><<<nb, 32 * kAiWarps, 0, s>>>(d);
+        else k_ai_bond<false><<<nb, 32 * kAiWarps, 0, s>>>(d);
     }
     if (d.energy) k_ai_sum_energy<<<blocks_for(32 * d.n, 128), 128, 0, s>>>(d, dts);
     else k_ai_sum<<<blocks_for(d.n, 128), 128, 0, s>>>(d, dts);
