@@ -1258,15 +1258,21 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
         if (k < nc) cp_async16_pol(r + 32 * k, cf + (int64_t)32 * k, pol);
         cp_async_commit();
     }
-    // trial displacements of contributors k .. k+3, loaded one group ahead
-    double un[4][3];
+    // trial displacements of contributors k .. k+3, loaded one group ahead:
+    // the two threads of a node (lanes 2s, 2s+1: same node, same pattern, the
+    // same loop) each load two of the four (contributors k + 2v + grp) and
+    // swap them with a pair-masked shuffle, so every displacement is loaded
+    // once per node instead of once per thread
+    const unsigned pair = 3u << (threadIdx.x & 30);
+    double mine[2][3];
     auto load_group = [&](int k) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int v = 0; v < 2; ++v) {
+            const int u = 2 * v + grp;
             const int m = (int)i + (k + u < nc ? __ldg(po + k + u) : 0);
-            un[u][0] = __ldg(us + m);
-            un[u][1] = __ldg(us + N + m);
-            un[u][2] = __ldg(us + 2 * N + m);
+            mine[v][0] = __ldg(us + m);
+            mine[v][1] = __ldg(us + N + m);
+            mine[v][2] = __ldg(us + 2 * N + m);
         }
     };
     load_group(0);
@@ -1275,10 +1281,19 @@ __global__ void __launch_bounds__(256, 2) k_gather_f32c_ring(Dev d, const double
     for (int k = 0; k < nc; k += 4) {
         double dd[4][3];
 #pragma unroll
+        for (int v = 0; v < 2; ++v) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double other = __shfl_xor_sync(pair, mine[v][c], 1);
+                dd[2 * v][c] = grp ? other : mine[v][c];
+                dd[2 * v + 1][c] = grp ? mine[v][c] : other;
+            }
+        }
+#pragma unroll
         for (int u = 0; u < 4; ++u) {
-            dd[u][0] = un[u][0] - u0;
-            dd[u][1] = un[u][1] - u1;
-            dd[u][2] = un[u][2] - u2;
+            dd[u][0] -= u0;
+            dd[u][1] -= u1;
+            dd[u][2] -= u2;
         }
         if (k + 4 < nc) load_group(k + 4);
         cp_async_wait<kRing - 4>();  // slots k .. k+3 have landed
