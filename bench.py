@@ -465,7 +465,7 @@ def run_batch(args):
                              "value": ev_step * args.steps / t_other},
             "sequential": {"value": ev_step * args.steps / t_seq, "ms_per_step": 1e3 * t_seq / args.steps,
                            "speedup_batched_over_sequential": t_seq / t_b},
-            "gpu_launches": 1 if bt.persistent else 13 * args.steps,
+            "gpu_launches": 1 if bt.persistent else (13 + (4 if (tune or {}).get("force_stencil") else 0)) * args.steps,
             "clocks": clocks, "setup_s": setup_s}
     print(json.dumps(line))
     shutil.rmtree(tmp, ignore_errors=True)
@@ -954,7 +954,9 @@ def run_ours(args):
         "rel_err_vs_fp64": {"U": err_u, "V": err_v, "after_steps": args.warmup + args.steps},
         "e2e": {"value": ws * evals_step * args.steps / (ms_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 2 * 3 * n * 8, "d2h_bytes_per_step": 2 * 3 * n * 8},
-        "gpu_launches": 13 * args.steps,
+        # per step: 4 stages x (gather, force, epilogue) + the time advance;
+        # the stencil force is two launches (series pass, exact pass)
+        "gpu_launches": (13 + (4 if sten else 0)) * args.steps,
         "roofline": {"bound": "fp32", "kernel": force_kernel, "achieved": force_flops / (force_ms / 1e3) / 1e12,
                      "peak": peak32 / 1e12, "unit": "TFLOP/s",
                      "frac": force_flops / (force_ms / 1e3) / peak32, "traffic": traffic,

@@ -116,6 +116,7 @@ struct pd_ctx {
     int4* fst_u2 = nullptr;
     uint32_t* fst_mask = nullptr;
     float4* fst_tab = nullptr;
+    uint8_t* fst_wide = nullptr;     // stencil force: tiles left to the exact pass (one byte per tile)
     int4* fst_box = nullptr;         // stencil force boxes (dims, first tile) and (first node, first pair)
     longlong2* fst_boxb = nullptr;
     std::vector<int64_t> box_first;  // pd_set_boxes: node ranges that are complete box lattices
@@ -784,6 +785,9 @@ static void fsten_release(pd_ctx* c) {
     dfree(c, c->fst_tab);
     dfree(c, c->fst_box);
     dfree(c, c->fst_boxb);
+    dfree(c, c->fst_wide);
+    c->fst_wide = nullptr;
+    c->d.sten_wide = nullptr;
     c->fst_box = nullptr;
     c->fst_boxb = nullptr;
     c->d.sten_box = nullptr;
@@ -824,6 +828,12 @@ static int fsten_tiles(pd_ctx* c, int by, int bz) {
         if (t > INT32_MAX) return fail(PD_ERR_ARG, "pd_set_option: too many stencil force tiles");
     }
     PD_TRY(upload(c, c->fst_box, bx.data(), sizeof(int4) * bx.size()));
+    dfree(c, c->fst_wide);
+    c->fst_wide = nullptr;
+    c->d.sten_wide = nullptr;
+    PD_TRY(dalloc(c, &c->fst_wide, (size_t)std::max<int64_t>(t, 1)));
+    PD_CUDA_TRY(cudaMemsetAsync(c->fst_wide, 0, (size_t)std::max<int64_t>(t, 1), c->stream));
+    c->d.sten_wide = c->fst_wide;
     c->d.sten_ntiles = t;
     return PD_OK;
 }

@@ -167,9 +167,13 @@ __device__ __forceinline__ void pt_force(float x0, float x1, float x2, float K, 
 
 // The same for two points at once (lo and hi lanes), lane by lane the
 // operations of pt_force; a lane outside the series range takes pt_exact.
-template <bool HASFAIL>
+// SERIES: the series form only, with no branch to the exact form (so the
+// point chains of a bond interleave freely); a lane outside the series range
+// sets *wide, and the caller discards the result and evaluates again without
+// SERIES.
+template <bool HASFAIL, bool SERIES = false>
 __device__ __forceinline__ void pt_force2(f2 x0, f2 x1, f2 x2, f2 K, f2 r2inv, f2 e0, f2 e1, f2 e2, float epsc,
-                                          f2* F) {
+                                          f2* F, bool* wide = nullptr) {
     const f2 y0 = f2_add(x0, e0), y1 = f2_add(x1, e1), y2 = f2_add(x2, e2);
     const f2 dd = f2_fma(e0, f2_add(x0, y0), f2_fma(e1, f2_add(x1, y1), f2_mul(e2, f2_add(x2, y2))));
     const f2 eps = f2_mul(dd, r2inv);
@@ -179,7 +183,9 @@ __device__ __forceinline__ void pt_force2(f2 x0, f2 x1, f2 x2, f2 K, f2 r2inv, f
     f2 h = f2_mul(eps, c);
     float el, eh;
     f2_split(eps, el, eh);
-    if (!(fabsf(el) < kSeriesMax) || !(fabsf(eh) < kSeriesMax)) {
+    if (SERIES) {
+        *wide = *wide | !(fabsf(el) < kSeriesMax) | !(fabsf(eh) < kSeriesMax);
+    } else if (!(fabsf(el) < kSeriesMax) || !(fabsf(eh) < kSeriesMax)) {
         float hl, hh, dl, dh, a0, b0, a1, b1, a2, b2;
         f2_split(h, hl, hh);
         f2_split(dd, dl, dh);
@@ -563,9 +569,10 @@ __global__ void __launch_bounds__(128, 3) k_force_f32c_quad(Dev d, PointPack<8> 
 // bit 1 = node B holds it.  Compiled for both sides together (the lattice
 // interior, where the sides' independent chains interleave) and for each
 // side alone.
-template <bool HASFAIL, bool BDRY, bool SFAC, int SIDES>
+template <bool HASFAIL, bool BDRY, bool SFAC, int SIDES, bool SERIES>
 __device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, int NX, int64_t NXY, const f2* hx,
-                                           const f2* hy, const f2* hz, const float* epsc, float h, Own& A, Own& B) {
+                                           const f2* hy, const f2* hz, const float* epsc, float h, Own& A, Own& B,
+                                           bool& wide) {
     const int64_t N = d.n;
     const float4* __restrict__ blk = reinterpret_cast<const float4*>(d.nblk);
     const int4 E = __ldg(d.sten_u2 + u);  // (id offset in one box), ox, oy, oz from A
@@ -616,8 +623,9 @@ __device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, int 
                 if (!((SIDES >> side) & 1)) continue;
                 const float4 T = __ldg(tab + (side * nu + u) * 4 + k);  // K lo hi, 1/r^2 lo hi
                 const f2 x0 = f2_add(dx0s[side], hx[k]);
-                pt_force2<HASFAIL>(x0, x1, x2, f2_make(T.x, T.y), f2_make(T.z, T.w), f2_add(du[side][0], gx),
-                                   f2_add(du[side][1], gy), f2_add(du[side][2], gz), epsc[side], F[side]);
+                pt_force2<HASFAIL, SERIES>(x0, x1, x2, f2_make(T.x, T.y), f2_make(T.z, T.w),
+                                           f2_add(du[side][0], gx), f2_add(du[side][1], gy),
+                                           f2_add(du[side][2], gz), epsc[side], F[side], &wide);
             }
         }
     }
@@ -634,11 +642,24 @@ __device__ __forceinline__ void sten_entry(const Dev& d, int u, int64_t ia, int 
     }
 }
 
-// Five blocks per SM (96 registers, 20 warps; 8 bytes of spill): the walk is
-// latency-bound, and 4 blocks at 110 registers measured 5.00 against 4.70 ms
-// per plate step (6 blocks at 80 registers: 4.71, with 104 bytes of spill).
-template <bool HASFAIL, bool BDRY, bool SFAC>
+// Five blocks per SM (96 registers, 20 warps): the walk is latency-bound, and
+// 4 blocks at 110 registers measured 5.00 against 4.70 ms per plate step
+// (6 blocks at 80 registers: 4.71, with 104 bytes of spill).
+// Two passes over the same tiles: EXACT = false evaluates every point with the
+// series form alone (no branch between the point chains: 4.69 -> 3.9 ms of
+// force per plate step); a tile in which any point left the series range
+// stores nothing and is marked in sten_wide.  EXACT = true returns at once
+// for unmarked tiles and evaluates the marked ones with the exact form where
+// needed, then clears the mark.  Every point of every tile therefore takes
+// the same operations as in the single-pass kernel.
+template <bool HASFAIL, bool BDRY, bool SFAC, bool EXACT>
 __global__ void __launch_bounds__(128, 5) k_force_f32c_sten(Dev d, PointPack<8> G, double dts) {
+    if (EXACT) {
+        const bool marked = d.sten_wide[blockIdx.x] != 0;
+        __syncthreads();  // every thread has read the mark before it is cleared
+        if (!marked) return;
+        if (threadIdx.x == 0) d.sten_wide[blockIdx.x] = 0;
+    }
     // the box of this tile: the last whose first tile is at most blockIdx.x
     int lo = 0, hi = d.sten_nbox - 1;
     while (lo < hi) {
@@ -686,6 +707,7 @@ __global__ void __launch_bounds__(128, 5) k_force_f32c_sten(Dev d, PointPack<8> 
     }
     const int nw = d.sten_nw;
     int nba = 0, nbb = 0;
+    bool wide = false;  // a point of this thread left the series range (series pass)
     for (int w = 0; w < nw; ++w) {
         const uint32_t ma = valid ? __ldg(d.sten_mask + (int64_t)w * NP + p) : 0u;
         const uint32_t mb = hb ? __ldg(d.sten_mask + (int64_t)(nw + w) * NP + p) : 0u;
@@ -697,10 +719,17 @@ __global__ void __launch_bounds__(128, 5) k_force_f32c_sten(Dev d, PointPack<8> 
             m &= m - 1;
             const bool ha = ((ma >> bit) & 1u) != 0, hbit = ((mb >> bit) & 1u) != 0;
             const int u = 32 * w + bit;
-            if (ha && hbit) sten_entry<HASFAIL, BDRY, SFAC, 3>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B);
-            else if (ha) sten_entry<HASFAIL, BDRY, SFAC, 1>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B);
-            else if (hbit) sten_entry<HASFAIL, BDRY, SFAC, 2>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B);
+            if (ha && hbit)
+                sten_entry<HASFAIL, BDRY, SFAC, 3, !EXACT>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B, wide);
+            else if (ha)
+                sten_entry<HASFAIL, BDRY, SFAC, 1, !EXACT>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B, wide);
+            else if (hbit)
+                sten_entry<HASFAIL, BDRY, SFAC, 2, !EXACT>(d, u, ia, NX, NXY, hx, hy, hz, epsc, h, A, B, wide);
         }
+    }
+    if (!EXACT && __syncthreads_or(wide)) {  // left to the exact pass: nothing stored
+        if (threadIdx.x == 0) d.sten_wide[blockIdx.x] = 1;
+        return;
     }
     if (valid) store_own<false>(d, ia, A, nba, dts, d.vbuf);
     if (hb) store_own<false>(d, ia + 1, B, nbb, dts, d.vbuf);
@@ -1608,7 +1637,11 @@ void launch_force_f32c(const Dev& d, double dts, cudaStream_t s) {
         const unsigned nbk = (unsigned)d.sten_ntiles;
         const bool bd = d.bdry_on != 0, sf = d.sfac != nullptr;
         const PointPack<8> P = pack_points<8>(d, d.gc_host);
-#define PD_STEN(HF, BD, SF) k_force_f32c_sten<HF, BD, SF><<<nbk, 128, 0, s>>>(d, P, dts)
+#define PD_STEN(HF, BD, SF)                                              \
+    do {                                                                 \
+        k_force_f32c_sten<HF, BD, SF, false><<<nbk, 128, 0, s>>>(d, P, dts); \
+        k_force_f32c_sten<HF, BD, SF, true><<<nbk, 128, 0, s>>>(d, P, dts);  \
+    } while (0)
         if (d.hasfail) {
             if (bd) { if (sf) PD_STEN(true, true, true); else PD_STEN(true, true, false); }
             else { if (sf) PD_STEN(true, false, true); else PD_STEN(true, false, false); }

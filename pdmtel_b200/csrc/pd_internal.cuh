@@ -137,6 +137,7 @@ struct Dev {
     int64_t sten_np;
     int sten_nbox;
     int64_t sten_ntiles;
+    uint8_t* sten_wide;           // [sten_ntiles] 1: the series pass left this tile to the exact pass
     const int4* sten_box;
     const longlong2* sten_boxb;
     const int4* sten_u2;

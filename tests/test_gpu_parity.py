@@ -476,6 +476,45 @@ def test_fp32c_stencil_force_variants_equal_pair_kernel(tmp_path, case):
             assert np.array_equal(U0, U1) and np.array_equal(V0, V1), (name, shape)
 
 
+@pytest.mark.parametrize("shape", [1, 3])
+def test_fp32c_stencil_force_exact_pass_on_large_strains(tmp_path, shape):
+    """Points whose bond strain leaves the series range (|eps| >= 1/64) send
+    their tile of the stencil kernel to its exact pass.  With large random
+    displacements in one end of a plate (some tiles marked, most not) and
+    three RK4 steps from that state, the stencil trajectory still equals the
+    pair kernel's bit for bit."""
+    D.config_plate(dims=(40, 24, 4), spacing=5e-4, slit_half_length=2.5e-3, dt=5e-9, vel=5.0).write(str(tmp_path))
+    dt, h = 5e-9, 5e-4
+    dm0 = gpu_model(str(tmp_path))
+    x = dm0.nodes()[0].reshape(-1, 3)
+    U = np.zeros_like(x)
+    end = x[:, 0] < x[:, 0].min() + 8 * h
+    U[end] = 0.02 * h * np.random.default_rng(11).standard_normal((int(end.sum()), 3))
+    # nearest-neighbour stretches in the loaded end reach well past 1/128
+    # (eps is about twice the stretch, so points leave the series range)
+    i = np.flatnonzero(end)[:200]
+    j = i + 1
+    ok = np.isclose(x[j, 0] - x[i, 0], h)
+    s = (np.linalg.norm(x[j] + U[j] - x[i] - U[i], axis=1) - h) / h
+    assert np.abs(s[ok]).max() > 1.0 / 64
+
+    def run(stencil):
+        dm = gpu_model(str(tmp_path))
+        dm.SetPrecision(P.PREC_FP32C)
+        ctx = dm.context()
+        if stencil:
+            ctx.set_option(P.OPT_FORCE_STENCIL, stencil)
+        ctx.set_state(U.reshape(-1), np.zeros(U.size))
+        ctx.rk4_steps(dt, 0.0, 3)
+        ctx.sync()
+        return ctx.get_state()
+
+    U0, V0 = run(0)
+    U1, V1 = run(shape)
+    assert np.abs(V0).max() > 0
+    assert np.array_equal(U0, U1) and np.array_equal(V0, V1)
+
+
 def test_fp32c_stencil_force_rejects_and_resets(tmp_path):
     """Problems off a complete box lattice are refused (deleted nodes, 3x3x3
     points, CCI); a new bond search turns the stencil force off."""
