@@ -335,6 +335,35 @@ def run_reference_arm(args):
 IDENT = dict(dims=(64, 64, 8), spacing=1e-3, vel=0.02, dt=1e-8, sigma=0.2, corr=5e-3, every=50)
 
 
+def accuracy_leg(ctx, dt, marks=(100, 500)):
+    """The precision form's error over a longer window than the timed steps:
+    the plate from rest in FP32C and in FP64 (untimed, same context and
+    launch shapes), relative L2 error of U and V at each step count."""
+    import numpy as np
+    import pdmtel_b200 as P
+    try:
+        states = {}
+        for name, prec in (("fp32c", P.PREC_FP32C), ("fp64", P.PREC_FP64)):
+            ctx.set_precision(prec)
+            ctx.reset_state()
+            done = 0
+            for m in marks:
+                ctx.rk4_steps(dt, done * dt, m - done)
+                ctx.sync()
+                done = m
+                states[(name, m)] = ctx.get_state()
+        out = {}
+        for m in marks:
+            U32, V32 = states[("fp32c", m)]
+            U64, V64 = states[("fp64", m)]
+            out[str(m)] = {"U": float(np.linalg.norm(U32 - U64) / max(np.linalg.norm(U64), 1e-300)),
+                           "V": float(np.linalg.norm(V32 - V64) / max(np.linalg.norm(V64), 1e-300))}
+        out["note"] = "plate from rest, FP32C against FP64, untimed; keys are RK4 step counts"
+        return out
+    except Exception as e:  # the headline line is printed whatever happens here
+        return {"error": repr(e)}
+
+
 def adjoint_leg(tmp, steps):
     """Seconds per RK4 step of the adjoint pair on the identification
     specimen: pd_adjoint_forward (checkpoints) + pd_adjoint_backward."""
@@ -972,6 +1001,8 @@ def run_ours(args):
                                         "other": prof64[3]}},
         "clocks": clocks, "setup_s": setup_s, "autotune": tune,
     }
+    if rank == 0 and not args.no_accuracy_leg:
+        line["rel_err_vs_fp64_long"] = accuracy_leg(ctx, dt)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = adjoint_leg(tmp, args.adjoint_steps)
     if rank == 0 and not args.no_static:
@@ -1005,6 +1036,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-accuracy-leg", action="store_true",
+                    help="leave out the untimed 100/500-step FP32C-vs-FP64 error check of the headline line")
     ap.add_argument("--no-static", action="store_true", help="leave the static solve out of the headline line")
     ap.add_argument("--shape", default=None,
                     help="skip pd_autotune and apply these launch shapes, a JSON object with keys of its result "
