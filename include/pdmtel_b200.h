@@ -412,6 +412,10 @@ int pd_static_solve(pd_ctx* ctx, double time, int precision, double rtol, int ma
  *   and the results agree to FP32 rounding).
  *   Turning it on or off changes the layout of the node blocks that
  *   pd_gather stores for pd_force_stage: gather again after the change.
+ *   Each force stage is two launches on the context's stream: a pass that
+ *   evaluates every Gauss point with the strain series alone, then a pass
+ *   that redoes, with the exact form where needed, only the tiles in which
+ *   a point left the series range (one byte per tile, kept by the context).
  * PD_OPT_GATHER_STENCIL: 1 lets the FP32-form gather (one thread per four
  *   points) take every node's MLS contributors from a pattern of id offsets
  *   (nodes whose lists are translates of each other share one; kept with
